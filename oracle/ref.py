@@ -1,0 +1,89 @@
+"""Loaders for the reference's own CPU code compiled into ``oracle/_ref/``.
+
+TEST INFRASTRUCTURE ONLY.  ``make -C oracle ref`` compiles, in place from the
+pHyFlow sources, the Cython direct Gauss kernel
+(``src/cpp/blobs/cython/vv2parGauss_Cython/vv2parGauss_Cython_cpu.pyx``), the
+Cython vortex-panel kernel
+(``src/cpp/panels/cython/vortexPanel_Cython/_vortexPanel_Cython_cpu.pyx``) and
+the C++ CPU FMM (``src/cpp/blobs/c++/fmm2d_py_cpu_gpu/*.cpp`` behind
+``oracle/ref_fmm_driver.cpp``).  The built files travel with the repository
+snapshot; the sources they were built from do not.
+"""
+import ctypes
+import importlib.util
+import os
+import sysconfig
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(_HERE, "_ref")
+_SUF = sysconfig.get_config_var("EXT_SUFFIX")
+_cache = {}
+
+# constant of the Oseen smoother in the reference FMM binding
+# (src/python/blobs/base/induced/_induced.py:239)
+FMM_ALPHA = 1.2564312086261696770
+
+
+def available():
+    return all(os.path.exists(p) for p in (
+        os.path.join(REF_DIR, "vv2parGauss_Cython_cpu" + _SUF),
+        os.path.join(REF_DIR, "_vortexPanel_Cython_cpu" + _SUF),
+        os.path.join(REF_DIR, "libreffmm.so")))
+
+
+def _module(name):
+    if name not in _cache:
+        path = os.path.join(REF_DIR, name + _SUF)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle ref` where the reference exists")
+        spec = importlib.util.spec_from_file_location(name, path)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _cache[name] = mod
+    return _cache[name]
+
+
+def direct_gauss(x, y, g, ksigmasqr):
+    """Reference Cython direct sum at the blobs themselves -> (vx, vy)."""
+    blobs = np.ascontiguousarray(np.stack([x, y, g], axis=1), dtype=np.float64)
+    v = _module("vv2parGauss_Cython_cpu").vv2parGauss_Cython_cpu(blobs, float(ksigmasqr))
+    return np.array(v[:, 0]), np.array(v[:, 1])
+
+
+def panel_velocity(gamma, xs, ys, xe, ye, cosa, sina, xv, yv):
+    """Reference Cython vortex-panel induced velocity -> (vx, vy)."""
+    f = [np.ascontiguousarray(a, dtype=np.float64) for a in (gamma, xv, yv, xs, ys, xe, ye, cosa, sina)]
+    vx, vy = _module("_vortexPanel_Cython_cpu").inducedVelocity(*f)
+    return np.array(vx), np.array(vy)
+
+
+def _fmm_lib():
+    if "fmm" not in _cache:
+        path = os.path.join(REF_DIR, "libreffmm.so")
+        lib = ctypes.CDLL(path)
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.ref_fmm2d.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, dp, dp, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, dp, dp]
+        lib.ref_fmm2d.restype = None
+        _cache["fmm"] = lib
+    return _cache["fmm"]
+
+
+def fmm_velocity(x, y, g, sigma, k=2.0, xt=None, yt=None, ndirect=35, tol=1e-6, cutoff=None):
+    """Reference CPU FMM, mapped to velocities as the reference Python layer
+    does (``_induced.py:236-251``): vx = -qi/(2 pi), vy = -qr/(2 pi)."""
+    x, y, g = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, g))
+    xt = x if xt is None else np.ascontiguousarray(xt, dtype=np.float64)
+    yt = y if yt is None else np.ascontiguousarray(yt, dtype=np.float64)
+    xopt = np.sqrt(FMM_ALPHA * k * sigma * sigma)
+    if cutoff is None:
+        cutoff = 5.0 * xopt
+    qr = np.zeros(xt.shape[0])
+    qi = np.zeros(xt.shape[0])
+    dp = ctypes.POINTER(ctypes.c_double)
+    p = lambda a: a.ctypes.data_as(dp)
+    _fmm_lib().ref_fmm2d(x.shape[0], p(x), p(y), p(g), xt.shape[0], p(xt), p(yt), int(ndirect),
+                         float(xopt), float(cutoff), float(tol), p(qr), p(qi))
+    return -qi / (2.0 * np.pi), -qr / (2.0 * np.pi)

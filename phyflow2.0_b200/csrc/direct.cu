@@ -1,0 +1,143 @@
+// direct.cu -- Gaussian-blob Biot-Savart velocity by direct summation.
+//
+// One simulation per launch (the plain path).  Each CTA owns DT_THREADS*TPT
+// targets (TPT per thread, coalesced); all CTAs stream the whole source set
+// through shared memory in tiles of DT_THREADS blobs, converted on load from
+// FP64 to hi/lo float pairs (so no scratch buffer is needed).  Per thread the
+// pair sums run in FP32 over chunks of 32 sources and are folded into a
+// TwoSum-compensated (hi, lo) accumulator after each chunk.
+//
+// Replaces vv2par_kernel (src/cpp/blobs/cuda/vv2parGauss_gpu/
+// vv2parGauss_device.cu:107-162: FP64, one target per thread, 2 exp per pair,
+// targets padded to a multiple of the block size by the Python caller).
+#include "gauss_pair.cuh"
+
+namespace {
+
+constexpr int DT_THREADS = 256;
+constexpr int DT_CHUNK = 32;
+constexpr double INV_2PI = 0.15915494309189535;  // 0.5/pi
+
+template <int TPT>
+__global__ void __launch_bounds__(DT_THREADS)
+k_direct_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
+               const double *__restrict__ gs, int64_t ns, const double *__restrict__ xt,
+               const double *__restrict__ yt, int64_t nt, pfd::GaussParams gp,
+               double *__restrict__ vx, double *__restrict__ vy) {
+    __shared__ float4 s_pos[DT_THREADS];  // x_hi, y_hi, x_lo, y_lo
+    __shared__ float s_g[DT_THREADS];
+
+    const int64_t base = (int64_t)blockIdx.x * (DT_THREADS * TPT) + threadIdx.x;
+    float txh[TPT], txl[TPT], tyh[TPT], tyl[TPT];
+    float hx[TPT], lx[TPT], hy[TPT], ly[TPT];
+#pragma unroll
+    for (int j = 0; j < TPT; ++j) {
+        int64_t i = base + (int64_t)j * DT_THREADS;
+        double x = 0.0, y = 0.0;
+        if (i < nt) {
+            x = xt[i];
+            y = yt[i];
+        }
+        pfd::split_hilo(x, txh[j], txl[j]);
+        pfd::split_hilo(y, tyh[j], tyl[j]);
+        hx[j] = lx[j] = hy[j] = ly[j] = 0.0f;
+    }
+
+    for (int64_t t0 = 0; t0 < ns; t0 += DT_THREADS) {
+        const int64_t s = t0 + threadIdx.x;
+        double x = 0.0, y = 0.0, g = 0.0;  // padding blobs carry g = 0
+        if (s < ns) {
+            x = xs[s];
+            y = ys[s];
+            g = gs[s];
+        }
+        float4 p;
+        pfd::split_hilo(x, p.x, p.z);
+        pfd::split_hilo(y, p.y, p.w);
+        __syncthreads();
+        s_pos[threadIdx.x] = p;
+        s_g[threadIdx.x] = (float)g;
+        __syncthreads();
+        const int nvalid = (int)min((int64_t)DT_THREADS, ns - t0);
+        for (int c0 = 0; c0 < nvalid; c0 += DT_CHUNK) {
+            float px[TPT], py[TPT];
+#pragma unroll
+            for (int j = 0; j < TPT; ++j) px[j] = py[j] = 0.0f;
+#pragma unroll 4
+            for (int k = 0; k < DT_CHUNK; ++k) {
+                const float4 q = s_pos[c0 + k];
+                const float gk = s_g[c0 + k];
+#pragma unroll
+                for (int j = 0; j < TPT; ++j) {
+                    const float dx = (txh[j] - q.x) + (txl[j] - q.z);
+                    const float dy = (tyh[j] - q.y) + (tyl[j] - q.w);
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
+                    const float sc = pfd::gauss_s(r2, gk, gp);
+                    px[j] = fmaf(-dy, sc, px[j]);
+                    py[j] = fmaf(dx, sc, py[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < TPT; ++j) {
+                pfd::comp_add(hx[j], lx[j], px[j]);
+                pfd::comp_add(hy[j], ly[j], py[j]);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < TPT; ++j) {
+        int64_t i = base + (int64_t)j * DT_THREADS;
+        if (i < nt) {
+            vx[i] = INV_2PI * ((double)hx[j] + (double)lx[j]);
+            vy[i] = INV_2PI * ((double)hy[j] + (double)ly[j]);
+        }
+    }
+}
+
+}  // namespace
+
+namespace pf {
+
+// Launch the plain direct sum on `stream` (no argument checks; used internally
+// by the FMM's tol == 0 path and by the C-ABI entry below).
+pf_status launch_direct(int64_t ns, const double *x, const double *y, const double *g,
+                        int64_t nt, const double *xt, const double *yt, double ksigmasqr,
+                        double *vx, double *vy, cudaStream_t stream) {
+    if (nt == 0) return PF_OK;
+    const pfd::GaussParams gp = pfd::make_gauss_params(ksigmasqr);
+    constexpr int TPT = 2;
+    const int64_t per = DT_THREADS * TPT;
+    const int64_t grid = ceil_div(nt, per);
+    if (grid > INT32_MAX) {
+        set_error("pf_velocity_direct: too many targets (%lld)", (long long)nt);
+        return PF_ERR_INVALID_ARG;
+    }
+    k_direct_gauss<TPT><<<(unsigned)grid, DT_THREADS, 0, stream>>>(x, y, g, ns, xt, yt, nt, gp,
+                                                                   vx, vy);
+    return launch_status("k_direct_gauss");
+}
+
+}  // namespace pf
+
+extern "C" pf_status pf_velocity_direct(pf_ctx *ctx, int64_t n_src, const double *x,
+                                        const double *y, const double *g, int64_t n_tgt,
+                                        const double *xt, const double *yt, double ksigmasqr,
+                                        double *vx, double *vy, void *stream) {
+    pf::clear_error();
+    PF_CHECK_ARG(ctx != nullptr, "pf_velocity_direct: NULL context");
+    PF_CHECK_ARG(n_src >= 0 && n_tgt >= 0, "pf_velocity_direct: negative size");
+    PF_CHECK_ARG(ksigmasqr > 0.0 && ksigmasqr < 1e300,
+                 "pf_velocity_direct: ksigmasqr must be positive and finite (got %g)", ksigmasqr);
+    PF_CHECK_ARG(n_src == 0 || (x && y && g), "pf_velocity_direct: NULL blob array");
+    PF_CHECK_ARG(n_tgt == 0 || (xt && yt && vx && vy),
+                 "pf_velocity_direct: NULL target/output array");
+    pf::DeviceGuard dg(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n_tgt == 0) return PF_OK;
+    if (n_src == 0) {
+        PF_CUDA_TRY(cudaMemsetAsync(vx, 0, sizeof(double) * n_tgt, st));
+        PF_CUDA_TRY(cudaMemsetAsync(vy, 0, sizeof(double) * n_tgt, st));
+        return PF_OK;
+    }
+    return pf::launch_direct(n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
+}

@@ -1,0 +1,134 @@
+// pf_common.cuh -- shared host/device helpers of libpfblob.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "../../include/pfblob.h"
+
+#define PF_VERSION 10000
+
+namespace pf {
+
+// --------------------------------------------------------------------------
+// Error plumbing: every C-ABI entry returns a pf_status and stores a message
+// in a thread-local buffer read by pf_last_error().
+void set_error(const char *fmt, ...);
+void clear_error();
+
+#define PF_CUDA_TRY(expr)                                                         \
+    do {                                                                          \
+        cudaError_t pf_e_ = (expr);                                               \
+        if (pf_e_ != cudaSuccess) {                                               \
+            ::pf::set_error("%s failed: %s (%s:%d)", #expr,                       \
+                            cudaGetErrorString(pf_e_), __FILE__, __LINE__);       \
+            return PF_ERR_CUDA;                                                   \
+        }                                                                         \
+    } while (0)
+
+#define PF_CHECK_ARG(cond, ...)                                                   \
+    do {                                                                          \
+        if (!(cond)) {                                                            \
+            ::pf::set_error(__VA_ARGS__);                                         \
+            return PF_ERR_INVALID_ARG;                                            \
+        }                                                                         \
+    } while (0)
+
+#define PF_TRY(expr)                                                              \
+    do {                                                                          \
+        pf_status pf_s_ = (expr);                                                 \
+        if (pf_s_ != PF_OK) return pf_s_;                                         \
+    } while (0)
+
+// Last launch error of this thread, as a status.  Every kernel launch site
+// calls it right after the launch, which also counts the launch.
+pf_status launch_status(const char *what);
+
+// --------------------------------------------------------------------------
+// Device scratch arena: one grow-only allocation per context, carved into
+// 256-byte aligned slices per call (stack discipline: reset at call start).
+struct Arena {
+    char *base = nullptr;
+    size_t cap = 0;
+    size_t used = 0;
+};
+
+}  // namespace pf
+
+struct pf_ctx {
+    int device = 0;
+    int num_sms = 0;
+    size_t smem_optin = 0;
+    pf::Arena arena;
+    // host-side pinned staging for small device->host reads
+    int64_t *host_small = nullptr;
+};
+
+namespace pf {
+
+// Make sure the arena holds at least `bytes`; may cudaFree/cudaMalloc, which
+// synchronises the device.  Done before any kernel of a call is enqueued.
+pf_status arena_reserve(pf_ctx *ctx, size_t bytes);
+// Carve a slice (after arena_reserve made room).  Returns nullptr if out of room.
+void *arena_take(pf_ctx *ctx, size_t bytes);
+inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace pf
+
+// --------------------------------------------------------------------------
+// Device helpers
+namespace pfd {
+
+// Split a double into a float pair (hi + lo == x to ~2^-48 relative).
+__device__ __forceinline__ void split_hilo(double x, float &hi, float &lo) {
+    hi = __double2float_rn(x);
+    lo = __double2float_rn(x - (double)hi);
+}
+
+// Knuth TwoSum: s + e == a + b exactly.
+__device__ __forceinline__ void two_sum(float a, float b, float &s, float &e) {
+    s = __fadd_rn(a, b);
+    float bb = __fsub_rn(s, a);
+    e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+// Compensated accumulator: fold a partial sum p into (hi, lo).
+__device__ __forceinline__ void comp_add(float &hi, float &lo, float p) {
+    float s, e;
+    two_sum(hi, p, s, e);
+    hi = s;
+    lo = __fadd_rn(lo, e);
+}
+
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+}  // namespace pfd

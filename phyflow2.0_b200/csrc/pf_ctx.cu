@@ -1,0 +1,147 @@
+// pf_ctx.cu -- context, scratch arena and error reporting of libpfblob.
+#include "pf_common.cuh"
+
+#include <atomic>
+#include <cstring>
+#include <new>
+
+namespace pf {
+
+static thread_local char g_err[1024] = {0};
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+void clear_error() { g_err[0] = 0; }
+
+static std::atomic<uint64_t> g_launches{0};
+
+pf_status launch_status(const char *what) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("launch of %s failed: %s", what, cudaGetErrorString(e));
+        return PF_ERR_CUDA;
+    }
+    return PF_OK;
+}
+
+pf_status arena_reserve(pf_ctx *ctx, size_t bytes) {
+    ctx->arena.used = 0;
+    if (bytes <= ctx->arena.cap) return PF_OK;
+    // grow geometrically so that size sweeps do not reallocate every call
+    size_t want = ctx->arena.cap ? ctx->arena.cap : (size_t(1) << 20);
+    while (want < bytes) want *= 2;
+    if (ctx->arena.base) {
+        // the old slice may still be read by queued work of an earlier call
+        PF_CUDA_TRY(cudaDeviceSynchronize());
+        PF_CUDA_TRY(cudaFree(ctx->arena.base));
+        ctx->arena.base = nullptr;
+        ctx->arena.cap = 0;
+    }
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        // retry with the exact size before giving up
+        e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("scratch arena: cudaMalloc of %zu bytes failed (%s)", bytes,
+                      cudaGetErrorString(e));
+            return PF_ERR_OOM;
+        }
+        want = bytes;
+    }
+    ctx->arena.base = static_cast<char *>(p);
+    ctx->arena.cap = want;
+    return PF_OK;
+}
+
+void *arena_take(pf_ctx *ctx, size_t bytes) {
+    size_t b = align256(bytes);
+    if (ctx->arena.used + b > ctx->arena.cap) return nullptr;
+    void *p = ctx->arena.base + ctx->arena.used;
+    ctx->arena.used += b;
+    return p;
+}
+
+}  // namespace pf
+
+extern "C" {
+
+pf_status pf_create(int device, pf_ctx **out) {
+    pf::clear_error();
+    PF_CHECK_ARG(out != nullptr, "pf_create: out is NULL");
+    *out = nullptr;
+    int n = 0;
+    PF_CUDA_TRY(cudaGetDeviceCount(&n));
+    PF_CHECK_ARG(device >= 0 && device < n, "pf_create: device %d out of range (%d devices)",
+                 device, n);
+    pf::DeviceGuard dg(device);
+    pf_ctx *c = new (std::nothrow) pf_ctx();
+    if (!c) {
+        pf::set_error("pf_create: host allocation failed");
+        return PF_ERR_OOM;
+    }
+    c->device = device;
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) {
+        delete c;
+        pf::set_error("cudaGetDeviceProperties failed: %s", cudaGetErrorString(e));
+        return PF_ERR_CUDA;
+    }
+    c->num_sms = prop.multiProcessorCount;
+    c->smem_optin = prop.sharedMemPerBlockOptin;
+    e = cudaMallocHost(&c->host_small, 4096);
+    if (e != cudaSuccess) {
+        delete c;
+        pf::set_error("cudaMallocHost failed: %s", cudaGetErrorString(e));
+        return PF_ERR_CUDA;
+    }
+    *out = c;
+    return PF_OK;
+}
+
+pf_status pf_destroy(pf_ctx *ctx) {
+    pf::clear_error();
+    if (!ctx) return PF_OK;
+    pf::DeviceGuard dg(ctx->device);
+    cudaDeviceSynchronize();
+    if (ctx->arena.base) cudaFree(ctx->arena.base);
+    if (ctx->host_small) cudaFreeHost(ctx->host_small);
+    delete ctx;
+    return PF_OK;
+}
+
+const char *pf_last_error(void) { return pf::g_err; }
+
+pf_status pf_mem_usage(const pf_ctx *ctx, size_t *bytes) {
+    PF_CHECK_ARG(ctx && bytes, "pf_mem_usage: NULL argument");
+    *bytes = ctx->arena.cap;
+    return PF_OK;
+}
+
+pf_status pf_trim(pf_ctx *ctx) {
+    PF_CHECK_ARG(ctx, "pf_trim: NULL context");
+    pf::DeviceGuard dg(ctx->device);
+    if (ctx->arena.base) {
+        PF_CUDA_TRY(cudaDeviceSynchronize());
+        PF_CUDA_TRY(cudaFree(ctx->arena.base));
+    }
+    ctx->arena.base = nullptr;
+    ctx->arena.cap = 0;
+    ctx->arena.used = 0;
+    return PF_OK;
+}
+
+int pf_version(void) { return PF_VERSION; }
+
+uint64_t pf_kernel_launches(void) { return pf::g_launches.load(std::memory_order_relaxed); }
+
+}  // extern "C"

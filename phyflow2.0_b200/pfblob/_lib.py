@@ -1,0 +1,111 @@
+"""ctypes binding of libpfblob.so (the C ABI declared in include/pfblob.h).
+
+The library is required: importing this module raises if the shared object
+is missing or fails to load.  There is no CPU path behind it.
+"""
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpfblob.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"pfblob: {LIB_PATH} is not built; run `python phyflow2.0_b200/build.py` "
+        "(the package has no CPU fallback)")
+
+lib = ctypes.CDLL(LIB_PATH)
+
+_c = ctypes
+_vp = _c.c_void_p
+_i64 = _c.c_int64
+_dbl = _c.c_double
+_int = _c.c_int
+
+PF_OK = 0
+STATUS_NAMES = {0: "PF_OK", 1: "PF_ERR_INVALID_ARG", 2: "PF_ERR_OOM", 3: "PF_ERR_CUDA",
+                4: "PF_ERR_TIMEOUT", 5: "PF_ERR_NAN_INPUT", 6: "PF_ERR_CAPACITY",
+                7: "PF_ERR_NOT_BUILT"}
+
+# (name, argtypes) for every entry point declared in include/pfblob.h
+PROTOTYPES = {
+    "pf_create": [_int, _c.POINTER(_vp)],
+    "pf_destroy": [_vp],
+    "pf_last_error": [],
+    "pf_mem_usage": [_vp, _c.POINTER(_c.c_size_t)],
+    "pf_trim": [_vp],
+    "pf_version": [],
+    "pf_kernel_launches": [],
+    "pf_velocity_direct": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _vp, _vp, _vp],
+    "pf_velocity_fmm": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _int,
+                        _vp, _vp, _vp],
+    "pf_panel_velocity": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp,
+                          _int, _vp],
+    "pf_remesh": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp, _vp, _vp,
+                  _c.POINTER(_i64), _vp],
+    "pf_moments": [_vp, _i64, _vp, _vp, _vp, _vp, _vp],
+}
+
+for _name, _args in PROTOTYPES.items():
+    if not hasattr(lib, _name):
+        continue  # optional entry points are checked by the symbol test
+    f = getattr(lib, _name)
+    f.argtypes = _args
+    f.restype = _int
+lib.pf_last_error.restype = _c.c_char_p
+lib.pf_version.restype = _int
+lib.pf_kernel_launches.restype = _c.c_uint64
+
+
+class PfError(RuntimeError):
+    """A libpfblob call returned a status other than PF_OK."""
+
+    def __init__(self, status, msg):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+
+
+class CapacityError(PfError):
+    def __init__(self, status, msg, needed):
+        self.needed = needed
+        super().__init__(status, msg)
+
+
+def check(status):
+    if status != PF_OK:
+        msg = lib.pf_last_error()
+        raise PfError(status, msg.decode() if msg else "")
+
+
+_ctx_lock = threading.Lock()
+_ctx = {}
+
+
+def context(device=0):
+    """Per-(device, thread) pf_ctx handle (contexts are not shared between
+    host threads)."""
+    key = (device, threading.get_ident())
+    with _ctx_lock:
+        h = _ctx.get(key)
+        if h is None:
+            p = _vp()
+            check(lib.pf_create(int(device), _c.byref(p)))
+            h = p.value
+            _ctx[key] = h
+    return h
+
+
+def mem_usage(device=0):
+    n = _c.c_size_t()
+    check(lib.pf_mem_usage(context(device), _c.byref(n)))
+    return n.value
+
+
+def version():
+    return lib.pf_version()
+
+
+def kernel_launches():
+    """Process-wide number of library kernel launches so far."""
+    return int(lib.pf_kernel_launches())

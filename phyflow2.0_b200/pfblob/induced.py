@@ -1,0 +1,90 @@
+"""Blob induced velocity with pHyFlow's call surface.
+
+``velocity`` keeps the signature, argument meaning and option constants of
+``pHyFlow.blobs.base.induced.velocity`` (``src/python/blobs/base/induced/
+_induced.py:34-166``): ``fullOption = 100*method + 10*hardware + kernel``
+selects direct or FMM summation of the Gaussian kernel.
+
+Differences, by design of this library:
+* every combination runs on the B200 (``hardware`` is accepted for
+  compatibility; there is no CPU path);
+* the cutoff kernel (``kernel=0``) is outside this library's scope and raises,
+  as the reference does for its unsupported combinations (:159-163);
+* ``blocksize`` is accepted and ignored: no padding is needed.
+"""
+import ctypes
+import math
+
+import torch
+
+from . import _lib
+from ._arrays import Marshal, ptr
+
+GAUSS_KERNEL = 1
+CUTOFF_KERNEL = 0
+CPU_HARDWARE = 0
+GPU_HARDWARE = 1
+FMM_METHOD = 0
+DIRECT_METHOD = 1
+
+# Oseen smoother constant of the reference FMM binding (_induced.py:239, :321)
+FMM_ALPHA = 1.2564312086261696770
+
+
+def fmm_parameters(sigma, k=2.0, cutoff=None):
+    """(ksigmasqr, xopt, cutoff) as ``_velocity_fmm_*_gauss`` derives them."""
+    ksigmasqr = k * sigma * sigma
+    xopt = math.sqrt(FMM_ALPHA * ksigmasqr)
+    if cutoff is None:
+        cutoff = 5.0 * xopt
+    return ksigmasqr, xopt, cutoff
+
+
+def velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=DIRECT_METHOD, xopt=None,
+                    cutoff=None, tol=1e-6, ndirect=35, stream=None, device=None):
+    """Device-tensor entry: all arguments CUDA float64 tensors; writes vx, vy."""
+    dev = x.device.index if device is None else device
+    st = ctypes.c_void_p(torch.cuda.current_stream(x.device).cuda_stream if stream is None
+                         else stream)
+    ctx = _lib.context(dev)
+    if method == DIRECT_METHOD or tol == 0.0:
+        _lib.check(_lib.lib.pf_velocity_direct(ctx, x.numel(), ptr(x), ptr(y), ptr(g), xt.numel(),
+                                               ptr(xt), ptr(yt), float(ksigmasqr), ptr(vx),
+                                               ptr(vy), st))
+    else:
+        if xopt is None:
+            xopt = math.sqrt(FMM_ALPHA * ksigmasqr)
+        if cutoff is None:
+            cutoff = 5.0 * xopt
+        _lib.check(_lib.lib.pf_velocity_fmm(ctx, x.numel(), ptr(x), ptr(y), ptr(g), xt.numel(),
+                                            ptr(xt), ptr(yt), float(ksigmasqr), float(xopt),
+                                            float(cutoff), float(tol), int(ndirect), ptr(vx),
+                                            ptr(vy), st))
+
+
+def velocity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None, hardware=0,
+             blocksize=128, method=0, Ndirect=35, tol=1.0e-6, cutoff=None):
+    """Induced velocity of Gaussian vortex blobs at (xEval, yEval).
+
+    Same arguments and return value as pHyFlow's ``velocity``; returns
+    ``(vx, vy)`` as numpy arrays for numpy input, CUDA tensors for CUDA input.
+    """
+    if kernel != GAUSS_KERNEL:
+        raise NotImplementedError("pfblob: only the Gaussian kernel (kernel=1) is provided")
+    if method not in (FMM_METHOD, DIRECT_METHOD):
+        raise ValueError(f"pfblob: unknown method {method}")
+    m = Marshal(xBlob.device.index if isinstance(xBlob, torch.Tensor) and xBlob.is_cuda else None)
+    x, y, g = m.dev(xBlob), m.dev(yBlob), m.dev(wBlob)
+    if not (x.numel() == y.numel() == g.numel()):
+        raise ValueError("pfblob: xBlob, yBlob, wBlob must have the same length")
+    if xEval is None:
+        xt, yt = x, y
+    else:
+        xt, yt = m.dev(xEval), m.dev(yEval)
+        if xt.numel() != yt.numel():
+            raise ValueError("pfblob: xEval and yEval must have the same length")
+    vx, vy = m.empty(xt.numel()), m.empty(xt.numel())
+    ksigmasqr, xopt, cut = fmm_parameters(float(sigma), float(k), cutoff)
+    velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=method, xopt=xopt, cutoff=cut,
+                    tol=float(tol), ndirect=int(Ndirect), device=m.index)
+    return m.out(vx), m.out(vy)

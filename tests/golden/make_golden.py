@@ -1,0 +1,157 @@
+"""Generate the golden fixtures in tests/golden/ from the reference's own code.
+
+Run here, where the pHyFlow sources exist (they do not travel with the repo):
+
+    make -C oracle ref
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+Sources of truth:
+* direct Gauss velocity   - the reference Cython kernel
+  (src/cpp/blobs/cython/vv2parGauss_Cython/vv2parGauss_Cython_cpu.pyx), built
+  into oracle/_ref/;
+* vortex-panel velocity   - the reference Cython panel kernel
+  (src/cpp/panels/cython/vortexPanel_Cython/_vortexPanel_Cython_cpu.pyx);
+* remesh                  - the reference ``Regrid`` itself
+  (src/python/blobs/base/regrid/_regridding.py), imported under Python 3 with
+  stub modules for its two pHyFlow imports: ``blobOptions`` (the constant
+  M4PRIME_INTERPKERNEL = 0) and ``m4kernel_1d``, which the reference builds
+  with boost.python and which is supplied here by our C restatement of
+  _interpolation_kernels_1d.cpp:75-89;
+* FMM                     - the reference C++ CPU FMM (oracle/_ref/libreffmm.so).
+
+The fixtures are small .npz files; the generating code is this script.
+"""
+import argparse
+import ast
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "phyflow2.0_b200"))
+
+import oracle  # noqa: E402
+from oracle import ref  # noqa: E402
+from pfblob import workloads as wl  # noqa: E402
+
+
+def load_reference_regrid(refroot):
+    """Import the reference _regridding.py with stub pHyFlow modules."""
+    pk = types.ModuleType("pHyFlow")
+    blobs = types.ModuleType("pHyFlow.blobs")
+    opts = types.ModuleType("pHyFlow.blobs.blobOptions")
+    opts.M4PRIME_INTERPKERNEL = 0
+    blobs.blobOptions = opts
+    cpp = types.ModuleType("pHyFlow.cpp")
+    cppb = types.ModuleType("pHyFlow.cpp.blobs")
+    rem = types.ModuleType("pHyFlow.cpp.blobs.remesh")
+    rem.m4kernel_1d = lambda x, c: oracle.m4prime(np.asarray(x).ravel(), c)
+    rem.__all__ = ["m4kernel_1d"]
+    for name, mod in [("pHyFlow", pk), ("pHyFlow.blobs", blobs), ("pHyFlow.blobs.blobOptions", opts),
+                      ("pHyFlow.cpp", cpp), ("pHyFlow.cpp.blobs", cppb),
+                      ("pHyFlow.cpp.blobs.remesh", rem)]:
+        sys.modules[name] = mod
+    path = os.path.join(refroot, "src/python/blobs/base/regrid/_regridding.py")
+    # The module is Python 2 code: `/` between two ints is floor division
+    # there (``kernelSize/2`` at :201-218).  Compile it with every `/` routed
+    # through a helper with Python 2 semantics; nothing else is changed.
+    tree = ast.parse(open(path).read(), filename=path)
+
+    class Py2Div(ast.NodeTransformer):
+        def visit_BinOp(self, node):
+            self.generic_visit(node)
+            if isinstance(node.op, ast.Div):
+                return ast.copy_location(ast.Call(func=ast.Name("_py2div", ast.Load()),
+                                                  args=[node.left, node.right], keywords=[]), node)
+            return node
+
+    tree = ast.fix_missing_locations(Py2Div().visit(tree))
+    mod = types.ModuleType("ref_regridding")
+    mod.__file__ = path
+    mod._py2div = lambda a, b: a // b if (isinstance(a, int) and isinstance(b, int)) else a / b
+    exec(compile(tree, path, "exec"), mod.__dict__)
+    return mod
+
+
+def rand_blobs(n, sigma, seed, lo=0.0, hi=1.0):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    x = rng.uniform(lo, hi, n)
+    y = rng.uniform(lo, hi, n)
+    g = rng.standard_normal(n) / n
+    return x, y, g, sigma
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    assert ref.available(), "build oracle/_ref first: make -C oracle ref"
+
+    # 1. direct Gauss, C1 Lamb-Oseen lattice (N = 10 000)
+    c1 = wl.lamb_oseen_lattice()
+    vx, vy = ref.direct_gauss(c1.x, c1.y, c1.g, c1.ksigmasqr)
+    np.savez_compressed(os.path.join(HERE, "direct_c1.npz"), x=c1.x, y=c1.y, g=c1.g,
+                        ksigmasqr=c1.ksigmasqr, sigma=c1.sigma, vx=vx, vy=vy)
+
+    # 2. direct Gauss, random blobs with edge cases: a duplicated blob (r = 0
+    #    between distinct blobs, EPS path), a zero-circulation blob, a far blob
+    x, y, g, sigma = rand_blobs(3000, 0.01, 7)
+    x[10], y[10] = x[11], y[11]
+    g[20] = 0.0
+    x[30], y[30] = 25.0, -13.0
+    k2 = 2.0 * sigma * sigma
+    vx, vy = ref.direct_gauss(x, y, g, k2)
+    np.savez_compressed(os.path.join(HERE, "direct_rand.npz"), x=x, y=y, g=g, ksigmasqr=k2,
+                        sigma=sigma, vx=vx, vy=vy)
+
+    # 3. vortex panels: 64 panels on the unit cylinder, targets around it,
+    #    including points on a panel line extension and very close to panels
+    ps = wl.cylinder_panels(64, config=3, instance=7)
+    rng = np.random.Generator(np.random.PCG64(11))
+    r = rng.uniform(1.0005, 3.0, 2000)
+    t = rng.uniform(-np.pi, np.pi, 2000)
+    xv = r * np.cos(t)
+    yv = r * np.sin(t)
+    # points on the extension of panel 0 and right next to its midpoint
+    dx, dy = ps.xe[0] - ps.xs[0], ps.ye[0] - ps.ys[0]
+    xv[:3] = ps.xe[0] + dx * np.array([0.5, 1.0, 3.0])
+    yv[:3] = ps.ye[0] + dy * np.array([0.5, 1.0, 3.0])
+    xv[3] = 0.5 * (ps.xs[0] + ps.xe[0]) - 1e-6 * dy
+    yv[3] = 0.5 * (ps.ys[0] + ps.ye[0]) + 1e-6 * dx
+    vx, vy = ref.panel_velocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina, xv, yv)
+    np.savez_compressed(os.path.join(HERE, "panel_cyl.npz"), gamma=ps.gamma, xs=ps.xs, ys=ps.ys,
+                        xe=ps.xe, ye=ps.ye, cosa=ps.cosa, sina=ps.sina, xv=xv, yv=yv, vx=vx, vy=vy)
+
+    # 4. remesh through the reference Regrid: C1 lattice, and random blobs with
+    #    and without the Wee diffusion term, and blobs sitting exactly on nodes
+    R = load_reference_regrid(args.ref)
+    xb, yb = c1.bounds()
+    xn, yn, gn = R.Regrid(c1.x, c1.y, c1.g, c1.sigma, c1.overlap, xb, yb, 0, 0.0)
+    np.savez_compressed(os.path.join(HERE, "regrid_c1.npz"), x=c1.x, y=c1.y, g=c1.g,
+                        sigma=c1.sigma, overlap=c1.overlap, xb=xb, yb=yb, c=0.0,
+                        xn=xn, yn=yn, gn=gn)
+    x, y, g, sigma = rand_blobs(2000, 0.01, 13, -0.3, 0.4)
+    h = sigma * 0.8
+    # blobs exactly on lattice nodes: |u| hits 0, 1 and 2 exactly
+    x[:50] = (np.arange(50) - 20) * h + 0.5 * h + (-1.5 * h)
+    y[:50] = 0.5 * h + (-1.5 * h)
+    for tag, c in (("c0", 0.0), ("c3", 0.3)):
+        xb = np.array([-1.5 * h, 1.5 * h])
+        xn, yn, gn = R.Regrid(x, y, g, sigma, 0.8, xb, xb, 0, c)
+        np.savez_compressed(os.path.join(HERE, f"regrid_rand_{tag}.npz"), x=x, y=y, g=g,
+                            sigma=sigma, overlap=0.8, xb=xb, yb=xb, c=c, xn=xn, yn=yn, gn=gn)
+
+    # 5. reference CPU FMM on random blobs (cross-check of the FMM path)
+    x, y, g, sigma = rand_blobs(4096, 0.01, 17)
+    vx, vy = ref.fmm_velocity(x, y, g, sigma, tol=1e-6)
+    np.savez_compressed(os.path.join(HERE, "fmm_rand.npz"), x=x, y=y, g=g, sigma=sigma,
+                        tol=1e-6, vx=vx, vy=vy)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,60 @@
+"""The C ABI library loads and exports every symbol include/pfblob.h declares
+(no compute: these run without a GPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "pfblob.h")
+LIB = os.path.join(ROOT, "phyflow2.0_b200", "pfblob", "libpfblob.so")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(pf_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ("pf_create", "pf_destroy", "pf_last_error", "pf_velocity_direct", "pf_velocity_fmm",
+              "pf_panel_velocity", "pf_remesh", "pf_moments"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(LIB)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, f"libpfblob.so lacks {missing}"
+
+
+def test_python_prototypes_cover_header():
+    import pfblob._lib as L
+    assert set(declared_symbols()) <= set(L.PROTOTYPES)
+
+
+def test_version_and_error_string_without_gpu():
+    import pfblob._lib as L
+    assert L.lib.pf_version() >= 10000
+    assert isinstance(L.lib.pf_last_error(), bytes)
+
+
+def test_create_reports_missing_device_as_status():
+    import torch
+    import pfblob._lib as L
+    if torch.cuda.is_available():
+        pytest.skip("host without a GPU only")
+    p = ctypes.c_void_p()
+    s = L.lib.pf_create(0, ctypes.byref(p))
+    assert s in (1, 3)  # PF_ERR_INVALID_ARG (0 devices) or PF_ERR_CUDA
+    assert L.lib.pf_last_error()
+
+
+def test_null_context_is_rejected_without_gpu():
+    import pfblob._lib as L
+    s = L.lib.pf_velocity_direct(None, 10, None, None, None, 10, None, None, 1.0, None, None, None)
+    assert s == 1
+    assert b"NULL context" in L.lib.pf_last_error()

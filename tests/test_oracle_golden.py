@@ -1,0 +1,72 @@
+"""Pin the CPU oracle against outputs of the reference's own code (fixtures in
+tests/golden/, made by tests/golden/make_golden.py from the compiled reference
+Cython kernels, the reference Regrid and the reference C++ FMM)."""
+import numpy as np
+
+import oracle
+from conftest import normwise_err
+
+
+def test_direct_c1_bit_exact(golden):
+    d = golden("direct_c1")
+    vx, vy = oracle.velocity_direct(d["x"], d["y"], d["g"], float(d["ksigmasqr"]))
+    assert np.array_equal(vx, d["vx"]) and np.array_equal(vy, d["vy"])
+
+
+def test_direct_edge_cases_bit_exact(golden):
+    d = golden("direct_rand")
+    vx, vy = oracle.velocity_direct(d["x"], d["y"], d["g"], float(d["ksigmasqr"]))
+    assert np.array_equal(vx, d["vx"]) and np.array_equal(vy, d["vy"])
+
+
+def test_direct_separate_targets_match_self_targets(golden):
+    d = golden("direct_rand")
+    vx, vy = oracle.velocity_direct(d["x"], d["y"], d["g"], float(d["ksigmasqr"]),
+                                    d["x"][:100].copy(), d["y"][:100].copy())
+    assert np.array_equal(vx, d["vx"][:100])
+
+
+def test_panel_bit_exact(golden):
+    p = golden("panel_cyl")
+    vx, vy = oracle.panel_velocity(p["gamma"], p["xs"], p["ys"], p["xe"], p["ye"], p["cosa"],
+                                   p["sina"], p["xv"], p["yv"])
+    assert np.array_equal(vx, p["vx"]) and np.array_equal(vy, p["vy"])
+
+
+def test_regrid_matches_reference_regrid(golden):
+    for name in ("regrid_c1", "regrid_rand_c0", "regrid_rand_c3"):
+        r = golden(name)
+        xn, yn, gn, ix, iy = oracle.regrid(r["x"], r["y"], r["g"], float(r["sigma"]),
+                                           float(r["overlap"]), r["xb"], r["yb"], float(r["c"]))
+        assert np.array_equal(xn, r["xn"]) and np.array_equal(yn, r["yn"]), name
+        assert np.array_equal(gn, r["gn"]), name
+
+
+def test_regrid_conserves_moments(golden):
+    r = golden("regrid_c1")
+    m0 = oracle.moments(r["x"], r["y"], r["g"])
+    m1 = oracle.moments(r["xn"], r["yn"], r["gn"])
+    assert abs(m1[0] - m0[0]) / m0[3] < 1e-13
+    xs = np.abs(r["x"]).max()
+    assert max(abs(m1[1] - m0[1]), abs(m1[2] - m0[2])) / (m0[3] * xs) < 1e-13
+
+
+def test_m4prime_branches():
+    x = np.array([0.0, 0.5, -0.5, 1.0, -1.0, 1.5, 2.0, -2.5])
+    w = oracle.m4prime(x, 0.0)
+    assert w[0] == 1.0
+    assert w[3] == 0.0 and w[4] == 0.0  # |x| == 1 falls through to 0
+    assert w[6] == 0.0 and w[7] == 0.0
+    assert np.isclose(w[1], 1 - 2.5 * 0.25 + 1.5 * 0.125)
+    assert np.isclose(w[5], 0.5 * 0.25 * (-0.5))
+    # partition of unity on a shifted window (c = 0)
+    for s in (0.1, 0.37, 0.73):
+        u = np.array([1.0, 0.0, -1.0, -2.0]) + s
+        assert abs(oracle.m4prime(u, 0.0).sum() - 1.0) < 1e-15
+
+
+def test_reference_fmm_within_tolerance_of_direct_oracle(golden):
+    f = golden("fmm_rand")
+    sig = float(f["sigma"])
+    vx, vy = oracle.velocity_direct(f["x"], f["y"], f["g"], 2.0 * sig * sig)
+    assert normwise_err(f["vx"], f["vy"], vx, vy) < 1e-6

@@ -1,0 +1,53 @@
+"""Vortex-panel velocity on the GPU vs the reference Cython kernel (golden)
+and the oracle.  Gate: normwise relative error <= 1e-6."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import normwise_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def test_cylinder_vs_reference_golden(golden):
+    import pfblob
+    p = golden("panel_cyl")
+    vx, vy = pfblob.inducedVelocity(p["gamma"], p["xs"], p["ys"], p["xe"], p["ye"], p["cosa"],
+                                    p["sina"], p["xv"], p["yv"])
+    # the point 1e-6 from the panel (index 3) has a large, well-defined value
+    assert normwise_err(vx[4:], vy[4:], p["vx"][4:], p["vy"][4:]) <= TOL
+    assert abs(vx[3] - p["vx"][3]) <= 1e-5 * abs(p["vx"][3]) + 1e-6
+    # on the line extension of a panel: finite and equal to the reference
+    assert np.allclose(vx[:3], p["vx"][:3], rtol=1e-5, atol=1e-7)
+
+
+def test_512_panels_shear_layer_points():
+    import pfblob
+    from pfblob import workloads as wl
+    ps = wl.cylinder_panels(512)
+    rng = np.random.default_rng(2)
+    r = rng.uniform(1.0, 1.5, 20000)
+    t = rng.uniform(-np.pi, np.pi, 20000)
+    xv, yv = r * np.cos(t), r * np.sin(t)
+    rx, ry = oracle.panel_velocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina, xv, yv)
+    vx, vy = pfblob.inducedVelocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina, xv, yv)
+    assert normwise_err(vx, vy, rx, ry) <= TOL
+
+
+def test_accumulate_onto_blob_velocity():
+    import pfblob
+    from pfblob import workloads as wl
+    ps = wl.cylinder_panels(64)
+    dev = torch.device("cuda", 0)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    xv = T(np.linspace(-2, 2, 1000))
+    yv = T(np.full(1000, 1.7))
+    vx = torch.full((1000,), 0.25, dtype=torch.float64, device=dev)
+    vy = torch.full((1000,), -0.5, dtype=torch.float64, device=dev)
+    pfblob.panel_velocity_device(T(ps.gamma), T(ps.xs), T(ps.ys), T(ps.xe), T(ps.ye), T(ps.cosa),
+                                 T(ps.sina), xv, yv, vx, vy, accumulate=True)
+    rx, ry = oracle.panel_velocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina,
+                                   xv.cpu().numpy(), yv.cpu().numpy())
+    assert normwise_err(vx.cpu().numpy() - 0.25, vy.cpu().numpy() + 0.5, rx, ry) <= TOL

@@ -1,0 +1,108 @@
+"""M4' remesh on the GPU vs the reference Regrid (golden) and the oracle.
+
+Gates: lattice indices and new coordinates bit-exact, circulations within
+1e-12 relative (normwise), circulation and linear impulse conserved to 1e-12."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+GTOL = 1e-12
+
+
+def _regrid_gpu(x, y, g, sigma, overlap, xb, yb, c=0.0):
+    import pfblob
+    return pfblob.Regrid(x, y, g, sigma, overlap, xb, yb, 0, c)
+
+
+@pytest.mark.parametrize("name", ["regrid_c1", "regrid_rand_c0", "regrid_rand_c3"])
+def test_vs_reference_regrid_golden(golden, name):
+    r = golden(name)
+    xn, yn, gn = _regrid_gpu(r["x"], r["y"], r["g"], float(r["sigma"]), float(r["overlap"]),
+                             r["xb"], r["yb"], float(r["c"]))
+    assert xn.shape == r["xn"].shape
+    assert np.array_equal(xn, r["xn"]) and np.array_equal(yn, r["yn"])
+    assert np.abs(gn - r["gn"]).max() <= GTOL * np.abs(r["gn"]).max()
+    # explicit zero-weight cells are kept, as in the reference
+    assert np.array_equal(gn == 0.0, r["gn"] == 0.0) or np.abs(gn[r["gn"] == 0]).max() < 1e-300
+
+
+def test_c2_full_size_indices_bit_exact_and_conservation():
+    import pfblob
+    from pfblob import workloads as wl
+    b = wl.uniform_square()
+    xb, yb = b.bounds()
+    dev = torch.device("cuda", 0)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    x, y, g = T(b.x), T(b.y), T(b.g)
+    xn, yn, gn, ixn, iyn = pfblob.remesh_device(x, y, g, b.h, xb[0], yb[0], with_indices=True)
+    rx, ry, rg, rix, riy = oracle.regrid(b.x, b.y, b.g, b.sigma, b.overlap, xb, yb)
+    assert np.array_equal(ixn.cpu().numpy(), rix) and np.array_equal(iyn.cpu().numpy(), riy)
+    assert np.array_equal(xn.cpu().numpy(), rx) and np.array_equal(yn.cpu().numpy(), ry)
+    assert np.abs(gn.cpu().numpy() - rg).max() <= GTOL * np.abs(rg).max()
+    m0 = pfblob.moments_device(x, y, g).cpu().numpy()
+    m1 = pfblob.moments_device(xn, yn, gn).cpu().numpy()
+    circ, imp = pfblob.conservation_error(m0, m1, float(np.abs(b.x).max()))
+    assert circ <= 1e-12 and imp <= 1e-12
+
+
+def test_deterministic_repeat():
+    import pfblob
+    from pfblob import workloads as wl
+    b = wl.mixed_instance(50000, config=4, instance=3)
+    xb, yb = b.bounds()
+    a = _regrid_gpu(b.x, b.y, b.g, b.sigma, b.overlap, xb, yb)
+    c = _regrid_gpu(b.x, b.y, b.g, b.sigma, b.overlap, xb, yb)
+    for u, v in zip(a, c):
+        assert np.array_equal(u, v)
+
+
+def test_coincident_blobs_and_nodes():
+    """Many blobs in one cell, blobs exactly on lattice nodes."""
+    rng = np.random.default_rng(3)
+    h = 0.01
+    n = 3000
+    x = np.full(n, 0.123)
+    y = np.full(n, -0.456)
+    x[:1000] = (np.arange(1000) % 37) * h + 0.5 * h - 1.5 * h
+    y[:1000] = (np.arange(1000) // 37) * h + 0.5 * h - 1.5 * h
+    g = rng.standard_normal(n)
+    xb = np.array([-1.5 * h, 1.5 * h])
+    xn, yn, gn = _regrid_gpu(x, y, g, h / 0.8, 0.8, xb, xb)
+    rx, ry, rg, _, _ = oracle.regrid(x, y, g, h / 0.8, 0.8, xb, xb)
+    assert np.array_equal(xn, rx) and np.array_equal(yn, ry)
+    assert np.abs(gn - rg).max() <= GTOL * np.abs(rg).max()
+
+
+def test_single_blob_and_empty():
+    import pfblob
+    xn, yn, gn = _regrid_gpu(np.array([0.3]), np.array([0.7]), np.array([2.0]), 0.1, 0.8,
+                             [-0.12, 0.12], [-0.12, 0.12])
+    assert xn.shape == (16,) and abs(gn.sum() - 2.0) < 1e-15
+    e = np.zeros(0)
+    out = pfblob.Regrid(e, e, e, 0.1, 0.8, [0, 1], [0, 1])
+    assert out[0].shape == (0,)
+
+
+def test_nan_input_is_an_error():
+    import pfblob
+    x = np.array([0.1, np.nan, 0.3])
+    with pytest.raises(pfblob._lib.PfError) as ei:
+        pfblob.Regrid(x, x * 0, x * 0 + 1, 0.1, 0.8, [0, 1], [0, 1])
+    assert ei.value.status == 5
+
+
+def test_capacity_error_reports_needed_size():
+    import ctypes
+    import pfblob
+    from pfblob import _lib
+    from pfblob._arrays import ptr
+    dev = torch.device("cuda", 0)
+    x = torch.tensor([0.3, 0.5], dtype=torch.float64, device=dev)
+    out = torch.empty(4, dtype=torch.float64, device=dev)
+    n = ctypes.c_int64(0)
+    s = _lib.lib.pf_remesh(_lib.context(0), 2, ptr(x), ptr(x), ptr(x), 0.08, -0.12, -0.12, 0.0, 4,
+                           ptr(out), ptr(out), ptr(out), None, None, ctypes.byref(n), None)
+    assert s == 6 and n.value > 4

@@ -111,9 +111,13 @@ def gpu_id_for_smi(torch):
 
 
 # ---------------------------------------------------------------------------
-def workload_c2():
+N_DEFAULT = 1 << 20
+
+
+def workload_c2(n=None):
+    """C2 blobs; a smaller n (profiling cases) keeps sigma and the domain."""
     from pfblob import workloads as wl
-    return wl.uniform_square(n=1 << 20, sigma=0.002, overlap=0.8, config=2, instance=0)
+    return wl.uniform_square(n=n or N_DEFAULT, sigma=0.002, overlap=0.8, config=2, instance=0)
 
 
 def pick_method(arg):
@@ -139,7 +143,7 @@ def run_ours(args, rank, world):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    b = workload_c2()
+    b = workload_c2(args.n)
     n = b.n
     method = pick_method(args.method)
     meth_id = pfblob.FMM_METHOD if method == "fmm" else pfblob.DIRECT_METHOD
@@ -343,6 +347,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--method", default="auto", choices=["auto", "fmm", "direct"])
     ap.add_argument("--ndirect", type=int, default=35)
+    ap.add_argument("--n", type=int, default=None,
+                    help="blob count (default 2^20; smaller only for profiling captures)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -99,6 +99,41 @@ pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x, const dou
                           double ksigmasqr, double xopt, double cutoff, double tol,
                           int ndirect, double *vx, double *vy, void *stream);
 
+/* Tuning of the FMM for the calling host thread (0 = automatic):
+ * leaf_level in [2, 11]; expansion_terms (p+1) in {16, 20, 24, 28, 32};
+ * block_level_drop in [0, 2] (P2P blocks of 2^drop x 2^drop leaves).  The
+ * reference fixes these at build time (FMM_THETA, Ndirect-based level count,
+ * p from tol: src/cpp/blobs/c++/fmm2d_py_cpu_gpu/fmm.cpp:538-555); here the
+ * autotuner and experiments set them at run time. */
+pf_status pf_fmm_set_tuning(int leaf_level, int expansion_terms, int block_level_drop);
+
+/* Leaf Morton keys of points for a tree with origin (x0, y0), leaf width
+ * `leaf_width` and leaf level `leaf_level` (<= 15): key = interleave(qx, qy)
+ * with qx = clamp(floor((x - x0)/leaf_width), 0, 2^L - 1), x in the even
+ * bits.  The same kernel sorts the FMM's particles; exported so the integer
+ * keys can be checked bit for bit.  keys: device uint32 array of n entries. */
+pf_status pf_fmm_tree_keys(pf_ctx *ctx, int64_t n, const double *x, const double *y, double x0,
+                           double y0, double leaf_width, int leaf_level, uint32_t *keys,
+                           void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Host-only (no device work): the interaction offset tables of the FMM tree
+ * for leaf level `leaf_level` (root box width `root_width`, boxes at level l
+ * of width root_width/2^l), P2P blocks of 2^block_level_drop leaves a side,
+ * separation parameter `theta` and Gaussian `cutoff`.  Two same-level boxes
+ * at integer offset (i, j) are well separated when (i^2+j^2) theta^2 >= 2 and
+ * (sqrt(i^2+j^2) - sqrt 2) w >= cutoff -- the two connectivity checks of the
+ * reference FMM (src/cpp/blobs/c++/fmm2d_py_cpu_gpu/fmm.cpp:1735-1835,
+ * THETACUTOFFCHECK), which replaces its per-box list build
+ * (MPexp_connect_CPU_, fmmsort.cpp:792-910) for a uniform tree.
+ * Flattened int32 layout:
+ *   L, kb; for l = 0..L: n, n (i, j) pairs (near); for l = 1..L: npos, then per
+ *   position n, n (i, j) pairs (M2L); then n, n (i, j) pairs (P2P block list).
+ * *needed receives the length; PF_ERR_CAPACITY if `capacity` is smaller.
+ * ------------------------------------------------------------------------- */
+pf_status pf_fmm_lists(int leaf_level, int block_level_drop, double root_width, double cutoff,
+                       double theta, int32_t *buf, int64_t capacity, int64_t *needed);
+
 /* ---------------------------------------------------------------------------
  * Constant-strength straight vortex panels -> induced velocity at points,
  * accumulated into (vx, vy) when `accumulate` != 0 (the blob + panel sum of

@@ -1,10 +1,884 @@
-// fmm.cu -- 2D FMM for Gaussian blobs (entry point).
-#include "pf_common.cuh"
+// fmm.cu -- 2D fast multipole method for Gaussian vortex blobs on B200.
+//
+// Tree: uniform quadtree over the bounding square of sources and targets,
+// every level a dense 2^l x 2^l grid addressed by Morton index (box (l, m) at
+// global slot off[l] + m, off[l] = (4^l - 1)/3).  Particles are counting-
+// sorted by leaf Morton key (ties in input order, so every sum has a fixed
+// order) -- this replaces the reference's median-split partition
+// (src/cpp/blobs/c++/fmm2d_py_cpu_gpu/fmmsort.cpp:441-790).
+//
+// Expansions (FP64, complex, scaled by the box width w so that all
+// coefficients are O(sum |g|)):
+//   multipole  M(z) = sum_j g_j / (z - z_j) = sum_k a_k w^k / (z - c)^(k+1),
+//              a_k = sum_j g_j ((z_j - c)/w)^k                       (P2M)
+//   local      L(z) = (1/w) sum_n lam_n ((z - c)/w)^n
+//   M2M  a'_k  = sum_{m<=k} C(k,m) tau^(k-m) 2^-m a_m,  tau = (c_child - c_par)/w_par
+//   M2L  lam_n += sum_k (-1)^(k+1) C(n+k,k) rho^(n+k+1) a_k,  rho = 1/(i + i j)
+//              for a far box at integer offset (i, j): the operator depends
+//              only on the offset, so rho^m is tabulated per offset
+//   L2L  lam'_n = (1/2) sum_{m>=n} C(m,n) tau^(m-n) 2^-n lam_m
+//   L2P  W = L(z);  u = Im W / 2pi,  v = Re W / 2pi
+// (reference counterparts: mpexp_init fmm.cpp:1452-1509, shift_m2m
+// fmmshift.cpp:80-236, shift_m2ps fmmshift.cpp:237-621, shift_p2p
+// fmmshift.cpp:622-767, mpexp_eval fmm.cpp:1875-1931).
+//
+// Near field: the Gaussian kernel itself, FP32 with hi/lo coordinates and
+// compensated accumulation (gauss_pair.cuh), for every target of a P2P block
+// (2^kb x 2^kb leaves) against the block's source leaves; those leaves are
+// sorted by Morton index and merged into runs of consecutive leaves, which
+// are contiguous in the sorted particle arrays, and streamed through shared
+// memory in full tiles.  The interaction lists come from fmm_plan.cu.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "fmm_plan.cuh"
+#include "gauss_pair.cuh"
+#include "scan.cuh"
 
 namespace pf {
 pf_status launch_direct(int64_t ns, const double *x, const double *y, const double *g,
                         int64_t nt, const double *xt, const double *yt, double ksigmasqr,
                         double *vx, double *vy, cudaStream_t stream);
+}
+
+namespace {
+
+constexpr double THETA = 0.5;
+constexpr double INV_2PI = 0.15915494309189535;
+constexpr int MAX_LEVEL = 11;
+constexpr int P2P_THREADS = 128;
+constexpr int P2P_QMAX = 1024;
+constexpr int WARP_BOX_THREADS = 128;  // 4 warps, one box each
+constexpr unsigned INVALID_KEY = 0xFFFFFFFFu;
+
+// ---------------------------------------------------------------------------
+// Morton helpers (x in even bits, y in odd bits)
+__host__ __device__ __forceinline__ uint32_t part1by1(uint32_t v) {
+    v &= 0x0000ffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+__host__ __device__ __forceinline__ uint32_t compact1by1(uint32_t v) {
+    v &= 0x55555555u;
+    v = (v | (v >> 1)) & 0x33333333u;
+    v = (v | (v >> 2)) & 0x0f0f0f0fu;
+    v = (v | (v >> 4)) & 0x00ff00ffu;
+    v = (v | (v >> 8)) & 0x0000ffffu;
+    return v;
+}
+__host__ __device__ __forceinline__ uint32_t morton2(uint32_t x, uint32_t y) {
+    return part1by1(x) | (part1by1(y) << 1);
+}
+
+// leaf coordinate of a position: floor((x - x0) / w) clamped to [0, 2^L)
+__device__ __forceinline__ uint32_t leaf_coord(double x, double x0, double w, int L) {
+    const double q = floor(__ddiv_rn(__dsub_rn(x, x0), w));
+    const double hi = (double)((1u << L) - 1u);
+    return (uint32_t)fmin(fmax(q, 0.0), hi);
+}
+
+// ---------------------------------------------------------------------------
+// bounding box with order-preserving integer images of doubles
+__device__ __forceinline__ unsigned long long ord_d(double v) {
+    unsigned long long u = (unsigned long long)__double_as_longlong(v);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__host__ inline double unord_d(unsigned long long u) {
+    u = (u >> 63) ? (u & 0x7fffffffffffffffull) : ~u;
+    double d;
+    memcpy(&d, &u, 8);
+    return d;
+}
+
+struct BBox {
+    unsigned long long mnx, mxx, mny, mxy;
+    int bad;
+    int pad[7];
+};
+
+__global__ void k_bbox_init(BBox *b) {
+    b->mnx = b->mny = ~0ull;
+    b->mxx = b->mxy = 0ull;
+    b->bad = 0;
+}
+
+__global__ void __launch_bounds__(256)
+k_bbox(const double *__restrict__ x, const double *__restrict__ y, int64_t n, BBox *b) {
+    unsigned long long mnx = ~0ull, mxx = 0, mny = ~0ull, mxy = 0;
+    int bad = 0;
+    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+        const double a = x[i], c = y[i];
+        if (!isfinite(a) || !isfinite(c)) {
+            bad = 1;
+            continue;
+        }
+        const unsigned long long oa = ord_d(a), oc = ord_d(c);
+        mnx = min(mnx, oa);
+        mxx = max(mxx, oa);
+        mny = min(mny, oc);
+        mxy = max(mxy, oc);
+    }
+    for (int o = 16; o; o >>= 1) {
+        mnx = min(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+        mxx = max(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+        mny = min(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+        mxy = max(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+    }
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&b->mnx, mnx);
+        atomicMax(&b->mxx, mxx);
+        atomicMin(&b->mny, mny);
+        atomicMax(&b->mxy, mxy);
+        if (bad) atomicOr(&b->bad, 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// counting sort by leaf key
+__global__ void __launch_bounds__(256)
+k_leaf_keys(const double *__restrict__ x, const double *__restrict__ y, int64_t n, double x0,
+            double y0, double wl, int L, uint32_t *__restrict__ key, int32_t *__restrict__ rank,
+            int32_t *__restrict__ cnt) {
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t k = morton2(leaf_coord(x[i], x0, wl, L), leaf_coord(y[i], y0, wl, L));
+    key[i] = k;
+    if (rank) rank[i] = atomicAdd(&cnt[k], 1);
+}
+
+__global__ void __launch_bounds__(256)
+k_place(int64_t n, const uint32_t *__restrict__ key, const int32_t *__restrict__ rank,
+        const int32_t *__restrict__ start, int32_t *__restrict__ perm) {
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    perm[start[key[i]] + rank[i]] = (int32_t)i;
+}
+
+// Per leaf: order the leaf's particles by input index, then write the sorted
+// copies: FP64 (x, y[, g]) and hi/lo float4 (+ float g).
+__global__ void __launch_bounds__(256)
+k_order(int64_t nleaf, const int32_t *__restrict__ start, const int32_t *__restrict__ cnt,
+        int32_t *__restrict__ perm, const double *__restrict__ x, const double *__restrict__ y,
+        const double *__restrict__ g, double *__restrict__ sx, double *__restrict__ sy,
+        double *__restrict__ sg, float4 *__restrict__ hl, float *__restrict__ g32) {
+    const int64_t m = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (m >= nleaf) return;
+    const int c = cnt[m];
+    if (c == 0) return;
+    const int s0 = start[m];
+    for (int k = 1; k < c; ++k) {
+        const int32_t v = perm[s0 + k];
+        int j = k - 1;
+        while (j >= 0 && perm[s0 + j] > v) {
+            perm[s0 + j + 1] = perm[s0 + j];
+            --j;
+        }
+        perm[s0 + j + 1] = v;
+    }
+    for (int k = 0; k < c; ++k) {
+        const int32_t i = perm[s0 + k];
+        const double a = x[i], b = y[i];
+        sx[s0 + k] = a;
+        sy[s0 + k] = b;
+        float4 h;
+        pfd::split_hilo(a, h.x, h.z);
+        pfd::split_hilo(b, h.y, h.w);
+        hl[s0 + k] = h;
+        if (g) {
+            const double gi = g[i];
+            sg[s0 + k] = gi;
+            g32[s0 + k] = (float)gi;
+        }
+    }
+}
+
+// box counts of level l from level l+1 (children 4m..4m+3)
+__global__ void __launch_bounds__(256)
+k_count_up(int64_t nbox, const int32_t *__restrict__ child, int32_t *__restrict__ par) {
+    const int64_t m = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (m >= nbox) return;
+    const int32_t *c = child + 4 * m;  // not 16-byte aligned in general
+    par[m] = c[0] + c[1] + c[2] + c[3];
+}
+
+// ---------------------------------------------------------------------------
+// complex helpers
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {  // a*b + c
+    return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+
+// P2M: one thread per leaf
+template <int NP>
+__global__ void __launch_bounds__(128)
+k_p2m(int L, double x0, double y0, double wl, const int32_t *__restrict__ start,
+      const int32_t *__restrict__ cnt, const double *__restrict__ sx,
+      const double *__restrict__ sy, const double *__restrict__ sg, double2 *__restrict__ M) {
+    const int64_t nleaf = (int64_t)1 << (2 * L);
+    const int64_t m = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    if (m >= nleaf) return;
+    const int c = cnt[m];
+    if (c == 0) return;
+    const uint32_t ix = compact1by1((uint32_t)m), iy = compact1by1((uint32_t)m >> 1);
+    const double cx = x0 + ((double)ix + 0.5) * wl, cy = y0 + ((double)iy + 0.5) * wl;
+    const double iw = 1.0 / wl;
+    double2 a[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) a[k] = make_double2(0.0, 0.0);
+    const int s0 = start[m];
+    for (int j = 0; j < c; ++j) {
+        const double2 z = make_double2((sx[s0 + j] - cx) * iw, (sy[s0 + j] - cy) * iw);
+        double2 zk = make_double2(sg[s0 + j], 0.0);
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            a[k].x += zk.x;
+            a[k].y += zk.y;
+            zk = cmul(zk, z);
+        }
+    }
+    const int64_t base = ((((int64_t)1 << (2 * L)) - 1) / 3 + m) * NP;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) M[base + k] = a[k];
+}
+
+__host__ __device__ __forceinline__ int64_t level_off(int l) {
+    return ((((int64_t)1) << (2 * l)) - 1) / 3;
+}
+
+// M2M at parent level l: one warp per parent box, lane k = coefficient
+template <int NP>
+__global__ void __launch_bounds__(WARP_BOX_THREADS)
+k_m2m(int l, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
+      const double2 *__restrict__ opT /* [4][NP(m)][NP(k)] */) {
+    __shared__ double2 s_a[WARP_BOX_THREADS / 32][32];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t m = (int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid;
+    if (m >= ((int64_t)1 << (2 * l))) return;
+    const int64_t bg = level_off(l) + m;
+    if (scnt[bg] == 0) return;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int c = 0; c < 4; ++c) {
+        const int64_t cg = level_off(l + 1) + 4 * m + c;
+        if (scnt[cg] == 0) continue;
+        if (lane < NP) s_a[wid][lane] = M[cg * NP + lane];
+        __syncwarp();
+        if (lane < NP) {
+            const double2 *op = opT + (int64_t)c * NP * NP;
+#pragma unroll 4
+            for (int mm = 0; mm <= lane; ++mm) acc = cfma(op[mm * NP + lane], s_a[wid][mm], acc);
+        }
+        __syncwarp();
+    }
+    if (lane < NP) M[bg * NP + lane] = acc;
+}
+
+// M2L for all levels 2..L: one warp per target box, lane n = local coefficient
+template <int NP>
+__global__ void __launch_bounds__(WARP_BOX_THREADS)
+k_m2l(int L, int Bp, int64_t bg0, int64_t nbg, const int32_t *__restrict__ scnt,
+      const int32_t *__restrict__ tcnt, const double2 *__restrict__ M, double2 *__restrict__ Lc,
+      const int4 *__restrict__ far, const int32_t *__restrict__ far_ptr, int maxpos,
+      const double2 *__restrict__ pw /* [nop][NP+1] */, const double *__restrict__ binom) {
+    __shared__ double s_bin[NP * NP];
+    __shared__ double2 s_c[WARP_BOX_THREADS / 32][32];
+    for (int t = threadIdx.x; t < NP * NP; t += WARP_BOX_THREADS) s_bin[t] = binom[t];
+    __syncthreads();
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t w = (int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid;
+    if (w >= nbg) return;
+    const int64_t bg = bg0 + w;
+    if (tcnt[bg] == 0) return;
+    int l = 2;
+    while (l < L && bg >= level_off(l + 1)) ++l;
+    const uint32_t m = (uint32_t)(bg - level_off(l));
+    const int ix = (int)compact1by1(m), iy = (int)compact1by1(m >> 1);
+    const int pos = (l == L) ? ((ix % Bp) + Bp * (iy % Bp)) : ((ix & 1) | ((iy & 1) << 1));
+    const int side = 1 << l;
+    const int e0 = far_ptr[l * maxpos + pos], e1 = far_ptr[l * maxpos + pos + 1];
+    double2 acc = make_double2(0.0, 0.0);
+    for (int e = e0; e < e1; ++e) {
+        const int4 f = far[e];
+        const int sx = ix + f.x, sy = iy + f.y;
+        if (sx < 0 || sy < 0 || sx >= side || sy >= side) continue;
+        const int64_t sg = level_off(l) + morton2((uint32_t)sx, (uint32_t)sy);
+        if (scnt[sg] == 0) continue;
+        const double2 *rp = pw + (int64_t)f.z * (NP + 1);
+        if (lane < NP) {
+            double2 c = cmul(M[sg * NP + lane], rp[lane]);
+            if ((lane & 1) == 0) c = make_double2(-c.x, -c.y);  // (-1)^(k+1)
+            s_c[wid][lane] = c;
+        }
+        __syncwarp();
+        if (lane < NP) {
+            double ux = 0.0, uy = 0.0;
+#pragma unroll
+            for (int k = 0; k < NP; ++k) {
+                const double b = s_bin[k * NP + lane];
+                const double2 c = s_c[wid][k];
+                ux = fma(b, c.x, ux);
+                uy = fma(b, c.y, uy);
+            }
+            acc = cfma(rp[lane + 1], make_double2(ux, uy), acc);
+        }
+        __syncwarp();
+    }
+    if (lane < NP) Lc[bg * NP + lane] = acc;
+}
+
+// L2L into child level l: one warp per child box
+template <int NP>
+__global__ void __launch_bounds__(WARP_BOX_THREADS)
+k_l2l(int l, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
+      const double2 *__restrict__ opT /* [4][NP(m)][NP(n)] */) {
+    __shared__ double2 s_b[WARP_BOX_THREADS / 32][32];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t m = (int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid;
+    if (m >= ((int64_t)1 << (2 * l))) return;
+    const int64_t bg = level_off(l) + m;
+    if (tcnt[bg] == 0) return;
+    const int64_t pg = level_off(l - 1) + (m >> 2);
+    const int c = (int)(m & 3);
+    if (lane < NP) s_b[wid][lane] = Lc[pg * NP + lane];
+    __syncwarp();
+    if (lane < NP) {
+        const double2 *op = opT + (int64_t)c * NP * NP;
+        double2 acc = Lc[bg * NP + lane];
+#pragma unroll 4
+        for (int mm = lane; mm < NP; ++mm) acc = cfma(op[mm * NP + lane], s_b[wid][mm], acc);
+        Lc[bg * NP + lane] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// P2P near field: one CTA per P2P block (level L - kb box)
+__global__ void __launch_bounds__(P2P_THREADS)
+k_p2p(int L, int kb, const int32_t *__restrict__ tstart, const int32_t *__restrict__ tcnt,
+      const int32_t *__restrict__ sstart, const int32_t *__restrict__ scnt,
+      const float4 *__restrict__ shl, const float *__restrict__ sg32,
+      const float4 *__restrict__ thl, const int2 *__restrict__ q, int nq, int nqp,
+      pfd::GaussParams gp, double2 *__restrict__ nearv) {
+    __shared__ uint32_t s_key[P2P_QMAX];
+    __shared__ int s_rstart[P2P_QMAX + 1];  // particle start of run r
+    __shared__ int s_rpre[P2P_QMAX + 1];    // stream prefix of run r
+    __shared__ int s_nruns;
+    __shared__ float4 s_pos[P2P_THREADS];
+    __shared__ float s_g[P2P_THREADS];
+    const uint32_t b = blockIdx.x;
+    const uint32_t leaf0 = b << (2 * kb), nl = 1u << (2 * kb);
+    const int t0 = tstart[leaf0];
+    const int tn = tstart[leaf0 + nl - 1] + tcnt[leaf0 + nl - 1] - t0;
+    if (tn == 0) return;
+    const int ox = (int)(compact1by1(b) << kb), oy = (int)(compact1by1(b >> 1) << kb);
+    const int side = 1 << L;
+    // 1. source leaves of the block, sorted
+    for (int t = threadIdx.x; t < nqp; t += P2P_THREADS) {
+        uint32_t k = INVALID_KEY;
+        if (t < nq) {
+            const int lx = ox + q[t].x, ly = oy + q[t].y;
+            if (lx >= 0 && ly >= 0 && lx < side && ly < side) k = morton2(lx, ly);
+        }
+        s_key[t] = k;
+    }
+    __syncthreads();
+    for (int kk = 2; kk <= nqp; kk <<= 1) {
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            for (int t = threadIdx.x; t < nqp; t += P2P_THREADS) {
+                const int p = t ^ j;
+                if (p > t) {
+                    const uint32_t a = s_key[t], c = s_key[p];
+                    const bool up = ((t & kk) == 0);
+                    if ((a > c) == up) {
+                        s_key[t] = c;
+                        s_key[p] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // 2. runs of consecutive Morton leaves (contiguous particle ranges)
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int nr = 0, pre = 0;
+        for (int base = 0; base < nqp; base += 32) {
+            const int t = base + lane;
+            const uint32_t k = (t < nqp) ? s_key[t] : INVALID_KEY;
+            const bool valid = k != INVALID_KEY;
+            const bool head = valid && (t == 0 || s_key[t - 1] + 1u != k);
+            const unsigned hm = __ballot_sync(0xffffffffu, head);
+            // a run ends at t if valid and (next invalid or next not consecutive)
+            const uint32_t kn = (t + 1 < nqp) ? s_key[t + 1] : INVALID_KEY;
+            const bool tail = valid && (kn == INVALID_KEY || kn != k + 1u);
+            // heads: record particle start; tails: record run length
+            if (head) {
+                const int r = nr + __popc(hm & ((1u << lane) - 1u));
+                s_rstart[r] = sstart[k];
+            }
+            // tails close runs in order: the run index of a tail is the number
+            // of heads at or before it, minus one
+            if (tail) {
+                const int r = nr + __popc(hm & ((2u << lane) - 1u)) - 1;
+                s_rpre[r + 1] = sstart[k] + scnt[k];  // end particle (temporarily)
+            }
+            nr += __popc(hm);
+            __syncwarp();
+        }
+        // convert run ends into stream prefix sums
+        if (lane == 0) {
+            s_rpre[0] = 0;
+            for (int r = 0; r < nr; ++r) {
+                const int len = s_rpre[r + 1] - s_rstart[r];
+                s_rpre[r + 1] = pre + len;
+                pre += len;
+            }
+            s_nruns = nr;
+        }
+    }
+    __syncthreads();
+    const int nr = s_nruns;
+    const int S = s_rpre[nr];
+    // 3. targets in passes of P2P_THREADS
+    for (int tp = 0; tp < tn; tp += P2P_THREADS) {
+        const int ti = tp + threadIdx.x;
+        float4 th = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ti < tn) th = thl[t0 + ti];
+        float hx = 0.f, lx = 0.f, hy = 0.f, ly = 0.f;
+        for (int s0 = 0; s0 < S; s0 += P2P_THREADS) {
+            const int p = s0 + threadIdx.x;
+            float4 sp = make_float4(0.f, 0.f, 0.f, 0.f);
+            float gg = 0.f;
+            if (p < S) {
+                int lo = 0, hi = nr - 1;  // largest r with rpre[r] <= p
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_rpre[mid] <= p) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int src = s_rstart[lo] + (p - s_rpre[lo]);
+                sp = shl[src];
+                gg = sg32[src];
+            }
+            __syncthreads();
+            s_pos[threadIdx.x] = sp;
+            s_g[threadIdx.x] = gg;
+            __syncthreads();
+            const int cntt = min(P2P_THREADS, S - s0);
+            for (int c0 = 0; c0 < cntt; c0 += 32) {
+                float px = 0.f, py = 0.f;
+#pragma unroll 4
+                for (int k = 0; k < 32; ++k) {
+                    const float4 qq = s_pos[c0 + k];
+                    const float dx = (th.x - qq.x) + (th.z - qq.z);
+                    const float dy = (th.y - qq.y) + (th.w - qq.w);
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
+                    const float sc = pfd::gauss_s(r2, s_g[c0 + k], gp);
+                    px = fmaf(-dy, sc, px);
+                    py = fmaf(dx, sc, py);
+                }
+                pfd::comp_add(hx, lx, px);
+                pfd::comp_add(hy, ly, py);
+            }
+        }
+        if (ti < tn)
+            nearv[t0 + ti] = make_double2(INV_2PI * ((double)hx + (double)lx),
+                                          INV_2PI * ((double)hy + (double)ly));
+        __syncthreads();
+    }
+}
+
+// L2P + near + scatter to input order: one thread per sorted target
+template <int NP>
+__global__ void __launch_bounds__(256)
+k_l2p(int64_t nt, int L, double x0, double y0, double wl, const double *__restrict__ tx,
+      const double *__restrict__ ty, const uint32_t *__restrict__ tkey_sorted,
+      const double2 *__restrict__ Lc, const double2 *__restrict__ nearv,
+      const int32_t *__restrict__ perm, double *__restrict__ vx, double *__restrict__ vy) {
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i >= nt) return;
+    const uint32_t m = tkey_sorted[i];
+    const uint32_t ix = compact1by1(m), iy = compact1by1(m >> 1);
+    const double iw = 1.0 / wl;
+    const double2 z = make_double2((tx[i] - (x0 + ((double)ix + 0.5) * wl)) * iw,
+                                   (ty[i] - (y0 + ((double)iy + 0.5) * wl)) * iw);
+    const double2 *lam = Lc + (level_off(L) + m) * NP;
+    double2 w = lam[NP - 1];
+#pragma unroll
+    for (int n = NP - 2; n >= 0; --n) w = cfma(w, z, lam[n]);
+    const double2 nv = nearv[i];
+    const int32_t o = perm[i];
+    vx[o] = nv.x + INV_2PI * iw * w.y;
+    vy[o] = nv.y + INV_2PI * iw * w.x;
+}
+
+// sorted target keys (leaf of every sorted target)
+__global__ void __launch_bounds__(256)
+k_sorted_keys(int64_t n, const int32_t *__restrict__ perm, const uint32_t *__restrict__ key,
+              uint32_t *__restrict__ skey) {
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i < n) skey[i] = key[perm[i]];
+}
+
+// ---------------------------------------------------------------------------
+// Host: plan cache (tables + operators on the device)
+struct FmmCache {
+    int L = -1, kb = -1, np = -1;
+    double ratio = -1.0;  // cutoff / root width
+    int maxpos = 0, nq = 0, nqp = 0;
+    int4 *d_far = nullptr;
+    int32_t *d_far_ptr = nullptr;
+    int2 *d_q = nullptr;
+    double2 *d_pw = nullptr, *d_m2m = nullptr, *d_l2l = nullptr;
+    double *d_bin = nullptr;
+    void release() {
+        cudaFree(d_far);
+        cudaFree(d_far_ptr);
+        cudaFree(d_q);
+        cudaFree(d_pw);
+        cudaFree(d_m2m);
+        cudaFree(d_l2l);
+        cudaFree(d_bin);
+        d_far = nullptr;
+        d_far_ptr = nullptr;
+        d_q = nullptr;
+        d_pw = nullptr;
+        d_m2m = d_l2l = nullptr;
+        d_bin = nullptr;
+        L = -1;
+    }
+};
+
+struct cplx {
+    double re, im;
+};
+static cplx cm(cplx a, cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+
+static double binom_d(int n, int k) {
+    if (k < 0 || k > n) return 0.0;
+    double r = 1.0;  // exact while the value stays below 2^53
+    for (int i = 1; i <= k; ++i) r = r * (double)(n - k + i) / (double)i;
+    return r;
+}
+
+template <typename T>
+static pf_status upload(T **dst, const std::vector<T> &v) {
+    if (v.empty()) {
+        *dst = nullptr;
+        return PF_OK;
+    }
+    PF_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(dst), sizeof(T) * v.size()));
+    PF_CUDA_TRY(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return PF_OK;
+}
+
+static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, double cutoff) {
+    c.release();
+    pf::fmm::Tables t;
+    pf::fmm::build_tables(L, kb, w0, cutoff, THETA, t);
+    const int B = 1 << kb, Bp = B > 2 ? B : 2;
+    c.maxpos = std::max(4, Bp * Bp);
+    // far lists with offset ids
+    std::vector<int4> far;
+    std::vector<int32_t> ptr((L + 1) * c.maxpos + 1, 0);
+    std::vector<pf::fmm::Off> ops;
+    auto op_id = [&](const pf::fmm::Off &o) {
+        for (size_t k = 0; k < ops.size(); ++k)
+            if (ops[k] == o) return (int)k;
+        ops.push_back(o);
+        return (int)ops.size() - 1;
+    };
+    for (int l = 0; l <= L; ++l) {
+        for (int p = 0; p < c.maxpos; ++p) {
+            ptr[l * c.maxpos + p] = (int32_t)far.size();
+            if (l >= 2 && p < (int)t.far[l].size())
+                for (const auto &o : t.far[l][p]) far.push_back(make_int4(o.i, o.j, op_id(o), 0));
+        }
+    }
+    ptr[(L + 1) * c.maxpos] = (int32_t)far.size();  // [l*maxpos + pos] .. next slot
+    // powers rho^m, m = 0..np, rho = 1/(i + i j)
+    std::vector<double2> pw(ops.size() * (np + 1));
+    for (size_t k = 0; k < ops.size(); ++k) {
+        const double i = ops[k].i, j = ops[k].j, d = i * i + j * j;
+        const cplx rho = {i / d, -j / d};
+        cplx pm = {1.0, 0.0};
+        for (int m = 0; m <= np; ++m) {
+            pw[k * (np + 1) + m] = make_double2(pm.re, pm.im);
+            pm = cm(pm, rho);
+        }
+    }
+    // M2M / L2L operators, stored transposed for coalesced lane access
+    std::vector<double2> m2m(4 * np * np), l2l(4 * np * np);
+    for (int cc = 0; cc < 4; ++cc) {
+        const cplx tau = {(cc & 1) ? 0.25 : -0.25, (cc & 2) ? 0.25 : -0.25};
+        std::vector<cplx> tp(np);
+        tp[0] = {1.0, 0.0};
+        for (int k = 1; k < np; ++k) tp[k] = cm(tp[k - 1], tau);
+        for (int k = 0; k < np; ++k)
+            for (int m = 0; m < np; ++m) {
+                // M2M: out k, in m (m <= k): C(k,m) tau^(k-m) 2^-m   -> opT[c][m][k]
+                cplx a = {0.0, 0.0};
+                if (m <= k) {
+                    const double s = binom_d(k, m) * std::ldexp(1.0, -m);
+                    a = {tp[k - m].re * s, tp[k - m].im * s};
+                }
+                m2m[(size_t)cc * np * np + (size_t)m * np + k] = make_double2(a.re, a.im);
+                // L2L: out n = k, in m (m >= n): 1/2 C(m,n) tau^(m-n) 2^-n -> opT[c][m][n]
+                cplx b = {0.0, 0.0};
+                if (m >= k) {
+                    const double s = 0.5 * binom_d(m, k) * std::ldexp(1.0, -k);
+                    b = {tp[m - k].re * s, tp[m - k].im * s};
+                }
+                l2l[(size_t)cc * np * np + (size_t)m * np + k] = make_double2(b.re, b.im);
+            }
+    }
+    std::vector<double> bin(np * np);
+    for (int k = 0; k < np; ++k)
+        for (int n = 0; n < np; ++n) bin[k * np + n] = binom_d(n + k, k);
+    std::vector<int2> q;
+    for (const auto &o : t.p2p) q.push_back(make_int2(o.i, o.j));
+    c.nq = (int)q.size();
+    c.nqp = 1;
+    while (c.nqp < c.nq) c.nqp <<= 1;
+    PF_TRY(upload(&c.d_far, far));
+    PF_TRY(upload(&c.d_far_ptr, ptr));
+    PF_TRY(upload(&c.d_q, q));
+    PF_TRY(upload(&c.d_pw, pw));
+    PF_TRY(upload(&c.d_m2m, m2m));
+    PF_TRY(upload(&c.d_l2l, l2l));
+    PF_TRY(upload(&c.d_bin, bin));
+    c.L = L;
+    c.kb = kb;
+    c.np = np;
+    c.ratio = cutoff / w0;
+    return PF_OK;
+}
+
+struct Sorted {
+    uint32_t *key = nullptr;
+    int32_t *rank = nullptr, *perm = nullptr, *cnt = nullptr, *start = nullptr;
+    double *x = nullptr, *y = nullptr, *g = nullptr;
+    float4 *hl = nullptr;
+    float *g32 = nullptr;
+};
+
+static pf_status sort_points(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                             const double *g, double x0, double y0, double wl, int L, Sorted &s,
+                             int32_t *scan_tmp, cudaStream_t st) {
+    const int64_t nleaf = (int64_t)1 << (2 * L);
+    PF_CUDA_TRY(cudaMemsetAsync(s.cnt, 0, sizeof(int32_t) * nleaf, st));
+    if (n == 0) {
+        PF_CUDA_TRY(cudaMemsetAsync(s.start, 0, sizeof(int32_t) * nleaf, st));
+        return PF_OK;
+    }
+    const unsigned gn = (unsigned)pf::ceil_div(n, 256);
+    k_leaf_keys<<<gn, 256, 0, st>>>(x, y, n, x0, y0, wl, L, s.key, s.rank, s.cnt);
+    PF_TRY(pf::launch_status("k_leaf_keys"));
+    PF_TRY(pf::exclusive_scan_i32(s.cnt, s.start, nleaf, scan_tmp, nullptr, st));
+    k_place<<<gn, 256, 0, st>>>(n, s.key, s.rank, s.start, s.perm);
+    PF_TRY(pf::launch_status("k_place"));
+    k_order<<<(unsigned)pf::ceil_div(nleaf, 256), 256, 0, st>>>(nleaf, s.start, s.cnt, s.perm, x, y,
+                                                               g, s.x, s.y, s.g, s.hl, s.g32);
+    return pf::launch_status("k_order");
+}
+
+static pf_status count_up(int L, int32_t *cnt_all, cudaStream_t st) {
+    for (int l = L - 1; l >= 0; --l) {
+        const int64_t nb = (int64_t)1 << (2 * l);
+        k_count_up<<<(unsigned)pf::ceil_div(nb, 256), 256, 0, st>>>(
+            nb, cnt_all + level_off(l + 1), cnt_all + level_off(l));
+        PF_TRY(pf::launch_status("k_count_up"));
+    }
+    return PF_OK;
+}
+
+struct FmmArgs {
+    int64_t ns, nt;
+    const double *x, *y, *g, *xt, *yt;
+    double ksigmasqr, cutoff, tol;
+    int ndirect;
+    double *vx, *vy;
+};
+
+template <int NP>
+static pf_status run_fmm(pf_ctx *ctx, const FmmArgs &a, int L, int kb, double x0, double y0,
+                         double w0, FmmCache &c, cudaStream_t st) {
+    const bool same = (a.xt == a.x && a.yt == a.y && a.nt == a.ns);
+    const double wl = std::ldexp(w0, -L);
+    const int64_t nleaf = (int64_t)1 << (2 * L);
+    const int64_t nbox = level_off(L + 1);
+    const int64_t ns = a.ns, nt = a.nt;
+    size_t need = 0;
+    auto add = [&](size_t b) { need += pf::align256(b); };
+    add(4 * ns); add(4 * ns); add(4 * ns);          // key rank perm
+    add(8 * ns); add(8 * ns); add(8 * ns);          // x y g
+    add(16 * ns); add(4 * ns);                      // hl g32
+    if (!same) {
+        add(4 * nt); add(4 * nt); add(4 * nt);
+        add(8 * nt); add(8 * nt); add(16 * nt);
+    }
+    add(4 * nt);                                    // sorted target keys
+    add(4 * nbox); add(4 * nbox);                   // counts (all levels) src, tgt
+    add(4 * nleaf); add(4 * nleaf);                 // starts src, tgt
+    add(16 * (size_t)nbox * NP); add(16 * (size_t)nbox * NP);  // M, L
+    add(16 * nt);                                   // near velocities
+    add(4 * pf::scan_tmp_ints(nleaf));
+    need += 4096;
+    PF_TRY(pf::arena_reserve(ctx, need));
+    auto take = [&](size_t b) { return pf::arena_take(ctx, b); };
+    Sorted S, T;
+    S.key = (uint32_t *)take(4 * ns);
+    S.rank = (int32_t *)take(4 * ns);
+    S.perm = (int32_t *)take(4 * ns);
+    S.x = (double *)take(8 * ns);
+    S.y = (double *)take(8 * ns);
+    S.g = (double *)take(8 * ns);
+    S.hl = (float4 *)take(16 * ns);
+    S.g32 = (float *)take(4 * ns);
+    if (!same) {
+        T.key = (uint32_t *)take(4 * nt);
+        T.rank = (int32_t *)take(4 * nt);
+        T.perm = (int32_t *)take(4 * nt);
+        T.x = (double *)take(8 * nt);
+        T.y = (double *)take(8 * nt);
+        T.hl = (float4 *)take(16 * nt);
+    }
+    uint32_t *tkey_sorted = (uint32_t *)take(4 * nt);
+    int32_t *scnt_all = (int32_t *)take(4 * nbox);
+    int32_t *tcnt_all = (int32_t *)take(4 * nbox);
+    S.cnt = scnt_all + level_off(L);
+    S.start = (int32_t *)take(4 * nleaf);
+    int32_t *tstart = (int32_t *)take(4 * nleaf);
+    double2 *M = (double2 *)take(16 * (size_t)nbox * NP);
+    double2 *Lc = (double2 *)take(16 * (size_t)nbox * NP);
+    double2 *nearv = (double2 *)take(16 * nt);
+    int32_t *tmp = (int32_t *)take(4 * pf::scan_tmp_ints(nleaf));
+    if (!tmp) {
+        pf::set_error("pf_velocity_fmm: scratch layout error");
+        return PF_ERR_OOM;
+    }
+    if (same) {
+        T = S;
+        T.cnt = tcnt_all + level_off(L);
+        T.start = tstart;
+    } else {
+        T.cnt = tcnt_all + level_off(L);
+        T.start = tstart;
+    }
+
+    // sort sources (and targets)
+    PF_TRY(sort_points(ctx, ns, a.x, a.y, a.g, x0, y0, wl, L, S, tmp, st));
+    if (same) {
+        PF_CUDA_TRY(cudaMemcpyAsync(T.cnt, S.cnt, 4 * nleaf, cudaMemcpyDeviceToDevice, st));
+        PF_CUDA_TRY(cudaMemcpyAsync(tstart, S.start, 4 * nleaf, cudaMemcpyDeviceToDevice, st));
+    } else {
+        PF_TRY(sort_points(ctx, nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, st));
+    }
+    PF_TRY(count_up(L, scnt_all, st));
+    PF_TRY(count_up(L, tcnt_all, st));
+    k_sorted_keys<<<(unsigned)pf::ceil_div(nt, 256), 256, 0, st>>>(nt, T.perm, T.key, tkey_sorted);
+    PF_TRY(pf::launch_status("k_sorted_keys"));
+
+    // upward pass
+    k_p2m<NP><<<(unsigned)pf::ceil_div(nleaf, 128), 128, 0, st>>>(L, x0, y0, wl, S.start, S.cnt,
+                                                                 S.x, S.y, S.g, M);
+    PF_TRY(pf::launch_status("k_p2m"));
+    for (int l = L - 1; l >= 2; --l) {
+        const int64_t nb = (int64_t)1 << (2 * l);
+        k_m2m<NP><<<(unsigned)pf::ceil_div(nb, WARP_BOX_THREADS / 32), WARP_BOX_THREADS, 0, st>>>(
+            l, scnt_all, M, c.d_m2m);
+        PF_TRY(pf::launch_status("k_m2m"));
+    }
+    // M2L, all levels >= 2
+    const int B = 1 << kb, Bp = B > 2 ? B : 2;
+    {
+        const int64_t bg0 = level_off(2), nbg = nbox - bg0;
+        k_m2l<NP><<<(unsigned)pf::ceil_div(nbg, WARP_BOX_THREADS / 32), WARP_BOX_THREADS, 0, st>>>(
+            L, Bp, bg0, nbg, scnt_all, tcnt_all, M, Lc, c.d_far, c.d_far_ptr, c.maxpos, c.d_pw,
+            c.d_bin);
+        PF_TRY(pf::launch_status("k_m2l"));
+    }
+    for (int l = 3; l <= L; ++l) {
+        const int64_t nb = (int64_t)1 << (2 * l);
+        k_l2l<NP><<<(unsigned)pf::ceil_div(nb, WARP_BOX_THREADS / 32), WARP_BOX_THREADS, 0, st>>>(
+            l, tcnt_all, Lc, c.d_l2l);
+        PF_TRY(pf::launch_status("k_l2l"));
+    }
+    // near field
+    {
+        const int64_t nblk = (int64_t)1 << (2 * (L - kb));
+        k_p2p<<<(unsigned)nblk, P2P_THREADS, 0, st>>>(L, kb, tstart, T.cnt, S.start, S.cnt, S.hl,
+                                                     S.g32, T.hl, c.d_q, c.nq, c.nqp,
+                                                     pfd::make_gauss_params(a.ksigmasqr), nearv);
+        PF_TRY(pf::launch_status("k_p2p"));
+    }
+    k_l2p<NP><<<(unsigned)pf::ceil_div(nt, 256), 256, 0, st>>>(nt, L, x0, y0, wl, T.x, T.y,
+                                                               tkey_sorted, Lc, nearv, T.perm,
+                                                               a.vx, a.vy);
+    return pf::launch_status("k_l2p");
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+namespace pf {
+
+struct FmmTuning {
+    int leaf_level = 0;  // 0 = automatic
+    int np = 0;          // 0 = from tol
+    int kb = 1;
+};
+static thread_local FmmTuning g_tune;
+
+static int np_for_tol(double tol) {
+    // truncation of a translation decays like theta^p; the constant is set so
+    // that the end-to-end error stays below tol on the test distributions
+    const double p = std::ceil(std::log2(1.0 / tol)) + 2.0;
+    const int want = (int)p + 1;
+    const int opts[] = {16, 20, 24, 28, 32};
+    for (int o : opts)
+        if (o >= want) return o;
+    return 32;
+}
+
+}  // namespace pf
+
+extern "C" pf_status pf_fmm_set_tuning(int leaf_level, int expansion_terms, int block_level_drop) {
+    pf::clear_error();
+    PF_CHECK_ARG(leaf_level == 0 || (leaf_level >= 2 && leaf_level <= MAX_LEVEL),
+                 "pf_fmm_set_tuning: leaf level must be 0 (auto) or in [2, %d]", MAX_LEVEL);
+    PF_CHECK_ARG(expansion_terms == 0 || expansion_terms == 16 || expansion_terms == 20 ||
+                     expansion_terms == 24 || expansion_terms == 28 || expansion_terms == 32,
+                 "pf_fmm_set_tuning: expansion terms must be 0 (auto) or one of 16,20,24,28,32");
+    PF_CHECK_ARG(block_level_drop >= 0 && block_level_drop <= 2,
+                 "pf_fmm_set_tuning: block level drop must be in [0, 2]");
+    pf::g_tune.leaf_level = leaf_level;
+    pf::g_tune.np = expansion_terms;
+    pf::g_tune.kb = block_level_drop;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_fmm_tree_keys(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                                      double x0, double y0, double leaf_width, int leaf_level,
+                                      uint32_t *keys, void *stream) {
+    pf::clear_error();
+    PF_CHECK_ARG(ctx != nullptr, "pf_fmm_tree_keys: NULL context");
+    PF_CHECK_ARG(leaf_level >= 1 && leaf_level <= 15, "pf_fmm_tree_keys: leaf level outside [1, 15]");
+    PF_CHECK_ARG(leaf_width > 0.0, "pf_fmm_tree_keys: leaf width must be positive");
+    PF_CHECK_ARG(n >= 0 && (n == 0 || (x && y && keys)), "pf_fmm_tree_keys: bad arrays");
+    pf::DeviceGuard dg(ctx->device);
+    if (n == 0) return PF_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    k_leaf_keys<<<(unsigned)pf::ceil_div(n, 256), 256, 0, st>>>(x, y, n, x0, y0, leaf_width,
+                                                               leaf_level, keys, nullptr, nullptr);
+    return pf::launch_status("k_leaf_keys");
 }
 
 extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x, const double *y,
@@ -14,11 +888,89 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
                                      double *vy, void *stream) {
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_velocity_fmm: NULL context");
+    PF_CHECK_ARG(n_src >= 0 && n_tgt >= 0 && n_src < ((int64_t)1 << 31) &&
+                     n_tgt < ((int64_t)1 << 31),
+                 "pf_velocity_fmm: sizes outside [0, 2^31)");
+    PF_CHECK_ARG(ksigmasqr > 0.0 && std::isfinite(ksigmasqr), "pf_velocity_fmm: bad ksigmasqr");
+    PF_CHECK_ARG(std::isfinite(cutoff) && cutoff >= 0.0, "pf_velocity_fmm: bad cutoff");
+    PF_CHECK_ARG(tol >= 0.0 && tol < 1.0, "pf_velocity_fmm: tol must be in [0, 1)");
+    PF_CHECK_ARG(n_src == 0 || (x && y && g), "pf_velocity_fmm: NULL blob array");
+    PF_CHECK_ARG(n_tgt == 0 || (xt && yt && vx && vy), "pf_velocity_fmm: NULL target array");
     (void)xopt;
-    (void)cutoff;
-    (void)ndirect;
-    if (tol == 0.0)
-        return pf_velocity_direct(ctx, n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, stream);
-    pf::set_error("pf_velocity_fmm: FMM path not built yet");
-    return PF_ERR_NOT_BUILT;
+    pf::DeviceGuard dg(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n_tgt == 0) return PF_OK;
+    if (n_src == 0) {
+        PF_CUDA_TRY(cudaMemsetAsync(vx, 0, sizeof(double) * n_tgt, st));
+        PF_CUDA_TRY(cudaMemsetAsync(vy, 0, sizeof(double) * n_tgt, st));
+        return PF_OK;
+    }
+    if (ndirect < 1) ndirect = 1;
+    // leaf level: as the reference's level count, ceil(log4(N / Ndirect))
+    int L = pf::g_tune.leaf_level;
+    if (L == 0) {
+        L = (int)std::ceil(0.5 * std::log2((double)n_src / (double)ndirect));
+        L = std::min(std::max(L, 0), MAX_LEVEL);
+    }
+    if (tol == 0.0 || L < 3)
+        return pf::launch_direct(n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
+    const int np = pf::g_tune.np ? pf::g_tune.np : pf::np_for_tol(tol);
+    int kb = pf::g_tune.kb;
+
+    // bounding square of sources and targets
+    PF_TRY(pf::arena_reserve(ctx, 4096));
+    BBox *bb = static_cast<BBox *>(pf::arena_take(ctx, sizeof(BBox)));
+    k_bbox_init<<<1, 1, 0, st>>>(bb);
+    PF_TRY(pf::launch_status("k_bbox_init"));
+    const int cap = ctx->num_sms * 4;
+    k_bbox<<<(unsigned)std::min<int64_t>(pf::ceil_div(n_src, 256), cap), 256, 0, st>>>(x, y, n_src, bb);
+    PF_TRY(pf::launch_status("k_bbox"));
+    if (!(xt == x && yt == y)) {
+        k_bbox<<<(unsigned)std::min<int64_t>(pf::ceil_div(n_tgt, 256), cap), 256, 0, st>>>(xt, yt,
+                                                                                      n_tgt, bb);
+        PF_TRY(pf::launch_status("k_bbox"));
+    }
+    BBox hb;
+    PF_CUDA_TRY(cudaMemcpyAsync(ctx->host_small, bb, sizeof(BBox), cudaMemcpyDeviceToHost, st));
+    PF_CUDA_TRY(cudaStreamSynchronize(st));
+    memcpy(&hb, ctx->host_small, sizeof(BBox));
+    if (hb.bad) {
+        pf::set_error("pf_velocity_fmm: NaN or Inf coordinate");
+        return PF_ERR_NAN_INPUT;
+    }
+    const double xmin = unord_d(hb.mnx), xmax = unord_d(hb.mxx);
+    const double ymin = unord_d(hb.mny), ymax = unord_d(hb.mxy);
+    double w0 = std::max(xmax - xmin, ymax - ymin);
+    if (!(w0 > 0.0)) w0 = 1.0;
+    w0 *= 1.0 + 1e-9;
+    // the cutoff sets a floor on the leaf width: P2P blocks must stay bounded
+    FmmCache *cache = static_cast<FmmCache *>(ctx->fmm_cache);
+    if (!cache) {
+        cache = new FmmCache();
+        ctx->fmm_cache = cache;
+        ctx->fmm_cache_free = [](void *p) {
+            auto *c = static_cast<FmmCache *>(p);
+            c->release();
+            delete c;
+        };
+    }
+    for (;;) {
+        const double ratio = cutoff / w0;
+        if (cache->L != L || cache->kb != kb || cache->np != np || cache->ratio != ratio)
+            PF_TRY(build_cache(*cache, L, kb, np, w0, cutoff));
+        if (cache->nqp <= P2P_QMAX) break;
+        if (L <= 3) {
+            cache->release();
+            return pf::launch_direct(n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
+        }
+        --L;  // cutoff too large for this leaf width: coarser leaves
+    }
+    FmmArgs a{n_src, n_tgt, x, y, g, xt, yt, ksigmasqr, cutoff, tol, ndirect, vx, vy};
+    switch (np) {
+        case 16: return run_fmm<16>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
+        case 20: return run_fmm<20>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
+        case 24: return run_fmm<24>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
+        case 28: return run_fmm<28>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
+        default: return run_fmm<32>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
+    }
 }

@@ -7,7 +7,9 @@
 // and rotate back.  Evaluated here as
 //   theta = atan2(yP*x2, xP*(xP-x2) + yP^2)         (one atan2, same value in
 //           (-pi, pi]: the angle between the two end-point rays)
-//   log   = log1p(x2*(2xP-x2) / ((xP-x2)^2 + yP^2))  (no cancellation far away)
+//   log   = log1p(u), u = x2*(2xP-x2) / ((xP-x2)^2 + yP^2), while |u| < 1/2
+//           (no cancellation far away), else log of the ratio itself (no
+//           cancellation in 1+u next to the panel's start point)
 // Geometry and accumulation in FP64, the two transcendentals in FP32.
 // Panels are staged through shared memory in tiles; one target per thread.
 #include "pf_common.cuh"
@@ -64,7 +66,11 @@ k_panel_velocity(int64_t m, const double *__restrict__ gamma, const double *__re
             const double den_t = xp * xm + yp * yp;
             const double num_l = q.x2 * (2.0 * xp - q.x2);
             const float theta = atan2f((float)num_t, (float)den_t);
-            const float lg = log1pf((float)num_l / (float)a2);
+            // log(b2/a2): log1p of u = (b2 - a2)/a2 while |u| < 1/2, else the
+            // log of the FP32-rounded ratio; both ~1 ulp absolute.
+            const float a2f = (float)a2;
+            const float u = (float)num_l / a2f;
+            const float lg = (fabsf(u) < 0.5f) ? log1pf(u) : logf((float)(xp * xp + yp * yp) / a2f);
             const double vxp = (q.gam * INV_2PI) * (double)theta;
             const double vyp = -(q.gam * INV_4PI) * (double)lg;
             ax += q.c * vxp - q.s * vyp;

@@ -66,6 +66,9 @@ struct pf_ctx {
     pf::Arena arena;
     // host-side pinned staging for small device->host reads
     int64_t *host_small = nullptr;
+    // FMM plan cache (tables and operators on the device), owned by fmm.cu
+    void *fmm_cache = nullptr;
+    void (*fmm_cache_free)(void *) = nullptr;
 };
 
 namespace pf {

@@ -45,6 +45,9 @@ PROTOTYPES = {
     "pf_remesh": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp, _vp, _vp,
                   _c.POINTER(_i64), _vp],
     "pf_moments": [_vp, _i64, _vp, _vp, _vp, _vp, _vp],
+    "pf_fmm_lists": [_int, _int, _dbl, _dbl, _dbl, _vp, _i64, _c.POINTER(_i64)],
+    "pf_fmm_set_tuning": [_int, _int, _int],
+    "pf_fmm_tree_keys": [_vp, _i64, _vp, _vp, _dbl, _dbl, _dbl, _int, _vp, _vp],
 }
 
 for _name, _args in PROTOTYPES.items():

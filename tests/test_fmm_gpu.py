@@ -1,0 +1,134 @@
+"""FMM blob velocity on the GPU vs the FP64 direct oracle (the reference's own
+direct Gauss sum restated; pinned to the reference Cython kernel).
+
+Gate: max_i |v_i - v_ref_i| / max_i |v_ref_i| <= 1e-6 (at the default tol)."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from conftest import normwise_err
+from oracle import lists
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+DEV = torch.device("cuda", 0)
+
+
+def T(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def fmm(x, y, g, sigma, xt=None, yt=None, tol=1e-6, ndirect=35):
+    import pfblob
+    vx, vy = pfblob.velocity(T(x), T(y), T(g), sigma, method=pfblob.FMM_METHOD, hardware=1,
+                             xEval=None if xt is None else T(xt),
+                             yEval=None if yt is None else T(yt), tol=tol, Ndirect=ndirect)
+    return vx.cpu().numpy(), vy.cpu().numpy()
+
+
+def test_c1_lamb_oseen_vs_reference_golden(golden):
+    d = golden("direct_c1")
+    vx, vy = fmm(d["x"], d["y"], d["g"], float(d["sigma"]), ndirect=8)
+    assert normwise_err(vx, vy, d["vx"], d["vy"]) <= TOL
+
+
+def test_random_vs_reference_fmm_golden(golden):
+    """Same input the reference CPU FMM was run on (tests/golden/fmm_rand)."""
+    f = golden("fmm_rand")
+    sig = float(f["sigma"])
+    vx, vy = fmm(f["x"], f["y"], f["g"], sig, ndirect=8)
+    rx, ry = oracle.velocity_direct(f["x"], f["y"], f["g"], 2 * sig * sig)
+    assert normwise_err(vx, vy, rx, ry) <= TOL
+    # and within 2e-6 of the reference's own FMM result
+    assert normwise_err(vx, vy, f["vx"], f["vy"]) <= 2e-6
+
+
+@pytest.mark.parametrize("n,sigma,seed", [(20000, 0.002, 1), (50000, 0.01, 2), (65536, 0.002, 3)])
+def test_uniform_vs_oracle(n, sigma, seed):
+    rng = np.random.default_rng(seed)
+    x, y = rng.random(n), rng.random(n)
+    g = rng.standard_normal(n) / n
+    vx, vy = fmm(x, y, g, sigma)
+    rx, ry = oracle.velocity_direct(x, y, g, 2 * sigma * sigma)
+    assert normwise_err(vx, vy, rx, ry) <= TOL
+
+
+def test_c2_full_size_subset_vs_oracle():
+    """C2 (N = 2^20, sigma = 0.002) at all blobs; oracle on 4096 of them."""
+    from pfblob import workloads as wl
+    b = wl.uniform_square()
+    vx, vy = fmm(b.x, b.y, b.g, b.sigma)
+    idx = np.random.default_rng(4).choice(b.n, 4096, replace=False)
+    rx, ry = oracle.velocity_direct(b.x, b.y, b.g, b.ksigmasqr, b.x[idx], b.y[idx])
+    assert normwise_err(vx[idx], vy[idx], rx, ry) <= TOL
+
+
+def test_shear_layer_annulus_subset():
+    """Non-uniform fill (annulus) with separate targets."""
+    from pfblob import workloads as wl
+    b = wl.shear_layer(n=1 << 18)
+    rng = np.random.default_rng(5)
+    xt = rng.uniform(-1.6, 1.6, 3000)
+    yt = rng.uniform(-1.6, 1.6, 3000)
+    vx, vy = fmm(b.x, b.y, b.g, b.sigma, xt, yt)
+    rx, ry = oracle.velocity_direct(b.x, b.y, b.g, b.ksigmasqr, xt, yt)
+    assert normwise_err(vx, vy, rx, ry) <= TOL
+
+
+def test_mixed_instance_and_clusters():
+    from pfblob import workloads as wl
+    b = wl.mixed_instance(100000, config=4, instance=1)
+    x, y, g = b.x.copy(), b.y.copy(), b.g.copy()
+    x[:5000] = 0.3 + 1e-4 * np.random.default_rng(6).standard_normal(5000)  # dense cluster
+    y[:5000] = -0.2 + 1e-4 * np.random.default_rng(7).standard_normal(5000)
+    vx, vy = fmm(x, y, g, b.sigma)
+    idx = np.random.default_rng(8).choice(x.shape[0], 3000, replace=False)
+    idx[:100] = np.arange(100)
+    rx, ry = oracle.velocity_direct(x, y, g, b.ksigmasqr, x[idx], y[idx])
+    assert normwise_err(vx[idx], vy[idx], rx, ry) <= TOL
+
+
+def test_tol_zero_is_direct_and_small_n():
+    import pfblob
+    rng = np.random.default_rng(9)
+    x, y, g = rng.random(500), rng.random(500), rng.standard_normal(500)
+    a = fmm(x, y, g, 0.01, tol=0.0)
+    b = pfblob.velocity(x, y, g, 0.01, method=1)
+    assert np.array_equal(a[0], b[0])
+    c = fmm(x, y, g, 0.01)  # too small for a tree: direct path
+    assert normwise_err(c[0], c[1], b[0], b[1]) <= TOL
+
+
+def test_deterministic_repeat():
+    from pfblob import workloads as wl
+    b = wl.uniform_square(n=200000, config=2, instance=5)
+    a = fmm(b.x, b.y, b.g, b.sigma)
+    c = fmm(b.x, b.y, b.g, b.sigma)
+    assert np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1])
+
+
+def test_morton_keys_bit_exact():
+    import pfblob._lib as lb
+    from pfblob._arrays import ptr
+    from pfblob import workloads as wl
+    b = wl.uniform_square(n=300000, config=2, instance=6)
+    x, y = T(b.x), T(b.y)
+    L = 9
+    x0, y0, w = 0.0, 0.0, 1.0 / 512
+    keys = torch.empty(b.n, dtype=torch.int32, device=DEV)
+    lb.check(lb.lib.pf_fmm_tree_keys(lb.context(0), b.n, ptr(x), ptr(y), x0, y0, w, L,
+                                     ptr(keys), None))
+    got = keys.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, lists.leaf_keys(b.x, b.y, x0, y0, w, L))
+
+
+def test_nan_input_rejected():
+    import pfblob
+    x = np.random.default_rng(1).random(5000)
+    x[7] = np.nan
+    with pytest.raises(pfblob._lib.PfError) as ei:
+        fmm(x, x, x, 0.01)
+    assert ei.value.status == 5

@@ -176,13 +176,20 @@ def run_ours(args, rank, world):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
+    fmm_stats = []
+    if method == "fmm":
+        _lib.fmm_profile(True, dev.index)
     l0 = _lib.kernel_launches()
     with ClockSampler(gpu_id_for_smi(torch)) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
             step(evs[k])
+            if method == "fmm":  # the remesh already synchronised the stream
+                fmm_stats.append(_lib.fmm_last_stats(dev.index))
         torch.cuda.synchronize()
     launches = _lib.kernel_launches() - l0
+    if method == "fmm":
+        _lib.fmm_profile(False, dev.index)
     if world > 1:
         torch.distributed.barrier()
     vel_ms = [e[0].elapsed_time(e[1]) for e in evs]
@@ -233,8 +240,36 @@ def run_ours(args, rank, world):
                                f"({pk['source']}) / {MUFU_PER_INTERACTION} MUFU per interaction",
                 "per_unit": "1 interaction = 2 MUFU (ex2, rcp) + 14 FP32 flops"}
     else:
-        roof = {"bound": "mufu", "kernel": "fmm", "achieved": None, "peak": None, "frac": None,
-                "unit": "Ginteractions/s", "traffic": None}
+        st0 = fmm_stats[-1]
+        ms_p2p = statistics.mean(f["ms_p2p"] for f in fmm_stats)
+        pairs = st0["p2p_pairs"]
+        ach = pairs / (ms_p2p * 1e-3)
+        peak = (pk["sm_max_mhz"] * 1e6 * MUFU_PER_SM_CLK * torch.cuda.get_device_properties(dev)
+                .multi_processor_count / MUFU_PER_INTERACTION)
+        roof = {"bound": "mufu", "kernel": "k_p2p (FMM near field)", "achieved": ach / 1e9,
+                "peak": peak / 1e9, "unit": "Ginteractions/s", "frac": ach / peak,
+                "traffic": traffic.get("k_p2p"), "pairs_per_launch": pairs,
+                "launch_ms": ms_p2p,
+                "peak_source": f"{MUFU_PER_SM_CLK} MUFU/SM/clk x SMs x sm_max_mhz "
+                               f"({pk['source']}) / {MUFU_PER_INTERACTION} MUFU per interaction",
+                "per_unit": "1 interaction = 2 MUFU (ex2, rcp) + 14 FP32 flops"}
+        npt = st0["expansion_terms"]
+        ms_m2l = statistics.mean(f["ms_m2l"] for f in fmm_stats)
+        m2l_flops = st0["m2l_translations"] * 8.0 * npt * npt
+        fp64_peak = 148 * 64 * 2 * pk["sm_max_mhz"] * 1e6
+        roof_m2l = {"bound": "fp64", "kernel": "k_m2l", "achieved": m2l_flops / (ms_m2l * 1e-3) / 1e12,
+                    "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
+                    "frac": m2l_flops / (ms_m2l * 1e-3) / fp64_peak,
+                    "per_unit": "8 (p+1)^2 FP64 flops per translation",
+                    "translations": st0["m2l_translations"],
+                    "peak_source": "148 SMs x 64 FP64 FMA/clk x 2 x sm_max_mhz (nominal)"}
+        fmm_info = {"leaf_level": st0["leaf_level"], "expansion_terms": npt,
+                    "block_level_drop": st0["block_level_drop"], "p2p_pairs": pairs,
+                    "m2l_translations": st0["m2l_translations"],
+                    "phase_ms": {k[3:]: statistics.mean(f[k] for f in fmm_stats)
+                                 for k in ("ms_sort", "ms_upward", "ms_m2l", "ms_downward",
+                                           "ms_p2p", "ms_l2p", "ms_total")},
+                    "roofline_m2l": roof_m2l}
     alg_bytes = 24 * n + 24 * nout
     roof_rm = {"bound": "hbm", "kernel": "remesh (all passes)", "achieved": alg_bytes / (rm_avg * 1e-3) / 1e9,
                "peak": pk["hbm_gbs"], "unit": "GB/s",
@@ -253,6 +288,7 @@ def run_ours(args, rank, world):
                    "parallelism": f"replicas x{world}"},
         "phase_ms": {"velocity": vel_avg, "remesh": rm_avg},
         "gpu_launches": launches, "roofline": roof, "roofline_remesh": roof_rm,
+        "fmm": fmm_info if method == "fmm" else None,
         "clocks": clk.summary(), "e2e": e2e,
     }
     return line

@@ -107,6 +107,25 @@ pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x, const dou
  * autotuner and experiments set them at run time. */
 pf_status pf_fmm_set_tuning(int leaf_level, int expansion_terms, int block_level_drop);
 
+/* Statistics of the last pf_velocity_fmm call on a context.  Counters are
+ * always collected (one atomic per CTA/warp); phase times only while
+ * profiling is enabled with pf_fmm_profile (CUDA events recorded on the
+ * call's stream around each phase; -1 otherwise).  pf_fmm_last_stats waits
+ * for the last call's stream. */
+typedef struct pf_fmm_stats {
+    int32_t leaf_level;       /* L (leaves are 2^L x 2^L) */
+    int32_t expansion_terms;  /* p + 1 */
+    int32_t block_level_drop; /* P2P blocks of 2^kb x 2^kb leaves */
+    int32_t used_direct;      /* 1 if the call fell back to the direct sum */
+    int64_t n_src, n_tgt;
+    int64_t p2p_pairs;        /* near-field pair interactions evaluated */
+    int64_t m2l_translations; /* multipole-to-local translations */
+    float ms_sort, ms_upward, ms_m2l, ms_downward, ms_p2p, ms_l2p, ms_total;
+    float reserved;
+} pf_fmm_stats;
+pf_status pf_fmm_profile(pf_ctx *ctx, int enable);
+pf_status pf_fmm_last_stats(pf_ctx *ctx, pf_fmm_stats *out);
+
 /* Leaf Morton keys of points for a tree with origin (x0, y0), leaf width
  * `leaf_width` and leaf level `leaf_level` (<= 15): key = interleave(qx, qy)
  * with qx = clamp(floor((x - x0)/leaf_width), 0, 2^L - 1), x in the even
@@ -179,6 +198,22 @@ pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const double *y, co
                     double *x_out, double *y_out, double *g_out, int64_t *ix_out,
                     int64_t *iy_out, int64_t *n_out, void *stream);
 
+/* Remesh onto a caller-given lattice window, with no host synchronisation
+ * (for stream-ordered pipelines and CUDA-graph capture).  The window holds the
+ * base cells ix in [ixmin, ixmin + nbx), iy in [iymin, iymin + nby) (a blob's
+ * base cell is its window-left index, as in pf_remesh); outputs span
+ * (nbx + 3) x (nby + 3) cells.  The output count is written to the DEVICE
+ * int64 *n_out_dev; if it exceeds `capacity` nothing is written.  The DEVICE
+ * int32 *status_dev (may be NULL) receives 0, or 4 if some blob lay outside
+ * the window (such blobs are skipped).  Same values and order as pf_remesh.
+ * ------------------------------------------------------------------------- */
+pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                           const double *g, double h, double xb0, double yb0, double c,
+                           int64_t ixmin, int64_t iymin, int64_t nbx, int64_t nby,
+                           int64_t capacity, double *x_out, double *y_out, double *g_out,
+                           int64_t *ix_out, int64_t *iy_out, int64_t *n_out_dev,
+                           int32_t *status_dev, void *stream);
+
 /* ---------------------------------------------------------------------------
  * FP64 moments of a blob set, written to the DEVICE array out4:
  * out4 = {sum g, sum g x, sum g y, sum |g|}, in a fixed reduction order
@@ -188,6 +223,53 @@ pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const double *y, co
  * ------------------------------------------------------------------------- */
 pf_status pf_moments(pf_ctx *ctx, int64_t n, const double *x, const double *y,
                      const double *g, double *out4, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Batched execution: many independent blob simulations (uneven sizes) per
+ * launch.  No reference counterpart: the reference evaluates one blob set per
+ * call (src/python/blobs/__blobsClass.py:546-628, :828-897).
+ *
+ * pf_batch_create plans every instance (FMM tree or direct sum, remesh
+ * lattice window), allocates all buffers and captures the whole step --
+ * velocity of every instance at its own blobs, then optionally its remesh --
+ * into one CUDA graph; pf_batch_run replays it with one graph launch on
+ * `stream`.  Direct-sum instances run together in one persistent kernel;
+ * FMM and remesh jobs run on library streams inside the graph.  The batch
+ * keeps the instance pointers: inputs may change in value between runs but
+ * not in size (create a new batch when sizes change).  Results are the same
+ * as the single-instance calls with the same method and tree.
+ * ------------------------------------------------------------------------- */
+typedef struct pf_batch_instance {
+    int64_t n;                      /* blobs */
+    const double *x, *y, *g;        /* device, n entries */
+    double *vx, *vy;                /* device, n entries: velocity at the blobs */
+    double ksigmasqr;               /* k sigma^2 */
+    double cutoff;                  /* FMM Gaussian cutoff (reference: 5 xopt) */
+    double box[4];                  /* xmin, xmax, ymin, ymax containing every blob */
+    int32_t method;                 /* PF_FMM_METHOD or PF_DIRECT_METHOD */
+    int32_t leaf_level;             /* FMM leaf level, 0 = automatic */
+    int32_t expansion_terms;        /* FMM p+1, 0 = from tol */
+    int32_t remesh;                 /* nonzero: M4' remesh after the velocity */
+    double h, xb0, yb0, c;          /* remesh lattice spacing, origin, Wee coefficient */
+    int64_t capacity;               /* remesh output capacity */
+    double *x_out, *y_out, *g_out;  /* remesh outputs, capacity entries (device) */
+} pf_batch_instance;
+
+typedef struct pf_batch pf_batch;
+
+pf_status pf_batch_create(pf_ctx *ctx, int32_t n, const pf_batch_instance *inst, double tol,
+                          int32_t n_streams, pf_batch **out);
+/* One graph launch: the whole batch step, ordered after prior work on stream. */
+pf_status pf_batch_run(pf_batch *b, void *stream);
+/* Waits for the last run; per instance: remesh output count (n_out) and
+ * status (0, or 4 if a blob lay outside its box).  Host arrays of n entries,
+ * either may be NULL. */
+pf_status pf_batch_results(pf_batch *b, int64_t *n_out, int32_t *status);
+/* Resolved method and FMM leaf level (0 for direct) per instance, and the
+ * number of kernel nodes in the captured graph (any pointer may be NULL). */
+pf_status pf_batch_info(const pf_batch *b, int32_t *methods, int32_t *leaf_levels,
+                        int64_t *kernel_nodes);
+pf_status pf_batch_destroy(pf_batch *b);
 
 #ifdef __cplusplus
 }

@@ -10,6 +10,7 @@
 // Replaces vv2par_kernel (src/cpp/blobs/cuda/vv2parGauss_gpu/
 // vv2parGauss_device.cu:107-162: FP64, one target per thread, 2 exp per pair,
 // targets padded to a multiple of the block size by the Python caller).
+#include "direct_api.cuh"
 #include "gauss_pair.cuh"
 
 namespace {
@@ -18,16 +19,17 @@ constexpr int DT_THREADS = 256;
 constexpr int DT_CHUNK = 32;
 constexpr double INV_2PI = 0.15915494309189535;  // 0.5/pi
 
+// One CTA computes the DT_THREADS*TPT targets of tile `tile`.
 template <int TPT>
-__global__ void __launch_bounds__(DT_THREADS)
-k_direct_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
-               const double *__restrict__ gs, int64_t ns, const double *__restrict__ xt,
-               const double *__restrict__ yt, int64_t nt, pfd::GaussParams gp,
-               double *__restrict__ vx, double *__restrict__ vy) {
-    __shared__ float4 s_pos[DT_THREADS];  // x_hi, y_hi, x_lo, y_lo
-    __shared__ float s_g[DT_THREADS];
-
-    const int64_t base = (int64_t)blockIdx.x * (DT_THREADS * TPT) + threadIdx.x;
+__device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
+                                            const double *__restrict__ ys,
+                                            const double *__restrict__ gs, int64_t ns,
+                                            const double *__restrict__ xt,
+                                            const double *__restrict__ yt, int64_t nt,
+                                            const pfd::GaussParams &gp, double *__restrict__ vx,
+                                            double *__restrict__ vy, int64_t tile,
+                                            float4 *s_pos, float *s_g) {
+    const int64_t base = tile * (DT_THREADS * TPT) + threadIdx.x;
     float txh[TPT], txl[TPT], tyh[TPT], tyl[TPT];
     float hx[TPT], lx[TPT], hy[TPT], ly[TPT];
 #pragma unroll
@@ -94,6 +96,39 @@ k_direct_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
     }
 }
 
+template <int TPT>
+__global__ void __launch_bounds__(DT_THREADS)
+k_direct_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
+               const double *__restrict__ gs, int64_t ns, const double *__restrict__ xt,
+               const double *__restrict__ yt, int64_t nt, pfd::GaussParams gp,
+               double *__restrict__ vx, double *__restrict__ vy) {
+    __shared__ float4 s_pos[DT_THREADS];  // x_hi, y_hi, x_lo, y_lo
+    __shared__ float s_g[DT_THREADS];
+    direct_tile<TPT>(xs, ys, gs, ns, xt, yt, nt, gp, vx, vy, blockIdx.x, s_pos, s_g);
+}
+
+// Persistent batched direct sum: CTAs take (instance, target tile) items from
+// a device counter until the list is exhausted.  Items are ordered by cost,
+// largest first; each item is computed by one CTA, so results do not depend
+// on which CTA takes it.
+__global__ void __launch_bounds__(DT_THREADS)
+k_direct_batch(const pf::DirectInstance *__restrict__ inst, const int2 *__restrict__ items,
+               int n_items, int *__restrict__ counter) {
+    __shared__ float4 s_pos[DT_THREADS];
+    __shared__ float s_g[DT_THREADS];
+    __shared__ int s_item;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const int2 w = items[it];
+        const pf::DirectInstance d = inst[w.x];
+        direct_tile<2>(d.x, d.y, d.g, d.n, d.xt, d.yt, d.nt, d.gp, d.vx, d.vy, w.y, s_pos, s_g);
+    }
+}
+
 }  // namespace
 
 namespace pf {
@@ -115,6 +150,23 @@ pf_status launch_direct(int64_t ns, const double *x, const double *y, const doub
     k_direct_gauss<TPT><<<(unsigned)grid, DT_THREADS, 0, stream>>>(x, y, g, ns, xt, yt, nt, gp,
                                                                    vx, vy);
     return launch_status("k_direct_gauss");
+}
+
+int direct_tile_targets() { return DT_THREADS * 2; }
+
+pf_status launch_direct_batch(const DirectInstance *inst_dev, const int2 *items_dev, int n_items,
+                              int *counter_dev, int grid, cudaStream_t st) {
+    PF_CUDA_TRY(cudaMemsetAsync(counter_dev, 0, sizeof(int), st));
+    if (n_items == 0) return PF_OK;
+    k_direct_batch<<<grid, DT_THREADS, 0, st>>>(inst_dev, items_dev, n_items, counter_dev);
+    return launch_status("k_direct_batch");
+}
+
+int direct_batch_grid(int num_sms) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_direct_batch, DT_THREADS, 0);
+    if (per_sm < 1) per_sm = 1;
+    return num_sms * per_sm;
 }
 
 }  // namespace pf

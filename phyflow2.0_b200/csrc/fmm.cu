@@ -34,6 +34,7 @@
 #include <memory>
 #include <vector>
 
+#include "fmm_api.cuh"
 #include "fmm_plan.cuh"
 #include "gauss_pair.cuh"
 #include "scan.cuh"
@@ -48,9 +49,12 @@ namespace {
 
 constexpr double THETA = 0.5;
 constexpr double INV_2PI = 0.15915494309189535;
-constexpr int MAX_LEVEL = 11;
-constexpr int P2P_THREADS = 128;
-constexpr int P2P_QMAX = 1024;
+constexpr int MAX_LEVEL = pf::fmmx::MAX_LEVEL;
+constexpr int P2P_SETUP_THREADS = 128;
+constexpr int P2P_QMAX = 1024;   // source leaves per P2P block
+constexpr int P2P_WARPS = 4;     // P2P blocks per CTA (one warp each)
+constexpr int P2P_RUNS_SM = 64;  // runs staged in shared memory at a time
+constexpr int P2P_TILE = 64;     // sources per warp tile
 constexpr int WARP_BOX_THREADS = 128;  // 4 warps, one box each
 constexpr unsigned INVALID_KEY = 0xFFFFFFFFu;
 
@@ -287,14 +291,16 @@ __global__ void __launch_bounds__(WARP_BOX_THREADS)
 k_m2l(int L, int Bp, int64_t bg0, int64_t nbg, const int32_t *__restrict__ scnt,
       const int32_t *__restrict__ tcnt, const double2 *__restrict__ M, double2 *__restrict__ Lc,
       const int4 *__restrict__ far, const int32_t *__restrict__ far_ptr, int maxpos,
-      const double2 *__restrict__ pw /* [nop][NP+1] */, const double *__restrict__ binom) {
-    __shared__ double s_bin[NP * NP];
+      const double2 *__restrict__ pw /* [nop][NP+1] */, const double *__restrict__ binom,
+      unsigned long long *__restrict__ ntrans) {
     __shared__ double2 s_c[WARP_BOX_THREADS / 32][32];
-    for (int t = threadIdx.x; t < NP * NP; t += WARP_BOX_THREADS) s_bin[t] = binom[t];
-    __syncthreads();
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t w = (int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid;
     if (w >= nbg) return;
+    // this lane's row of the binomial matrix C(n+k, k), n = lane, in registers
+    double brow[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) brow[k] = (lane < NP) ? binom[k * NP + lane] : 0.0;
     const int64_t bg = bg0 + w;
     if (tcnt[bg] == 0) return;
     int l = 2;
@@ -305,12 +311,14 @@ k_m2l(int L, int Bp, int64_t bg0, int64_t nbg, const int32_t *__restrict__ scnt,
     const int side = 1 << l;
     const int e0 = far_ptr[l * maxpos + pos], e1 = far_ptr[l * maxpos + pos + 1];
     double2 acc = make_double2(0.0, 0.0);
+    unsigned nt = 0;
     for (int e = e0; e < e1; ++e) {
         const int4 f = far[e];
         const int sx = ix + f.x, sy = iy + f.y;
         if (sx < 0 || sy < 0 || sx >= side || sy >= side) continue;
         const int64_t sg = level_off(l) + morton2((uint32_t)sx, (uint32_t)sy);
         if (scnt[sg] == 0) continue;
+        ++nt;
         const double2 *rp = pw + (int64_t)f.z * (NP + 1);
         if (lane < NP) {
             double2 c = cmul(M[sg * NP + lane], rp[lane]);
@@ -322,16 +330,16 @@ k_m2l(int L, int Bp, int64_t bg0, int64_t nbg, const int32_t *__restrict__ scnt,
             double ux = 0.0, uy = 0.0;
 #pragma unroll
             for (int k = 0; k < NP; ++k) {
-                const double b = s_bin[k * NP + lane];
                 const double2 c = s_c[wid][k];
-                ux = fma(b, c.x, ux);
-                uy = fma(b, c.y, uy);
+                ux = fma(brow[k], c.x, ux);
+                uy = fma(brow[k], c.y, uy);
             }
             acc = cfma(rp[lane + 1], make_double2(ux, uy), acc);
         }
         __syncwarp();
     }
     if (lane < NP) Lc[bg * NP + lane] = acc;
+    if (lane == 0 && nt) atomicAdd(ntrans, (unsigned long long)nt);
 }
 
 // L2L into child level l: one warp per child box
@@ -359,28 +367,20 @@ k_l2l(int l, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
 }
 
 // ---------------------------------------------------------------------------
-// P2P near field: one CTA per P2P block (level L - kb box)
-__global__ void __launch_bounds__(P2P_THREADS)
-k_p2p(int L, int kb, const int32_t *__restrict__ tstart, const int32_t *__restrict__ tcnt,
-      const int32_t *__restrict__ sstart, const int32_t *__restrict__ scnt,
-      const float4 *__restrict__ shl, const float *__restrict__ sg32,
-      const float4 *__restrict__ thl, const int2 *__restrict__ q, int nq, int nqp,
-      pfd::GaussParams gp, double2 *__restrict__ nearv) {
+// P2P run lists (once per plan; geometry only).  For P2P block b, the source
+// leaves b's origin + q are sorted by Morton index and merged into runs of
+// consecutive indices; consecutive leaves are contiguous in the sorted
+// particle arrays, so a run is one particle range.  Pass 1 (runs == nullptr)
+// writes the run count of each block, pass 2 the runs (first, last leaf).
+__global__ void __launch_bounds__(P2P_SETUP_THREADS)
+k_p2p_runs(int L, int kb, const int2 *__restrict__ q, int nq, int nqp,
+           int32_t *__restrict__ nruns_or_off, int2 *__restrict__ runs) {
     __shared__ uint32_t s_key[P2P_QMAX];
-    __shared__ int s_rstart[P2P_QMAX + 1];  // particle start of run r
-    __shared__ int s_rpre[P2P_QMAX + 1];    // stream prefix of run r
-    __shared__ int s_nruns;
-    __shared__ float4 s_pos[P2P_THREADS];
-    __shared__ float s_g[P2P_THREADS];
+    __shared__ int s_n;
     const uint32_t b = blockIdx.x;
-    const uint32_t leaf0 = b << (2 * kb), nl = 1u << (2 * kb);
-    const int t0 = tstart[leaf0];
-    const int tn = tstart[leaf0 + nl - 1] + tcnt[leaf0 + nl - 1] - t0;
-    if (tn == 0) return;
     const int ox = (int)(compact1by1(b) << kb), oy = (int)(compact1by1(b >> 1) << kb);
     const int side = 1 << L;
-    // 1. source leaves of the block, sorted
-    for (int t = threadIdx.x; t < nqp; t += P2P_THREADS) {
+    for (int t = threadIdx.x; t < nqp; t += P2P_SETUP_THREADS) {
         uint32_t k = INVALID_KEY;
         if (t < nq) {
             const int lx = ox + q[t].x, ly = oy + q[t].y;
@@ -391,7 +391,7 @@ k_p2p(int L, int kb, const int32_t *__restrict__ tstart, const int32_t *__restri
     __syncthreads();
     for (int kk = 2; kk <= nqp; kk <<= 1) {
         for (int j = kk >> 1; j > 0; j >>= 1) {
-            for (int t = threadIdx.x; t < nqp; t += P2P_THREADS) {
+            for (int t = threadIdx.x; t < nqp; t += P2P_SETUP_THREADS) {
                 const int p = t ^ j;
                 if (p > t) {
                     const uint32_t a = s_key[t], c = s_key[p];
@@ -405,94 +405,159 @@ k_p2p(int L, int kb, const int32_t *__restrict__ tstart, const int32_t *__restri
             __syncthreads();
         }
     }
-    // 2. runs of consecutive Morton leaves (contiguous particle ranges)
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
-        int nr = 0, pre = 0;
+        int nr = 0;
+        const int base_out = runs ? nruns_or_off[b] : 0;
         for (int base = 0; base < nqp; base += 32) {
             const int t = base + lane;
             const uint32_t k = (t < nqp) ? s_key[t] : INVALID_KEY;
             const bool valid = k != INVALID_KEY;
             const bool head = valid && (t == 0 || s_key[t - 1] + 1u != k);
-            const unsigned hm = __ballot_sync(0xffffffffu, head);
-            // a run ends at t if valid and (next invalid or next not consecutive)
             const uint32_t kn = (t + 1 < nqp) ? s_key[t + 1] : INVALID_KEY;
             const bool tail = valid && (kn == INVALID_KEY || kn != k + 1u);
-            // heads: record particle start; tails: record run length
-            if (head) {
-                const int r = nr + __popc(hm & ((1u << lane) - 1u));
-                s_rstart[r] = sstart[k];
-            }
-            // tails close runs in order: the run index of a tail is the number
-            // of heads at or before it, minus one
-            if (tail) {
-                const int r = nr + __popc(hm & ((2u << lane) - 1u)) - 1;
-                s_rpre[r + 1] = sstart[k] + scnt[k];  // end particle (temporarily)
+            const unsigned hm = __ballot_sync(0xffffffffu, head);
+            if (runs) {
+                if (head) runs[base_out + nr + __popc(hm & ((1u << lane) - 1u))].x = (int)k;
+                // the run index of a tail is the number of heads at or before it, minus one
+                if (tail) runs[base_out + nr + __popc(hm & ((2u << lane) - 1u)) - 1].y = (int)k;
             }
             nr += __popc(hm);
-            __syncwarp();
         }
-        // convert run ends into stream prefix sums
-        if (lane == 0) {
-            s_rpre[0] = 0;
-            for (int r = 0; r < nr; ++r) {
-                const int len = s_rpre[r + 1] - s_rstart[r];
-                s_rpre[r + 1] = pre + len;
-                pre += len;
-            }
-            s_nruns = nr;
-        }
+        if (lane == 0) s_n = nr;
     }
     __syncthreads();
-    const int nr = s_nruns;
-    const int S = s_rpre[nr];
-    // 3. targets in passes of P2P_THREADS
-    for (int tp = 0; tp < tn; tp += P2P_THREADS) {
-        const int ti = tp + threadIdx.x;
-        float4 th = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (ti < tn) th = thl[t0 + ti];
-        float hx = 0.f, lx = 0.f, hy = 0.f, ly = 0.f;
-        for (int s0 = 0; s0 < S; s0 += P2P_THREADS) {
-            const int p = s0 + threadIdx.x;
-            float4 sp = make_float4(0.f, 0.f, 0.f, 0.f);
-            float gg = 0.f;
-            if (p < S) {
-                int lo = 0, hi = nr - 1;  // largest r with rpre[r] <= p
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s_rpre[mid] <= p) lo = mid;
-                    else hi = mid - 1;
-                }
-                const int src = s_rstart[lo] + (p - s_rpre[lo]);
-                sp = shl[src];
-                gg = sg32[src];
-            }
-            __syncthreads();
-            s_pos[threadIdx.x] = sp;
-            s_g[threadIdx.x] = gg;
-            __syncthreads();
-            const int cntt = min(P2P_THREADS, S - s0);
-            for (int c0 = 0; c0 < cntt; c0 += 32) {
-                float px = 0.f, py = 0.f;
+    if (!runs && threadIdx.x == 0) nruns_or_off[b] = s_n;
+}
+
+// P2P near field: one warp per P2P block, two targets per lane (a group of
+// 64), warp-private source tiles of 64 (no CTA barriers, so blocks with few
+// targets leave no idle target slots behind).
+template <bool TWO>
+__device__ __forceinline__ void p2p_tile(const float4 *__restrict__ sp, const float *__restrict__ sg,
+                                         int cnt, const float4 &ta, const float4 &tb,
+                                         const pfd::GaussParams &gp, float (&acc)[8]) {
+    for (int c0 = 0; c0 < cnt; c0 += 32) {
+        float pxa = 0.f, pya = 0.f, pxb = 0.f, pyb = 0.f;
 #pragma unroll 4
-                for (int k = 0; k < 32; ++k) {
-                    const float4 qq = s_pos[c0 + k];
-                    const float dx = (th.x - qq.x) + (th.z - qq.z);
-                    const float dy = (th.y - qq.y) + (th.w - qq.w);
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
-                    const float sc = pfd::gauss_s(r2, s_g[c0 + k], gp);
-                    px = fmaf(-dy, sc, px);
-                    py = fmaf(dx, sc, py);
-                }
-                pfd::comp_add(hx, lx, px);
-                pfd::comp_add(hy, ly, py);
+        for (int k = 0; k < 32; ++k) {
+            const float4 qq = sp[c0 + k];
+            const float g = sg[c0 + k];
+            {
+                const float dx = (ta.x - qq.x) + (ta.z - qq.z);
+                const float dy = (ta.y - qq.y) + (ta.w - qq.w);
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
+                const float sc = pfd::gauss_s(r2, g, gp);
+                pxa = fmaf(-dy, sc, pxa);
+                pya = fmaf(dx, sc, pya);
+            }
+            if (TWO) {
+                const float dx = (tb.x - qq.x) + (tb.z - qq.z);
+                const float dy = (tb.y - qq.y) + (tb.w - qq.w);
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
+                const float sc = pfd::gauss_s(r2, g, gp);
+                pxb = fmaf(-dy, sc, pxb);
+                pyb = fmaf(dx, sc, pyb);
             }
         }
-        if (ti < tn)
-            nearv[t0 + ti] = make_double2(INV_2PI * ((double)hx + (double)lx),
-                                          INV_2PI * ((double)hy + (double)ly));
-        __syncthreads();
+        pfd::comp_add(acc[0], acc[1], pxa);
+        pfd::comp_add(acc[2], acc[3], pya);
+        if (TWO) {
+            pfd::comp_add(acc[4], acc[5], pxb);
+            pfd::comp_add(acc[6], acc[7], pyb);
+        }
     }
+}
+
+__global__ void __launch_bounds__(P2P_WARPS * 32)
+k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *__restrict__ tcnt,
+      const int32_t *__restrict__ sstart, const int32_t *__restrict__ scnt,
+      const float4 *__restrict__ shl, const float *__restrict__ sg32,
+      const float4 *__restrict__ thl, const int32_t *__restrict__ run_off,
+      const int2 *__restrict__ runs, pfd::GaussParams gp, double2 *__restrict__ nearv,
+      unsigned long long *__restrict__ pairs) {
+    __shared__ int s_rs[P2P_WARPS][P2P_RUNS_SM];      // particle start of run
+    __shared__ int s_rp[P2P_WARPS][P2P_RUNS_SM + 1];  // stream prefix of run
+    __shared__ float4 s_pos[P2P_WARPS][P2P_TILE];
+    __shared__ float s_g[P2P_WARPS][P2P_TILE];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t b = (int64_t)blockIdx.x * P2P_WARPS + wid;
+    if (b >= nblk) return;
+    const uint32_t leaf0 = (uint32_t)b << (2 * kb), nl = 1u << (2 * kb);
+    const int t0 = tstart[leaf0];
+    const int tn = tstart[leaf0 + nl - 1] + tcnt[leaf0 + nl - 1] - t0;
+    if (tn == 0) return;
+    const int r0 = run_off[b], r1 = run_off[b + 1];
+    unsigned long long npairs = 0;
+    for (int tg = 0; tg < tn; tg += 64) {
+        const int ia = tg + lane, ib = tg + 32 + lane;
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 ta = (ia < tn) ? thl[t0 + ia] : z4;
+        const float4 tb = (ib < tn) ? thl[t0 + ib] : z4;
+        const bool two = (tg + 32 < tn);  // warp-uniform
+        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int rc = r0; rc < r1; rc += P2P_RUNS_SM) {
+            const int nrc = min(P2P_RUNS_SM, r1 - rc);
+            int pre = 0;
+            for (int k0 = 0; k0 < nrc; k0 += 32) {
+                const int k = k0 + lane;
+                int st = 0, len = 0;
+                if (k < nrc) {
+                    const int2 rr = runs[rc + k];
+                    st = sstart[rr.x];
+                    len = sstart[rr.y] + scnt[rr.y] - st;
+                }
+                int inc = len;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += t;
+                }
+                if (k < nrc) {
+                    s_rs[wid][k] = st;
+                    s_rp[wid][k] = pre + inc - len;
+                }
+                pre += __shfl_sync(0xffffffffu, inc, 31);
+            }
+            if (lane == 0) s_rp[wid][nrc] = pre;
+            __syncwarp();
+            const int S = pre;
+            npairs += (unsigned long long)S * (unsigned long long)min(64, tn - tg);
+            for (int s0 = 0; s0 < S; s0 += P2P_TILE) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int p = s0 + h * 32 + lane;
+                    float4 spv = z4;
+                    float gg = 0.f;
+                    if (p < S) {
+                        int lo = 0, hi = nrc - 1;  // largest r with prefix <= p
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (s_rp[wid][mid] <= p) lo = mid;
+                            else hi = mid - 1;
+                        }
+                        const int src = s_rs[wid][lo] + (p - s_rp[wid][lo]);
+                        spv = shl[src];
+                        gg = sg32[src];
+                    }
+                    s_pos[wid][h * 32 + lane] = spv;
+                    s_g[wid][h * 32 + lane] = gg;
+                }
+                __syncwarp();
+                const int cnt = min(P2P_TILE, S - s0);
+                if (two) p2p_tile<true>(s_pos[wid], s_g[wid], cnt, ta, tb, gp, acc);
+                else p2p_tile<false>(s_pos[wid], s_g[wid], cnt, ta, tb, gp, acc);
+                __syncwarp();
+            }
+        }
+        if (ia < tn)
+            nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),
+                                          INV_2PI * ((double)acc[2] + (double)acc[3]));
+        if (ib < tn)
+            nearv[t0 + ib] = make_double2(INV_2PI * ((double)acc[4] + (double)acc[5]),
+                                          INV_2PI * ((double)acc[6] + (double)acc[7]));
+    }
+    if (lane == 0) atomicAdd(pairs, npairs);
 }
 
 // L2P + near + scatter to input order: one thread per sorted target
@@ -532,10 +597,14 @@ k_sorted_keys(int64_t n, const int32_t *__restrict__ perm, const uint32_t *__res
 struct FmmCache {
     int L = -1, kb = -1, np = -1;
     double ratio = -1.0;  // cutoff / root width
+    double x0 = 0.0, y0 = 0.0, w0 = 1.0;  // root box of the current call
     int maxpos = 0, nq = 0, nqp = 0;
     int4 *d_far = nullptr;
     int32_t *d_far_ptr = nullptr;
     int2 *d_q = nullptr;
+    int32_t *d_run_off = nullptr;  // [nblk + 1]
+    int2 *d_runs = nullptr;        // (first, last) leaf of each run
+    int64_t nruns = 0;
     double2 *d_pw = nullptr, *d_m2m = nullptr, *d_l2l = nullptr;
     double *d_bin = nullptr;
     void release() {
@@ -546,6 +615,10 @@ struct FmmCache {
         cudaFree(d_m2m);
         cudaFree(d_l2l);
         cudaFree(d_bin);
+        cudaFree(d_run_off);
+        cudaFree(d_runs);
+        d_run_off = nullptr;
+        d_runs = nullptr;
         d_far = nullptr;
         d_far_ptr = nullptr;
         d_q = nullptr;
@@ -654,6 +727,32 @@ static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, doub
     PF_TRY(upload(&c.d_m2m, m2m));
     PF_TRY(upload(&c.d_l2l, l2l));
     PF_TRY(upload(&c.d_bin, bin));
+    if (c.nqp <= P2P_QMAX) {
+        // P2P run lists of every block (geometry only, reused by every call)
+        const int64_t nblk = (int64_t)1 << (2 * (L - kb));
+        PF_CUDA_TRY(cudaMalloc(&c.d_run_off, sizeof(int32_t) * (nblk + 1)));
+        k_p2p_runs<<<(unsigned)nblk, P2P_SETUP_THREADS>>>(L, kb, c.d_q, c.nq, c.nqp, c.d_run_off,
+                                                          nullptr);
+        PF_TRY(pf::launch_status("k_p2p_runs"));
+        std::vector<int32_t> cnt(nblk + 1, 0);
+        PF_CUDA_TRY(cudaMemcpy(cnt.data(), c.d_run_off, sizeof(int32_t) * nblk,
+                               cudaMemcpyDeviceToHost));
+        int64_t acc = 0;
+        for (int64_t b = 0; b < nblk; ++b) {
+            const int32_t v = cnt[b];
+            cnt[b] = (int32_t)acc;
+            acc += v;
+        }
+        cnt[nblk] = (int32_t)acc;
+        c.nruns = acc;
+        PF_CUDA_TRY(cudaMemcpy(c.d_run_off, cnt.data(), sizeof(int32_t) * (nblk + 1),
+                               cudaMemcpyHostToDevice));
+        PF_CUDA_TRY(cudaMalloc(&c.d_runs, sizeof(int2) * (acc > 0 ? acc : 1)));
+        k_p2p_runs<<<(unsigned)nblk, P2P_SETUP_THREADS>>>(L, kb, c.d_q, c.nq, c.nqp, c.d_run_off,
+                                                          c.d_runs);
+        PF_TRY(pf::launch_status("k_p2p_runs"));
+        PF_CUDA_TRY(cudaDeviceSynchronize());
+    }
     c.L = L;
     c.kb = kb;
     c.np = np;
@@ -669,7 +768,7 @@ struct Sorted {
     float *g32 = nullptr;
 };
 
-static pf_status sort_points(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+static pf_status sort_points(int64_t n, const double *x, const double *y,
                              const double *g, double x0, double y0, double wl, int L, Sorted &s,
                              int32_t *scan_tmp, cudaStream_t st) {
     const int64_t nleaf = (int64_t)1 << (2 * L);
@@ -707,14 +806,10 @@ struct FmmArgs {
     double *vx, *vy;
 };
 
-template <int NP>
-static pf_status run_fmm(pf_ctx *ctx, const FmmArgs &a, int L, int kb, double x0, double y0,
-                         double w0, FmmCache &c, cudaStream_t st) {
-    const bool same = (a.xt == a.x && a.yt == a.y && a.nt == a.ns);
-    const double wl = std::ldexp(w0, -L);
+static size_t fmm_scratch_bytes(const FmmCache &c, int64_t ns, int64_t nt, bool same) {
+    const int L = c.L, NP = c.np;
     const int64_t nleaf = (int64_t)1 << (2 * L);
     const int64_t nbox = level_off(L + 1);
-    const int64_t ns = a.ns, nt = a.nt;
     size_t need = 0;
     auto add = [&](size_t b) { need += pf::align256(b); };
     add(4 * ns); add(4 * ns); add(4 * ns);          // key rank perm
@@ -730,9 +825,24 @@ static pf_status run_fmm(pf_ctx *ctx, const FmmArgs &a, int L, int kb, double x0
     add(16 * (size_t)nbox * NP); add(16 * (size_t)nbox * NP);  // M, L
     add(16 * nt);                                   // near velocities
     add(4 * pf::scan_tmp_ints(nleaf));
-    need += 4096;
-    PF_TRY(pf::arena_reserve(ctx, need));
-    auto take = [&](size_t b) { return pf::arena_take(ctx, b); };
+    return need + 4096;
+}
+
+// Run the FMM for one blob set on `st` with a built plan and a scratch region
+// of fmm_scratch_bytes(); enqueues kernels only (no host synchronisation).
+// ctr: 2 device counters (P2P pairs, M2L translations), zeroed here.
+// ev: 7 events recorded around the phases, or nullptr.
+template <int NP>
+static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c,
+                          unsigned long long *ctr, cudaEvent_t *ev, cudaStream_t st) {
+    const int L = c.L, kb = c.kb;
+    const double x0 = c.x0, y0 = c.y0, w0 = c.w0;
+    const bool same = (a.xt == a.x && a.yt == a.y && a.nt == a.ns);
+    const double wl = std::ldexp(w0, -L);
+    const int64_t nleaf = (int64_t)1 << (2 * L);
+    const int64_t nbox = level_off(L + 1);
+    const int64_t ns = a.ns, nt = a.nt;
+    auto take = [&](size_t b) { return sc.take(b); };
     Sorted S, T;
     S.key = (uint32_t *)take(4 * ns);
     S.rank = (int32_t *)take(4 * ns);
@@ -773,19 +883,26 @@ static pf_status run_fmm(pf_ctx *ctx, const FmmArgs &a, int L, int kb, double x0
         T.start = tstart;
     }
 
+    PF_CUDA_TRY(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st));
+    auto mark = [&](int k) -> pf_status {
+        if (ev) PF_CUDA_TRY(cudaEventRecord(ev[k], st));
+        return PF_OK;
+    };
+    PF_TRY(mark(0));
     // sort sources (and targets)
-    PF_TRY(sort_points(ctx, ns, a.x, a.y, a.g, x0, y0, wl, L, S, tmp, st));
+    PF_TRY(sort_points(ns, a.x, a.y, a.g, x0, y0, wl, L, S, tmp, st));
     if (same) {
         PF_CUDA_TRY(cudaMemcpyAsync(T.cnt, S.cnt, 4 * nleaf, cudaMemcpyDeviceToDevice, st));
         PF_CUDA_TRY(cudaMemcpyAsync(tstart, S.start, 4 * nleaf, cudaMemcpyDeviceToDevice, st));
     } else {
-        PF_TRY(sort_points(ctx, nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, st));
+        PF_TRY(sort_points(nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, st));
     }
     PF_TRY(count_up(L, scnt_all, st));
     PF_TRY(count_up(L, tcnt_all, st));
     k_sorted_keys<<<(unsigned)pf::ceil_div(nt, 256), 256, 0, st>>>(nt, T.perm, T.key, tkey_sorted);
     PF_TRY(pf::launch_status("k_sorted_keys"));
 
+    PF_TRY(mark(1));
     // upward pass
     k_p2m<NP><<<(unsigned)pf::ceil_div(nleaf, 128), 128, 0, st>>>(L, x0, y0, wl, S.start, S.cnt,
                                                                  S.x, S.y, S.g, M);
@@ -796,33 +913,38 @@ static pf_status run_fmm(pf_ctx *ctx, const FmmArgs &a, int L, int kb, double x0
             l, scnt_all, M, c.d_m2m);
         PF_TRY(pf::launch_status("k_m2m"));
     }
+    PF_TRY(mark(2));
     // M2L, all levels >= 2
     const int B = 1 << kb, Bp = B > 2 ? B : 2;
     {
         const int64_t bg0 = level_off(2), nbg = nbox - bg0;
         k_m2l<NP><<<(unsigned)pf::ceil_div(nbg, WARP_BOX_THREADS / 32), WARP_BOX_THREADS, 0, st>>>(
             L, Bp, bg0, nbg, scnt_all, tcnt_all, M, Lc, c.d_far, c.d_far_ptr, c.maxpos, c.d_pw,
-            c.d_bin);
+            c.d_bin, ctr + 1);
         PF_TRY(pf::launch_status("k_m2l"));
     }
+    PF_TRY(mark(3));
     for (int l = 3; l <= L; ++l) {
         const int64_t nb = (int64_t)1 << (2 * l);
         k_l2l<NP><<<(unsigned)pf::ceil_div(nb, WARP_BOX_THREADS / 32), WARP_BOX_THREADS, 0, st>>>(
             l, tcnt_all, Lc, c.d_l2l);
         PF_TRY(pf::launch_status("k_l2l"));
     }
+    PF_TRY(mark(4));
     // near field
     {
         const int64_t nblk = (int64_t)1 << (2 * (L - kb));
-        k_p2p<<<(unsigned)nblk, P2P_THREADS, 0, st>>>(L, kb, tstart, T.cnt, S.start, S.cnt, S.hl,
-                                                     S.g32, T.hl, c.d_q, c.nq, c.nqp,
-                                                     pfd::make_gauss_params(a.ksigmasqr), nearv);
+        k_p2p<<<(unsigned)pf::ceil_div(nblk, P2P_WARPS), P2P_WARPS * 32, 0, st>>>(
+            nblk, kb, tstart, T.cnt, S.start, S.cnt, S.hl, S.g32, T.hl, c.d_run_off, c.d_runs,
+            pfd::make_gauss_params(a.ksigmasqr), nearv, ctr);
         PF_TRY(pf::launch_status("k_p2p"));
     }
+    PF_TRY(mark(5));
     k_l2p<NP><<<(unsigned)pf::ceil_div(nt, 256), 256, 0, st>>>(nt, L, x0, y0, wl, T.x, T.y,
                                                                tkey_sorted, Lc, nearv, T.perm,
                                                                a.vx, a.vy);
-    return pf::launch_status("k_l2p");
+    PF_TRY(pf::launch_status("k_l2p"));
+    return mark(6);
 }
 
 }  // namespace
@@ -837,15 +959,29 @@ struct FmmTuning {
 };
 static thread_local FmmTuning g_tune;
 
-static int np_for_tol(double tol) {
-    // truncation of a translation decays like theta^p; the constant is set so
-    // that the end-to-end error stays below tol on the test distributions
-    const double p = std::ceil(std::log2(1.0 / tol)) + 2.0;
-    const int want = (int)p + 1;
+int fmmx::np_for_tol(double tol) {
+    // Truncation after p+1 terms is bounded by ~theta^(p+1) per translation
+    // (theta = 1/2), but the measured end-to-end error is far below that bound:
+    // with 16 terms the point-vortex limit (theta-bound at every level) and the
+    // Gaussian configurations all stay near 1e-7 at tol = 1e-6, where the FP32
+    // near field sets the floor.  So p+1 = log2(1/tol) - 4, rounded up to an
+    // instantiated size.
+    const int want = (int)std::ceil(std::log2(1.0 / tol)) - 4;
     const int opts[] = {16, 20, 24, 28, 32};
     for (int o : opts)
         if (o >= want) return o;
     return 32;
+}
+
+pf_status fmm_exec(const FmmCache &c, Bump &sc, const FmmArgs &a, unsigned long long *ctr,
+                   cudaEvent_t *ev, cudaStream_t st) {
+    switch (c.np) {
+        case 16: return exec_fmm<16>(sc, a, c, ctr, ev, st);
+        case 20: return exec_fmm<20>(sc, a, c, ctr, ev, st);
+        case 24: return exec_fmm<24>(sc, a, c, ctr, ev, st);
+        case 28: return exec_fmm<28>(sc, a, c, ctr, ev, st);
+        default: return exec_fmm<32>(sc, a, c, ctr, ev, st);
+    }
 }
 
 }  // namespace pf
@@ -899,6 +1035,12 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
     (void)xopt;
     pf::DeviceGuard dg(ctx->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    ctx->last_stream = st;
+    pf_fmm_stats &stt = ctx->last_stats;
+    memset(&stt, 0, sizeof(stt));
+    stt.n_src = n_src;
+    stt.n_tgt = n_tgt;
+    stt.used_direct = 1;
     if (n_tgt == 0) return PF_OK;
     if (n_src == 0) {
         PF_CUDA_TRY(cudaMemsetAsync(vx, 0, sizeof(double) * n_tgt, st));
@@ -908,13 +1050,10 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
     if (ndirect < 1) ndirect = 1;
     // leaf level: as the reference's level count, ceil(log4(N / Ndirect))
     int L = pf::g_tune.leaf_level;
-    if (L == 0) {
-        L = (int)std::ceil(0.5 * std::log2((double)n_src / (double)ndirect));
-        L = std::min(std::max(L, 0), MAX_LEVEL);
-    }
+    if (L == 0) L = pf::fmmx::auto_level(n_src, ndirect);
     if (tol == 0.0 || L < 3)
         return pf::launch_direct(n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
-    const int np = pf::g_tune.np ? pf::g_tune.np : pf::np_for_tol(tol);
+    const int np = pf::g_tune.np ? pf::g_tune.np : pf::fmmx::np_for_tol(tol);
     int kb = pf::g_tune.kb;
 
     // bounding square of sources and targets
@@ -966,11 +1105,103 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
         --L;  // cutoff too large for this leaf width: coarser leaves
     }
     FmmArgs a{n_src, n_tgt, x, y, g, xt, yt, ksigmasqr, cutoff, tol, ndirect, vx, vy};
-    switch (np) {
-        case 16: return run_fmm<16>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
-        case 20: return run_fmm<20>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
-        case 24: return run_fmm<24>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
-        case 28: return run_fmm<28>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
-        default: return run_fmm<32>(ctx, a, L, kb, xmin, ymin, w0, *cache, st);
-    }
+    stt.used_direct = 0;
+    stt.leaf_level = L;
+    stt.expansion_terms = np;
+    stt.block_level_drop = kb;
+    cache->x0 = xmin;
+    cache->y0 = ymin;
+    cache->w0 = w0;
+    const bool same = (xt == x && yt == y && n_tgt == n_src);
+    PF_TRY(pf::arena_reserve(ctx, fmm_scratch_bytes(*cache, n_src, n_tgt, same)));
+    pf::Bump sc{ctx->arena.base, ctx->arena.cap, 0};
+    return pf::fmm_exec(*cache, sc, a, reinterpret_cast<unsigned long long *>(ctx->dev_small),
+                        ctx->fmm_profile ? ctx->ev : nullptr, st);
 }
+
+extern "C" pf_status pf_fmm_profile(pf_ctx *ctx, int enable) {
+    pf::clear_error();
+    PF_CHECK_ARG(ctx != nullptr, "pf_fmm_profile: NULL context");
+    ctx->fmm_profile = enable != 0;
+    return PF_OK;
+}
+
+extern "C" pf_status pf_fmm_last_stats(pf_ctx *ctx, pf_fmm_stats *out) {
+    pf::clear_error();
+    PF_CHECK_ARG(ctx != nullptr && out != nullptr, "pf_fmm_last_stats: NULL argument");
+    pf::DeviceGuard dg(ctx->device);
+    pf_fmm_stats s = ctx->last_stats;
+    s.ms_sort = s.ms_upward = s.ms_m2l = s.ms_downward = s.ms_p2p = s.ms_l2p = s.ms_total = -1.f;
+    if (!s.used_direct) {
+        PF_CUDA_TRY(cudaStreamSynchronize(ctx->last_stream));
+        unsigned long long c[2];
+        PF_CUDA_TRY(cudaMemcpy(c, ctx->dev_small, sizeof(c), cudaMemcpyDeviceToHost));
+        s.p2p_pairs = (int64_t)c[0];
+        s.m2l_translations = (int64_t)c[1];
+        if (ctx->fmm_profile) {
+            float t[6];
+            for (int k = 0; k < 6; ++k) PF_CUDA_TRY(cudaEventElapsedTime(&t[k], ctx->ev[k], ctx->ev[k + 1]));
+            s.ms_sort = t[0];
+            s.ms_upward = t[1];
+            s.ms_m2l = t[2];
+            s.ms_downward = t[3];
+            s.ms_p2p = t[4];
+            s.ms_l2p = t[5];
+            PF_CUDA_TRY(cudaEventElapsedTime(&s.ms_total, ctx->ev[0], ctx->ev[6]));
+        }
+    }
+    *out = s;
+    return PF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// internal interface (fmm_api.cuh)
+namespace pf {
+namespace fmmx {
+
+struct Plan {
+    FmmCache c;
+};
+
+Plan *plan_new() { return new Plan(); }
+
+void plan_free(Plan *p) {
+    if (!p) return;
+    p->c.release();
+    delete p;
+}
+
+pf_status plan_build(Plan *p, int L, int kb, int np, double x0, double y0, double w0,
+                     double cutoff, bool *p2p_ok) {
+    const double ratio = cutoff / w0;
+    if (p->c.L != L || p->c.kb != kb || p->c.np != np || p->c.ratio != ratio)
+        PF_TRY(build_cache(p->c, L, kb, np, w0, cutoff));
+    p->c.x0 = x0;
+    p->c.y0 = y0;
+    p->c.w0 = w0;
+    *p2p_ok = p->c.nqp <= P2P_QMAX;
+    return PF_OK;
+}
+
+int plan_level(const Plan *p) { return p->c.L; }
+
+size_t plan_scratch(const Plan *p, int64_t ns, int64_t nt, bool same) {
+    return fmm_scratch_bytes(p->c, ns, nt, same);
+}
+
+pf_status plan_exec(const Plan *p, Bump &sc, int64_t ns, const double *x, const double *y,
+                    const double *g, int64_t nt, const double *xt, const double *yt,
+                    double ksigmasqr, double *vx, double *vy, unsigned long long *ctr,
+                    cudaEvent_t *ev, cudaStream_t st) {
+    FmmArgs a{ns, nt, x, y, g, xt, yt, ksigmasqr, 0.0, 0.0, 0, vx, vy};
+    return fmm_exec(p->c, sc, a, ctr, ev, st);
+}
+
+int auto_level(int64_t ns, int ndirect) {
+    if (ndirect < 1) ndirect = 1;
+    int L = (int)std::ceil(0.5 * std::log2((double)ns / (double)ndirect));
+    return std::min(std::max(L, 0), MAX_LEVEL);
+}
+
+}  // namespace fmmx
+}  // namespace pf

@@ -1,0 +1,33 @@
+// fmm_api.cuh -- internal interface of the FMM for other library modules
+// (the batch runtime): plans are built on the host once, executions only
+// enqueue kernels (no synchronisation, capturable in a CUDA graph).
+#pragma once
+#include "pf_common.cuh"
+
+namespace pf {
+namespace fmmx {
+
+struct Plan;  // tables + device operators for one tree geometry
+
+Plan *plan_new();
+void plan_free(Plan *p);
+// Build for leaf level L, P2P block drop kb, p+1 = np terms, root box
+// [x0, x0+w0] x [y0, y0+w0] and Gaussian cutoff.  Allocates and uploads
+// (not capturable).  *p2p_ok = false when the cutoff makes P2P blocks too
+// large for this L (use a coarser L).
+pf_status plan_build(Plan *p, int L, int kb, int np, double x0, double y0, double w0,
+                     double cutoff, bool *p2p_ok);
+int plan_level(const Plan *p);
+size_t plan_scratch(const Plan *p, int64_t ns, int64_t nt, bool same);
+pf_status plan_exec(const Plan *p, Bump &sc, int64_t ns, const double *x, const double *y,
+                    const double *g, int64_t nt, const double *xt, const double *yt,
+                    double ksigmasqr, double *vx, double *vy, unsigned long long *ctr,
+                    cudaEvent_t *ev, cudaStream_t st);
+// leaf level from the blob count, as the reference's level count
+int auto_level(int64_t ns, int ndirect);
+// expansion terms for a tolerance
+int np_for_tol(double tol);
+constexpr int MAX_LEVEL = 11;
+
+}  // namespace fmmx
+}  // namespace pf

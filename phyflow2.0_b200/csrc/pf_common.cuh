@@ -69,9 +69,29 @@ struct pf_ctx {
     // FMM plan cache (tables and operators on the device), owned by fmm.cu
     void *fmm_cache = nullptr;
     void (*fmm_cache_free)(void *) = nullptr;
+    // small persistent device buffer (FMM counters) and profiling events
+    int64_t *dev_small = nullptr;
+    bool fmm_profile = false;
+    cudaEvent_t ev[8] = {};
+    cudaStream_t last_stream = nullptr;
+    pf_fmm_stats last_stats = {};
 };
 
 namespace pf {
+
+// Bump allocator over a device buffer (scratch of one call or one batch slot).
+struct Bump {
+    char *base = nullptr;
+    size_t cap = 0;
+    size_t used = 0;
+    void *take(size_t bytes) {
+        const size_t b = (bytes + 255) & ~size_t(255);
+        if (used + b > cap) return nullptr;
+        void *p = base + used;
+        used += b;
+        return p;
+    }
+};
 
 // Make sure the arena holds at least `bytes`; may cudaFree/cudaMalloc, which
 // synchronises the device.  Done before any kernel of a call is enqueued.

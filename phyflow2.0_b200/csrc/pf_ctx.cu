@@ -99,11 +99,18 @@ pf_status pf_create(int device, pf_ctx **out) {
     c->num_sms = prop.multiProcessorCount;
     c->smem_optin = prop.sharedMemPerBlockOptin;
     e = cudaMallocHost(&c->host_small, 4096);
+    if (e == cudaSuccess) e = cudaMalloc(&c->dev_small, 4096);
+    for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaEventCreate(&c->ev[k]);
     if (e != cudaSuccess) {
+        if (c->host_small) cudaFreeHost(c->host_small);
+        if (c->dev_small) cudaFree(c->dev_small);
+        for (int k = 0; k < 8; ++k)
+            if (c->ev[k]) cudaEventDestroy(c->ev[k]);
         delete c;
-        pf::set_error("cudaMallocHost failed: %s", cudaGetErrorString(e));
+        pf::set_error("context allocation failed: %s", cudaGetErrorString(e));
         return PF_ERR_CUDA;
     }
+    cudaMemset(c->dev_small, 0, 4096);
     *out = c;
     return PF_OK;
 }
@@ -116,6 +123,9 @@ pf_status pf_destroy(pf_ctx *ctx) {
     if (ctx->fmm_cache && ctx->fmm_cache_free) ctx->fmm_cache_free(ctx->fmm_cache);
     if (ctx->arena.base) cudaFree(ctx->arena.base);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
+    if (ctx->dev_small) cudaFree(ctx->dev_small);
+    for (int k = 0; k < 8; ++k)
+        if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     delete ctx;
     return PF_OK;
 }

@@ -2,26 +2,26 @@
 //
 // Pipeline (all FP64 values, integer cell work bit-exact):
 //   1. k_rm_extent : window-left lattice index of every blob,
-//        xl = ceil(((x - xb0) - 2h) + 0.5h) / h) - 1     (_regridding.py:157-158)
+//        xl = ceil((((x - xb0) - 2h) + 0.5h) / h) - 1     (_regridding.py:157-158)
 //      with the same operation order as numpy (IEEE, no FMA contraction:
-//      2h and 0.5h are formed on the host); min/max over blobs -> extent.
-//   [host reads the extent: one stream sync]
-//   2. k_rm_count  : counting sort of blobs by base cell (xl, yl), base
-//      cells in ix-major order; rank of a blob in its cell from atomicAdd.
+//      2h and 0.5h are formed on the host); min/max over blobs -> window.
+//      [pf_remesh reads the window back: one stream sync.  pf_remesh_window
+//       takes the window from the caller instead and never synchronises.]
+//   2. k_rm_count  : counting sort of blobs by base cell (xl, yl), base cells
+//      ix-major; rank of a blob in its cell from atomicAdd.
 //   3. scan of the per-cell counts -> cell starts.
 //   4. k_rm_place  : blob index -> its slot.
-//   5. k_rm_order  : per base cell, order its blobs by input index (so every
-//      sum below has a fixed order, independent of atomic timing) and write
-//      the blob data in that order (x/h, y/h, g): a cell-sorted copy.
-//   6. k_rm_gather : one thread per output cell (ix, iy); it sums, in fixed
-//      order, the M4'(ux) M4'(uy) g contributions of the blobs of the 16 base
-//      cells whose windows cover it (_regridding.py:183-184, weights of
-//      _interpolation_kernels_1d.cpp:75-89), and flags cells touched by at
-//      least one window (explicit zeros are kept, like the CSR sum of the
-//      reference, _regridding.py:200-202).
+//   5. k_rm_order  : per base cell, order its blobs by input index (every sum
+//      below then has a fixed order, independent of atomic timing) and write,
+//      in that order, each blob's four x weights M4'(ux_a), four y weights
+//      M4'(uy_b) (_interpolation_kernels_1d.cpp:75-89; u as _regridding.py:183)
+//      and g.
+//   6. k_rm_gather : one thread per output cell (ix, iy) sums, in fixed order,
+//      (wx_a wy_b) g over the blobs of the 16 base cells whose windows cover it,
+//      and flags cells touched by at least one window (explicit zeros are
+//      kept, like the CSR sum of the reference, _regridding.py:200-202).
 //   7. scan of the flags -> output slots, in (ix, iy) order.
 //   8. k_rm_emit   : x = ix*h + 0.5h + xb0 (same order as :217-218), g, ix, iy.
-//   [host reads the count: second stream sync]
 // No floating-point atomics: each output value is produced by one thread.
 #include <cmath>
 #include <cstring>
@@ -31,22 +31,21 @@
 namespace {
 
 constexpr int RM_THREADS = 256;
+constexpr int64_t IDX_LIMIT = (int64_t)1 << 30;
 
 struct Extent {
     int32_t ixmin, ixmax, iymin, iymax;
-    int32_t bad;  // 1: NaN/Inf coordinate, 2: index outside +-2^30
+    int32_t bad;  // 1: NaN/Inf coordinate, 2: index outside +-2^30, 4: outside window
     int32_t pad[3];
 };
 
 __device__ __forceinline__ int64_t left_index(double x, double b0, double h2, double h05,
                                               double h) {
     // ((x - b0) - 2h) + 0.5h, then / h, ceil, -1 ; each op rounded separately
-    double t = __dadd_rn(__dsub_rn(__dsub_rn(x, b0), h2), h05);
-    double q = __ddiv_rn(t, h);
+    const double t = __dadd_rn(__dsub_rn(__dsub_rn(x, b0), h2), h05);
+    const double q = __ddiv_rn(t, h);
     return (int64_t)ceil(q) - 1;
 }
-
-__device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
 
 __global__ void k_rm_extent_init(Extent *e) {
     e->ixmin = INT32_MAX;
@@ -65,16 +64,15 @@ __device__ __forceinline__ int warp_max(int v) {
     return v;
 }
 
-constexpr int64_t IDX_LIMIT = (int64_t)1 << 30;
-
 __global__ void __launch_bounds__(RM_THREADS)
 k_rm_extent(const double *__restrict__ x, const double *__restrict__ y, int64_t n, double xb0,
             double yb0, double h2, double h05, double h, Extent *e) {
+    __shared__ int s_v[5][RM_THREADS / 32];
     int mnx = INT32_MAX, mxx = INT32_MIN, mny = INT32_MAX, mxy = INT32_MIN, bad = 0;
     for (int64_t i = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * RM_THREADS) {
         const double xi = x[i], yi = y[i];
-        if (!finite_d(xi) || !finite_d(yi)) {
+        if (!isfinite(xi) || !isfinite(yi)) {
             bad |= 1;
             continue;
         }
@@ -94,26 +92,53 @@ k_rm_extent(const double *__restrict__ x, const double *__restrict__ y, int64_t 
     mny = warp_min(mny);
     mxy = warp_max(mxy);
     bad = __reduce_or_sync(0xffffffffu, bad);
-    if ((threadIdx.x & 31) == 0) {
-        if (mnx != INT32_MAX) {
-            atomicMin(&e->ixmin, mnx);
-            atomicMax(&e->ixmax, mxx);
-            atomicMin(&e->iymin, mny);
-            atomicMax(&e->iymax, mxy);
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s_v[0][wid] = mnx;
+        s_v[1][wid] = mxx;
+        s_v[2][wid] = mny;
+        s_v[3][wid] = mxy;
+        s_v[4][wid] = bad;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const bool in = lane < RM_THREADS / 32;
+        mnx = warp_min(in ? s_v[0][lane] : INT32_MAX);
+        mxx = warp_max(in ? s_v[1][lane] : INT32_MIN);
+        mny = warp_min(in ? s_v[2][lane] : INT32_MAX);
+        mxy = warp_max(in ? s_v[3][lane] : INT32_MIN);
+        bad = __reduce_or_sync(0xffffffffu, in ? s_v[4][lane] : 0);
+        if (lane == 0) {
+            if (mnx != INT32_MAX) {
+                atomicMin(&e->ixmin, mnx);
+                atomicMax(&e->ixmax, mxx);
+                atomicMin(&e->iymin, mny);
+                atomicMax(&e->iymax, mxy);
+            }
+            if (bad) atomicOr(&e->bad, bad);
         }
-        if (bad) atomicOr(&e->bad, bad);
     }
 }
 
 // base cell grid: bx in [0, nbx), by in [0, nby), id = bx*nby + by
 __global__ void __launch_bounds__(RM_THREADS)
 k_rm_count(const double *__restrict__ x, const double *__restrict__ y, int64_t n, double xb0,
-           double yb0, double h2, double h05, double h, int32_t ixmin, int32_t iymin, int64_t nby,
-           int32_t *__restrict__ cell, int32_t *__restrict__ rank, int32_t *__restrict__ count) {
+           double yb0, double h2, double h05, double h, int32_t ixmin, int32_t iymin, int64_t nbx,
+           int64_t nby, int32_t *__restrict__ cell, int32_t *__restrict__ rank,
+           int32_t *__restrict__ count, int32_t *__restrict__ bad) {
     const int64_t i = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     if (i >= n) return;
-    const int64_t a = left_index(x[i], xb0, h2, h05, h) - ixmin;
-    const int64_t b = left_index(y[i], yb0, h2, h05, h) - iymin;
+    const double xi = x[i], yi = y[i];
+    int64_t a = -1, b = -1;
+    if (isfinite(xi) && isfinite(yi)) {
+        a = left_index(xi, xb0, h2, h05, h) - ixmin;
+        b = left_index(yi, yb0, h2, h05, h) - iymin;
+    }
+    if (a < 0 || b < 0 || a >= nbx || b >= nby) {  // outside the window: skipped, reported
+        cell[i] = -1;
+        atomicOr(bad, 4);
+        return;
+    }
     const int32_t c = (int32_t)(a * nby + b);
     cell[i] = c;
     rank[i] = atomicAdd(&count[c], 1);
@@ -124,35 +149,9 @@ k_rm_place(int64_t n, const int32_t *__restrict__ cell, const int32_t *__restric
            const int32_t *__restrict__ start, int32_t *__restrict__ perm) {
     const int64_t i = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     if (i >= n) return;
-    perm[start[cell[i]] + rank[i]] = (int32_t)i;
-}
-
-__global__ void __launch_bounds__(RM_THREADS)
-k_rm_order(int64_t ncell, const int32_t *__restrict__ start, const int32_t *__restrict__ count,
-           int32_t *__restrict__ perm, const double *__restrict__ x, const double *__restrict__ y,
-           const double *__restrict__ g, double h, double *__restrict__ sxh,
-           double *__restrict__ syh, double *__restrict__ sg) {
-    const int64_t c = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
-    if (c >= ncell) return;
-    const int cnt = count[c];
-    if (cnt == 0) return;
-    const int s0 = start[c];
-    // insertion sort of the cell's blob indices (cells hold a few blobs)
-    for (int k = 1; k < cnt; ++k) {
-        const int32_t v = perm[s0 + k];
-        int j = k - 1;
-        while (j >= 0 && perm[s0 + j] > v) {
-            perm[s0 + j + 1] = perm[s0 + j];
-            --j;
-        }
-        perm[s0 + j + 1] = v;
-    }
-    for (int k = 0; k < cnt; ++k) {
-        const int32_t i = perm[s0 + k];
-        sxh[s0 + k] = __ddiv_rn(x[i], h);
-        syh[s0 + k] = __ddiv_rn(y[i], h);
-        sg[s0 + k] = g[i];
-    }
+    const int32_t c = cell[i];
+    if (c < 0) return;
+    perm[start[c] + rank[i]] = (int32_t)i;
 }
 
 // M4' weight with the Wee term: branch structure of
@@ -171,29 +170,70 @@ __device__ __forceinline__ double m4p(double u, double c2) {
     return 0.0;
 }
 
+struct W9 {
+    double wx[4], wy[4], g;
+};
+
+__global__ void __launch_bounds__(RM_THREADS)
+k_rm_order(int64_t ncell, int64_t nby, int32_t ixmin, int32_t iymin,
+           const int32_t *__restrict__ start, const int32_t *__restrict__ count,
+           int32_t *__restrict__ perm, const double *__restrict__ x, const double *__restrict__ y,
+           const double *__restrict__ g, double h, double qx0, double qy0, double c2,
+           W9 *__restrict__ w) {
+    const int64_t c = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
+    if (c >= ncell) return;
+    const int cnt = count[c];
+    if (cnt == 0) return;
+    const int s0 = start[c];
+    // insertion sort of the cell's blob indices (cells hold a few blobs)
+    for (int k = 1; k < cnt; ++k) {
+        const int32_t v = perm[s0 + k];
+        int j = k - 1;
+        while (j >= 0 && perm[s0 + j] > v) {
+            perm[s0 + j + 1] = perm[s0 + j];
+            --j;
+        }
+        perm[s0 + j + 1] = v;
+    }
+    const int64_t bx = c / nby, by = c - bx * nby;
+    // numpy order: ((ix + 0.5) + xb0/h) - x/h, ix the absolute lattice index
+    double px[4], py[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        px[a] = ((double)(ixmin + bx + a) + 0.5) + qx0;
+        py[a] = ((double)(iymin + by + a) + 0.5) + qy0;
+    }
+    for (int k = 0; k < cnt; ++k) {
+        const int32_t i = perm[s0 + k];
+        const double xh = __ddiv_rn(x[i], h), yh = __ddiv_rn(y[i], h);
+        W9 r;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            r.wx[a] = m4p(__dsub_rn(px[a], xh), c2);
+            r.wy[a] = m4p(__dsub_rn(py[a], yh), c2);
+        }
+        r.g = g[i];
+        w[s0 + k] = r;
+    }
+}
+
 // Output cell grid: ox in [0, nbx+3), oy in [0, nby+3); lattice index
 // ix = ixmin + ox.  A base cell (bx, by) covers ox in bx..bx+3, oy in by..by+3.
 __global__ void __launch_bounds__(RM_THREADS)
-k_rm_gather(int64_t nbx, int64_t nby, int32_t ixmin, int32_t iymin, double qx0, double qy0,
-            double c2, const int32_t *__restrict__ start, const int32_t *__restrict__ count,
-            const double *__restrict__ sxh, const double *__restrict__ syh,
-            const double *__restrict__ sg, double *__restrict__ acc, int32_t *__restrict__ flag) {
+k_rm_gather(int64_t nbx, int64_t nby, const int32_t *__restrict__ start,
+            const int32_t *__restrict__ count, const W9 *__restrict__ w,
+            double *__restrict__ acc, int32_t *__restrict__ flag) {
     const int64_t noy = nby + 3;
     const int64_t cid = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     if (cid >= (nbx + 3) * noy) return;
     const int64_t ox = cid / noy, oy = cid - ox * noy;
-    // numpy: (ix + 0.5) + xb0/h - x/h  with ix the absolute lattice index
-    const double px = ((double)(ixmin + ox) + 0.5) + qx0;
-    const double py = ((double)(iymin + oy) + 0.5) + qy0;
     double sum = 0.0;
     int touched = 0;
-    // window offsets: x offset a = ox - bx fastest in the reference numbering,
-    // but each output cell sums over (a, b) in a fixed order of its own
-#pragma unroll 1
+#pragma unroll
     for (int b = 0; b < 4; ++b) {
         const int64_t by = oy - b;
         if (by < 0 || by >= nby) continue;
-#pragma unroll 1
+#pragma unroll
         for (int a = 0; a < 4; ++a) {
             const int64_t bx = ox - a;
             if (bx < 0 || bx >= nbx) continue;
@@ -203,9 +243,8 @@ k_rm_gather(int64_t nbx, int64_t nby, int32_t ixmin, int32_t iymin, double qx0, 
             touched = 1;
             const int s0 = start[bc];
             for (int k = 0; k < cnt; ++k) {
-                const double wx = m4p(__dsub_rn(px, sxh[s0 + k]), c2);
-                const double wy = m4p(__dsub_rn(py, syh[s0 + k]), c2);
-                sum += (wx * wy) * sg[s0 + k];
+                const W9 &r = w[s0 + k];
+                sum += (r.wx[a] * r.wy[b]) * r.g;
             }
         }
     }
@@ -235,17 +274,75 @@ k_rm_emit(int64_t ncell, int64_t noy, int32_t ixmin, int32_t iymin, double h, do
     if (iyo) iyo[p] = iy;
 }
 
+__global__ void k_rm_finish(const int32_t *__restrict__ total, const int32_t *__restrict__ bad,
+                            int64_t *__restrict__ n_out_dev, int32_t *__restrict__ status_dev) {
+    if (n_out_dev) *n_out_dev = *total;
+    if (status_dev) *status_dev = *bad;
+}
+
 }  // namespace
 
 namespace pf {
 
-// Dense-window limit: base cells <= max(2^26, 64 n).  Beyond it the blob set
-// is too sparse for a dense lattice window and the call is rejected.
+// Dense-window limit: base cells <= max(2^26, 64 n).
 static int64_t dense_cell_limit(int64_t n) {
-    int64_t a = (int64_t)1 << 26;
-    int64_t b = 64 * n;
-    int64_t lim = a > b ? a : b;
+    const int64_t a = (int64_t)1 << 26, b = 64 * n;
+    const int64_t lim = a > b ? a : b;
     return lim < ((int64_t)1 << 30) ? lim : ((int64_t)1 << 30);
+}
+
+size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby) {
+    const int64_t nbase = nbx * nby, ncell = (nbx + 3) * (nby + 3);
+    const int64_t big = ncell > nbase ? ncell : nbase;
+    return align256(4 * n) * 3 + align256(sizeof(W9) * n) + 2 * align256(4 * nbase) +
+           align256(8 * ncell) + 2 * align256(4 * ncell) + align256(4 * scan_tmp_ints(big)) +
+           2 * align256(16) + 1024;
+}
+
+// Everything after the window is known; no host synchronisation.  total_dev
+// receives the output count, bad_dev the flags of k_rm_count (4 = a blob
+// outside the window, skipped).
+pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, const double *g,
+                      double h, double xb0, double yb0, double c, int32_t ixmin, int32_t iymin,
+                      int64_t nbx, int64_t nby, int64_t capacity, double *xo, double *yo,
+                      double *go, int64_t *ixo, int64_t *iyo, int32_t *total, int32_t *bad,
+                      cudaStream_t st) {
+    const int64_t nbase = nbx * nby, ncell = (nbx + 3) * (nby + 3);
+    const int64_t big = ncell > nbase ? ncell : nbase;
+    int32_t *cell = (int32_t *)sc.take(4 * n);
+    int32_t *rank = (int32_t *)sc.take(4 * n);
+    int32_t *perm = (int32_t *)sc.take(4 * n);
+    W9 *w = (W9 *)sc.take(sizeof(W9) * n);
+    int32_t *count = (int32_t *)sc.take(4 * nbase);
+    int32_t *start = (int32_t *)sc.take(4 * nbase);
+    double *acc = (double *)sc.take(8 * ncell);
+    int32_t *flag = (int32_t *)sc.take(4 * ncell);
+    int32_t *slot = (int32_t *)sc.take(4 * ncell);
+    int32_t *tmp = (int32_t *)sc.take(4 * scan_tmp_ints(big));
+    if (!tmp) {
+        set_error("remesh: scratch too small");
+        return PF_ERR_OOM;
+    }
+    const double h2 = 2.0 * h, h05 = 0.5 * h;
+    const unsigned gn = (unsigned)ceil_div(n, RM_THREADS);
+    PF_CUDA_TRY(cudaMemsetAsync(count, 0, 4 * nbase, st));
+    k_rm_count<<<gn, RM_THREADS, 0, st>>>(x, y, n, xb0, yb0, h2, h05, h, ixmin, iymin, nbx, nby,
+                                          cell, rank, count, bad);
+    PF_TRY(launch_status("k_rm_count"));
+    PF_TRY(exclusive_scan_i32(count, start, nbase, tmp, nullptr, st));
+    k_rm_place<<<gn, RM_THREADS, 0, st>>>(n, cell, rank, start, perm);
+    PF_TRY(launch_status("k_rm_place"));
+    k_rm_order<<<(unsigned)ceil_div(nbase, RM_THREADS), RM_THREADS, 0, st>>>(
+        nbase, nby, ixmin, iymin, start, count, perm, x, y, g, h, xb0 / h, yb0 / h, c * c, w);
+    PF_TRY(launch_status("k_rm_order"));
+    k_rm_gather<<<(unsigned)ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(nbx, nby, start,
+                                                                             count, w, acc, flag);
+    PF_TRY(launch_status("k_rm_gather"));
+    PF_TRY(exclusive_scan_i32(flag, slot, ncell, tmp, total, st));
+    k_rm_emit<<<(unsigned)ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(
+        ncell, nby + 3, ixmin, iymin, h, h05, xb0, yb0, flag, slot, acc, total, capacity, xo, yo,
+        go, ixo, iyo);
+    return launch_status("k_rm_emit");
 }
 
 }  // namespace pf
@@ -271,14 +368,13 @@ extern "C" pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const do
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     const double h2 = 2.0 * h, h05 = 0.5 * h;
-    // scratch phase 1: the extent record
     PF_TRY(pf::arena_reserve(ctx, 4096));
     Extent *ext = static_cast<Extent *>(pf::arena_take(ctx, sizeof(Extent)));
     k_rm_extent_init<<<1, 1, 0, st>>>(ext);
     PF_TRY(pf::launch_status("k_rm_extent_init"));
     {
         int64_t grid = pf::ceil_div(n, RM_THREADS);
-        int64_t cap = (int64_t)ctx->num_sms * 8;
+        const int64_t cap = (int64_t)ctx->num_sms * 4;
         if (grid > cap) grid = cap;
         k_rm_extent<<<(unsigned)grid, RM_THREADS, 0, st>>>(x, y, n, xb0, yb0, h2, h05, h, ext);
         PF_TRY(pf::launch_status("k_rm_extent"));
@@ -297,63 +393,18 @@ extern "C" pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const do
     }
     const int64_t nbx = (int64_t)he.ixmax - he.ixmin + 1;
     const int64_t nby = (int64_t)he.iymax - he.iymin + 1;
-    const int64_t nbase = nbx * nby;
-    const int64_t ncell = (nbx + 3) * (nby + 3);
-    if (nbase > pf::dense_cell_limit(n) || ncell >= ((int64_t)1 << 31)) {
+    if (nbx * nby > pf::dense_cell_limit(n) || (nbx + 3) * (nby + 3) >= ((int64_t)1 << 31)) {
         pf::set_error("pf_remesh: lattice window %lld x %lld is too large for %lld blobs",
                       (long long)nbx, (long long)nby, (long long)n);
         return PF_ERR_INVALID_ARG;
     }
-
-    // scratch phase 2
-    const size_t need = pf::align256(sizeof(Extent)) + 2 * pf::align256(4 * n) /* cell, rank */ +
-                        pf::align256(4 * n) /* perm */ + 3 * pf::align256(8 * n) /* sorted */ +
-                        2 * pf::align256(4 * nbase) /* count, start */ +
-                        pf::align256(8 * ncell) /* acc */ + 2 * pf::align256(4 * ncell) /* flag, slot */ +
-                        pf::align256(4 * pf::scan_tmp_ints(ncell > nbase ? ncell : nbase)) +
-                        pf::align256(16) + 4096;
-    PF_TRY(pf::arena_reserve(ctx, need));
-    (void)pf::arena_take(ctx, sizeof(Extent));
-    int32_t *cell = static_cast<int32_t *>(pf::arena_take(ctx, 4 * n));
-    int32_t *rank = static_cast<int32_t *>(pf::arena_take(ctx, 4 * n));
-    int32_t *perm = static_cast<int32_t *>(pf::arena_take(ctx, 4 * n));
-    double *sxh = static_cast<double *>(pf::arena_take(ctx, 8 * n));
-    double *syh = static_cast<double *>(pf::arena_take(ctx, 8 * n));
-    double *sg = static_cast<double *>(pf::arena_take(ctx, 8 * n));
-    int32_t *count = static_cast<int32_t *>(pf::arena_take(ctx, 4 * nbase));
-    int32_t *start = static_cast<int32_t *>(pf::arena_take(ctx, 4 * nbase));
-    double *acc = static_cast<double *>(pf::arena_take(ctx, 8 * ncell));
-    int32_t *flag = static_cast<int32_t *>(pf::arena_take(ctx, 4 * ncell));
-    int32_t *slot = static_cast<int32_t *>(pf::arena_take(ctx, 4 * ncell));
-    int32_t *tmp = static_cast<int32_t *>(
-        pf::arena_take(ctx, 4 * pf::scan_tmp_ints(ncell > nbase ? ncell : nbase)));
-    int32_t *total = static_cast<int32_t *>(pf::arena_take(ctx, 16));
-    if (!total) {
-        pf::set_error("pf_remesh: internal scratch layout error");
-        return PF_ERR_OOM;
-    }
-
-    const unsigned gn = (unsigned)pf::ceil_div(n, RM_THREADS);
-    PF_CUDA_TRY(cudaMemsetAsync(count, 0, 4 * nbase, st));
-    k_rm_count<<<gn, RM_THREADS, 0, st>>>(x, y, n, xb0, yb0, h2, h05, h, he.ixmin, he.iymin, nby,
-                                          cell, rank, count);
-    PF_TRY(pf::launch_status("k_rm_count"));
-    PF_TRY(pf::exclusive_scan_i32(count, start, nbase, tmp, nullptr, st));
-    k_rm_place<<<gn, RM_THREADS, 0, st>>>(n, cell, rank, start, perm);
-    PF_TRY(pf::launch_status("k_rm_place"));
-    k_rm_order<<<(unsigned)pf::ceil_div(nbase, RM_THREADS), RM_THREADS, 0, st>>>(
-        nbase, start, count, perm, x, y, g, h, sxh, syh, sg);
-    PF_TRY(pf::launch_status("k_rm_order"));
-    const double qx0 = xb0 / h, qy0 = yb0 / h;
-    const double c2 = c * c;
-    k_rm_gather<<<(unsigned)pf::ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(
-        nbx, nby, he.ixmin, he.iymin, qx0, qy0, c2, start, count, sxh, syh, sg, acc, flag);
-    PF_TRY(pf::launch_status("k_rm_gather"));
-    PF_TRY(pf::exclusive_scan_i32(flag, slot, ncell, tmp, total, st));
-    k_rm_emit<<<(unsigned)pf::ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(
-        ncell, nby + 3, he.ixmin, he.iymin, h, h05, xb0, yb0, flag, slot, acc, total, capacity,
-        x_out, y_out, g_out, ix_out, iy_out);
-    PF_TRY(pf::launch_status("k_rm_emit"));
+    PF_TRY(pf::arena_reserve(ctx, pf::remesh_scratch_bytes(n, nbx, nby)));
+    pf::Bump sc{ctx->arena.base, ctx->arena.cap, 0};
+    int32_t *total = (int32_t *)sc.take(16);
+    int32_t *bad = (int32_t *)sc.take(16);
+    PF_CUDA_TRY(cudaMemsetAsync(bad, 0, 4, st));
+    PF_TRY(pf::remesh_core(sc, n, x, y, g, h, xb0, yb0, c, he.ixmin, he.iymin, nbx, nby, capacity,
+                           x_out, y_out, g_out, ix_out, iy_out, total, bad, st));
     PF_CUDA_TRY(cudaMemcpyAsync(ctx->host_small, total, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     PF_CUDA_TRY(cudaStreamSynchronize(st));
     const int64_t nout = *reinterpret_cast<int32_t *>(ctx->host_small);
@@ -364,4 +415,38 @@ extern "C" pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const do
         return PF_ERR_CAPACITY;
     }
     return PF_OK;
+}
+
+extern "C" pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                                      const double *g, double h, double xb0, double yb0, double c,
+                                      int64_t ixmin, int64_t iymin, int64_t nbx, int64_t nby,
+                                      int64_t capacity, double *x_out, double *y_out,
+                                      double *g_out, int64_t *ix_out, int64_t *iy_out,
+                                      int64_t *n_out_dev, int32_t *status_dev, void *stream) {
+    pf::clear_error();
+    PF_CHECK_ARG(ctx != nullptr, "pf_remesh_window: NULL context");
+    PF_CHECK_ARG(n >= 0 && n < ((int64_t)1 << 31), "pf_remesh_window: bad n");
+    PF_CHECK_ARG(std::isfinite(h) && h > 0.0, "pf_remesh_window: bad h");
+    PF_CHECK_ARG(nbx > 0 && nby > 0 && (nbx + 3) * (nby + 3) < ((int64_t)1 << 31),
+                 "pf_remesh_window: bad window %lld x %lld", (long long)nbx, (long long)nby);
+    PF_CHECK_ARG(ixmin > -((int64_t)1 << 30) && iymin > -((int64_t)1 << 30) &&
+                     ixmin + nbx < ((int64_t)1 << 30) && iymin + nby < ((int64_t)1 << 30),
+                 "pf_remesh_window: window outside +-2^30");
+    PF_CHECK_ARG(n == 0 || (x && y && g), "pf_remesh_window: NULL input array");
+    PF_CHECK_ARG(capacity >= 0 && (capacity == 0 || (x_out && y_out && g_out)),
+                 "pf_remesh_window: bad output arrays");
+    PF_CHECK_ARG(n_out_dev != nullptr, "pf_remesh_window: n_out_dev is NULL");
+    pf::DeviceGuard dg(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    PF_TRY(pf::arena_reserve(ctx, pf::remesh_scratch_bytes(n, nbx, nby)));
+    pf::Bump sc{ctx->arena.base, ctx->arena.cap, 0};
+    int32_t *total = (int32_t *)sc.take(16);
+    int32_t *bad = (int32_t *)sc.take(16);
+    PF_CUDA_TRY(cudaMemsetAsync(total, 0, 4, st));
+    PF_CUDA_TRY(cudaMemsetAsync(bad, 0, 4, st));
+    if (n > 0)
+        PF_TRY(pf::remesh_core(sc, n, x, y, g, h, xb0, yb0, c, (int32_t)ixmin, (int32_t)iymin, nbx,
+                               nby, capacity, x_out, y_out, g_out, ix_out, iy_out, total, bad, st));
+    k_rm_finish<<<1, 1, 0, st>>>(total, bad, n_out_dev, status_dev);
+    return pf::launch_status("k_rm_finish");
 }

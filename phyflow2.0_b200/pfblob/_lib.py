@@ -45,8 +45,17 @@ PROTOTYPES = {
     "pf_remesh": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp, _vp, _vp,
                   _c.POINTER(_i64), _vp],
     "pf_moments": [_vp, _i64, _vp, _vp, _vp, _vp, _vp],
+    "pf_remesh_window": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _i64, _i64,
+                         _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "pf_fmm_lists": [_int, _int, _dbl, _dbl, _dbl, _vp, _i64, _c.POINTER(_i64)],
     "pf_fmm_set_tuning": [_int, _int, _int],
+    "pf_batch_create": [_vp, _c.c_int32, _vp, _dbl, _c.c_int32, _c.POINTER(_vp)],
+    "pf_batch_run": [_vp, _vp],
+    "pf_batch_results": [_vp, _vp, _vp],
+    "pf_batch_info": [_vp, _vp, _vp, _vp],
+    "pf_batch_destroy": [_vp],
+    "pf_fmm_profile": [_vp, _int],
+    "pf_fmm_last_stats": [_vp, _vp],
     "pf_fmm_tree_keys": [_vp, _i64, _vp, _vp, _dbl, _dbl, _dbl, _int, _vp, _vp],
 }
 
@@ -112,3 +121,41 @@ def version():
 def kernel_launches():
     """Process-wide number of library kernel launches so far."""
     return int(lib.pf_kernel_launches())
+
+
+class FmmStats(_c.Structure):
+    """Mirror of pf_fmm_stats (include/pfblob.h)."""
+    _fields_ = [("leaf_level", _c.c_int32), ("expansion_terms", _c.c_int32),
+                ("block_level_drop", _c.c_int32), ("used_direct", _c.c_int32),
+                ("n_src", _c.c_int64), ("n_tgt", _c.c_int64), ("p2p_pairs", _c.c_int64),
+                ("m2l_translations", _c.c_int64), ("ms_sort", _c.c_float),
+                ("ms_upward", _c.c_float), ("ms_m2l", _c.c_float), ("ms_downward", _c.c_float),
+                ("ms_p2p", _c.c_float), ("ms_l2p", _c.c_float), ("ms_total", _c.c_float),
+                ("reserved", _c.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+def fmm_profile(enable, device=0):
+    check(lib.pf_fmm_profile(context(device), int(bool(enable))))
+
+
+def fmm_last_stats(device=0):
+    s = FmmStats()
+    check(lib.pf_fmm_last_stats(context(device), _c.byref(s)))
+    return s.as_dict()
+
+
+def fmm_set_tuning(leaf_level=0, expansion_terms=0, block_level_drop=1):
+    check(lib.pf_fmm_set_tuning(int(leaf_level), int(expansion_terms), int(block_level_drop)))
+
+
+class BatchInstance(_c.Structure):
+    """Mirror of pf_batch_instance (include/pfblob.h)."""
+    _fields_ = [("n", _c.c_int64), ("x", _vp), ("y", _vp), ("g", _vp), ("vx", _vp), ("vy", _vp),
+                ("ksigmasqr", _c.c_double), ("cutoff", _c.c_double), ("box", _c.c_double * 4),
+                ("method", _c.c_int32), ("leaf_level", _c.c_int32),
+                ("expansion_terms", _c.c_int32), ("remesh", _c.c_int32), ("h", _c.c_double),
+                ("xb0", _c.c_double), ("yb0", _c.c_double), ("c", _c.c_double),
+                ("capacity", _c.c_int64), ("x_out", _vp), ("y_out", _vp), ("g_out", _vp)]

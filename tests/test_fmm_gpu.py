@@ -132,3 +132,17 @@ def test_nan_input_rejected():
     with pytest.raises(pfblob._lib.PfError) as ei:
         fmm(x, x, x, 0.01)
     assert ei.value.status == 5
+
+
+def test_point_vortex_limit_theta_bound():
+    """sigma far below the leaf width: every separation is set by theta alone,
+    so the multipole truncation (not the near field) bounds the error."""
+    rng = np.random.default_rng(10)
+    n = 200000
+    x, y = rng.random(n), rng.random(n)
+    g = rng.standard_normal(n) / n
+    sigma = 1e-5
+    vx, vy = fmm(x, y, g, sigma)
+    idx = rng.choice(n, 3000, replace=False)
+    rx, ry = oracle.velocity_direct(x, y, g, 2 * sigma * sigma, x[idx], y[idx])
+    assert normwise_err(vx[idx], vy[idx], rx, ry) <= TOL

@@ -215,6 +215,32 @@ pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, const double
                            int32_t *status_dev, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * pf_remesh_window without any device allocation, for callers that cannot
+ * allocate: a process whose device memory is already committed to another
+ * allocator (e.g. a serving loop that gives all free HBM to its own pool), or
+ * a latency-critical thread that must not trigger the device-wide
+ * synchronisation cudaMalloc/cudaFree can cause.  No counterpart in the
+ * reference (its Regrid allocates new arrays on every call).
+ *
+ * Scratch is one fixed buffer of PF_NOALLOC_SCRATCH_BYTES per GPU, held from
+ * library load to process exit; no pf_ctx is needed and none is created.  The
+ * call works on the current device; its first call on a device looks up the
+ * buffer's device address (make that first call before any stream capture).
+ * Blob sets needing more scratch than the buffer holds (about 84 bytes per
+ * blob plus 24 bytes per window cell) are rejected with PF_ERR_INVALID_ARG.
+ * Every call shares the buffer: calls that overlap on the GPU (different
+ * streams, or different host threads) race and must be serialised by the
+ * caller.  Arguments and results as pf_remesh_window.
+ * ------------------------------------------------------------------------- */
+#define PF_NOALLOC_SCRATCH_BYTES (32u << 20)
+pf_status pf_remesh_window_noalloc(int64_t n, const double *x, const double *y, const double *g,
+                                   double h, double xb0, double yb0, double c, int64_t ixmin,
+                                   int64_t iymin, int64_t nbx, int64_t nby, int64_t capacity,
+                                   double *x_out, double *y_out, double *g_out, int64_t *ix_out,
+                                   int64_t *iy_out, int64_t *n_out_dev, int32_t *status_dev,
+                                   void *stream);
+
+/* ---------------------------------------------------------------------------
  * FP64 moments of a blob set, written to the DEVICE array out4:
  * out4 = {sum g, sum g x, sum g y, sum |g|}, in a fixed reduction order
  * (deterministic).  Used for the circulation / linear impulse conservation

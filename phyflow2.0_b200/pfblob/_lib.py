@@ -47,6 +47,8 @@ PROTOTYPES = {
     "pf_moments": [_vp, _i64, _vp, _vp, _vp, _vp, _vp],
     "pf_remesh_window": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _i64, _i64,
                          _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pf_remesh_window_noalloc": [_i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _i64,
+                                 _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "pf_fmm_lists": [_int, _int, _dbl, _dbl, _dbl, _vp, _i64, _c.POINTER(_i64)],
     "pf_fmm_set_tuning": [_int, _int, _int],
     "pf_batch_create": [_vp, _c.c_int32, _vp, _dbl, _c.c_int32, _c.POINTER(_vp)],

@@ -375,6 +375,106 @@ def run_reference(args):
     }
 
 
+# ---------------------------------------------------------------------------
+# Batched (config 4) and served (config 5) sections: same metric, many blob sets
+def _sims_on_device(sizes, config, dev):
+    import torch
+    from pfblob import workloads as wl
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    out = []
+    for i, n in enumerate(sizes):
+        b = wl.mixed_instance(int(n), config=config, instance=i)
+        out.append((b, T(b.x), T(b.y), T(b.g)))
+    return out
+
+
+def run_batched(dev, n_sims=256, steps=5):
+    """256 simulations, N log-uniform in [2048, 262144]: one CUDA-graph launch
+    per step vs one simulation per launch sequence (same methods and trees)."""
+    import torch
+    import pfblob
+    from pfblob import _lib, workloads as wl
+    from pfblob.batch import Batch
+    from pfblob.tune import Tuner
+    sizes = wl.log_uniform_sizes(n_sims, 2048, 262144, config=4)
+    sims = _sims_on_device(sizes, 4, dev)
+    tun = Tuner(dev.index)
+    tun.calibrate(save=False)
+    bt = Batch([{"x": x, "y": y, "g": g, "sigma": b.sigma} for b, x, y, g in sims], tol=1e-6,
+               n_streams=8, tuner=tun)
+    for _ in range(3):
+        bt.run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tb = []
+    for _ in range(steps):
+        e0.record()
+        bt.run()
+        e1.record()
+        torch.cuda.synchronize()
+        tb.append(e0.elapsed_time(e1))
+    res = bt.results()
+    ntot = int(sizes.sum())
+
+    def plain_step():
+        for (b, x, y, g), r in zip(sims, bt.sims):
+            ks, xo, cut = pfblob.fmm_parameters(b.sigma)
+            if r["method"] == 0:
+                _lib.fmm_set_tuning(r["leaf_level"], 0, 1)
+            pfblob.velocity_device(x, y, g, ks, x, y, r["vx"], r["vy"], method=r["method"],
+                                   xopt=xo, cutoff=cut, tol=1e-6)
+            xb, yb = b.bounds()
+            pfblob.remesh_device(x, y, g, b.h, xb[0], yb[0])
+        _lib.fmm_set_tuning(0, 0, 1)
+
+    plain_step()
+    torch.cuda.synchronize()
+    tp = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        plain_step()
+        torch.cuda.synchronize()
+        tp.append((time.perf_counter() - t0) * 1e3)
+    out = {"workload": f"{n_sims} simulations, N log-uniform [2048, 262144] (sum {ntot}), "
+                       "Lamb-Oseen + uniform mix in [-1,1]^2, sigma U[0.002, 0.01]; "
+                       "velocity (autotuned direct/FMM) + M4' remesh per simulation",
+           "n_blobs": ntot, "batched_ms": statistics.median(tb),
+           "batched_evals_per_s": ntot / (statistics.median(tb) * 1e-3),
+           "plain_ms": statistics.median(tp), "plain_evals_per_s": ntot / (statistics.median(tp) * 1e-3),
+           "ratio": statistics.median(tp) / statistics.median(tb),
+           "n_direct": sum(1 for r in res if r["method"] == 1),
+           "n_fmm": sum(1 for r in res if r["method"] == 0), "graph_kernel_nodes": bt.kernel_nodes,
+           "launches_per_step": 1}
+    bt.close()
+    return out
+
+
+def run_served(dev, n_sims=1024, n_req=400, rates=(100, 1000, 5000), slots=8):
+    """1024 resident simulations, N log-uniform in [1024, 2^20]; Poisson arrivals
+    of velocity+remesh requests; continuous batching over `slots` worker streams
+    vs one request at a time."""
+    from pfblob import workloads as wl
+    from pfblob.serve import Server, Simulation, poisson_trace, summarize
+    sizes = wl.log_uniform_sizes(n_sims, 1024, 1 << 20, config=5)
+    sims = [Simulation(x, y, g, sigma=b.sigma) for b, x, y, g in _sims_on_device(sizes, 5, dev)]
+    out = {"workload": f"{n_sims} resident simulations, N log-uniform [1024, 1048576] "
+                       f"(sum {int(sizes.sum())}); Poisson arrivals, {n_req} requests per rate",
+           "slots": slots, "rates": {}}
+    srv = Server(sims, n_slots=slots)
+    srv.warmup()
+    for rate in rates:
+        out["rates"][str(rate)] = summarize(srv.run_trace(poisson_trace(n_req, rate, n_sims, seed=rate)))
+    srv.close()
+    one = Server(sims, n_slots=1)
+    one.warmup(every_sim=False)
+    sat = max(rates)
+    out["plain_one_at_a_time"] = summarize(one.run_trace(poisson_trace(n_req, sat, n_sims, seed=sat)))
+    one.close()
+    out["ratio_at_saturation"] = (out["rates"][str(sat)]["evals_per_s"] /
+                                  out["plain_one_at_a_time"]["evals_per_s"])
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,6 +487,8 @@ def main():
                     help="blob count (default 2^20; smaller only for profiling captures)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched (256 simulations) and served (1024 simulations) sections")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -402,6 +504,10 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line = run_ours(args, rank, world)
+    if rank == 0 and world == 1 and not args.no_extras and args.n is None:
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+        line["batched"] = run_batched(dev)
+        line["served"] = run_served(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, desc, threads, kind = cpu_reference_step(line["config"]["method"])
         line["cpu_baseline"] = {"value": v, "unit": "evals/s", "cores": threads, "kind": kind,

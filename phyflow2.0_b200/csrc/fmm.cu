@@ -31,7 +31,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "fmm_api.cuh"
@@ -597,7 +599,6 @@ k_sorted_keys(int64_t n, const int32_t *__restrict__ perm, const uint32_t *__res
 struct FmmCache {
     int L = -1, kb = -1, np = -1;
     double ratio = -1.0;  // cutoff / root width
-    double x0 = 0.0, y0 = 0.0, w0 = 1.0;  // root box of the current call
     int maxpos = 0, nq = 0, nqp = 0;
     int4 *d_far = nullptr;
     int32_t *d_far_ptr = nullptr;
@@ -605,6 +606,8 @@ struct FmmCache {
     int32_t *d_run_off = nullptr;  // [nblk + 1]
     int2 *d_runs = nullptr;        // (first, last) leaf of each run
     int64_t nruns = 0;
+    size_t dev_bytes = 0;          // device memory held by this plan
+    size_t bytes() const { return dev_bytes; }
     double2 *d_pw = nullptr, *d_m2m = nullptr, *d_l2l = nullptr;
     double *d_bin = nullptr;
     void release() {
@@ -642,11 +645,12 @@ static double binom_d(int n, int k) {
 }
 
 template <typename T>
-static pf_status upload(T **dst, const std::vector<T> &v) {
+static pf_status upload(T **dst, const std::vector<T> &v, size_t &tally) {
     if (v.empty()) {
         *dst = nullptr;
         return PF_OK;
     }
+    tally += sizeof(T) * v.size();
     PF_CUDA_TRY(cudaMalloc(reinterpret_cast<void **>(dst), sizeof(T) * v.size()));
     PF_CUDA_TRY(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
     return PF_OK;
@@ -654,6 +658,7 @@ static pf_status upload(T **dst, const std::vector<T> &v) {
 
 static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, double cutoff) {
     c.release();
+    size_t tally = 0;
     pf::fmm::Tables t;
     pf::fmm::build_tables(L, kb, w0, cutoff, THETA, t);
     const int B = 1 << kb, Bp = B > 2 ? B : 2;
@@ -720,13 +725,13 @@ static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, doub
     c.nq = (int)q.size();
     c.nqp = 1;
     while (c.nqp < c.nq) c.nqp <<= 1;
-    PF_TRY(upload(&c.d_far, far));
-    PF_TRY(upload(&c.d_far_ptr, ptr));
-    PF_TRY(upload(&c.d_q, q));
-    PF_TRY(upload(&c.d_pw, pw));
-    PF_TRY(upload(&c.d_m2m, m2m));
-    PF_TRY(upload(&c.d_l2l, l2l));
-    PF_TRY(upload(&c.d_bin, bin));
+    PF_TRY(upload(&c.d_far, far, tally));
+    PF_TRY(upload(&c.d_far_ptr, ptr, tally));
+    PF_TRY(upload(&c.d_q, q, tally));
+    PF_TRY(upload(&c.d_pw, pw, tally));
+    PF_TRY(upload(&c.d_m2m, m2m, tally));
+    PF_TRY(upload(&c.d_l2l, l2l, tally));
+    PF_TRY(upload(&c.d_bin, bin, tally));
     if (c.nqp <= P2P_QMAX) {
         // P2P run lists of every block (geometry only, reused by every call)
         const int64_t nblk = (int64_t)1 << (2 * (L - kb));
@@ -752,7 +757,9 @@ static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, doub
                                                           c.d_runs);
         PF_TRY(pf::launch_status("k_p2p_runs"));
         PF_CUDA_TRY(cudaDeviceSynchronize());
+        tally += sizeof(int32_t) * (nblk + 1) + sizeof(int2) * (acc > 0 ? acc : 1);
     }
+    c.dev_bytes = tally;
     c.L = L;
     c.kb = kb;
     c.np = np;
@@ -833,10 +840,10 @@ static size_t fmm_scratch_bytes(const FmmCache &c, int64_t ns, int64_t nt, bool 
 // ctr: 2 device counters (P2P pairs, M2L translations), zeroed here.
 // ev: 7 events recorded around the phases, or nullptr.
 template <int NP>
-static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c,
-                          unsigned long long *ctr, cudaEvent_t *ev, cudaStream_t st) {
+static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, double x0,
+                          double y0, double w0, unsigned long long *ctr, cudaEvent_t *ev,
+                          cudaStream_t st) {
     const int L = c.L, kb = c.kb;
-    const double x0 = c.x0, y0 = c.y0, w0 = c.w0;
     const bool same = (a.xt == a.x && a.yt == a.y && a.nt == a.ns);
     const double wl = std::ldexp(w0, -L);
     const int64_t nleaf = (int64_t)1 << (2 * L);
@@ -973,15 +980,76 @@ int fmmx::np_for_tol(double tol) {
     return 32;
 }
 
-pf_status fmm_exec(const FmmCache &c, Bump &sc, const FmmArgs &a, unsigned long long *ctr,
-                   cudaEvent_t *ev, cudaStream_t st) {
+pf_status fmm_exec(const FmmCache &c, double x0, double y0, double w0, Bump &sc,
+                   const FmmArgs &a, unsigned long long *ctr, cudaEvent_t *ev, cudaStream_t st) {
     switch (c.np) {
-        case 16: return exec_fmm<16>(sc, a, c, ctr, ev, st);
-        case 20: return exec_fmm<20>(sc, a, c, ctr, ev, st);
-        case 24: return exec_fmm<24>(sc, a, c, ctr, ev, st);
-        case 28: return exec_fmm<28>(sc, a, c, ctr, ev, st);
-        default: return exec_fmm<32>(sc, a, c, ctr, ev, st);
+        case 16: return exec_fmm<16>(sc, a, c, x0, y0, w0, ctr, ev, st);
+        case 20: return exec_fmm<20>(sc, a, c, x0, y0, w0, ctr, ev, st);
+        case 24: return exec_fmm<24>(sc, a, c, x0, y0, w0, ctr, ev, st);
+        case 28: return exec_fmm<28>(sc, a, c, x0, y0, w0, ctr, ev, st);
+        default: return exec_fmm<32>(sc, a, c, x0, y0, w0, ctr, ev, st);
     }
+}
+
+// Process-wide cache of read-only plans, shared by every context and thread.
+// Tables depend on the geometry only through cutoff / root width, so plans are
+// built normalised (root width 1) and keyed by (device, L, kb, np, ratio).
+// Least recently used plans are dropped past PF_PLAN_CACHE_BYTES (env,
+// default 4 GiB); their device memory is freed when the last user lets go.
+struct PlanKey {
+    int dev, L, kb, np;
+    double ratio;
+    bool operator<(const PlanKey &o) const {
+        if (dev != o.dev) return dev < o.dev;
+        if (L != o.L) return L < o.L;
+        if (kb != o.kb) return kb < o.kb;
+        if (np != o.np) return np < o.np;
+        return ratio < o.ratio;
+    }
+};
+struct PlanCacheStore {
+    std::mutex mu;
+    std::map<PlanKey, std::pair<std::shared_ptr<FmmCache>, uint64_t>> map;  // plan, last use
+    uint64_t tick = 0;
+    size_t bytes = 0;
+};
+static PlanCacheStore &plan_store() {
+    static PlanCacheStore *s = new PlanCacheStore();  // never destroyed: outlives the contexts
+    return *s;
+}
+static size_t plan_budget() {
+    const char *e = getenv("PF_PLAN_CACHE_BYTES");
+    return e ? (size_t)strtoull(e, nullptr, 10) : ((size_t)4 << 30);
+}
+
+pf_status shared_plan(int dev, int L, int kb, int np, double ratio,
+                      std::shared_ptr<FmmCache> *out) {
+    PlanCacheStore &ps = plan_store();
+    const PlanKey key{dev, L, kb, np, ratio};
+    std::lock_guard<std::mutex> lock(ps.mu);
+    auto it = ps.map.find(key);
+    if (it != ps.map.end()) {
+        it->second.second = ++ps.tick;
+        *out = it->second.first;
+        return PF_OK;
+    }
+    auto c = std::shared_ptr<FmmCache>(new FmmCache(), [](FmmCache *p) {
+        p->release();
+        delete p;
+    });
+    PF_TRY(build_cache(*c, L, kb, np, 1.0, ratio));
+    const size_t b = c->bytes();
+    while (!ps.map.empty() && ps.bytes + b > plan_budget()) {
+        auto old = ps.map.begin();
+        for (auto j = ps.map.begin(); j != ps.map.end(); ++j)
+            if (j->second.second < old->second.second) old = j;
+        ps.bytes -= old->second.first->bytes();
+        ps.map.erase(old);
+    }
+    ps.map[key] = {c, ++ps.tick};
+    ps.bytes += b;
+    *out = c;
+    return PF_OK;
 }
 
 }  // namespace pf
@@ -1083,39 +1151,24 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
     if (!(w0 > 0.0)) w0 = 1.0;
     w0 *= 1.0 + 1e-9;
     // the cutoff sets a floor on the leaf width: P2P blocks must stay bounded
-    FmmCache *cache = static_cast<FmmCache *>(ctx->fmm_cache);
-    if (!cache) {
-        cache = new FmmCache();
-        ctx->fmm_cache = cache;
-        ctx->fmm_cache_free = [](void *p) {
-            auto *c = static_cast<FmmCache *>(p);
-            c->release();
-            delete c;
-        };
-    }
+    std::shared_ptr<FmmCache> cache;
     for (;;) {
-        const double ratio = cutoff / w0;
-        if (cache->L != L || cache->kb != kb || cache->np != np || cache->ratio != ratio)
-            PF_TRY(build_cache(*cache, L, kb, np, w0, cutoff));
+        PF_TRY(pf::shared_plan(ctx->device, L, kb, np, cutoff / w0, &cache));
         if (cache->nqp <= P2P_QMAX) break;
-        if (L <= 3) {
-            cache->release();
-            return pf::launch_direct(n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
-        }
+        if (L <= 3) return pf::launch_direct(n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
         --L;  // cutoff too large for this leaf width: coarser leaves
     }
+    ctx->fmm_plan_hold = cache;  // keep the plan alive while this call's kernels run
     FmmArgs a{n_src, n_tgt, x, y, g, xt, yt, ksigmasqr, cutoff, tol, ndirect, vx, vy};
     stt.used_direct = 0;
     stt.leaf_level = L;
     stt.expansion_terms = np;
     stt.block_level_drop = kb;
-    cache->x0 = xmin;
-    cache->y0 = ymin;
-    cache->w0 = w0;
     const bool same = (xt == x && yt == y && n_tgt == n_src);
     PF_TRY(pf::arena_reserve(ctx, fmm_scratch_bytes(*cache, n_src, n_tgt, same)));
     pf::Bump sc{ctx->arena.base, ctx->arena.cap, 0};
-    return pf::fmm_exec(*cache, sc, a, reinterpret_cast<unsigned long long *>(ctx->dev_small),
+    return pf::fmm_exec(*cache, xmin, ymin, w0, sc, a,
+                        reinterpret_cast<unsigned long long *>(ctx->dev_small),
                         ctx->fmm_profile ? ctx->ev : nullptr, st);
 }
 
@@ -1161,6 +1214,7 @@ namespace fmmx {
 
 struct Plan {
     FmmCache c;
+    double x0 = 0.0, y0 = 0.0, w0 = 1.0;
 };
 
 Plan *plan_new() { return new Plan(); }
@@ -1175,10 +1229,10 @@ pf_status plan_build(Plan *p, int L, int kb, int np, double x0, double y0, doubl
                      double cutoff, bool *p2p_ok) {
     const double ratio = cutoff / w0;
     if (p->c.L != L || p->c.kb != kb || p->c.np != np || p->c.ratio != ratio)
-        PF_TRY(build_cache(p->c, L, kb, np, w0, cutoff));
-    p->c.x0 = x0;
-    p->c.y0 = y0;
-    p->c.w0 = w0;
+        PF_TRY(build_cache(p->c, L, kb, np, 1.0, ratio));
+    p->x0 = x0;
+    p->y0 = y0;
+    p->w0 = w0;
     *p2p_ok = p->c.nqp <= P2P_QMAX;
     return PF_OK;
 }
@@ -1194,7 +1248,7 @@ pf_status plan_exec(const Plan *p, Bump &sc, int64_t ns, const double *x, const 
                     double ksigmasqr, double *vx, double *vy, unsigned long long *ctr,
                     cudaEvent_t *ev, cudaStream_t st) {
     FmmArgs a{ns, nt, x, y, g, xt, yt, ksigmasqr, 0.0, 0.0, 0, vx, vy};
-    return fmm_exec(p->c, sc, a, ctr, ev, st);
+    return fmm_exec(p->c, p->x0, p->y0, p->w0, sc, a, ctr, ev, st);
 }
 
 int auto_level(int64_t ns, int ndirect) {

@@ -6,6 +6,7 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <memory>
 #include <string>
 
 #include "../../include/pfblob.h"
@@ -66,9 +67,9 @@ struct pf_ctx {
     pf::Arena arena;
     // host-side pinned staging for small device->host reads
     int64_t *host_small = nullptr;
-    // FMM plan cache (tables and operators on the device), owned by fmm.cu
-    void *fmm_cache = nullptr;
-    void (*fmm_cache_free)(void *) = nullptr;
+    // the shared FMM plan used by this context's last call (kept alive until
+    // the next call replaces it)
+    std::shared_ptr<void> fmm_plan_hold;
     // small persistent device buffer (FMM counters) and profiling events
     int64_t *dev_small = nullptr;
     bool fmm_profile = false;

@@ -120,7 +120,7 @@ pf_status pf_destroy(pf_ctx *ctx) {
     if (!ctx) return PF_OK;
     pf::DeviceGuard dg(ctx->device);
     cudaDeviceSynchronize();
-    if (ctx->fmm_cache && ctx->fmm_cache_free) ctx->fmm_cache_free(ctx->fmm_cache);
+    ctx->fmm_plan_hold.reset();
     if (ctx->arena.base) cudaFree(ctx->arena.base);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
     if (ctx->dev_small) cudaFree(ctx->dev_small);

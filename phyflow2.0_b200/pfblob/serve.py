@@ -1,0 +1,254 @@
+"""Serving loop: velocity + remesh steps of resident simulations, continuously
+batched on one GPU.
+
+Simulations stay on the device (x, y, g as CUDA tensors).  A request asks for
+one step of one simulation: the velocity at its blobs (direct sum or FMM, as
+the autotuner chose for that simulation) and an M4' remesh of its blobs
+(optionally after a forward-Euler move by dt, the reference's
+``_convection_fe``; optionally replacing the resident state).
+
+Execution: ``n_slots`` worker threads, each with its own CUDA stream and its
+own library context (scratch arena).  A dispatcher admits waiting requests in
+arrival order as soon as a slot is free and the device has room: a request's
+scratch need is estimated from its blob count, and a slot may only grow its
+arena into free HBM (``torch.cuda.mem_get_info``, minus a reserve) that no other
+admitted request has claimed.  Requests that arrive while others run are
+admitted as slots and memory free up, so their kernels overlap on the device.
+Every kernel is deterministic, so a request's result does not depend on what
+runs beside it.
+
+The reference has no counterpart (one blob set per call, synchronous).
+"""
+import math
+import queue
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from .induced import DIRECT_METHOD, FMM_METHOD, fmm_parameters, velocity_device
+from .regrid import remesh_device
+from .tune import Tuner
+
+# scratch bytes per blob of one step (FMM arrays + remesh arrays), measured
+# from the library's scratch layouts, plus a per-cell term for the window
+BYTES_PER_BLOB = 260
+BYTES_PER_CELL = 24
+
+
+@dataclass
+class Simulation:
+    x: torch.Tensor
+    y: torch.Tensor
+    g: torch.Tensor
+    sigma: float
+    k: float = 2.0
+    overlap: float = 0.8
+    c: float = 0.0
+    method: int = -1
+    leaf_level: int = 0
+
+    @property
+    def n(self):
+        return self.x.numel()
+
+    @property
+    def h(self):
+        return self.sigma * self.overlap
+
+
+@dataclass
+class Request:
+    sim: int
+    t_arrival: float
+    dt: float = 0.0
+    update: bool = False
+    t_start: float = 0.0
+    t_done: float = 0.0
+    n: int = 0
+    slot: int = -1
+    claim: int = 0
+    result: dict = field(default_factory=dict)
+    error: str = ""
+
+    @property
+    def latency_ms(self):
+        return (self.t_done - self.t_arrival) * 1e3
+
+
+class Server:
+    def __init__(self, sims, n_slots=8, tol=1e-6, tuner=None, hbm_reserve=2 << 30,
+                 free_hbm=None, keep_results=False, device=None):
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        self.sims = list(sims)
+        self.tol = tol
+        self.keep = keep_results
+        self.tuner = tuner or Tuner(self.device.index)
+        self.reserve = hbm_reserve
+        self.free_hbm = free_hbm or (lambda: torch.cuda.mem_get_info(self.device)[0])
+        for s in self.sims:
+            if s.method < 0:
+                box = (float(s.x.min()), float(s.x.max()), float(s.y.min()), float(s.y.max()))
+                s.method, s.leaf_level = self.tuner.choose(s.n, s.k * s.sigma * s.sigma, box, tol)
+        self.n_slots = n_slots
+        self._need = {}
+        for i in range(len(self.sims)):
+            self.need_bytes(i)
+        self._lock = threading.Condition()
+        self._slot_free = [True] * n_slots
+        self._slot_bytes = [0] * n_slots    # arena bytes a slot may already hold
+        self._claimed = 0                    # bytes of growth claimed by admitted requests
+        self._queues = [queue.Queue() for _ in range(n_slots)]
+        self._done = []
+        self._threads = [threading.Thread(target=self._worker, args=(i,), daemon=True)
+                         for i in range(n_slots)]
+        for t in self._threads:
+            t.start()
+
+    def warmup(self, every_sim=True, timeout=None):
+        """Grow every slot's arena to the largest request and build every
+        simulation's FMM plan before serving, so that no request pays for an
+        allocation or a plan build (both synchronise the device)."""
+        big = max(range(len(self.sims)), key=lambda i: self.need_bytes(i))
+        self.run_trace([(0.0, big)] * self.n_slots, timeout=timeout)
+        if every_sim:
+            self.run_trace([(0.0, i) for i in range(len(self.sims))], timeout=timeout)
+
+    # -- memory model -----------------------------------------------------------
+    def need_bytes(self, sim):
+        """Scratch estimate of one step of simulation `sim` (cached per state)."""
+        s = self.sims[sim]
+        key = (sim, s.n, s.x.data_ptr())
+        v = self._need.get(key)
+        if v is None:
+            span = max(float(s.x.max() - s.x.min()), float(s.y.max() - s.y.min())) if s.n else 0.0
+            cells = (span / s.h + 8.0) ** 2 if s.n else 0.0
+            v = int(BYTES_PER_BLOB * s.n + BYTES_PER_CELL * cells) + (1 << 20)
+            self._need[key] = v
+        return v
+
+    # -- workers ------------------------------------------------------------------
+    def _worker(self, slot):
+        torch.cuda.set_device(self.device)
+        stream = torch.cuda.Stream(self.device)
+        while True:
+            req = self._queues[slot].get()
+            if req is None:
+                return
+            try:
+                with torch.cuda.stream(stream):
+                    self._step(req)
+                stream.synchronize()
+            except Exception as e:  # reported on the request, the server keeps going
+                req.error = f"{type(e).__name__}: {e}"
+            req.t_done = time.perf_counter()
+            with self._lock:
+                self._slot_free[slot] = True
+                self._claimed -= req.claim  # now allocated, hence seen by free_hbm()
+                self._done.append(req)
+                self._lock.notify_all()
+
+    def _step(self, req):
+        s = self.sims[req.sim]
+        ks, xo, cut = fmm_parameters(s.sigma, s.k)
+        vx = torch.empty_like(s.x)
+        vy = torch.empty_like(s.x)
+        if s.method == FMM_METHOD:
+            _lib.fmm_set_tuning(s.leaf_level, 0, 1)
+        velocity_device(s.x, s.y, s.g, ks, s.x, s.y, vx, vy, method=s.method, xopt=xo, cutoff=cut,
+                        tol=self.tol)
+        if req.dt != 0.0:
+            xm = s.x + req.dt * vx
+            ym = s.y + req.dt * vy
+        else:
+            xm, ym = s.x, s.y
+        h = s.h
+        xn, yn, gn = remesh_device(xm, ym, s.g, h, -1.5 * h, -1.5 * h, s.c)
+        req.n = s.n
+        if self.keep:
+            req.result = {"vx": vx, "vy": vy, "x": xn, "y": yn, "g": gn}
+        if req.update:
+            s.x, s.y, s.g = xn, yn, gn
+
+    # -- dispatcher ---------------------------------------------------------------
+    def _try_admit(self, req):
+        """Admit `req` to a free slot if memory allows; returns True if started."""
+        need = self.need_bytes(req.sim)
+        free_slots = [i for i in range(self.n_slots) if self._slot_free[i]]
+        if not free_slots:
+            return False
+        # prefer a slot whose arena already holds the need (no growth)
+        fit = [i for i in free_slots if self._slot_bytes[i] >= need]
+        slot = fit[0] if fit else max(free_slots, key=lambda i: self._slot_bytes[i])
+        growth = max(0, need - self._slot_bytes[slot])
+        if growth > 0 and growth + self._claimed > self.free_hbm() - self.reserve:
+            return False
+        self._slot_free[slot] = False
+        self._slot_bytes[slot] = max(self._slot_bytes[slot], need)
+        self._claimed += growth
+        req.claim = growth
+        req.slot = slot
+        req.t_start = time.perf_counter()
+        self._queues[slot].put(req)
+        return True
+
+    def run_trace(self, trace, dt=0.0, update=False, timeout=None):
+        """Replay (t_offset_seconds, sim_id) arrivals in real time; returns the
+        completed requests in completion order."""
+        trace = sorted(trace)
+        t0 = time.perf_counter()
+        pending = []
+        reqs = []
+        i = 0
+        with self._lock:
+            self._done = []
+        deadline = None if timeout is None else t0 + timeout
+        while True:
+            now = time.perf_counter()
+            while i < len(trace) and t0 + trace[i][0] <= now:
+                r = Request(sim=int(trace[i][1]), t_arrival=t0 + trace[i][0], dt=dt, update=update)
+                pending.append(r)
+                reqs.append(r)
+                i += 1
+            with self._lock:
+                while pending and self._try_admit(pending[0]):
+                    pending.pop(0)
+                if i >= len(trace) and not pending and len(self._done) == len(reqs):
+                    break
+                if deadline is not None and now > deadline:
+                    raise TimeoutError("serving trace did not finish in time")
+                wait = 0.002
+                if i < len(trace):
+                    wait = min(wait, max(0.0, t0 + trace[i][0] - now))
+                self._lock.wait(timeout=wait)
+        with self._lock:
+            return list(self._done)
+
+    def close(self):
+        for q in self._queues:
+            q.put(None)
+        for t in self._threads:
+            t.join(timeout=10)
+
+
+def poisson_trace(n_requests, rate, n_sims, seed=0):
+    """Arrival offsets (s) of a Poisson process of `rate` requests/s, each for a
+    uniformly chosen simulation."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    sims = rng.integers(0, n_sims, n_requests)
+    return list(zip(t.tolist(), sims.tolist()))
+
+
+def summarize(done, t_span=None):
+    lat = np.array([r.latency_ms for r in done if not r.error])
+    n = sum(r.n for r in done if not r.error)
+    if t_span is None and done:
+        t_span = max(r.t_done for r in done) - min(r.t_arrival for r in done)
+    return {"requests": len(done), "errors": sum(1 for r in done if r.error),
+            "p50_ms": float(np.percentile(lat, 50)) if lat.size else math.nan,
+            "p99_ms": float(np.percentile(lat, 99)) if lat.size else math.nan,
+            "evals_per_s": n / t_span if t_span else math.nan, "blobs": n, "span_s": t_span}

@@ -1,0 +1,81 @@
+"""Serving loop: trace generation and summaries (CPU), and on the GPU:
+results are the same alone and in the mix, admission follows free HBM, a
+simulated out-of-memory device makes requests wait and the loop report it."""
+import numpy as np
+import pytest
+import torch
+
+
+def test_poisson_trace_and_summary_cpu():
+    from pfblob.serve import Request, poisson_trace, summarize
+    tr = poisson_trace(1000, 500.0, 7, seed=3)
+    t = np.array([a for a, _ in tr])
+    assert np.all(np.diff(t) > 0) and abs(t[-1] - 2.0) < 0.3
+    assert {s for _, s in tr} <= set(range(7))
+    reqs = [Request(sim=0, t_arrival=0.0, t_done=0.001 * (i + 1), n=100) for i in range(100)]
+    s = summarize(reqs, t_span=1.0)
+    assert abs(s["p50_ms"] - 50.5) < 1e-9 and s["evals_per_s"] == 10000
+
+
+def _sims(sizes, config=5):
+    from pfblob import workloads as wl
+    from pfblob.serve import Simulation
+    dev = torch.device("cuda", 0)
+    out = []
+    for i, n in enumerate(sizes):
+        b = wl.mixed_instance(int(n), config=config, instance=i)
+        T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        out.append(Simulation(T(b.x), T(b.y), T(b.g), sigma=b.sigma))
+    return out
+
+
+@pytest.mark.gpu
+def test_same_result_alone_and_in_the_mix():
+    from pfblob.serve import Server, poisson_trace
+    sizes = [1500, 6000, 20000, 50000, 120000, 3000, 9000, 70000]
+    trace = poisson_trace(24, 20000.0, len(sizes), seed=1)  # arrivals faster than service
+    mix = Server(_sims(sizes), n_slots=6, keep_results=True)
+    done_mix = mix.run_trace(trace, timeout=120)
+    mix.close()
+    alone = Server(_sims(sizes), n_slots=1, keep_results=True)
+    done_alone = alone.run_trace(trace, timeout=120)
+    alone.close()
+    assert len(done_mix) == len(done_alone) == 24
+    assert not any(r.error for r in done_mix + done_alone)
+    # requests overlapped in the mix
+    iv = sorted((r.t_start, r.t_done) for r in done_mix)
+    assert any(b[0] < a[1] for a, b in zip(iv, iv[1:]))
+    key = lambda r: (r.t_arrival, r.sim)
+    for a, b in zip(sorted(done_mix, key=key), sorted(done_alone, key=key)):
+        assert a.sim == b.sim
+        for k in ("vx", "vy", "x", "y", "g"):
+            assert torch.equal(a.result[k], b.result[k]), k
+
+
+@pytest.mark.gpu
+def test_admission_follows_free_hbm_and_reports_oom():
+    from pfblob.serve import Server, poisson_trace
+    sims = _sims([30000, 30000, 30000, 30000])
+    # a device with room for one request's scratch growth at a time
+    srv = Server(sims, n_slots=4, hbm_reserve=0)
+    one = max(srv.need_bytes(i) for i in range(4))
+    srv.free_hbm = lambda: one + 1
+    done = srv.run_trace(poisson_trace(4, 1e6, 4, seed=2), timeout=120)
+    grown = sorted((r.t_start, r.t_done) for r in done if r.claim > 0)
+    assert len(done) == 4 and all(b[0] >= a[1] for a, b in zip(grown, grown[1:]))
+    srv.close()
+    # no room at all: the request waits, the loop reports instead of hanging
+    srv = Server(_sims([40000]), n_slots=2, hbm_reserve=0, free_hbm=lambda: 0)
+    with pytest.raises(TimeoutError):
+        srv.run_trace([(0.0, 0)], timeout=1.0)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_update_replaces_resident_state():
+    from pfblob.serve import Server
+    sims = _sims([5000])
+    srv = Server(sims, n_slots=1, keep_results=True)
+    done = srv.run_trace([(0.0, 0)], update=True, timeout=60)
+    assert sims[0].n == done[0].result["x"].numel() != 5000
+    srv.close()

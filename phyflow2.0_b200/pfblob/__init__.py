@@ -11,13 +11,14 @@ All computation runs in libpfblob.so (hand-written CUDA for sm_100a) through
 the C ABI of include/pfblob.h; PyTorch provides device buffers and streams.
 """
 from . import _lib
+from .blobs import Blobs
 from .conservation import conservation_error, moments_device
 from .induced import (CPU_HARDWARE, DIRECT_METHOD, FMM_METHOD, GAUSS_KERNEL, GPU_HARDWARE,
                       fmm_parameters, velocity, velocity_device)
 from .panels import inducedVelocity, panel_velocity_device
 from .regrid import Regrid, remesh_device
 
-__all__ = ["velocity", "velocity_device", "Regrid", "remesh_device", "inducedVelocity",
+__all__ = ["Blobs", "velocity", "velocity_device", "Regrid", "remesh_device", "inducedVelocity",
            "panel_velocity_device", "moments_device", "conservation_error", "fmm_parameters",
            "GAUSS_KERNEL", "CPU_HARDWARE", "GPU_HARDWARE", "FMM_METHOD", "DIRECT_METHOD"]
 

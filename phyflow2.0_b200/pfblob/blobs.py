@@ -1,0 +1,227 @@
+"""``Blobs``: the vortex-blob state object with pHyFlow's call surface, the
+blob set resident on the GPU.
+
+Keeps the constructor arguments, parameter dictionaries, methods and
+properties of ``pHyFlow.blobs.Blobs`` (``src/python/blobs/__blobsClass.py``)
+that touch the hot path: ``evaluateVelocity`` (:546-628), ``redistribute``
+(:828-897), ``populationControl`` (:783-825), ``addBlobs`` / ``removeBlobs``
+(:499-544, :900-960), the construction-time population control and
+redistribution (:490-494), and ``evolve`` (:705-781) with the reference's
+convection integrators (``_evolution.py:537-701``) and Wee diffusion
+(``_evolution.py:138-235``, time step from ``__compute_deltaTd`` :2248-2318).
+Properties return numpy copies, as the reference's numpy-backed object does.
+"""
+import math
+
+import numpy as np
+import torch
+
+from .induced import DIRECT_METHOD, FMM_METHOD, fmm_parameters, velocity_device
+from .regrid import remesh_device
+
+default_diffusion_params = {'method': 'regrid_wee', 'c2': 'optimized'}
+default_time_integration_params = {'method': 'rk4'}
+default_blob_control_params = {'stepRedistribution': 1, 'stepPopulationControl': 1,
+                               'gThresholdLocal': 1e-8, 'gThresholdGlobal': 1e-8}
+default_velocity_computation_params = {'method': 'fmm', 'hardware': 'gpu'}
+
+
+class Blobs:
+    def __init__(self, wField, vInf, nu, deltaTc, h, overlap,
+                 timeIntegrationParams=default_time_integration_params,
+                 blobControlParams=default_blob_control_params,
+                 velocityComputationParams=default_velocity_computation_params,
+                 diffusionParams=default_diffusion_params, device=None):
+        if len(wField) != 3:
+            raise ValueError("wField must have exactly 3 arrays. It has %d." % len(wField))
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        if callable(wField[0]):
+            x, y, g = self._blobs_from_function(wField, h)
+        else:
+            x, y, g = (np.asarray(a, dtype=np.float64).ravel() for a in wField)
+            if not (x.shape == y.shape == g.shape):
+                raise ValueError("wField arrays must have the same shape")
+        self._x, self._y, self._g = (self._dev(a) for a in (x, y, g))
+        self.vInf = np.asarray(vInf, dtype=np.float64)
+        self.nu = float(nu)
+        self.deltaTc = float(deltaTc)
+        self.h = float(h)
+        self.overlap = float(overlap)
+        self.sigma = self.h / self.overlap
+        self.timeIntegrationParams = dict(timeIntegrationParams)
+        self.blobControlParams = dict(blobControlParams)
+        self.velocityComputationParams = dict(velocityComputationParams)
+        self.diffusionParams = dict(diffusionParams)
+        if self.timeIntegrationParams['method'] not in ('euler', 'rk4'):
+            raise ValueError("timeIntegrationParams['method'] must be 'euler' or 'rk4'")
+        if self.velocityComputationParams['method'] not in ('fmm', 'direct'):
+            raise ValueError("velocityComputationParams['method'] must be 'fmm' or 'direct'")
+        if self.diffusionParams['method'] != 'regrid_wee':
+            raise NotImplementedError("pfblob: only 'regrid_wee' diffusion is provided")
+        self.deltaTd, self.stepDiffusion = self._compute_deltaTd()
+        self.tStep = 0
+        self.t = 0.0
+        if self.stepPopulationControl > 0:
+            self.populationControl()
+        if self.stepRedistribution > 0:
+            self.redistribute()
+
+    # -- helpers ----------------------------------------------------------------
+    def _dev(self, a):
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(self.device)
+
+    def _blobs_from_function(self, wField, h):
+        """(wExactFunction, xBounds, yBounds): blobs on the lattice of spacing h
+        containing (0, 0), inside the bounds, circulation w(x, y) h^2."""
+        f, xb, yb = wField
+        ix = np.arange(math.ceil(xb[0] / h), math.floor(xb[1] / h) + 1)
+        iy = np.arange(math.ceil(yb[0] / h), math.floor(yb[1] / h) + 1)
+        X, Y = np.meshgrid(ix * h, iy * h, indexing="ij")
+        x, y = X.ravel(), Y.ravel()
+        return x, y, f(x, y) * h * h
+
+    def _compute_deltaTd(self):
+        """Wee diffusion time step (__blobsClass.py:2248-2288)."""
+        if self.nu == 0.0:
+            return 0.0, 0
+        c2 = self.diffusionParams['c2']
+        deltaTd = ((1.0 / 3.0) * self.h * self.h) / self.nu if c2 == 'optimized' else \
+            (float(c2) * self.h * self.h) / self.nu
+        if deltaTd >= self.deltaTc:
+            step = int(round(deltaTd / self.deltaTc))
+            return step * self.deltaTc, step
+        raise ValueError('Regrid Wee: deltaTc is too large. Reduce deltaTc to a value smaller '
+                         'than %f.' % deltaTd)
+
+    def _method(self):
+        return FMM_METHOD if self.velocityComputationParams['method'] == 'fmm' else DIRECT_METHOD
+
+    def _velocity_at(self, xs, ys, xt, yt, Ndirect=35, tol=1.0e-6, cutoff=None):
+        ks, xo, cut = fmm_parameters(self.sigma, 2.0, cutoff)
+        vx = torch.empty_like(xt)
+        vy = torch.empty_like(xt)
+        velocity_device(xs, ys, self._g, ks, xt, yt, vx, vy, method=self._method(), xopt=xo,
+                        cutoff=cut, tol=tol, ndirect=Ndirect)
+        return vx, vy
+
+    def _regrid(self, c):
+        h = self.h
+        self._x, self._y, self._g = remesh_device(self._x, self._y, self._g, h, -1.5 * h,
+                                                  -1.5 * h, c)
+
+    # -- hot-path methods ---------------------------------------------------------
+    def evaluateVelocity(self, xEval=None, yEval=None, Ndirect=35, tol=1.0e-6, cutoff=None):
+        """Induced velocity at (xEval, yEval) (the blobs if None); numpy in and
+        out, or CUDA tensors in and out."""
+        if xEval is None:
+            xt, yt, host = self._x, self._y, True
+        else:
+            host = not isinstance(xEval, torch.Tensor)
+            xt = xEval.to(self.device, torch.float64) if not host else self._dev(xEval)
+            yt = yEval.to(self.device, torch.float64) if not host else self._dev(yEval)
+        vx, vy = self._velocity_at(self._x, self._y, xt, yt, Ndirect, tol, cutoff)
+        return (vx.cpu().numpy(), vy.cpu().numpy()) if host else (vx, vy)
+
+    def redistribute(self, interpKernel=0):
+        """M4' remesh onto the lattice containing (0, 0) (xBounds = [-1.5h, 1.5h])."""
+        if interpKernel != 0:
+            raise NotImplementedError("pfblob: only the M4' kernel (interpKernel=0) exists")
+        if self.numBlobs > 0:
+            self._regrid(0.0)
+
+    def populationControl(self):
+        """Drop blobs with |g| below gThresholdLocal while the dropped
+        circulation stays below gThresholdGlobal (threshold /10 otherwise),
+        as PopulationControl (_regridding.py:227-330)."""
+        thr = float(self.blobControlParams['gThresholdLocal'])
+        tot = float(self.blobControlParams['gThresholdGlobal'])
+        a = self._g.abs()
+        while True:
+            flag = a < thr
+            if float(a[flag].sum()) < tot:
+                break
+            thr /= 10.0
+        keep = ~flag
+        self._x, self._y, self._g = self._x[keep], self._y[keep], self._g[keep]
+
+    def evolve(self):
+        """One time step: convection (FE or the reference's RK4), Wee diffusion
+        every stepDiffusion steps, redistribution and population control."""
+        vinf = self.vInf
+        if self.timeIntegrationParams['method'] == 'euler':
+            vx, vy = self._velocity_at(self._x, self._y, self._x, self._y)
+            xn = self._x + (vx + vinf[0]) * self.deltaTc
+            yn = self._y + (vy + vinf[1]) * self.deltaTc
+        else:
+            # _evolution.py:679-693 evaluates all four stages at the start
+            # positions (the stage increment it adds stays zero), so the four
+            # velocities are identical: evaluate once, apply the four weighted
+            # updates in the reference's order.
+            vx, vy = self._velocity_at(self._x, self._y, self._x, self._y)
+            kx, ky = vx + vinf[0], vy + vinf[1]
+            xn, yn = self._x.clone(), self._y.clone()
+            for w in (1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0):
+                xn += w * kx * self.deltaTc
+                yn += w * ky * self.deltaTc
+        self._x, self._y = xn, yn
+        if self.stepDiffusion != 0 and (self.tStep % self.stepDiffusion) == 0:
+            self._regrid(math.sqrt(self.nu * self.deltaTd) / self.h)
+        if self.stepRedistribution != 0 and (self.tStep % self.stepRedistribution) == 0:
+            self.redistribute()
+        self.tStep += 1
+        self.t += self.deltaTc
+        if self.stepPopulationControl != 0 and (self.tStep % self.stepPopulationControl) == 0:
+            self.populationControl()
+
+    def addBlobs(self, xNew, yNew, gNew):
+        self._x = torch.cat([self._x, self._dev(xNew)])
+        self._y = torch.cat([self._y, self._dev(yNew)])
+        self._g = torch.cat([self._g, self._dev(gNew)])
+
+    def removeBlobs(self, iBlobs):
+        iBlobs = np.asarray(iBlobs)
+        keep = np.ones(self.numBlobs, dtype=bool)
+        keep[iBlobs] = False
+        k = torch.from_numpy(keep).to(self.device)
+        self._x, self._y, self._g = self._x[k], self._y[k], self._g[k]
+
+    # -- properties ---------------------------------------------------------------
+    @property
+    def x(self):
+        return self._x.cpu().numpy()
+
+    @property
+    def y(self):
+        return self._y.cpu().numpy()
+
+    @property
+    def g(self):
+        return self._g.cpu().numpy()
+
+    @property
+    def numBlobs(self):
+        return self._x.numel()
+
+    @property
+    def stepRedistribution(self):
+        return int(self.blobControlParams['stepRedistribution'])
+
+    @property
+    def stepPopulationControl(self):
+        return int(self.blobControlParams['stepPopulationControl'])
+
+    @property
+    def gThresholdLocal(self):
+        return float(self.blobControlParams['gThresholdLocal'])
+
+    @property
+    def gThresholdGlobal(self):
+        return float(self.blobControlParams['gThresholdGlobal'])
+
+    @property
+    def integrationMethod(self):
+        return self.timeIntegrationParams['method']
+
+    @property
+    def computationMethod(self):
+        return (self.velocityComputationParams['method'], self.velocityComputationParams['hardware'])

@@ -19,8 +19,9 @@ constexpr int DT_THREADS = 256;
 constexpr int DT_CHUNK = 32;
 constexpr double INV_2PI = 0.15915494309189535;  // 0.5/pi
 
-// One CTA computes the DT_THREADS*TPT targets of tile `tile`.
-template <int TPT>
+// One CTA computes the 2*DT_THREADS targets of tile `tile`: each thread owns
+// targets base and base + DT_THREADS and evaluates both against every source
+// with the packed f32x2 pair arithmetic (gauss_pair.cuh).
 __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
                                             const double *__restrict__ ys,
                                             const double *__restrict__ gs, int64_t ns,
@@ -28,22 +29,25 @@ __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
                                             const double *__restrict__ yt, int64_t nt,
                                             const pfd::GaussParams &gp, double *__restrict__ vx,
                                             double *__restrict__ vy, int64_t tile,
-                                            float4 *s_pos, float *s_g) {
-    const int64_t base = tile * (DT_THREADS * TPT) + threadIdx.x;
-    float txh[TPT], txl[TPT], tyh[TPT], tyl[TPT];
-    float hx[TPT], lx[TPT], hy[TPT], ly[TPT];
+                                            ulonglong2 *s_hi, ulonglong2 *s_lo,
+                                            unsigned long long *s_g2) {
+    const int64_t base = tile * (DT_THREADS * 2) + threadIdx.x;
+    float th[2][4];
 #pragma unroll
-    for (int j = 0; j < TPT; ++j) {
-        int64_t i = base + (int64_t)j * DT_THREADS;
+    for (int j = 0; j < 2; ++j) {
+        const int64_t i = base + (int64_t)j * DT_THREADS;
         double x = 0.0, y = 0.0;
         if (i < nt) {
             x = xt[i];
             y = yt[i];
         }
-        pfd::split_hilo(x, txh[j], txl[j]);
-        pfd::split_hilo(y, tyh[j], tyl[j]);
-        hx[j] = lx[j] = hy[j] = ly[j] = 0.0f;
+        pfd::split_hilo(x, th[j][0], th[j][2]);
+        pfd::split_hilo(y, th[j][1], th[j][3]);
     }
+    const pfd::f32x2 txh = pfd::pack2(th[0][0], th[1][0]), tyh = pfd::pack2(th[0][1], th[1][1]);
+    const pfd::f32x2 txl = pfd::pack2(th[0][2], th[1][2]), tyl = pfd::pack2(th[0][3], th[1][3]);
+    const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
     for (int64_t t0 = 0; t0 < ns; t0 += DT_THREADS) {
         const int64_t s = t0 + threadIdx.x;
@@ -53,45 +57,37 @@ __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
             y = ys[s];
             g = gs[s];
         }
-        float4 p;
-        pfd::split_hilo(x, p.x, p.z);
-        pfd::split_hilo(y, p.y, p.w);
+        float xh, xl, yh, yl;
+        pfd::split_hilo(x, xh, xl);
+        pfd::split_hilo(y, yh, yl);
+        const float gf = (float)g;
         __syncthreads();
-        s_pos[threadIdx.x] = p;
-        s_g[threadIdx.x] = (float)g;
+        s_hi[threadIdx.x] = make_ulonglong2(pfd::pack2(xh, xh), pfd::pack2(yh, yh));
+        s_lo[threadIdx.x] = make_ulonglong2(pfd::pack2(xl, xl), pfd::pack2(yl, yl));
+        s_g2[threadIdx.x] = pfd::pack2(gf, gf);
         __syncthreads();
         const int nvalid = (int)min((int64_t)DT_THREADS, ns - t0);
         for (int c0 = 0; c0 < nvalid; c0 += DT_CHUNK) {
-            float px[TPT], py[TPT];
-#pragma unroll
-            for (int j = 0; j < TPT; ++j) px[j] = py[j] = 0.0f;
+            pfd::f32x2 nx = 0ull, ny = 0ull;
 #pragma unroll 4
-            for (int k = 0; k < DT_CHUNK; ++k) {
-                const float4 q = s_pos[c0 + k];
-                const float gk = s_g[c0 + k];
-#pragma unroll
-                for (int j = 0; j < TPT; ++j) {
-                    const float dx = (txh[j] - q.x) + (txl[j] - q.z);
-                    const float dy = (tyh[j] - q.y) + (tyl[j] - q.w);
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
-                    const float sc = pfd::gauss_s(r2, gk, gp);
-                    px[j] = fmaf(-dy, sc, px[j]);
-                    py[j] = fmaf(dx, sc, py[j]);
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < TPT; ++j) {
-                pfd::comp_add(hx[j], lx[j], px[j]);
-                pfd::comp_add(hy[j], ly[j], py[j]);
-            }
+            for (int k = 0; k < DT_CHUNK; ++k)
+                pfd::pair2(s_hi[c0 + k], s_lo[c0 + k], s_g2[c0 + k], txh, tyh, txl, tyl, gp2, nx,
+                           ny);
+            float nxa, nxb, nya, nyb;
+            pfd::unpack2(nx, nxa, nxb);
+            pfd::unpack2(ny, nya, nyb);
+            pfd::comp_add(acc[0], acc[1], -nxa);
+            pfd::comp_add(acc[2], acc[3], nya);
+            pfd::comp_add(acc[4], acc[5], -nxb);
+            pfd::comp_add(acc[6], acc[7], nyb);
         }
     }
 #pragma unroll
-    for (int j = 0; j < TPT; ++j) {
-        int64_t i = base + (int64_t)j * DT_THREADS;
+    for (int j = 0; j < 2; ++j) {
+        const int64_t i = base + (int64_t)j * DT_THREADS;
         if (i < nt) {
-            vx[i] = INV_2PI * ((double)hx[j] + (double)lx[j]);
-            vy[i] = INV_2PI * ((double)hy[j] + (double)ly[j]);
+            vx[i] = INV_2PI * ((double)acc[4 * j] + (double)acc[4 * j + 1]);
+            vy[i] = INV_2PI * ((double)acc[4 * j + 2] + (double)acc[4 * j + 3]);
         }
     }
 }
@@ -102,9 +98,11 @@ k_direct_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
                const double *__restrict__ gs, int64_t ns, const double *__restrict__ xt,
                const double *__restrict__ yt, int64_t nt, pfd::GaussParams gp,
                double *__restrict__ vx, double *__restrict__ vy) {
-    __shared__ float4 s_pos[DT_THREADS];  // x_hi, y_hi, x_lo, y_lo
-    __shared__ float s_g[DT_THREADS];
-    direct_tile<TPT>(xs, ys, gs, ns, xt, yt, nt, gp, vx, vy, blockIdx.x, s_pos, s_g);
+    static_assert(TPT == 2, "two targets per thread (packed pairs)");
+    __shared__ ulonglong2 s_hi[DT_THREADS];  // {x_hi, x_hi}, {y_hi, y_hi}
+    __shared__ ulonglong2 s_lo[DT_THREADS];  // {x_lo, x_lo}, {y_lo, y_lo}
+    __shared__ unsigned long long s_g2[DT_THREADS];
+    direct_tile(xs, ys, gs, ns, xt, yt, nt, gp, vx, vy, blockIdx.x, s_hi, s_lo, s_g2);
 }
 
 // Persistent batched direct sum: CTAs take (instance, target tile) items from
@@ -114,8 +112,9 @@ k_direct_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
 __global__ void __launch_bounds__(DT_THREADS)
 k_direct_batch(const pf::DirectInstance *__restrict__ inst, const int2 *__restrict__ items,
                int n_items, int *__restrict__ counter) {
-    __shared__ float4 s_pos[DT_THREADS];
-    __shared__ float s_g[DT_THREADS];
+    __shared__ ulonglong2 s_hi[DT_THREADS];
+    __shared__ ulonglong2 s_lo[DT_THREADS];
+    __shared__ unsigned long long s_g2[DT_THREADS];
     __shared__ int s_item;
     for (;;) {
         __syncthreads();
@@ -125,7 +124,7 @@ k_direct_batch(const pf::DirectInstance *__restrict__ inst, const int2 *__restri
         if (it >= n_items) break;
         const int2 w = items[it];
         const pf::DirectInstance d = inst[w.x];
-        direct_tile<2>(d.x, d.y, d.g, d.n, d.xt, d.yt, d.nt, d.gp, d.vx, d.vy, w.y, s_pos, s_g);
+        direct_tile(d.x, d.y, d.g, d.n, d.xt, d.yt, d.nt, d.gp, d.vx, d.vy, w.y, s_hi, s_lo, s_g2);
     }
 }
 

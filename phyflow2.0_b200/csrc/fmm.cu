@@ -260,34 +260,47 @@ __host__ __device__ __forceinline__ int64_t level_off(int l) {
     return ((((int64_t)1) << (2 * l)) - 1) / 3;
 }
 
-// M2M at parent level l: one warp per parent box, lane k = coefficient
+// Boxes handled per warp by the translation kernels: with p+1 <= 16 terms two
+// boxes share a warp (one half-warp each, lane n = coefficient n), otherwise
+// one box per warp.
+template <int NP>
+struct BoxLanes {
+    static constexpr int BPW = NP <= 16 ? 2 : 1;  // boxes per warp
+    static constexpr int W = 32 / BPW;            // lanes per box
+};
+
+// M2M at parent level l: lane k of a box group = coefficient k
 template <int NP>
 __global__ void __launch_bounds__(WARP_BOX_THREADS)
 k_m2m(int l, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
       const double2 *__restrict__ opT /* [4][NP(m)][NP(k)] */) {
+    using BL = BoxLanes<NP>;
     __shared__ double2 s_a[WARP_BOX_THREADS / 32][32];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t m = (int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid;
-    if (m >= ((int64_t)1 << (2 * l))) return;
-    const int64_t bg = level_off(l) + m;
-    if (scnt[bg] == 0) return;
+    const int half = lane / BL::W, k = lane % BL::W;
+    const int64_t m = ((int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid) * BL::BPW + half;
+    const bool box_ok = m < ((int64_t)1 << (2 * l));
+    const int64_t bg = level_off(l) + (box_ok ? m : 0);
+    const bool live = box_ok && scnt[bg] != 0;
+    if (!__any_sync(0xffffffffu, live)) return;
     double2 acc = make_double2(0.0, 0.0);
     for (int c = 0; c < 4; ++c) {
-        const int64_t cg = level_off(l + 1) + 4 * m + c;
-        if (scnt[cg] == 0) continue;
-        if (lane < NP) s_a[wid][lane] = M[cg * NP + lane];
+        const int64_t cg = level_off(l + 1) + 4 * (box_ok ? m : 0) + c;
+        const bool use = live && scnt[cg] != 0;
+        if (use && k < NP) s_a[wid][lane] = M[cg * NP + k];
         __syncwarp();
-        if (lane < NP) {
+        if (use && k < NP) {
             const double2 *op = opT + (int64_t)c * NP * NP;
+            const double2 *sa = &s_a[wid][half * BL::W];
 #pragma unroll 4
-            for (int mm = 0; mm <= lane; ++mm) acc = cfma(op[mm * NP + lane], s_a[wid][mm], acc);
+            for (int mm = 0; mm <= k; ++mm) acc = cfma(op[mm * NP + k], sa[mm], acc);
         }
         __syncwarp();
     }
-    if (lane < NP) M[bg * NP + lane] = acc;
+    if (live && k < NP) M[bg * NP + k] = acc;
 }
 
-// M2L for all levels 2..L: one warp per target box, lane n = local coefficient
+// M2L for all levels 2..L: lane n of a box group = local coefficient n
 template <int NP>
 __global__ void __launch_bounds__(WARP_BOX_THREADS)
 k_m2l(int L, int Bp, int64_t bg0, int64_t nbg, const int32_t *__restrict__ scnt,
@@ -295,76 +308,95 @@ k_m2l(int L, int Bp, int64_t bg0, int64_t nbg, const int32_t *__restrict__ scnt,
       const int4 *__restrict__ far, const int32_t *__restrict__ far_ptr, int maxpos,
       const double2 *__restrict__ pw /* [nop][NP+1] */, const double *__restrict__ binom,
       unsigned long long *__restrict__ ntrans) {
+    using BL = BoxLanes<NP>;
     __shared__ double2 s_c[WARP_BOX_THREADS / 32][32];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t w = (int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid;
-    if (w >= nbg) return;
-    // this lane's row of the binomial matrix C(n+k, k), n = lane, in registers
+    const int half = lane / BL::W, n = lane % BL::W;
+    const int64_t w = ((int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid) * BL::BPW + half;
+    const int64_t bg = bg0 + (w < nbg ? w : 0);
+    const bool live = w < nbg && tcnt[bg] != 0;
+    if (!__any_sync(0xffffffffu, live)) return;
+    // this lane's row of the binomial matrix C(n+k, k), in registers
     double brow[NP];
 #pragma unroll
-    for (int k = 0; k < NP; ++k) brow[k] = (lane < NP) ? binom[k * NP + lane] : 0.0;
-    const int64_t bg = bg0 + w;
-    if (tcnt[bg] == 0) return;
+    for (int k = 0; k < NP; ++k) brow[k] = (n < NP) ? binom[k * NP + n] : 0.0;
     int l = 2;
     while (l < L && bg >= level_off(l + 1)) ++l;
     const uint32_t m = (uint32_t)(bg - level_off(l));
     const int ix = (int)compact1by1(m), iy = (int)compact1by1(m >> 1);
     const int pos = (l == L) ? ((ix % Bp) + Bp * (iy % Bp)) : ((ix & 1) | ((iy & 1) << 1));
     const int side = 1 << l;
-    const int e0 = far_ptr[l * maxpos + pos], e1 = far_ptr[l * maxpos + pos + 1];
+    const int e0 = far_ptr[l * maxpos + pos];
+    const int len = live ? far_ptr[l * maxpos + pos + 1] - e0 : 0;
+    int lmax = len;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
     double2 acc = make_double2(0.0, 0.0);
     unsigned nt = 0;
-    for (int e = e0; e < e1; ++e) {
-        const int4 f = far[e];
-        const int sx = ix + f.x, sy = iy + f.y;
-        if (sx < 0 || sy < 0 || sx >= side || sy >= side) continue;
-        const int64_t sg = level_off(l) + morton2((uint32_t)sx, (uint32_t)sy);
-        if (scnt[sg] == 0) continue;
-        ++nt;
-        const double2 *rp = pw + (int64_t)f.z * (NP + 1);
-        if (lane < NP) {
-            double2 c = cmul(M[sg * NP + lane], rp[lane]);
-            if ((lane & 1) == 0) c = make_double2(-c.x, -c.y);  // (-1)^(k+1)
+    const double2 *sc = &s_c[wid][half * BL::W];
+    for (int e = 0; e < lmax; ++e) {
+        bool use = e < len;
+        int64_t sg = 0;
+        int op = 0;
+        if (use) {
+            const int4 f = far[e0 + e];
+            const int sx = ix + f.x, sy = iy + f.y;
+            use = sx >= 0 && sy >= 0 && sx < side && sy < side;
+            if (use) {
+                sg = level_off(l) + morton2((uint32_t)sx, (uint32_t)sy);
+                use = scnt[sg] != 0;
+                op = f.z;
+            }
+        }
+        nt += use ? 1u : 0u;
+        const double2 *rp = pw + (int64_t)op * (NP + 1);
+        if (use && n < NP) {
+            double2 c = cmul(M[sg * NP + n], rp[n]);
+            if ((n & 1) == 0) c = make_double2(-c.x, -c.y);  // (-1)^(k+1)
             s_c[wid][lane] = c;
         }
         __syncwarp();
-        if (lane < NP) {
+        if (use && n < NP) {
             double ux = 0.0, uy = 0.0;
 #pragma unroll
             for (int k = 0; k < NP; ++k) {
-                const double2 c = s_c[wid][k];
+                const double2 c = sc[k];
                 ux = fma(brow[k], c.x, ux);
                 uy = fma(brow[k], c.y, uy);
             }
-            acc = cfma(rp[lane + 1], make_double2(ux, uy), acc);
+            acc = cfma(rp[n + 1], make_double2(ux, uy), acc);
         }
         __syncwarp();
     }
-    if (lane < NP) Lc[bg * NP + lane] = acc;
-    if (lane == 0 && nt) atomicAdd(ntrans, (unsigned long long)nt);
+    if (live && n < NP) Lc[bg * NP + n] = acc;
+    if (live && n == 0 && nt) atomicAdd(ntrans, (unsigned long long)nt);
 }
 
-// L2L into child level l: one warp per child box
+// L2L into child level l: lane n of a box group = coefficient n
 template <int NP>
 __global__ void __launch_bounds__(WARP_BOX_THREADS)
 k_l2l(int l, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
       const double2 *__restrict__ opT /* [4][NP(m)][NP(n)] */) {
+    using BL = BoxLanes<NP>;
     __shared__ double2 s_b[WARP_BOX_THREADS / 32][32];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t m = (int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid;
-    if (m >= ((int64_t)1 << (2 * l))) return;
-    const int64_t bg = level_off(l) + m;
-    if (tcnt[bg] == 0) return;
-    const int64_t pg = level_off(l - 1) + (m >> 2);
+    const int half = lane / BL::W, n = lane % BL::W;
+    const int64_t m = ((int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid) * BL::BPW + half;
+    const bool box_ok = m < ((int64_t)1 << (2 * l));
+    const int64_t bg = level_off(l) + (box_ok ? m : 0);
+    const bool live = box_ok && tcnt[bg] != 0;
+    if (!__any_sync(0xffffffffu, live)) return;
+    const int64_t pg = level_off(l - 1) + ((box_ok ? m : 0) >> 2);
     const int c = (int)(m & 3);
-    if (lane < NP) s_b[wid][lane] = Lc[pg * NP + lane];
+    if (live && n < NP) s_b[wid][lane] = Lc[pg * NP + n];
     __syncwarp();
-    if (lane < NP) {
+    if (live && n < NP) {
         const double2 *op = opT + (int64_t)c * NP * NP;
-        double2 acc = Lc[bg * NP + lane];
+        const double2 *sb = &s_b[wid][half * BL::W];
+        double2 acc = Lc[bg * NP + n];
 #pragma unroll 4
-        for (int mm = lane; mm < NP; ++mm) acc = cfma(op[mm * NP + lane], s_b[wid][mm], acc);
-        Lc[bg * NP + lane] = acc;
+        for (int mm = n; mm < NP; ++mm) acc = cfma(op[mm * NP + n], sb[mm], acc);
+        Lc[bg * NP + n] = acc;
     }
 }
 
@@ -434,39 +466,52 @@ k_p2p_runs(int L, int kb, const int2 *__restrict__ q, int nq, int nqp,
 
 // P2P near field: one warp per P2P block, two targets per lane (a group of
 // 64), warp-private source tiles of 64 (no CTA barriers, so blocks with few
-// targets leave no idle target slots behind).
+// targets leave no idle target slots behind).  With two targets the pair
+// arithmetic runs packed (f32x2); a group of at most 32 targets runs scalar.
 template <bool TWO>
-__device__ __forceinline__ void p2p_tile(const float4 *__restrict__ sp, const float *__restrict__ sg,
-                                         int cnt, const float4 &ta, const float4 &tb,
-                                         const pfd::GaussParams &gp, float (&acc)[8]) {
-    for (int c0 = 0; c0 < cnt; c0 += 32) {
-        float pxa = 0.f, pya = 0.f, pxb = 0.f, pyb = 0.f;
+__device__ __forceinline__ void p2p_tile(const ulonglong2 *__restrict__ shi,
+                                         const ulonglong2 *__restrict__ slo,
+                                         const unsigned long long *__restrict__ sg2, int cnt,
+                                         const float4 &ta, const float4 &tb,
+                                         const pfd::GaussParams &gp,
+                                         const pfd::GaussParams2 &gp2, float (&acc)[8]) {
+    if (TWO) {
+        const pfd::f32x2 txh = pfd::pack2(ta.x, tb.x), tyh = pfd::pack2(ta.y, tb.y);
+        const pfd::f32x2 txl = pfd::pack2(ta.z, tb.z), tyl = pfd::pack2(ta.w, tb.w);
+        for (int c0 = 0; c0 < cnt; c0 += 32) {
+            pfd::f32x2 nx = 0ull, ny = 0ull;  // +0.0f in both halves
 #pragma unroll 4
-        for (int k = 0; k < 32; ++k) {
-            const float4 qq = sp[c0 + k];
-            const float g = sg[c0 + k];
-            {
-                const float dx = (ta.x - qq.x) + (ta.z - qq.z);
-                const float dy = (ta.y - qq.y) + (ta.w - qq.w);
+            for (int k = 0; k < 32; ++k)
+                pfd::pair2(shi[c0 + k], slo[c0 + k], sg2[c0 + k], txh, tyh, txl, tyl, gp2, nx, ny);
+            float nxa, nxb, nya, nyb;
+            pfd::unpack2(nx, nxa, nxb);
+            pfd::unpack2(ny, nya, nyb);
+            pfd::comp_add(acc[0], acc[1], -nxa);
+            pfd::comp_add(acc[2], acc[3], nya);
+            pfd::comp_add(acc[4], acc[5], -nxb);
+            pfd::comp_add(acc[6], acc[7], nyb);
+        }
+    } else {
+        for (int c0 = 0; c0 < cnt; c0 += 32) {
+            float pxa = 0.f, pya = 0.f;
+#pragma unroll 4
+            for (int k = 0; k < 32; ++k) {
+                const ulonglong2 h = shi[c0 + k], l = slo[c0 + k];
+                float sxh, syh, sxl, syl, g, dummy;
+                pfd::unpack2(h.x, sxh, dummy);
+                pfd::unpack2(h.y, syh, dummy);
+                pfd::unpack2(l.x, sxl, dummy);
+                pfd::unpack2(l.y, syl, dummy);
+                pfd::unpack2(sg2[c0 + k], g, dummy);
+                const float dx = (ta.x - sxh) + (ta.z - sxl);
+                const float dy = (ta.y - syh) + (ta.w - syl);
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
                 const float sc = pfd::gauss_s(r2, g, gp);
                 pxa = fmaf(-dy, sc, pxa);
                 pya = fmaf(dx, sc, pya);
             }
-            if (TWO) {
-                const float dx = (tb.x - qq.x) + (tb.z - qq.z);
-                const float dy = (tb.y - qq.y) + (tb.w - qq.w);
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
-                const float sc = pfd::gauss_s(r2, g, gp);
-                pxb = fmaf(-dy, sc, pxb);
-                pyb = fmaf(dx, sc, pyb);
-            }
-        }
-        pfd::comp_add(acc[0], acc[1], pxa);
-        pfd::comp_add(acc[2], acc[3], pya);
-        if (TWO) {
-            pfd::comp_add(acc[4], acc[5], pxb);
-            pfd::comp_add(acc[6], acc[7], pyb);
+            pfd::comp_add(acc[0], acc[1], pxa);
+            pfd::comp_add(acc[2], acc[3], pya);
         }
     }
 }
@@ -480,8 +525,10 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
       unsigned long long *__restrict__ pairs) {
     __shared__ int s_rs[P2P_WARPS][P2P_RUNS_SM];      // particle start of run
     __shared__ int s_rp[P2P_WARPS][P2P_RUNS_SM + 1];  // stream prefix of run
-    __shared__ float4 s_pos[P2P_WARPS][P2P_TILE];
-    __shared__ float s_g[P2P_WARPS][P2P_TILE];
+    __shared__ ulonglong2 s_hi[P2P_WARPS][P2P_TILE];  // {x_hi, x_hi}, {y_hi, y_hi}
+    __shared__ ulonglong2 s_lo[P2P_WARPS][P2P_TILE];  // {x_lo, x_lo}, {y_lo, y_lo}
+    __shared__ unsigned long long s_g2[P2P_WARPS][P2P_TILE];  // {g, g}
+    const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t b = (int64_t)blockIdx.x * P2P_WARPS + wid;
     if (b >= nblk) return;
@@ -525,6 +572,10 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
             __syncwarp();
             const int S = pre;
             npairs += (unsigned long long)S * (unsigned long long)min(64, tn - tg);
+            // each lane's two stream positions only move forward (by 64 per
+            // tile), so the run holding them is found by advancing an index:
+            // the largest r with prefix[r] <= p (empty runs are stepped over)
+            int rr[2] = {0, 0};
             for (int s0 = 0; s0 < S; s0 += P2P_TILE) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
@@ -532,23 +583,25 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                     float4 spv = z4;
                     float gg = 0.f;
                     if (p < S) {
-                        int lo = 0, hi = nrc - 1;  // largest r with prefix <= p
-                        while (lo < hi) {
-                            const int mid = (lo + hi + 1) >> 1;
-                            if (s_rp[wid][mid] <= p) lo = mid;
-                            else hi = mid - 1;
-                        }
-                        const int src = s_rs[wid][lo] + (p - s_rp[wid][lo]);
+                        int r = rr[h];
+                        while (r + 1 < nrc && s_rp[wid][r + 1] <= p) ++r;
+                        rr[h] = r;
+                        const int src = s_rs[wid][r] + (p - s_rp[wid][r]);
                         spv = shl[src];
                         gg = sg32[src];
                     }
-                    s_pos[wid][h * 32 + lane] = spv;
-                    s_g[wid][h * 32 + lane] = gg;
+                    s_hi[wid][h * 32 + lane] =
+                        make_ulonglong2(pfd::pack2(spv.x, spv.x), pfd::pack2(spv.y, spv.y));
+                    s_lo[wid][h * 32 + lane] =
+                        make_ulonglong2(pfd::pack2(spv.z, spv.z), pfd::pack2(spv.w, spv.w));
+                    s_g2[wid][h * 32 + lane] = pfd::pack2(gg, gg);
                 }
                 __syncwarp();
                 const int cnt = min(P2P_TILE, S - s0);
-                if (two) p2p_tile<true>(s_pos[wid], s_g[wid], cnt, ta, tb, gp, acc);
-                else p2p_tile<false>(s_pos[wid], s_g[wid], cnt, ta, tb, gp, acc);
+                if (two)
+                    p2p_tile<true>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, gp, gp2, acc);
+                else
+                    p2p_tile<false>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, gp, gp2, acc);
                 __syncwarp();
             }
         }
@@ -914,9 +967,10 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     k_p2m<NP><<<(unsigned)pf::ceil_div(nleaf, 128), 128, 0, st>>>(L, x0, y0, wl, S.start, S.cnt,
                                                                  S.x, S.y, S.g, M);
     PF_TRY(pf::launch_status("k_p2m"));
+    constexpr int BOXES_PER_CTA = (WARP_BOX_THREADS / 32) * BoxLanes<NP>::BPW;
     for (int l = L - 1; l >= 2; --l) {
         const int64_t nb = (int64_t)1 << (2 * l);
-        k_m2m<NP><<<(unsigned)pf::ceil_div(nb, WARP_BOX_THREADS / 32), WARP_BOX_THREADS, 0, st>>>(
+        k_m2m<NP><<<(unsigned)pf::ceil_div(nb, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
             l, scnt_all, M, c.d_m2m);
         PF_TRY(pf::launch_status("k_m2m"));
     }
@@ -925,7 +979,7 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     const int B = 1 << kb, Bp = B > 2 ? B : 2;
     {
         const int64_t bg0 = level_off(2), nbg = nbox - bg0;
-        k_m2l<NP><<<(unsigned)pf::ceil_div(nbg, WARP_BOX_THREADS / 32), WARP_BOX_THREADS, 0, st>>>(
+        k_m2l<NP><<<(unsigned)pf::ceil_div(nbg, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
             L, Bp, bg0, nbg, scnt_all, tcnt_all, M, Lc, c.d_far, c.d_far_ptr, c.maxpos, c.d_pw,
             c.d_bin, ctr + 1);
         PF_TRY(pf::launch_status("k_m2l"));
@@ -933,7 +987,7 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     PF_TRY(mark(3));
     for (int l = 3; l <= L; ++l) {
         const int64_t nb = (int64_t)1 << (2 * l);
-        k_l2l<NP><<<(unsigned)pf::ceil_div(nb, WARP_BOX_THREADS / 32), WARP_BOX_THREADS, 0, st>>>(
+        k_l2l<NP><<<(unsigned)pf::ceil_div(nb, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
             l, tcnt_all, Lc, c.d_l2l);
         PF_TRY(pf::launch_status("k_l2l"));
     }

@@ -50,4 +50,96 @@ __device__ __forceinline__ float gauss_s(float r2, float g, const GaussParams &p
     return g * om * rcp_approx(r2);
 }
 
+
+// ---------------------------------------------------------------------------
+// Two targets against one source with Blackwell's packed f32x2 arithmetic.
+// A 64-bit register holds (target a, target b); every packed operation is the
+// element-wise IEEE round-to-nearest operation, in the same order as the
+// scalar code above, so each lane's two results are bitwise those of two
+// scalar evaluations.  Only ex2 and rcp (MUFU) stay scalar.
+//
+// Source layout in shared memory (broadcast form, so loads land directly in
+// packed registers):  hi = {x_hi, x_hi, y_hi, y_hi}, lo = {x_lo, x_lo, y_lo,
+// y_lo} (two ulonglong2), g2 = {g, g}.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pack2(float a, float b) {
+    f32x2 d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ void unpack2(f32x2 v, float &a, float &b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+struct GaussParams2 {
+    f32x2 c_t, c_x, eps, one;
+    float r2_series, c_x1;
+};
+
+__device__ __forceinline__ GaussParams2 make_params2(const GaussParams &p) {
+    GaussParams2 q;
+    q.c_t = pack2(p.c_t, p.c_t);
+    q.c_x = pack2(p.c_x, p.c_x);
+    q.eps = pack2(1e-12f, 1e-12f);
+    q.one = pack2(1.0f, 1.0f);
+    q.r2_series = p.r2_series;
+    q.c_x1 = p.c_x;
+    return q;
+}
+
+__device__ __forceinline__ float series_om(float r2, float c_x) {
+    const float x = r2 * c_x;
+    float q = fmaf(x, -1.0f / 720.0f, 1.0f / 120.0f);
+    q = fmaf(x, q, -1.0f / 24.0f);
+    q = fmaf(x, q, 1.0f / 6.0f);
+    q = fmaf(x, q, -0.5f);
+    q = fmaf(x, q, 1.0f);
+    return x * q;
+}
+
+// Accumulates, for targets (a, b): nx += dy*s, ny += dx*s  (note the sign:
+// the x velocity is -nx; negation is exact, so -nx equals the scalar sum).
+__device__ __forceinline__ void pair2(const ulonglong2 &hi, const ulonglong2 &lo, f32x2 g2,
+                                      f32x2 txh, f32x2 tyh, f32x2 txl, f32x2 tyl,
+                                      const GaussParams2 &gp, f32x2 &nx, f32x2 &ny) {
+    const f32x2 dx = add2(sub2(txh, hi.x), sub2(txl, lo.x));
+    const f32x2 dy = add2(sub2(tyh, hi.y), sub2(tyl, lo.y));
+    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, gp.eps));
+    float ta, tb, ra, rb;
+    unpack2(mul2(r2, gp.c_t), ta, tb);
+    f32x2 om = sub2(gp.one, pack2(ex2_approx(ta), ex2_approx(tb)));
+    unpack2(r2, ra, rb);
+    if (fminf(ra, rb) < gp.r2_series) {  // 1 - exp(-x) cancels: series
+        float oa, ob;
+        unpack2(om, oa, ob);
+        if (ra < gp.r2_series) oa = series_om(ra, gp.c_x1);
+        if (rb < gp.r2_series) ob = series_om(rb, gp.c_x1);
+        om = pack2(oa, ob);
+    }
+    const f32x2 s = mul2(mul2(g2, om), pack2(rcp_approx(ra), rcp_approx(rb)));
+    nx = fma2(dy, s, nx);
+    ny = fma2(dx, s, ny);
+}
+
 }  // namespace pfd

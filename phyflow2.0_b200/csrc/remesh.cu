@@ -11,11 +11,11 @@
 //      ix-major; rank of a blob in its cell from atomicAdd.
 //   3. scan of the per-cell counts -> cell starts.
 //   4. k_rm_place  : blob index -> its slot.
-//   5. k_rm_order  : per base cell, order its blobs by input index (every sum
-//      below then has a fixed order, independent of atomic timing) and write,
-//      in that order, each blob's four x weights M4'(ux_a), four y weights
-//      M4'(uy_b) (_interpolation_kernels_1d.cpp:75-89; u as _regridding.py:183)
-//      and g.
+//   5. k_rm_sortcells : per base cell, order its blobs by input index (every
+//      sum below then has a fixed order, independent of atomic timing);
+//      k_rm_weights : one thread per blob in that order writes its four x
+//      weights M4'(ux_a), four y weights M4'(uy_b) (_interpolation_kernels_1d.cpp:
+//      75-89; u as _regridding.py:183) and g.
 //   6. k_rm_gather : one thread per output cell (ix, iy) sums, in fixed order,
 //      (wx_a wy_b) g over the blobs of the 16 base cells whose windows cover it,
 //      and flags cells touched by at least one window (explicit zeros are
@@ -174,18 +174,16 @@ struct W9 {
     double wx[4], wy[4], g;
 };
 
+// Per base cell: order the cell's blob indices by input index (cells hold a
+// few blobs; the atomic ranks of k_rm_count are not reproducible).
 __global__ void __launch_bounds__(RM_THREADS)
-k_rm_order(int64_t ncell, int64_t nby, int32_t ixmin, int32_t iymin,
-           const int32_t *__restrict__ start, const int32_t *__restrict__ count,
-           int32_t *__restrict__ perm, const double *__restrict__ x, const double *__restrict__ y,
-           const double *__restrict__ g, double h, double qx0, double qy0, double c2,
-           W9 *__restrict__ w) {
+k_rm_sortcells(int64_t ncell, const int32_t *__restrict__ start,
+               const int32_t *__restrict__ count, int32_t *__restrict__ perm) {
     const int64_t c = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     if (c >= ncell) return;
     const int cnt = count[c];
-    if (cnt == 0) return;
+    if (cnt < 2) return;
     const int s0 = start[c];
-    // insertion sort of the cell's blob indices (cells hold a few blobs)
     for (int k = 1; k < cnt; ++k) {
         const int32_t v = perm[s0 + k];
         int j = k - 1;
@@ -195,26 +193,33 @@ k_rm_order(int64_t ncell, int64_t nby, int32_t ixmin, int32_t iymin,
         }
         perm[s0 + j + 1] = v;
     }
-    const int64_t bx = c / nby, by = c - bx * nby;
-    // numpy order: ((ix + 0.5) + xb0/h) - x/h, ix the absolute lattice index
-    double px[4], py[4];
+}
+
+// One thread per blob in cell order: its four x weights M4'(ux_a), four y
+// weights M4'(uy_b) and g, written in that order.
+__global__ void __launch_bounds__(RM_THREADS)
+k_rm_weights(int64_t n, int64_t nby, int32_t ixmin, int32_t iymin,
+             const int32_t *__restrict__ perm, const int32_t *__restrict__ cell,
+             const double *__restrict__ x, const double *__restrict__ y,
+             const double *__restrict__ g, double h, double qx0, double qy0, double c2,
+             W9 *__restrict__ w, int32_t *__restrict__ nvalid) {
+    const int64_t j = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
+    if (j >= *nvalid) return;
+    const int32_t i = perm[j];
+    const int64_t cc = cell[i];
+    const int64_t bx = cc / nby, by = cc - bx * nby;
+    const double xh = __ddiv_rn(x[i], h), yh = __ddiv_rn(y[i], h);
+    W9 r;
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-        px[a] = ((double)(ixmin + bx + a) + 0.5) + qx0;
-        py[a] = ((double)(iymin + by + a) + 0.5) + qy0;
+        // numpy order: ((ix + 0.5) + xb0/h) - x/h, ix the absolute lattice index
+        const double px = ((double)(ixmin + bx + a) + 0.5) + qx0;
+        const double py = ((double)(iymin + by + a) + 0.5) + qy0;
+        r.wx[a] = m4p(__dsub_rn(px, xh), c2);
+        r.wy[a] = m4p(__dsub_rn(py, yh), c2);
     }
-    for (int k = 0; k < cnt; ++k) {
-        const int32_t i = perm[s0 + k];
-        const double xh = __ddiv_rn(x[i], h), yh = __ddiv_rn(y[i], h);
-        W9 r;
-#pragma unroll
-        for (int a = 0; a < 4; ++a) {
-            r.wx[a] = m4p(__dsub_rn(px[a], xh), c2);
-            r.wy[a] = m4p(__dsub_rn(py[a], yh), c2);
-        }
-        r.g = g[i];
-        w[s0 + k] = r;
-    }
+    r.g = g[i];
+    w[j] = r;
 }
 
 // Output cell grid: ox in [0, nbx+3), oy in [0, nby+3); lattice index
@@ -296,7 +301,7 @@ size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby) {
     const int64_t big = ncell > nbase ? ncell : nbase;
     return align256(4 * n) * 3 + align256(sizeof(W9) * n) + 2 * align256(4 * nbase) +
            align256(8 * ncell) + 2 * align256(4 * ncell) + align256(4 * scan_tmp_ints(big)) +
-           2 * align256(16) + 1024;
+           3 * align256(16) + 1024;
 }
 
 // Everything after the window is known; no host synchronisation.  total_dev
@@ -319,7 +324,8 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     int32_t *flag = (int32_t *)sc.take(4 * ncell);
     int32_t *slot = (int32_t *)sc.take(4 * ncell);
     int32_t *tmp = (int32_t *)sc.take(4 * scan_tmp_ints(big));
-    if (!tmp) {
+    int32_t *nvalid = (int32_t *)sc.take(16);
+    if (!nvalid) {
         set_error("remesh: scratch too small");
         return PF_ERR_OOM;
     }
@@ -329,12 +335,15 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     k_rm_count<<<gn, RM_THREADS, 0, st>>>(x, y, n, xb0, yb0, h2, h05, h, ixmin, iymin, nbx, nby,
                                           cell, rank, count, bad);
     PF_TRY(launch_status("k_rm_count"));
-    PF_TRY(exclusive_scan_i32(count, start, nbase, tmp, nullptr, st));
+    PF_TRY(exclusive_scan_i32(count, start, nbase, tmp, nvalid, st));
     k_rm_place<<<gn, RM_THREADS, 0, st>>>(n, cell, rank, start, perm);
     PF_TRY(launch_status("k_rm_place"));
-    k_rm_order<<<(unsigned)ceil_div(nbase, RM_THREADS), RM_THREADS, 0, st>>>(
-        nbase, nby, ixmin, iymin, start, count, perm, x, y, g, h, xb0 / h, yb0 / h, c * c, w);
-    PF_TRY(launch_status("k_rm_order"));
+    k_rm_sortcells<<<(unsigned)ceil_div(nbase, RM_THREADS), RM_THREADS, 0, st>>>(nbase, start,
+                                                                                count, perm);
+    PF_TRY(launch_status("k_rm_sortcells"));
+    k_rm_weights<<<gn, RM_THREADS, 0, st>>>(n, nby, ixmin, iymin, perm, cell, x, y, g, h, xb0 / h,
+                                            yb0 / h, c * c, w, nvalid);
+    PF_TRY(launch_status("k_rm_weights"));
     k_rm_gather<<<(unsigned)ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(nbx, nby, start,
                                                                              count, w, acc, flag);
     PF_TRY(launch_status("k_rm_gather"));

@@ -57,6 +57,10 @@ constexpr int P2P_QMAX = 1024;   // source leaves per P2P block
 constexpr int P2P_WARPS = 4;     // P2P blocks per CTA (one warp each)
 constexpr int P2P_RUNS_SM = 64;  // runs staged in shared memory at a time
 constexpr int P2P_TILE = 64;     // sources per warp tile
+#ifndef PF_P2P_MIN_CTAS
+#define PF_P2P_MIN_CTAS 8
+#endif
+constexpr int P2P_MIN_CTAS = PF_P2P_MIN_CTAS;  // resident CTAs per SM the register budget allows
 constexpr int WARP_BOX_THREADS = 128;  // 4 warps, one box each
 constexpr unsigned INVALID_KEY = 0xFFFFFFFFu;
 
@@ -464,25 +468,49 @@ k_p2p_runs(int L, int kb, const int2 *__restrict__ q, int nq, int nqp,
     if (!runs && threadIdx.x == 0) nruns_or_off[b] = s_n;
 }
 
-// P2P near field: one warp per P2P block, two targets per lane (a group of
-// 64), warp-private source tiles of 64 (no CTA barriers, so blocks with few
-// targets leave no idle target slots behind).  With two targets the pair
-// arithmetic runs packed (f32x2); a group of at most 32 targets runs scalar.
-template <bool TWO>
+// P2P near field: one warp per P2P block, up to three targets per lane (a
+// group of up to 96), warp-private source tiles of 64 (no CTA barriers, so
+// blocks with few targets leave no idle target slots behind).  Targets a and b
+// of a lane run packed (f32x2), target c scalar; NT = targets per lane in use.
+__device__ __forceinline__ void scalar_pair(const ulonglong2 &h, const ulonglong2 &l,
+                                            unsigned long long g2, const float4 &t,
+                                            const pfd::GaussParams &gp, float &px, float &py) {
+    float sxh, syh, sxl, syl, g, dummy;
+    pfd::unpack2(h.x, sxh, dummy);
+    pfd::unpack2(h.y, syh, dummy);
+    pfd::unpack2(l.x, sxl, dummy);
+    pfd::unpack2(l.y, syl, dummy);
+    pfd::unpack2(g2, g, dummy);
+    const float dx = (t.x - sxh) + (t.z - sxl);
+    const float dy = (t.y - syh) + (t.w - syl);
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
+    const float sc = pfd::gauss_s(r2, g, gp);
+    px = fmaf(-dy, sc, px);
+    py = fmaf(dx, sc, py);
+}
+
+template <int NT>
 __device__ __forceinline__ void p2p_tile(const ulonglong2 *__restrict__ shi,
                                          const ulonglong2 *__restrict__ slo,
                                          const unsigned long long *__restrict__ sg2, int cnt,
-                                         const float4 &ta, const float4 &tb,
+                                         const float4 &ta, const float4 &tb, const float4 &tc,
                                          const pfd::GaussParams &gp,
-                                         const pfd::GaussParams2 &gp2, float (&acc)[8]) {
-    if (TWO) {
-        const pfd::f32x2 txh = pfd::pack2(ta.x, tb.x), tyh = pfd::pack2(ta.y, tb.y);
-        const pfd::f32x2 txl = pfd::pack2(ta.z, tb.z), tyl = pfd::pack2(ta.w, tb.w);
-        for (int c0 = 0; c0 < cnt; c0 += 32) {
-            pfd::f32x2 nx = 0ull, ny = 0ull;  // +0.0f in both halves
+                                         const pfd::GaussParams2 &gp2, float (&acc)[12]) {
+    const pfd::f32x2 txh = pfd::pack2(ta.x, tb.x), tyh = pfd::pack2(ta.y, tb.y);
+    const pfd::f32x2 txl = pfd::pack2(ta.z, tb.z), tyl = pfd::pack2(ta.w, tb.w);
+    for (int c0 = 0; c0 < cnt; c0 += 32) {
+        pfd::f32x2 nx = 0ull, ny = 0ull;  // +0.0f in both halves
+        float pxa = 0.f, pya = 0.f, pxc = 0.f, pyc = 0.f;
 #pragma unroll 4
-            for (int k = 0; k < 32; ++k)
+        for (int k = 0; k < 32; ++k) {
+            if (NT >= 2) {
                 pfd::pair2(shi[c0 + k], slo[c0 + k], sg2[c0 + k], txh, tyh, txl, tyl, gp2, nx, ny);
+            } else {
+                scalar_pair(shi[c0 + k], slo[c0 + k], sg2[c0 + k], ta, gp, pxa, pya);
+            }
+            if (NT == 3) scalar_pair(shi[c0 + k], slo[c0 + k], sg2[c0 + k], tc, gp, pxc, pyc);
+        }
+        if (NT >= 2) {
             float nxa, nxb, nya, nyb;
             pfd::unpack2(nx, nxa, nxb);
             pfd::unpack2(ny, nya, nyb);
@@ -490,33 +518,18 @@ __device__ __forceinline__ void p2p_tile(const ulonglong2 *__restrict__ shi,
             pfd::comp_add(acc[2], acc[3], nya);
             pfd::comp_add(acc[4], acc[5], -nxb);
             pfd::comp_add(acc[6], acc[7], nyb);
-        }
-    } else {
-        for (int c0 = 0; c0 < cnt; c0 += 32) {
-            float pxa = 0.f, pya = 0.f;
-#pragma unroll 4
-            for (int k = 0; k < 32; ++k) {
-                const ulonglong2 h = shi[c0 + k], l = slo[c0 + k];
-                float sxh, syh, sxl, syl, g, dummy;
-                pfd::unpack2(h.x, sxh, dummy);
-                pfd::unpack2(h.y, syh, dummy);
-                pfd::unpack2(l.x, sxl, dummy);
-                pfd::unpack2(l.y, syl, dummy);
-                pfd::unpack2(sg2[c0 + k], g, dummy);
-                const float dx = (ta.x - sxh) + (ta.z - sxl);
-                const float dy = (ta.y - syh) + (ta.w - syl);
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
-                const float sc = pfd::gauss_s(r2, g, gp);
-                pxa = fmaf(-dy, sc, pxa);
-                pya = fmaf(dx, sc, pya);
-            }
+        } else {
             pfd::comp_add(acc[0], acc[1], pxa);
             pfd::comp_add(acc[2], acc[3], pya);
+        }
+        if (NT == 3) {
+            pfd::comp_add(acc[8], acc[9], pxc);
+            pfd::comp_add(acc[10], acc[11], pyc);
         }
     }
 }
 
-__global__ void __launch_bounds__(P2P_WARPS * 32)
+__global__ void __launch_bounds__(P2P_WARPS * 32, P2P_MIN_CTAS)
 k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *__restrict__ tcnt,
       const int32_t *__restrict__ sstart, const int32_t *__restrict__ scnt,
       const float4 *__restrict__ shl, const float *__restrict__ sg32,
@@ -538,13 +551,14 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
     if (tn == 0) return;
     const int r0 = run_off[b], r1 = run_off[b + 1];
     unsigned long long npairs = 0;
-    for (int tg = 0; tg < tn; tg += 64) {
-        const int ia = tg + lane, ib = tg + 32 + lane;
+    for (int tg = 0; tg < tn; tg += 96) {
+        const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane;
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 ta = (ia < tn) ? thl[t0 + ia] : z4;
         const float4 tb = (ib < tn) ? thl[t0 + ib] : z4;
-        const bool two = (tg + 32 < tn);  // warp-uniform
-        float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        const float4 tc = (ic < tn) ? thl[t0 + ic] : z4;
+        const int nt = (tn - tg <= 32) ? 1 : (tn - tg <= 64) ? 2 : 3;  // warp-uniform
+        float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         for (int rc = r0; rc < r1; rc += P2P_RUNS_SM) {
             const int nrc = min(P2P_RUNS_SM, r1 - rc);
             int pre = 0;
@@ -571,7 +585,7 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
             if (lane == 0) s_rp[wid][nrc] = pre;
             __syncwarp();
             const int S = pre;
-            npairs += (unsigned long long)S * (unsigned long long)min(64, tn - tg);
+            npairs += (unsigned long long)S * (unsigned long long)min(96, tn - tg);
             // each lane's two stream positions only move forward (by 64 per
             // tile), so the run holding them is found by advancing an index:
             // the largest r with prefix[r] <= p (empty runs are stepped over)
@@ -598,10 +612,12 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                 }
                 __syncwarp();
                 const int cnt = min(P2P_TILE, S - s0);
-                if (two)
-                    p2p_tile<true>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, gp, gp2, acc);
+                if (nt == 2)
+                    p2p_tile<2>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, tc, gp, gp2, acc);
+                else if (nt == 3)
+                    p2p_tile<3>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, tc, gp, gp2, acc);
                 else
-                    p2p_tile<false>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, gp, gp2, acc);
+                    p2p_tile<1>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, tc, gp, gp2, acc);
                 __syncwarp();
             }
         }
@@ -611,6 +627,9 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         if (ib < tn)
             nearv[t0 + ib] = make_double2(INV_2PI * ((double)acc[4] + (double)acc[5]),
                                           INV_2PI * ((double)acc[6] + (double)acc[7]));
+        if (ic < tn)
+            nearv[t0 + ic] = make_double2(INV_2PI * ((double)acc[8] + (double)acc[9]),
+                                          INV_2PI * ((double)acc[10] + (double)acc[11]));
     }
     if (lane == 0) atomicAdd(pairs, npairs);
 }

@@ -99,6 +99,19 @@ pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x, const dou
                           double ksigmasqr, double xopt, double cutoff, double tol,
                           int ndirect, double *vx, double *vy, void *stream);
 
+/* pf_velocity_fmm with the tree's bounding box given by the caller:
+ * box = {xmin, xmax, ymin, ymax} (host array) must contain every source and
+ * target (points outside are clamped into the edge leaves, which voids the
+ * error bound).  Skips the device bounding-box pass and its read-back, so the
+ * call never synchronises once the FMM plan for the box is cached (for
+ * resident blob sets whose box is known, e.g. a serving loop).  No NaN check.
+ * Results equal pf_velocity_fmm's when box is the exact bounding box. */
+pf_status pf_velocity_fmm_box(pf_ctx *ctx, int64_t n_src, const double *x, const double *y,
+                              const double *g, int64_t n_tgt, const double *xt, const double *yt,
+                              double ksigmasqr, double xopt, double cutoff, double tol,
+                              int ndirect, const double *box, double *vx, double *vy,
+                              void *stream);
+
 /* Tuning of the FMM for the calling host thread (0 = automatic):
  * leaf_level in [2, 11]; expansion_terms (p+1) in {16, 20, 24, 28, 32};
  * block_level_drop in [0, 2] (P2P blocks of 2^drop x 2^drop leaves).  The
@@ -239,6 +252,43 @@ pf_status pf_remesh_window_noalloc(int64_t n, const double *x, const double *y, 
                                    double *x_out, double *y_out, double *g_out, int64_t *ix_out,
                                    int64_t *iy_out, int64_t *n_out_dev, int32_t *status_dev,
                                    void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Population control: drop the blobs with |g| < thr, where thr starts at
+ * g_threshold_local and is divided by 10 (each division rounded, as the
+ * reference's loop) until the dropped circulation sum(|g|) is below
+ * g_threshold_global; the kept blobs keep their input order.  The threshold
+ * search runs on the device (FP64 sums in a fixed order; a dropped sum within
+ * rounding of g_threshold_global may be decided differently from numpy's
+ * pairwise sum).  g_threshold_global must be positive and finite (the
+ * reference loops forever otherwise).  Outputs hold n entries and must not
+ * alias the inputs; the DEVICE int64 *n_out_dev receives the kept count, the
+ * DEVICE double *threshold_dev (may be NULL) the threshold used.  No host
+ * synchronisation.
+ *
+ * Replaces PopulationControl (src/python/blobs/base/regrid/_regridding.py:
+ * 226-330), called from Blobs.populationControl
+ * (src/python/blobs/__blobsClass.py:783-825).
+ * ------------------------------------------------------------------------- */
+pf_status pf_population_control(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                                const double *g, double g_threshold_local,
+                                double g_threshold_global, double *x_out, double *y_out,
+                                double *g_out, int64_t *n_out_dev, double *threshold_dev,
+                                void *stream);
+
+/* pf_remesh followed by population control of the remeshed blobs in the same
+ * pass: the dropped cells are never emitted.  Results equal pf_remesh then
+ * pf_population_control on its output.  *threshold_used (host, may be NULL)
+ * receives the threshold used; *n_out and capacity as pf_remesh (capacity
+ * covers the kept blobs).  Replaces the redistribute + populationControl
+ * pair of Blobs.evolve (src/python/blobs/__blobsClass.py:768-781). */
+pf_status pf_remesh_population_control(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                                       const double *g, double h, double xb0, double yb0,
+                                       double c, double g_threshold_local,
+                                       double g_threshold_global, int64_t capacity,
+                                       double *x_out, double *y_out, double *g_out,
+                                       int64_t *ix_out, int64_t *iy_out, int64_t *n_out,
+                                       double *threshold_used, void *stream);
 
 /* ---------------------------------------------------------------------------
  * FP64 moments of a blob set, written to the DEVICE array out4:

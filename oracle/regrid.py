@@ -14,6 +14,8 @@ Follows ``src/python/blobs/base/regrid/_regridding.py:107-222`` step by step:
 
 The kernel-size half is the integer 2 (the reference is Python 2, where
 ``kernelSize/2`` is integer division).
+
+``population_control`` restates PopulationControl (same module, :316-330).
 """
 import numpy as np
 import scipy.sparse
@@ -65,3 +67,20 @@ def regrid(x, y, g, sigma, overlap, xbounds, ybounds, c=0.0):
     xn = ixn * h + 0.5 * h + xb0
     yn = iyn * h + 0.5 * h + yb0
     return xn, yn, gn, ixn, iyn
+
+
+def population_control(x, y, g, thr_local, thr_global):
+    """Drop blobs with |g| < thr, thr divided by 10 while the dropped
+    circulation sum(|g|) is not below thr_global (``_regridding.py:316-330``).
+    Returns (x, y, g, thr) of the kept blobs in input order."""
+    a = np.abs(np.asarray(g, dtype=np.float64))
+    thr = float(thr_local)
+    if not (np.isfinite(thr) and np.isfinite(thr_global) and thr_global > 0.0):
+        raise ValueError("thresholds must be finite and thr_global > 0")
+    while True:
+        flagged = a < thr
+        if a[flagged].sum() < thr_global:
+            break
+        thr /= 10.0
+    keep = ~flagged
+    return x[keep], y[keep], g[keep], thr

@@ -21,15 +21,7 @@
 
 #include "direct_api.cuh"
 #include "fmm_api.cuh"
-
-namespace pf {
-size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby);
-pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, const double *g,
-                      double h, double xb0, double yb0, double c, int32_t ixmin, int32_t iymin,
-                      int64_t nbx, int64_t nby, int64_t capacity, double *xo, double *yo,
-                      double *go, int64_t *ixo, int64_t *iyo, int32_t *total, int32_t *bad,
-                      cudaStream_t st);
-}
+#include "popctl.cuh"
 
 namespace {
 
@@ -77,6 +69,9 @@ struct pf_batch {
     pf::DirectInstance *d_dinst = nullptr;
     int2 *d_items = nullptr;
     int n_items = 0;
+    int2 *d_red_items = nullptr;  // (instance, tile) reductions of split instances
+    int n_red = 0;
+    float4 *d_part = nullptr;     // partial sums of all split instances
     int *d_counter = nullptr;
     int direct_grid = 0;
     int32_t *d_totals = nullptr, *d_bads = nullptr, *d_status = nullptr;
@@ -100,6 +95,8 @@ static void batch_free(pf_batch *b) {
     cudaFree(b->d_ctr);
     cudaFree(b->d_dinst);
     cudaFree(b->d_items);
+    cudaFree(b->d_red_items);
+    cudaFree(b->d_part);
     cudaFree(b->d_counter);
     cudaFree(b->d_totals);
     cudaFree(b->d_bads);
@@ -118,7 +115,10 @@ static pf_status batch_build(pf_batch *b, double tol) {
     b->nbx.assign(n, 0);
     b->nby.assign(n, 0);
     std::vector<Job> jobs;
-    std::vector<std::pair<double, int2>> items;  // cost, (inst, tile)
+    std::vector<std::pair<double, int2>> items;  // cost, (inst, tile * splits + segment)
+    std::vector<int2> red_items;                  // (inst, tile) of split instances
+    std::vector<std::pair<int, size_t>> part_off; // (inst, offset in float4) of split instances
+    size_t part_total = 0;
     std::vector<pf::DirectInstance> dinst(n);
     const int tile = pf::direct_tile_targets();
     for (int i = 0; i < n; ++i) {
@@ -154,16 +154,26 @@ static pf_status batch_build(pf_batch *b, double tol) {
         }
         b->method[i] = m;
         if (m == PF_DIRECT_METHOD && d.n > 0) {
+            const pf::DirectSplit sp = pf::direct_split(d.n, d.n);
             dinst[i] = {d.x, d.y, d.g, d.n, d.x, d.y, d.n, pfd::make_gauss_params(d.ksigmasqr),
-                        d.vx, d.vy};
+                        d.vx, d.vy, sp.splits, sp.seg, nullptr};
             const int64_t tiles = pf::ceil_div(d.n, tile);
-            for (int64_t t = 0; t < tiles; ++t)
-                items.push_back({(double)d.n * (double)std::min<int64_t>(tile, d.n - t * tile),
-                                 make_int2(i, (int)t)});
+            for (int64_t t = 0; t < tiles; ++t) {
+                const double tn = (double)std::min<int64_t>(tile, d.n - t * tile);
+                for (int k = 0; k < sp.splits; ++k) {
+                    const double sn = (double)std::min<int64_t>(sp.seg, d.n - k * sp.seg);
+                    items.push_back({sn * tn, make_int2(i, (int)(t * sp.splits + k))});
+                }
+                if (sp.splits > 1) red_items.push_back(make_int2(i, (int)t));
+            }
+            if (sp.splits > 1) {
+                part_off.push_back({i, part_total});
+                part_total += (size_t)sp.splits * (size_t)d.n;
+            }
             ++b->n_direct;
         } else {
             dinst[i] = {nullptr, nullptr, nullptr, 0, nullptr, nullptr, 0,
-                        pfd::make_gauss_params(1.0), nullptr, nullptr};
+                        pfd::make_gauss_params(1.0), nullptr, nullptr, 1, 1, nullptr};
         }
         if (d.remesh && d.n > 0) {
             b->ixmin[i] = left_index_host(d.box[0], d.xb0, d.h);
@@ -191,6 +201,15 @@ static pf_status batch_build(pf_batch *b, double tol) {
         PF_CUDA_TRY(cudaMalloc(&b->d_items, sizeof(int2) * std::max<size_t>(1, it.size())));
         if (!it.empty())
             PF_CUDA_TRY(cudaMemcpy(b->d_items, it.data(), sizeof(int2) * it.size(),
+                                   cudaMemcpyHostToDevice));
+        if (part_total > 0) {
+            PF_CUDA_TRY(cudaMalloc(&b->d_part, sizeof(float4) * part_total));
+            for (const auto &po : part_off) dinst[po.first].part = b->d_part + po.second;
+        }
+        b->n_red = (int)red_items.size();
+        PF_CUDA_TRY(cudaMalloc(&b->d_red_items, sizeof(int2) * std::max<size_t>(1, red_items.size())));
+        if (!red_items.empty())
+            PF_CUDA_TRY(cudaMemcpy(b->d_red_items, red_items.data(), sizeof(int2) * red_items.size(),
                                    cudaMemcpyHostToDevice));
         PF_CUDA_TRY(cudaMalloc(&b->d_dinst, sizeof(pf::DirectInstance) * std::max(1, n)));
         PF_CUDA_TRY(cudaMemcpy(b->d_dinst, dinst.data(), sizeof(pf::DirectInstance) * n,
@@ -243,8 +262,8 @@ static pf_status batch_enqueue(pf_batch *b) {
     PF_CUDA_TRY(cudaEventRecord(b->events[1], cap));
     for (int s = 0; s < S; ++s) PF_CUDA_TRY(cudaStreamWaitEvent(b->streams[s], b->events[1], 0));
     // the persistent direct kernel
-    PF_TRY(pf::launch_direct_batch(b->d_dinst, b->d_items, b->n_items, b->d_counter,
-                                   b->direct_grid, b->direct_stream));
+    PF_TRY(pf::launch_direct_batch(b->d_dinst, b->d_items, b->n_items, b->d_red_items, b->n_red,
+                                   b->d_counter, b->direct_grid, b->direct_stream));
     for (int s = 0; s < S; ++s) {
         cudaStream_t st = b->streams[s];
         for (const Job &j : b->slot_jobs[s]) {

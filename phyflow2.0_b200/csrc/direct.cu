@@ -1,11 +1,18 @@
 // direct.cu -- Gaussian-blob Biot-Savart velocity by direct summation.
 //
 // One simulation per launch (the plain path).  Each CTA owns DT_THREADS*TPT
-// targets (TPT per thread, coalesced); all CTAs stream the whole source set
-// through shared memory in tiles of DT_THREADS blobs, converted on load from
-// FP64 to hi/lo float pairs (so no scratch buffer is needed).  Per thread the
-// pair sums run in FP32 over chunks of 32 sources and are folded into a
-// TwoSum-compensated (hi, lo) accumulator after each chunk.
+// targets (TPT per thread, coalesced) and streams a range of sources through
+// shared memory in tiles of DT_THREADS blobs, converted on load from FP64 to
+// hi/lo float pairs.  Per thread the pair sums run in FP32 over chunks of 32
+// sources and are folded into a TwoSum-compensated (hi, lo) accumulator
+// after each chunk.
+//
+// Source splits: with fewer target tiles than DT_SPLIT_CTAS the sources are
+// cut into S contiguous segments (direct_split, a function of the two sizes
+// only), CTA (tile, s) writes its (hi, lo) pairs to a partial buffer, and
+// k_direct_reduce adds the S partials of each target in segment order in
+// FP64.  The batched kernel uses the same segments, so a blob set gets
+// bitwise the same velocities alone and in a batch.
 //
 // Replaces vv2par_kernel (src/cpp/blobs/cuda/vv2parGauss_gpu/
 // vv2parGauss_device.cu:107-162: FP64, one target per thread, 2 exp per pair,
@@ -13,25 +20,30 @@
 #include "direct_api.cuh"
 #include "gauss_pair.cuh"
 
+#include <algorithm>
+
 namespace {
 
 constexpr int DT_THREADS = 256;
 constexpr int DT_CHUNK = 32;
 constexpr double INV_2PI = 0.15915494309189535;  // 0.5/pi
+constexpr int64_t DT_TILE = DT_THREADS * 2;      // targets per CTA
 
 // One CTA computes the 2*DT_THREADS targets of tile `tile`: each thread owns
 // targets base and base + DT_THREADS and evaluates both against every source
 // with the packed f32x2 pair arithmetic (gauss_pair.cuh).
+// Sources [s_begin, s_end) only; with `part` non-null the (hi, lo) sums go to
+// part[split * nt + target] instead of the velocities.
 __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
                                             const double *__restrict__ ys,
-                                            const double *__restrict__ gs, int64_t ns,
-                                            const double *__restrict__ xt,
+                                            const double *__restrict__ gs, int64_t s_begin,
+                                            int64_t s_end, const double *__restrict__ xt,
                                             const double *__restrict__ yt, int64_t nt,
                                             const pfd::GaussParams &gp, double *__restrict__ vx,
-                                            double *__restrict__ vy, int64_t tile,
-                                            ulonglong2 *s_hi, ulonglong2 *s_lo,
-                                            unsigned long long *s_g2) {
-    const int64_t base = tile * (DT_THREADS * 2) + threadIdx.x;
+                                            double *__restrict__ vy, float4 *__restrict__ part,
+                                            int64_t split, int64_t tile, ulonglong2 *s_hi,
+                                            ulonglong2 *s_lo, unsigned long long *s_g2) {
+    const int64_t base = tile * DT_TILE + threadIdx.x;
     float th[2][4];
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
@@ -49,10 +61,10 @@ __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
     const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
-    for (int64_t t0 = 0; t0 < ns; t0 += DT_THREADS) {
+    for (int64_t t0 = s_begin; t0 < s_end; t0 += DT_THREADS) {
         const int64_t s = t0 + threadIdx.x;
         double x = 0.0, y = 0.0, g = 0.0;  // padding blobs carry g = 0
-        if (s < ns) {
+        if (s < s_end) {
             x = xs[s];
             y = ys[s];
             g = gs[s];
@@ -66,7 +78,7 @@ __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
         s_lo[threadIdx.x] = make_ulonglong2(pfd::pack2(xl, xl), pfd::pack2(yl, yl));
         s_g2[threadIdx.x] = pfd::pack2(gf, gf);
         __syncthreads();
-        const int nvalid = (int)min((int64_t)DT_THREADS, ns - t0);
+        const int nvalid = (int)min((int64_t)DT_THREADS, s_end - t0);
         for (int c0 = 0; c0 < nvalid; c0 += DT_CHUNK) {
             pfd::f32x2 nx = 0ull, ny = 0ull;
 #pragma unroll 4
@@ -85,31 +97,60 @@ __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
         const int64_t i = base + (int64_t)j * DT_THREADS;
-        if (i < nt) {
+        if (i >= nt) continue;
+        if (part) {
+            part[split * nt + i] = make_float4(acc[4 * j], acc[4 * j + 1], acc[4 * j + 2],
+                                               acc[4 * j + 3]);
+        } else {
             vx[i] = INV_2PI * ((double)acc[4 * j] + (double)acc[4 * j + 1]);
             vy[i] = INV_2PI * ((double)acc[4 * j + 2] + (double)acc[4 * j + 3]);
         }
     }
 }
 
+// v = 1/(2 pi) * sum over segments s = 0..S-1 of (hi_s + lo_s), in FP64.
+__device__ __forceinline__ void reduce_target(const float4 *__restrict__ part, int64_t nt,
+                                              int splits, int64_t i, double *__restrict__ vx,
+                                              double *__restrict__ vy) {
+    double sx = 0.0, sy = 0.0;
+    for (int s = 0; s < splits; ++s) {
+        const float4 p = part[(int64_t)s * nt + i];
+        sx += (double)p.x + (double)p.y;
+        sy += (double)p.z + (double)p.w;
+    }
+    vx[i] = INV_2PI * sx;
+    vy[i] = INV_2PI * sy;
+}
+
+__global__ void __launch_bounds__(DT_THREADS)
+k_direct_reduce(const float4 *__restrict__ part, int64_t nt, int splits, double *__restrict__ vx,
+                double *__restrict__ vy) {
+    const int64_t i = (int64_t)blockIdx.x * DT_THREADS + threadIdx.x;
+    if (i < nt) reduce_target(part, nt, splits, i, vx, vy);
+}
+
+// grid (target tiles, source segments); one segment = the plain sum.
 template <int TPT>
 __global__ void __launch_bounds__(DT_THREADS)
 k_direct_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
-               const double *__restrict__ gs, int64_t ns, const double *__restrict__ xt,
-               const double *__restrict__ yt, int64_t nt, pfd::GaussParams gp,
-               double *__restrict__ vx, double *__restrict__ vy) {
+               const double *__restrict__ gs, int64_t ns, int64_t seg,
+               const double *__restrict__ xt, const double *__restrict__ yt, int64_t nt,
+               pfd::GaussParams gp, double *__restrict__ vx, double *__restrict__ vy,
+               float4 *__restrict__ part) {
     static_assert(TPT == 2, "two targets per thread (packed pairs)");
     __shared__ ulonglong2 s_hi[DT_THREADS];  // {x_hi, x_hi}, {y_hi, y_hi}
     __shared__ ulonglong2 s_lo[DT_THREADS];  // {x_lo, x_lo}, {y_lo, y_lo}
     __shared__ unsigned long long s_g2[DT_THREADS];
-    direct_tile(xs, ys, gs, ns, xt, yt, nt, gp, vx, vy, blockIdx.x, s_hi, s_lo, s_g2);
+    const int64_t s0 = (int64_t)blockIdx.y * seg;
+    direct_tile(xs, ys, gs, s0, min(ns, s0 + seg), xt, yt, nt, gp, vx, vy, part, blockIdx.y,
+                blockIdx.x, s_hi, s_lo, s_g2);
 }
 
 // Persistent batched direct sum: CTAs take (instance, target tile) items from
 // a device counter until the list is exhausted.  Items are ordered by cost,
 // largest first; each item is computed by one CTA, so results do not depend
 // on which CTA takes it.
-__global__ void __launch_bounds__(DT_THREADS)
+__global__ void __launch_bounds__(DT_THREADS, 4)
 k_direct_batch(const pf::DirectInstance *__restrict__ inst, const int2 *__restrict__ items,
                int n_items, int *__restrict__ counter) {
     __shared__ ulonglong2 s_hi[DT_THREADS];
@@ -124,7 +165,23 @@ k_direct_batch(const pf::DirectInstance *__restrict__ inst, const int2 *__restri
         if (it >= n_items) break;
         const int2 w = items[it];
         const pf::DirectInstance d = inst[w.x];
-        direct_tile(d.x, d.y, d.g, d.n, d.xt, d.yt, d.nt, d.gp, d.vx, d.vy, w.y, s_hi, s_lo, s_g2);
+        const int64_t tile = w.y / d.splits, sp = w.y - tile * d.splits;
+        const int64_t s0 = sp * d.seg;
+        direct_tile(d.x, d.y, d.g, s0, min(d.n, s0 + d.seg), d.xt, d.yt, d.nt, d.gp, d.vx, d.vy,
+                    d.splits > 1 ? d.part : nullptr, sp, tile, s_hi, s_lo, s_g2);
+    }
+}
+
+// Batched reduction of split instances: one CTA per (instance, target tile).
+__global__ void __launch_bounds__(DT_THREADS)
+k_direct_reduce_batch(const pf::DirectInstance *__restrict__ inst,
+                      const int2 *__restrict__ items) {
+    const int2 w = items[blockIdx.x];
+    const pf::DirectInstance d = inst[w.x];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        const int64_t i = (int64_t)w.y * DT_TILE + j * DT_THREADS + threadIdx.x;
+        if (i < d.nt) reduce_target(d.part, d.nt, d.splits, i, d.vx, d.vy);
     }
 }
 
@@ -132,33 +189,61 @@ k_direct_batch(const pf::DirectInstance *__restrict__ inst, const int2 *__restri
 
 namespace pf {
 
+DirectSplit direct_split(int64_t ns, int64_t nt) {
+    const int64_t tiles = ceil_div(nt, DT_TILE);
+    if (tiles >= DT_SPLIT_CTAS || ns <= DT_SPLIT_MIN_SRC) return {1, ns > 0 ? ns : 1};
+    int64_t s = std::min(ceil_div(DT_SPLIT_CTAS, tiles), ceil_div(ns, DT_SPLIT_MIN_SRC));
+    s = std::min<int64_t>(s, DT_SPLIT_MAX);
+    const int64_t seg = ceil_div(ceil_div(ns, s), DT_THREADS) * DT_THREADS;
+    return {(int)ceil_div(ns, seg), seg};
+}
+
 // Launch the plain direct sum on `stream` (no argument checks; used internally
-// by the FMM's tol == 0 path and by the C-ABI entry below).
-pf_status launch_direct(int64_t ns, const double *x, const double *y, const double *g,
-                        int64_t nt, const double *xt, const double *yt, double ksigmasqr,
-                        double *vx, double *vy, cudaStream_t stream) {
+// by the FMM's tol == 0 path and by the C-ABI entry below).  Split launches
+// take their partial buffer from the context's arena.
+pf_status launch_direct(pf_ctx *ctx, int64_t ns, const double *x, const double *y,
+                        const double *g, int64_t nt, const double *xt, const double *yt,
+                        double ksigmasqr, double *vx, double *vy, cudaStream_t stream) {
     if (nt == 0) return PF_OK;
     const pfd::GaussParams gp = pfd::make_gauss_params(ksigmasqr);
     constexpr int TPT = 2;
-    const int64_t per = DT_THREADS * TPT;
-    const int64_t grid = ceil_div(nt, per);
+    const int64_t grid = ceil_div(nt, DT_TILE);
     if (grid > INT32_MAX) {
         set_error("pf_velocity_direct: too many targets (%lld)", (long long)nt);
         return PF_ERR_INVALID_ARG;
     }
-    k_direct_gauss<TPT><<<(unsigned)grid, DT_THREADS, 0, stream>>>(x, y, g, ns, xt, yt, nt, gp,
-                                                                   vx, vy);
-    return launch_status("k_direct_gauss");
+    const DirectSplit sp = direct_split(ns, nt);
+    float4 *part = nullptr;
+    if (sp.splits > 1) {
+        const size_t bytes = sizeof(float4) * (size_t)sp.splits * (size_t)nt;
+        PF_TRY(arena_reserve(ctx, bytes + 256));
+        part = static_cast<float4 *>(arena_take(ctx, bytes));
+        if (!part) {
+            set_error("pf_velocity_direct: scratch too small");
+            return PF_ERR_OOM;
+        }
+    }
+    k_direct_gauss<TPT><<<dim3((unsigned)grid, (unsigned)sp.splits), DT_THREADS, 0, stream>>>(
+        x, y, g, ns, sp.seg, xt, yt, nt, gp, vx, vy, part);
+    PF_TRY(launch_status("k_direct_gauss"));
+    if (!part) return PF_OK;
+    k_direct_reduce<<<(unsigned)ceil_div(nt, DT_THREADS), DT_THREADS, 0, stream>>>(part, nt,
+                                                                                 sp.splits, vx, vy);
+    return launch_status("k_direct_reduce");
 }
 
 int direct_tile_targets() { return DT_THREADS * 2; }
 
 pf_status launch_direct_batch(const DirectInstance *inst_dev, const int2 *items_dev, int n_items,
-                              int *counter_dev, int grid, cudaStream_t st) {
+                              const int2 *reduce_items_dev, int n_reduce, int *counter_dev,
+                              int grid, cudaStream_t st) {
     PF_CUDA_TRY(cudaMemsetAsync(counter_dev, 0, sizeof(int), st));
     if (n_items == 0) return PF_OK;
     k_direct_batch<<<grid, DT_THREADS, 0, st>>>(inst_dev, items_dev, n_items, counter_dev);
-    return launch_status("k_direct_batch");
+    PF_TRY(launch_status("k_direct_batch"));
+    if (n_reduce == 0) return PF_OK;
+    k_direct_reduce_batch<<<n_reduce, DT_THREADS, 0, st>>>(inst_dev, reduce_items_dev);
+    return launch_status("k_direct_reduce_batch");
 }
 
 int direct_batch_grid(int num_sms) {
@@ -190,5 +275,5 @@ extern "C" pf_status pf_velocity_direct(pf_ctx *ctx, int64_t n_src, const double
         PF_CUDA_TRY(cudaMemsetAsync(vy, 0, sizeof(double) * n_tgt, st));
         return PF_OK;
     }
-    return pf::launch_direct(n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
+    return pf::launch_direct(ctx, n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
 }

@@ -41,11 +41,7 @@
 #include "gauss_pair.cuh"
 #include "scan.cuh"
 
-namespace pf {
-pf_status launch_direct(int64_t ns, const double *x, const double *y, const double *g,
-                        int64_t nt, const double *xt, const double *yt, double ksigmasqr,
-                        double *vx, double *vy, cudaStream_t stream);
-}
+#include "direct_api.cuh"
 
 namespace {
 
@@ -1158,12 +1154,15 @@ extern "C" pf_status pf_fmm_tree_keys(pf_ctx *ctx, int64_t n, const double *x, c
     return pf::launch_status("k_leaf_keys");
 }
 
-extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x, const double *y,
-                                     const double *g, int64_t n_tgt, const double *xt,
-                                     const double *yt, double ksigmasqr, double xopt,
-                                     double cutoff, double tol, int ndirect, double *vx,
-                                     double *vy, void *stream) {
-    pf::clear_error();
+namespace {
+
+// pf_velocity_fmm (box == nullptr: bounding box of sources and targets read
+// back from the device, one synchronisation) and pf_velocity_fmm_box (box
+// given by the caller, no synchronisation).
+pf_status velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x, const double *y,
+                       const double *g, int64_t n_tgt, const double *xt, const double *yt,
+                       double ksigmasqr, double cutoff, double tol, int ndirect, double *vx,
+                       double *vy, const double *box, void *stream) {
     PF_CHECK_ARG(ctx != nullptr, "pf_velocity_fmm: NULL context");
     PF_CHECK_ARG(n_src >= 0 && n_tgt >= 0 && n_src < ((int64_t)1 << 31) &&
                      n_tgt < ((int64_t)1 << 31),
@@ -1173,7 +1172,9 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
     PF_CHECK_ARG(tol >= 0.0 && tol < 1.0, "pf_velocity_fmm: tol must be in [0, 1)");
     PF_CHECK_ARG(n_src == 0 || (x && y && g), "pf_velocity_fmm: NULL blob array");
     PF_CHECK_ARG(n_tgt == 0 || (xt && yt && vx && vy), "pf_velocity_fmm: NULL target array");
-    (void)xopt;
+    PF_CHECK_ARG(!box || (std::isfinite(box[0]) && std::isfinite(box[1]) && std::isfinite(box[2]) &&
+                          std::isfinite(box[3]) && box[0] <= box[1] && box[2] <= box[3]),
+                 "pf_velocity_fmm_box: box must be finite with min <= max");
     pf::DeviceGuard dg(ctx->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     ctx->last_stream = st;
@@ -1193,33 +1194,45 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
     int L = pf::g_tune.leaf_level;
     if (L == 0) L = pf::fmmx::auto_level(n_src, ndirect);
     if (tol == 0.0 || L < 3)
-        return pf::launch_direct(n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
+        return pf::launch_direct(ctx, n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
     const int np = pf::g_tune.np ? pf::g_tune.np : pf::fmmx::np_for_tol(tol);
     int kb = pf::g_tune.kb;
 
     // bounding square of sources and targets
-    PF_TRY(pf::arena_reserve(ctx, 4096));
-    BBox *bb = static_cast<BBox *>(pf::arena_take(ctx, sizeof(BBox)));
-    k_bbox_init<<<1, 1, 0, st>>>(bb);
-    PF_TRY(pf::launch_status("k_bbox_init"));
-    const int cap = ctx->num_sms * 4;
-    k_bbox<<<(unsigned)std::min<int64_t>(pf::ceil_div(n_src, 256), cap), 256, 0, st>>>(x, y, n_src, bb);
-    PF_TRY(pf::launch_status("k_bbox"));
-    if (!(xt == x && yt == y)) {
-        k_bbox<<<(unsigned)std::min<int64_t>(pf::ceil_div(n_tgt, 256), cap), 256, 0, st>>>(xt, yt,
-                                                                                      n_tgt, bb);
+    double xmin, xmax, ymin, ymax;
+    if (box) {
+        xmin = box[0];
+        xmax = box[1];
+        ymin = box[2];
+        ymax = box[3];
+    } else {
+        PF_TRY(pf::arena_reserve(ctx, 4096));
+        BBox *bb = static_cast<BBox *>(pf::arena_take(ctx, sizeof(BBox)));
+        k_bbox_init<<<1, 1, 0, st>>>(bb);
+        PF_TRY(pf::launch_status("k_bbox_init"));
+        const int cap = ctx->num_sms * 4;
+        k_bbox<<<(unsigned)std::min<int64_t>(pf::ceil_div(n_src, 256), cap), 256, 0, st>>>(
+            x, y, n_src, bb);
         PF_TRY(pf::launch_status("k_bbox"));
+        if (!(xt == x && yt == y)) {
+            k_bbox<<<(unsigned)std::min<int64_t>(pf::ceil_div(n_tgt, 256), cap), 256, 0, st>>>(
+                xt, yt, n_tgt, bb);
+            PF_TRY(pf::launch_status("k_bbox"));
+        }
+        BBox hb;
+        PF_CUDA_TRY(
+            cudaMemcpyAsync(ctx->host_small, bb, sizeof(BBox), cudaMemcpyDeviceToHost, st));
+        PF_CUDA_TRY(cudaStreamSynchronize(st));
+        memcpy(&hb, ctx->host_small, sizeof(BBox));
+        if (hb.bad) {
+            pf::set_error("pf_velocity_fmm: NaN or Inf coordinate");
+            return PF_ERR_NAN_INPUT;
+        }
+        xmin = unord_d(hb.mnx);
+        xmax = unord_d(hb.mxx);
+        ymin = unord_d(hb.mny);
+        ymax = unord_d(hb.mxy);
     }
-    BBox hb;
-    PF_CUDA_TRY(cudaMemcpyAsync(ctx->host_small, bb, sizeof(BBox), cudaMemcpyDeviceToHost, st));
-    PF_CUDA_TRY(cudaStreamSynchronize(st));
-    memcpy(&hb, ctx->host_small, sizeof(BBox));
-    if (hb.bad) {
-        pf::set_error("pf_velocity_fmm: NaN or Inf coordinate");
-        return PF_ERR_NAN_INPUT;
-    }
-    const double xmin = unord_d(hb.mnx), xmax = unord_d(hb.mxx);
-    const double ymin = unord_d(hb.mny), ymax = unord_d(hb.mxy);
     double w0 = std::max(xmax - xmin, ymax - ymin);
     if (!(w0 > 0.0)) w0 = 1.0;
     w0 *= 1.0 + 1e-9;
@@ -1228,7 +1241,7 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
     for (;;) {
         PF_TRY(pf::shared_plan(ctx->device, L, kb, np, cutoff / w0, &cache));
         if (cache->nqp <= P2P_QMAX) break;
-        if (L <= 3) return pf::launch_direct(n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
+        if (L <= 3) return pf::launch_direct(ctx, n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
         --L;  // cutoff too large for this leaf width: coarser leaves
     }
     ctx->fmm_plan_hold = cache;  // keep the plan alive while this call's kernels run
@@ -1243,6 +1256,32 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
     return pf::fmm_exec(*cache, xmin, ymin, w0, sc, a,
                         reinterpret_cast<unsigned long long *>(ctx->dev_small),
                         ctx->fmm_profile ? ctx->ev : nullptr, st);
+}
+
+}  // namespace
+
+extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x, const double *y,
+                                     const double *g, int64_t n_tgt, const double *xt,
+                                     const double *yt, double ksigmasqr, double xopt,
+                                     double cutoff, double tol, int ndirect, double *vx,
+                                     double *vy, void *stream) {
+    pf::clear_error();
+    (void)xopt;
+    return velocity_fmm(ctx, n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, cutoff, tol, ndirect, vx,
+                        vy, nullptr, stream);
+}
+
+extern "C" pf_status pf_velocity_fmm_box(pf_ctx *ctx, int64_t n_src, const double *x,
+                                         const double *y, const double *g, int64_t n_tgt,
+                                         const double *xt, const double *yt, double ksigmasqr,
+                                         double xopt, double cutoff, double tol, int ndirect,
+                                         const double *box, double *vx, double *vy,
+                                         void *stream) {
+    pf::clear_error();
+    (void)xopt;
+    PF_CHECK_ARG(box != nullptr, "pf_velocity_fmm_box: NULL box");
+    return velocity_fmm(ctx, n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, cutoff, tol, ndirect, vx,
+                        vy, box, stream);
 }
 
 extern "C" pf_status pf_fmm_profile(pf_ctx *ctx, int enable) {

@@ -20,12 +20,15 @@
 //      (wx_a wy_b) g over the blobs of the 16 base cells whose windows cover it,
 //      and flags cells touched by at least one window (explicit zeros are
 //      kept, like the CSR sum of the reference, _regridding.py:200-202).
+//   6b. (pf_remesh_population_control only) PopulationControl of the cell
+//      values (popctl.cu), which clears the flags of the dropped cells.
 //   7. scan of the flags -> output slots, in (ix, iy) order.
 //   8. k_rm_emit   : x = ix*h + 0.5h + xb0 (same order as :217-218), g, ix, iy.
 // No floating-point atomics: each output value is produced by one thread.
 #include <cmath>
 #include <cstring>
 
+#include "popctl.cuh"
 #include "scan.cuh"
 
 namespace {
@@ -301,7 +304,7 @@ size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby) {
     const int64_t big = ncell > nbase ? ncell : nbase;
     return align256(4 * n) * 3 + align256(sizeof(W9) * n) + 2 * align256(4 * nbase) +
            align256(8 * ncell) + 2 * align256(4 * ncell) + align256(4 * scan_tmp_ints(big)) +
-           3 * align256(16) + 1024;
+           3 * align256(16) + align256(sizeof(PcState)) + popctl_scratch_bytes() + 1024;
 }
 
 // Everything after the window is known; no host synchronisation.  total_dev
@@ -311,7 +314,7 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
                       double h, double xb0, double yb0, double c, int32_t ixmin, int32_t iymin,
                       int64_t nbx, int64_t nby, int64_t capacity, double *xo, double *yo,
                       double *go, int64_t *ixo, int64_t *iyo, int32_t *total, int32_t *bad,
-                      cudaStream_t st) {
+                      cudaStream_t st, const PopCtlArgs *pc) {
     const int64_t nbase = nbx * nby, ncell = (nbx + 3) * (nby + 3);
     const int64_t big = ncell > nbase ? ncell : nbase;
     int32_t *cell = (int32_t *)sc.take(4 * n);
@@ -347,6 +350,10 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     k_rm_gather<<<(unsigned)ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(nbx, nby, start,
                                                                              count, w, acc, flag);
     PF_TRY(launch_status("k_rm_gather"));
+    if (pc) {
+        PF_TRY(popctl_decide(sc, ncell, acc, flag, *pc, st));
+        PF_TRY(popctl_flags(ncell, acc, flag, pc->state, flag, st));
+    }
     PF_TRY(exclusive_scan_i32(flag, slot, ncell, tmp, total, st));
     k_rm_emit<<<(unsigned)ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(
         ncell, nby + 3, ixmin, iymin, h, h05, xb0, yb0, flag, slot, acc, total, capacity, xo, yo,
@@ -356,11 +363,16 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
 
 }  // namespace pf
 
-extern "C" pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const double *y,
-                               const double *g, double h, double xb0, double yb0, double c,
-                               int64_t capacity, double *x_out, double *y_out, double *g_out,
-                               int64_t *ix_out, int64_t *iy_out, int64_t *n_out, void *stream) {
-    pf::clear_error();
+namespace {
+
+// pf_remesh and pf_remesh_population_control: window from the blobs (one
+// synchronisation), remesh, optional population control of the cells
+// (popctl = {gThresholdLocal, gThresholdGlobal}), output count read back.
+pf_status remesh_sync(pf_ctx *ctx, int64_t n, const double *x, const double *y, const double *g,
+                      double h, double xb0, double yb0, double c, int64_t capacity,
+                      double *x_out, double *y_out, double *g_out, int64_t *ix_out,
+                      int64_t *iy_out, int64_t *n_out, const double *popctl, double *thr_used,
+                      void *stream) {
     PF_CHECK_ARG(ctx != nullptr, "pf_remesh: NULL context");
     PF_CHECK_ARG(n_out != nullptr, "pf_remesh: n_out is NULL");
     *n_out = 0;
@@ -411,19 +423,53 @@ extern "C" pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const do
     pf::Bump sc{ctx->arena.base, ctx->arena.cap, 0};
     int32_t *total = (int32_t *)sc.take(16);
     int32_t *bad = (int32_t *)sc.take(16);
+    pf::PcState *state = (pf::PcState *)sc.take(sizeof(pf::PcState));
     PF_CUDA_TRY(cudaMemsetAsync(bad, 0, 4, st));
+    pf::PopCtlArgs pc{popctl ? popctl[0] : 0.0, popctl ? popctl[1] : 0.0, state};
     PF_TRY(pf::remesh_core(sc, n, x, y, g, h, xb0, yb0, c, he.ixmin, he.iymin, nbx, nby, capacity,
-                           x_out, y_out, g_out, ix_out, iy_out, total, bad, st));
+                           x_out, y_out, g_out, ix_out, iy_out, total, bad, st,
+                           popctl ? &pc : nullptr));
     PF_CUDA_TRY(cudaMemcpyAsync(ctx->host_small, total, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    if (popctl)
+        PF_CUDA_TRY(cudaMemcpyAsync(ctx->host_small + 1, &state->thr, sizeof(double),
+                                    cudaMemcpyDeviceToHost, st));
     PF_CUDA_TRY(cudaStreamSynchronize(st));
     const int64_t nout = *reinterpret_cast<int32_t *>(ctx->host_small);
     *n_out = nout;
+    if (popctl && thr_used) memcpy(thr_used, ctx->host_small + 1, sizeof(double));
     if (nout > capacity) {
         pf::set_error("pf_remesh: output needs %lld entries, capacity is %lld", (long long)nout,
                       (long long)capacity);
         return PF_ERR_CAPACITY;
     }
     return PF_OK;
+}
+
+}  // namespace
+
+extern "C" pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                               const double *g, double h, double xb0, double yb0, double c,
+                               int64_t capacity, double *x_out, double *y_out, double *g_out,
+                               int64_t *ix_out, int64_t *iy_out, int64_t *n_out, void *stream) {
+    pf::clear_error();
+    return remesh_sync(ctx, n, x, y, g, h, xb0, yb0, c, capacity, x_out, y_out, g_out, ix_out,
+                       iy_out, n_out, nullptr, nullptr, stream);
+}
+
+extern "C" pf_status pf_remesh_population_control(
+    pf_ctx *ctx, int64_t n, const double *x, const double *y, const double *g, double h,
+    double xb0, double yb0, double c, double g_threshold_local, double g_threshold_global,
+    int64_t capacity, double *x_out, double *y_out, double *g_out, int64_t *ix_out,
+    int64_t *iy_out, int64_t *n_out, double *threshold_used, void *stream) {
+    pf::clear_error();
+    PF_CHECK_ARG(n_out != nullptr, "pf_remesh_population_control: n_out is NULL");
+    *n_out = 0;
+    PF_TRY(pf::popctl_check(g_threshold_local, g_threshold_global,
+                            "pf_remesh_population_control"));
+    const double pc[2] = {g_threshold_local, g_threshold_global};
+    if (threshold_used) *threshold_used = g_threshold_local;
+    return remesh_sync(ctx, n, x, y, g, h, xb0, yb0, c, capacity, x_out, y_out, g_out, ix_out,
+                       iy_out, n_out, pc, threshold_used, stream);
 }
 
 extern "C" pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, const double *y,

@@ -14,16 +14,7 @@
 // same as pf_remesh_window's for the same window.
 #include <mutex>
 
-#include "pf_common.cuh"
-
-namespace pf {
-size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby);
-pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, const double *g,
-                      double h, double xb0, double yb0, double c, int32_t ixmin, int32_t iymin,
-                      int64_t nbx, int64_t nby, int64_t capacity, double *xo, double *yo,
-                      double *go, int64_t *ixo, int64_t *iyo, int32_t *total, int32_t *bad,
-                      cudaStream_t st);
-}
+#include "popctl.cuh"
 
 namespace {
 

@@ -40,11 +40,17 @@ PROTOTYPES = {
     "pf_velocity_direct": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _vp, _vp, _vp],
     "pf_velocity_fmm": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _int,
                         _vp, _vp, _vp],
+    "pf_velocity_fmm_box": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _dbl, _dbl, _dbl,
+                            _int, _c.POINTER(_dbl), _vp, _vp, _vp],
     "pf_panel_velocity": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp,
                           _int, _vp],
     "pf_remesh": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp, _vp, _vp,
                   _c.POINTER(_i64), _vp],
     "pf_moments": [_vp, _i64, _vp, _vp, _vp, _vp, _vp],
+    "pf_population_control": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pf_remesh_population_control": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl,
+                                     _i64, _vp, _vp, _vp, _vp, _vp, _c.POINTER(_i64),
+                                     _c.POINTER(_dbl), _vp],
     "pf_remesh_window": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _i64, _i64,
                          _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "pf_remesh_window_noalloc": [_i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _i64,

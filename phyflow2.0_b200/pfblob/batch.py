@@ -47,7 +47,7 @@ class Batch:
             if methods is not None:
                 m, L = int(methods[i]), int(leaf_levels[i]) if leaf_levels is not None else 0
             else:
-                m, L = self.tuner.choose(n, ks, box, tol, cutoff)
+                m, L = self.tuner.choose(n, ks, box, tol, cutoff, batch=True)
             vx = torch.empty(n, dtype=torch.float64, device=self.device)
             vy = torch.empty(n, dtype=torch.float64, device=self.device)
             d = descs[i]

@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from .induced import DIRECT_METHOD, FMM_METHOD, fmm_parameters, velocity_device
-from .regrid import remesh_device
+from .regrid import population_control_device, remesh_device
 
 default_diffusion_params = {'method': 'regrid_wee', 'c2': 'optimized'}
 default_time_integration_params = {'method': 'rk4'}
@@ -104,10 +104,18 @@ class Blobs:
                         cutoff=cut, tol=tol, ndirect=Ndirect)
         return vx, vy
 
-    def _regrid(self, c):
-        h = self.h
-        self._x, self._y, self._g = remesh_device(self._x, self._y, self._g, h, -1.5 * h,
-                                                  -1.5 * h, c)
+    def _regrid(self, c, population_control=False):
+        # The reference passes (sigma, overlap) to Regrid, which remeshes with
+        # h = sigma*overlap (_regridding.py:118), and bounds -1.5 h from the
+        # stored h (__blobsClass.py:891-892); the two can differ in the last bit.
+        h = self.sigma * self.overlap
+        b0 = -1.5 * self.h
+        if population_control:
+            self._x, self._y, self._g, _ = remesh_device(
+                self._x, self._y, self._g, h, b0, b0, c,
+                population_control=(self.gThresholdLocal, self.gThresholdGlobal))
+        else:
+            self._x, self._y, self._g = remesh_device(self._x, self._y, self._g, h, b0, b0, c)
 
     # -- hot-path methods ---------------------------------------------------------
     def evaluateVelocity(self, xEval=None, yEval=None, Ndirect=35, tol=1.0e-6, cutoff=None):
@@ -132,17 +140,10 @@ class Blobs:
     def populationControl(self):
         """Drop blobs with |g| below gThresholdLocal while the dropped
         circulation stays below gThresholdGlobal (threshold /10 otherwise),
-        as PopulationControl (_regridding.py:227-330)."""
-        thr = float(self.blobControlParams['gThresholdLocal'])
-        tot = float(self.blobControlParams['gThresholdGlobal'])
-        a = self._g.abs()
-        while True:
-            flag = a < thr
-            if float(a[flag].sum()) < tot:
-                break
-            thr /= 10.0
-        keep = ~flag
-        self._x, self._y, self._g = self._x[keep], self._y[keep], self._g[keep]
+        as PopulationControl (_regridding.py:227-330), on the device
+        (pf_population_control)."""
+        self._x, self._y, self._g, _ = population_control_device(
+            self._x, self._y, self._g, self.gThresholdLocal, self.gThresholdGlobal)
 
     def evolve(self):
         """One time step: convection (FE or the reference's RK4), Wee diffusion
@@ -166,11 +167,19 @@ class Blobs:
         self._x, self._y = xn, yn
         if self.stepDiffusion != 0 and (self.tStep % self.stepDiffusion) == 0:
             self._regrid(math.sqrt(self.nu * self.deltaTd) / self.h)
-        if self.stepRedistribution != 0 and (self.tStep % self.stepRedistribution) == 0:
+        redistribute = self.stepRedistribution != 0 and (self.tStep % self.stepRedistribution) == 0
+        control = (self.stepPopulationControl != 0 and
+                   ((self.tStep + 1) % self.stepPopulationControl) == 0)
+        # redistribution followed by population control (after the time
+        # advance, which does not touch the blobs) runs as one fused remesh
+        fused = redistribute and control and self.numBlobs > 0
+        if fused:
+            self._regrid(0.0, population_control=True)
+        elif redistribute:
             self.redistribute()
         self.tStep += 1
         self.t += self.deltaTc
-        if self.stepPopulationControl != 0 and (self.tStep % self.stepPopulationControl) == 0:
+        if control and not fused:
             self.populationControl()
 
     def addBlobs(self, xNew, yNew, gNew):

@@ -41,8 +41,10 @@ def fmm_parameters(sigma, k=2.0, cutoff=None):
 
 
 def velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=DIRECT_METHOD, xopt=None,
-                    cutoff=None, tol=1e-6, ndirect=35, stream=None, device=None):
-    """Device-tensor entry: all arguments CUDA float64 tensors; writes vx, vy."""
+                    cutoff=None, tol=1e-6, ndirect=35, stream=None, device=None, box=None):
+    """Device-tensor entry: all arguments CUDA float64 tensors; writes vx, vy.
+    ``box = (xmin, xmax, ymin, ymax)`` containing all sources and targets lets
+    the FMM skip its bounding-box read-back (pf_velocity_fmm_box)."""
     dev = x.device.index if device is None else device
     st = ctypes.c_void_p(torch.cuda.current_stream(x.device).cuda_stream if stream is None
                          else stream)
@@ -56,10 +58,18 @@ def velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=DIRECT_METHOD, xo
             xopt = math.sqrt(FMM_ALPHA * ksigmasqr)
         if cutoff is None:
             cutoff = 5.0 * xopt
-        _lib.check(_lib.lib.pf_velocity_fmm(ctx, x.numel(), ptr(x), ptr(y), ptr(g), xt.numel(),
-                                            ptr(xt), ptr(yt), float(ksigmasqr), float(xopt),
-                                            float(cutoff), float(tol), int(ndirect), ptr(vx),
-                                            ptr(vy), st))
+        if box is None:
+            _lib.check(_lib.lib.pf_velocity_fmm(ctx, x.numel(), ptr(x), ptr(y), ptr(g),
+                                                xt.numel(), ptr(xt), ptr(yt), float(ksigmasqr),
+                                                float(xopt), float(cutoff), float(tol),
+                                                int(ndirect), ptr(vx), ptr(vy), st))
+        else:
+            b = (ctypes.c_double * 4)(*[float(v) for v in box])
+            _lib.check(_lib.lib.pf_velocity_fmm_box(ctx, x.numel(), ptr(x), ptr(y), ptr(g),
+                                                    xt.numel(), ptr(xt), ptr(yt),
+                                                    float(ksigmasqr), float(xopt), float(cutoff),
+                                                    float(tol), int(ndirect), b, ptr(vx),
+                                                    ptr(vy), st))
 
 
 def velocity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None, hardware=0,

@@ -1,6 +1,7 @@
 """M4' remesh with pHyFlow's ``Regrid`` call surface
 (``src/python/blobs/base/regrid/_regridding.py:36-222``)."""
 import ctypes
+import math
 
 import numpy as np
 import torch
@@ -11,11 +12,14 @@ from ._arrays import Marshal, ptr
 M4PRIME_INTERPKERNEL = 0
 
 
-def remesh_device(x, y, g, h, xb0, yb0, c=0.0, capacity=None, with_indices=False, stream=None):
+def remesh_device(x, y, g, h, xb0, yb0, c=0.0, capacity=None, with_indices=False, stream=None,
+                  population_control=None):
     """Device-tensor entry.  Returns (x, y, g[, ix, iy]) CUDA tensors of the
     new blobs in (ix, iy) order.  ``capacity`` bounds the output (default
     16 n, the window count); a retry with the exact size follows a capacity
-    error."""
+    error.  ``population_control = (gThresholdLocal, gThresholdGlobal)``
+    applies PopulationControl to the new blobs in the same pass (dropped cells
+    are never written); the threshold used is then appended to the result."""
     n = x.numel()
     dev = x.device
     st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
@@ -29,9 +33,17 @@ def remesh_device(x, y, g, h, xb0, yb0, c=0.0, capacity=None, with_indices=False
         ixo = torch.empty(capacity, dtype=torch.int64, device=dev) if with_indices else None
         iyo = torch.empty(capacity, dtype=torch.int64, device=dev) if with_indices else None
         nout = ctypes.c_int64(0)
-        s = _lib.lib.pf_remesh(ctx, n, ptr(x), ptr(y), ptr(g), float(h), float(xb0), float(yb0),
-                               float(c), capacity, ptr(xo), ptr(yo), ptr(go), ptr(ixo), ptr(iyo),
-                               ctypes.byref(nout), st)
+        thr = ctypes.c_double(0.0)
+        if population_control is None:
+            s = _lib.lib.pf_remesh(ctx, n, ptr(x), ptr(y), ptr(g), float(h), float(xb0),
+                                   float(yb0), float(c), capacity, ptr(xo), ptr(yo), ptr(go),
+                                   ptr(ixo), ptr(iyo), ctypes.byref(nout), st)
+        else:
+            tl, tg = population_control
+            s = _lib.lib.pf_remesh_population_control(
+                ctx, n, ptr(x), ptr(y), ptr(g), float(h), float(xb0), float(yb0), float(c),
+                float(tl), float(tg), capacity, ptr(xo), ptr(yo), ptr(go), ptr(ixo), ptr(iyo),
+                ctypes.byref(nout), ctypes.byref(thr), st)
         if s == 6 and nout.value > capacity:  # PF_ERR_CAPACITY
             capacity = nout.value
             continue
@@ -40,7 +52,77 @@ def remesh_device(x, y, g, h, xb0, yb0, c=0.0, capacity=None, with_indices=False
         out = (xo[:k], yo[:k], go[:k])
         if with_indices:
             out = out + (ixo[:k], iyo[:k])
+        if population_control is not None:
+            out = out + (thr.value,)
         return out
+
+
+def lattice_window(box, h, xb0, yb0):
+    """Base-cell window (ixmin, iymin, nbx, nby) holding every blob inside
+    box = (xmin, xmax, ymin, ymax): the remesh's window-left index
+    ceil((((x - xb0) - 2h) + h/2) / h) - 1 (same rounding as the device) of
+    the box corners."""
+    h2, h05 = 2.0 * h, 0.5 * h
+
+    def left(v, b0):
+        return math.ceil((((v - b0) - h2) + h05) / h) - 1
+
+    ix0, ix1 = left(box[0], xb0), left(box[1], xb0)
+    iy0, iy1 = left(box[2], yb0), left(box[3], yb0)
+    return ix0, iy0, ix1 - ix0 + 1, iy1 - iy0 + 1
+
+
+def remesh_window_device(x, y, g, h, xb0, yb0, window, c=0.0, stream=None):
+    """Remesh onto a known base-cell window (pf_remesh_window): no host
+    synchronisation.  Returns (x, y, g, n_out) where the outputs hold the
+    window's (nbx+3)(nby+3) cells and n_out is a 1-element CUDA int64 tensor
+    with the number of new blobs (the first n_out entries)."""
+    n = x.numel()
+    dev = x.device
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
+    ctx = _lib.context(dev.index)
+    ixmin, iymin, nbx, nby = (int(v) for v in window)
+    cap = (nbx + 3) * (nby + 3)
+    xo = torch.empty(cap, dtype=torch.float64, device=dev)
+    yo = torch.empty(cap, dtype=torch.float64, device=dev)
+    go = torch.empty(cap, dtype=torch.float64, device=dev)
+    nout = torch.zeros(1, dtype=torch.int64, device=dev)
+    _lib.check(_lib.lib.pf_remesh_window(ctx, n, ptr(x), ptr(y), ptr(g), float(h), float(xb0),
+                                         float(yb0), float(c), ixmin, iymin, nbx, nby, cap,
+                                         ptr(xo), ptr(yo), ptr(go), None, None, ptr(nout), None,
+                                         st))
+    return xo, yo, go, nout
+
+
+def population_control_device(x, y, g, g_threshold_local, g_threshold_global, stream=None):
+    """PopulationControl of device tensors: returns (x, y, g, threshold used)
+    with the kept blobs in input order (reads the kept count back: one
+    synchronisation)."""
+    n = x.numel()
+    dev = x.device
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
+    ctx = _lib.context(dev.index)
+    xo = torch.empty(n, dtype=torch.float64, device=dev)
+    yo = torch.empty(n, dtype=torch.float64, device=dev)
+    go = torch.empty(n, dtype=torch.float64, device=dev)
+    res = torch.empty(2, dtype=torch.float64, device=dev)  # [n_out (int64 bits), threshold]
+    _lib.check(_lib.lib.pf_population_control(
+        ctx, n, ptr(x), ptr(y), ptr(g), float(g_threshold_local), float(g_threshold_global),
+        ptr(xo), ptr(yo), ptr(go), ptr(res), res.data_ptr() + 8, st))
+    r = res.cpu()
+    k = int(r[:1].view(torch.int64).item())
+    return xo[:k], yo[:k], go[:k], float(r[1].item())
+
+
+def PopulationControl(xBlob, yBlob, wBlob, wThreshold, wTotalThreshold):
+    """Drop blobs with |g| below wThreshold, lowering the threshold by decades
+    until the dropped circulation is below wTotalThreshold; same arguments and
+    results as pHyFlow's ``PopulationControl``
+    (``src/python/blobs/base/regrid/_regridding.py:226-330``)."""
+    m = Marshal(xBlob.device.index if isinstance(xBlob, torch.Tensor) and xBlob.is_cuda else None)
+    x, y, g = m.dev(xBlob), m.dev(yBlob), m.dev(wBlob)
+    xn, yn, gn, _ = population_control_device(x, y, g, wThreshold, wTotalThreshold)
+    return m.out(xn), m.out(yn), m.out(gn)
 
 
 def Regrid(xBlob, yBlob, wBlob, sigma, overlap, xBounds, yBounds, interpKernel=0, c=0.0):

@@ -30,13 +30,14 @@ import torch
 
 from . import _lib
 from .induced import DIRECT_METHOD, FMM_METHOD, fmm_parameters, velocity_device
-from .regrid import remesh_device
+from .regrid import lattice_window, remesh_device, remesh_window_device
 from .tune import Tuner
 
 # scratch bytes per blob of one step (FMM arrays + remesh arrays), measured
 # from the library's scratch layouts, plus a per-cell term for the window
+# (remesh sums, flags and slots, and the three output arrays)
 BYTES_PER_BLOB = 260
-BYTES_PER_CELL = 24
+BYTES_PER_CELL = 48
 
 
 @dataclass
@@ -50,6 +51,8 @@ class Simulation:
     c: float = 0.0
     method: int = -1
     leaf_level: int = 0
+    box: tuple = None     # (xmin, xmax, ymin, ymax) of the resident blobs, None = unknown
+    window: tuple = None  # remesh base-cell window of `box`
 
     @property
     def n(self):
@@ -90,9 +93,9 @@ class Server:
         self.reserve = hbm_reserve
         self.free_hbm = free_hbm or (lambda: torch.cuda.mem_get_info(self.device)[0])
         for s in self.sims:
+            self._box(s)
             if s.method < 0:
-                box = (float(s.x.min()), float(s.x.max()), float(s.y.min()), float(s.y.max()))
-                s.method, s.leaf_level = self.tuner.choose(s.n, s.k * s.sigma * s.sigma, box, tol)
+                s.method, s.leaf_level = self.tuner.choose(s.n, s.k * s.sigma * s.sigma, s.box, tol)
         self.n_slots = n_slots
         self._need = {}
         for i in range(len(self.sims)):
@@ -124,11 +127,23 @@ class Server:
         key = (sim, s.n, s.x.data_ptr())
         v = self._need.get(key)
         if v is None:
-            span = max(float(s.x.max() - s.x.min()), float(s.y.max() - s.y.min())) if s.n else 0.0
+            b = self._box(s)
+            span = max(b[1] - b[0], b[3] - b[2]) if s.n else 0.0
             cells = (span / s.h + 8.0) ** 2 if s.n else 0.0
             v = int(BYTES_PER_BLOB * s.n + BYTES_PER_CELL * cells) + (1 << 20)
             self._need[key] = v
         return v
+
+    @staticmethod
+    def _box(s):
+        """Bounding box of a simulation's blobs (one synchronisation; cached
+        until the state is replaced)."""
+        if s.box is None and s.n:
+            b = torch.stack([s.x.min(), s.x.max(), s.y.min(), s.y.max()]).cpu().tolist()
+            s.box = tuple(b)
+            h = s.h
+            s.window = lattice_window(s.box, h, -1.5 * h, -1.5 * h)
+        return s.box
 
     # -- workers ------------------------------------------------------------------
     def _worker(self, slot):
@@ -152,26 +167,37 @@ class Server:
                 self._lock.notify_all()
 
     def _step(self, req):
+        """Enqueue one step on the current stream.  With the blob box known
+        (resident state, no move) nothing here waits for the device: the FMM
+        takes the cached box and the remesh the cached lattice window."""
         s = self.sims[req.sim]
         ks, xo, cut = fmm_parameters(s.sigma, s.k)
         vx = torch.empty_like(s.x)
         vy = torch.empty_like(s.x)
+        box = self._box(s)
         if s.method == FMM_METHOD:
             _lib.fmm_set_tuning(s.leaf_level, 0, 1)
         velocity_device(s.x, s.y, s.g, ks, s.x, s.y, vx, vy, method=s.method, xopt=xo, cutoff=cut,
-                        tol=self.tol)
-        if req.dt != 0.0:
-            xm = s.x + req.dt * vx
-            ym = s.y + req.dt * vy
+                        tol=self.tol, box=box)
+        h = s.h
+        if req.dt == 0.0 and box is not None:
+            xn, yn, gn, nout = remesh_window_device(s.x, s.y, s.g, h, -1.5 * h, -1.5 * h,
+                                                    s.window, s.c)
+            if self.keep or req.update:
+                k = int(nout.item())
+                xn, yn, gn = xn[:k], yn[:k], gn[:k]
         else:
             xm, ym = s.x, s.y
-        h = s.h
-        xn, yn, gn = remesh_device(xm, ym, s.g, h, -1.5 * h, -1.5 * h, s.c)
+            if req.dt != 0.0:
+                xm = s.x + req.dt * vx
+                ym = s.y + req.dt * vy
+            xn, yn, gn = remesh_device(xm, ym, s.g, h, -1.5 * h, -1.5 * h, s.c)
         req.n = s.n
         if self.keep:
             req.result = {"vx": vx, "vy": vy, "x": xn, "y": yn, "g": gn}
         if req.update:
             s.x, s.y, s.g = xn, yn, gn
+            s.box = s.window = None
 
     # -- dispatcher ---------------------------------------------------------------
     def _try_admit(self, req):

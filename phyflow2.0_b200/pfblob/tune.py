@@ -27,7 +27,7 @@ from ._arrays import ptr
 CACHE_ENV = "PFBLOB_TUNE_CACHE"
 DEFAULT_RATES = {  # B200 measurements, used until calibrate() runs
     "r_direct": 1.4e12, "r_p2p": 8.4e11, "r_m2l": 1.5e13, "c_blob": 2.5e-10,
-    "t_fixed": 2.5e-4,
+    "t_fixed": 2.5e-4, "t_fixed_batch": 3e-5,
 }
 
 
@@ -134,16 +134,20 @@ class Tuner:
         return self.rates
 
     # -- model ----------------------------------------------------------------
-    def fmm_cost(self, n, L, w0, cutoff, np_terms=16):
+    def fmm_cost(self, n, L, w0, cutoff, np_terms=16, batch=False):
         near, far_avg, nq = self._tables_cached(L, w0, cutoff)
         occ = n / 4.0 ** L
         pairs = n * occ * nq
         trans = sum(4.0 ** l * far_avg[l] for l in range(2, L + 1))
         r = self.rates
-        return pairs / r["r_p2p"] + trans * np_terms ** 2 / r["r_m2l"] + n * r["c_blob"] + r["t_fixed"]
+        fixed = r["t_fixed_batch"] if batch else r["t_fixed"]
+        return pairs / r["r_p2p"] + trans * np_terms ** 2 / r["r_m2l"] + n * r["c_blob"] + fixed
 
-    def choose(self, n, ksigmasqr, box, tol=1e-6, cutoff=None):
-        """(method, leaf_level): method 0 = FMM, 1 = direct."""
+    def choose(self, n, ksigmasqr, box, tol=1e-6, cutoff=None, batch=False):
+        """(method, leaf_level): method 0 = FMM, 1 = direct.  ``batch``: the set
+        runs inside a captured batch, where the FMM's per-call latency (plan
+        look-up, bounding-box read-back, launch gaps) overlaps other sets'
+        work and only its device time counts."""
         if n < 64 or tol == 0.0:
             return 1, 0
         w0 = max(box[1] - box[0], box[3] - box[2]) or 1.0
@@ -156,7 +160,7 @@ class Tuner:
             near, far_avg, nq = self._tables_cached(L, w0, cutoff)
             if nq > 1024:
                 continue
-            t = self.fmm_cost(n, L, w0, cutoff)
+            t = self.fmm_cost(n, L, w0, cutoff, batch=batch)
             if t < best[0]:
                 best = (t, 0, L)
         return best[1], best[2]

@@ -17,7 +17,9 @@ Sources of truth:
   M4PRIME_INTERPKERNEL = 0) and ``m4kernel_1d``, which the reference builds
   with boost.python and which is supplied here by our C restatement of
   _interpolation_kernels_1d.cpp:75-89;
-* FMM                     - the reference C++ CPU FMM (oracle/_ref/libreffmm.so).
+* FMM                     - the reference C++ CPU FMM (oracle/_ref/libreffmm.so);
+* population control      - the reference ``PopulationControl`` (same module
+  as ``Regrid``).
 
 The fixtures are small .npz files; the generating code is this script.
 """
@@ -88,7 +90,12 @@ def rand_blobs(n, sigma, seed, lo=0.0, hi=1.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--only", choices=["popctl"], default=None,
+                    help="write only this group of fixtures")
     args = ap.parse_args()
+    if args.only == "popctl":
+        population_control_fixtures(args.ref)
+        return
     assert ref.available(), "build oracle/_ref first: make -C oracle ref"
 
     # 1. direct Gauss, C1 Lamb-Oseen lattice (N = 10 000)
@@ -150,7 +157,36 @@ def main():
     vx, vy = ref.fmm_velocity(x, y, g, sigma, tol=1e-6)
     np.savez_compressed(os.path.join(HERE, "fmm_rand.npz"), x=x, y=y, g=g, sigma=sigma,
                         tol=1e-6, vx=vx, vy=vy)
+    population_control_fixtures(args.ref)
     print("golden fixtures written to", HERE)
+
+
+def population_control_fixtures(refroot):
+    """6. the reference PopulationControl on (a) the C1 remesh output (explicit
+    zeros, default thresholds), (b) circulations spread over 12 decades with a
+    threshold that must drop several decades, (c) a global limit 30 decades
+    below the local threshold (more than 16 decade steps), with exact zeros and
+    ties at the thresholds."""
+    R = load_reference_regrid(refroot)
+    c1 = wl.lamb_oseen_lattice()
+    xb, yb = c1.bounds()
+    xn, yn, gn = R.Regrid(c1.x, c1.y, c1.g, c1.sigma, c1.overlap, xb, yb, 0, 0.0)
+    cases = [("c1", xn, yn, gn, 1e-8, 1e-8)]
+    rng = np.random.Generator(np.random.PCG64(23))
+    n = 5000
+    x = rng.uniform(-1, 1, n)
+    y = rng.uniform(-1, 1, n)
+    g = np.sign(rng.standard_normal(n)) * 10.0 ** rng.uniform(-14, -2, n)
+    g[:5] = 0.0
+    g[5:10] = 1e-3  # exactly at the starting threshold: kept (|g| < thr is false)
+    cases.append(("decades", x, y, g, 1e-3, 1e-6))
+    g2 = np.sign(rng.standard_normal(n)) * 10.0 ** rng.uniform(-45, -1, n)
+    g2[:3] = 0.0
+    cases.append(("deep", x, y, g2, 1.0, 1e-30))
+    for tag, xa, ya, ga, tl, tg in cases:
+        xo, yo, go = R.PopulationControl(xa.copy(), ya.copy(), ga.copy(), tl, tg)
+        np.savez_compressed(os.path.join(HERE, f"popctl_{tag}.npz"), x=xa, y=ya, g=ga,
+                            thr_local=tl, thr_global=tg, xo=xo, yo=yo, go=go)
 
 
 if __name__ == "__main__":

@@ -103,3 +103,20 @@ def test_invalid_sigma_raises():
     import pfblob
     with pytest.raises(pfblob._lib.PfError):
         pfblob.velocity(np.ones(4), np.ones(4), np.ones(4), 0.0, method=1)
+
+
+@pytest.mark.parametrize("n", [1025, 4096, 30000, 200000])
+def test_source_split_sizes_deterministic_vs_oracle(n):
+    """Sizes where the sources are cut into segments (fewer target tiles than
+    CTAs to fill the GPU): within tolerance, and bitwise repeatable."""
+    import pfblob
+    rng = np.random.default_rng(n + 7)
+    x, y = rng.random(n), rng.random(n)
+    g = rng.standard_normal(n) / n
+    sigma = 0.004
+    a = pfblob.velocity(x, y, g, sigma, method=1)
+    b = pfblob.velocity(x, y, g, sigma, method=1)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    sub = rng.choice(n, min(n, 4096), replace=False)
+    rx, ry = oracle.velocity_direct(x, y, g, 2 * sigma * sigma, x[sub].copy(), y[sub].copy())
+    assert normwise_err(a[0][sub], a[1][sub], rx, ry) <= TOL

@@ -146,3 +146,21 @@ def test_point_vortex_limit_theta_bound():
     idx = rng.choice(n, 3000, replace=False)
     rx, ry = oracle.velocity_direct(x, y, g, 2 * sigma * sigma, x[idx], y[idx])
     assert normwise_err(vx[idx], vy[idx], rx, ry) <= TOL
+
+
+def test_caller_box_equals_computed_box():
+    """pf_velocity_fmm_box with the exact bounding box gives bitwise the
+    pf_velocity_fmm result; a larger box is a different tree, same tolerance."""
+    import pfblob
+    from pfblob import workloads as wl
+    b = wl.uniform_square(n=150000, config=2, instance=9)
+    x, y, g = T(b.x), T(b.y), T(b.g)
+    ks, xo, cut = pfblob.fmm_parameters(b.sigma)
+    out = []
+    for box in (None, (b.x.min(), b.x.max(), b.y.min(), b.y.max()), (-0.5, 1.5, -0.25, 1.25)):
+        vx, vy = torch.empty_like(x), torch.empty_like(x)
+        pfblob.velocity_device(x, y, g, ks, x, y, vx, vy, method=pfblob.FMM_METHOD, xopt=xo,
+                               cutoff=cut, box=box)
+        out.append((vx.cpu().numpy(), vy.cpu().numpy()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert normwise_err(out[2][0], out[2][1], out[0][0], out[0][1]) <= TOL

@@ -70,3 +70,17 @@ def test_reference_fmm_within_tolerance_of_direct_oracle(golden):
     sig = float(f["sigma"])
     vx, vy = oracle.velocity_direct(f["x"], f["y"], f["g"], 2.0 * sig * sig)
     assert normwise_err(f["vx"], f["vy"], vx, vy) < 1e-6
+
+
+def test_population_control_matches_reference(golden):
+    for name, k in (("popctl_c1", 3), ("popctl_decades", 6), ("popctl_deep", 32)):
+        d = golden(name)
+        tl, tg = float(d["thr_local"]), float(d["thr_global"])
+        xo, yo, go, thr = oracle.population_control(d["x"], d["y"], d["g"], tl, tg)
+        assert np.array_equal(xo, d["xo"]) and np.array_equal(yo, d["yo"]), name
+        assert np.array_equal(go, d["go"]), name
+        # the threshold went down k decades (each division rounded)
+        t = tl
+        for _ in range(k):
+            t /= 10.0
+        assert thr == t, name

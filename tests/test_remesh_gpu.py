@@ -106,3 +106,23 @@ def test_capacity_error_reports_needed_size():
     s = _lib.lib.pf_remesh(_lib.context(0), 2, ptr(x), ptr(x), ptr(x), 0.08, -0.12, -0.12, 0.0, 4,
                            ptr(out), ptr(out), ptr(out), None, None, ctypes.byref(n), None)
     assert s == 6 and n.value > 4
+
+
+def test_window_remesh_equals_remesh():
+    """The sync-free remesh on the window of the blobs' bounding box gives
+    bitwise the pf_remesh result."""
+    import pfblob
+    from pfblob import workloads as wl
+    from pfblob.regrid import lattice_window, remesh_window_device
+    b = wl.mixed_instance(100000, config=4, instance=3)
+    dev = torch.device("cuda", 0)
+    x, y, g = (torch.from_numpy(a).to(dev) for a in (b.x, b.y, b.g))
+    h = b.h
+    xb, yb = b.bounds()
+    xn, yn, gn = pfblob.remesh_device(x, y, g, h, xb[0], yb[0])
+    box = (b.x.min(), b.x.max(), b.y.min(), b.y.max())
+    win = lattice_window(box, h, xb[0], yb[0])
+    wx, wy, wg, nout = remesh_window_device(x, y, g, h, xb[0], yb[0], win)
+    k = int(nout.item())
+    assert k == xn.numel()
+    assert torch.equal(wx[:k], xn) and torch.equal(wy[:k], yn) and torch.equal(wg[:k], gn)

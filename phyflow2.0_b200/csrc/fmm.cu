@@ -50,13 +50,9 @@ constexpr double INV_2PI = 0.15915494309189535;
 constexpr int MAX_LEVEL = pf::fmmx::MAX_LEVEL;
 constexpr int P2P_SETUP_THREADS = 128;
 constexpr int P2P_QMAX = 1024;   // source leaves per P2P block
-constexpr int P2P_WARPS = 4;     // P2P blocks per CTA (one warp each)
 constexpr int P2P_RUNS_SM = 64;  // runs staged in shared memory at a time
 constexpr int P2P_TILE = 64;     // sources per warp tile
-#ifndef PF_P2P_MIN_CTAS
-#define PF_P2P_MIN_CTAS 8
-#endif
-constexpr int P2P_MIN_CTAS = PF_P2P_MIN_CTAS;  // resident CTAs per SM the register budget allows
+constexpr int P2P_MIN_CTAS = 32; // one-warp CTAs resident per SM (64 registers per thread)
 constexpr int WARP_BOX_THREADS = 128;  // 4 warps, one box each
 constexpr unsigned INVALID_KEY = 0xFFFFFFFFu;
 
@@ -464,10 +460,14 @@ k_p2p_runs(int L, int kb, const int2 *__restrict__ q, int nq, int nqp,
     if (!runs && threadIdx.x == 0) nruns_or_off[b] = s_n;
 }
 
-// P2P near field: one warp per P2P block, up to three targets per lane (a
-// group of up to 96), warp-private source tiles of 64 (no CTA barriers, so
-// blocks with few targets leave no idle target slots behind).  Targets a and b
-// of a lane run packed (f32x2), target c scalar; NT = targets per lane in use.
+// P2P near field: one warp (one CTA) per P2P block, up to three targets per
+// lane (a group of up to 96), warp-private source tiles of 64.  Targets a and
+// b of a lane run packed (f32x2), target c scalar; NT = targets per lane.
+// A tile whose sources all lie farther than the series radius
+// sqrt(r2_series) from the group's target box (with a rounding margin) runs
+// the pair code without the small-x check; every pair there has r2 above
+// r2_series, so results are bitwise those of the checked code.
+template <bool SERIES>
 __device__ __forceinline__ void scalar_pair(const ulonglong2 &h, const ulonglong2 &l,
                                             unsigned long long g2, const float4 &t,
                                             const pfd::GaussParams &gp, float &px, float &py) {
@@ -480,12 +480,12 @@ __device__ __forceinline__ void scalar_pair(const ulonglong2 &h, const ulonglong
     const float dx = (t.x - sxh) + (t.z - sxl);
     const float dy = (t.y - syh) + (t.w - syl);
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
-    const float sc = pfd::gauss_s(r2, g, gp);
+    const float sc = pfd::gauss_s<SERIES>(r2, g, gp);
     px = fmaf(-dy, sc, px);
     py = fmaf(dx, sc, py);
 }
 
-template <int NT>
+template <int NT, bool SERIES>
 __device__ __forceinline__ void p2p_tile(const ulonglong2 *__restrict__ shi,
                                          const ulonglong2 *__restrict__ slo,
                                          const unsigned long long *__restrict__ sg2, int cnt,
@@ -500,11 +500,12 @@ __device__ __forceinline__ void p2p_tile(const ulonglong2 *__restrict__ shi,
 #pragma unroll 4
         for (int k = 0; k < 32; ++k) {
             if (NT >= 2) {
-                pfd::pair2(shi[c0 + k], slo[c0 + k], sg2[c0 + k], txh, tyh, txl, tyl, gp2, nx, ny);
+                pfd::pair2<SERIES>(shi[c0 + k], slo[c0 + k], sg2[c0 + k], txh, tyh, txl, tyl,
+                                   gp2, nx, ny);
             } else {
-                scalar_pair(shi[c0 + k], slo[c0 + k], sg2[c0 + k], ta, gp, pxa, pya);
+                scalar_pair<SERIES>(shi[c0 + k], slo[c0 + k], sg2[c0 + k], ta, gp, pxa, pya);
             }
-            if (NT == 3) scalar_pair(shi[c0 + k], slo[c0 + k], sg2[c0 + k], tc, gp, pxc, pyc);
+            if (NT == 3) scalar_pair<SERIES>(shi[c0 + k], slo[c0 + k], sg2[c0 + k], tc, gp, pxc, pyc);
         }
         if (NT >= 2) {
             float nxa, nxb, nya, nyb;
@@ -525,27 +526,40 @@ __device__ __forceinline__ void p2p_tile(const ulonglong2 *__restrict__ shi,
     }
 }
 
-__global__ void __launch_bounds__(P2P_WARPS * 32, P2P_MIN_CTAS)
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__global__ void __launch_bounds__(32, P2P_MIN_CTAS)
 k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *__restrict__ tcnt,
       const int32_t *__restrict__ sstart, const int32_t *__restrict__ scnt,
       const float4 *__restrict__ shl, const float *__restrict__ sg32,
       const float4 *__restrict__ thl, const int32_t *__restrict__ run_off,
       const int2 *__restrict__ runs, pfd::GaussParams gp, double2 *__restrict__ nearv,
       unsigned long long *__restrict__ pairs) {
-    __shared__ int s_rs[P2P_WARPS][P2P_RUNS_SM];      // particle start of run
-    __shared__ int s_rp[P2P_WARPS][P2P_RUNS_SM + 1];  // stream prefix of run
-    __shared__ ulonglong2 s_hi[P2P_WARPS][P2P_TILE];  // {x_hi, x_hi}, {y_hi, y_hi}
-    __shared__ ulonglong2 s_lo[P2P_WARPS][P2P_TILE];  // {x_lo, x_lo}, {y_lo, y_lo}
-    __shared__ unsigned long long s_g2[P2P_WARPS][P2P_TILE];  // {g, g}
+    __shared__ int s_rs[P2P_RUNS_SM];      // particle start of run
+    __shared__ int s_rp[P2P_RUNS_SM + 1];  // stream prefix of run
+    __shared__ ulonglong2 s_hi[P2P_TILE];  // {x_hi, x_hi}, {y_hi, y_hi}
+    __shared__ ulonglong2 s_lo[P2P_TILE];  // {x_lo, x_lo}, {y_lo, y_lo}
+    __shared__ unsigned long long s_g2[P2P_TILE];  // {g, g}
     const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t b = (int64_t)blockIdx.x * P2P_WARPS + wid;
+    const int lane = threadIdx.x;
+    const int64_t b = blockIdx.x;
     if (b >= nblk) return;
     const uint32_t leaf0 = (uint32_t)b << (2 * kb), nl = 1u << (2 * kb);
     const int t0 = tstart[leaf0];
     const int tn = tstart[leaf0 + nl - 1] + tcnt[leaf0 + nl - 1] - t0;
     if (tn == 0) return;
     const int r0 = run_off[b], r1 = run_off[b + 1];
+    const float rser = sqrtf(gp.r2_series);
     unsigned long long npairs = 0;
     for (int tg = 0; tg < tn; tg += 96) {
         const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane;
@@ -554,6 +568,20 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         const float4 tb = (ib < tn) ? thl[t0 + ib] : z4;
         const float4 tc = (ic < tn) ? thl[t0 + ic] : z4;
         const int nt = (tn - tg <= 32) ? 1 : (tn - tg <= 64) ? 2 : 3;  // warp-uniform
+        // box of the group's targets (hi parts), for the series-free test
+        float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
+        if (ia < tn) { bx0 = bx1 = ta.x; by0 = by1 = ta.y; }
+        if (ib < tn) { bx0 = fminf(bx0, tb.x); bx1 = fmaxf(bx1, tb.x); by0 = fminf(by0, tb.y); by1 = fmaxf(by1, tb.y); }
+        if (ic < tn) { bx0 = fminf(bx0, tc.x); bx1 = fmaxf(bx1, tc.x); by0 = fminf(by0, tc.y); by1 = fmaxf(by1, tc.y); }
+        bx0 = warp_min(bx0);
+        bx1 = warp_max(bx1);
+        by0 = warp_min(by0);
+        by1 = warp_max(by1);
+        // a source at box distance d has r2 >= (d - e)^2 for every target, e
+        // covering the hi-part rounding of both points (2^-23 relative each)
+        const float mag = fmaxf(fmaxf(fabsf(bx0), fabsf(bx1)), fmaxf(fabsf(by0), fabsf(by1)));
+        const float reach = rser * 1.001f + (mag + rser) * 4.8e-7f + 1e-30f;
+        const float reach2 = reach * reach;
         float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         for (int rc = r0; rc < r1; rc += P2P_RUNS_SM) {
             const int nrc = min(P2P_RUNS_SM, r1 - rc);
@@ -573,12 +601,12 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                     if (lane >= o) inc += t;
                 }
                 if (k < nrc) {
-                    s_rs[wid][k] = st;
-                    s_rp[wid][k] = pre + inc - len;
+                    s_rs[k] = st;
+                    s_rp[k] = pre + inc - len;
                 }
                 pre += __shfl_sync(0xffffffffu, inc, 31);
             }
-            if (lane == 0) s_rp[wid][nrc] = pre;
+            if (lane == 0) s_rp[nrc] = pre;
             __syncwarp();
             const int S = pre;
             npairs += (unsigned long long)S * (unsigned long long)min(96, tn - tg);
@@ -587,6 +615,7 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
             // the largest r with prefix[r] <= p (empty runs are stepped over)
             int rr[2] = {0, 0};
             for (int s0 = 0; s0 < S; s0 += P2P_TILE) {
+                bool near = false;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
                     const int p = s0 + h * 32 + lane;
@@ -594,26 +623,39 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                     float gg = 0.f;
                     if (p < S) {
                         int r = rr[h];
-                        while (r + 1 < nrc && s_rp[wid][r + 1] <= p) ++r;
+                        while (r + 1 < nrc && s_rp[r + 1] <= p) ++r;
                         rr[h] = r;
-                        const int src = s_rs[wid][r] + (p - s_rp[wid][r]);
+                        const int src = s_rs[r] + (p - s_rp[r]);
                         spv = shl[src];
                         gg = sg32[src];
+                        const float ex = fmaxf(fmaxf(bx0 - spv.x, spv.x - bx1), 0.f);
+                        const float ey = fmaxf(fmaxf(by0 - spv.y, spv.y - by1), 0.f);
+                        near |= !(ex * ex + ey * ey > reach2);
                     }
-                    s_hi[wid][h * 32 + lane] =
+                    s_hi[h * 32 + lane] =
                         make_ulonglong2(pfd::pack2(spv.x, spv.x), pfd::pack2(spv.y, spv.y));
-                    s_lo[wid][h * 32 + lane] =
+                    s_lo[h * 32 + lane] =
                         make_ulonglong2(pfd::pack2(spv.z, spv.z), pfd::pack2(spv.w, spv.w));
-                    s_g2[wid][h * 32 + lane] = pfd::pack2(gg, gg);
+                    s_g2[h * 32 + lane] = pfd::pack2(gg, gg);
                 }
+                const bool series = __any_sync(0xffffffffu, near);
                 __syncwarp();
                 const int cnt = min(P2P_TILE, S - s0);
-                if (nt == 2)
-                    p2p_tile<2>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, tc, gp, gp2, acc);
-                else if (nt == 3)
-                    p2p_tile<3>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, tc, gp, gp2, acc);
-                else
-                    p2p_tile<1>(s_hi[wid], s_lo[wid], s_g2[wid], cnt, ta, tb, tc, gp, gp2, acc);
+                if (series) {
+                    if (nt == 2)
+                        p2p_tile<2, true>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
+                    else if (nt == 3)
+                        p2p_tile<3, true>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
+                    else
+                        p2p_tile<1, true>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
+                } else {
+                    if (nt == 2)
+                        p2p_tile<2, false>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
+                    else if (nt == 3)
+                        p2p_tile<3, false>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
+                    else
+                        p2p_tile<1, false>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
+                }
                 __syncwarp();
             }
         }
@@ -1010,7 +1052,7 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     // near field
     {
         const int64_t nblk = (int64_t)1 << (2 * (L - kb));
-        k_p2p<<<(unsigned)pf::ceil_div(nblk, P2P_WARPS), P2P_WARPS * 32, 0, st>>>(
+        k_p2p<<<(unsigned)nblk, 32, 0, st>>>(
             nblk, kb, tstart, T.cnt, S.start, S.cnt, S.hl, S.g32, T.hl, c.d_run_off, c.d_runs,
             pfd::make_gauss_params(a.ksigmasqr), nearv, ctr);
         PF_TRY(pf::launch_status("k_p2p"));

@@ -34,11 +34,13 @@ __host__ __device__ inline GaussParams make_gauss_params(double ksigmasqr) {
     return p;
 }
 
-// (1 - exp(-x)) / r2 * g given r2, with the series branch for small x.
+// (1 - exp(-x)) / r2 * g given r2, with the series branch for small x
+// (SERIES = false: caller guarantees r2 >= r2_series).
+template <bool SERIES = true>
 __device__ __forceinline__ float gauss_s(float r2, float g, const GaussParams &p) {
     float e = ex2_approx(r2 * p.c_t);
     float om = 1.0f - e;
-    if (r2 < p.r2_series) {
+    if (SERIES && r2 < p.r2_series) {
         float x = r2 * p.c_x;
         float q = fmaf(x, -1.0f / 720.0f, 1.0f / 120.0f);
         q = fmaf(x, q, -1.0f / 24.0f);
@@ -120,6 +122,9 @@ __device__ __forceinline__ float series_om(float r2, float c_x) {
 
 // Accumulates, for targets (a, b): nx += dy*s, ny += dx*s  (note the sign:
 // the x velocity is -nx; negation is exact, so -nx equals the scalar sum).
+// SERIES = false omits the small-x check: only for pairs known to have
+// r2 >= r2_series, where the result is bitwise that of SERIES = true.
+template <bool SERIES = true>
 __device__ __forceinline__ void pair2(const ulonglong2 &hi, const ulonglong2 &lo, f32x2 g2,
                                       f32x2 txh, f32x2 tyh, f32x2 txl, f32x2 tyl,
                                       const GaussParams2 &gp, f32x2 &nx, f32x2 &ny) {
@@ -130,7 +135,7 @@ __device__ __forceinline__ void pair2(const ulonglong2 &hi, const ulonglong2 &lo
     unpack2(mul2(r2, gp.c_t), ta, tb);
     f32x2 om = sub2(gp.one, pack2(ex2_approx(ta), ex2_approx(tb)));
     unpack2(r2, ra, rb);
-    if (fminf(ra, rb) < gp.r2_series) {  // 1 - exp(-x) cancels: series
+    if (SERIES && fminf(ra, rb) < gp.r2_series) {  // 1 - exp(-x) cancels: series
         float oa, ob;
         unpack2(om, oa, ob);
         if (ra < gp.r2_series) oa = series_om(ra, gp.c_x1);

@@ -211,6 +211,19 @@ pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const double *y, co
                     double *x_out, double *y_out, double *g_out, int64_t *ix_out,
                     int64_t *iy_out, int64_t *n_out, void *stream);
 
+/* Remesh with Tutty's diffusive redistribution weights instead of M4':
+ * reference node i = xL + 1, Delta = (x - x_i)/h, q = 1 - 2 (hnu/h)^2 and the
+ * four weights of nodes i-1..i+2 built from f = q - Delta^2 and
+ * g = q - (Delta - 1)^2, hnu = sqrt(dt nu) (0 = plain Tutty redistribution).
+ * Lattice, output order, explicit zeros and arguments as pf_remesh.
+ * Replaces diffusion_tutty (src/python/blobs/base/evolution/_evolution.py:
+ * 238-445), called from Blobs._diffusion (src/python/blobs/__blobsClass.py:
+ * 1073-1111). */
+pf_status pf_remesh_tutty(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                          const double *g, double h, double xb0, double yb0, double hnu,
+                          int64_t capacity, double *x_out, double *y_out, double *g_out,
+                          int64_t *ix_out, int64_t *iy_out, int64_t *n_out, void *stream);
+
 /* Remesh onto a caller-given lattice window, with no host synchronisation
  * (for stream-ordered pipelines and CUDA-graph capture).  The window holds the
  * base cells ix in [ixmin, ixmin + nbx), iy in [iymin, iymin + nby) (a blob's

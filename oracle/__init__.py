@@ -24,7 +24,7 @@ Contents
 """
 from .core import (velocity_direct, panel_velocity, m4prime, remesh_left_index,
                    moments, oracle_lib)
-from .regrid import population_control, regrid
+from .regrid import diffusion_tutty, population_control, regrid
 
 __all__ = ["velocity_direct", "panel_velocity", "m4prime", "remesh_left_index",
-           "moments", "regrid", "population_control", "oracle_lib"]
+           "moments", "regrid", "population_control", "diffusion_tutty", "oracle_lib"]

@@ -15,7 +15,9 @@ Follows ``src/python/blobs/base/regrid/_regridding.py:107-222`` step by step:
 The kernel-size half is the integer 2 (the reference is Python 2, where
 ``kernelSize/2`` is integer division).
 
-``population_control`` restates PopulationControl (same module, :316-330).
+``population_control`` restates PopulationControl (same module, :316-330);
+``diffusion_tutty`` restates the Tutty redistribution of
+``src/python/blobs/base/evolution/_evolution.py:334-443``.
 """
 import numpy as np
 import scipy.sparse
@@ -84,3 +86,50 @@ def population_control(x, y, g, thr_local, thr_global):
         thr /= 10.0
     keep = ~flagged
     return x[keep], y[keep], g[keep], thr
+
+
+def diffusion_tutty(x, y, g, dt, nu, sigma, overlap, xbounds, ybounds):
+    """Tutty diffusive redistribution (``_evolution.py:334-443``): same window
+    and duplicate summation as ``regrid``, weights from the reference node
+    i = xL + 1.  Returns (x_new, y_new, g_new, ix, iy)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    if x.size < 1:
+        e = np.zeros(0, dtype=np.int64)
+        return x, y, g, e, e
+    h = sigma * overlap
+    xb0, yb0 = float(xbounds[0]), float(ybounds[0])
+    k = KERNEL_SIZE
+    xl = remesh_left_index(x, xb0, h)
+    yl = remesh_left_index(y, yb0, h)
+    ix = np.tile(xl, (k * k, 1)) + np.tile(np.arange(k), k).reshape(k * k, 1)
+    iy = np.tile(yl, (k * k, 1)) + np.repeat(np.arange(k), k).reshape(k * k, 1)
+    hnu = np.sqrt(dt * nu)
+    q = 1.0 - 2.0 * (hnu / h) ** 2.0
+
+    def weights(v, il, b0):
+        vi = (il + 1) * h + 0.5 * h + b0
+        d = (v - vi) / h
+        d1 = d - 1.0
+        f = q - d * d
+        gg = q - d1 * d1
+        return ((1.0 - d) * (0.5 * (1.0 - f - d)),
+                (1.0 - d) * f + d * (0.5 * (1.0 - gg - d1)),
+                (1.0 - d) * (0.5 * (1.0 - f + d)) + d * gg,
+                d * (0.5 * (1.0 - gg + d1)))
+
+    fx = weights(x, xl, xb0)
+    gy = weights(y, yl, yb0)
+    fw = np.tile(np.vstack(fx), (k, 1)).flatten()
+    gw = np.vstack([np.tile(w, (k, 1)) for w in gy]).flatten()
+    w = fw * gw
+    w *= np.tile(g, (k * k, 1)).flatten()
+    half = k // 2
+    ixmin, iymin = ix.min(), iy.min()
+    mat = scipy.sparse.csr_matrix((w, (ix.flatten() - ixmin + half,
+                                       iy.flatten() - iymin + half))).tocoo()
+    gn, ii, jj = mat.data, mat.row.astype(np.int64), mat.col.astype(np.int64)
+    ixn = ii + ixmin - half
+    iyn = jj + iymin - half
+    return ixn * h + 0.5 * h + xb0, iyn * h + 0.5 * h + yb0, gn, ixn, iyn

@@ -40,12 +40,15 @@ pf_status popctl_flags(int64_t n, const double *g, const int32_t *flag_in, const
                        int32_t *flag_out, cudaStream_t st);
 
 // Remesh core (remesh.cu), optionally followed by population control of the
-// remeshed cells before they are emitted.
+// remeshed cells before they are emitted.  kernel REMESH_M4: M4' weights with
+// the Wee coefficient c; REMESH_TUTTY: Tutty weights with c = hNu.
+constexpr int REMESH_M4 = 0;
+constexpr int REMESH_TUTTY = 1;
 size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby);
 pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, const double *g,
                       double h, double xb0, double yb0, double c, int32_t ixmin, int32_t iymin,
                       int64_t nbx, int64_t nby, int64_t capacity, double *xo, double *yo,
                       double *go, int64_t *ixo, int64_t *iyo, int32_t *total, int32_t *bad,
-                      cudaStream_t st, const PopCtlArgs *pc = nullptr);
+                      cudaStream_t st, const PopCtlArgs *pc = nullptr, int kernel = REMESH_M4);
 
 }  // namespace pf

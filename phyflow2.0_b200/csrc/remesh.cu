@@ -173,6 +173,26 @@ __device__ __forceinline__ double m4p(double u, double c2) {
     return 0.0;
 }
 
+// Tutty redistribution weights (src/python/blobs/base/evolution/_evolution.py:
+// 360-404): reference node i = xL + 1 at xi = i h + h/2 + b0, Delta =
+// (x - xi)/h, q = 1 - 2 (hNu/h)^2, f = q - Delta^2, g = q - (Delta - 1)^2; the
+// four weights of nodes i-1..i+2, each operation rounded as numpy does.
+__device__ __forceinline__ void tutty_w(double x, int64_t xl, double h, double h05, double b0,
+                                        double q, double (&w)[4]) {
+    const double xi = __dadd_rn(__dadd_rn(__dmul_rn((double)(xl + 1), h), h05), b0);
+    const double d = __ddiv_rn(__dsub_rn(x, xi), h);
+    const double d1 = __dsub_rn(d, 1.0);
+    const double f = __dsub_rn(q, __dmul_rn(d, d));
+    const double gg = __dsub_rn(q, __dmul_rn(d1, d1));
+    const double omd = __dsub_rn(1.0, d);
+    w[0] = __dmul_rn(omd, __dmul_rn(0.5, __dsub_rn(__dsub_rn(1.0, f), d)));
+    w[1] = __dadd_rn(__dmul_rn(omd, f),
+                     __dmul_rn(d, __dmul_rn(0.5, __dsub_rn(__dsub_rn(1.0, gg), d1))));
+    w[2] = __dadd_rn(__dmul_rn(omd, __dmul_rn(0.5, __dadd_rn(__dsub_rn(1.0, f), d))),
+                     __dmul_rn(d, gg));
+    w[3] = __dmul_rn(d, __dmul_rn(0.5, __dadd_rn(__dsub_rn(1.0, gg), d1)));
+}
+
 struct W9 {
     double wx[4], wy[4], g;
 };
@@ -198,28 +218,39 @@ k_rm_sortcells(int64_t ncell, const int32_t *__restrict__ start,
     }
 }
 
-// One thread per blob in cell order: its four x weights M4'(ux_a), four y
-// weights M4'(uy_b) and g, written in that order.
+// One thread per blob in cell order: its four x weights, four y weights and
+// g, written in that order.  M4' (TUTTY = false): M4'(ux_a) with the Wee
+// coefficient c^2 = prm; Tutty (TUTTY = true): prm = hNu = sqrt(dt nu).
+template <bool TUTTY>
 __global__ void __launch_bounds__(RM_THREADS)
 k_rm_weights(int64_t n, int64_t nby, int32_t ixmin, int32_t iymin,
              const int32_t *__restrict__ perm, const int32_t *__restrict__ cell,
              const double *__restrict__ x, const double *__restrict__ y,
-             const double *__restrict__ g, double h, double qx0, double qy0, double c2,
+             const double *__restrict__ g, double h, double xb0, double yb0, double prm,
              W9 *__restrict__ w, int32_t *__restrict__ nvalid) {
     const int64_t j = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     if (j >= *nvalid) return;
     const int32_t i = perm[j];
     const int64_t cc = cell[i];
     const int64_t bx = cc / nby, by = cc - bx * nby;
-    const double xh = __ddiv_rn(x[i], h), yh = __ddiv_rn(y[i], h);
     W9 r;
+    if (TUTTY) {
+        const double rr = __ddiv_rn(prm, h);
+        const double q = __dsub_rn(1.0, __dmul_rn(2.0, __dmul_rn(rr, rr)));
+        const double h05 = __dmul_rn(0.5, h);
+        tutty_w(x[i], ixmin + bx, h, h05, xb0, q, r.wx);
+        tutty_w(y[i], iymin + by, h, h05, yb0, q, r.wy);
+    } else {
+        const double xh = __ddiv_rn(x[i], h), yh = __ddiv_rn(y[i], h);
+        const double qx0 = __ddiv_rn(xb0, h), qy0 = __ddiv_rn(yb0, h);
 #pragma unroll
-    for (int a = 0; a < 4; ++a) {
-        // numpy order: ((ix + 0.5) + xb0/h) - x/h, ix the absolute lattice index
-        const double px = ((double)(ixmin + bx + a) + 0.5) + qx0;
-        const double py = ((double)(iymin + by + a) + 0.5) + qy0;
-        r.wx[a] = m4p(__dsub_rn(px, xh), c2);
-        r.wy[a] = m4p(__dsub_rn(py, yh), c2);
+        for (int a = 0; a < 4; ++a) {
+            // numpy order: ((ix + 0.5) + xb0/h) - x/h, ix the absolute lattice index
+            const double px = __dadd_rn((double)(ixmin + bx + a) + 0.5, qx0);
+            const double py = __dadd_rn((double)(iymin + by + a) + 0.5, qy0);
+            r.wx[a] = m4p(__dsub_rn(px, xh), prm);
+            r.wy[a] = m4p(__dsub_rn(py, yh), prm);
+        }
     }
     r.g = g[i];
     w[j] = r;
@@ -314,7 +345,7 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
                       double h, double xb0, double yb0, double c, int32_t ixmin, int32_t iymin,
                       int64_t nbx, int64_t nby, int64_t capacity, double *xo, double *yo,
                       double *go, int64_t *ixo, int64_t *iyo, int32_t *total, int32_t *bad,
-                      cudaStream_t st, const PopCtlArgs *pc) {
+                      cudaStream_t st, const PopCtlArgs *pc, int kernel) {
     const int64_t nbase = nbx * nby, ncell = (nbx + 3) * (nby + 3);
     const int64_t big = ncell > nbase ? ncell : nbase;
     int32_t *cell = (int32_t *)sc.take(4 * n);
@@ -344,8 +375,12 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     k_rm_sortcells<<<(unsigned)ceil_div(nbase, RM_THREADS), RM_THREADS, 0, st>>>(nbase, start,
                                                                                 count, perm);
     PF_TRY(launch_status("k_rm_sortcells"));
-    k_rm_weights<<<gn, RM_THREADS, 0, st>>>(n, nby, ixmin, iymin, perm, cell, x, y, g, h, xb0 / h,
-                                            yb0 / h, c * c, w, nvalid);
+    if (kernel == REMESH_TUTTY)
+        k_rm_weights<true><<<gn, RM_THREADS, 0, st>>>(n, nby, ixmin, iymin, perm, cell, x, y, g, h,
+                                                      xb0, yb0, c, w, nvalid);
+    else
+        k_rm_weights<false><<<gn, RM_THREADS, 0, st>>>(n, nby, ixmin, iymin, perm, cell, x, y, g,
+                                                       h, xb0, yb0, c * c, w, nvalid);
     PF_TRY(launch_status("k_rm_weights"));
     k_rm_gather<<<(unsigned)ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(nbx, nby, start,
                                                                              count, w, acc, flag);
@@ -372,7 +407,7 @@ pf_status remesh_sync(pf_ctx *ctx, int64_t n, const double *x, const double *y, 
                       double h, double xb0, double yb0, double c, int64_t capacity,
                       double *x_out, double *y_out, double *g_out, int64_t *ix_out,
                       int64_t *iy_out, int64_t *n_out, const double *popctl, double *thr_used,
-                      void *stream) {
+                      int kernel, void *stream) {
     PF_CHECK_ARG(ctx != nullptr, "pf_remesh: NULL context");
     PF_CHECK_ARG(n_out != nullptr, "pf_remesh: n_out is NULL");
     *n_out = 0;
@@ -428,7 +463,7 @@ pf_status remesh_sync(pf_ctx *ctx, int64_t n, const double *x, const double *y, 
     pf::PopCtlArgs pc{popctl ? popctl[0] : 0.0, popctl ? popctl[1] : 0.0, state};
     PF_TRY(pf::remesh_core(sc, n, x, y, g, h, xb0, yb0, c, he.ixmin, he.iymin, nbx, nby, capacity,
                            x_out, y_out, g_out, ix_out, iy_out, total, bad, st,
-                           popctl ? &pc : nullptr));
+                           popctl ? &pc : nullptr, kernel));
     PF_CUDA_TRY(cudaMemcpyAsync(ctx->host_small, total, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     if (popctl)
         PF_CUDA_TRY(cudaMemcpyAsync(ctx->host_small + 1, &state->thr, sizeof(double),
@@ -453,7 +488,18 @@ extern "C" pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const do
                                int64_t *ix_out, int64_t *iy_out, int64_t *n_out, void *stream) {
     pf::clear_error();
     return remesh_sync(ctx, n, x, y, g, h, xb0, yb0, c, capacity, x_out, y_out, g_out, ix_out,
-                       iy_out, n_out, nullptr, nullptr, stream);
+                       iy_out, n_out, nullptr, nullptr, pf::REMESH_M4, stream);
+}
+
+extern "C" pf_status pf_remesh_tutty(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                                     const double *g, double h, double xb0, double yb0,
+                                     double hnu, int64_t capacity, double *x_out, double *y_out,
+                                     double *g_out, int64_t *ix_out, int64_t *iy_out,
+                                     int64_t *n_out, void *stream) {
+    pf::clear_error();
+    PF_CHECK_ARG(std::isfinite(hnu) && hnu >= 0.0, "pf_remesh_tutty: hnu must be >= 0 and finite");
+    return remesh_sync(ctx, n, x, y, g, h, xb0, yb0, hnu, capacity, x_out, y_out, g_out, ix_out,
+                       iy_out, n_out, nullptr, nullptr, pf::REMESH_TUTTY, stream);
 }
 
 extern "C" pf_status pf_remesh_population_control(
@@ -469,7 +515,7 @@ extern "C" pf_status pf_remesh_population_control(
     const double pc[2] = {g_threshold_local, g_threshold_global};
     if (threshold_used) *threshold_used = g_threshold_local;
     return remesh_sync(ctx, n, x, y, g, h, xb0, yb0, c, capacity, x_out, y_out, g_out, ix_out,
-                       iy_out, n_out, pc, threshold_used, stream);
+                       iy_out, n_out, pc, threshold_used, pf::REMESH_M4, stream);
 }
 
 extern "C" pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, const double *y,

@@ -46,6 +46,8 @@ PROTOTYPES = {
                           _int, _vp],
     "pf_remesh": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp, _vp, _vp,
                   _c.POINTER(_i64), _vp],
+    "pf_remesh_tutty": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp,
+                        _vp, _vp, _c.POINTER(_i64), _vp],
     "pf_moments": [_vp, _i64, _vp, _vp, _vp, _vp, _vp],
     "pf_population_control": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _vp, _vp, _vp, _vp, _vp, _vp],
     "pf_remesh_population_control": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl,

@@ -7,8 +7,9 @@ that touch the hot path: ``evaluateVelocity`` (:546-628), ``redistribute``
 (:828-897), ``populationControl`` (:783-825), ``addBlobs`` / ``removeBlobs``
 (:499-544, :900-960), the construction-time population control and
 redistribution (:490-494), and ``evolve`` (:705-781) with the reference's
-convection integrators (``_evolution.py:537-701``) and Wee diffusion
-(``_evolution.py:138-235``, time step from ``__compute_deltaTd`` :2248-2318).
+convection integrators (``_evolution.py:537-701``) and Wee or Tutty diffusion
+(``_evolution.py:138-445``, ``_diffusion`` :1002-1111, time step from
+``__compute_deltaTd`` :2248-2318).
 Properties return numpy copies, as the reference's numpy-backed object does.
 """
 import math
@@ -56,8 +57,8 @@ class Blobs:
             raise ValueError("timeIntegrationParams['method'] must be 'euler' or 'rk4'")
         if self.velocityComputationParams['method'] not in ('fmm', 'direct'):
             raise ValueError("velocityComputationParams['method'] must be 'fmm' or 'direct'")
-        if self.diffusionParams['method'] != 'regrid_wee':
-            raise NotImplementedError("pfblob: only 'regrid_wee' diffusion is provided")
+        if self.diffusionParams['method'] not in ('regrid_wee', 'regrid_tutty'):
+            raise ValueError("diffusionParams['method'] must be 'regrid_wee' or 'regrid_tutty'")
         self.deltaTd, self.stepDiffusion = self._compute_deltaTd()
         self.tStep = 0
         self.t = 0.0
@@ -81,9 +82,19 @@ class Blobs:
         return x, y, f(x, y) * h * h
 
     def _compute_deltaTd(self):
-        """Wee diffusion time step (__blobsClass.py:2248-2288)."""
+        """Diffusion time step and interval (__blobsClass.py:2248-2318): Wee
+        rounds the stable step to a multiple of deltaTc; Tutty diffuses every
+        step and needs hNu/h <= 1/sqrt(2)."""
         if self.nu == 0.0:
             return 0.0, 0
+        if self.diffusionParams['method'] == 'regrid_tutty':
+            deltaTd = self.deltaTc
+            hnu = np.sqrt(deltaTd * self.nu)
+            if ((hnu / self.h) - (1.0 / np.sqrt(2.0))) > np.spacing(1000):
+                deltaTd = (((1.0 / np.sqrt(2.0)) * self.h) ** 2) / self.nu
+                raise ValueError('Regrid Tutty: deltaTc is to large. Reduce deltaTc to a value '
+                                 'smaller than %f.' % deltaTd)
+            return deltaTd, 1
         c2 = self.diffusionParams['c2']
         deltaTd = ((1.0 / 3.0) * self.h * self.h) / self.nu if c2 == 'optimized' else \
             (float(c2) * self.h * self.h) / self.nu
@@ -104,13 +115,16 @@ class Blobs:
                         cutoff=cut, tol=tol, ndirect=Ndirect)
         return vx, vy
 
-    def _regrid(self, c, population_control=False):
+    def _regrid(self, c, population_control=False, tutty_hnu=None):
         # The reference passes (sigma, overlap) to Regrid, which remeshes with
         # h = sigma*overlap (_regridding.py:118), and bounds -1.5 h from the
         # stored h (__blobsClass.py:891-892); the two can differ in the last bit.
         h = self.sigma * self.overlap
         b0 = -1.5 * self.h
-        if population_control:
+        if tutty_hnu is not None:
+            self._x, self._y, self._g = remesh_device(self._x, self._y, self._g, h, b0, b0,
+                                                      tutty_hnu=tutty_hnu)
+        elif population_control:
             self._x, self._y, self._g, _ = remesh_device(
                 self._x, self._y, self._g, h, b0, b0, c,
                 population_control=(self.gThresholdLocal, self.gThresholdGlobal))
@@ -146,8 +160,10 @@ class Blobs:
             self._x, self._y, self._g, self.gThresholdLocal, self.gThresholdGlobal)
 
     def evolve(self):
-        """One time step: convection (FE or the reference's RK4), Wee diffusion
-        every stepDiffusion steps, redistribution and population control."""
+        """One time step: convection (FE or the reference's RK4), diffusion
+        (Wee every stepDiffusion steps, or Tutty every step), redistribution
+        and population control.  With Wee and nu = 0 the reference divides by
+        stepDiffusion = 0; here diffusion is skipped."""
         vinf = self.vInf
         if self.timeIntegrationParams['method'] == 'euler':
             vx, vy = self._velocity_at(self._x, self._y, self._x, self._y)
@@ -165,7 +181,13 @@ class Blobs:
                 xn += w * kx * self.deltaTc
                 yn += w * ky * self.deltaTc
         self._x, self._y = xn, yn
-        if self.stepDiffusion != 0 and (self.tStep % self.stepDiffusion) == 0:
+        if self.diffusionParams['method'] == 'regrid_tutty':
+            # __blobsClass.py:1073-1111: redistribute, then Tutty's diffusive
+            # redistribution, every step (hNu = 0 when nu = 0)
+            self.redistribute()
+            if self.numBlobs > 0:
+                self._regrid(0.0, tutty_hnu=float(np.sqrt(self.deltaTd * self.nu)))
+        elif self.stepDiffusion != 0 and (self.tStep % self.stepDiffusion) == 0:
             self._regrid(math.sqrt(self.nu * self.deltaTd) / self.h)
         redistribute = self.stepRedistribution != 0 and (self.tStep % self.stepRedistribution) == 0
         control = (self.stepPopulationControl != 0 and

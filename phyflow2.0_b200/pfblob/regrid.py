@@ -13,13 +13,15 @@ M4PRIME_INTERPKERNEL = 0
 
 
 def remesh_device(x, y, g, h, xb0, yb0, c=0.0, capacity=None, with_indices=False, stream=None,
-                  population_control=None):
+                  population_control=None, tutty_hnu=None):
     """Device-tensor entry.  Returns (x, y, g[, ix, iy]) CUDA tensors of the
     new blobs in (ix, iy) order.  ``capacity`` bounds the output (default
     16 n, the window count); a retry with the exact size follows a capacity
     error.  ``population_control = (gThresholdLocal, gThresholdGlobal)``
     applies PopulationControl to the new blobs in the same pass (dropped cells
-    are never written); the threshold used is then appended to the result."""
+    are never written); the threshold used is then appended to the result.
+    ``tutty_hnu`` (= sqrt(dt nu)) selects Tutty's diffusive weights instead of
+    M4' (``c`` is then unused)."""
     n = x.numel()
     dev = x.device
     st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
@@ -34,7 +36,13 @@ def remesh_device(x, y, g, h, xb0, yb0, c=0.0, capacity=None, with_indices=False
         iyo = torch.empty(capacity, dtype=torch.int64, device=dev) if with_indices else None
         nout = ctypes.c_int64(0)
         thr = ctypes.c_double(0.0)
-        if population_control is None:
+        if tutty_hnu is not None:
+            if population_control is not None:
+                raise ValueError("population_control applies to the M4' remesh only")
+            s = _lib.lib.pf_remesh_tutty(ctx, n, ptr(x), ptr(y), ptr(g), float(h), float(xb0),
+                                         float(yb0), float(tutty_hnu), capacity, ptr(xo), ptr(yo),
+                                         ptr(go), ptr(ixo), ptr(iyo), ctypes.byref(nout), st)
+        elif population_control is None:
             s = _lib.lib.pf_remesh(ctx, n, ptr(x), ptr(y), ptr(g), float(h), float(xb0),
                                    float(yb0), float(c), capacity, ptr(xo), ptr(yo), ptr(go),
                                    ptr(ixo), ptr(iyo), ctypes.byref(nout), st)

@@ -19,7 +19,10 @@ Sources of truth:
   _interpolation_kernels_1d.cpp:75-89;
 * FMM                     - the reference C++ CPU FMM (oracle/_ref/libreffmm.so);
 * population control      - the reference ``PopulationControl`` (same module
-  as ``Regrid``).
+  as ``Regrid``);
+* Tutty diffusion         - the reference ``diffusion_tutty``
+  (src/python/blobs/base/evolution/_evolution.py), imported the same way with
+  a stub for its ``velocity`` import and the reference ``Regrid`` above.
 
 The fixtures are small .npz files; the generating code is this script.
 """
@@ -39,6 +42,44 @@ sys.path.insert(0, os.path.join(ROOT, "phyflow2.0_b200"))
 import oracle  # noqa: E402
 from oracle import ref  # noqa: E402
 from pfblob import workloads as wl  # noqa: E402
+
+
+def _py2_module(path, name, env, source=None):
+    """Compile a Python-2 module of the reference (or `source`, a part of it)
+    with `/` between ints as floor division (Python 2 semantics); nothing else
+    is changed."""
+    tree = ast.parse(open(path).read() if source is None else source, filename=path)
+
+    class Py2Div(ast.NodeTransformer):
+        def visit_BinOp(self, node):
+            self.generic_visit(node)
+            if isinstance(node.op, ast.Div):
+                return ast.copy_location(ast.Call(func=ast.Name("_py2div", ast.Load()),
+                                                  args=[node.left, node.right], keywords=[]), node)
+            return node
+
+    tree = ast.fix_missing_locations(Py2Div().visit(tree))
+    mod = types.ModuleType(name)
+    mod.__file__ = path
+    mod._py2div = lambda a, b: a // b if (isinstance(a, int) and isinstance(b, int)) else a / b
+    mod.__dict__.update(env)
+    exec(compile(tree, path, "exec"), mod.__dict__)
+    return mod
+
+
+def load_reference_tutty(refroot):
+    """The reference diffusion_tutty, compiled from its own source lines in
+    _evolution.py (the rest of that module has Python-2 print statements; this
+    function uses only numpy and scipy.sparse)."""
+    import scipy
+    import scipy.sparse  # noqa: F401
+    path = os.path.join(refroot, "src/python/blobs/base/evolution/_evolution.py")
+    lines = open(path).read().split("\n")
+    a = next(i for i, ln in enumerate(lines) if ln.startswith("def diffusion_tutty("))
+    b = next(i for i in range(a + 1, len(lines)) if lines[i].startswith("def "))
+    mod = _py2_module(path, "ref_tutty", {"numpy": np, "scipy": scipy},
+                      source="\n".join(lines[a:b]))
+    return mod.diffusion_tutty
 
 
 def load_reference_regrid(refroot):
@@ -90,11 +131,14 @@ def rand_blobs(n, sigma, seed, lo=0.0, hi=1.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["popctl"], default=None,
+    ap.add_argument("--only", choices=["popctl", "tutty"], default=None,
                     help="write only this group of fixtures")
     args = ap.parse_args()
     if args.only == "popctl":
         population_control_fixtures(args.ref)
+        return
+    if args.only == "tutty":
+        tutty_fixtures(args.ref)
         return
     assert ref.available(), "build oracle/_ref first: make -C oracle ref"
 
@@ -158,7 +202,29 @@ def main():
     np.savez_compressed(os.path.join(HERE, "fmm_rand.npz"), x=x, y=y, g=g, sigma=sigma,
                         tol=1e-6, vx=vx, vy=vy)
     population_control_fixtures(args.ref)
+    tutty_fixtures(args.ref)
     print("golden fixtures written to", HERE)
+
+
+def tutty_fixtures(refroot):
+    """7. the reference diffusion_tutty on random blobs (with blobs exactly on
+    lattice nodes) for hNu/h = 0.5 and for hNu = 0, and on the C1 lattice."""
+    tutty = load_reference_tutty(refroot)
+    x, y, g, sigma = rand_blobs(2000, 0.01, 29, -0.3, 0.4)
+    h = sigma * 0.8
+    x[:40] = (np.arange(40) - 20) * h + 0.5 * h + (-1.5 * h)
+    y[:40] = 0.5 * h + (-1.5 * h)
+    xb = np.array([-1.5 * h, 1.5 * h])
+    cases = [("rand", x, y, g, sigma, 0.8, xb, 0.25 * h * h, 1.0),
+             ("rand_nu0", x, y, g, sigma, 0.8, xb, 0.01, 0.0)]
+    c1 = wl.lamb_oseen_lattice()
+    c1b, _ = c1.bounds()
+    cases.append(("c1", c1.x, c1.y, c1.g, c1.sigma, c1.overlap, c1b, 1e-4, 0.5))
+    for tag, xa, ya, ga, sg, ov, bnd, dt, nu in cases:
+        xn, yn, gn = tutty(dt, nu, sg * ov, xa.copy(), ya.copy(), ga.copy(), sg, bnd, bnd,
+                           overlap=ov)
+        np.savez_compressed(os.path.join(HERE, f"tutty_{tag}.npz"), x=xa, y=ya, g=ga, sigma=sg,
+                            overlap=ov, xb=bnd, yb=bnd, dt=dt, nu=nu, xn=xn, yn=yn, gn=gn)
 
 
 def population_control_fixtures(refroot):

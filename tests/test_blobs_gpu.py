@@ -76,3 +76,37 @@ def test_wee_diffusion_time_step_and_conservation():
     # blobs sitting exactly on lattice nodes lose a little circulation; the
     # remesh reproduces this (pinned by the regrid_rand_c3 golden).
     assert abs(b.g.sum() - g0) <= 1e-9 * np.abs(c1.g).sum()
+
+
+def test_tutty_diffusion_step_matches_reference_sequence():
+    """Blobs with 'regrid_tutty': one evolve = FE convection, redistribute,
+    Tutty redistribution with hNu = sqrt(deltaTc nu), redistribute again
+    (__blobsClass.py:705-781, 1073-1111), done here step by step with the
+    oracle."""
+    import pfblob
+    from pfblob import workloads as wl
+    c1 = wl.lamb_oseen_lattice()
+    nu, dt = 0.5, 1e-4
+    kw = dict(vInf=[0.0, 0.0], nu=nu, deltaTc=dt, h=c1.h, overlap=0.8,
+              timeIntegrationParams={'method': 'euler'},
+              velocityComputationParams={'method': 'direct', 'hardware': 'gpu'},
+              blobControlParams={'stepRedistribution': 1, 'stepPopulationControl': 0,
+                                 'gThresholdLocal': 1e-8, 'gThresholdGlobal': 1e-8},
+              diffusionParams={'method': 'regrid_tutty'})
+    b = pfblob.Blobs((c1.x, c1.y, c1.g), **kw)
+    assert b.deltaTd == dt and b.stepDiffusion == 1
+    x0, y0, g0 = b.x, b.y, b.g
+    vx, vy = b.evaluateVelocity()
+    b.evolve()
+    h = c1.h
+    bnd = np.array([-1.5 * h, 1.5 * h])
+    x1, y1 = x0 + (vx + 0.0) * dt, y0 + (vy + 0.0) * dt
+    r = oracle.regrid(x1, y1, g0, b.sigma, 0.8, bnd, bnd)
+    t = oracle.diffusion_tutty(r[0], r[1], r[2], dt, nu, b.sigma, 0.8, bnd, bnd)
+    e = oracle.regrid(t[0], t[1], t[2], b.sigma, 0.8, bnd, bnd)
+    assert np.array_equal(b.x, e[0]) and np.array_equal(b.y, e[1])
+    assert np.abs(b.g - e[2]).max() <= 1e-12 * np.abs(e[2]).max()
+    assert abs(b.g.sum() - g0.sum()) <= 1e-12 * np.abs(g0).sum()
+    # the stability bound hNu/h <= 1/sqrt(2) is enforced as in the reference
+    with pytest.raises(ValueError):
+        pfblob.Blobs((c1.x, c1.y, c1.g), **dict(kw, deltaTc=1.0))

@@ -84,3 +84,13 @@ def test_population_control_matches_reference(golden):
         for _ in range(k):
             t /= 10.0
         assert thr == t, name
+
+
+def test_tutty_matches_reference(golden):
+    for name in ("tutty_rand", "tutty_rand_nu0", "tutty_c1"):
+        d = golden(name)
+        xn, yn, gn, _, _ = oracle.diffusion_tutty(d["x"], d["y"], d["g"], float(d["dt"]),
+                                                  float(d["nu"]), float(d["sigma"]),
+                                                  float(d["overlap"]), d["xb"], d["yb"])
+        assert np.array_equal(xn, d["xn"]) and np.array_equal(yn, d["yn"]), name
+        assert np.array_equal(gn, d["gn"]), name

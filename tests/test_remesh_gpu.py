@@ -126,3 +126,37 @@ def test_window_remesh_equals_remesh():
     k = int(nout.item())
     assert k == xn.numel()
     assert torch.equal(wx[:k], xn) and torch.equal(wy[:k], yn) and torch.equal(wg[:k], gn)
+
+
+@pytest.mark.parametrize("name", ["tutty_rand", "tutty_rand_nu0", "tutty_c1"])
+def test_tutty_vs_reference_golden(golden, name):
+    """Tutty diffusive redistribution: lattice nodes and their order bit-exact,
+    circulations within 1e-12, circulation and linear impulse conserved."""
+    import pfblob
+    d = golden(name)
+    xn, yn, gn = pfblob.diffusion_tutty(float(d["dt"]), float(d["nu"]), 0.0, d["x"], d["y"],
+                                        d["g"], float(d["sigma"]), d["xb"], d["yb"],
+                                        overlap=float(d["overlap"]))
+    assert np.array_equal(xn, d["xn"]) and np.array_equal(yn, d["yn"])
+    assert np.abs(gn - d["gn"]).max() <= GTOL * np.abs(d["gn"]).max()
+    m0 = oracle.moments(d["x"], d["y"], d["g"])
+    m1 = oracle.moments(xn, yn, gn)
+    assert abs(m1[0] - m0[0]) <= 1e-12 * m0[3]
+    xs = max(np.abs(d["x"]).max(), np.abs(d["y"]).max())
+    assert max(abs(m1[1] - m0[1]), abs(m1[2] - m0[2])) <= 1e-12 * m0[3] * xs
+
+
+def test_wee_diffusion_matches_remesh_with_c():
+    """diffusion_wee is the remesh with c = sqrt(nu dt)/h (oracle Regrid)."""
+    import pfblob
+    rng = np.random.default_rng(3)
+    n = 3000
+    x, y = rng.uniform(-0.2, 0.3, n), rng.uniform(-0.2, 0.3, n)
+    g = rng.standard_normal(n) / n
+    sigma, ov, h, dt, nu = 0.01, 0.8, 0.008, 1e-3, 0.01
+    b = np.array([-1.5 * h, 1.5 * h])
+    xn, yn, gn = pfblob.diffusion_wee(dt, nu, h, x, y, g, sigma, b, b, overlap=ov)
+    c = np.sqrt(nu * dt) / h
+    rx, ry, rg, _, _ = oracle.regrid(x, y, g, sigma, ov, b, b, c)
+    assert np.array_equal(xn, rx) and np.array_equal(yn, ry)
+    assert np.abs(gn - rg).max() <= GTOL * np.abs(rg).max()

@@ -38,9 +38,20 @@ class Marshal:
         return torch.empty(int(n), dtype=torch.float64, device=self.device)
 
     def out(self, t):
-        if self.host:
-            return t.cpu().numpy()
-        return t
+        return self.outs(t)[0]
+
+    def outs(self, *ts):
+        """Results in the caller's form.  Host results are copied straight into
+        pinned buffers (no staging, no first-touch page faults of fresh
+        pageable memory) with one synchronisation for all of them; the numpy
+        arrays returned keep those buffers alive."""
+        if not self.host:
+            return ts
+        hs = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in ts]
+        for h, t in zip(hs, ts):
+            h.copy_(t, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return tuple(h.numpy() for h in hs)
 
     @property
     def stream(self):

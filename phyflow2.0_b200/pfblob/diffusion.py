@@ -29,7 +29,7 @@ def _run(xBlob, yBlob, wBlob, sigma, overlap, xBounds, yBounds, **kw):
     if x.numel() < 1:  # the reference returns its inputs unchanged
         return xBlob, yBlob, wBlob
     xn, yn, gn = remesh_device(x, y, g, sigma * overlap, _first(xBounds), _first(yBounds), **kw)
-    return m.out(xn), m.out(yn), m.out(gn)
+    return m.outs(xn, yn, gn)
 
 
 def diffusion_wee(dt, nu, h, xBlob, yBlob, wBlob, sigma, xBounds, yBounds, overlap=0.5, k=2,

@@ -97,4 +97,4 @@ def velocity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None, 
     ksigmasqr, xopt, cut = fmm_parameters(float(sigma), float(k), cutoff)
     velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=method, xopt=xopt, cutoff=cut,
                     tol=float(tol), ndirect=int(Ndirect), device=m.index)
-    return m.out(vx), m.out(vy)
+    return m.outs(vx, vy)

@@ -41,4 +41,4 @@ def inducedVelocity(strength, xPanelStart, yPanelStart, xPanelEnd, yPanelEnd, co
     xv, yv = m.dev(xEval), m.dev(yEval)
     vx, vy = m.empty(xv.numel()), m.empty(xv.numel())
     panel_velocity_device(*arrs, xv, yv, vx, vy)
-    return m.out(vx), m.out(vy)
+    return m.outs(vx, vy)

@@ -130,7 +130,7 @@ def PopulationControl(xBlob, yBlob, wBlob, wThreshold, wTotalThreshold):
     m = Marshal(xBlob.device.index if isinstance(xBlob, torch.Tensor) and xBlob.is_cuda else None)
     x, y, g = m.dev(xBlob), m.dev(yBlob), m.dev(wBlob)
     xn, yn, gn, _ = population_control_device(x, y, g, wThreshold, wTotalThreshold)
-    return m.out(xn), m.out(yn), m.out(gn)
+    return m.outs(xn, yn, gn)
 
 
 def Regrid(xBlob, yBlob, wBlob, sigma, overlap, xBounds, yBounds, interpKernel=0, c=0.0):
@@ -150,4 +150,4 @@ def Regrid(xBlob, yBlob, wBlob, sigma, overlap, xBounds, yBounds, interpKernel=0
     xb0 = float(np.asarray(xBounds)[0]) if not isinstance(xBounds, torch.Tensor) else float(xBounds[0])
     yb0 = float(np.asarray(yBounds)[0]) if not isinstance(yBounds, torch.Tensor) else float(yBounds[0])
     xn, yn, gn = remesh_device(x, y, g, h, xb0, yb0, c)
-    return m.out(xn), m.out(yn), m.out(gn)
+    return m.outs(xn, yn, gn)

@@ -12,19 +12,21 @@
 //   3. scan of the per-cell counts -> cell starts.
 //   4. k_rm_place  : blob index -> its slot.
 //   5. k_rm_sortcells : per base cell, order its blobs by input index (every
-//      sum below then has a fixed order, independent of atomic timing);
-//      k_rm_weights : one thread per blob in that order writes its four x
-//      weights M4'(ux_a), four y weights M4'(uy_b) (_interpolation_kernels_1d.cpp:
-//      75-89; u as _regridding.py:183) and g.
-//   6. k_rm_gather : one thread per output cell (ix, iy) sums, in fixed order,
-//      (wx_a wy_b) g over the blobs of the 16 base cells whose windows cover it,
-//      and flags cells touched by at least one window (explicit zeros are
-//      kept, like the CSR sum of the reference, _regridding.py:200-202).
+//      sum below then has a fixed order, independent of atomic timing).
+//   6. k_rm_gather : per tile of output cells, the weights of the blobs of
+//      the covering base cells -- four x weights M4'(ux_a), four y weights
+//      M4'(uy_b) (_interpolation_kernels_1d.cpp:75-89; u as _regridding.py:183)
+//      or Tutty's -- are built in shared memory; one thread per output cell
+//      (ix, iy) sums, in fixed order, (wx_a wy_b) g over the blobs of the 16
+//      base cells whose windows cover it, and flags cells touched by at least
+//      one window (explicit zeros are kept, like the CSR sum of the
+//      reference, _regridding.py:200-202).
 //   6b. (pf_remesh_population_control only) PopulationControl of the cell
 //      values (popctl.cu), which clears the flags of the dropped cells.
 //   7. scan of the flags -> output slots, in (ix, iy) order.
 //   8. k_rm_emit   : x = ix*h + 0.5h + xb0 (same order as :217-218), g, ix, iy.
 // No floating-point atomics: each output value is produced by one thread.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -218,20 +220,21 @@ k_rm_sortcells(int64_t ncell, const int32_t *__restrict__ start,
     }
 }
 
-// One thread per blob in cell order: its four x weights, four y weights and
-// g, written in that order.  M4' (TUTTY = false): M4'(ux_a) with the Wee
-// coefficient c^2 = prm; Tutty (TUTTY = true): prm = hNu = sqrt(dt nu).
+// The four x weights, four y weights and g of blob i in base cell cc.  M4'
+// (TUTTY = false): M4'(ux_a) with the Wee coefficient c^2 = prm; Tutty
+// (TUTTY = true): prm = hNu = sqrt(dt nu).
+struct WParams {
+    double h, xb0, yb0;
+    double qx0, qy0;  // xb0/h, yb0/h (IEEE division on the host)
+    double prm;       // M4': c^2; Tutty: hNu
+};
+
 template <bool TUTTY>
-__global__ void __launch_bounds__(RM_THREADS)
-k_rm_weights(int64_t n, int64_t nby, int32_t ixmin, int32_t iymin,
-             const int32_t *__restrict__ perm, const int32_t *__restrict__ cell,
-             const double *__restrict__ x, const double *__restrict__ y,
-             const double *__restrict__ g, double h, double xb0, double yb0, double prm,
-             W9 *__restrict__ w, int32_t *__restrict__ nvalid) {
-    const int64_t j = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
-    if (j >= *nvalid) return;
-    const int32_t i = perm[j];
-    const int64_t cc = cell[i];
+__device__ __forceinline__ W9 blob_w9(int32_t i, int64_t cc, int64_t nby, int32_t ixmin,
+                                      int32_t iymin, const double *__restrict__ x,
+                                      const double *__restrict__ y, const double *__restrict__ g,
+                                      const WParams &wp) {
+    const double h = wp.h, xb0 = wp.xb0, yb0 = wp.yb0, prm = wp.prm;
     const int64_t bx = cc / nby, by = cc - bx * nby;
     W9 r;
     if (TUTTY) {
@@ -242,7 +245,7 @@ k_rm_weights(int64_t n, int64_t nby, int32_t ixmin, int32_t iymin,
         tutty_w(y[i], iymin + by, h, h05, yb0, q, r.wy);
     } else {
         const double xh = __ddiv_rn(x[i], h), yh = __ddiv_rn(y[i], h);
-        const double qx0 = __ddiv_rn(xb0, h), qy0 = __ddiv_rn(yb0, h);
+        const double qx0 = wp.qx0, qy0 = wp.qy0;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             // numpy order: ((ix + 0.5) + xb0/h) - x/h, ix the absolute lattice index
@@ -253,19 +256,95 @@ k_rm_weights(int64_t n, int64_t nby, int32_t ixmin, int32_t iymin,
         }
     }
     r.g = g[i];
-    w[j] = r;
+    return r;
 }
 
 // Output cell grid: ox in [0, nbx+3), oy in [0, nby+3); lattice index
 // ix = ixmin + ox.  A base cell (bx, by) covers ox in bx..bx+3, oy in by..by+3.
-__global__ void __launch_bounds__(RM_THREADS)
-k_rm_gather(int64_t nbx, int64_t nby, const int32_t *__restrict__ start,
-            const int32_t *__restrict__ count, const W9 *__restrict__ w,
-            double *__restrict__ acc, int32_t *__restrict__ flag) {
-    const int64_t noy = nby + 3;
-    const int64_t cid = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
-    if (cid >= (nbx + 3) * noy) return;
-    const int64_t ox = cid / noy, oy = cid - ox * noy;
+//
+// One CTA per tile of tw x th output cells (ox x oy), one thread per cell.  The
+// CTA first computes, into shared memory, the weight records of every blob
+// in the (tw+3) x (th+3) base cells covering the tile: per base-cell
+// column their cell-ordered positions are one contiguous range, so the
+// records are built from contiguous perm ranges, all columns at once.  Each
+// thread then sums (wx_a wy_b) g over the blobs of its 16 covering base cells
+// in a fixed order (b, a, blob) and flags cells touched by at least one
+// window (explicit zeros are kept, like the CSR sum of the reference,
+// _regridding.py:200-202).  A tile with more than `cap` blobs computes the
+// records where it uses them instead (same values); the host sizes the tile
+// and `cap` from the mean blob density so that this stays rare.
+constexpr int RG_TMAX = 16, RG_CAPMAX = 1536;  // 108 KB of records: 2 CTAs per SM
+constexpr int RG_BMAX = RG_TMAX + 3;
+
+template <bool TUTTY>
+__global__ void __launch_bounds__(RG_TMAX *RG_TMAX)
+k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, int32_t ixmin,
+            int32_t iymin,
+            const int32_t *__restrict__ start, const int32_t *__restrict__ count,
+            const int32_t *__restrict__ perm, const int32_t *__restrict__ cell,
+            const double *__restrict__ x, const double *__restrict__ y,
+            const double *__restrict__ g, WParams wp, double *__restrict__ acc,
+            int32_t *__restrict__ flag) {
+    extern __shared__ double s_w_raw[];  // cap weight records
+    W9 *s_w = reinterpret_cast<W9 *>(s_w_raw);
+    __shared__ int s_cs[RG_BMAX][RG_BMAX];  // staged start of each base cell
+    __shared__ int s_cn[RG_BMAX][RG_BMAX];  // its blob count
+    __shared__ int s_colg[RG_BMAX], s_coln[RG_BMAX], s_col[RG_BMAX + 1];
+    const int bw = tw + 3, bh = th + 3;
+    const int nthr = tw * th;
+    const int64_t noy = nby + 3, nox = nbx + 3;
+    const int64_t tile = blockIdx.x;
+    const int64_t ox0 = (tile / tiles_y) * tw, oy0 = (tile % tiles_y) * th;
+    const int64_t bx0 = ox0 - 3, by0 = oy0 - 3;
+    const int64_t blo = by0 > 0 ? by0 : 0;
+    const int64_t bhi = (by0 + bh < nby) ? by0 + bh : nby;  // exclusive
+    if (threadIdx.x < bw) {
+        const int64_t bx = bx0 + threadIdx.x;
+        int g0 = 0, n = 0;
+        if (bx >= 0 && bx < nbx && blo < bhi) {
+            const int64_t c0 = bx * nby + blo, c1 = bx * nby + bhi - 1;
+            g0 = start[c0];
+            n = start[c1] + count[c1] - g0;
+        }
+        s_colg[threadIdx.x] = g0;
+        s_coln[threadIdx.x] = n;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int p = 0;
+        for (int c = 0; c < bw; ++c) {
+            s_col[c] = p;
+            p += s_coln[c];
+        }
+        s_col[bw] = p;
+    }
+    __syncthreads();
+    const int total = s_col[bw];
+    const bool staged = total <= cap;
+    if (staged) {
+        for (int f = threadIdx.x; f < total; f += nthr) {
+            int c = 0;
+            while (s_col[c + 1] <= f) ++c;  // f < total, so c < bw
+            const int32_t i = perm[s_colg[c] + (f - s_col[c])];
+            s_w[f] = blob_w9<TUTTY>(i, cell[i], nby, ixmin, iymin, x, y, g, wp);
+        }
+        for (int k = threadIdx.x; k < bw * bh; k += nthr) {
+            const int c = k / bh, r = k - c * bh;
+            const int64_t bx = bx0 + c, by = by0 + r;
+            int ls = 0, ln = 0;
+            if (bx >= 0 && bx < nbx && by >= 0 && by < nby) {
+                const int64_t bc = bx * nby + by;
+                ls = start[bc] - s_colg[c] + s_col[c];
+                ln = count[bc];
+            }
+            s_cs[c][r] = ls;
+            s_cn[c][r] = ln;
+        }
+    }
+    __syncthreads();
+    const int tx = threadIdx.x / th, ty = threadIdx.x - tx * th;
+    const int64_t ox = ox0 + tx, oy = oy0 + ty;
+    if (ox >= nox || oy >= noy) return;
     double sum = 0.0;
     int touched = 0;
 #pragma unroll
@@ -276,19 +355,30 @@ k_rm_gather(int64_t nbx, int64_t nby, const int32_t *__restrict__ start,
         for (int a = 0; a < 4; ++a) {
             const int64_t bx = ox - a;
             if (bx < 0 || bx >= nbx) continue;
-            const int64_t bc = bx * nby + by;
-            const int cnt = count[bc];
-            if (cnt == 0) continue;
-            touched = 1;
-            const int s0 = start[bc];
-            for (int k = 0; k < cnt; ++k) {
-                const W9 &r = w[s0 + k];
-                sum += (r.wx[a] * r.wy[b]) * r.g;
+            if (staged) {
+                const int cnt = s_cn[tx + 3 - a][ty + 3 - b];
+                const int s0 = s_cs[tx + 3 - a][ty + 3 - b];
+                if (cnt == 0) continue;
+                touched = 1;
+                for (int k = 0; k < cnt; ++k) {
+                    const W9 &r = s_w[s0 + k];
+                    sum += (r.wx[a] * r.wy[b]) * r.g;
+                }
+            } else {
+                const int64_t bc = bx * nby + by;
+                const int cnt = count[bc], s0 = start[bc];
+                if (cnt == 0) continue;
+                touched = 1;
+                for (int k = 0; k < cnt; ++k) {
+                    const int32_t i = perm[s0 + k];
+                    const W9 r = blob_w9<TUTTY>(i, bc, nby, ixmin, iymin, x, y, g, wp);
+                    sum += (r.wx[a] * r.wy[b]) * r.g;
+                }
             }
         }
     }
-    acc[cid] = sum;
-    flag[cid] = touched;
+    acc[ox * noy + oy] = sum;
+    flag[ox * noy + oy] = touched;
 }
 
 __global__ void __launch_bounds__(RM_THREADS)
@@ -333,7 +423,7 @@ static int64_t dense_cell_limit(int64_t n) {
 size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby) {
     const int64_t nbase = nbx * nby, ncell = (nbx + 3) * (nby + 3);
     const int64_t big = ncell > nbase ? ncell : nbase;
-    return align256(4 * n) * 3 + align256(sizeof(W9) * n) + 2 * align256(4 * nbase) +
+    return align256(4 * n) * 3 + 2 * align256(4 * nbase) +
            align256(8 * ncell) + 2 * align256(4 * ncell) + align256(4 * scan_tmp_ints(big)) +
            3 * align256(16) + align256(sizeof(PcState)) + popctl_scratch_bytes() + 1024;
 }
@@ -351,7 +441,6 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     int32_t *cell = (int32_t *)sc.take(4 * n);
     int32_t *rank = (int32_t *)sc.take(4 * n);
     int32_t *perm = (int32_t *)sc.take(4 * n);
-    W9 *w = (W9 *)sc.take(sizeof(W9) * n);
     int32_t *count = (int32_t *)sc.take(4 * nbase);
     int32_t *start = (int32_t *)sc.take(4 * nbase);
     double *acc = (double *)sc.take(8 * ncell);
@@ -375,15 +464,37 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     k_rm_sortcells<<<(unsigned)ceil_div(nbase, RM_THREADS), RM_THREADS, 0, st>>>(nbase, start,
                                                                                 count, perm);
     PF_TRY(launch_status("k_rm_sortcells"));
-    if (kernel == REMESH_TUTTY)
-        k_rm_weights<true><<<gn, RM_THREADS, 0, st>>>(n, nby, ixmin, iymin, perm, cell, x, y, g, h,
-                                                      xb0, yb0, c, w, nvalid);
-    else
-        k_rm_weights<false><<<gn, RM_THREADS, 0, st>>>(n, nby, ixmin, iymin, perm, cell, x, y, g,
-                                                       h, xb0, yb0, c * c, w, nvalid);
-    PF_TRY(launch_status("k_rm_weights"));
-    k_rm_gather<<<(unsigned)ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(nbx, nby, start,
-                                                                             count, w, acc, flag);
+    // tile: the largest of 16x16, 16x8, 8x8, 8x4, 4x4 output cells whose
+    // covering base cells hold, at 1.5x the mean density, at most RG_CAPMAX
+    // blobs; shared memory for that many
+    const double rho = (double)n / (double)nbase;
+    int TX = 16, TY = 16;
+    auto need = [&](int tx, int ty) { return (tx + 3) * (ty + 3) * rho * 1.5 + 32.0; };
+    while (TX * TY > 16 && need(TX, TY) > RG_CAPMAX) {
+        if (TX == TY)
+            TY /= 2;
+        else
+            TX /= 2;
+    }
+    const int cap = (int)std::min<double>(RG_CAPMAX, std::ceil(need(TX, TY) / 32.0) * 32.0);
+    const int64_t tiles_y = ceil_div(nby + 3, TY), tiles = ceil_div(nbx + 3, TX) * tiles_y;
+    const int smem = cap * (int)sizeof(W9);
+    WParams wp{h, xb0, yb0, xb0 / h, yb0 / h, kernel == REMESH_TUTTY ? c : c * c};
+    if (kernel == REMESH_TUTTY) {
+        PF_CUDA_TRY(cudaFuncSetAttribute(k_rm_gather<true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         RG_CAPMAX * (int)sizeof(W9)));
+        k_rm_gather<true><<<(unsigned)tiles, TX * TY, smem, st>>>(
+            nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, perm, cell, x, y, g, wp, acc,
+            flag);
+    } else {
+        PF_CUDA_TRY(cudaFuncSetAttribute(k_rm_gather<false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         RG_CAPMAX * (int)sizeof(W9)));
+        k_rm_gather<false><<<(unsigned)tiles, TX * TY, smem, st>>>(
+            nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, perm, cell, x, y, g, wp, acc,
+            flag);
+    }
     PF_TRY(launch_status("k_rm_gather"));
     if (pc) {
         PF_TRY(popctl_decide(sc, ncell, acc, flag, *pc, st));

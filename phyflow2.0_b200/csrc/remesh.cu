@@ -230,12 +230,11 @@ struct WParams {
 };
 
 template <bool TUTTY>
-__device__ __forceinline__ W9 blob_w9(int32_t i, int64_t cc, int64_t nby, int32_t ixmin,
+__device__ __forceinline__ W9 blob_w9(int32_t i, int64_t bx, int64_t by, int32_t ixmin,
                                       int32_t iymin, const double *__restrict__ x,
                                       const double *__restrict__ y, const double *__restrict__ g,
                                       const WParams &wp) {
     const double h = wp.h, xb0 = wp.xb0, yb0 = wp.yb0, prm = wp.prm;
-    const int64_t bx = cc / nby, by = cc - bx * nby;
     W9 r;
     if (TUTTY) {
         const double rr = __ddiv_rn(prm, h);
@@ -246,11 +245,13 @@ __device__ __forceinline__ W9 blob_w9(int32_t i, int64_t cc, int64_t nby, int32_
     } else {
         const double xh = __ddiv_rn(x[i], h), yh = __ddiv_rn(y[i], h);
         const double qx0 = wp.qx0, qy0 = wp.qy0;
+        const double ix0 = (double)(ixmin + bx), iy0 = (double)(iymin + by);
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-            // numpy order: ((ix + 0.5) + xb0/h) - x/h, ix the absolute lattice index
-            const double px = __dadd_rn((double)(ixmin + bx + a) + 0.5, qx0);
-            const double py = __dadd_rn((double)(iymin + by + a) + 0.5, qy0);
+            // numpy order: ((ix + 0.5) + xb0/h) - x/h, ix the absolute lattice
+            // index (ix0 + a and + 0.5 are exact)
+            const double px = __dadd_rn((ix0 + (double)a) + 0.5, qx0);
+            const double py = __dadd_rn((iy0 + (double)a) + 0.5, qy0);
             r.wx[a] = m4p(__dsub_rn(px, xh), prm);
             r.wy[a] = m4p(__dsub_rn(py, yh), prm);
         }
@@ -326,7 +327,8 @@ k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, 
             int c = 0;
             while (s_col[c + 1] <= f) ++c;  // f < total, so c < bw
             const int32_t i = perm[s_colg[c] + (f - s_col[c])];
-            s_w[f] = blob_w9<TUTTY>(i, cell[i], nby, ixmin, iymin, x, y, g, wp);
+            const int64_t bx = bx0 + c;
+            s_w[f] = blob_w9<TUTTY>(i, bx, cell[i] - bx * nby, ixmin, iymin, x, y, g, wp);
         }
         for (int k = threadIdx.x; k < bw * bh; k += nthr) {
             const int c = k / bh, r = k - c * bh;
@@ -371,7 +373,7 @@ k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, 
                 touched = 1;
                 for (int k = 0; k < cnt; ++k) {
                     const int32_t i = perm[s0 + k];
-                    const W9 r = blob_w9<TUTTY>(i, bc, nby, ixmin, iymin, x, y, g, wp);
+                    const W9 r = blob_w9<TUTTY>(i, bx, by, ixmin, iymin, x, y, g, wp);
                     sum += (r.wx[a] * r.wy[b]) * r.g;
                 }
             }

@@ -81,6 +81,21 @@ pf_status pf_velocity_direct(pf_ctx *ctx, int64_t n_src, const double *x, const 
                              void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Induced vorticity of Gaussian blobs by direct summation (same FP32
+ * hi/lo + compensated scheme as pf_velocity_direct), FP64 in and out:
+ *
+ *   w_k = 1/(pi ksigmasqr) sum_m g_m exp(-r2/ksigmasqr),  r2 = dx^2 + dy^2 + 1e-12
+ *
+ * Replaces ww2parGauss_C_cpu (src/cpp/blobs/c/ww2parGauss_C/
+ * ww2parGauss_C_cpu.c:89-150) and ww2parGauss_gpu
+ * (src/cpp/blobs/cuda/ww2parGauss_gpu/ww2parGauss_py_gpu.cu), reached from
+ * vorticity (src/python/blobs/base/induced/_induced.py:702-963).
+ * ------------------------------------------------------------------------- */
+pf_status pf_vorticity_direct(pf_ctx *ctx, int64_t n_src, const double *x, const double *y,
+                              const double *g, int64_t n_tgt, const double *xt,
+                              const double *yt, double ksigmasqr, double *w, void *stream);
+
+/* ---------------------------------------------------------------------------
  * Blob velocity by the 2D fast multipole method (uniform quadtree, FP64
  * multipole/local expansions, FP32-compensated near field with the Gaussian
  * kernel).  Arguments as fmm2d_py: sigma-derived xopt/cutoff are computed by

@@ -31,11 +31,14 @@ def oracle_lib():
         lib = ctypes.CDLL(path)
         i64, dbl, cint = ctypes.c_int64, ctypes.c_double, ctypes.c_int
         lib.or_velocity_direct_gauss.argtypes = [i64, _dp, _dp, _dp, i64, _dp, _dp, dbl, _dp, _dp, cint]
+        lib.or_vorticity_direct_gauss.argtypes = [i64, _dp, _dp, _dp, i64, _dp, _dp, dbl, _dp,
+                                                  cint]
         lib.or_panel_velocity.argtypes = [i64, _dp, _dp, _dp, _dp, _dp, _dp, _dp, i64, _dp, _dp, _dp, _dp, cint]
         lib.or_m4prime.argtypes = [i64, _dp, dbl, _dp]
         lib.or_remesh_left_index.argtypes = [i64, _dp, dbl, dbl, _ip]
         lib.or_moments.argtypes = [i64, _dp, _dp, _dp, _dp]
-        for f in (lib.or_velocity_direct_gauss, lib.or_panel_velocity, lib.or_m4prime,
+        for f in (lib.or_velocity_direct_gauss, lib.or_vorticity_direct_gauss,
+                  lib.or_panel_velocity, lib.or_m4prime,
                   lib.or_remesh_left_index, lib.or_moments):
             f.restype = None
         _LIB = lib
@@ -62,6 +65,18 @@ def velocity_direct(xs, ys, gs, ksigmasqr, xt=None, yt=None, nthreads=0):
                                           _p(xt), _p(yt), float(ksigmasqr), _p(vx), _p(vy),
                                           int(nthreads))
     return vx, vy
+
+
+def vorticity_direct(xs, ys, gs, ksigmasqr, xt=None, yt=None, nthreads=0):
+    """FP64 induced vorticity of Gaussian blobs; restates ``ww2parGauss_C_cpu``
+    (targets default to the blobs, as ``_vorticity_direct_cpu_gauss``)."""
+    xs, ys, gs = _f64(xs), _f64(ys), _f64(gs)
+    xt = xs if xt is None else _f64(xt)
+    yt = ys if yt is None else _f64(yt)
+    w = np.empty(xt.shape[0])
+    oracle_lib().or_vorticity_direct_gauss(xs.shape[0], _p(xs), _p(ys), _p(gs), xt.shape[0],
+                                           _p(xt), _p(yt), float(ksigmasqr), _p(w), int(nthreads))
+    return w
 
 
 def panel_velocity(gamma, xs, ys, xe, ye, cosa, sina, xv, yv, nthreads=0):

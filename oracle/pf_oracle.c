@@ -56,6 +56,31 @@ void or_velocity_direct_gauss(int64_t ns, const double *xs, const double *ys,
     }
 }
 
+/* Induced vorticity of Gaussian blobs: restates ww2parGauss_C_cpu
+ * (src/cpp/blobs/c/ww2parGauss_C/ww2parGauss_C_cpu.c:131-145):
+ *   w_k = (1/pi) sum_m g_m exp(-(dx^2 + dy^2 + 1e-12)/ksigmasqr) / ksigmasqr */
+void or_vorticity_direct_gauss(int64_t ns, const double *xs, const double *ys,
+                               const double *gs, int64_t nt, const double *xt,
+                               const double *yt, double ksigmasqr, double *w, int nthreads)
+{
+    const double EPS = 1e-12;
+    const double inv_pi = 1.0 / OR_PI;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t k = 0; k < nt; ++k) {
+        double wk = 0.0;
+        for (int64_t m = 0; m < ns; ++m) {
+            const double dx = xt[k] - xs[m];
+            const double dy = yt[k] - ys[m];
+            const double r2 = dx * dx + dy * dy + EPS;
+            wk += gs[m] * exp(-r2 / ksigmasqr);
+        }
+        w[k] = inv_pi * wk / ksigmasqr;
+    }
+}
+
 /* Constant-strength straight vortex panels, induced velocity at points.
  * Follows src/cpp/panels/cython/vortexPanel_Cython/_vortexPanel_Cython_cpu.pyx
  * :352-393 (Katz & Plotkin 11.2.3): rotate the point into the panel frame,

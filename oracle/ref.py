@@ -6,7 +6,9 @@ pHyFlow sources, the Cython direct Gauss kernel
 Cython vortex-panel kernel
 (``src/cpp/panels/cython/vortexPanel_Cython/_vortexPanel_Cython_cpu.pyx``) and
 the C++ CPU FMM (``src/cpp/blobs/c++/fmm2d_py_cpu_gpu/*.cpp`` behind
-``oracle/ref_fmm_driver.cpp``).  The built files travel with the repository
+``oracle/ref_fmm_driver.cpp``) and the induced-vorticity loop of
+``src/cpp/blobs/c/ww2parGauss_C/ww2parGauss_C_cpu.c`` (behind
+``oracle/ref_ww2_driver.c``).  The built files travel with the repository
 snapshot; the sources they were built from do not.
 """
 import ctypes
@@ -87,3 +89,23 @@ def fmm_velocity(x, y, g, sigma, k=2.0, xt=None, yt=None, ndirect=35, tol=1e-6, 
     _fmm_lib().ref_fmm2d(x.shape[0], p(x), p(y), p(g), xt.shape[0], p(xt), p(yt), int(ndirect),
                          float(xopt), float(cutoff), float(tol), p(qr), p(qi))
     return -qi / (2.0 * np.pi), -qr / (2.0 * np.pi)
+
+
+def vorticity_gauss(x, y, g, ksigmasqr, xt=None, yt=None):
+    """The reference's own ww2parGauss_C_cpu loop -> w at (xt, yt) (default:
+    the blobs)."""
+    if "ww2" not in _cache:
+        lib = ctypes.CDLL(os.path.join(REF_DIR, "libref_ww2.so"))
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.ref_ww2par_gauss.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, dp, dp,
+                                         ctypes.c_double, dp]
+        lib.ref_ww2par_gauss.restype = None
+        _cache["ww2"] = lib
+    x, y, g = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, g))
+    xt = x if xt is None else np.ascontiguousarray(xt, dtype=np.float64)
+    yt = y if yt is None else np.ascontiguousarray(yt, dtype=np.float64)
+    w = np.empty(xt.shape[0])
+    p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    _cache["ww2"].ref_ww2par_gauss(x.shape[0], p(x), p(y), p(g), xt.shape[0], p(xt), p(yt),
+                                   float(ksigmasqr), p(w))
+    return w

@@ -3,6 +3,7 @@
 Entry points (same names, arguments and results as pHyFlow):
 
 * ``velocity``         - pHyFlow.blobs.base.induced.velocity (direct / FMM, Gauss)
+* ``vorticity``        - pHyFlow.blobs.base.induced.vorticity (direct, Gauss)
 * ``Regrid``           - pHyFlow.blobs.base.regrid.Regrid (M4' remesh)
 * ``PopulationControl`` - pHyFlow.blobs.base.regrid.PopulationControl
 * ``diffusion_wee``, ``diffusion_tutty`` - pHyFlow.blobs.base.evolution
@@ -17,11 +18,11 @@ from .blobs import Blobs
 from .conservation import conservation_error, moments_device
 from .diffusion import diffusion_tutty, diffusion_wee
 from .induced import (CPU_HARDWARE, DIRECT_METHOD, FMM_METHOD, GAUSS_KERNEL, GPU_HARDWARE,
-                      fmm_parameters, velocity, velocity_device)
+                      fmm_parameters, velocity, velocity_device, vorticity)
 from .panels import inducedVelocity, panel_velocity_device
 from .regrid import PopulationControl, Regrid, population_control_device, remesh_device
 
-__all__ = ["Blobs", "velocity", "velocity_device", "Regrid", "remesh_device", "PopulationControl",
+__all__ = ["Blobs", "velocity", "velocity_device", "vorticity", "Regrid", "remesh_device", "PopulationControl",
            "population_control_device", "diffusion_wee", "diffusion_tutty", "inducedVelocity",
            "panel_velocity_device", "moments_device", "conservation_error", "fmm_parameters",
            "GAUSS_KERNEL", "CPU_HARDWARE", "GPU_HARDWARE", "FMM_METHOD", "DIRECT_METHOD"]

@@ -98,3 +98,29 @@ def velocity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None, 
     velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=method, xopt=xopt, cutoff=cut,
                     tol=float(tol), ndirect=int(Ndirect), device=m.index)
     return m.outs(vx, vy)
+
+
+def vorticity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None, hardware=0,
+              blocksize=128, method=1):
+    """Induced vorticity of Gaussian vortex blobs at (xEval, yEval) (the blobs
+    if None), by direct summation on the GPU.
+
+    Same arguments and return value as pHyFlow's ``vorticity``
+    (``src/python/blobs/base/induced/_induced.py:702-789``); like the
+    reference, the FMM method is not available for the vorticity."""
+    if kernel != GAUSS_KERNEL:
+        raise NotImplementedError("pfblob: only the Gaussian kernel (kernel=1) is provided")
+    if method != DIRECT_METHOD:
+        raise Exception('FMM method not implemented yet')
+    m = Marshal(xBlob.device.index if isinstance(xBlob, torch.Tensor) and xBlob.is_cuda else None)
+    x, y, g = m.dev(xBlob), m.dev(yBlob), m.dev(wBlob)
+    if xEval is None:
+        xt, yt = x, y
+    else:
+        xt, yt = m.dev(xEval), m.dev(yEval)
+    w = m.empty(xt.numel())
+    ctx = _lib.context(m.index)
+    _lib.check(_lib.lib.pf_vorticity_direct(ctx, x.numel(), ptr(x), ptr(y), ptr(g), xt.numel(),
+                                            ptr(xt), ptr(yt), float(k) * sigma * sigma, ptr(w),
+                                            m.stream))
+    return m.outs(w)[0]

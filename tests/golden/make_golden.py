@@ -20,6 +20,8 @@ Sources of truth:
 * FMM                     - the reference C++ CPU FMM (oracle/_ref/libreffmm.so);
 * population control      - the reference ``PopulationControl`` (same module
   as ``Regrid``);
+* induced vorticity       - the reference ww2parGauss_C_cpu loop
+  (src/cpp/blobs/c/ww2parGauss_C/ww2parGauss_C_cpu.c), built into oracle/_ref/;
 * Tutty diffusion         - the reference ``diffusion_tutty``
   (src/python/blobs/base/evolution/_evolution.py), imported the same way with
   a stub for its ``velocity`` import and the reference ``Regrid`` above.
@@ -131,7 +133,7 @@ def rand_blobs(n, sigma, seed, lo=0.0, hi=1.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["popctl", "tutty"], default=None,
+    ap.add_argument("--only", choices=["popctl", "tutty", "vorticity"], default=None,
                     help="write only this group of fixtures")
     args = ap.parse_args()
     if args.only == "popctl":
@@ -139,6 +141,9 @@ def main():
         return
     if args.only == "tutty":
         tutty_fixtures(args.ref)
+        return
+    if args.only == "vorticity":
+        vorticity_fixtures()
         return
     assert ref.available(), "build oracle/_ref first: make -C oracle ref"
 
@@ -203,7 +208,28 @@ def main():
                         tol=1e-6, vx=vx, vy=vy)
     population_control_fixtures(args.ref)
     tutty_fixtures(args.ref)
+    vorticity_fixtures()
     print("golden fixtures written to", HERE)
+
+
+def vorticity_fixtures():
+    """8. the reference induced-vorticity loop: C1 lattice at the blobs, and
+    random blobs (a duplicated blob, a zero one, a far one) at separate points."""
+    c1 = wl.lamb_oseen_lattice()
+    w = ref.vorticity_gauss(c1.x, c1.y, c1.g, c1.ksigmasqr)
+    np.savez_compressed(os.path.join(HERE, "vort_c1.npz"), x=c1.x, y=c1.y, g=c1.g,
+                        sigma=c1.sigma, ksigmasqr=c1.ksigmasqr, w=w)
+    x, y, g, sigma = rand_blobs(3000, 0.01, 31)
+    x[10], y[10] = x[11], y[11]
+    g[20] = 0.0
+    x[30], y[30] = 25.0, -13.0
+    rng = np.random.Generator(np.random.PCG64(37))
+    xt, yt = rng.uniform(-0.1, 1.1, 1500), rng.uniform(-0.1, 1.1, 1500)
+    xt[:5], yt[:5] = x[:5], y[:5]
+    k2 = 2.0 * sigma * sigma
+    w = ref.vorticity_gauss(x, y, g, k2, xt, yt)
+    np.savez_compressed(os.path.join(HERE, "vort_rand.npz"), x=x, y=y, g=g, sigma=sigma,
+                        ksigmasqr=k2, xt=xt, yt=yt, w=w)
 
 
 def tutty_fixtures(refroot):

@@ -94,3 +94,12 @@ def test_tutty_matches_reference(golden):
                                                   float(d["overlap"]), d["xb"], d["yb"])
         assert np.array_equal(xn, d["xn"]) and np.array_equal(yn, d["yn"]), name
         assert np.array_equal(gn, d["gn"]), name
+
+
+def test_vorticity_matches_reference_loop(golden):
+    d = golden("vort_c1")
+    w = oracle.vorticity_direct(d["x"], d["y"], d["g"], float(d["ksigmasqr"]))
+    assert np.array_equal(w, d["w"])
+    d = golden("vort_rand")
+    w = oracle.vorticity_direct(d["x"], d["y"], d["g"], float(d["ksigmasqr"]), d["xt"], d["yt"])
+    assert np.array_equal(w, d["w"])

@@ -136,6 +136,16 @@ def pick_method(arg):
     return "fmm" if ok else "direct"
 
 
+def reduce_max(value, dev, world):
+    """Max over ranks (the job's time is its slowest rank's)."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world):
     import torch
     import pfblob
@@ -195,11 +205,7 @@ def run_ours(args, rank, world):
     vel_ms = [e[0].elapsed_time(e[1]) for e in evs]
     rm_ms = [e[1].elapsed_time(e[2]) for e in evs]
     step_ms = sum(vel_ms + rm_ms) / args.steps
-    t_max = step_ms
-    if world > 1:
-        t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = reduce_max(step_ms, dev, world)
     value = world * n / (t_max * 1e-3)
 
     # end to end through the public API with host (numpy) buffers
@@ -216,11 +222,7 @@ def run_ours(args, rank, world):
             torch.cuda.synchronize()
             if k > 0:
                 e2e_ms.append((time.perf_counter() - t0) * 1e3)
-        em = statistics.median(e2e_ms)
-        if world > 1:
-            t = torch.tensor([em], dtype=torch.float64, device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            em = float(t.item())
+        em = reduce_max(statistics.median(e2e_ms), dev, world)
         e2e = {"value": world * n / (em * 1e-3), "unit": "evals/s", "ms_per_step": em,
                "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 16 * n + 24 * rxn.shape[0]}
 

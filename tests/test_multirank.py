@@ -1,0 +1,40 @@
+"""Multi-process paths of bench.py on CPU (gloo, world size 2): the job time is
+the max over ranks, and the reference arm runs on rank 0 only."""
+import os
+import subprocess
+import sys
+
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+
+
+def _worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sys.path.insert(0, ROOT)
+    import bench
+    v = bench.reduce_max(1.5 + rank, torch.device("cpu"), world)
+    out[rank] = v
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_reduce_max_over_two_gloo_ranks():
+    world = 2
+    port = 29500 + os.getpid() % 1000
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
+        assert out[0] == out[1] == 2.5
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--steps", "1", "--warmup", "0"], env=env, capture_output=True,
+                       text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == ""

@@ -199,6 +199,31 @@ pf_status pf_panel_velocity(pf_ctx *ctx, int64_t m, const double *gamma, const d
                             const double *xv, const double *yv, double *vx, double *vy,
                             int accumulate, void *stream);
 
+/* Influence matrix of M vortex panels on their collocation points, FP64:
+ * A[i*M + j] = (velocity at (xcp_i, ycp_i) of panel j at unit strength) .
+ * (cos_i, sin_i), row-major, device array of M*M.  Replaces
+ * assemble_influenceMatrix (src/cpp/panels/cython/vortexPanel_Cython/
+ * _vortexPanel_Cython_cpu.pyx:81-236), reached from influenceMatrix
+ * (src/python/panels/base/panelSolver.py:31-144) and Panels
+ * (src/python/panels/__panelsClass.py:872-962). */
+pf_status pf_panel_influence_matrix(pf_ctx *ctx, int64_t m, const double *xcp, const double *ycp,
+                                    const double *xs, const double *ys, const double *xe,
+                                    const double *ye, const double *cosa, const double *sina,
+                                    double *A, void *stream);
+
+/* Dense LU factorisation with partial pivoting of the row-major m x m FP64
+ * device matrix `a`, in place: P a = L U, L unit lower; ipiv[k] (device
+ * int32) is the row exchanged with row k at step k.  The DEVICE int32
+ * *info_dev receives 0, or k+1 if U[k][k] is exactly zero (the factorisation
+ * still completes, as LAPACK getrf).  pf_dense_lu_solve overwrites the device
+ * vector b with the solution.  No host synchronisation.  Replaces the
+ * scipy.linalg lu_factor / lu_solve pair of the panel solve
+ * (src/python/panels/__panelsClass.py:782, :960-962). */
+pf_status pf_dense_lu_factor(pf_ctx *ctx, int64_t m, double *a, int32_t *ipiv,
+                             int32_t *info_dev, void *stream);
+pf_status pf_dense_lu_solve(pf_ctx *ctx, int64_t m, const double *lu, const int32_t *ipiv,
+                            double *b, void *stream);
+
 /* ---------------------------------------------------------------------------
  * M4' remesh onto the lattice x_i = i h + h/2 + xb0 (same in y), h = sigma *
  * overlap.  Every cell touched by a blob's 4x4 window is emitted, including

@@ -109,3 +109,9 @@ def vorticity_gauss(x, y, g, ksigmasqr, xt=None, yt=None):
     _cache["ww2"].ref_ww2par_gauss(x.shape[0], p(x), p(y), p(g), xt.shape[0], p(xt), p(yt),
                                    float(ksigmasqr), p(w))
     return w
+
+
+def panel_influence(xcp, ycp, xs, ys, xe, ye, cosa, sina):
+    """Reference Cython assemble_influenceMatrix -> A (M, M)."""
+    f = [np.ascontiguousarray(a, dtype=np.float64) for a in (xcp, ycp, xs, ys, xe, ye, cosa, sina)]
+    return np.array(_module("_vortexPanel_Cython_cpu").assemble_influenceMatrix(*f))

@@ -87,7 +87,53 @@ k_panel_velocity(int64_t m, const double *__restrict__ gamma, const double *__re
     }
 }
 
+// Influence matrix of the panels on their collocation points
+// (_vortexPanel_Cython_cpu.pyx:217-234, all in FP64 as there): A[i][j] =
+// velocity induced at collocation point i by panel j at unit strength,
+// projected on the tangent (cos_i, sin_i) of panel i.  One thread per (i, j),
+// j fastest (coalesced rows).
+__global__ void __launch_bounds__(PN_THREADS)
+k_panel_influence(int64_t m, const double *__restrict__ xcp, const double *__restrict__ ycp,
+                  const double *__restrict__ xs, const double *__restrict__ ys,
+                  const double *__restrict__ xe, const double *__restrict__ ye,
+                  const double *__restrict__ cosa, const double *__restrict__ sina,
+                  double *__restrict__ A) {
+    const int64_t e = (int64_t)blockIdx.x * PN_THREADS + threadIdx.x;
+    if (e >= m * m) return;
+    const int64_t i = e / m, j = e - i * m;
+    const double cj = cosa[j], sj = sina[j];
+    const double lx = xe[j] - xs[j], ly = ye[j] - ys[j];
+    const double x2 = cj * lx + sj * ly;
+    const double dx = xcp[i] - xs[j], dy = ycp[i] - ys[j];
+    const double xp = cj * dx + sj * dy;
+    const double yp = -sj * dx + cj * dy;
+    const double vxp = INV_2PI * (atan2(yp, xp - x2) - atan2(yp, xp));
+    const double vyp = -INV_4PI * log((xp * xp + yp * yp) / ((xp - x2) * (xp - x2) + yp * yp));
+    const double vx = cj * vxp - sj * vyp;
+    const double vy = sj * vxp + cj * vyp;
+    A[e] = vx * cosa[i] + vy * sina[i];
+}
+
 }  // namespace
+
+extern "C" pf_status pf_panel_influence_matrix(pf_ctx *ctx, int64_t m, const double *xcp,
+                                               const double *ycp, const double *xs,
+                                               const double *ys, const double *xe,
+                                               const double *ye, const double *cosa,
+                                               const double *sina, double *A, void *stream) {
+    pf::clear_error();
+    PF_CHECK_ARG(ctx != nullptr, "pf_panel_influence_matrix: NULL context");
+    PF_CHECK_ARG(m >= 0 && m <= 32768, "pf_panel_influence_matrix: m = %lld outside [0, 32768]",
+                 (long long)m);
+    PF_CHECK_ARG(m == 0 || (xcp && ycp && xs && ys && xe && ye && cosa && sina && A),
+                 "pf_panel_influence_matrix: NULL array");
+    pf::DeviceGuard dg(ctx->device);
+    if (m == 0) return PF_OK;
+    k_panel_influence<<<(unsigned)pf::ceil_div(m * m, PN_THREADS), PN_THREADS, 0,
+                        static_cast<cudaStream_t>(stream)>>>(m, xcp, ycp, xs, ys, xe, ye, cosa,
+                                                             sina, A);
+    return pf::launch_status("k_panel_influence");
+}
 
 extern "C" pf_status pf_panel_velocity(pf_ctx *ctx, int64_t m, const double *gamma,
                                        const double *xs, const double *ys, const double *xe,

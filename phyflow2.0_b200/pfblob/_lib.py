@@ -50,6 +50,9 @@ PROTOTYPES = {
     "pf_remesh_tutty": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp,
                         _vp, _vp, _c.POINTER(_i64), _vp],
     "pf_moments": [_vp, _i64, _vp, _vp, _vp, _vp, _vp],
+    "pf_panel_influence_matrix": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pf_dense_lu_factor": [_vp, _i64, _vp, _vp, _vp, _vp],
+    "pf_dense_lu_solve": [_vp, _i64, _vp, _vp, _vp, _vp],
     "pf_population_control": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _vp, _vp, _vp, _vp, _vp, _vp],
     "pf_remesh_population_control": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _dbl, _dbl,
                                      _i64, _vp, _vp, _vp, _vp, _vp, _c.POINTER(_i64),

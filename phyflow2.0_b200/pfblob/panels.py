@@ -1,7 +1,12 @@
-"""Vortex-panel induced velocity with pHyFlow's ``inducedVelocity`` surface
-(``src/python/panels/base/panelSolver.py:148-262``)."""
+"""Vortex panels with pHyFlow's ``panelSolver`` surface
+(``src/python/panels/base/panelSolver.py``): ``inducedVelocity`` (:148-262)
+and ``influenceMatrix`` (:31-144), plus the LU factor / solve pair the
+``Panels`` class uses for the panel strengths (``__panelsClass.py:782,
+:960-962``), all on the GPU."""
 import ctypes
+import warnings
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -42,3 +47,59 @@ def inducedVelocity(strength, xPanelStart, yPanelStart, xPanelEnd, yPanelEnd, co
     vx, vy = m.empty(xv.numel()), m.empty(xv.numel())
     panel_velocity_device(*arrs, xv, yv, vx, vy)
     return m.outs(vx, vy)
+
+
+def influenceMatrix(xCP, yCP, xPanelStart, yPanelStart, xPanelEnd, yPanelEnd, cosAlpha, sinAlpha,
+                    hardware=0, method=1, panelKernel=1):
+    """Self-induction influence matrix A (M x M) of constant-strength vortex
+    panels on their collocation points; same arguments and result as
+    pHyFlow's ``influenceMatrix``."""
+    if panelKernel != PANEL_KERNEL_CSV:
+        raise NotImplementedError("pfblob: only constant-strength vortex panels (panelKernel=1)")
+    if method != DIRECT_METHOD:
+        raise NotImplementedError("pfblob: the influence matrix is assembled directly (method=1)")
+    m = Marshal(xCP.device.index if isinstance(xCP, torch.Tensor) and xCP.is_cuda else None)
+    arrs = [m.dev(a) for a in (xCP, yCP, xPanelStart, yPanelStart, xPanelEnd, yPanelEnd,
+                               cosAlpha, sinAlpha)]
+    n = arrs[0].numel()
+    A = torch.empty((n, n), dtype=torch.float64, device=m.device)
+    _lib.check(_lib.lib.pf_panel_influence_matrix(_lib.context(m.index), n,
+                                                  *[ptr(a) for a in arrs], ptr(A), m.stream))
+    return m.outs(A)[0]
+
+
+def lu_factor(a, overwrite_a=False):
+    """LU factorisation with partial pivoting on the GPU, for ``lu_solve``
+    (the factors are this library's row-major form, not LAPACK's layout).
+    Returns (lu, piv) in the input's kind (numpy or CUDA tensors); warns, as
+    scipy does, when a diagonal of U is exactly zero."""
+    if len(a.shape) != 2 or a.shape[0] != a.shape[1]:
+        raise ValueError("expected a square matrix")
+    n = int(a.shape[0])
+    m = Marshal(a.device.index if isinstance(a, torch.Tensor) and a.is_cuda else None)
+    A = m.dev(a).reshape(n, n)
+    if isinstance(a, torch.Tensor) and a.is_cuda and not overwrite_a and A.data_ptr() == a.data_ptr():
+        A = A.clone()
+    piv = torch.empty(n, dtype=torch.int32, device=m.device)
+    info = torch.zeros(1, dtype=torch.int32, device=m.device)
+    _lib.check(_lib.lib.pf_dense_lu_factor(_lib.context(m.index), n, ptr(A), ptr(piv), ptr(info),
+                                           m.stream))
+    k = int(info.item())
+    if k > 0:
+        warnings.warn("Diagonal number %d is exactly zero. Singular matrix." % k, RuntimeWarning)
+    lu, p = m.outs(A, piv)
+    return lu, p
+
+
+def lu_solve(lu_and_piv, b):
+    """Solution x of A x = b from ``lu_factor``'s factors."""
+    lu, piv = lu_and_piv
+    m = Marshal(b.device.index if isinstance(b, torch.Tensor) and b.is_cuda else None)
+    LU = m.dev(lu)
+    P = piv.to(m.device, torch.int32) if isinstance(piv, torch.Tensor) else \
+        torch.from_numpy(np.ascontiguousarray(piv, dtype=np.int32)).to(m.device)
+    x = m.dev(b).clone()
+    n = x.numel()
+    _lib.check(_lib.lib.pf_dense_lu_solve(_lib.context(m.index), n, ptr(LU), ptr(P), ptr(x),
+                                          m.stream))
+    return m.outs(x)[0]

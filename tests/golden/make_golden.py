@@ -133,7 +133,7 @@ def rand_blobs(n, sigma, seed, lo=0.0, hi=1.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["popctl", "tutty", "vorticity"], default=None,
+    ap.add_argument("--only", choices=["popctl", "tutty", "vorticity", "influence"], default=None,
                     help="write only this group of fixtures")
     args = ap.parse_args()
     if args.only == "popctl":
@@ -144,6 +144,9 @@ def main():
         return
     if args.only == "vorticity":
         vorticity_fixtures()
+        return
+    if args.only == "influence":
+        influence_fixtures()
         return
     assert ref.available(), "build oracle/_ref first: make -C oracle ref"
 
@@ -209,7 +212,24 @@ def main():
     population_control_fixtures(args.ref)
     tutty_fixtures(args.ref)
     vorticity_fixtures()
+    influence_fixtures()
     print("golden fixtures written to", HERE)
+
+
+def influence_fixtures():
+    """9. the reference Cython assemble_influenceMatrix for 96 panels on the unit
+    cylinder, collocation points at the panel centres moved slightly inside."""
+    ps = wl.cylinder_panels(96, config=3, instance=11)
+    xc = 0.5 * (ps.xs + ps.xe)
+    yc = 0.5 * (ps.ys + ps.ye)
+    nx, ny = ps.sina, -ps.cosa  # inward of a counter-clockwise contour
+    r = np.hypot(xc, yc)
+    s = -1.0 if np.mean(nx * xc / r + ny * yc / r) > 0 else 1.0
+    xcp = xc + s * 1e-6 * nx
+    ycp = yc + s * 1e-6 * ny
+    A = ref.panel_influence(xcp, ycp, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina)
+    np.savez_compressed(os.path.join(HERE, "panel_influence.npz"), xcp=xcp, ycp=ycp, xs=ps.xs,
+                        ys=ps.ys, xe=ps.xe, ye=ps.ye, cosa=ps.cosa, sina=ps.sina, A=A)
 
 
 def vorticity_fixtures():

@@ -157,7 +157,7 @@ def run_ours(args, rank, world):
     n = b.n
     method = pick_method(args.method)
     meth_id = pfblob.FMM_METHOD if method == "fmm" else pfblob.DIRECT_METHOD
-    ks, xopt, cut = pfblob.fmm_parameters(b.sigma, b.k)
+    ks, xopt, cut = pfblob.fmm_parameters(b.sigma, b.k, tol=1e-6)
     xb, yb = b.bounds()
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     x, y, g = T(b.x), T(b.y), T(b.g)

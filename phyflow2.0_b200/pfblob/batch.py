@@ -13,9 +13,9 @@ import numpy as np
 import torch
 
 from . import _lib
+from .induced import default_cutoff
 from .tune import Tuner
 
-FMM_ALPHA = 1.2564312086261696770
 
 
 class Batch:
@@ -42,7 +42,7 @@ class Batch:
             overlap = float(s.get("overlap", 0.8))
             h = sigma * overlap
             ks = k * sigma * sigma
-            cutoff = 5.0 * math.sqrt(FMM_ALPHA * ks)
+            cutoff = default_cutoff(ks, tol)
             box = (float(mins[i, 0]), float(maxs[i, 0]), float(mins[i, 1]), float(maxs[i, 1]))
             if methods is not None:
                 m, L = int(methods[i]), int(leaf_levels[i]) if leaf_levels is not None else 0

@@ -108,7 +108,7 @@ class Blobs:
         return FMM_METHOD if self.velocityComputationParams['method'] == 'fmm' else DIRECT_METHOD
 
     def _velocity_at(self, xs, ys, xt, yt, Ndirect=35, tol=1.0e-6, cutoff=None):
-        ks, xo, cut = fmm_parameters(self.sigma, 2.0, cutoff)
+        ks, xo, cut = fmm_parameters(self.sigma, 2.0, cutoff, tol)
         vx = torch.empty_like(xt)
         vy = torch.empty_like(xt)
         velocity_device(xs, ys, self._g, ks, xt, yt, vx, vy, method=self._method(), xopt=xo,

@@ -31,12 +31,26 @@ DIRECT_METHOD = 1
 FMM_ALPHA = 1.2564312086261696770
 
 
-def fmm_parameters(sigma, k=2.0, cutoff=None):
-    """(ksigmasqr, xopt, cutoff) as ``_velocity_fmm_*_gauss`` derives them."""
+def default_cutoff(ksigmasqr, tol=1e-6):
+    """FMM near-field radius when the caller gives none.  The reference uses
+    5 xopt (``_induced.py:239-241``), where the Gaussian core's correction to
+    the point-vortex kernel, exp(-r^2/ksigmasqr), is 2e-14.  With a tolerance
+    the radius is lowered to where that correction is tol/100
+    (r^2 = ksigmasqr ln(100/tol)), never raised: beyond it the far field's
+    point-vortex expansions are exact to well below tol."""
+    cut = 5.0 * math.sqrt(FMM_ALPHA * ksigmasqr)
+    if tol and tol > 0.0:
+        cut = min(cut, math.sqrt(ksigmasqr * math.log(100.0 / tol)))
+    return cut
+
+
+def fmm_parameters(sigma, k=2.0, cutoff=None, tol=1e-6):
+    """(ksigmasqr, xopt, cutoff) as ``_velocity_fmm_*_gauss`` derives them,
+    the cutoff from ``default_cutoff`` unless given."""
     ksigmasqr = k * sigma * sigma
     xopt = math.sqrt(FMM_ALPHA * ksigmasqr)
     if cutoff is None:
-        cutoff = 5.0 * xopt
+        cutoff = default_cutoff(ksigmasqr, tol)
     return ksigmasqr, xopt, cutoff
 
 
@@ -57,7 +71,7 @@ def velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=DIRECT_METHOD, xo
         if xopt is None:
             xopt = math.sqrt(FMM_ALPHA * ksigmasqr)
         if cutoff is None:
-            cutoff = 5.0 * xopt
+            cutoff = default_cutoff(ksigmasqr, tol)
         if box is None:
             _lib.check(_lib.lib.pf_velocity_fmm(ctx, x.numel(), ptr(x), ptr(y), ptr(g),
                                                 xt.numel(), ptr(xt), ptr(yt), float(ksigmasqr),
@@ -94,7 +108,7 @@ def velocity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None, 
         if xt.numel() != yt.numel():
             raise ValueError("pfblob: xEval and yEval must have the same length")
     vx, vy = m.empty(xt.numel()), m.empty(xt.numel())
-    ksigmasqr, xopt, cut = fmm_parameters(float(sigma), float(k), cutoff)
+    ksigmasqr, xopt, cut = fmm_parameters(float(sigma), float(k), cutoff, float(tol))
     velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=method, xopt=xopt, cutoff=cut,
                     tol=float(tol), ndirect=int(Ndirect), device=m.index)
     return m.outs(vx, vy)

@@ -171,7 +171,7 @@ class Server:
         (resident state, no move) nothing here waits for the device: the FMM
         takes the cached box and the remesh the cached lattice window."""
         s = self.sims[req.sim]
-        ks, xo, cut = fmm_parameters(s.sigma, s.k)
+        ks, xo, cut = fmm_parameters(s.sigma, s.k, tol=self.tol)
         vx = torch.empty_like(s.x)
         vy = torch.empty_like(s.x)
         box = self._box(s)

@@ -152,7 +152,8 @@ class Tuner:
             return 1, 0
         w0 = max(box[1] - box[0], box[3] - box[2]) or 1.0
         if cutoff is None:
-            cutoff = 5.0 * math.sqrt(1.2564312086261696770 * ksigmasqr)
+            from .induced import default_cutoff
+            cutoff = default_cutoff(ksigmasqr, tol)
         t_direct = float(n) * n / self.rates["r_direct"]
         best = (t_direct, 1, 0)
         L0 = max(3, int(math.ceil(0.5 * math.log2(max(n, 2) / 35.0))))

@@ -163,17 +163,19 @@ k_place(int64_t n, const uint32_t *__restrict__ key, const int32_t *__restrict__
     perm[start[key[i]] + rank[i]] = (int32_t)i;
 }
 
-// Per leaf: order the leaf's particles by input index, then write the sorted
-// copies: FP64 (x, y[, g]) and hi/lo float4 (+ float g).
-__global__ void __launch_bounds__(256)
-k_order(int64_t nleaf, const int32_t *__restrict__ start, const int32_t *__restrict__ cnt,
-        int32_t *__restrict__ perm, const double *__restrict__ x, const double *__restrict__ y,
-        const double *__restrict__ g, double *__restrict__ sx, double *__restrict__ sy,
-        double *__restrict__ sg, float4 *__restrict__ hl, float *__restrict__ g32) {
-    const int64_t m = (int64_t)blockIdx.x * 256 + threadIdx.x;
+__host__ __device__ __forceinline__ int64_t level_off(int l) {
+    return ((((int64_t)1) << (2 * l)) - 1) / 3;
+}
+
+// Per leaf: order the leaf's particles by input index (the counting sort's
+// atomic ranks are not reproducible; this fixes every later sum's order).
+__global__ void __launch_bounds__(128)
+k_leaf_sort(int64_t nleaf, const int32_t *__restrict__ start, const int32_t *__restrict__ cnt,
+            int32_t *__restrict__ perm) {
+    const int64_t m = (int64_t)blockIdx.x * 128 + threadIdx.x;
     if (m >= nleaf) return;
     const int c = cnt[m];
-    if (c == 0) return;
+    if (c < 2) return;
     const int s0 = start[m];
     for (int k = 1; k < c; ++k) {
         const int32_t v = perm[s0 + k];
@@ -184,30 +186,56 @@ k_order(int64_t nleaf, const int32_t *__restrict__ start, const int32_t *__restr
         }
         perm[s0 + j + 1] = v;
     }
-    for (int k = 0; k < c; ++k) {
-        const int32_t i = perm[s0 + k];
-        const double a = x[i], b = y[i];
-        sx[s0 + k] = a;
-        sy[s0 + k] = b;
-        float4 h;
-        pfd::split_hilo(a, h.x, h.z);
-        pfd::split_hilo(b, h.y, h.w);
-        hl[s0 + k] = h;
-        if (g) {
-            const double gi = g[i];
-            sg[s0 + k] = gi;
-            g32[s0 + k] = (float)gi;
-        }
+}
+
+// Sorted copies of the points, one thread per sorted position (coalesced
+// writes): FP64 x, y (g), the hi/lo float4 and float g of the near field.
+__global__ void __launch_bounds__(256)
+k_gather_sorted(int64_t n, const int32_t *__restrict__ perm, const double *__restrict__ x,
+                const double *__restrict__ y, const double *__restrict__ g,
+                double *__restrict__ sx, double *__restrict__ sy, double *__restrict__ sg,
+                float4 *__restrict__ hl, float *__restrict__ g32) {
+    const int64_t j = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (j >= n) return;
+    const int32_t i = perm[j];
+    const double a = x[i], b = y[i];
+    sx[j] = a;
+    sy[j] = b;
+    float4 h;
+    pfd::split_hilo(a, h.x, h.z);
+    pfd::split_hilo(b, h.y, h.w);
+    hl[j] = h;
+    if (g) {
+        const double gi = g[i];
+        sg[j] = gi;
+        g32[j] = (float)gi;
     }
 }
 
-// box counts of level l from level l+1 (children 4m..4m+3)
+// Box counts of nlev (<= 4) coarser levels from level lc: CTA b owns the
+// 4^nlev level-lc boxes below box b of level lc - nlev (one contiguous Morton
+// range) and sums them up level by level in shared memory (integer sums:
+// exact, any order).
 __global__ void __launch_bounds__(256)
-k_count_up(int64_t nbox, const int32_t *__restrict__ child, int32_t *__restrict__ par) {
-    const int64_t m = (int64_t)blockIdx.x * 256 + threadIdx.x;
-    if (m >= nbox) return;
-    const int32_t *c = child + 4 * m;  // not 16-byte aligned in general
-    par[m] = c[0] + c[1] + c[2] + c[3];
+k_count_up(int lc, int nlev, int32_t *__restrict__ cnt_all) {
+    __shared__ int32_t s_c[256];
+    const int nch = 1 << (2 * nlev);
+    if ((int)threadIdx.x < nch)
+        s_c[threadIdx.x] = cnt_all[level_off(lc) + (int64_t)blockIdx.x * nch + threadIdx.x];
+    __syncthreads();
+    for (int j = 1; j <= nlev; ++j) {
+        const int np = nch >> (2 * j);
+        int32_t v = 0;
+        if ((int)threadIdx.x < np)
+            v = s_c[4 * threadIdx.x] + s_c[4 * threadIdx.x + 1] + s_c[4 * threadIdx.x + 2] +
+                s_c[4 * threadIdx.x + 3];
+        __syncthreads();
+        if ((int)threadIdx.x < np) {
+            s_c[threadIdx.x] = v;
+            cnt_all[level_off(lc - j) + (int64_t)blockIdx.x * np + threadIdx.x] = v;
+        }
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -252,9 +280,6 @@ k_p2m(int L, double x0, double y0, double wl, const int32_t *__restrict__ start,
     for (int k = 0; k < NP; ++k) M[base + k] = a[k];
 }
 
-__host__ __device__ __forceinline__ int64_t level_off(int l) {
-    return ((((int64_t)1) << (2 * l)) - 1) / 3;
-}
 
 // Boxes handled per warp by the translation kernels: with p+1 <= 16 terms two
 // boxes share a warp (one half-warp each, lane n = coefficient n), otherwise
@@ -900,17 +925,19 @@ static pf_status sort_points(int64_t n, const double *x, const double *y,
     PF_TRY(pf::exclusive_scan_i32(s.cnt, s.start, nleaf, scan_tmp, nullptr, st));
     k_place<<<gn, 256, 0, st>>>(n, s.key, s.rank, s.start, s.perm);
     PF_TRY(pf::launch_status("k_place"));
-    k_order<<<(unsigned)pf::ceil_div(nleaf, 256), 256, 0, st>>>(nleaf, s.start, s.cnt, s.perm, x, y,
-                                                               g, s.x, s.y, s.g, s.hl, s.g32);
-    return pf::launch_status("k_order");
+    k_leaf_sort<<<(unsigned)pf::ceil_div(nleaf, 128), 128, 0, st>>>(nleaf, s.start, s.cnt, s.perm);
+    PF_TRY(pf::launch_status("k_leaf_sort"));
+    k_gather_sorted<<<gn, 256, 0, st>>>(n, s.perm, x, y, g, s.x, s.y, s.g, s.hl, s.g32);
+    return pf::launch_status("k_gather_sorted");
 }
 
 static pf_status count_up(int L, int32_t *cnt_all, cudaStream_t st) {
-    for (int l = L - 1; l >= 0; --l) {
-        const int64_t nb = (int64_t)1 << (2 * l);
-        k_count_up<<<(unsigned)pf::ceil_div(nb, 256), 256, 0, st>>>(
-            nb, cnt_all + level_off(l + 1), cnt_all + level_off(l));
+    for (int lc = L; lc > 0;) {
+        const int nlev = lc < 4 ? lc : 4;
+        const int64_t nblk = (int64_t)1 << (2 * (lc - nlev));
+        k_count_up<<<(unsigned)nblk, 256, 0, st>>>(lc, nlev, cnt_all);
         PF_TRY(pf::launch_status("k_count_up"));
+        lc -= nlev;
     }
     return PF_OK;
 }
@@ -1015,7 +1042,11 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
         PF_TRY(sort_points(nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, st));
     }
     PF_TRY(count_up(L, scnt_all, st));
-    PF_TRY(count_up(L, tcnt_all, st));
+    if (same)  // identical pyramid
+        PF_CUDA_TRY(cudaMemcpyAsync(tcnt_all, scnt_all, sizeof(int32_t) * level_off(L),
+                                    cudaMemcpyDeviceToDevice, st));
+    else
+        PF_TRY(count_up(L, tcnt_all, st));
     k_sorted_keys<<<(unsigned)pf::ceil_div(nt, 256), 256, 0, st>>>(nt, T.perm, T.key, tkey_sorted);
     PF_TRY(pf::launch_status("k_sorted_keys"));
 

@@ -321,6 +321,53 @@ k_m2m(int l, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
     if (live && k < NP) M[bg * NP + k] = acc;
 }
 
+// M2M over two levels in one launch: CTA b owns box b of level lc - 2, its 4
+// children (level lc - 1) and 16 grandchildren (level lc).  The grandchildren
+// are staged in shared memory (empty boxes as zeros, which they do not
+// contribute), the children are formed there and written, then the parent.
+// Every coefficient is summed in the order of k_m2m (child c = 0..3, then
+// mm = 0..k), so the results are bitwise those of two k_m2m launches.
+template <int NP>
+__global__ void __launch_bounds__(256)
+k_m2m2(int lc, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
+       const double2 *__restrict__ opT /* [4][NP(m)][NP(k)] */) {
+    __shared__ double2 s_g[16][NP];
+    __shared__ double2 s_c[4][NP];
+    const int64_t pb = blockIdx.x;
+    const int64_t g0 = level_off(lc) + 16 * pb, c0 = level_off(lc - 1) + 4 * pb;
+    for (int t = threadIdx.x; t < 16 * NP; t += 256) {
+        const int gi = t / NP, k = t - gi * NP;
+        s_g[gi][k] = scnt[g0 + gi] != 0 ? M[(g0 + gi) * NP + k] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 4 * NP; t += 256) {
+        const int ci = t / NP, k = t - ci * NP;
+        double2 acc = make_double2(0.0, 0.0);
+        if (scnt[c0 + ci] != 0) {
+            for (int c = 0; c < 4; ++c) {
+                if (scnt[g0 + 4 * ci + c] == 0) continue;
+                const double2 *op = opT + (int64_t)c * NP * NP;
+                for (int mm = 0; mm <= k; ++mm)
+                    acc = cfma(op[mm * NP + k], s_g[4 * ci + c][mm], acc);
+            }
+            M[(c0 + ci) * NP + k] = acc;
+        }
+        s_c[ci][k] = acc;
+    }
+    __syncthreads();
+    const int64_t p = level_off(lc - 2) + pb;
+    for (int k = threadIdx.x; k < NP; k += 256) {
+        if (scnt[p] == 0) continue;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int c = 0; c < 4; ++c) {
+            if (scnt[c0 + c] == 0) continue;
+            const double2 *op = opT + (int64_t)c * NP * NP;
+            for (int mm = 0; mm <= k; ++mm) acc = cfma(op[mm * NP + k], s_c[c][mm], acc);
+        }
+        M[p * NP + k] = acc;
+    }
+}
+
 // M2L for all levels 2..L: lane n of a box group = local coefficient n
 template <int NP>
 __global__ void __launch_bounds__(WARP_BOX_THREADS)
@@ -418,6 +465,43 @@ k_l2l(int l, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
 #pragma unroll 4
         for (int mm = n; mm < NP; ++mm) acc = cfma(op[mm * NP + n], sb[mm], acc);
         Lc[bg * NP + n] = acc;
+    }
+}
+
+// L2L over two levels in one launch: CTA b owns box b of level lp, its 4
+// children (level lp + 1) and 16 grandchildren (level lp + 2); each child's
+// local expansion receives its parent's, then each grandchild its child's,
+// in the order of k_l2l (bitwise equal to two k_l2l launches).
+template <int NP>
+__global__ void __launch_bounds__(256)
+k_l2l2(int lp, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
+       const double2 *__restrict__ opT /* [4][NP(m)][NP(n)] */) {
+    __shared__ double2 s_p[NP];
+    __shared__ double2 s_c[4][NP];
+    const int64_t pb = blockIdx.x;
+    const int64_t p = level_off(lp) + pb;
+    const int64_t c0 = level_off(lp + 1) + 4 * pb, g0 = level_off(lp + 2) + 16 * pb;
+    for (int k = threadIdx.x; k < NP; k += 256) s_p[k] = Lc[p * NP + k];
+    __syncthreads();
+    for (int t = threadIdx.x; t < 4 * NP; t += 256) {
+        const int ci = t / NP, n = t - ci * NP;
+        double2 acc = make_double2(0.0, 0.0);
+        if (tcnt[c0 + ci] != 0) {
+            const double2 *op = opT + (int64_t)ci * NP * NP;
+            acc = Lc[(c0 + ci) * NP + n];
+            for (int mm = n; mm < NP; ++mm) acc = cfma(op[mm * NP + n], s_p[mm], acc);
+            Lc[(c0 + ci) * NP + n] = acc;
+        }
+        s_c[ci][n] = acc;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 16 * NP; t += 256) {
+        const int gi = t / NP, n = t - gi * NP;
+        if (tcnt[g0 + gi] == 0) continue;
+        const double2 *op = opT + (int64_t)(gi & 3) * NP * NP;
+        double2 acc = Lc[(g0 + gi) * NP + n];
+        for (int mm = n; mm < NP; ++mm) acc = cfma(op[mm * NP + n], s_c[gi >> 2][mm], acc);
+        Lc[(g0 + gi) * NP + n] = acc;
     }
 }
 
@@ -1056,10 +1140,17 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
                                                                  S.x, S.y, S.g, M);
     PF_TRY(pf::launch_status("k_p2m"));
     constexpr int BOXES_PER_CTA = (WARP_BOX_THREADS / 32) * BoxLanes<NP>::BPW;
-    for (int l = L - 1; l >= 2; --l) {
-        const int64_t nb = (int64_t)1 << (2 * l);
+    // parents at levels L-1 .. 2: two levels per launch, one more when odd
+    int lp = L - 1;
+    for (; lp - 1 >= 2; lp -= 2) {
+        k_m2m2<NP><<<(unsigned)((int64_t)1 << (2 * (lp - 1))), 256, 0, st>>>(lp + 1, scnt_all, M,
+                                                                            c.d_m2m);
+        PF_TRY(pf::launch_status("k_m2m2"));
+    }
+    if (lp >= 2) {
+        const int64_t nb = (int64_t)1 << (2 * lp);
         k_m2m<NP><<<(unsigned)pf::ceil_div(nb, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
-            l, scnt_all, M, c.d_m2m);
+            lp, scnt_all, M, c.d_m2m);
         PF_TRY(pf::launch_status("k_m2m"));
     }
     PF_TRY(mark(2));
@@ -1073,10 +1164,17 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
         PF_TRY(pf::launch_status("k_m2l"));
     }
     PF_TRY(mark(3));
-    for (int l = 3; l <= L; ++l) {
-        const int64_t nb = (int64_t)1 << (2 * l);
+    // child levels 3 .. L: two levels per launch, one more when odd
+    int lch = 3;
+    for (; lch + 1 <= L; lch += 2) {
+        k_l2l2<NP><<<(unsigned)((int64_t)1 << (2 * (lch - 1))), 256, 0, st>>>(lch - 1, tcnt_all, Lc,
+                                                                             c.d_l2l);
+        PF_TRY(pf::launch_status("k_l2l2"));
+    }
+    if (lch <= L) {
+        const int64_t nb = (int64_t)1 << (2 * lch);
         k_l2l<NP><<<(unsigned)pf::ceil_div(nb, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
-            l, tcnt_all, Lc, c.d_l2l);
+            lch, tcnt_all, Lc, c.d_l2l);
         PF_TRY(pf::launch_status("k_l2l"));
     }
     PF_TRY(mark(4));

@@ -278,7 +278,7 @@ constexpr int RG_TMAX = 16, RG_CAPMAX = 1536;  // 108 KB of records: 2 CTAs per 
 constexpr int RG_BMAX = RG_TMAX + 3;
 
 template <bool TUTTY>
-__global__ void __launch_bounds__(RG_TMAX *RG_TMAX)
+__global__ void __launch_bounds__(2 * RG_TMAX * RG_TMAX)
 k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, int32_t ixmin,
             int32_t iymin,
             const int32_t *__restrict__ start, const int32_t *__restrict__ count,
@@ -292,7 +292,7 @@ k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, 
     __shared__ int s_cn[RG_BMAX][RG_BMAX];  // its blob count
     __shared__ int s_colg[RG_BMAX], s_coln[RG_BMAX], s_col[RG_BMAX + 1];
     const int bw = tw + 3, bh = th + 3;
-    const int nthr = tw * th;
+    const int nthr = blockDim.x;  // twice the tile: the extra threads help build the weights
     const int64_t noy = nby + 3, nox = nbx + 3;
     const int64_t tile = blockIdx.x;
     const int64_t ox0 = (tile / tiles_y) * tw, oy0 = (tile % tiles_y) * th;
@@ -344,6 +344,7 @@ k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, 
         }
     }
     __syncthreads();
+    if ((int)threadIdx.x >= tw * th) return;
     const int tx = threadIdx.x / th, ty = threadIdx.x - tx * th;
     const int64_t ox = ox0 + tx, oy = oy0 + ty;
     if (ox >= nox || oy >= noy) return;
@@ -486,14 +487,14 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
         PF_CUDA_TRY(cudaFuncSetAttribute(k_rm_gather<true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          RG_CAPMAX * (int)sizeof(W9)));
-        k_rm_gather<true><<<(unsigned)tiles, TX * TY, smem, st>>>(
+        k_rm_gather<true><<<(unsigned)tiles, 2 * TX * TY, smem, st>>>(
             nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, perm, cell, x, y, g, wp, acc,
             flag);
     } else {
         PF_CUDA_TRY(cudaFuncSetAttribute(k_rm_gather<false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          RG_CAPMAX * (int)sizeof(W9)));
-        k_rm_gather<false><<<(unsigned)tiles, TX * TY, smem, st>>>(
+        k_rm_gather<false><<<(unsigned)tiles, 2 * TX * TY, smem, st>>>(
             nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, perm, cell, x, y, g, wp, acc,
             flag);
     }

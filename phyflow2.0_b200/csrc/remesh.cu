@@ -13,6 +13,7 @@
 //   4. k_rm_place  : blob index -> its slot.
 //   5. k_rm_sortcells : per base cell, order its blobs by input index (every
 //      sum below then has a fixed order, independent of atomic timing).
+//   5b. k_rm_sorted : x, y, g and base cell copied into cell order.
 //   6. k_rm_gather : per tile of output cells, the weights of the blobs of
 //      the covering base cells -- four x weights M4'(ux_a), four y weights
 //      M4'(uy_b) (_interpolation_kernels_1d.cpp:75-89; u as _regridding.py:183)
@@ -260,6 +261,23 @@ __device__ __forceinline__ W9 blob_w9(int32_t i, int64_t bx, int64_t by, int32_t
     return r;
 }
 
+// Blob coordinates, circulation and base cell in cell order (one thread per
+// sorted position: coalesced writes), so the gather below reads each base-cell
+// column as contiguous ranges.
+__global__ void __launch_bounds__(RM_THREADS)
+k_rm_sorted(const int32_t *__restrict__ nvalid, const int32_t *__restrict__ perm,
+            const int32_t *__restrict__ cell, const double *__restrict__ x,
+            const double *__restrict__ y, const double *__restrict__ g, double *__restrict__ xs,
+            double *__restrict__ ys, double *__restrict__ gs, int32_t *__restrict__ cs) {
+    const int64_t j = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
+    if (j >= *nvalid) return;
+    const int32_t i = perm[j];
+    xs[j] = x[i];
+    ys[j] = y[i];
+    gs[j] = g[i];
+    cs[j] = cell[i];
+}
+
 // Output cell grid: ox in [0, nbx+3), oy in [0, nby+3); lattice index
 // ix = ixmin + ox.  A base cell (bx, by) covers ox in bx..bx+3, oy in by..by+3.
 //
@@ -267,7 +285,8 @@ __device__ __forceinline__ W9 blob_w9(int32_t i, int64_t bx, int64_t by, int32_t
 // CTA first computes, into shared memory, the weight records of every blob
 // in the (tw+3) x (th+3) base cells covering the tile: per base-cell
 // column their cell-ordered positions are one contiguous range, so the
-// records are built from contiguous perm ranges, all columns at once.  Each
+// records are built from contiguous ranges of the cell-ordered copies (xs, ys,
+// gs, cs of k_rm_sorted), all columns at once.  Each
 // thread then sums (wx_a wy_b) g over the blobs of its 16 covering base cells
 // in a fixed order (b, a, blob) and flags cells touched by at least one
 // window (explicit zeros are kept, like the CSR sum of the reference,
@@ -282,10 +301,9 @@ __global__ void __launch_bounds__(2 * RG_TMAX * RG_TMAX)
 k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, int32_t ixmin,
             int32_t iymin,
             const int32_t *__restrict__ start, const int32_t *__restrict__ count,
-            const int32_t *__restrict__ perm, const int32_t *__restrict__ cell,
-            const double *__restrict__ x, const double *__restrict__ y,
-            const double *__restrict__ g, WParams wp, double *__restrict__ acc,
-            int32_t *__restrict__ flag) {
+            const int32_t *__restrict__ cs, const double *__restrict__ x,
+            const double *__restrict__ y, const double *__restrict__ g, WParams wp,
+            double *__restrict__ acc, int32_t *__restrict__ flag) {
     extern __shared__ double s_w_raw[];  // cap weight records
     W9 *s_w = reinterpret_cast<W9 *>(s_w_raw);
     __shared__ int s_cs[RG_BMAX][RG_BMAX];  // staged start of each base cell
@@ -326,9 +344,9 @@ k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, 
         for (int f = threadIdx.x; f < total; f += nthr) {
             int c = 0;
             while (s_col[c + 1] <= f) ++c;  // f < total, so c < bw
-            const int32_t i = perm[s_colg[c] + (f - s_col[c])];
+            const int32_t j = s_colg[c] + (f - s_col[c]);
             const int64_t bx = bx0 + c;
-            s_w[f] = blob_w9<TUTTY>(i, bx, cell[i] - bx * nby, ixmin, iymin, x, y, g, wp);
+            s_w[f] = blob_w9<TUTTY>(j, bx, cs[j] - bx * nby, ixmin, iymin, x, y, g, wp);
         }
         for (int k = threadIdx.x; k < bw * bh; k += nthr) {
             const int c = k / bh, r = k - c * bh;
@@ -373,8 +391,7 @@ k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, 
                 if (cnt == 0) continue;
                 touched = 1;
                 for (int k = 0; k < cnt; ++k) {
-                    const int32_t i = perm[s0 + k];
-                    const W9 r = blob_w9<TUTTY>(i, bx, by, ixmin, iymin, x, y, g, wp);
+                    const W9 r = blob_w9<TUTTY>(s0 + k, bx, by, ixmin, iymin, x, y, g, wp);
                     sum += (r.wx[a] * r.wy[b]) * r.g;
                 }
             }
@@ -426,7 +443,7 @@ static int64_t dense_cell_limit(int64_t n) {
 size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby) {
     const int64_t nbase = nbx * nby, ncell = (nbx + 3) * (nby + 3);
     const int64_t big = ncell > nbase ? ncell : nbase;
-    return align256(4 * n) * 3 + 2 * align256(4 * nbase) +
+    return align256(4 * n) * 4 + align256(8 * n) * 3 + 2 * align256(4 * nbase) +
            align256(8 * ncell) + 2 * align256(4 * ncell) + align256(4 * scan_tmp_ints(big)) +
            3 * align256(16) + align256(sizeof(PcState)) + popctl_scratch_bytes() + 1024;
 }
@@ -444,6 +461,10 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     int32_t *cell = (int32_t *)sc.take(4 * n);
     int32_t *rank = (int32_t *)sc.take(4 * n);
     int32_t *perm = (int32_t *)sc.take(4 * n);
+    double *xs = (double *)sc.take(8 * n);
+    double *ys = (double *)sc.take(8 * n);
+    double *gs = (double *)sc.take(8 * n);
+    int32_t *cs = (int32_t *)sc.take(4 * n);
     int32_t *count = (int32_t *)sc.take(4 * nbase);
     int32_t *start = (int32_t *)sc.take(4 * nbase);
     double *acc = (double *)sc.take(8 * ncell);
@@ -467,6 +488,8 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     k_rm_sortcells<<<(unsigned)ceil_div(nbase, RM_THREADS), RM_THREADS, 0, st>>>(nbase, start,
                                                                                 count, perm);
     PF_TRY(launch_status("k_rm_sortcells"));
+    k_rm_sorted<<<gn, RM_THREADS, 0, st>>>(nvalid, perm, cell, x, y, g, xs, ys, gs, cs);
+    PF_TRY(launch_status("k_rm_sorted"));
     // tile: the largest of 16x16, 16x8, 8x8, 8x4, 4x4 output cells whose
     // covering base cells hold, at 1.5x the mean density, at most RG_CAPMAX
     // blobs; shared memory for that many
@@ -488,14 +511,14 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          RG_CAPMAX * (int)sizeof(W9)));
         k_rm_gather<true><<<(unsigned)tiles, 2 * TX * TY, smem, st>>>(
-            nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, perm, cell, x, y, g, wp, acc,
+            nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, cs, xs, ys, gs, wp, acc,
             flag);
     } else {
         PF_CUDA_TRY(cudaFuncSetAttribute(k_rm_gather<false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          RG_CAPMAX * (int)sizeof(W9)));
         k_rm_gather<false><<<(unsigned)tiles, 2 * TX * TY, smem, st>>>(
-            nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, perm, cell, x, y, g, wp, acc,
+            nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, cs, xs, ys, gs, wp, acc,
             flag);
     }
     PF_TRY(launch_status("k_rm_gather"));

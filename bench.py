@@ -31,6 +31,8 @@ for _p in (ROOT, os.path.join(ROOT, "phyflow2.0_b200")):
 L2_BYTES = 126 * 2 ** 20
 MUFU_PER_SM_CLK = 16
 MUFU_PER_INTERACTION = 2  # ex2 + rcp
+FP32_PER_SM_CLK = 128
+FP32_OPS_FULL, FP32_OPS_FAR = 14, 11  # FP32 lane ops of one pair: with / without the ex2
 
 
 def peaks():
@@ -245,16 +247,25 @@ def run_ours(args, rank, world):
         st0 = fmm_stats[-1]
         ms_p2p = statistics.mean(f["ms_p2p"] for f in fmm_stats)
         pairs = st0["p2p_pairs"]
+        far = st0["p2p_pairs_far"]
         ach = pairs / (ms_p2p * 1e-3)
-        peak = (pk["sm_max_mhz"] * 1e6 * MUFU_PER_SM_CLK * torch.cuda.get_device_properties(dev)
-                .multi_processor_count / MUFU_PER_INTERACTION)
-        roof = {"bound": "mufu", "kernel": "k_p2p (FMM near field)", "achieved": ach / 1e9,
-                "peak": peak / 1e9, "unit": "Ginteractions/s", "frac": ach / peak,
-                "traffic": traffic.get("k_p2p"), "pairs_per_launch": pairs,
-                "launch_ms": ms_p2p,
-                "peak_source": f"{MUFU_PER_SM_CLK} MUFU/SM/clk x SMs x sm_max_mhz "
-                               f"({pk['source']}) / {MUFU_PER_INTERACTION} MUFU per interaction",
-                "per_unit": "1 interaction = 2 MUFU (ex2, rcp) + 14 FP32 flops"}
+        # two-pipe roofline: the launch cannot beat the busier of the MUFU and
+        # FP32 pipes; pairs in tiles beyond the Gaussian's reach skip the ex2
+        sm_clk = pk["sm_max_mhz"] * 1e6 * torch.cuda.get_device_properties(dev).multi_processor_count
+        t_mufu = (MUFU_PER_INTERACTION * pairs - far) / (MUFU_PER_SM_CLK * sm_clk)
+        t_fp32 = (FP32_OPS_FULL * (pairs - far) + FP32_OPS_FAR * far) / (FP32_PER_SM_CLK * sm_clk)
+        peak = pairs / max(t_mufu, t_fp32)
+        roof = {"bound": "mufu" if t_mufu >= t_fp32 else "fp32", "kernel": "k_p2p (FMM near field)",
+                "achieved": ach / 1e9, "peak": peak / 1e9, "unit": "Ginteractions/s",
+                "frac": ach / peak, "traffic": traffic.get("k_p2p"), "pairs_per_launch": pairs,
+                "pairs_far": far, "launch_ms": ms_p2p,
+                "pipe_ms": {"mufu": t_mufu * 1e3, "fp32": t_fp32 * 1e3},
+                "peak_source": f"pairs / max(MUFU ops / ({MUFU_PER_SM_CLK} MUFU/SM/clk), FP32 lane "
+                               f"ops / ({FP32_PER_SM_CLK} FP32/SM/clk)) x SMs x sm_max_mhz "
+                               f"({pk['source']})",
+                "per_unit": f"pair within the Gaussian's reach: 2 MUFU (ex2, rcp) + {FP32_OPS_FULL} "
+                            f"FP32 ops; pair in a source tile beyond it (pairs_far): 1 MUFU (rcp) + "
+                            f"{FP32_OPS_FAR} FP32 ops"}
         npt = st0["expansion_terms"]
         ms_m2l = statistics.mean(f["ms_m2l"] for f in fmm_stats)
         m2l_flops = st0["m2l_translations"] * 8.0 * npt * npt
@@ -267,6 +278,7 @@ def run_ours(args, rank, world):
                     "peak_source": "148 SMs x 64 FP64 FMA/clk x 2 x sm_max_mhz (nominal)"}
         fmm_info = {"leaf_level": st0["leaf_level"], "expansion_terms": npt,
                     "block_level_drop": st0["block_level_drop"], "p2p_pairs": pairs,
+                    "p2p_pairs_far": far,
                     "m2l_translations": st0["m2l_translations"],
                     "phase_ms": {k[3:]: statistics.mean(f[k] for f in fmm_stats)
                                  for k in ("ms_sort", "ms_upward", "ms_m2l", "ms_downward",

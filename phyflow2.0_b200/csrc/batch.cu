@@ -65,7 +65,7 @@ struct pf_batch {
     std::vector<std::vector<Job>> slot_jobs;
     std::vector<char *> slot_scratch;
     std::vector<size_t> slot_bytes;
-    unsigned long long *d_ctr = nullptr;  // 2 per slot
+    unsigned long long *d_ctr = nullptr;  // FMM_COUNTERS per slot
     pf::DirectInstance *d_dinst = nullptr;
     int2 *d_items = nullptr;
     int n_items = 0;
@@ -241,7 +241,7 @@ static pf_status batch_build(pf_batch *b, double tol) {
             return PF_ERR_OOM;
         }
     }
-    PF_CUDA_TRY(cudaMalloc(&b->d_ctr, sizeof(unsigned long long) * 2 * std::max(1, S)));
+    PF_CUDA_TRY(cudaMalloc(&b->d_ctr, sizeof(unsigned long long) * pf::fmmx::FMM_COUNTERS * std::max(1, S)));
     PF_CUDA_TRY(cudaMalloc(&b->d_totals, sizeof(int32_t) * std::max(1, n)));
     PF_CUDA_TRY(cudaMalloc(&b->d_bads, sizeof(int32_t) * std::max(1, n)));
     PF_CUDA_TRY(cudaMalloc(&b->d_status, sizeof(int32_t) * std::max(1, n)));
@@ -271,7 +271,7 @@ static pf_status batch_enqueue(pf_batch *b) {
             pf::Bump sc{b->slot_scratch[s], b->slot_bytes[s], 0};
             if (j.kind == 0) {
                 PF_TRY(pf::fmmx::plan_exec(b->plans[j.inst], sc, d.n, d.x, d.y, d.g, d.n, d.x, d.y,
-                                           d.ksigmasqr, d.vx, d.vy, b->d_ctr + 2 * s, nullptr, st));
+                                           d.ksigmasqr, d.vx, d.vy, b->d_ctr + pf::fmmx::FMM_COUNTERS * s, nullptr, st));
             } else {
                 PF_TRY(pf::remesh_core(sc, d.n, d.x, d.y, d.g, d.h, d.xb0, d.yb0, d.c,
                                        (int32_t)b->ixmin[j.inst], (int32_t)b->iymin[j.inst],

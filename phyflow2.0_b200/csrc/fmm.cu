@@ -51,8 +51,11 @@ constexpr int MAX_LEVEL = pf::fmmx::MAX_LEVEL;
 constexpr int P2P_SETUP_THREADS = 128;
 constexpr int P2P_QMAX = 1024;   // source leaves per P2P block
 constexpr int P2P_RUNS_SM = 64;  // runs staged in shared memory at a time
-constexpr int P2P_TILE = 64;     // sources per warp tile
-constexpr int P2P_MIN_CTAS = 32; // one-warp CTAs resident per SM (64 registers per thread)
+constexpr int P2P_BUF = 64;      // sources per warp buffer (three buffers)
+// unroll of the pair loop over a full chunk: the kernel holds nine copies of
+// it (targets per lane x mode), which must stay within the instruction cache
+constexpr int P2P_UNROLL = 4;
+constexpr int P2P_MIN_CTAS = 24; // one-warp CTAs resident per SM (shared memory bound)
 constexpr int WARP_BOX_THREADS = 128;  // 4 warps, one box each
 constexpr unsigned INVALID_KEY = 0xFFFFFFFFu;
 
@@ -572,11 +575,20 @@ k_p2p_runs(int L, int kb, const int2 *__restrict__ q, int nq, int nqp,
 // P2P near field: one warp (one CTA) per P2P block, up to three targets per
 // lane (a group of up to 96), warp-private source tiles of 64.  Targets a and
 // b of a lane run packed (f32x2), target c scalar; NT = targets per lane.
-// A tile whose sources all lie farther than the series radius
-// sqrt(r2_series) from the group's target box (with a rounding margin) runs
-// the pair code without the small-x check; every pair there has r2 above
-// r2_series, so results are bitwise those of the checked code.
-template <bool SERIES>
+// Pair code modes, chosen per source from its box distance to the group's
+// target box (with a rounding margin):
+//   P2P_FAR:    sources beyond sqrt(r2_far): no ex2 (1 - exp(-x) rounds to
+//               1.0f for every pair);
+//   P2P_FULL:   the other sources beyond the series radius sqrt(r2_series):
+//               no small-x check (every pair has r2 above r2_series);
+//   P2P_SERIES: the sources within it: the pair code with the check.
+// Each pair gives bitwise the value of the checked code.  The group's
+// sources stream through three warp buffers, one per mode (each in stream
+// order), and each buffer runs 32 sources at a time as it fills (the rest
+// when the group's stream ends).
+constexpr int P2P_FAR = 0, P2P_FULL = 1, P2P_SERIES = 2;
+
+template <int MODE>
 __device__ __forceinline__ void scalar_pair(const ulonglong2 &h, const ulonglong2 &l,
                                             unsigned long long g2, const float4 &t,
                                             const pfd::GaussParams &gp, float &px, float &py) {
@@ -589,50 +601,146 @@ __device__ __forceinline__ void scalar_pair(const ulonglong2 &h, const ulonglong
     const float dx = (t.x - sxh) + (t.z - sxl);
     const float dy = (t.y - syh) + (t.w - syl);
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
-    const float sc = pfd::gauss_s<SERIES>(r2, g, gp);
+    const float sc = MODE == P2P_FAR ? g * pfd::rcp_approx(r2)
+                                     : pfd::gauss_s<MODE == P2P_SERIES>(r2, g, gp);
     px = fmaf(-dy, sc, px);
     py = fmaf(dx, sc, py);
 }
 
-template <int NT, bool SERIES>
-__device__ __forceinline__ void p2p_tile(const ulonglong2 *__restrict__ shi,
-                                         const ulonglong2 *__restrict__ slo,
-                                         const unsigned long long *__restrict__ sg2, int cnt,
-                                         const float4 &ta, const float4 &tb, const float4 &tc,
-                                         const pfd::GaussParams &gp,
-                                         const pfd::GaussParams2 &gp2, float (&acc)[12]) {
+// One pair of the given mode for the lane's targets (NT per lane).
+template <int NT, int MODE>
+__device__ __forceinline__ void p2p_pair(const ulonglong2 &h, const ulonglong2 &l,
+                                         unsigned long long g2, pfd::f32x2 txh, pfd::f32x2 tyh,
+                                         pfd::f32x2 txl, pfd::f32x2 tyl, const float4 &ta,
+                                         const float4 &tc, const pfd::GaussParams &gp,
+                                         const pfd::GaussParams2 &gp2, pfd::f32x2 &nx,
+                                         pfd::f32x2 &ny, float &pxa, float &pya, float &pxc,
+                                         float &pyc) {
+    if (NT >= 2) {
+        if (MODE == P2P_FAR)
+            pfd::pair2_far(h, l, g2, txh, tyh, txl, tyl, gp2, nx, ny);
+        else
+            pfd::pair2<MODE == P2P_SERIES>(h, l, g2, txh, tyh, txl, tyl, gp2, nx, ny);
+    } else {
+        scalar_pair<MODE>(h, l, g2, ta, gp, pxa, pya);
+    }
+    if (NT == 3) scalar_pair<MODE>(h, l, g2, tc, gp, pxc, pyc);
+}
+
+// Shared-memory loads by 32-bit shared address (the chunk functions below
+// are separate calls, which see only generic pointers otherwise).
+__device__ __forceinline__ ulonglong2 lds_u64x2(uint32_t a) {
+    ulonglong2 v;
+    asm("ld.shared.v2.u64 {%0, %1}, [%2];" : "=l"(v.x), "=l"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ unsigned long long lds_u64(uint32_t a) {
+    unsigned long long v;
+    asm("ld.shared.u64 %0, [%1];" : "=l"(v) : "r"(a));
+    return v;
+}
+
+struct P2PSums {
+    float s[6];  // NT >= 2: -nx_a, ny_a, -nx_b, ny_b; NT = 1: px_a, py_a; NT = 3: px_c, py_c
+};
+
+// Sources [0, cnt) of a buffer (cnt <= 32) against the lane's targets; the
+// partial sums are returned for one compensated fold by the caller.  Each
+// (NT, MODE) is its own function, not inlined: nine inlined copies of the
+// unrolled loop in one kernel measured about 20% more instructions (register
+// copies between the copies' allocations) and instruction-cache stalls.
+// (A per-source choice of the checked code inside a chunk, by a warp-uniform
+// branch, measured slower too: the branch breaks the overlap of consecutive
+// pairs.)
+template <int NT, int MODE>
+__device__ __noinline__ P2PSums p2p_chunk_sums(uint32_t a_hi, uint32_t a_lo, uint32_t a_g, int cnt,
+                                               float4 ta, float4 tb, float4 tc,
+                                               pfd::GaussParams gp) {
+    const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
     const pfd::f32x2 txh = pfd::pack2(ta.x, tb.x), tyh = pfd::pack2(ta.y, tb.y);
     const pfd::f32x2 txl = pfd::pack2(ta.z, tb.z), tyl = pfd::pack2(ta.w, tb.w);
-    for (int c0 = 0; c0 < cnt; c0 += 32) {
-        pfd::f32x2 nx = 0ull, ny = 0ull;  // +0.0f in both halves
-        float pxa = 0.f, pya = 0.f, pxc = 0.f, pyc = 0.f;
-#pragma unroll 4
-        for (int k = 0; k < 32; ++k) {
-            if (NT >= 2) {
-                pfd::pair2<SERIES>(shi[c0 + k], slo[c0 + k], sg2[c0 + k], txh, tyh, txl, tyl,
-                                   gp2, nx, ny);
-            } else {
-                scalar_pair<SERIES>(shi[c0 + k], slo[c0 + k], sg2[c0 + k], ta, gp, pxa, pya);
-            }
-            if (NT == 3) scalar_pair<SERIES>(shi[c0 + k], slo[c0 + k], sg2[c0 + k], tc, gp, pxc, pyc);
-        }
-        if (NT >= 2) {
-            float nxa, nxb, nya, nyb;
-            pfd::unpack2(nx, nxa, nxb);
-            pfd::unpack2(ny, nya, nyb);
-            pfd::comp_add(acc[0], acc[1], -nxa);
-            pfd::comp_add(acc[2], acc[3], nya);
-            pfd::comp_add(acc[4], acc[5], -nxb);
-            pfd::comp_add(acc[6], acc[7], nyb);
-        } else {
-            pfd::comp_add(acc[0], acc[1], pxa);
-            pfd::comp_add(acc[2], acc[3], pya);
-        }
-        if (NT == 3) {
-            pfd::comp_add(acc[8], acc[9], pxc);
-            pfd::comp_add(acc[10], acc[11], pyc);
-        }
+    pfd::f32x2 nx = 0ull, ny = 0ull;  // +0.0f in both halves
+    float pxa = 0.f, pya = 0.f, pxc = 0.f, pyc = 0.f;
+    if (cnt == 32) {  // full chunk (the common case)
+#pragma unroll(P2P_UNROLL)
+        for (int k = 0; k < 32; ++k)
+            p2p_pair<NT, MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k),
+                               lds_u64(a_g + 8 * k), txh, tyh, txl, tyl, ta, tc, gp, gp2, nx, ny,
+                               pxa, pya, pxc, pyc);
+    } else {  // the rest of a buffer at the end of a group: kept small in code
+#pragma unroll 1
+        for (int k = 0; k < cnt; ++k)
+            p2p_pair<NT, MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k),
+                               lds_u64(a_g + 8 * k), txh, tyh, txl, tyl, ta, tc, gp, gp2, nx, ny,
+                               pxa, pya, pxc, pyc);
     }
+    P2PSums r;
+    if (NT >= 2) {
+        float nxa, nxb, nya, nyb;
+        pfd::unpack2(nx, nxa, nxb);
+        pfd::unpack2(ny, nya, nyb);
+        r.s[0] = -nxa;
+        r.s[1] = nya;
+        r.s[2] = -nxb;
+        r.s[3] = nyb;
+    } else {
+        r.s[0] = pxa;
+        r.s[1] = pya;
+        r.s[2] = r.s[3] = 0.f;
+    }
+    r.s[4] = pxc;
+    r.s[5] = pyc;
+    return r;
+}
+
+template <int NT, int MODE>
+__device__ __forceinline__ void p2p_chunk(const ulonglong2 *shi, const ulonglong2 *slo,
+                                          const unsigned long long *sg2, int cnt,
+                                          const float4 &ta, const float4 &tb, const float4 &tc,
+                                          const pfd::GaussParams &gp, float (&acc)[12]) {
+    const P2PSums r = p2p_chunk_sums<NT, MODE>(
+        (uint32_t)__cvta_generic_to_shared(shi), (uint32_t)__cvta_generic_to_shared(slo),
+        (uint32_t)__cvta_generic_to_shared(sg2), cnt, ta, tb, tc, gp);
+    pfd::comp_add(acc[0], acc[1], r.s[0]);
+    pfd::comp_add(acc[2], acc[3], r.s[1]);
+    if (NT >= 2) {
+        pfd::comp_add(acc[4], acc[5], r.s[2]);
+        pfd::comp_add(acc[6], acc[7], r.s[3]);
+    }
+    if (NT == 3) {
+        pfd::comp_add(acc[8], acc[9], r.s[4]);
+        pfd::comp_add(acc[10], acc[11], r.s[5]);
+    }
+}
+
+// Drop the first 32 entries of a source buffer holding 32 + rest: entries
+// [32, 32 + rest) move to [0, rest) (rest < 32).
+__device__ __forceinline__ void p2p_buf_shift(ulonglong2 *__restrict__ shi,
+                                              ulonglong2 *__restrict__ slo,
+                                              unsigned long long *__restrict__ sg2, int rest,
+                                              int lane) {
+    __syncwarp();
+    if (lane < rest) {
+        shi[lane] = shi[32 + lane];
+        slo[lane] = slo[32 + lane];
+        sg2[lane] = sg2[32 + lane];
+    }
+    __syncwarp();
+}
+
+// p2p_chunk for the group's targets-per-lane count nt (warp-uniform).
+template <int MODE>
+__device__ __forceinline__ void p2p_run_chunk(int nt, const ulonglong2 *shi, const ulonglong2 *slo,
+                                              const unsigned long long *sg2, int cnt,
+                                              const float4 &ta, const float4 &tb,
+                                              const float4 &tc, const pfd::GaussParams &gp,
+                                              float (&acc)[12]) {
+    if (nt == 2)
+        p2p_chunk<2, MODE>(shi, slo, sg2, cnt, ta, tb, tc, gp, acc);
+    else if (nt == 3)
+        p2p_chunk<3, MODE>(shi, slo, sg2, cnt, ta, tb, tc, gp, acc);
+    else
+        p2p_chunk<1, MODE>(shi, slo, sg2, cnt, ta, tb, tc, gp, acc);
 }
 
 __device__ __forceinline__ float warp_min(float v) {
@@ -656,11 +764,12 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
       unsigned long long *__restrict__ pairs) {
     __shared__ int s_rs[P2P_RUNS_SM];      // particle start of run
     __shared__ int s_rp[P2P_RUNS_SM + 1];  // stream prefix of run
-    __shared__ ulonglong2 s_hi[P2P_TILE];  // {x_hi, x_hi}, {y_hi, y_hi}
-    __shared__ ulonglong2 s_lo[P2P_TILE];  // {x_lo, x_lo}, {y_lo, y_lo}
-    __shared__ unsigned long long s_g2[P2P_TILE];  // {g, g}
-    const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
+    // source buffers, one per mode: [P2P_FAR], [P2P_FULL], [P2P_SERIES]
+    __shared__ ulonglong2 s_hi[3][P2P_BUF];  // {x_hi, x_hi}, {y_hi, y_hi}
+    __shared__ ulonglong2 s_lo[3][P2P_BUF];  // {x_lo, x_lo}, {y_lo, y_lo}
+    __shared__ unsigned long long s_g2[3][P2P_BUF];  // {g, g}
     const int lane = threadIdx.x;
+    const unsigned lt = (1u << lane) - 1u;
     const int64_t b = blockIdx.x;
     if (b >= nblk) return;
     const uint32_t leaf0 = (uint32_t)b << (2 * kb), nl = 1u << (2 * kb);
@@ -669,7 +778,7 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
     if (tn == 0) return;
     const int r0 = run_off[b], r1 = run_off[b + 1];
     const float rser = sqrtf(gp.r2_series);
-    unsigned long long npairs = 0;
+    unsigned long long npairs = 0, nfar = 0;
     for (int tg = 0; tg < tn; tg += 96) {
         const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane;
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -691,7 +800,11 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         const float mag = fmaxf(fmaxf(fabsf(bx0), fabsf(bx1)), fmaxf(fabsf(by0), fabsf(by1)));
         const float reach = rser * 1.001f + (mag + rser) * 4.8e-7f + 1e-30f;
         const float reach2 = reach * reach;
+        const float rfar = sqrtf(gp.r2_far);
+        const float reachf = rfar * 1.001f + (mag + rfar) * 4.8e-7f + 1e-30f;
+        const float reachf2 = reachf * reachf;
         float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int c0 = 0, c1 = 0, c2 = 0;  // entries waiting in the three buffers
         for (int rc = r0; rc < r1; rc += P2P_RUNS_SM) {
             const int nrc = min(P2P_RUNS_SM, r1 - rc);
             int pre = 0;
@@ -719,55 +832,80 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
             __syncwarp();
             const int S = pre;
             npairs += (unsigned long long)S * (unsigned long long)min(96, tn - tg);
-            // each lane's two stream positions only move forward (by 64 per
-            // tile), so the run holding them is found by advancing an index:
-            // the largest r with prefix[r] <= p (empty runs are stepped over)
-            int rr[2] = {0, 0};
-            for (int s0 = 0; s0 < S; s0 += P2P_TILE) {
-                bool near = false;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int p = s0 + h * 32 + lane;
-                    float4 spv = z4;
-                    float gg = 0.f;
-                    if (p < S) {
-                        int r = rr[h];
-                        while (r + 1 < nrc && s_rp[r + 1] <= p) ++r;
-                        rr[h] = r;
-                        const int src = s_rs[r] + (p - s_rp[r]);
-                        spv = shl[src];
-                        gg = sg32[src];
-                        const float ex = fmaxf(fmaxf(bx0 - spv.x, spv.x - bx1), 0.f);
-                        const float ey = fmaxf(fmaxf(by0 - spv.y, spv.y - by1), 0.f);
-                        near |= !(ex * ex + ey * ey > reach2);
-                    }
-                    s_hi[h * 32 + lane] =
-                        make_ulonglong2(pfd::pack2(spv.x, spv.x), pfd::pack2(spv.y, spv.y));
-                    s_lo[h * 32 + lane] =
-                        make_ulonglong2(pfd::pack2(spv.z, spv.z), pfd::pack2(spv.w, spv.w));
-                    s_g2[h * 32 + lane] = pfd::pack2(gg, gg);
+            // each lane's stream position only moves forward (by 32 per
+            // round), so the run holding it is found by advancing an index:
+            // the largest r with prefix[r] <= p (empty runs are stepped over).
+            // The loads of round s0 + 32 are issued before round s0's chunks
+            // run, so their latency overlaps the pair work.
+            int rr = 0;
+            float4 spv = z4;
+            float gg = 0.f;
+            auto fetch = [&](int p, float4 &v, float &w) {
+                if (p < S) {
+                    while (rr + 1 < nrc && s_rp[rr + 1] <= p) ++rr;
+                    const int src = s_rs[rr] + (p - s_rp[rr]);
+                    v = shl[src];
+                    w = sg32[src];
                 }
-                const bool series = __any_sync(0xffffffffu, near);
-                __syncwarp();
-                const int cnt = min(P2P_TILE, S - s0);
-                if (series) {
-                    if (nt == 2)
-                        p2p_tile<2, true>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
-                    else if (nt == 3)
-                        p2p_tile<3, true>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
-                    else
-                        p2p_tile<1, true>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
-                } else {
-                    if (nt == 2)
-                        p2p_tile<2, false>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
-                    else if (nt == 3)
-                        p2p_tile<3, false>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
-                    else
-                        p2p_tile<1, false>(s_hi, s_lo, s_g2, cnt, ta, tb, tc, gp, gp2, acc);
+            };
+            fetch(lane, spv, gg);
+            for (int s0 = 0; s0 < S; s0 += 32) {
+                const int p = s0 + lane;
+                int cls = -1;  // 0 far, 1 full, 2 series; -1 past the stream
+                if (p < S) {
+                    const float ex = fmaxf(fmaxf(bx0 - spv.x, spv.x - bx1), 0.f);
+                    const float ey = fmaxf(fmaxf(by0 - spv.y, spv.y - by1), 0.f);
+                    const float d2 = ex * ex + ey * ey;
+                    cls = d2 > reachf2 ? 0 : d2 > reach2 ? 1 : 2;
                 }
+                // append each source to the buffer of its mode, in stream order
+                const unsigned m0 = __ballot_sync(0xffffffffu, cls == 0);
+                const unsigned m1 = __ballot_sync(0xffffffffu, cls == 1);
+                const unsigned m2 = __ballot_sync(0xffffffffu, cls == 2);
+                if (cls >= 0) {
+                    const unsigned mm = cls == 0 ? m0 : cls == 1 ? m1 : m2;
+                    const int k = (cls == 0 ? c0 : cls == 1 ? c1 : c2) + __popc(mm & lt);
+                    s_hi[cls][k] = make_ulonglong2(pfd::pack2(spv.x, spv.x),
+                                                   pfd::pack2(spv.y, spv.y));
+                    s_lo[cls][k] = make_ulonglong2(pfd::pack2(spv.z, spv.z),
+                                                   pfd::pack2(spv.w, spv.w));
+                    s_g2[cls][k] = pfd::pack2(gg, gg);
+                }
+                c0 += __popc(m0);
+                c1 += __popc(m1);
+                c2 += __popc(m2);
+                spv = z4;
+                gg = 0.f;
+                fetch(p + 32, spv, gg);
                 __syncwarp();
+                if (c0 >= 32) {
+                    p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], 32, ta, tb, tc, gp, acc);
+                    nfar += 32ull * (unsigned long long)min(96, tn - tg);
+                    c0 -= 32;
+                    p2p_buf_shift(s_hi[0], s_lo[0], s_g2[0], c0, lane);
+                }
+                if (c1 >= 32) {
+                    p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], 32, ta, tb, tc, gp, acc);
+                    c1 -= 32;
+                    p2p_buf_shift(s_hi[1], s_lo[1], s_g2[1], c1, lane);
+                }
+                if (c2 >= 32) {
+                    p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], 32, ta, tb, tc, gp,
+                                              acc);
+                    c2 -= 32;
+                    p2p_buf_shift(s_hi[2], s_lo[2], s_g2[2], c2, lane);
+                }
             }
         }
+        // what is left in the buffers (fewer than 32 each)
+        if (c0)
+            p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], c0, ta, tb, tc, gp, acc);
+        nfar += (unsigned long long)c0 * (unsigned long long)min(96, tn - tg);
+        if (c1)
+            p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], c1, ta, tb, tc, gp, acc);
+        if (c2)
+            p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], c2, ta, tb, tc, gp, acc);
+        __syncwarp();
         if (ia < tn)
             nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),
                                           INV_2PI * ((double)acc[2] + (double)acc[3]));
@@ -778,7 +916,10 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
             nearv[t0 + ic] = make_double2(INV_2PI * ((double)acc[8] + (double)acc[9]),
                                           INV_2PI * ((double)acc[10] + (double)acc[11]));
     }
-    if (lane == 0) atomicAdd(pairs, npairs);
+    if (lane == 0) {
+        atomicAdd(pairs, npairs);
+        atomicAdd(pairs + 2, nfar);
+    }
 }
 
 // L2P + near + scatter to input order: one thread per sorted target
@@ -1058,7 +1199,8 @@ static size_t fmm_scratch_bytes(const FmmCache &c, int64_t ns, int64_t nt, bool 
 
 // Run the FMM for one blob set on `st` with a built plan and a scratch region
 // of fmm_scratch_bytes(); enqueues kernels only (no host synchronisation).
-// ctr: 2 device counters (P2P pairs, M2L translations), zeroed here.
+// ctr: FMM_COUNTERS device counters (P2P pairs, M2L translations, P2P pairs
+// evaluated without the exponential), zeroed here.
 // ev: 7 events recorded around the phases, or nullptr.
 template <int NP>
 static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, double x0,
@@ -1111,7 +1253,7 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
         T.start = tstart;
     }
 
-    PF_CUDA_TRY(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st));
+    PF_CUDA_TRY(cudaMemsetAsync(ctr, 0, pf::fmmx::FMM_COUNTERS * sizeof(unsigned long long), st));
     auto mark = [&](int k) -> pf_status {
         if (ev) PF_CUDA_TRY(cudaEventRecord(ev[k], st));
         return PF_OK;
@@ -1470,10 +1612,11 @@ extern "C" pf_status pf_fmm_last_stats(pf_ctx *ctx, pf_fmm_stats *out) {
     s.ms_sort = s.ms_upward = s.ms_m2l = s.ms_downward = s.ms_p2p = s.ms_l2p = s.ms_total = -1.f;
     if (!s.used_direct) {
         PF_CUDA_TRY(cudaStreamSynchronize(ctx->last_stream));
-        unsigned long long c[2];
+        unsigned long long c[pf::fmmx::FMM_COUNTERS];
         PF_CUDA_TRY(cudaMemcpy(c, ctx->dev_small, sizeof(c), cudaMemcpyDeviceToHost));
         s.p2p_pairs = (int64_t)c[0];
         s.m2l_translations = (int64_t)c[1];
+        s.p2p_pairs_far = (int64_t)c[2];
         if (ctx->fmm_profile) {
             float t[6];
             for (int k = 0; k < 6; ++k) PF_CUDA_TRY(cudaEventElapsedTime(&t[k], ctx->ev[k], ctx->ev[k + 1]));

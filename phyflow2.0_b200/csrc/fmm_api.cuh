@@ -28,6 +28,8 @@ int auto_level(int64_t ns, int ndirect);
 // expansion terms for a tolerance
 int np_for_tol(double tol);
 constexpr int MAX_LEVEL = 11;
+// device counters one FMM call writes (see exec_fmm)
+constexpr int FMM_COUNTERS = 3;
 
 }  // namespace fmmx
 }  // namespace pf

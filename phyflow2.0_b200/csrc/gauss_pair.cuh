@@ -12,18 +12,23 @@
 // * 1 - exp(-x) cancels for small x = r2/ksigmasqr; below X_SERIES it is
 //   replaced by its Taylor series x(1 - x/2 + x^2/6 - ...) to x^6, whose
 //   truncation error at x = X_SERIES is below 5e-8 relative.
+// * Where r2 * log2(e)/ksigmasqr >= Y_FAR = 26, ex2 returns below 2^-25 and
+//   1 - ex2(...) rounds to 1.0f exactly, so s = g * rcp(r2) bitwise: callers
+//   that know every pair of a tile lies that far (pair2_far) skip the ex2.
 #pragma once
 #include "pf_common.cuh"
 
 namespace pfd {
 
 constexpr float X_SERIES = 0.25f;
+constexpr double Y_FAR = 26.0;
 constexpr float LOG2E_F = 1.4426950408889634f;
 
 struct GaussParams {
     float c_t;       // -log2(e)/ksigmasqr  (argument of ex2)
     float c_x;       // 1/ksigmasqr
     float r2_series; // X_SERIES * ksigmasqr
+    float r2_far;    // Y_FAR * ksigmasqr / log2(e): beyond it 1 - exp(-x) is 1.0f
 };
 
 __host__ __device__ inline GaussParams make_gauss_params(double ksigmasqr) {
@@ -31,6 +36,7 @@ __host__ __device__ inline GaussParams make_gauss_params(double ksigmasqr) {
     p.c_t = (float)(-1.4426950408889634 / ksigmasqr);
     p.c_x = (float)(1.0 / ksigmasqr);
     p.r2_series = (float)(0.25 * ksigmasqr);
+    p.r2_far = (float)(Y_FAR / 1.4426950408889634 * ksigmasqr);
     return p;
 }
 
@@ -143,6 +149,22 @@ __device__ __forceinline__ void pair2(const ulonglong2 &hi, const ulonglong2 &lo
         om = pack2(oa, ob);
     }
     const f32x2 s = mul2(mul2(g2, om), pack2(rcp_approx(ra), rcp_approx(rb)));
+    nx = fma2(dy, s, nx);
+    ny = fma2(dx, s, ny);
+}
+
+// pair2 for pairs known to have r2 * log2(e)/ksigmasqr >= Y_FAR (see the file
+// comment): om is 1.0f there and g * 1.0f = g, so this is bitwise pair2
+// without the ex2.
+__device__ __forceinline__ void pair2_far(const ulonglong2 &hi, const ulonglong2 &lo, f32x2 g2,
+                                          f32x2 txh, f32x2 tyh, f32x2 txl, f32x2 tyl,
+                                          const GaussParams2 &gp, f32x2 &nx, f32x2 &ny) {
+    const f32x2 dx = add2(sub2(txh, hi.x), sub2(txl, lo.x));
+    const f32x2 dy = add2(sub2(tyh, hi.y), sub2(tyl, lo.y));
+    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, gp.eps));
+    float ra, rb;
+    unpack2(r2, ra, rb);
+    const f32x2 s = mul2(g2, pack2(rcp_approx(ra), rcp_approx(rb)));
     nx = fma2(dy, s, nx);
     ny = fma2(dx, s, ny);
 }

@@ -145,7 +145,7 @@ class FmmStats(_c.Structure):
                 ("m2l_translations", _c.c_int64), ("ms_sort", _c.c_float),
                 ("ms_upward", _c.c_float), ("ms_m2l", _c.c_float), ("ms_downward", _c.c_float),
                 ("ms_p2p", _c.c_float), ("ms_l2p", _c.c_float), ("ms_total", _c.c_float),
-                ("reserved", _c.c_float)]
+                ("reserved", _c.c_float), ("p2p_pairs_far", _c.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -713,6 +713,22 @@ __device__ __forceinline__ void p2p_chunk(const ulonglong2 *shi, const ulonglong
     }
 }
 
+// The third target slot of a group of 65..96 targets: the rem = size - 64
+// remainder targets are spread over the warp, m = 32 / rem lanes per target,
+// lane (j + rem q) taking sources q, q + m, q + 2m, ... of the chunk for
+// target j; the m partial sums are combined at the end of the group.  Lanes
+// with no share get q >= 32.
+template <int MODE>
+__device__ __noinline__ float2 p2p_split_sums(uint32_t a_hi, uint32_t a_lo, uint32_t a_g, int cnt,
+                                              int q, int m, float4 tc, pfd::GaussParams gp) {
+    float px = 0.f, py = 0.f;
+#pragma unroll 2
+    for (int k = q; k < cnt; k += m)
+        scalar_pair<MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k), lds_u64(a_g + 8 * k),
+                          tc, gp, px, py);
+    return make_float2(px, py);
+}
+
 // Drop the first 32 entries of a source buffer holding 32 + rest: entries
 // [32, 32 + rest) move to [0, rest) (rest < 32).
 __device__ __forceinline__ void p2p_buf_shift(ulonglong2 *__restrict__ shi,
@@ -729,18 +745,26 @@ __device__ __forceinline__ void p2p_buf_shift(ulonglong2 *__restrict__ shi,
 }
 
 // p2p_chunk for the group's targets-per-lane count nt (warp-uniform).
+// nt = 3: targets a, b packed plus the lane's share (qs of msp) of a
+// remainder target c.
 template <int MODE>
 __device__ __forceinline__ void p2p_run_chunk(int nt, const ulonglong2 *shi, const ulonglong2 *slo,
                                               const unsigned long long *sg2, int cnt,
                                               const float4 &ta, const float4 &tb,
-                                              const float4 &tc, const pfd::GaussParams &gp,
-                                              float (&acc)[12]) {
-    if (nt == 2)
-        p2p_chunk<2, MODE>(shi, slo, sg2, cnt, ta, tb, tc, gp, acc);
-    else if (nt == 3)
-        p2p_chunk<3, MODE>(shi, slo, sg2, cnt, ta, tb, tc, gp, acc);
-    else
+                                              const float4 &tc, int qs, int msp,
+                                              const pfd::GaussParams &gp, float (&acc)[12]) {
+    if (nt == 1) {
         p2p_chunk<1, MODE>(shi, slo, sg2, cnt, ta, tb, tc, gp, acc);
+        return;
+    }
+    p2p_chunk<2, MODE>(shi, slo, sg2, cnt, ta, tb, tc, gp, acc);
+    if (nt == 3) {
+        const float2 r = p2p_split_sums<MODE>(
+            (uint32_t)__cvta_generic_to_shared(shi), (uint32_t)__cvta_generic_to_shared(slo),
+            (uint32_t)__cvta_generic_to_shared(sg2), cnt, qs, msp, tc, gp);
+        pfd::comp_add(acc[8], acc[9], r.x);
+        pfd::comp_add(acc[10], acc[11], r.y);
+    }
 }
 
 __device__ __forceinline__ float warp_min(float v) {
@@ -780,17 +804,23 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
     const float rser = sqrtf(gp.r2_series);
     unsigned long long npairs = 0, nfar = 0;
     for (int tg = 0; tg < tn; tg += 96) {
-        const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane;
+        const int gsz = min(96, tn - tg);
+        const int nt = (gsz <= 32) ? 1 : (gsz <= 64) ? 2 : 3;  // warp-uniform
+        // nt = 3: remainder targets tg + 64 + j, j < rem, each on msp lanes
+        const int rem = nt == 3 ? gsz - 64 : 32;
+        const int msp = 32 / rem;
+        const bool cval = nt == 3 && lane < rem * msp;
+        const int qs = cval ? lane / rem : 32;
+        const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane % rem;
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 ta = (ia < tn) ? thl[t0 + ia] : z4;
         const float4 tb = (ib < tn) ? thl[t0 + ib] : z4;
-        const float4 tc = (ic < tn) ? thl[t0 + ic] : z4;
-        const int nt = (tn - tg <= 32) ? 1 : (tn - tg <= 64) ? 2 : 3;  // warp-uniform
+        const float4 tc = cval ? thl[t0 + ic] : z4;
         // box of the group's targets (hi parts), for the series-free test
         float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
         if (ia < tn) { bx0 = bx1 = ta.x; by0 = by1 = ta.y; }
         if (ib < tn) { bx0 = fminf(bx0, tb.x); bx1 = fmaxf(bx1, tb.x); by0 = fminf(by0, tb.y); by1 = fmaxf(by1, tb.y); }
-        if (ic < tn) { bx0 = fminf(bx0, tc.x); bx1 = fmaxf(bx1, tc.x); by0 = fminf(by0, tc.y); by1 = fmaxf(by1, tc.y); }
+        if (cval) { bx0 = fminf(bx0, tc.x); bx1 = fmaxf(bx1, tc.x); by0 = fminf(by0, tc.y); by1 = fmaxf(by1, tc.y); }
         bx0 = warp_min(bx0);
         bx1 = warp_max(bx1);
         by0 = warp_min(by0);
@@ -879,19 +909,21 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                 fetch(p + 32, spv, gg);
                 __syncwarp();
                 if (c0 >= 32) {
-                    p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], 32, ta, tb, tc, gp, acc);
+                    p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], 32, ta, tb, tc,
+                                           qs, msp, gp, acc);
                     nfar += 32ull * (unsigned long long)min(96, tn - tg);
                     c0 -= 32;
                     p2p_buf_shift(s_hi[0], s_lo[0], s_g2[0], c0, lane);
                 }
                 if (c1 >= 32) {
-                    p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], 32, ta, tb, tc, gp, acc);
+                    p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], 32, ta, tb, tc,
+                                            qs, msp, gp, acc);
                     c1 -= 32;
                     p2p_buf_shift(s_hi[1], s_lo[1], s_g2[1], c1, lane);
                 }
                 if (c2 >= 32) {
-                    p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], 32, ta, tb, tc, gp,
-                                              acc);
+                    p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], 32, ta, tb, tc,
+                                              qs, msp, gp, acc);
                     c2 -= 32;
                     p2p_buf_shift(s_hi[2], s_lo[2], s_g2[2], c2, lane);
                 }
@@ -899,12 +931,15 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         }
         // what is left in the buffers (fewer than 32 each)
         if (c0)
-            p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], c0, ta, tb, tc, gp, acc);
+            p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], c0, ta, tb, tc,
+                                   qs, msp, gp, acc);
         nfar += (unsigned long long)c0 * (unsigned long long)min(96, tn - tg);
         if (c1)
-            p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], c1, ta, tb, tc, gp, acc);
+            p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], c1, ta, tb, tc,
+                                    qs, msp, gp, acc);
         if (c2)
-            p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], c2, ta, tb, tc, gp, acc);
+            p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], c2, ta, tb, tc,
+                                      qs, msp, gp, acc);
         __syncwarp();
         if (ia < tn)
             nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),
@@ -912,9 +947,23 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         if (ib < tn)
             nearv[t0 + ib] = make_double2(INV_2PI * ((double)acc[4] + (double)acc[5]),
                                           INV_2PI * ((double)acc[6] + (double)acc[7]));
-        if (ic < tn)
-            nearv[t0 + ic] = make_double2(INV_2PI * ((double)acc[8] + (double)acc[9]),
-                                          INV_2PI * ((double)acc[10] + (double)acc[11]));
+        if (nt == 3) {  // combine the msp shares of each remainder target, in lane order
+            float h0 = acc[8], l0 = acc[9], h1 = acc[10], l1 = acc[11];
+            for (int q = 1; q < msp; ++q) {
+                const int sl = lane % rem + rem * q;  // < rem * msp <= 32
+                const float a = __shfl_sync(0xffffffffu, acc[8], sl);
+                const float b = __shfl_sync(0xffffffffu, acc[9], sl);
+                const float c = __shfl_sync(0xffffffffu, acc[10], sl);
+                const float d = __shfl_sync(0xffffffffu, acc[11], sl);
+                pfd::comp_add(h0, l0, a);
+                l0 += b;
+                pfd::comp_add(h1, l1, c);
+                l1 += d;
+            }
+            if (lane < rem)
+                nearv[t0 + ic] = make_double2(INV_2PI * ((double)h0 + (double)l0),
+                                              INV_2PI * ((double)h1 + (double)l1));
+        }
     }
     if (lane == 0) {
         atomicAdd(pairs, npairs);

@@ -652,27 +652,64 @@ struct P2PSums {
 // (A per-source choice of the checked code inside a chunk, by a warp-uniform
 // branch, measured slower too: the branch breaks the overlap of consecutive
 // pairs.)
+//
+// P2P_FAR chunks hold coordinates relative to the group centre (cx, cy), one
+// float each: {x - cx, x - cx, y - cy, y - cy} in the hi slot (pair2_far_local).
+__device__ __forceinline__ void far_local_scalar(const ulonglong2 &loc, unsigned long long g2,
+                                                 float tx, float ty, float &px, float &py) {
+    float lx, ly, g, dummy;
+    pfd::unpack2(loc.x, lx, dummy);
+    pfd::unpack2(loc.y, ly, dummy);
+    pfd::unpack2(g2, g, dummy);
+    const float dx = tx - lx, dy = ty - ly;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, 1e-12f));
+    const float sc = g * pfd::rcp_approx(r2);
+    px = fmaf(-dy, sc, px);
+    py = fmaf(dx, sc, py);
+}
+
 template <int NT, int MODE>
 __device__ __noinline__ P2PSums p2p_chunk_sums(uint32_t a_hi, uint32_t a_lo, uint32_t a_g, int cnt,
-                                               float4 ta, float4 tb, float4 tc,
-                                               pfd::GaussParams gp) {
+                                               float4 ta, float4 tb, float4 tc, float cx,
+                                               float cy, pfd::GaussParams gp) {
     const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
-    const pfd::f32x2 txh = pfd::pack2(ta.x, tb.x), tyh = pfd::pack2(ta.y, tb.y);
-    const pfd::f32x2 txl = pfd::pack2(ta.z, tb.z), tyl = pfd::pack2(ta.w, tb.w);
     pfd::f32x2 nx = 0ull, ny = 0ull;  // +0.0f in both halves
     float pxa = 0.f, pya = 0.f, pxc = 0.f, pyc = 0.f;
-    if (cnt == 32) {  // full chunk (the common case)
+    if constexpr (MODE == P2P_FAR) {
+        const float axc = (ta.x - cx) + ta.z, ayc = (ta.y - cy) + ta.w;
+        const pfd::f32x2 txc = pfd::pack2(axc, (tb.x - cx) + tb.z);
+        const pfd::f32x2 tyc = pfd::pack2(ayc, (tb.y - cy) + tb.w);
+        auto one = [&](int k) {
+            const ulonglong2 loc = lds_u64x2(a_hi + 16 * k);
+            const unsigned long long g2 = lds_u64(a_g + 8 * k);
+            if (NT >= 2)
+                pfd::pair2_far_local(loc, g2, txc, tyc, gp2, nx, ny);
+            else
+                far_local_scalar(loc, g2, axc, ayc, pxa, pya);
+        };
+        if (cnt == 32) {
 #pragma unroll(P2P_UNROLL)
-        for (int k = 0; k < 32; ++k)
-            p2p_pair<NT, MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k),
-                               lds_u64(a_g + 8 * k), txh, tyh, txl, tyl, ta, tc, gp, gp2, nx, ny,
-                               pxa, pya, pxc, pyc);
-    } else {  // the rest of a buffer at the end of a group: kept small in code
+            for (int k = 0; k < 32; ++k) one(k);
+        } else {
 #pragma unroll 1
-        for (int k = 0; k < cnt; ++k)
-            p2p_pair<NT, MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k),
-                               lds_u64(a_g + 8 * k), txh, tyh, txl, tyl, ta, tc, gp, gp2, nx, ny,
-                               pxa, pya, pxc, pyc);
+            for (int k = 0; k < cnt; ++k) one(k);
+        }
+    } else {
+        const pfd::f32x2 txh = pfd::pack2(ta.x, tb.x), tyh = pfd::pack2(ta.y, tb.y);
+        const pfd::f32x2 txl = pfd::pack2(ta.z, tb.z), tyl = pfd::pack2(ta.w, tb.w);
+        if (cnt == 32) {  // full chunk (the common case)
+#pragma unroll(P2P_UNROLL)
+            for (int k = 0; k < 32; ++k)
+                p2p_pair<NT, MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k),
+                                   lds_u64(a_g + 8 * k), txh, tyh, txl, tyl, ta, tc, gp, gp2, nx,
+                                   ny, pxa, pya, pxc, pyc);
+        } else {  // the rest of a buffer at the end of a group: kept small in code
+#pragma unroll 1
+            for (int k = 0; k < cnt; ++k)
+                p2p_pair<NT, MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k),
+                                   lds_u64(a_g + 8 * k), txh, tyh, txl, tyl, ta, tc, gp, gp2, nx,
+                                   ny, pxa, pya, pxc, pyc);
+        }
     }
     P2PSums r;
     if (NT >= 2) {
@@ -697,10 +734,11 @@ template <int NT, int MODE>
 __device__ __forceinline__ void p2p_chunk(const ulonglong2 *shi, const ulonglong2 *slo,
                                           const unsigned long long *sg2, int cnt,
                                           const float4 &ta, const float4 &tb, const float4 &tc,
-                                          const pfd::GaussParams &gp, float (&acc)[12]) {
+                                          float cx, float cy, const pfd::GaussParams &gp,
+                                          float (&acc)[12]) {
     const P2PSums r = p2p_chunk_sums<NT, MODE>(
         (uint32_t)__cvta_generic_to_shared(shi), (uint32_t)__cvta_generic_to_shared(slo),
-        (uint32_t)__cvta_generic_to_shared(sg2), cnt, ta, tb, tc, gp);
+        (uint32_t)__cvta_generic_to_shared(sg2), cnt, ta, tb, tc, cx, cy, gp);
     pfd::comp_add(acc[0], acc[1], r.s[0]);
     pfd::comp_add(acc[2], acc[3], r.s[1]);
     if (NT >= 2) {
@@ -720,12 +758,20 @@ __device__ __forceinline__ void p2p_chunk(const ulonglong2 *shi, const ulonglong
 // with no share get q >= 32.
 template <int MODE>
 __device__ __noinline__ float2 p2p_split_sums(uint32_t a_hi, uint32_t a_lo, uint32_t a_g, int cnt,
-                                              int q, int m, float4 tc, pfd::GaussParams gp) {
+                                              int q, int m, float4 tc, float cx, float cy,
+                                              pfd::GaussParams gp) {
     float px = 0.f, py = 0.f;
+    if constexpr (MODE == P2P_FAR) {
+        const float tx = (tc.x - cx) + tc.z, ty = (tc.y - cy) + tc.w;
 #pragma unroll 2
-    for (int k = q; k < cnt; k += m)
-        scalar_pair<MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k), lds_u64(a_g + 8 * k),
-                          tc, gp, px, py);
+        for (int k = q; k < cnt; k += m)
+            far_local_scalar(lds_u64x2(a_hi + 16 * k), lds_u64(a_g + 8 * k), tx, ty, px, py);
+    } else {
+#pragma unroll 2
+        for (int k = q; k < cnt; k += m)
+            scalar_pair<MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k),
+                              lds_u64(a_g + 8 * k), tc, gp, px, py);
+    }
     return make_float2(px, py);
 }
 
@@ -751,17 +797,18 @@ template <int MODE>
 __device__ __forceinline__ void p2p_run_chunk(int nt, const ulonglong2 *shi, const ulonglong2 *slo,
                                               const unsigned long long *sg2, int cnt,
                                               const float4 &ta, const float4 &tb,
-                                              const float4 &tc, int qs, int msp,
-                                              const pfd::GaussParams &gp, float (&acc)[12]) {
+                                              const float4 &tc, int qs, int msp, float cx,
+                                              float cy, const pfd::GaussParams &gp,
+                                              float (&acc)[12]) {
     if (nt == 1) {
-        p2p_chunk<1, MODE>(shi, slo, sg2, cnt, ta, tb, tc, gp, acc);
+        p2p_chunk<1, MODE>(shi, slo, sg2, cnt, ta, tb, tc, cx, cy, gp, acc);
         return;
     }
-    p2p_chunk<2, MODE>(shi, slo, sg2, cnt, ta, tb, tc, gp, acc);
+    p2p_chunk<2, MODE>(shi, slo, sg2, cnt, ta, tb, tc, cx, cy, gp, acc);
     if (nt == 3) {
         const float2 r = p2p_split_sums<MODE>(
             (uint32_t)__cvta_generic_to_shared(shi), (uint32_t)__cvta_generic_to_shared(slo),
-            (uint32_t)__cvta_generic_to_shared(sg2), cnt, qs, msp, tc, gp);
+            (uint32_t)__cvta_generic_to_shared(sg2), cnt, qs, msp, tc, cx, cy, gp);
         pfd::comp_add(acc[8], acc[9], r.x);
         pfd::comp_add(acc[10], acc[11], r.y);
     }
@@ -833,6 +880,8 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         const float rfar = sqrtf(gp.r2_far);
         const float reachf = rfar * 1.001f + (mag + rfar) * 4.8e-7f + 1e-30f;
         const float reachf2 = reachf * reachf;
+        // centre for the far sources' relative coordinates (any float near the group)
+        const float cx = 0.5f * (bx0 + bx1), cy = 0.5f * (by0 + by1);
         float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int c0 = 0, c1 = 0, c2 = 0;  // entries waiting in the three buffers
         for (int rc = r0; rc < r1; rc += P2P_RUNS_SM) {
@@ -895,10 +944,15 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                 if (cls >= 0) {
                     const unsigned mm = cls == 0 ? m0 : cls == 1 ? m1 : m2;
                     const int k = (cls == 0 ? c0 : cls == 1 ? c1 : c2) + __popc(mm & lt);
-                    s_hi[cls][k] = make_ulonglong2(pfd::pack2(spv.x, spv.x),
-                                                   pfd::pack2(spv.y, spv.y));
-                    s_lo[cls][k] = make_ulonglong2(pfd::pack2(spv.z, spv.z),
-                                                   pfd::pack2(spv.w, spv.w));
+                    if (cls == 0) {  // far: coordinates relative to the group centre
+                        const float lx = (spv.x - cx) + spv.z, ly = (spv.y - cy) + spv.w;
+                        s_hi[0][k] = make_ulonglong2(pfd::pack2(lx, lx), pfd::pack2(ly, ly));
+                    } else {
+                        s_hi[cls][k] = make_ulonglong2(pfd::pack2(spv.x, spv.x),
+                                                       pfd::pack2(spv.y, spv.y));
+                        s_lo[cls][k] = make_ulonglong2(pfd::pack2(spv.z, spv.z),
+                                                       pfd::pack2(spv.w, spv.w));
+                    }
                     s_g2[cls][k] = pfd::pack2(gg, gg);
                 }
                 c0 += __popc(m0);
@@ -910,20 +964,20 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                 __syncwarp();
                 if (c0 >= 32) {
                     p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], 32, ta, tb, tc,
-                                           qs, msp, gp, acc);
+                                           qs, msp, cx, cy, gp, acc);
                     nfar += 32ull * (unsigned long long)min(96, tn - tg);
                     c0 -= 32;
                     p2p_buf_shift(s_hi[0], s_lo[0], s_g2[0], c0, lane);
                 }
                 if (c1 >= 32) {
                     p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], 32, ta, tb, tc,
-                                            qs, msp, gp, acc);
+                                            qs, msp, cx, cy, gp, acc);
                     c1 -= 32;
                     p2p_buf_shift(s_hi[1], s_lo[1], s_g2[1], c1, lane);
                 }
                 if (c2 >= 32) {
                     p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], 32, ta, tb, tc,
-                                              qs, msp, gp, acc);
+                                              qs, msp, cx, cy, gp, acc);
                     c2 -= 32;
                     p2p_buf_shift(s_hi[2], s_lo[2], s_g2[2], c2, lane);
                 }
@@ -932,14 +986,14 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         // what is left in the buffers (fewer than 32 each)
         if (c0)
             p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], c0, ta, tb, tc,
-                                   qs, msp, gp, acc);
+                                   qs, msp, cx, cy, gp, acc);
         nfar += (unsigned long long)c0 * (unsigned long long)min(96, tn - tg);
         if (c1)
             p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], c1, ta, tb, tc,
-                                    qs, msp, gp, acc);
+                                    qs, msp, cx, cy, gp, acc);
         if (c2)
             p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], c2, ta, tb, tc,
-                                      qs, msp, gp, acc);
+                                      qs, msp, cx, cy, gp, acc);
         __syncwarp();
         if (ia < tn)
             nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),

@@ -153,6 +153,24 @@ __device__ __forceinline__ void pair2(const ulonglong2 &hi, const ulonglong2 &lo
     ny = fma2(dx, s, ny);
 }
 
+// pair2_far on coordinates relative to a nearby centre c, one float each
+// (x - c rounded once): for far pairs the rounding of the relative
+// coordinates (|x - c| 2^-24, with |x - c| a few pair distances) stays near
+// 1e-7 of the pair distance, so the hi/lo split is not needed there.
+// loc = {x, x, y, y} of the source, txc/tyc the targets' relative coordinates.
+__device__ __forceinline__ void pair2_far_local(const ulonglong2 &loc, f32x2 g2, f32x2 txc,
+                                                f32x2 tyc, const GaussParams2 &gp, f32x2 &nx,
+                                                f32x2 &ny) {
+    const f32x2 dx = sub2(txc, loc.x);
+    const f32x2 dy = sub2(tyc, loc.y);
+    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, gp.eps));
+    float ra, rb;
+    unpack2(r2, ra, rb);
+    const f32x2 s = mul2(g2, pack2(rcp_approx(ra), rcp_approx(rb)));
+    nx = fma2(dy, s, nx);
+    ny = fma2(dx, s, ny);
+}
+
 // pair2 for pairs known to have r2 * log2(e)/ksigmasqr >= Y_FAR (see the file
 // comment): om is 1.0f there and g * 1.0f = g, so this is bitwise pair2
 // without the ex2.

@@ -32,7 +32,7 @@ L2_BYTES = 126 * 2 ** 20
 MUFU_PER_SM_CLK = 16
 MUFU_PER_INTERACTION = 2  # ex2 + rcp
 FP32_PER_SM_CLK = 128
-FP32_OPS_FULL, FP32_OPS_FAR = 14, 11  # FP32 lane ops of one pair: with / without the ex2
+FP32_OPS_FULL, FP32_OPS_FAR = 14, 7  # FP32 lane ops of one pair: full / far (no ex2, one-float coordinates)
 
 
 def peaks():
@@ -264,8 +264,8 @@ def run_ours(args, rank, world):
                                f"ops / ({FP32_PER_SM_CLK} FP32/SM/clk)) x SMs x sm_max_mhz "
                                f"({pk['source']})",
                 "per_unit": f"pair within the Gaussian's reach: 2 MUFU (ex2, rcp) + {FP32_OPS_FULL} "
-                            f"FP32 ops; pair in a source tile beyond it (pairs_far): 1 MUFU (rcp) + "
-                            f"{FP32_OPS_FAR} FP32 ops"}
+                            f"FP32 ops; pair with a source beyond it from the whole target group "
+                            f"(pairs_far): 1 MUFU (rcp) + {FP32_OPS_FAR} FP32 ops"}
         npt = st0["expansion_terms"]
         ms_m2l = statistics.mean(f["ms_m2l"] for f in fmm_stats)
         m2l_flops = st0["m2l_translations"] * 8.0 * npt * npt

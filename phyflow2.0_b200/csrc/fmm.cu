@@ -335,6 +335,7 @@ __global__ void __launch_bounds__(256)
 k_m2m2(int lc, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
        const double2 *__restrict__ opT /* [4][NP(m)][NP(k)] */) {
     __shared__ double2 s_g[16][NP];
+    __shared__ double2 s_part[4][4 * NP];  // [child term c][output]
     __shared__ double2 s_c[4][NP];
     const int64_t pb = blockIdx.x;
     const int64_t g0 = level_off(lc) + 16 * pb, c0 = level_off(lc - 1) + 4 * pb;
@@ -343,30 +344,50 @@ k_m2m2(int lc, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
         s_g[gi][k] = scnt[g0 + gi] != 0 ? M[(g0 + gi) * NP + k] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < 4 * NP; t += 256) {
-        const int ci = t / NP, k = t - ci * NP;
+    // level lc-1: output (ci, k) is the sum over its 4 children c; one thread
+    // per (output, c), the 4 partial sums added in c order
+    for (int t = threadIdx.x; t < 16 * NP; t += 256) {
+        const int c = t / (4 * NP), o = t - c * 4 * NP, ci = o / NP, k = o - ci * NP;
+        double2 acc = make_double2(0.0, 0.0);
+        if (scnt[g0 + 4 * ci + c] != 0) {
+            const double2 *op = opT + (int64_t)c * NP * NP;
+            for (int mm = 0; mm <= k; ++mm)
+                acc = cfma(op[mm * NP + k], s_g[4 * ci + c][mm], acc);
+        }
+        s_part[c][o] = acc;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < 4 * NP; o += 256) {
+        const int ci = o / NP, k = o - ci * NP;
         double2 acc = make_double2(0.0, 0.0);
         if (scnt[c0 + ci] != 0) {
-            for (int c = 0; c < 4; ++c) {
-                if (scnt[g0 + 4 * ci + c] == 0) continue;
-                const double2 *op = opT + (int64_t)c * NP * NP;
-                for (int mm = 0; mm <= k; ++mm)
-                    acc = cfma(op[mm * NP + k], s_g[4 * ci + c][mm], acc);
-            }
+            acc = s_part[0][o];
+#pragma unroll
+            for (int c = 1; c < 4; ++c)
+                acc = make_double2(acc.x + s_part[c][o].x, acc.y + s_part[c][o].y);
             M[(c0 + ci) * NP + k] = acc;
         }
         s_c[ci][k] = acc;
     }
     __syncthreads();
-    const int64_t p = level_off(lc - 2) + pb;
-    for (int k = threadIdx.x; k < NP; k += 256) {
-        if (scnt[p] == 0) continue;
+    // level lc-2: the same over the 4 boxes just formed
+    for (int t = threadIdx.x; t < 4 * NP; t += 256) {
+        const int c = t / NP, k = t - c * NP;
         double2 acc = make_double2(0.0, 0.0);
-        for (int c = 0; c < 4; ++c) {
-            if (scnt[c0 + c] == 0) continue;
+        if (scnt[c0 + c] != 0) {
             const double2 *op = opT + (int64_t)c * NP * NP;
             for (int mm = 0; mm <= k; ++mm) acc = cfma(op[mm * NP + k], s_c[c][mm], acc);
         }
+        s_part[c][k] = acc;
+    }
+    __syncthreads();
+    const int64_t p = level_off(lc - 2) + pb;
+    for (int k = threadIdx.x; k < NP; k += 256) {
+        if (scnt[p] == 0) continue;
+        double2 acc = s_part[0][k];
+#pragma unroll
+        for (int c = 1; c < 4; ++c)
+            acc = make_double2(acc.x + s_part[c][k].x, acc.y + s_part[c][k].y);
         M[p * NP + k] = acc;
     }
 }
@@ -485,19 +506,34 @@ __global__ void __launch_bounds__(256)
 k_l2l2(int lp, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
        const double2 *__restrict__ opT /* [4][NP(m)][NP(n)] */) {
     __shared__ double2 s_p[NP];
+    __shared__ double2 s_part[4][4 * NP];  // [term residue j][output]
     __shared__ double2 s_c[4][NP];
     const int64_t pb = blockIdx.x;
     const int64_t p = level_off(lp) + pb;
     const int64_t c0 = level_off(lp + 1) + 4 * pb, g0 = level_off(lp + 2) + 16 * pb;
     for (int k = threadIdx.x; k < NP; k += 256) s_p[k] = Lc[p * NP + k];
     __syncthreads();
-    for (int t = threadIdx.x; t < 4 * NP; t += 256) {
-        const int ci = t / NP, n = t - ci * NP;
+    // level lp+1: output (ci, n) sums the parent's terms mm >= n; one thread
+    // per (output, j) takes mm = n + j, n + j + 4, ...; partial sums added in
+    // j order
+    for (int t = threadIdx.x; t < 16 * NP; t += 256) {
+        const int j = t / (4 * NP), o = t - j * 4 * NP, ci = o / NP, n = o - ci * NP;
         double2 acc = make_double2(0.0, 0.0);
         if (tcnt[c0 + ci] != 0) {
             const double2 *op = opT + (int64_t)ci * NP * NP;
+            for (int mm = n + j; mm < NP; mm += 4) acc = cfma(op[mm * NP + n], s_p[mm], acc);
+        }
+        s_part[j][o] = acc;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < 4 * NP; o += 256) {
+        const int ci = o / NP, n = o - ci * NP;
+        double2 acc = make_double2(0.0, 0.0);
+        if (tcnt[c0 + ci] != 0) {
             acc = Lc[(c0 + ci) * NP + n];
-            for (int mm = n; mm < NP; ++mm) acc = cfma(op[mm * NP + n], s_p[mm], acc);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                acc = make_double2(acc.x + s_part[j][o].x, acc.y + s_part[j][o].y);
             Lc[(c0 + ci) * NP + n] = acc;
         }
         s_c[ci][n] = acc;

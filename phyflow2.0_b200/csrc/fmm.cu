@@ -117,17 +117,29 @@ __global__ void __launch_bounds__(256)
 k_bbox(const double *__restrict__ x, const double *__restrict__ y, int64_t n, BBox *b) {
     unsigned long long mnx = ~0ull, mxx = 0, mny = ~0ull, mxy = 0;
     int bad = 0;
-    for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
-        const double a = x[i], c = y[i];
-        if (!isfinite(a) || !isfinite(c)) {
-            bad = 1;
-            continue;
+    // four independent loads of x and y per thread in flight
+    const int64_t stride = (int64_t)gridDim.x * 256;
+    for (int64_t i0 = (int64_t)blockIdx.x * 256 + threadIdx.x; i0 < n; i0 += 4 * stride) {
+        double a[4], c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t i = i0 + u * stride;
+            a[u] = i < n ? x[i] : 0.0;
+            c[u] = i < n ? y[i] : 0.0;
         }
-        const unsigned long long oa = ord_d(a), oc = ord_d(c);
-        mnx = min(mnx, oa);
-        mxx = max(mxx, oa);
-        mny = min(mny, oc);
-        mxy = max(mxy, oc);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u * stride >= n) continue;
+            if (!isfinite(a[u]) || !isfinite(c[u])) {
+                bad = 1;
+                continue;
+            }
+            const unsigned long long oa = ord_d(a[u]), oc = ord_d(c[u]);
+            mnx = min(mnx, oa);
+            mxx = max(mxx, oa);
+            mny = min(mny, oc);
+            mxy = max(mxy, oc);
+        }
     }
     for (int o = 16; o; o >>= 1) {
         mnx = min(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
@@ -1667,7 +1679,7 @@ pf_status velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x, const double
         BBox *bb = static_cast<BBox *>(pf::arena_take(ctx, sizeof(BBox)));
         k_bbox_init<<<1, 1, 0, st>>>(bb);
         PF_TRY(pf::launch_status("k_bbox_init"));
-        const int cap = ctx->num_sms * 4;
+        const int cap = ctx->num_sms * 8;
         k_bbox<<<(unsigned)std::min<int64_t>(pf::ceil_div(n_src, 256), cap), 256, 0, st>>>(
             x, y, n_src, bb);
         PF_TRY(pf::launch_status("k_bbox"));

@@ -75,23 +75,35 @@ k_rm_extent(const double *__restrict__ x, const double *__restrict__ y, int64_t 
             double yb0, double h2, double h05, double h, Extent *e) {
     __shared__ int s_v[5][RM_THREADS / 32];
     int mnx = INT32_MAX, mxx = INT32_MIN, mny = INT32_MAX, mxy = INT32_MIN, bad = 0;
-    for (int64_t i = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * RM_THREADS) {
-        const double xi = x[i], yi = y[i];
-        if (!isfinite(xi) || !isfinite(yi)) {
-            bad |= 1;
-            continue;
+    // four independent loads of x and y per thread in flight
+    const int64_t stride = (int64_t)gridDim.x * RM_THREADS;
+    for (int64_t i0 = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x; i0 < n; i0 += 4 * stride) {
+        double xs[4], ys[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t i = i0 + u * stride;
+            xs[u] = i < n ? x[i] : 0.0;
+            ys[u] = i < n ? y[i] : 0.0;
         }
-        const int64_t a = left_index(xi, xb0, h2, h05, h);
-        const int64_t b = left_index(yi, yb0, h2, h05, h);
-        if (a < -IDX_LIMIT || a > IDX_LIMIT || b < -IDX_LIMIT || b > IDX_LIMIT) {
-            bad |= 2;
-            continue;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (i0 + u * stride >= n) continue;
+            const double xi = xs[u], yi = ys[u];
+            if (!isfinite(xi) || !isfinite(yi)) {
+                bad |= 1;
+                continue;
+            }
+            const int64_t a = left_index(xi, xb0, h2, h05, h);
+            const int64_t b = left_index(yi, yb0, h2, h05, h);
+            if (a < -IDX_LIMIT || a > IDX_LIMIT || b < -IDX_LIMIT || b > IDX_LIMIT) {
+                bad |= 2;
+                continue;
+            }
+            mnx = min(mnx, (int)a);
+            mxx = max(mxx, (int)a);
+            mny = min(mny, (int)b);
+            mxy = max(mxy, (int)b);
         }
-        mnx = min(mnx, (int)a);
-        mxx = max(mxx, (int)a);
-        mny = min(mny, (int)b);
-        mxy = max(mxy, (int)b);
     }
     mnx = warp_min(mnx);
     mxx = warp_max(mxx);
@@ -567,7 +579,7 @@ pf_status remesh_sync(pf_ctx *ctx, int64_t n, const double *x, const double *y, 
     PF_TRY(pf::launch_status("k_rm_extent_init"));
     {
         int64_t grid = pf::ceil_div(n, RM_THREADS);
-        const int64_t cap = (int64_t)ctx->num_sms * 4;
+        const int64_t cap = (int64_t)ctx->num_sms * 8;
         if (grid > cap) grid = cap;
         k_rm_extent<<<(unsigned)grid, RM_THREADS, 0, st>>>(x, y, n, xb0, yb0, h2, h05, h, ext);
         PF_TRY(pf::launch_status("k_rm_extent"));

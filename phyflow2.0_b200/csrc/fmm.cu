@@ -148,7 +148,26 @@ k_bbox(const double *__restrict__ x, const double *__restrict__ y, int64_t n, BB
         mxy = max(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
     }
     bad = __reduce_or_sync(0xffffffffu, bad);
+    // block reduction, then one set of atomics per block
+    __shared__ unsigned long long s_v[4][8];
+    __shared__ int s_bad[8];
+    const int wid = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
+        s_v[0][wid] = mnx;
+        s_v[1][wid] = mxx;
+        s_v[2][wid] = mny;
+        s_v[3][wid] = mxy;
+        s_bad[wid] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; ++w) {
+            mnx = min(mnx, s_v[0][w]);
+            mxx = max(mxx, s_v[1][w]);
+            mny = min(mny, s_v[2][w]);
+            mxy = max(mxy, s_v[3][w]);
+            bad |= s_bad[w];
+        }
         atomicMin(&b->mnx, mnx);
         atomicMax(&b->mxx, mxx);
         atomicMin(&b->mny, mny);

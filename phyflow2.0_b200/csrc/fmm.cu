@@ -922,8 +922,14 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
     const int r0 = run_off[b], r1 = run_off[b + 1];
     const float rser = sqrtf(gp.r2_series);
     unsigned long long npairs = 0, nfar = 0;
-    for (int tg = 0; tg < tn; tg += 96) {
-        const int gsz = min(96, tn - tg);
+    // groups of at most 96 targets, balanced (sizes differ by at most one):
+    // every group streams all the block's sources, so a small last group
+    // would cost nearly as much as a full one
+    const int ngrp = (tn + 95) / 96;
+    for (int gi = 0; gi < ngrp; ++gi) {
+        const int tg = (int)((int64_t)gi * tn / ngrp);
+        const int gsz = (int)((int64_t)(gi + 1) * tn / ngrp) - tg;
+        const int te = tg + gsz;  // end of this group's targets
         const int nt = (gsz <= 32) ? 1 : (gsz <= 64) ? 2 : 3;  // warp-uniform
         // nt = 3: remainder targets tg + 64 + j, j < rem, each on msp lanes
         const int rem = nt == 3 ? gsz - 64 : 32;
@@ -932,13 +938,13 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         const int qs = cval ? lane / rem : 32;
         const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane % rem;
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 ta = (ia < tn) ? thl[t0 + ia] : z4;
-        const float4 tb = (ib < tn) ? thl[t0 + ib] : z4;
+        const float4 ta = (ia < te) ? thl[t0 + ia] : z4;
+        const float4 tb = (ib < te) ? thl[t0 + ib] : z4;
         const float4 tc = cval ? thl[t0 + ic] : z4;
         // box of the group's targets (hi parts), for the series-free test
         float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
-        if (ia < tn) { bx0 = bx1 = ta.x; by0 = by1 = ta.y; }
-        if (ib < tn) { bx0 = fminf(bx0, tb.x); bx1 = fmaxf(bx1, tb.x); by0 = fminf(by0, tb.y); by1 = fmaxf(by1, tb.y); }
+        if (ia < te) { bx0 = bx1 = ta.x; by0 = by1 = ta.y; }
+        if (ib < te) { bx0 = fminf(bx0, tb.x); bx1 = fmaxf(bx1, tb.x); by0 = fminf(by0, tb.y); by1 = fmaxf(by1, tb.y); }
         if (cval) { bx0 = fminf(bx0, tc.x); bx1 = fmaxf(bx1, tc.x); by0 = fminf(by0, tc.y); by1 = fmaxf(by1, tc.y); }
         bx0 = warp_min(bx0);
         bx1 = warp_max(bx1);
@@ -982,7 +988,7 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
             if (lane == 0) s_rp[nrc] = pre;
             __syncwarp();
             const int S = pre;
-            npairs += (unsigned long long)S * (unsigned long long)min(96, tn - tg);
+            npairs += (unsigned long long)S * (unsigned long long)gsz;
             // each lane's stream position only moves forward (by 32 per
             // round), so the run holding it is found by advancing an index:
             // the largest r with prefix[r] <= p (empty runs are stepped over).
@@ -1037,7 +1043,7 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                 if (c0 >= 32) {
                     p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], 32, ta, tb, tc,
                                            qs, msp, cx, cy, gp, acc);
-                    nfar += 32ull * (unsigned long long)min(96, tn - tg);
+                    nfar += 32ull * (unsigned long long)gsz;
                     c0 -= 32;
                     p2p_buf_shift(s_hi[0], s_lo[0], s_g2[0], c0, lane);
                 }
@@ -1059,7 +1065,7 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         if (c0)
             p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], c0, ta, tb, tc,
                                    qs, msp, cx, cy, gp, acc);
-        nfar += (unsigned long long)c0 * (unsigned long long)min(96, tn - tg);
+        nfar += (unsigned long long)c0 * (unsigned long long)gsz;
         if (c1)
             p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], c1, ta, tb, tc,
                                     qs, msp, cx, cy, gp, acc);
@@ -1067,10 +1073,10 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
             p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], c2, ta, tb, tc,
                                       qs, msp, cx, cy, gp, acc);
         __syncwarp();
-        if (ia < tn)
+        if (ia < te)
             nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),
                                           INV_2PI * ((double)acc[2] + (double)acc[3]));
-        if (ib < tn)
+        if (ib < te)
             nearv[t0 + ib] = make_double2(INV_2PI * ((double)acc[4] + (double)acc[5]),
                                           INV_2PI * ((double)acc[6] + (double)acc[7]));
         if (nt == 3) {  // combine the msp shares of each remainder target, in lane order

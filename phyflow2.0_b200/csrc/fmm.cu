@@ -426,78 +426,105 @@ k_m2m2(int lc, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
 // M2L for all levels 2..L: lane n of a box group = local coefficient n
 template <int NP>
 __global__ void __launch_bounds__(WARP_BOX_THREADS)
-k_m2l(int L, int Bp, int64_t bg0, int64_t nbg, const int32_t *__restrict__ scnt,
+k_m2l(int L, int Bp, int64_t npair, const int32_t *__restrict__ scnt,
       const int32_t *__restrict__ tcnt, const double2 *__restrict__ M, double2 *__restrict__ Lc,
       const int4 *__restrict__ far, const int32_t *__restrict__ far_ptr, int maxpos,
       const double2 *__restrict__ pw /* [nop][NP+1] */, const double *__restrict__ binom,
       unsigned long long *__restrict__ ntrans) {
     using BL = BoxLanes<NP>;
-    __shared__ double2 s_c[WARP_BOX_THREADS / 32][32];
+    __shared__ double2 s_c[WARP_BOX_THREADS / 32][2][32];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int half = lane / BL::W, n = lane % BL::W;
-    const int64_t w = ((int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid) * BL::BPW + half;
-    const int64_t bg = bg0 + (w < nbg ? w : 0);
-    const bool live = w < nbg && tcnt[bg] != 0;
-    if (!__any_sync(0xffffffffu, live)) return;
+    // Each lane group takes two target boxes A, B of one level with the same
+    // far list (same position class): interleaving their translations gives
+    // two independent load chains per step, sharing the list entry, the
+    // operator powers and the binomial row.  Pair unit u -> level l, pair j.
+    const int64_t u = ((int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid) * BL::BPW + half;
+    int l = 2;
+    int64_t j = u < npair ? u : 0;
+    while (l < L && j >= ((int64_t)1 << (2 * l)) / 2) {
+        j -= ((int64_t)1 << (2 * l)) / 2;
+        ++l;
+    }
+    // boxes r and r + stride share the position class (Morton order)
+    const int64_t stride = (l == L) ? (int64_t)Bp * Bp : 4;
+    const int64_t rA = (j / stride) * 2 * stride + (j % stride);
+    const int64_t bgA = level_off(l) + rA, bgB = bgA + stride;
+    const bool liveA = u < npair && tcnt[bgA] != 0;
+    const bool liveB = u < npair && tcnt[bgB] != 0;
+    if (!__any_sync(0xffffffffu, liveA || liveB)) return;
     // this lane's row of the binomial matrix C(n+k, k), in registers (from
     // shared memory instead, the dot product below measured 28% slower)
     double brow[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) brow[k] = (n < NP) ? binom[k * NP + n] : 0.0;
-    int l = 2;
-    while (l < L && bg >= level_off(l + 1)) ++l;
-    const uint32_t m = (uint32_t)(bg - level_off(l));
-    const int ix = (int)compact1by1(m), iy = (int)compact1by1(m >> 1);
-    const int pos = (l == L) ? ((ix % Bp) + Bp * (iy % Bp)) : ((ix & 1) | ((iy & 1) << 1));
+    const uint32_t mA = (uint32_t)rA, mB = (uint32_t)(rA + stride);
+    const int ixA = (int)compact1by1(mA), iyA = (int)compact1by1(mA >> 1);
+    const int ixB = (int)compact1by1(mB), iyB = (int)compact1by1(mB >> 1);
+    const int pos = (l == L) ? ((ixA % Bp) + Bp * (iyA % Bp)) : ((ixA & 1) | ((iyA & 1) << 1));
     const int side = 1 << l;
     const int e0 = far_ptr[l * maxpos + pos];
-    const int len = live ? far_ptr[l * maxpos + pos + 1] - e0 : 0;
+    const int len = (liveA || liveB) ? far_ptr[l * maxpos + pos + 1] - e0 : 0;
     int lmax = len;
 #pragma unroll
     for (int o = 16; o; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    double2 acc = make_double2(0.0, 0.0);
+    double2 accA = make_double2(0.0, 0.0), accB = make_double2(0.0, 0.0);
     unsigned nt = 0;
-    const double2 *sc = &s_c[wid][half * BL::W];
+    const double2 *scA = &s_c[wid][0][half * BL::W];
+    const double2 *scB = &s_c[wid][1][half * BL::W];
     for (int e = 0; e < lmax; ++e) {
-        bool use = e < len;
-        int64_t sg = 0;
+        bool useA = false, useB = false;
+        int64_t sgA = 0, sgB = 0;
         int op = 0;
-        if (use) {
+        if (e < len) {
             const int4 f = far[e0 + e];
-            const int sx = ix + f.x, sy = iy + f.y;
-            use = sx >= 0 && sy >= 0 && sx < side && sy < side;
-            if (use) {
-                sg = level_off(l) + morton2((uint32_t)sx, (uint32_t)sy);
-                op = f.z;
-            }
+            op = f.z;
+            const int sxA = ixA + f.x, syA = iyA + f.y, sxB = ixB + f.x, syB = iyB + f.y;
+            useA = liveA && sxA >= 0 && syA >= 0 && sxA < side && syA < side;
+            useB = liveB && sxB >= 0 && syB >= 0 && sxB < side && syB < side;
+            if (useA) sgA = level_off(l) + morton2((uint32_t)sxA, (uint32_t)syA);
+            if (useB) sgB = level_off(l) + morton2((uint32_t)sxB, (uint32_t)syB);
         }
-        // the source's count and multipoles are loaded together (box sg is
-        // in range either way); an empty source box is then skipped
-        const int cnt_s = use ? scnt[sg] : 0;
+        // the sources' counts and multipoles are loaded together (boxes in
+        // range either way); an empty source box is then skipped
+        const int cA = useA ? scnt[sgA] : 0, cB = useB ? scnt[sgB] : 0;
         const double2 *rp = pw + (int64_t)op * (NP + 1);
-        const double2 mv = (use && n < NP) ? M[sg * NP + n] : make_double2(0.0, 0.0);
-        use = use && cnt_s != 0;
-        nt += use ? 1u : 0u;
-        if (use && n < NP) {
-            double2 c = cmul(mv, rp[n]);
-            if ((n & 1) == 0) c = make_double2(-c.x, -c.y);  // (-1)^(k+1)
-            s_c[wid][lane] = c;
+        const double2 z2 = make_double2(0.0, 0.0);
+        const double2 mvA = (useA && n < NP) ? M[sgA * NP + n] : z2;
+        const double2 mvB = (useB && n < NP) ? M[sgB * NP + n] : z2;
+        useA = useA && cA != 0;
+        useB = useB && cB != 0;
+        nt += (useA ? 1u : 0u) + (useB ? 1u : 0u);
+        if ((useA || useB) && n < NP) {
+            const double2 r = rp[n];
+            double2 ca = useA ? cmul(mvA, r) : z2, cb = useB ? cmul(mvB, r) : z2;
+            if ((n & 1) == 0) {  // (-1)^(k+1)
+                ca = make_double2(-ca.x, -ca.y);
+                cb = make_double2(-cb.x, -cb.y);
+            }
+            s_c[wid][0][lane] = ca;
+            s_c[wid][1][lane] = cb;
         }
         __syncwarp();
-        if (use && n < NP) {
-            double ux = 0.0, uy = 0.0;
+        if ((useA || useB) && n < NP) {
+            double uxa = 0.0, uya = 0.0, uxb = 0.0, uyb = 0.0;
 #pragma unroll
             for (int k = 0; k < NP; ++k) {
-                const double2 c = sc[k];
-                ux = fma(brow[k], c.x, ux);
-                uy = fma(brow[k], c.y, uy);
+                const double2 a = scA[k], b = scB[k];
+                uxa = fma(brow[k], a.x, uxa);
+                uya = fma(brow[k], a.y, uya);
+                uxb = fma(brow[k], b.x, uxb);
+                uyb = fma(brow[k], b.y, uyb);
             }
-            acc = cfma(rp[n + 1], make_double2(ux, uy), acc);
+            const double2 r1 = rp[n + 1];
+            if (useA) accA = cfma(r1, make_double2(uxa, uya), accA);
+            if (useB) accB = cfma(r1, make_double2(uxb, uyb), accB);
         }
         __syncwarp();
     }
-    if (live && n < NP) Lc[bg * NP + n] = acc;
-    if (live && n == 0 && nt) atomicAdd(ntrans, (unsigned long long)nt);
+    if (liveA && n < NP) Lc[bgA * NP + n] = accA;
+    if (liveB && n < NP) Lc[bgB * NP + n] = accB;
+    if ((liveA || liveB) && n == 0 && nt) atomicAdd(ntrans, (unsigned long long)nt);
 }
 
 // L2L into child level l: lane n of a box group = coefficient n
@@ -926,10 +953,8 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
     // every group streams all the block's sources, so a small last group
     // would cost nearly as much as a full one
     const int ngrp = (tn + 95) / 96;
-    for (int gi = 0; gi < ngrp; ++gi) {
-        const int tg = (int)((int64_t)gi * tn / ngrp);
-        const int gsz = (int)((int64_t)(gi + 1) * tn / ngrp) - tg;
-        const int te = tg + gsz;  // end of this group's targets
+    for (int tg = 0, gi = 1; tg < tn; ++gi) {
+        const int gsz = gi * tn / ngrp - tg;  // tn < 2^31 / ngrp
         const int nt = (gsz <= 32) ? 1 : (gsz <= 64) ? 2 : 3;  // warp-uniform
         // nt = 3: remainder targets tg + 64 + j, j < rem, each on msp lanes
         const int rem = nt == 3 ? gsz - 64 : 32;
@@ -938,13 +963,13 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         const int qs = cval ? lane / rem : 32;
         const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane % rem;
         const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 ta = (ia < te) ? thl[t0 + ia] : z4;
-        const float4 tb = (ib < te) ? thl[t0 + ib] : z4;
+        const float4 ta = (lane < gsz) ? thl[t0 + ia] : z4;
+        const float4 tb = (lane + 32 < gsz) ? thl[t0 + ib] : z4;
         const float4 tc = cval ? thl[t0 + ic] : z4;
         // box of the group's targets (hi parts), for the series-free test
         float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
-        if (ia < te) { bx0 = bx1 = ta.x; by0 = by1 = ta.y; }
-        if (ib < te) { bx0 = fminf(bx0, tb.x); bx1 = fmaxf(bx1, tb.x); by0 = fminf(by0, tb.y); by1 = fmaxf(by1, tb.y); }
+        if (lane < gsz) { bx0 = bx1 = ta.x; by0 = by1 = ta.y; }
+        if (lane + 32 < gsz) { bx0 = fminf(bx0, tb.x); bx1 = fmaxf(bx1, tb.x); by0 = fminf(by0, tb.y); by1 = fmaxf(by1, tb.y); }
         if (cval) { bx0 = fminf(bx0, tc.x); bx1 = fmaxf(bx1, tc.x); by0 = fminf(by0, tc.y); by1 = fmaxf(by1, tc.y); }
         bx0 = warp_min(bx0);
         bx1 = warp_max(bx1);
@@ -1073,10 +1098,10 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
             p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], c2, ta, tb, tc,
                                       qs, msp, cx, cy, gp, acc);
         __syncwarp();
-        if (ia < te)
+        if (lane < gsz)
             nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),
                                           INV_2PI * ((double)acc[2] + (double)acc[3]));
-        if (ib < te)
+        if (lane + 32 < gsz)
             nearv[t0 + ib] = make_double2(INV_2PI * ((double)acc[4] + (double)acc[5]),
                                           INV_2PI * ((double)acc[6] + (double)acc[7]));
         if (nt == 3) {  // combine the msp shares of each remainder target, in lane order
@@ -1096,6 +1121,7 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                 nearv[t0 + ic] = make_double2(INV_2PI * ((double)h0 + (double)l0),
                                               INV_2PI * ((double)h1 + (double)l1));
         }
+        tg += gsz;
     }
     if (lane == 0) {
         atomicAdd(pairs, npairs);
@@ -1480,9 +1506,9 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     // M2L, all levels >= 2
     const int B = 1 << kb, Bp = B > 2 ? B : 2;
     {
-        const int64_t bg0 = level_off(2), nbg = nbox - bg0;
-        k_m2l<NP><<<(unsigned)pf::ceil_div(nbg, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
-            L, Bp, bg0, nbg, scnt_all, tcnt_all, M, Lc, c.d_far, c.d_far_ptr, c.maxpos, c.d_pw,
+        const int64_t npair = (nbox - level_off(2)) / 2;  // box pairs of levels 2..L
+        k_m2l<NP><<<(unsigned)pf::ceil_div(npair, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
+            L, Bp, npair, scnt_all, tcnt_all, M, Lc, c.d_far, c.d_far_ptr, c.maxpos, c.d_pw,
             c.d_bin, ctr + 1);
         PF_TRY(pf::launch_status("k_m2l"));
     }

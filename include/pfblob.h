@@ -294,8 +294,8 @@ pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, const double
  * library load to process exit; no pf_ctx is needed and none is created.  The
  * call works on the current device; its first call on a device looks up the
  * buffer's device address (make that first call before any stream capture).
- * Blob sets needing more scratch than the buffer holds (about 40 bytes per
- * blob plus 24 bytes per window cell) are rejected with PF_ERR_INVALID_ARG.
+ * Blob sets needing more scratch than the buffer holds (about 12 bytes per
+ * blob plus 160 bytes per window cell) are rejected with PF_ERR_INVALID_ARG.
  * Every call shares the buffer: calls that overlap on the GPU (different
  * streams, or different host threads) race and must be serialised by the
  * caller.  Arguments and results as pf_remesh_window.

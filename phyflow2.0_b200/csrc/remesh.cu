@@ -13,19 +13,20 @@
 //   4. k_rm_place  : blob index -> its slot.
 //   5. k_rm_sortcells : per base cell, order its blobs by input index (every
 //      sum below then has a fixed order, independent of atomic timing).
-//   5b. k_rm_sorted : x, y, g and base cell copied into cell order.
-//   6. k_rm_gather : per tile of output cells, the weights of the blobs of
-//      the covering base cells -- four x weights M4'(ux_a), four y weights
-//      M4'(uy_b) (_interpolation_kernels_1d.cpp:75-89; u as _regridding.py:183)
-//      or Tutty's -- are built in shared memory; one thread per output cell
-//      (ix, iy) sums, in fixed order, (wx_a wy_b) g over the blobs of the 16
-//      base cells whose windows cover it, and flags cells touched by at least
-//      one window (explicit zeros are kept, like the CSR sum of the
-//      reference, _regridding.py:200-202).
+//   6. k_rm_stencil : one thread per base cell: the weights of each of its
+//      blobs -- four x weights M4'(ux_a), four y weights M4'(uy_b)
+//      (_interpolation_kernels_1d.cpp:75-89; u as _regridding.py:183) or
+//      Tutty's -- and the cell's 4 x 4 stencil of partial sums
+//      sum over its blobs (in cell order) of (wx_a wy_b) g, stored
+//      stencil-major (coalesced).
+//   7. k_rm_sum : one thread per output cell (ix, iy): the 16 partial sums of
+//      the base cells whose windows cover it, added in fixed (b, a) order;
+//      flags cells touched by at least one window (explicit zeros are kept,
+//      like the CSR sum of the reference, _regridding.py:200-202).
 //   6b. (pf_remesh_population_control only) PopulationControl of the cell
 //      values (popctl.cu), which clears the flags of the dropped cells.
-//   7. scan of the flags -> output slots, in (ix, iy) order.
-//   8. k_rm_emit   : x = ix*h + 0.5h + xb0 (same order as :217-218), g, ix, iy.
+//   8. scan of the flags -> output slots, in (ix, iy) order.
+//   9. k_rm_emit   : x = ix*h + 0.5h + xb0 (same order as :217-218), g, ix, iy.
 // No floating-point atomics: each output value is produced by one thread.
 #include <algorithm>
 #include <cmath>
@@ -273,111 +274,48 @@ __device__ __forceinline__ W9 blob_w9(int32_t i, int64_t bx, int64_t by, int32_t
     return r;
 }
 
-// Blob coordinates, circulation and base cell in cell order (one thread per
-// sorted position: coalesced writes), so the gather below reads each base-cell
-// column as contiguous ranges.
+// Base cell bc = bx*nby + by: the 4 x 4 stencil of partial sums of its blobs,
+// part[(a*4 + b) * nbase + bc] = sum over the cell's blobs, in cell order, of
+// (wx_a wy_b) g; output cell (bx + a, by + b) of the window grid.  Empty
+// cells write nothing (k_rm_sum reads their count first).
+template <bool TUTTY>
 __global__ void __launch_bounds__(RM_THREADS)
-k_rm_sorted(const int32_t *__restrict__ nvalid, const int32_t *__restrict__ perm,
-            const int32_t *__restrict__ cell, const double *__restrict__ x,
-            const double *__restrict__ y, const double *__restrict__ g, double *__restrict__ xs,
-            double *__restrict__ ys, double *__restrict__ gs, int32_t *__restrict__ cs) {
-    const int64_t j = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
-    if (j >= *nvalid) return;
-    const int32_t i = perm[j];
-    xs[j] = x[i];
-    ys[j] = y[i];
-    gs[j] = g[i];
-    cs[j] = cell[i];
+k_rm_stencil(int64_t nbase, int64_t nby, int32_t ixmin, int32_t iymin,
+             const int32_t *__restrict__ start, const int32_t *__restrict__ count,
+             const int32_t *__restrict__ perm, const double *__restrict__ x,
+             const double *__restrict__ y, const double *__restrict__ g, WParams wp,
+             double *__restrict__ part) {
+    const int64_t bc = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
+    if (bc >= nbase) return;
+    const int cnt = count[bc];
+    if (cnt == 0) return;
+    const int s0 = start[bc];
+    const int64_t bx = bc / nby, by = bc - bx * nby;
+    double p[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) p[k] = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+        const W9 r = blob_w9<TUTTY>(perm[s0 + k], bx, by, ixmin, iymin, x, y, g, wp);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) p[a * 4 + b] += (r.wx[a] * r.wy[b]) * r.g;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) part[k * nbase + bc] = p[k];
 }
 
-// Output cell grid: ox in [0, nbx+3), oy in [0, nby+3); lattice index
-// ix = ixmin + ox.  A base cell (bx, by) covers ox in bx..bx+3, oy in by..by+3.
-//
-// One CTA per tile of tw x th output cells (ox x oy), one thread per cell.  The
-// CTA first computes, into shared memory, the weight records of every blob
-// in the (tw+3) x (th+3) base cells covering the tile: per base-cell
-// column their cell-ordered positions are one contiguous range, so the
-// records are built from contiguous ranges of the cell-ordered copies (xs, ys,
-// gs, cs of k_rm_sorted), all columns at once.  Each
-// thread then sums (wx_a wy_b) g over the blobs of its 16 covering base cells
-// in a fixed order (b, a, blob) and flags cells touched by at least one
-// window (explicit zeros are kept, like the CSR sum of the reference,
-// _regridding.py:200-202).  A tile with more than `cap` blobs computes the
-// records where it uses them instead (same values); the host sizes the tile
-// and `cap` from the mean blob density so that this stays rare.
-constexpr int RG_TMAX = 16, RG_CAPMAX = 1536;  // 108 KB of records: 2 CTAs per SM
-constexpr int RG_BMAX = RG_TMAX + 3;
-
-template <bool TUTTY>
-__global__ void __launch_bounds__(2 * RG_TMAX * RG_TMAX)
-k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, int32_t ixmin,
-            int32_t iymin,
-            const int32_t *__restrict__ start, const int32_t *__restrict__ count,
-            const int32_t *__restrict__ cs, const double *__restrict__ x,
-            const double *__restrict__ y, const double *__restrict__ g, WParams wp,
-            double *__restrict__ acc, int32_t *__restrict__ flag) {
-    extern __shared__ double s_w_raw[];  // cap weight records
-    W9 *s_w = reinterpret_cast<W9 *>(s_w_raw);
-    __shared__ int s_cs[RG_BMAX][RG_BMAX];  // staged start of each base cell
-    __shared__ int s_cn[RG_BMAX][RG_BMAX];  // its blob count
-    __shared__ int s_colg[RG_BMAX], s_coln[RG_BMAX], s_col[RG_BMAX + 1];
-    const int bw = tw + 3, bh = th + 3;
-    const int nthr = blockDim.x;  // twice the tile: the extra threads help build the weights
-    const int64_t noy = nby + 3, nox = nbx + 3;
-    const int64_t tile = blockIdx.x;
-    const int64_t ox0 = (tile / tiles_y) * tw, oy0 = (tile % tiles_y) * th;
-    const int64_t bx0 = ox0 - 3, by0 = oy0 - 3;
-    const int64_t blo = by0 > 0 ? by0 : 0;
-    const int64_t bhi = (by0 + bh < nby) ? by0 + bh : nby;  // exclusive
-    if (threadIdx.x < bw) {
-        const int64_t bx = bx0 + threadIdx.x;
-        int g0 = 0, n = 0;
-        if (bx >= 0 && bx < nbx && blo < bhi) {
-            const int64_t c0 = bx * nby + blo, c1 = bx * nby + bhi - 1;
-            g0 = start[c0];
-            n = start[c1] + count[c1] - g0;
-        }
-        s_colg[threadIdx.x] = g0;
-        s_coln[threadIdx.x] = n;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int p = 0;
-        for (int c = 0; c < bw; ++c) {
-            s_col[c] = p;
-            p += s_coln[c];
-        }
-        s_col[bw] = p;
-    }
-    __syncthreads();
-    const int total = s_col[bw];
-    const bool staged = total <= cap;
-    if (staged) {
-        for (int f = threadIdx.x; f < total; f += nthr) {
-            int c = 0;
-            while (s_col[c + 1] <= f) ++c;  // f < total, so c < bw
-            const int32_t j = s_colg[c] + (f - s_col[c]);
-            const int64_t bx = bx0 + c;
-            s_w[f] = blob_w9<TUTTY>(j, bx, cs[j] - bx * nby, ixmin, iymin, x, y, g, wp);
-        }
-        for (int k = threadIdx.x; k < bw * bh; k += nthr) {
-            const int c = k / bh, r = k - c * bh;
-            const int64_t bx = bx0 + c, by = by0 + r;
-            int ls = 0, ln = 0;
-            if (bx >= 0 && bx < nbx && by >= 0 && by < nby) {
-                const int64_t bc = bx * nby + by;
-                ls = start[bc] - s_colg[c] + s_col[c];
-                ln = count[bc];
-            }
-            s_cs[c][r] = ls;
-            s_cn[c][r] = ln;
-        }
-    }
-    __syncthreads();
-    if ((int)threadIdx.x >= tw * th) return;
-    const int tx = threadIdx.x / th, ty = threadIdx.x - tx * th;
-    const int64_t ox = ox0 + tx, oy = oy0 + ty;
-    if (ox >= nox || oy >= noy) return;
+// Output cell grid: ox in [0, nbx+3), oy in [0, nby+3), cid = ox*(nby+3) + oy;
+// lattice index ix = ixmin + ox.  Base cell (bx, by) covers ox in bx..bx+3,
+// oy in by..by+3.  One thread per output cell adds the stencil entries of its
+// covering base cells in fixed (b, a) order.
+__global__ void __launch_bounds__(RM_THREADS)
+k_rm_sum(int64_t nbx, int64_t nby, const int32_t *__restrict__ count,
+         const double *__restrict__ part, double *__restrict__ acc, int32_t *__restrict__ flag) {
+    const int64_t noy = nby + 3, ncell = (nbx + 3) * noy;
+    const int64_t cid = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
+    if (cid >= ncell) return;
+    const int64_t ox = cid / noy, oy = cid - ox * noy, nbase = nbx * nby;
     double sum = 0.0;
     int touched = 0;
 #pragma unroll
@@ -388,29 +326,14 @@ k_rm_gather(int64_t nbx, int64_t nby, int tw, int th, int cap, int64_t tiles_y, 
         for (int a = 0; a < 4; ++a) {
             const int64_t bx = ox - a;
             if (bx < 0 || bx >= nbx) continue;
-            if (staged) {
-                const int cnt = s_cn[tx + 3 - a][ty + 3 - b];
-                const int s0 = s_cs[tx + 3 - a][ty + 3 - b];
-                if (cnt == 0) continue;
-                touched = 1;
-                for (int k = 0; k < cnt; ++k) {
-                    const W9 &r = s_w[s0 + k];
-                    sum += (r.wx[a] * r.wy[b]) * r.g;
-                }
-            } else {
-                const int64_t bc = bx * nby + by;
-                const int cnt = count[bc], s0 = start[bc];
-                if (cnt == 0) continue;
-                touched = 1;
-                for (int k = 0; k < cnt; ++k) {
-                    const W9 r = blob_w9<TUTTY>(s0 + k, bx, by, ixmin, iymin, x, y, g, wp);
-                    sum += (r.wx[a] * r.wy[b]) * r.g;
-                }
-            }
+            const int64_t bc = bx * nby + by;
+            if (count[bc] == 0) continue;
+            touched = 1;
+            sum += part[(a * 4 + b) * nbase + bc];
         }
     }
-    acc[ox * noy + oy] = sum;
-    flag[ox * noy + oy] = touched;
+    acc[cid] = sum;
+    flag[cid] = touched;
 }
 
 __global__ void __launch_bounds__(RM_THREADS)
@@ -455,7 +378,7 @@ static int64_t dense_cell_limit(int64_t n) {
 size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby) {
     const int64_t nbase = nbx * nby, ncell = (nbx + 3) * (nby + 3);
     const int64_t big = ncell > nbase ? ncell : nbase;
-    return align256(4 * n) * 4 + align256(8 * n) * 3 + 2 * align256(4 * nbase) +
+    return align256(4 * n) * 3 + align256(8 * 16 * nbase) + 2 * align256(4 * nbase) +
            align256(8 * ncell) + 2 * align256(4 * ncell) + align256(4 * scan_tmp_ints(big)) +
            3 * align256(16) + align256(sizeof(PcState)) + popctl_scratch_bytes() + 1024;
 }
@@ -473,10 +396,7 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     int32_t *cell = (int32_t *)sc.take(4 * n);
     int32_t *rank = (int32_t *)sc.take(4 * n);
     int32_t *perm = (int32_t *)sc.take(4 * n);
-    double *xs = (double *)sc.take(8 * n);
-    double *ys = (double *)sc.take(8 * n);
-    double *gs = (double *)sc.take(8 * n);
-    int32_t *cs = (int32_t *)sc.take(4 * n);
+    double *part = (double *)sc.take(8 * 16 * nbase);
     int32_t *count = (int32_t *)sc.take(4 * nbase);
     int32_t *start = (int32_t *)sc.take(4 * nbase);
     double *acc = (double *)sc.take(8 * ncell);
@@ -500,40 +420,18 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     k_rm_sortcells<<<(unsigned)ceil_div(nbase, RM_THREADS), RM_THREADS, 0, st>>>(nbase, start,
                                                                                 count, perm);
     PF_TRY(launch_status("k_rm_sortcells"));
-    k_rm_sorted<<<gn, RM_THREADS, 0, st>>>(nvalid, perm, cell, x, y, g, xs, ys, gs, cs);
-    PF_TRY(launch_status("k_rm_sorted"));
-    // tile: the largest of 16x16, 16x8, 8x8, 8x4, 4x4 output cells whose
-    // covering base cells hold, at 1.5x the mean density, at most RG_CAPMAX
-    // blobs; shared memory for that many
-    const double rho = (double)n / (double)nbase;
-    int TX = 16, TY = 16;
-    auto need = [&](int tx, int ty) { return (tx + 3) * (ty + 3) * rho * 1.5 + 32.0; };
-    while (TX * TY > 16 && need(TX, TY) > RG_CAPMAX) {
-        if (TX == TY)
-            TY /= 2;
-        else
-            TX /= 2;
-    }
-    const int cap = (int)std::min<double>(RG_CAPMAX, std::ceil(need(TX, TY) / 32.0) * 32.0);
-    const int64_t tiles_y = ceil_div(nby + 3, TY), tiles = ceil_div(nbx + 3, TX) * tiles_y;
-    const int smem = cap * (int)sizeof(W9);
     WParams wp{h, xb0, yb0, xb0 / h, yb0 / h, kernel == REMESH_TUTTY ? c : c * c};
-    if (kernel == REMESH_TUTTY) {
-        PF_CUDA_TRY(cudaFuncSetAttribute(k_rm_gather<true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         RG_CAPMAX * (int)sizeof(W9)));
-        k_rm_gather<true><<<(unsigned)tiles, 2 * TX * TY, smem, st>>>(
-            nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, cs, xs, ys, gs, wp, acc,
-            flag);
-    } else {
-        PF_CUDA_TRY(cudaFuncSetAttribute(k_rm_gather<false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         RG_CAPMAX * (int)sizeof(W9)));
-        k_rm_gather<false><<<(unsigned)tiles, 2 * TX * TY, smem, st>>>(
-            nbx, nby, TX, TY, cap, tiles_y, ixmin, iymin, start, count, cs, xs, ys, gs, wp, acc,
-            flag);
-    }
-    PF_TRY(launch_status("k_rm_gather"));
+    const unsigned gb = (unsigned)ceil_div(nbase, RM_THREADS);
+    if (kernel == REMESH_TUTTY)
+        k_rm_stencil<true><<<gb, RM_THREADS, 0, st>>>(nbase, nby, ixmin, iymin, start, count, perm,
+                                                       x, y, g, wp, part);
+    else
+        k_rm_stencil<false><<<gb, RM_THREADS, 0, st>>>(nbase, nby, ixmin, iymin, start, count,
+                                                        perm, x, y, g, wp, part);
+    PF_TRY(launch_status("k_rm_stencil"));
+    k_rm_sum<<<(unsigned)ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(nbx, nby, count, part,
+                                                                           acc, flag);
+    PF_TRY(launch_status("k_rm_sum"));
     if (pc) {
         PF_TRY(popctl_decide(sc, ncell, acc, flag, *pc, st));
         PF_TRY(popctl_flags(ncell, acc, flag, pc->state, flag, st));

@@ -11,22 +11,22 @@
 //      ix-major; rank of a blob in its cell from atomicAdd.
 //   3. scan of the per-cell counts -> cell starts.
 //   4. k_rm_place  : blob index -> its slot.
-//   5. k_rm_sortcells : per base cell, order its blobs by input index (every
-//      sum below then has a fixed order, independent of atomic timing).
-//   6. k_rm_stencil : one thread per base cell: the weights of each of its
+//   5. k_rm_stencil : one thread per base cell: orders the cell's blobs by
+//      input index (every sum below then has a fixed order, independent of
+//      atomic timing), then the weights of each of its
 //      blobs -- four x weights M4'(ux_a), four y weights M4'(uy_b)
 //      (_interpolation_kernels_1d.cpp:75-89; u as _regridding.py:183) or
 //      Tutty's -- and the cell's 4 x 4 stencil of partial sums
 //      sum over its blobs (in cell order) of (wx_a wy_b) g, stored
 //      stencil-major (coalesced).
-//   7. k_rm_sum : one thread per output cell (ix, iy): the 16 partial sums of
+//   6. k_rm_sum : one thread per output cell (ix, iy): the 16 partial sums of
 //      the base cells whose windows cover it, added in fixed (b, a) order;
 //      flags cells touched by at least one window (explicit zeros are kept,
 //      like the CSR sum of the reference, _regridding.py:200-202).
 //   6b. (pf_remesh_population_control only) PopulationControl of the cell
 //      values (popctl.cu), which clears the flags of the dropped cells.
-//   8. scan of the flags -> output slots, in (ix, iy) order.
-//   9. k_rm_emit   : x = ix*h + 0.5h + xb0 (same order as :217-218), g, ix, iy.
+//   7. scan of the flags -> output slots, in (ix, iy) order.
+//   8. k_rm_emit   : x = ix*h + 0.5h + xb0 (same order as :217-218), g, ix, iy.
 // No floating-point atomics: each output value is produced by one thread.
 #include <algorithm>
 #include <cmath>
@@ -213,16 +213,9 @@ struct W9 {
     double wx[4], wy[4], g;
 };
 
-// Per base cell: order the cell's blob indices by input index (cells hold a
-// few blobs; the atomic ranks of k_rm_count are not reproducible).
-__global__ void __launch_bounds__(RM_THREADS)
-k_rm_sortcells(int64_t ncell, const int32_t *__restrict__ start,
-               const int32_t *__restrict__ count, int32_t *__restrict__ perm) {
-    const int64_t c = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
-    if (c >= ncell) return;
-    const int cnt = count[c];
-    if (cnt < 2) return;
-    const int s0 = start[c];
+// Order a base cell's blob indices perm[s0 .. s0+cnt) by input index (cells
+// hold a few blobs; the atomic ranks of k_rm_count are not reproducible).
+__device__ __forceinline__ void sort_cell(int32_t *__restrict__ perm, int s0, int cnt) {
     for (int k = 1; k < cnt; ++k) {
         const int32_t v = perm[s0 + k];
         int j = k - 1;
@@ -282,7 +275,7 @@ template <bool TUTTY>
 __global__ void __launch_bounds__(RM_THREADS)
 k_rm_stencil(int64_t nbase, int64_t nby, int32_t ixmin, int32_t iymin,
              const int32_t *__restrict__ start, const int32_t *__restrict__ count,
-             const int32_t *__restrict__ perm, const double *__restrict__ x,
+             int32_t *__restrict__ perm, const double *__restrict__ x,
              const double *__restrict__ y, const double *__restrict__ g, WParams wp,
              double *__restrict__ part) {
     const int64_t bc = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
@@ -290,6 +283,7 @@ k_rm_stencil(int64_t nbase, int64_t nby, int32_t ixmin, int32_t iymin,
     const int cnt = count[bc];
     if (cnt == 0) return;
     const int s0 = start[bc];
+    sort_cell(perm, s0, cnt);  // this thread owns the cell's range
     const int64_t bx = bc / nby, by = bc - bx * nby;
     double p[16];
 #pragma unroll
@@ -417,9 +411,6 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     PF_TRY(exclusive_scan_i32(count, start, nbase, tmp, nvalid, st));
     k_rm_place<<<gn, RM_THREADS, 0, st>>>(n, cell, rank, start, perm);
     PF_TRY(launch_status("k_rm_place"));
-    k_rm_sortcells<<<(unsigned)ceil_div(nbase, RM_THREADS), RM_THREADS, 0, st>>>(nbase, start,
-                                                                                count, perm);
-    PF_TRY(launch_status("k_rm_sortcells"));
     WParams wp{h, xb0, yb0, xb0 / h, yb0 / h, kernel == REMESH_TUTTY ? c : c * c};
     const unsigned gb = (unsigned)ceil_div(nbase, RM_THREADS);
     if (kernel == REMESH_TUTTY)

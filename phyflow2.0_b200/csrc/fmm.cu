@@ -1451,10 +1451,10 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
         pf::set_error("pf_velocity_fmm: scratch layout error");
         return PF_ERR_OOM;
     }
-    if (same) {
+    if (same) {  // targets are the sources: one tree, the target arrays alias the source ones
         T = S;
-        T.cnt = tcnt_all + level_off(L);
-        T.start = tstart;
+        tcnt_all = scnt_all;
+        tstart = S.start;
     } else {
         T.cnt = tcnt_all + level_off(L);
         T.start = tstart;
@@ -1468,18 +1468,9 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     PF_TRY(mark(0));
     // sort sources (and targets)
     PF_TRY(sort_points(ns, a.x, a.y, a.g, x0, y0, wl, L, S, tmp, st));
-    if (same) {
-        PF_CUDA_TRY(cudaMemcpyAsync(T.cnt, S.cnt, 4 * nleaf, cudaMemcpyDeviceToDevice, st));
-        PF_CUDA_TRY(cudaMemcpyAsync(tstart, S.start, 4 * nleaf, cudaMemcpyDeviceToDevice, st));
-    } else {
-        PF_TRY(sort_points(nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, st));
-    }
+    if (!same) PF_TRY(sort_points(nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, st));
     PF_TRY(count_up(L, scnt_all, st));
-    if (same)  // identical pyramid
-        PF_CUDA_TRY(cudaMemcpyAsync(tcnt_all, scnt_all, sizeof(int32_t) * level_off(L),
-                                    cudaMemcpyDeviceToDevice, st));
-    else
-        PF_TRY(count_up(L, tcnt_all, st));
+    if (!same) PF_TRY(count_up(L, tcnt_all, st));
     k_sorted_keys<<<(unsigned)pf::ceil_div(nt, 256), 256, 0, st>>>(nt, T.perm, T.key, tkey_sorted);
     PF_TRY(pf::launch_status("k_sorted_keys"));
 

@@ -270,7 +270,8 @@ __device__ __forceinline__ W9 blob_w9(int32_t i, int64_t bx, int64_t by, int32_t
 // Base cell bc = bx*nby + by: the 4 x 4 stencil of partial sums of its blobs,
 // part[(a*4 + b) * nbase + bc] = sum over the cell's blobs, in cell order, of
 // (wx_a wy_b) g; output cell (bx + a, by + b) of the window grid.  Empty
-// cells write nothing (k_rm_sum reads their count first).
+// cells write zeros (k_rm_sum then loads every entry without waiting for the
+// cell's count; adding +0.0 changes no sum).
 template <bool TUTTY>
 __global__ void __launch_bounds__(RM_THREADS)
 k_rm_stencil(int64_t nbase, int64_t nby, int32_t ixmin, int32_t iymin,
@@ -281,7 +282,6 @@ k_rm_stencil(int64_t nbase, int64_t nby, int32_t ixmin, int32_t iymin,
     const int64_t bc = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     if (bc >= nbase) return;
     const int cnt = count[bc];
-    if (cnt == 0) return;
     const int s0 = start[bc];
     sort_cell(perm, s0, cnt);  // this thread owns the cell's range
     const int64_t bx = bc / nby, by = bc - bx * nby;
@@ -321,8 +321,7 @@ k_rm_sum(int64_t nbx, int64_t nby, const int32_t *__restrict__ count,
             const int64_t bx = ox - a;
             if (bx < 0 || bx >= nbx) continue;
             const int64_t bc = bx * nby + by;
-            if (count[bc] == 0) continue;
-            touched = 1;
+            touched |= count[bc] != 0;
             sum += part[(a * 4 + b) * nbase + bc];
         }
     }

@@ -81,6 +81,16 @@ __host__ __device__ __forceinline__ uint32_t morton2(uint32_t x, uint32_t y) {
     return part1by1(x) | (part1by1(y) << 1);
 }
 
+// Morton code of (x + dx, y + dy) from the code m of (x, y) and the dilated
+// offset d = morton2(dx mod 2^16, dy mod 2^16): each coordinate's bits are
+// added with the other coordinate's bit positions filled with ones, so the
+// carries run through them ("dilated integer" addition).  Exact whenever the
+// shifted coordinates lie in [0, 2^16).
+__device__ __forceinline__ uint32_t morton_add(uint32_t m, uint32_t d) {
+    const uint32_t xm = 0x55555555u, ym = 0xaaaaaaaau;
+    return (((m | ym) + (d & xm)) & xm) | (((m | xm) + (d & ym)) & ym);
+}
+
 // leaf coordinate of a position: floor((x - x0) / w) clamped to [0, 2^L)
 __device__ __forceinline__ uint32_t leaf_coord(double x, double x0, double w, int L) {
     const double q = floor(__ddiv_rn(__dsub_rn(x, x0), w));
@@ -482,8 +492,8 @@ k_m2l(int L, int Bp, int64_t npair, const int32_t *__restrict__ scnt,
             const int sxA = ixA + f.x, syA = iyA + f.y, sxB = ixB + f.x, syB = iyB + f.y;
             useA = liveA && sxA >= 0 && syA >= 0 && sxA < side && syA < side;
             useB = liveB && sxB >= 0 && syB >= 0 && sxB < side && syB < side;
-            if (useA) sgA = level_off(l) + morton2((uint32_t)sxA, (uint32_t)syA);
-            if (useB) sgB = level_off(l) + morton2((uint32_t)sxB, (uint32_t)syB);
+            if (useA) sgA = level_off(l) + morton_add(mA, (uint32_t)f.w);
+            if (useB) sgB = level_off(l) + morton_add(mB, (uint32_t)f.w);
         }
         // the sources' counts and multipoles are loaded together (boxes in
         // range either way); an empty source box is then skipped
@@ -1244,7 +1254,12 @@ static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, doub
         for (int p = 0; p < c.maxpos; ++p) {
             ptr[l * c.maxpos + p] = (int32_t)far.size();
             if (l >= 2 && p < (int)t.far[l].size())
-                for (const auto &o : t.far[l][p]) far.push_back(make_int4(o.i, o.j, op_id(o), 0));
+                for (const auto &o : t.far[l][p]) {
+                    // .w: the offset in Morton-dilated form (two's complement per
+                    // coordinate, 16 bits each), for morton_add in k_m2l
+                    const uint32_t d = morton2((uint32_t)o.i & 0xffffu, (uint32_t)o.j & 0xffffu);
+                    far.push_back(make_int4(o.i, o.j, op_id(o), (int)d));
+                }
         }
     }
     ptr[(L + 1) * c.maxpos] = (int32_t)far.size();  // [l*maxpos + pos] .. next slot

@@ -297,19 +297,22 @@ __global__ void __launch_bounds__(128)
 k_p2m(int L, double x0, double y0, double wl, const int32_t *__restrict__ start,
       const int32_t *__restrict__ cnt, const double *__restrict__ sx,
       const double *__restrict__ sy, const double *__restrict__ sg, double2 *__restrict__ M) {
+    // four consecutive lanes per leaf, lane q taking the leaf's particles
+    // q, q + 4, ...; the four partial expansions are added in a fixed tree order
     const int64_t nleaf = (int64_t)1 << (2 * L);
-    const int64_t m = (int64_t)blockIdx.x * 128 + threadIdx.x;
-    if (m >= nleaf) return;
-    const int c = cnt[m];
-    if (c == 0) return;
+    const int64_t t = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    const int64_t m = t >> 2;
+    const int q = (int)(t & 3);
+    const bool live = m < nleaf;
+    const int c = live ? cnt[m] : 0;
     const uint32_t ix = compact1by1((uint32_t)m), iy = compact1by1((uint32_t)m >> 1);
     const double cx = x0 + ((double)ix + 0.5) * wl, cy = y0 + ((double)iy + 0.5) * wl;
     const double iw = 1.0 / wl;
     double2 a[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) a[k] = make_double2(0.0, 0.0);
-    const int s0 = start[m];
-    for (int j = 0; j < c; ++j) {
+    const int s0 = live ? start[m] : 0;
+    for (int j = q; j < c; j += 4) {
         const double2 z = make_double2((sx[s0 + j] - cx) * iw, (sy[s0 + j] - cy) * iw);
         double2 zk = make_double2(sg[s0 + j], 0.0);
 #pragma unroll
@@ -319,9 +322,19 @@ k_p2m(int L, double x0, double y0, double wl, const int32_t *__restrict__ start,
             zk = cmul(zk, z);
         }
     }
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+#pragma unroll
+        for (int o = 1; o <= 2; o <<= 1) {
+            a[k].x += __shfl_xor_sync(0xffffffffu, a[k].x, o);
+            a[k].y += __shfl_xor_sync(0xffffffffu, a[k].y, o);
+        }
+    }
+    if (!live || c == 0) return;
     const int64_t base = ((((int64_t)1 << (2 * L)) - 1) / 3 + m) * NP;
 #pragma unroll
-    for (int k = 0; k < NP; ++k) M[base + k] = a[k];
+    for (int k = 0; k < NP; ++k)
+        if ((k & 3) == q) M[base + k] = a[k];
 }
 
 
@@ -1491,7 +1504,7 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
 
     PF_TRY(mark(1));
     // upward pass
-    k_p2m<NP><<<(unsigned)pf::ceil_div(nleaf, 128), 128, 0, st>>>(L, x0, y0, wl, S.start, S.cnt,
+    k_p2m<NP><<<(unsigned)pf::ceil_div(4 * nleaf, 128), 128, 0, st>>>(L, x0, y0, wl, S.start, S.cnt,
                                                                  S.x, S.y, S.g, M);
     PF_TRY(pf::launch_status("k_p2m"));
     constexpr int BOXES_PER_CTA = (WARP_BOX_THREADS / 32) * BoxLanes<NP>::BPW;

@@ -237,11 +237,13 @@ k_leaf_sort(int64_t nleaf, const int32_t *__restrict__ start, const int32_t *__r
 __global__ void __launch_bounds__(256)
 k_gather_sorted(int64_t n, const int32_t *__restrict__ perm, const double *__restrict__ x,
                 const double *__restrict__ y, const double *__restrict__ g,
-                double *__restrict__ sx, double *__restrict__ sy, double *__restrict__ sg,
-                float4 *__restrict__ hl, float *__restrict__ g32) {
+                const uint32_t *__restrict__ key, double *__restrict__ sx,
+                double *__restrict__ sy, double *__restrict__ sg, float4 *__restrict__ hl,
+                float *__restrict__ g32, uint32_t *__restrict__ skey) {
     const int64_t j = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (j >= n) return;
     const int32_t i = perm[j];
+    if (skey) skey[j] = key[i];  // leaf key in sorted order (targets)
     const double a = x[i], b = y[i];
     sx[j] = a;
     sy[j] = b;
@@ -1176,13 +1178,6 @@ k_l2p(int64_t nt, int L, double x0, double y0, double wl, const double *__restri
     vy[o] = nv.y + INV_2PI * iw * w.x;
 }
 
-// sorted target keys (leaf of every sorted target)
-__global__ void __launch_bounds__(256)
-k_sorted_keys(int64_t n, const int32_t *__restrict__ perm, const uint32_t *__restrict__ key,
-              uint32_t *__restrict__ skey) {
-    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
-    if (i < n) skey[i] = key[perm[i]];
-}
 
 // ---------------------------------------------------------------------------
 // Host: plan cache (tables + operators on the device)
@@ -1372,7 +1367,7 @@ struct Sorted {
 
 static pf_status sort_points(int64_t n, const double *x, const double *y,
                              const double *g, double x0, double y0, double wl, int L, Sorted &s,
-                             int32_t *scan_tmp, cudaStream_t st) {
+                             int32_t *scan_tmp, uint32_t *skey, cudaStream_t st) {
     const int64_t nleaf = (int64_t)1 << (2 * L);
     PF_CUDA_TRY(cudaMemsetAsync(s.cnt, 0, sizeof(int32_t) * nleaf, st));
     if (n == 0) {
@@ -1387,7 +1382,8 @@ static pf_status sort_points(int64_t n, const double *x, const double *y,
     PF_TRY(pf::launch_status("k_place"));
     k_leaf_sort<<<(unsigned)pf::ceil_div(nleaf, 128), 128, 0, st>>>(nleaf, s.start, s.cnt, s.perm);
     PF_TRY(pf::launch_status("k_leaf_sort"));
-    k_gather_sorted<<<gn, 256, 0, st>>>(n, s.perm, x, y, g, s.x, s.y, s.g, s.hl, s.g32);
+    k_gather_sorted<<<gn, 256, 0, st>>>(n, s.perm, x, y, g, s.key, s.x, s.y, s.g, s.hl, s.g32,
+                                        skey);
     return pf::launch_status("k_gather_sorted");
 }
 
@@ -1495,12 +1491,13 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     };
     PF_TRY(mark(0));
     // sort sources (and targets)
-    PF_TRY(sort_points(ns, a.x, a.y, a.g, x0, y0, wl, L, S, tmp, st));
-    if (!same) PF_TRY(sort_points(nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, st));
+    // sorted target keys come out of the sorted copies of the targets
+    PF_TRY(sort_points(ns, a.x, a.y, a.g, x0, y0, wl, L, S, tmp, same ? tkey_sorted : nullptr,
+                       st));
+    if (!same)
+        PF_TRY(sort_points(nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, tkey_sorted, st));
     PF_TRY(count_up(L, scnt_all, st));
     if (!same) PF_TRY(count_up(L, tcnt_all, st));
-    k_sorted_keys<<<(unsigned)pf::ceil_div(nt, 256), 256, 0, st>>>(nt, T.perm, T.key, tkey_sorted);
-    PF_TRY(pf::launch_status("k_sorted_keys"));
 
     PF_TRY(mark(1));
     // upward pass

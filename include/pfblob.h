@@ -150,8 +150,9 @@ typedef struct pf_fmm_stats {
     int64_t m2l_translations; /* multipole-to-local translations */
     float ms_sort, ms_upward, ms_m2l, ms_downward, ms_p2p, ms_l2p, ms_total;
     float reserved;
-    int64_t p2p_pairs_far;    /* of p2p_pairs, those in source tiles beyond the
-                                 Gaussian's reach (no exponential evaluated) */
+    int64_t p2p_pairs_far;    /* of p2p_pairs, those whose source lies beyond the
+                                 Gaussian's reach of every target of its group
+                                 (no exponential evaluated) */
 } pf_fmm_stats;
 pf_status pf_fmm_profile(pf_ctx *ctx, int enable);
 pf_status pf_fmm_last_stats(pf_ctx *ctx, pf_fmm_stats *out);

@@ -696,17 +696,19 @@ k_p2p_runs(int L, int kb, const int2 *__restrict__ q, int nq, int nqp,
     if (!runs && threadIdx.x == 0) nruns_or_off[b] = s_n;
 }
 
-// P2P near field: one warp (one CTA) per P2P block, up to three targets per
-// lane (a group of up to 96), warp-private source tiles of 64.  Targets a and
-// b of a lane run packed (f32x2), target c scalar; NT = targets per lane.
-// Pair code modes, chosen per source from its box distance to the group's
-// target box (with a rounding margin):
+// P2P near field: one warp (one CTA) per P2P block, its targets in balanced
+// groups of at most 96.  Targets a and b of a lane run packed (f32x2); in a
+// group of 65..96 the remaining targets are spread over the warp, each lane
+// taking a share of the sources (p2p_split_sums).  Pair code modes, chosen
+// per source from its box distance to the group's target box (with a
+// rounding margin):
 //   P2P_FAR:    sources beyond sqrt(r2_far): no ex2 (1 - exp(-x) rounds to
-//               1.0f for every pair);
+//               1.0f for every pair), one-float coordinates relative to the
+//               group centre;
 //   P2P_FULL:   the other sources beyond the series radius sqrt(r2_series):
 //               no small-x check (every pair has r2 above r2_series);
 //   P2P_SERIES: the sources within it: the pair code with the check.
-// Each pair gives bitwise the value of the checked code.  The group's
+// Full and series pairs give bitwise the value of the checked code.  The group's
 // sources stream through three warp buffers, one per mode (each in stream
 // order), and each buffer runs 32 sources at a time as it fills (the rest
 // when the group's stream ends).

@@ -957,8 +957,8 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
       const int32_t *__restrict__ sstart, const int32_t *__restrict__ scnt,
       const float4 *__restrict__ shl, const float *__restrict__ sg32,
       const float4 *__restrict__ thl, const int32_t *__restrict__ run_off,
-      const int2 *__restrict__ runs, pfd::GaussParams gp, double2 *__restrict__ nearv,
-      unsigned long long *__restrict__ pairs) {
+      const int2 *__restrict__ runs, const int32_t *__restrict__ order, pfd::GaussParams gp,
+      double2 *__restrict__ nearv, unsigned long long *__restrict__ pairs) {
     __shared__ int s_rs[P2P_RUNS_SM];      // particle start of run
     __shared__ int s_rp[P2P_RUNS_SM + 1];  // stream prefix of run
     // source buffers, one per mode: [P2P_FAR], [P2P_FULL], [P2P_SERIES]
@@ -967,8 +967,8 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
     __shared__ unsigned long long s_g2[3][P2P_BUF];  // {g, g}
     const int lane = threadIdx.x;
     const unsigned lt = (1u << lane) - 1u;
-    const int64_t b = blockIdx.x;
-    if (b >= nblk) return;
+    if ((int64_t)blockIdx.x >= nblk) return;
+    const int64_t b = order[blockIdx.x];
     const uint32_t leaf0 = (uint32_t)b << (2 * kb), nl = 1u << (2 * kb);
     const int t0 = tstart[leaf0];
     const int tn = tstart[leaf0 + nl - 1] + tcnt[leaf0 + nl - 1] - t0;
@@ -1192,6 +1192,7 @@ struct FmmCache {
     int2 *d_q = nullptr;
     int32_t *d_run_off = nullptr;  // [nblk + 1]
     int2 *d_runs = nullptr;        // (first, last) leaf of each run
+    int32_t *d_blk_order = nullptr;  // P2P block launch order (heaviest first)
     int64_t nruns = 0;
     size_t dev_bytes = 0;          // device memory held by this plan
     size_t bytes() const { return dev_bytes; }
@@ -1207,6 +1208,8 @@ struct FmmCache {
         cudaFree(d_bin);
         cudaFree(d_run_off);
         cudaFree(d_runs);
+        cudaFree(d_blk_order);
+        d_blk_order = nullptr;
         d_run_off = nullptr;
         d_runs = nullptr;
         d_far = nullptr;
@@ -1350,6 +1353,20 @@ static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, doub
         PF_TRY(pf::launch_status("k_p2p_runs"));
         PF_CUDA_TRY(cudaDeviceSynchronize());
         tally += sizeof(int32_t) * (nblk + 1) + sizeof(int2) * (acc > 0 ? acc : 1);
+        // launch order of the blocks: most near-set leaves first, so that the
+        // lighter blocks (near the domain edges) fill the end of the launch
+        std::vector<int2> runs(acc > 0 ? acc : 1);
+        if (acc > 0)
+            PF_CUDA_TRY(cudaMemcpy(runs.data(), c.d_runs, sizeof(int2) * acc,
+                                   cudaMemcpyDeviceToHost));
+        std::vector<int64_t> wgt(nblk, 0);
+        for (int64_t b = 0; b < nblk; ++b)
+            for (int32_t r = cnt[b]; r < cnt[b + 1]; ++r) wgt[b] += runs[r].y - runs[r].x + 1;
+        std::vector<int32_t> order(nblk);
+        for (int64_t b = 0; b < nblk; ++b) order[b] = (int32_t)b;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int32_t a, int32_t b) { return wgt[a] > wgt[b]; });
+        PF_TRY(upload(&c.d_blk_order, order, tally));
     }
     c.dev_bytes = tally;
     c.L = L;
@@ -1550,7 +1567,7 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
         const int64_t nblk = (int64_t)1 << (2 * (L - kb));
         k_p2p<<<(unsigned)nblk, 32, 0, st>>>(
             nblk, kb, tstart, T.cnt, S.start, S.cnt, S.hl, S.g32, T.hl, c.d_run_off, c.d_runs,
-            pfd::make_gauss_params(a.ksigmasqr), nearv, ctr);
+            c.d_blk_order, pfd::make_gauss_params(a.ksigmasqr), nearv, ctr);
         PF_TRY(pf::launch_status("k_p2p"));
     }
     PF_TRY(mark(5));

@@ -164,3 +164,23 @@ def test_caller_box_equals_computed_box():
         out.append((vx.cpu().numpy(), vy.cpu().numpy()))
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     assert normwise_err(out[2][0], out[2][1], out[0][0], out[0][1]) <= TOL
+
+
+def test_stats_pair_counts():
+    """pf_fmm_last_stats (the C struct read through ctypes): sizes as given,
+    the far-pair count (sources beyond the Gaussian's reach of their whole
+    target group) strictly between 0 and the near-field pair count for a
+    uniform set, the pair count between n and n^2, M2L translations > 0."""
+    import pfblob
+    from pfblob import _lib
+    n, sigma = 65536, 0.002
+    rng = np.random.default_rng(11)
+    x, y = rng.random(n), rng.random(n)
+    g = rng.standard_normal(n) / n
+    fmm(x, y, g, sigma)
+    st = _lib.fmm_last_stats(0)
+    assert st["used_direct"] == 0
+    assert st["n_src"] == n and st["n_tgt"] == n
+    assert 0 < st["p2p_pairs_far"] < st["p2p_pairs"]
+    assert st["m2l_translations"] > 0
+    assert n <= st["p2p_pairs"] <= n * n  # each blob meets at least itself

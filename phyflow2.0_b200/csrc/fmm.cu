@@ -952,13 +952,216 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
+constexpr int P2P_OWN_GROUPS = 4;  // target groups a block's own CTA computes at most
+
+// Work-distribution state of the P2P launches, zeroed before the first.
+struct P2PWork {
+    unsigned *heavy_n;   // entries in heavy
+    int32_t *heavy;      // blocks with several target groups [nblk]
+    int32_t *grp_next;   // groups of each heavy block handed out so far [nblk]
+};
+
+// Target group gi of block b (groups of at most 96 targets, balanced: sizes
+// differ by at most one; every group streams all the block's sources, so a
+// small last group would cost nearly as much as a full one) against the
+// block's whole source stream; writes the group's near-field velocities.
+__device__ __forceinline__ void p2p_group_body(
+    int64_t b, int t0, int tn, int ngrp, int gi, const int32_t *__restrict__ sstart,
+    const int32_t *__restrict__ scnt, const float4 *__restrict__ shl,
+    const float *__restrict__ sg32, const float4 *__restrict__ thl,
+    const int32_t *__restrict__ run_off, const int2 *__restrict__ runs, pfd::GaussParams gp,
+    double2 *__restrict__ nearv, ulonglong2 (*s_hi)[P2P_BUF], ulonglong2 (*s_lo)[P2P_BUF],
+    unsigned long long (*s_g2)[P2P_BUF], int *s_rs, int *s_rp, unsigned long long &npairs,
+    unsigned long long &nfar) {
+    const int lane = threadIdx.x;
+    const unsigned lt = (1u << lane) - 1u;
+    const float rser = sqrtf(gp.r2_series);
+    const int r0 = run_off[b], r1 = run_off[b + 1];
+    const int tg = (int)((int64_t)gi * tn / ngrp);
+    const int gsz = (int)((int64_t)(gi + 1) * tn / ngrp) - tg;
+    const int nt = (gsz <= 32) ? 1 : (gsz <= 64) ? 2 : 3;  // warp-uniform
+    // nt = 3: remainder targets tg + 64 + j, j < rem, each on msp lanes
+    const int rem = nt == 3 ? gsz - 64 : 32;
+    const int msp = 32 / rem;
+    const bool cval = nt == 3 && lane < rem * msp;
+    const int qs = cval ? lane / rem : 32;
+    const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane % rem;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 ta = (lane < gsz) ? thl[t0 + ia] : z4;
+    const float4 tb = (lane + 32 < gsz) ? thl[t0 + ib] : z4;
+    const float4 tc = cval ? thl[t0 + ic] : z4;
+    // box of the group's targets (hi parts), for the series-free test
+    float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
+    if (lane < gsz) { bx0 = bx1 = ta.x; by0 = by1 = ta.y; }
+    if (lane + 32 < gsz) { bx0 = fminf(bx0, tb.x); bx1 = fmaxf(bx1, tb.x); by0 = fminf(by0, tb.y); by1 = fmaxf(by1, tb.y); }
+    if (cval) { bx0 = fminf(bx0, tc.x); bx1 = fmaxf(bx1, tc.x); by0 = fminf(by0, tc.y); by1 = fmaxf(by1, tc.y); }
+    bx0 = warp_min(bx0);
+    bx1 = warp_max(bx1);
+    by0 = warp_min(by0);
+    by1 = warp_max(by1);
+    // a source at box distance d has r2 >= (d - e)^2 for every target, e
+    // covering the hi-part rounding of both points (2^-23 relative each)
+    const float mag = fmaxf(fmaxf(fabsf(bx0), fabsf(bx1)), fmaxf(fabsf(by0), fabsf(by1)));
+    const float reach = rser * 1.001f + (mag + rser) * 4.8e-7f + 1e-30f;
+    const float reach2 = reach * reach;
+    const float rfar = sqrtf(gp.r2_far);
+    const float reachf = rfar * 1.001f + (mag + rfar) * 4.8e-7f + 1e-30f;
+    const float reachf2 = reachf * reachf;
+    // centre for the far sources' relative coordinates (any float near the group)
+    const float cx = 0.5f * (bx0 + bx1), cy = 0.5f * (by0 + by1);
+    float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int c0 = 0, c1 = 0, c2 = 0;  // entries waiting in the three buffers
+    for (int rc = r0; rc < r1; rc += P2P_RUNS_SM) {
+        const int nrc = min(P2P_RUNS_SM, r1 - rc);
+        int pre = 0;
+        for (int k0 = 0; k0 < nrc; k0 += 32) {
+            const int k = k0 + lane;
+            int st = 0, len = 0;
+            if (k < nrc) {
+                const int2 rr = runs[rc + k];
+                st = sstart[rr.x];
+                len = sstart[rr.y] + scnt[rr.y] - st;
+            }
+            int inc = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += t;
+            }
+            if (k < nrc) {
+                s_rs[k] = st;
+                s_rp[k] = pre + inc - len;
+            }
+            pre += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        if (lane == 0) s_rp[nrc] = pre;
+        __syncwarp();
+        const int S = pre;
+        npairs += (unsigned long long)S * (unsigned long long)gsz;
+        // each lane's stream position only moves forward (by 32 per
+        // round), so the run holding it is found by advancing an index:
+        // the largest r with prefix[r] <= p (empty runs are stepped over).
+        // The loads of round s0 + 32 are issued before round s0's chunks
+        // run, so their latency overlaps the pair work.
+        int rr = 0;
+        float4 spv = z4;
+        float gg = 0.f;
+        auto fetch = [&](int p, float4 &v, float &w) {
+            if (p < S) {
+                while (rr + 1 < nrc && s_rp[rr + 1] <= p) ++rr;
+                const int src = s_rs[rr] + (p - s_rp[rr]);
+                v = shl[src];
+                w = sg32[src];
+            }
+        };
+        fetch(lane, spv, gg);
+        for (int s0 = 0; s0 < S; s0 += 32) {
+            const int p = s0 + lane;
+            int cls = -1;  // 0 far, 1 full, 2 series; -1 past the stream
+            if (p < S) {
+                const float ex = fmaxf(fmaxf(bx0 - spv.x, spv.x - bx1), 0.f);
+                const float ey = fmaxf(fmaxf(by0 - spv.y, spv.y - by1), 0.f);
+                const float d2 = ex * ex + ey * ey;
+                cls = d2 > reachf2 ? 0 : d2 > reach2 ? 1 : 2;
+            }
+            // append each source to the buffer of its mode, in stream order
+            const unsigned m0 = __ballot_sync(0xffffffffu, cls == 0);
+            const unsigned m1 = __ballot_sync(0xffffffffu, cls == 1);
+            const unsigned m2 = __ballot_sync(0xffffffffu, cls == 2);
+            if (cls >= 0) {
+                const unsigned mm = cls == 0 ? m0 : cls == 1 ? m1 : m2;
+                const int k = (cls == 0 ? c0 : cls == 1 ? c1 : c2) + __popc(mm & lt);
+                if (cls == 0) {  // far: coordinates relative to the group centre
+                    const float lx = (spv.x - cx) + spv.z, ly = (spv.y - cy) + spv.w;
+                    s_hi[0][k] = make_ulonglong2(pfd::pack2(lx, lx), pfd::pack2(ly, ly));
+                } else {
+                    s_hi[cls][k] = make_ulonglong2(pfd::pack2(spv.x, spv.x),
+                                                   pfd::pack2(spv.y, spv.y));
+                    s_lo[cls][k] = make_ulonglong2(pfd::pack2(spv.z, spv.z),
+                                                   pfd::pack2(spv.w, spv.w));
+                }
+                s_g2[cls][k] = pfd::pack2(gg, gg);
+            }
+            c0 += __popc(m0);
+            c1 += __popc(m1);
+            c2 += __popc(m2);
+            spv = z4;
+            gg = 0.f;
+            fetch(p + 32, spv, gg);
+            __syncwarp();
+            if (c0 >= 32) {
+                p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], 32, ta, tb, tc,
+                                       qs, msp, cx, cy, gp, acc);
+                nfar += 32ull * (unsigned long long)gsz;
+                c0 -= 32;
+                p2p_buf_shift(s_hi[0], s_lo[0], s_g2[0], c0, lane);
+            }
+            if (c1 >= 32) {
+                p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], 32, ta, tb, tc,
+                                        qs, msp, cx, cy, gp, acc);
+                c1 -= 32;
+                p2p_buf_shift(s_hi[1], s_lo[1], s_g2[1], c1, lane);
+            }
+            if (c2 >= 32) {
+                p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], 32, ta, tb, tc,
+                                          qs, msp, cx, cy, gp, acc);
+                c2 -= 32;
+                p2p_buf_shift(s_hi[2], s_lo[2], s_g2[2], c2, lane);
+            }
+        }
+    }
+    // what is left in the buffers (fewer than 32 each)
+    if (c0)
+        p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], c0, ta, tb, tc,
+                               qs, msp, cx, cy, gp, acc);
+    nfar += (unsigned long long)c0 * (unsigned long long)gsz;
+    if (c1)
+        p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], c1, ta, tb, tc,
+                                qs, msp, cx, cy, gp, acc);
+    if (c2)
+        p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], c2, ta, tb, tc,
+                                  qs, msp, cx, cy, gp, acc);
+    __syncwarp();
+    if (lane < gsz)
+        nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),
+                                      INV_2PI * ((double)acc[2] + (double)acc[3]));
+    if (lane + 32 < gsz)
+        nearv[t0 + ib] = make_double2(INV_2PI * ((double)acc[4] + (double)acc[5]),
+                                      INV_2PI * ((double)acc[6] + (double)acc[7]));
+    if (nt == 3) {  // combine the msp shares of each remainder target, in lane order
+        float h0 = acc[8], l0 = acc[9], h1 = acc[10], l1 = acc[11];
+        for (int q = 1; q < msp; ++q) {
+            const int sl = lane % rem + rem * q;  // < rem * msp <= 32
+            const float a = __shfl_sync(0xffffffffu, acc[8], sl);
+            const float b = __shfl_sync(0xffffffffu, acc[9], sl);
+            const float c = __shfl_sync(0xffffffffu, acc[10], sl);
+            const float d = __shfl_sync(0xffffffffu, acc[11], sl);
+            pfd::comp_add(h0, l0, a);
+            l0 += b;
+            pfd::comp_add(h1, l1, c);
+            l1 += d;
+        }
+        if (lane < rem)
+            nearv[t0 + ic] = make_double2(INV_2PI * ((double)h0 + (double)l0),
+                                          INV_2PI * ((double)h1 + (double)l1));
+    }
+}
+
+// Two launches of one kernel.  HEAVY = false: one CTA per P2P block (in
+// launch order) computes the block's target groups, unless there are more
+// than P2P_OWN_GROUPS of them: such a block (a dense cluster) is listed as
+// heavy.  HEAVY = true: persistent CTAs share out the groups of the heavy
+// blocks through per-block counters (counters only, no waits; each group is
+// computed by exactly one CTA, so results do not depend on the schedule).
+// Without dense clusters the second launch finds nothing to do.
+template <bool HEAVY>
 __global__ void __launch_bounds__(32, P2P_MIN_CTAS)
 k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *__restrict__ tcnt,
       const int32_t *__restrict__ sstart, const int32_t *__restrict__ scnt,
       const float4 *__restrict__ shl, const float *__restrict__ sg32,
       const float4 *__restrict__ thl, const int32_t *__restrict__ run_off,
       const int2 *__restrict__ runs, const int32_t *__restrict__ order, pfd::GaussParams gp,
-      double2 *__restrict__ nearv, unsigned long long *__restrict__ pairs) {
+      double2 *__restrict__ nearv, unsigned long long *__restrict__ pairs, P2PWork work) {
     __shared__ int s_rs[P2P_RUNS_SM];      // particle start of run
     __shared__ int s_rp[P2P_RUNS_SM + 1];  // stream prefix of run
     // source buffers, one per mode: [P2P_FAR], [P2P_FULL], [P2P_SERIES]
@@ -966,194 +1169,61 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
     __shared__ ulonglong2 s_lo[3][P2P_BUF];  // {x_lo, x_lo}, {y_lo, y_lo}
     __shared__ unsigned long long s_g2[3][P2P_BUF];  // {g, g}
     const int lane = threadIdx.x;
-    const unsigned lt = (1u << lane) - 1u;
-    if ((int64_t)blockIdx.x >= nblk) return;
-    const int64_t b = order[blockIdx.x];
-    const uint32_t leaf0 = (uint32_t)b << (2 * kb), nl = 1u << (2 * kb);
-    const int t0 = tstart[leaf0];
-    const int tn = tstart[leaf0 + nl - 1] + tcnt[leaf0 + nl - 1] - t0;
-    if (tn == 0) return;
-    const int r0 = run_off[b], r1 = run_off[b + 1];
-    const float rser = sqrtf(gp.r2_series);
     unsigned long long npairs = 0, nfar = 0;
-    // groups of at most 96 targets, balanced (sizes differ by at most one):
-    // every group streams all the block's sources, so a small last group
-    // would cost nearly as much as a full one
-    const int ngrp = (tn + 95) / 96;
-    for (int tg = 0, gi = 1; tg < tn; ++gi) {
-        const int gsz = gi * tn / ngrp - tg;  // tn < 2^31 / ngrp
-        const int nt = (gsz <= 32) ? 1 : (gsz <= 64) ? 2 : 3;  // warp-uniform
-        // nt = 3: remainder targets tg + 64 + j, j < rem, each on msp lanes
-        const int rem = nt == 3 ? gsz - 64 : 32;
-        const int msp = 32 / rem;
-        const bool cval = nt == 3 && lane < rem * msp;
-        const int qs = cval ? lane / rem : 32;
-        const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane % rem;
-        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 ta = (lane < gsz) ? thl[t0 + ia] : z4;
-        const float4 tb = (lane + 32 < gsz) ? thl[t0 + ib] : z4;
-        const float4 tc = cval ? thl[t0 + ic] : z4;
-        // box of the group's targets (hi parts), for the series-free test
-        float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
-        if (lane < gsz) { bx0 = bx1 = ta.x; by0 = by1 = ta.y; }
-        if (lane + 32 < gsz) { bx0 = fminf(bx0, tb.x); bx1 = fmaxf(bx1, tb.x); by0 = fminf(by0, tb.y); by1 = fmaxf(by1, tb.y); }
-        if (cval) { bx0 = fminf(bx0, tc.x); bx1 = fmaxf(bx1, tc.x); by0 = fminf(by0, tc.y); by1 = fmaxf(by1, tc.y); }
-        bx0 = warp_min(bx0);
-        bx1 = warp_max(bx1);
-        by0 = warp_min(by0);
-        by1 = warp_max(by1);
-        // a source at box distance d has r2 >= (d - e)^2 for every target, e
-        // covering the hi-part rounding of both points (2^-23 relative each)
-        const float mag = fmaxf(fmaxf(fabsf(bx0), fabsf(bx1)), fmaxf(fabsf(by0), fabsf(by1)));
-        const float reach = rser * 1.001f + (mag + rser) * 4.8e-7f + 1e-30f;
-        const float reach2 = reach * reach;
-        const float rfar = sqrtf(gp.r2_far);
-        const float reachf = rfar * 1.001f + (mag + rfar) * 4.8e-7f + 1e-30f;
-        const float reachf2 = reachf * reachf;
-        // centre for the far sources' relative coordinates (any float near the group)
-        const float cx = 0.5f * (bx0 + bx1), cy = 0.5f * (by0 + by1);
-        float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        int c0 = 0, c1 = 0, c2 = 0;  // entries waiting in the three buffers
-        for (int rc = r0; rc < r1; rc += P2P_RUNS_SM) {
-            const int nrc = min(P2P_RUNS_SM, r1 - rc);
-            int pre = 0;
-            for (int k0 = 0; k0 < nrc; k0 += 32) {
-                const int k = k0 + lane;
-                int st = 0, len = 0;
-                if (k < nrc) {
-                    const int2 rr = runs[rc + k];
-                    st = sstart[rr.x];
-                    len = sstart[rr.y] + scnt[rr.y] - st;
-                }
-                int inc = len;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int t = __shfl_up_sync(0xffffffffu, inc, o);
-                    if (lane >= o) inc += t;
-                }
-                if (k < nrc) {
-                    s_rs[k] = st;
-                    s_rp[k] = pre + inc - len;
-                }
-                pre += __shfl_sync(0xffffffffu, inc, 31);
-            }
-            if (lane == 0) s_rp[nrc] = pre;
-            __syncwarp();
-            const int S = pre;
-            npairs += (unsigned long long)S * (unsigned long long)gsz;
-            // each lane's stream position only moves forward (by 32 per
-            // round), so the run holding it is found by advancing an index:
-            // the largest r with prefix[r] <= p (empty runs are stepped over).
-            // The loads of round s0 + 32 are issued before round s0's chunks
-            // run, so their latency overlaps the pair work.
-            int rr = 0;
-            float4 spv = z4;
-            float gg = 0.f;
-            auto fetch = [&](int p, float4 &v, float &w) {
-                if (p < S) {
-                    while (rr + 1 < nrc && s_rp[rr + 1] <= p) ++rr;
-                    const int src = s_rs[rr] + (p - s_rp[rr]);
-                    v = shl[src];
-                    w = sg32[src];
-                }
-            };
-            fetch(lane, spv, gg);
-            for (int s0 = 0; s0 < S; s0 += 32) {
-                const int p = s0 + lane;
-                int cls = -1;  // 0 far, 1 full, 2 series; -1 past the stream
-                if (p < S) {
-                    const float ex = fmaxf(fmaxf(bx0 - spv.x, spv.x - bx1), 0.f);
-                    const float ey = fmaxf(fmaxf(by0 - spv.y, spv.y - by1), 0.f);
-                    const float d2 = ex * ex + ey * ey;
-                    cls = d2 > reachf2 ? 0 : d2 > reach2 ? 1 : 2;
-                }
-                // append each source to the buffer of its mode, in stream order
-                const unsigned m0 = __ballot_sync(0xffffffffu, cls == 0);
-                const unsigned m1 = __ballot_sync(0xffffffffu, cls == 1);
-                const unsigned m2 = __ballot_sync(0xffffffffu, cls == 2);
-                if (cls >= 0) {
-                    const unsigned mm = cls == 0 ? m0 : cls == 1 ? m1 : m2;
-                    const int k = (cls == 0 ? c0 : cls == 1 ? c1 : c2) + __popc(mm & lt);
-                    if (cls == 0) {  // far: coordinates relative to the group centre
-                        const float lx = (spv.x - cx) + spv.z, ly = (spv.y - cy) + spv.w;
-                        s_hi[0][k] = make_ulonglong2(pfd::pack2(lx, lx), pfd::pack2(ly, ly));
-                    } else {
-                        s_hi[cls][k] = make_ulonglong2(pfd::pack2(spv.x, spv.x),
-                                                       pfd::pack2(spv.y, spv.y));
-                        s_lo[cls][k] = make_ulonglong2(pfd::pack2(spv.z, spv.z),
-                                                       pfd::pack2(spv.w, spv.w));
-                    }
-                    s_g2[cls][k] = pfd::pack2(gg, gg);
-                }
-                c0 += __popc(m0);
-                c1 += __popc(m1);
-                c2 += __popc(m2);
-                spv = z4;
-                gg = 0.f;
-                fetch(p + 32, spv, gg);
-                __syncwarp();
-                if (c0 >= 32) {
-                    p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], 32, ta, tb, tc,
-                                           qs, msp, cx, cy, gp, acc);
-                    nfar += 32ull * (unsigned long long)gsz;
-                    c0 -= 32;
-                    p2p_buf_shift(s_hi[0], s_lo[0], s_g2[0], c0, lane);
-                }
-                if (c1 >= 32) {
-                    p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], 32, ta, tb, tc,
-                                            qs, msp, cx, cy, gp, acc);
-                    c1 -= 32;
-                    p2p_buf_shift(s_hi[1], s_lo[1], s_g2[1], c1, lane);
-                }
-                if (c2 >= 32) {
-                    p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], 32, ta, tb, tc,
-                                              qs, msp, cx, cy, gp, acc);
-                    c2 -= 32;
-                    p2p_buf_shift(s_hi[2], s_lo[2], s_g2[2], c2, lane);
-                }
+    auto targets = [&](int64_t b, int &t0) {
+        const uint32_t leaf0 = (uint32_t)b << (2 * kb), nl = 1u << (2 * kb);
+        t0 = tstart[leaf0];
+        return tstart[leaf0 + nl - 1] + tcnt[leaf0 + nl - 1] - t0;
+    };
+    if (!HEAVY) {
+        if ((int64_t)blockIdx.x >= nblk) return;
+        const int64_t b = order[blockIdx.x];
+        int t0;
+        const int tn = targets(b, t0);
+        if (tn == 0) return;
+        const int ngrp = (tn + 95) / 96;
+        if (ngrp > P2P_OWN_GROUPS) {  // left to the second launch
+            if (lane == 0) work.heavy[atomicAdd(work.heavy_n, 1u)] = (int32_t)b;
+        } else {
+            for (int gi = 0; gi < ngrp; ++gi)
+                p2p_group_body(b, t0, tn, ngrp, gi, sstart, scnt, shl, sg32, thl, run_off, runs,
+                               gp, nearv, s_hi, s_lo, s_g2, s_rs, s_rp, npairs, nfar);
+        }
+    } else {
+        const unsigned nh = *work.heavy_n;  // complete: written by the first launch
+        for (unsigned k = 0; k < nh; ++k) {
+            const int64_t b = work.heavy[k];
+            int t0;
+            const int tn = targets(b, t0);
+            const int ngrp = (tn + 95) / 96;
+            for (;;) {
+                unsigned gi = 0;
+                if (lane == 0) gi = atomicAdd((unsigned *)&work.grp_next[b], 1u);
+                gi = __shfl_sync(0xffffffffu, gi, 0);
+                if ((int)gi >= ngrp) break;
+                p2p_group_body(b, t0, tn, ngrp, (int)gi, sstart, scnt, shl, sg32, thl, run_off,
+                               runs, gp, nearv, s_hi, s_lo, s_g2, s_rs, s_rp, npairs, nfar);
             }
         }
-        // what is left in the buffers (fewer than 32 each)
-        if (c0)
-            p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], c0, ta, tb, tc,
-                                   qs, msp, cx, cy, gp, acc);
-        nfar += (unsigned long long)c0 * (unsigned long long)gsz;
-        if (c1)
-            p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], c1, ta, tb, tc,
-                                    qs, msp, cx, cy, gp, acc);
-        if (c2)
-            p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], c2, ta, tb, tc,
-                                      qs, msp, cx, cy, gp, acc);
-        __syncwarp();
-        if (lane < gsz)
-            nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),
-                                          INV_2PI * ((double)acc[2] + (double)acc[3]));
-        if (lane + 32 < gsz)
-            nearv[t0 + ib] = make_double2(INV_2PI * ((double)acc[4] + (double)acc[5]),
-                                          INV_2PI * ((double)acc[6] + (double)acc[7]));
-        if (nt == 3) {  // combine the msp shares of each remainder target, in lane order
-            float h0 = acc[8], l0 = acc[9], h1 = acc[10], l1 = acc[11];
-            for (int q = 1; q < msp; ++q) {
-                const int sl = lane % rem + rem * q;  // < rem * msp <= 32
-                const float a = __shfl_sync(0xffffffffu, acc[8], sl);
-                const float b = __shfl_sync(0xffffffffu, acc[9], sl);
-                const float c = __shfl_sync(0xffffffffu, acc[10], sl);
-                const float d = __shfl_sync(0xffffffffu, acc[11], sl);
-                pfd::comp_add(h0, l0, a);
-                l0 += b;
-                pfd::comp_add(h1, l1, c);
-                l1 += d;
-            }
-            if (lane < rem)
-                nearv[t0 + ic] = make_double2(INV_2PI * ((double)h0 + (double)l0),
-                                              INV_2PI * ((double)h1 + (double)l1));
-        }
-        tg += gsz;
     }
     if (lane == 0) {
         atomicAdd(pairs, npairs);
         atomicAdd(pairs + 2, nfar);
     }
+}
+
+// SMs of the current device (cached per device).
+static int p2p_sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (cached[dev] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+            v = 148;
+        cached[dev] = v;
+    }
+    return cached[dev];
 }
 
 // L2P + near + scatter to input order: one thread per sorted target
@@ -1443,6 +1513,7 @@ static size_t fmm_scratch_bytes(const FmmCache &c, int64_t ns, int64_t nt, bool 
     add(4 * nleaf); add(4 * nleaf);                 // starts src, tgt
     add(16 * (size_t)nbox * NP); add(16 * (size_t)nbox * NP);  // M, L
     add(16 * nt);                                   // near velocities
+    add(4 * (64 + 2 * ((size_t)1 << (2 * (c.L - c.kb)))));  // P2P work distribution
     add(4 * pf::scan_tmp_ints(nleaf));
     return need + 4096;
 }
@@ -1489,6 +1560,10 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     double2 *M = (double2 *)take(16 * (size_t)nbox * NP);
     double2 *Lc = (double2 *)take(16 * (size_t)nbox * NP);
     double2 *nearv = (double2 *)take(16 * nt);
+    // P2P work distribution: counters (64 words), heavy list, group counters
+    const int64_t nblk_w = (int64_t)1 << (2 * (L - kb));
+    const size_t p2pw_bytes = 4 * (64 + 2 * (size_t)nblk_w);
+    unsigned *p2pw_mem = (unsigned *)take(p2pw_bytes);
     int32_t *tmp = (int32_t *)take(4 * pf::scan_tmp_ints(nleaf));
     if (!tmp) {
         pf::set_error("pf_velocity_fmm: scratch layout error");
@@ -1565,9 +1640,18 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     // near field
     {
         const int64_t nblk = (int64_t)1 << (2 * (L - kb));
-        k_p2p<<<(unsigned)nblk, 32, 0, st>>>(
+        PF_CUDA_TRY(cudaMemsetAsync(p2pw_mem, 0, p2pw_bytes, st));
+        P2PWork work{p2pw_mem, (int32_t *)(p2pw_mem + 64), (int32_t *)(p2pw_mem + 64) + nblk};
+        const pfd::GaussParams gp = pfd::make_gauss_params(a.ksigmasqr);
+        k_p2p<false><<<(unsigned)nblk, 32, 0, st>>>(
             nblk, kb, tstart, T.cnt, S.start, S.cnt, S.hl, S.g32, T.hl, c.d_run_off, c.d_runs,
-            c.d_blk_order, pfd::make_gauss_params(a.ksigmasqr), nearv, ctr);
+            c.d_blk_order, gp, nearv, ctr, work);
+        PF_TRY(pf::launch_status("k_p2p"));
+        // the remaining groups of blocks with more than 96 targets (if any)
+        const int64_t grid = std::min<int64_t>((int64_t)p2p_sm_count() * P2P_MIN_CTAS, nt / 96 + 1);
+        k_p2p<true><<<(unsigned)grid, 32, 0, st>>>(
+            nblk, kb, tstart, T.cnt, S.start, S.cnt, S.hl, S.g32, T.hl, c.d_run_off, c.d_runs,
+            c.d_blk_order, gp, nearv, ctr, work);
         PF_TRY(pf::launch_status("k_p2p"));
     }
     PF_TRY(mark(5));

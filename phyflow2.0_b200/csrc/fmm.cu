@@ -40,6 +40,7 @@
 #include "fmm_plan.cuh"
 #include "gauss_pair.cuh"
 #include "scan.cuh"
+#include "segsort.cuh"
 
 #include "direct_api.cuh"
 
@@ -201,10 +202,14 @@ k_leaf_keys(const double *__restrict__ x, const double *__restrict__ y, int64_t 
 
 __global__ void __launch_bounds__(256)
 k_place(int64_t n, const uint32_t *__restrict__ key, const int32_t *__restrict__ rank,
-        const int32_t *__restrict__ start, int32_t *__restrict__ perm) {
+        const int32_t *__restrict__ start, int32_t *__restrict__ perm, int32_t *__restrict__ big,
+        int32_t *__restrict__ big_n) {
     const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (i >= n) return;
     perm[start[key[i]] + rank[i]] = (int32_t)i;
+    // a leaf of more than SEG_SMALL particles (exactly one has this rank) is
+    // listed for the segment sort
+    if (rank[i] == pf::SEG_SMALL) big[atomicAdd(big_n, 1)] = (int32_t)key[i];
 }
 
 __host__ __device__ __forceinline__ int64_t level_off(int l) {
@@ -219,7 +224,7 @@ k_leaf_sort(int64_t nleaf, const int32_t *__restrict__ start, const int32_t *__r
     const int64_t m = (int64_t)blockIdx.x * 128 + threadIdx.x;
     if (m >= nleaf) return;
     const int c = cnt[m];
-    if (c < 2) return;
+    if (c < 2 || c > pf::SEG_SMALL) return;  // larger leaves: seg_sort_listed
     const int s0 = start[m];
     for (int k = 1; k < c; ++k) {
         const int32_t v = perm[s0 + k];
@@ -1456,7 +1461,8 @@ struct Sorted {
 
 static pf_status sort_points(int64_t n, const double *x, const double *y,
                              const double *g, double x0, double y0, double wl, int L, Sorted &s,
-                             int32_t *scan_tmp, uint32_t *skey, cudaStream_t st) {
+                             int32_t *scan_tmp, uint32_t *skey, int32_t *big, int32_t *big_n,
+                             cudaStream_t st) {
     const int64_t nleaf = (int64_t)1 << (2 * L);
     PF_CUDA_TRY(cudaMemsetAsync(s.cnt, 0, sizeof(int32_t) * nleaf, st));
     if (n == 0) {
@@ -1467,10 +1473,14 @@ static pf_status sort_points(int64_t n, const double *x, const double *y,
     k_leaf_keys<<<gn, 256, 0, st>>>(x, y, n, x0, y0, wl, L, s.key, s.rank, s.cnt);
     PF_TRY(pf::launch_status("k_leaf_keys"));
     PF_TRY(pf::exclusive_scan_i32(s.cnt, s.start, nleaf, scan_tmp, nullptr, st));
-    k_place<<<gn, 256, 0, st>>>(n, s.key, s.rank, s.start, s.perm);
+    PF_CUDA_TRY(cudaMemsetAsync(big_n, 0, sizeof(int32_t), st));
+    k_place<<<gn, 256, 0, st>>>(n, s.key, s.rank, s.start, s.perm, big, big_n);
     PF_TRY(pf::launch_status("k_place"));
     k_leaf_sort<<<(unsigned)pf::ceil_div(nleaf, 128), 128, 0, st>>>(nleaf, s.start, s.cnt, s.perm);
     PF_TRY(pf::launch_status("k_leaf_sort"));
+    // leaves above SEG_SMALL particles (dense clusters); the ranks are free now
+    PF_TRY(pf::seg_sort_listed(big, big_n, s.start, s.cnt, s.perm, s.rank,
+                               n / (pf::SEG_SMALL + 1) + 1, st));
     k_gather_sorted<<<gn, 256, 0, st>>>(n, s.perm, x, y, g, s.key, s.x, s.y, s.g, s.hl, s.g32,
                                         skey);
     return pf::launch_status("k_gather_sorted");
@@ -1513,6 +1523,7 @@ static size_t fmm_scratch_bytes(const FmmCache &c, int64_t ns, int64_t nt, bool 
     add(4 * nleaf); add(4 * nleaf);                 // starts src, tgt
     add(16 * (size_t)nbox * NP); add(16 * (size_t)nbox * NP);  // M, L
     add(16 * nt);                                   // near velocities
+    add(4 * (std::max(ns, nt) / (pf::SEG_SMALL + 1) + 3));  // leaves for the segment sort
     add(4 * (64 + 2 * ((size_t)1 << (2 * (c.L - c.kb)))));  // P2P work distribution
     add(4 * pf::scan_tmp_ints(nleaf));
     return need + 4096;
@@ -1560,6 +1571,8 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     double2 *M = (double2 *)take(16 * (size_t)nbox * NP);
     double2 *Lc = (double2 *)take(16 * (size_t)nbox * NP);
     double2 *nearv = (double2 *)take(16 * nt);
+    // leaves listed for the segment sort: [0] count, [1 ..] leaf ids
+    int32_t *big = (int32_t *)take(4 * (std::max(ns, nt) / (pf::SEG_SMALL + 1) + 3));
     // P2P work distribution: counters (64 words), heavy list, group counters
     const int64_t nblk_w = (int64_t)1 << (2 * (L - kb));
     const size_t p2pw_bytes = 4 * (64 + 2 * (size_t)nblk_w);
@@ -1587,9 +1600,10 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     // sort sources (and targets)
     // sorted target keys come out of the sorted copies of the targets
     PF_TRY(sort_points(ns, a.x, a.y, a.g, x0, y0, wl, L, S, tmp, same ? tkey_sorted : nullptr,
-                       st));
+                       big + 1, big, st));
     if (!same)
-        PF_TRY(sort_points(nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, tkey_sorted, st));
+        PF_TRY(sort_points(nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, tkey_sorted, big + 1,
+                           big, st));
     PF_TRY(count_up(L, scnt_all, st));
     if (!same) PF_TRY(count_up(L, tcnt_all, st));
 

@@ -34,6 +34,7 @@
 
 #include "popctl.cuh"
 #include "scan.cuh"
+#include "segsort.cuh"
 
 namespace {
 
@@ -165,12 +166,16 @@ k_rm_count(const double *__restrict__ x, const double *__restrict__ y, int64_t n
 
 __global__ void __launch_bounds__(RM_THREADS)
 k_rm_place(int64_t n, const int32_t *__restrict__ cell, const int32_t *__restrict__ rank,
-           const int32_t *__restrict__ start, int32_t *__restrict__ perm) {
+           const int32_t *__restrict__ start, int32_t *__restrict__ perm, int32_t *__restrict__ big,
+           int32_t *__restrict__ big_n) {
     const int64_t i = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     if (i >= n) return;
     const int32_t c = cell[i];
     if (c < 0) return;
     perm[start[c] + rank[i]] = (int32_t)i;
+    // a cell of more than SEG_SMALL blobs (exactly one has this rank) is
+    // listed for the segment sort
+    if (rank[i] == pf::SEG_SMALL) big[atomicAdd(big_n, 1)] = c;
 }
 
 // M4' weight with the Wee term: branch structure of
@@ -283,7 +288,8 @@ k_rm_stencil(int64_t nbase, int64_t nby, int32_t ixmin, int32_t iymin,
     if (bc >= nbase) return;
     const int cnt = count[bc];
     const int s0 = start[bc];
-    sort_cell(perm, s0, cnt);  // this thread owns the cell's range
+    if (cnt <= pf::SEG_SMALL) sort_cell(perm, s0, cnt);  // this thread owns the cell's range
+                                                     // (larger cells: seg_sort_listed)
     const int64_t bx = bc / nby, by = bc - bx * nby;
     double p[16];
 #pragma unroll
@@ -372,6 +378,7 @@ size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby) {
     const int64_t nbase = nbx * nby, ncell = (nbx + 3) * (nby + 3);
     const int64_t big = ncell > nbase ? ncell : nbase;
     return align256(4 * n) * 3 + align256(8 * 16 * nbase) + 2 * align256(4 * nbase) +
+           align256(4 * (n / (SEG_SMALL + 1) + 3)) +
            align256(8 * ncell) + 2 * align256(4 * ncell) + align256(4 * scan_tmp_ints(big)) +
            3 * align256(16) + align256(sizeof(PcState)) + popctl_scratch_bytes() + 1024;
 }
@@ -390,6 +397,8 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     int32_t *rank = (int32_t *)sc.take(4 * n);
     int32_t *perm = (int32_t *)sc.take(4 * n);
     double *part = (double *)sc.take(8 * 16 * nbase);
+    // cells listed for the segment sort: [0] count, [1 ..] cell ids
+    int32_t *bigc = (int32_t *)sc.take(4 * (n / (SEG_SMALL + 1) + 3));
     int32_t *count = (int32_t *)sc.take(4 * nbase);
     int32_t *start = (int32_t *)sc.take(4 * nbase);
     double *acc = (double *)sc.take(8 * ncell);
@@ -408,8 +417,12 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
                                           cell, rank, count, bad);
     PF_TRY(launch_status("k_rm_count"));
     PF_TRY(exclusive_scan_i32(count, start, nbase, tmp, nvalid, st));
-    k_rm_place<<<gn, RM_THREADS, 0, st>>>(n, cell, rank, start, perm);
+    PF_CUDA_TRY(cudaMemsetAsync(bigc, 0, sizeof(int32_t), st));
+    k_rm_place<<<gn, RM_THREADS, 0, st>>>(n, cell, rank, start, perm, bigc + 1, bigc);
     PF_TRY(launch_status("k_rm_place"));
+    // cells above SEG_SMALL blobs (dense clusters); the ranks are free now
+    PF_TRY(seg_sort_listed(bigc + 1, bigc, start, count, perm, rank, n / (SEG_SMALL + 1) + 1,
+                           st));
     WParams wp{h, xb0, yb0, xb0 / h, yb0 / h, kernel == REMESH_TUTTY ? c : c * c};
     const unsigned gb = (unsigned)ceil_div(nbase, RM_THREADS);
     if (kernel == REMESH_TUTTY)

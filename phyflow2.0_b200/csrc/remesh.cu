@@ -287,9 +287,9 @@ k_rm_stencil(int64_t nbase, int64_t nby, int32_t ixmin, int32_t iymin,
     const int64_t bc = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     if (bc >= nbase) return;
     const int cnt = count[bc];
+    if (cnt > pf::SEG_SMALL) return;  // larger cells: k_rm_stencil_big
     const int s0 = start[bc];
-    if (cnt <= pf::SEG_SMALL) sort_cell(perm, s0, cnt);  // this thread owns the cell's range
-                                                     // (larger cells: seg_sort_listed)
+    sort_cell(perm, s0, cnt);  // this thread owns the cell's range
     const int64_t bx = bc / nby, by = bc - bx * nby;
     double p[16];
 #pragma unroll
@@ -303,6 +303,48 @@ k_rm_stencil(int64_t nbase, int64_t nby, int32_t ixmin, int32_t iymin,
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k) part[k * nbase + bc] = p[k];
+}
+
+// The stencil of each listed cell of more than SEG_SMALL blobs (sorted by
+// seg_sort_listed), one CTA per cell: thread t sums the blobs t, t + RM_THREADS,
+// ... of the cell (in cell order), then the CTA adds the threads' partial sums
+// in a fixed tree order.
+template <bool TUTTY>
+__global__ void __launch_bounds__(RM_THREADS)
+k_rm_stencil_big(const int32_t *__restrict__ list, const int32_t *__restrict__ list_n,
+                 int64_t nbase, int64_t nby, int32_t ixmin, int32_t iymin,
+                 const int32_t *__restrict__ start, const int32_t *__restrict__ count,
+                 const int32_t *__restrict__ perm, const double *__restrict__ x,
+                 const double *__restrict__ y, const double *__restrict__ g, WParams wp,
+                 double *__restrict__ part) {
+    __shared__ double s_p[16][RM_THREADS];
+    const int nlist = *list_n;
+    for (int k = blockIdx.x; k < nlist; k += gridDim.x) {
+        const int64_t bc = list[k];
+        const int cnt = count[bc], s0 = start[bc];
+        const int64_t bx = bc / nby, by = bc - bx * nby;
+        double p[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) p[q] = 0.0;
+        for (int j = threadIdx.x; j < cnt; j += RM_THREADS) {
+            const W9 r = blob_w9<TUTTY>(perm[s0 + j], bx, by, ixmin, iymin, x, y, g, wp);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) p[a * 4 + b] += (r.wx[a] * r.wy[b]) * r.g;
+        }
+#pragma unroll
+        for (int q = 0; q < 16; ++q) s_p[q][threadIdx.x] = p[q];
+        __syncthreads();
+        for (int w = RM_THREADS / 2; w > 0; w >>= 1) {
+            if ((int)threadIdx.x < w)
+#pragma unroll
+                for (int q = 0; q < 16; ++q) s_p[q][threadIdx.x] += s_p[q][threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x < 16) part[threadIdx.x * nbase + bc] = s_p[threadIdx.x][0];
+        __syncthreads();
+    }
 }
 
 // Output cell grid: ox in [0, nbx+3), oy in [0, nby+3), cid = ox*(nby+3) + oy;
@@ -432,6 +474,17 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
         k_rm_stencil<false><<<gb, RM_THREADS, 0, st>>>(nbase, nby, ixmin, iymin, start, count,
                                                         perm, x, y, g, wp, part);
     PF_TRY(launch_status("k_rm_stencil"));
+    {
+        // a few CTAs suffice (such cells are rare); each loops over the list
+        const unsigned gbig = (unsigned)std::min<int64_t>(n / (SEG_SMALL + 1) + 1, 64);
+        if (kernel == REMESH_TUTTY)
+            k_rm_stencil_big<true><<<gbig, RM_THREADS, 0, st>>>(
+                bigc + 1, bigc, nbase, nby, ixmin, iymin, start, count, perm, x, y, g, wp, part);
+        else
+            k_rm_stencil_big<false><<<gbig, RM_THREADS, 0, st>>>(
+                bigc + 1, bigc, nbase, nby, ixmin, iymin, start, count, perm, x, y, g, wp, part);
+        PF_TRY(launch_status("k_rm_stencil_big"));
+    }
     k_rm_sum<<<(unsigned)ceil_div(ncell, RM_THREADS), RM_THREADS, 0, st>>>(nbx, nby, count, part,
                                                                            acc, flag);
     PF_TRY(launch_status("k_rm_sum"));

@@ -95,7 +95,8 @@ pf_status seg_sort_listed(const int32_t *list, const int32_t *list_n, const int3
                           const int32_t *cnt, int32_t *vals, int32_t *tmp, int64_t max_segments,
                           cudaStream_t st) {
     if (max_segments <= 0) return PF_OK;
-    const unsigned grid = (unsigned)std::min<int64_t>(max_segments, 296);
+    // a few CTAs suffice (large segments are rare); each loops over the list
+    const unsigned grid = (unsigned)std::min<int64_t>(max_segments, 64);
     k_seg_sort<<<grid, SEG_THREADS, 0, st>>>(list, list_n, start, cnt, vals, tmp);
     return launch_status("k_seg_sort");
 }

@@ -375,7 +375,8 @@ def run_reference(args):
     return {
         "impl": "reference",
         "metric": "blob velocity evals/s at <=1e-6 rel err vs FP64 (velocity + M4' remesh step)",
-        "value": value, "unit": "evals/s", "n_gpus": 0, "steps": args.steps,
+        "value": value, "unit": "evals/s", "n_gpus": args.gpus, "device": "host cores",
+        "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": n / value * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"single large instance: N={n} blobs U[0,1)^2, sigma=0.002, "

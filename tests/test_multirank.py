@@ -38,3 +38,27 @@ def test_reference_arm_other_ranks_exit_without_work():
                         "--steps", "1", "--warmup", "0"], env=env, capture_output=True,
                        text=True, timeout=60)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_reference_arm_line_on_rank0():
+    """Rank 0 prints one JSON line with the contract's keys; its metric and
+    config workload are those of the GPU arm's line."""
+    import json
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--steps", "1", "--warmup", "0"], env=env, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+              "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+              "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["unit"] == "evals/s" and d["higher_is_better"]
+    assert d["value"] > 0 and d["cpu_baseline"]["value"] == d["value"]
+    assert d["cpu_baseline"]["kind"] in ("reference", "port")
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert d["config"]["n_blobs"] == 1 << 20
+    assert "velocity at all blobs" in d["config"]["workload"]

@@ -29,6 +29,7 @@
 // are contiguous in the sorted particle arrays, and streamed through shared
 // memory in full tiles.  The interaction lists come from fmm_plan.cu.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -1217,18 +1218,19 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
     }
 }
 
-// SMs of the current device (cached per device).
+// SMs of the current device (cached per device; host threads may race to
+// fill an entry, all with the same value).
 static int p2p_sm_count() {
-    static int cached[64] = {0};
+    static std::atomic<int> cached[64];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-    if (cached[dev] == 0) {
-        int v = 0;
+    int v = cached[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
         if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
             v = 148;
-        cached[dev] = v;
+        cached[dev].store(v, std::memory_order_relaxed);
     }
-    return cached[dev];
+    return v;
 }
 
 // L2P + near + scatter to input order: one thread per sorted target

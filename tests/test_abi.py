@@ -58,3 +58,28 @@ def test_null_context_is_rejected_without_gpu():
     s = L.lib.pf_velocity_direct(None, 10, None, None, None, 10, None, None, 1.0, None, None, None)
     assert s == 1
     assert b"NULL context" in L.lib.pf_last_error()
+
+
+NO_STATUS = {"pf_last_error", "pf_version", "pf_kernel_launches"}
+NULL_IS_NOOP = {"pf_destroy", "pf_batch_destroy"}  # like free(NULL)
+ZEROS_VALID = {"pf_fmm_set_tuning"}  # 0 = automatic choice of every knob
+
+
+def test_every_entry_point_rejects_null_arguments_without_gpu():
+    """NULL handles and arrays with zero sizes and parameters: every entry
+    point returns PF_ERR_INVALID_ARG with a message naming it, never crashes
+    and never reaches the device."""
+    import pfblob._lib as L
+    for name, argtypes in L.PROTOTYPES.items():
+        if name in NO_STATUS:
+            continue
+        args = [0.0 if t is ctypes.c_double else
+                0 if t in (ctypes.c_int, ctypes.c_int32, ctypes.c_int64) else None
+                for t in argtypes]
+        s = getattr(L.lib, name)(*args)
+        if name in NULL_IS_NOOP or name in ZEROS_VALID:
+            assert s == 0, name
+            continue
+        assert s == 1, (name, s)
+        msg = L.lib.pf_last_error().decode()
+        assert msg.startswith(name.replace("_tutty", "")), (name, msg)

@@ -1,6 +1,7 @@
-"""Serving loop: trace generation and summaries (CPU), and on the GPU:
-results are the same alone and in the mix, admission follows free HBM, a
-simulated out-of-memory device makes requests wait and the loop report it."""
+"""Serving loop: trace generation, summaries and the admission policy (CPU),
+and on the GPU: results are the same alone and in the mix, admission follows
+free HBM, a simulated out-of-memory device makes requests wait and the loop
+report it."""
 import numpy as np
 import pytest
 import torch
@@ -15,6 +16,61 @@ def test_poisson_trace_and_summary_cpu():
     reqs = [Request(sim=0, t_arrival=0.0, t_done=0.001 * (i + 1), n=100) for i in range(100)]
     s = summarize(reqs, t_span=1.0)
     assert abs(s["p50_ms"] - 50.5) < 1e-9 and s["evals_per_s"] == 10000
+
+
+def _admission_only_server(n_slots, free, reserve, needs):
+    """A Server with its admission state and no device or worker threads: the
+    policy of _try_admit on the host, with a fake free-HBM reading."""
+    import queue
+    from pfblob.serve import Server
+    s = Server.__new__(Server)
+    s.n_slots = n_slots
+    s._slot_free = [True] * n_slots
+    s._slot_bytes = [0] * n_slots
+    s._claimed = 0
+    s._queues = [queue.Queue() for _ in range(n_slots)]
+    s.reserve = reserve
+    s.free_hbm = lambda: free[0]
+    s.need_bytes = lambda sim: needs[sim]
+    return s
+
+
+def test_admission_policy_cpu():
+    from pfblob.serve import Request
+    GB = 1 << 30
+    free = [10 * GB]
+    s = _admission_only_server(2, free, reserve=2 * GB, needs={0: 3 * GB, 1: 6 * GB, 2: 1 * GB})
+    a = Request(sim=0, t_arrival=0.0)
+    assert s._try_admit(a) and a.claim == 3 * GB and s._claimed == 3 * GB
+    # 6 GB more would exceed free - reserve - claimed = 5 GB: waits
+    b = Request(sim=1, t_arrival=0.0)
+    assert not s._try_admit(b) and b.slot == -1
+    # a request that fits in the remaining room is admitted to the other slot
+    c = Request(sim=2, t_arrival=0.0)
+    assert s._try_admit(c) and c.slot != a.slot and c.claim == 1 * GB
+    # no free slot: waits whatever the memory
+    assert not s._try_admit(Request(sim=2, t_arrival=0.0))
+    # slot of `a` done (its growth now allocated, so no longer claimed); a
+    # request that fits the 3 GB arena of that slot needs no growth
+    s._slot_free[a.slot] = True
+    s._claimed -= a.claim
+    free[0] = 7 * GB
+    d = Request(sim=0, t_arrival=0.0)
+    assert s._try_admit(d) and d.slot == a.slot and d.claim == 0
+    assert s._queues[a.slot].qsize() == 2 and s._queues[c.slot].qsize() == 1
+
+
+def test_admission_prefers_the_slot_that_already_fits_cpu():
+    from pfblob.serve import Request
+    GB = 1 << 30
+    s = _admission_only_server(3, [100 * GB], reserve=0, needs={0: 4 * GB})
+    s._slot_bytes = [1 * GB, 5 * GB, 2 * GB]
+    r = Request(sim=0, t_arrival=0.0)
+    assert s._try_admit(r) and r.slot == 1 and r.claim == 0
+    # slot 1 is busy now: no free slot fits, so the largest free arena grows
+    # (the least growth)
+    r2 = Request(sim=0, t_arrival=0.0)
+    assert s._try_admit(r2) and r2.slot == 2 and r2.claim == 2 * GB
 
 
 def _sims(sizes, config=5):

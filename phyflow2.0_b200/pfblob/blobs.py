@@ -27,6 +27,14 @@ default_blob_control_params = {'stepRedistribution': 1, 'stepPopulationControl':
 default_velocity_computation_params = {'method': 'fmm', 'hardware': 'gpu'}
 
 
+def _round_half_away(r):
+    """Nearest integer to r >= 0, halves away from zero: the rounding of the
+    reference's Python-2 ``round`` (Python 3's rounds halves to even, so a
+    ratio of exactly 2.5 would give 2 instead of the reference's 3)."""
+    q = math.floor(r)
+    return int(q) + (1 if r - q >= 0.5 else 0)
+
+
 class Blobs:
     def __init__(self, wField, vInf, nu, deltaTc, h, overlap,
                  timeIntegrationParams=default_time_integration_params,
@@ -99,7 +107,7 @@ class Blobs:
         deltaTd = ((1.0 / 3.0) * self.h * self.h) / self.nu if c2 == 'optimized' else \
             (float(c2) * self.h * self.h) / self.nu
         if deltaTd >= self.deltaTc:
-            step = int(round(deltaTd / self.deltaTc))
+            step = _round_half_away(deltaTd / self.deltaTc)
             return step * self.deltaTc, step
         raise ValueError('Regrid Wee: deltaTc is too large. Reduce deltaTc to a value smaller '
                          'than %f.' % deltaTd)

@@ -1,0 +1,54 @@
+"""Host logic of the Blobs class (no GPU): the diffusion time step and its
+multiple of the convection step (src/python/blobs/__blobsClass.py:2248-2318),
+with the reference's Python-2 rounding of halves."""
+import pytest
+
+
+def _blobs(method, nu, h, deltaTc, c2="optimized"):
+    from pfblob.blobs import Blobs
+    b = Blobs.__new__(Blobs)
+    b.nu, b.h, b.deltaTc = float(nu), float(h), float(deltaTc)
+    b.diffusionParams = {"method": method, "c2": c2}
+    return b
+
+
+def test_wee_optimized_step_is_rounded_to_a_multiple_of_deltaTc():
+    # ideal deltaTd = h^2 / (3 nu) = 1/3 * 1e-4 / 1e-3 = 0.0333..; / 0.01 = 3.33 -> 3 steps
+    b = _blobs("regrid_wee", nu=1e-3, h=0.01, deltaTc=0.01)
+    dtd, step = b._compute_deltaTd()
+    assert step == 3 and dtd == 3 * 0.01
+
+
+def test_wee_half_way_ratio_rounds_up_like_the_reference():
+    # ideal deltaTd = c2 h^2 / nu = 0.625; deltaTc = 0.25: ratio exactly 2.5.
+    # The reference's Python-2 round gives 3 (Python 3's round would give 2).
+    b = _blobs("regrid_wee", nu=1.0, h=1.0, deltaTc=0.25, c2=0.625)
+    dtd, step = b._compute_deltaTd()
+    assert step == 3 and dtd == 0.75
+    b = _blobs("regrid_wee", nu=1.0, h=1.0, deltaTc=0.25, c2=0.875)  # ratio 3.5 -> 4
+    assert b._compute_deltaTd() == (1.0, 4)
+
+
+def test_wee_step_too_large_raises():
+    b = _blobs("regrid_wee", nu=1.0, h=0.01, deltaTc=1.0)
+    with pytest.raises(ValueError, match="Regrid Wee"):
+        b._compute_deltaTd()
+
+
+def test_inviscid_has_no_diffusion():
+    for m in ("regrid_wee", "regrid_tutty"):
+        assert _blobs(m, nu=0.0, h=0.01, deltaTc=0.1)._compute_deltaTd() == (0.0, 0)
+
+
+def test_tutty_diffuses_every_step_within_its_stability_limit():
+    b = _blobs("regrid_tutty", nu=1e-3, h=0.01, deltaTc=0.01)  # hNu/h = 0.316
+    assert b._compute_deltaTd() == (0.01, 1)
+    b = _blobs("regrid_tutty", nu=1e-3, h=0.01, deltaTc=0.06)  # hNu/h = 0.775 > 1/sqrt(2)
+    with pytest.raises(ValueError, match="Regrid Tutty"):
+        b._compute_deltaTd()
+
+
+def test_round_half_away():
+    from pfblob.blobs import _round_half_away
+    assert [_round_half_away(v) for v in (1.0, 1.49999, 1.5, 2.5, 2.5000001, 7.0)] == \
+        [1, 1, 2, 3, 3, 7]

@@ -631,6 +631,8 @@ extern "C" pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, c
     PF_CHECK_ARG(ctx != nullptr, "pf_remesh_window: NULL context");
     PF_CHECK_ARG(n >= 0 && n < ((int64_t)1 << 31), "pf_remesh_window: bad n");
     PF_CHECK_ARG(std::isfinite(h) && h > 0.0, "pf_remesh_window: bad h");
+    PF_CHECK_ARG(std::isfinite(xb0) && std::isfinite(yb0) && std::isfinite(c),
+                 "pf_remesh_window: bounds and c must be finite");
     PF_CHECK_ARG(nbx > 0 && nby > 0 && (nbx + 3) * (nby + 3) < ((int64_t)1 << 31),
                  "pf_remesh_window: bad window %lld x %lld", (long long)nbx, (long long)nby);
     PF_CHECK_ARG(ixmin > -((int64_t)1 << 30) && iymin > -((int64_t)1 << 30) &&

@@ -12,6 +12,7 @@
 //
 // The same kernels as pf_remesh_window run on that buffer, so results are the
 // same as pf_remesh_window's for the same window.
+#include <cmath>
 #include <mutex>
 
 #include "popctl.cuh"
@@ -70,6 +71,8 @@ extern "C" pf_status pf_remesh_window_noalloc(int64_t n, const double *x, const 
     pf::clear_error();
     PF_CHECK_ARG(n >= 0 && n < ((int64_t)1 << 31), "pf_remesh_window_noalloc: bad n");
     PF_CHECK_ARG(h > 0.0 && h < 1e300, "pf_remesh_window_noalloc: h must be positive and finite");
+    PF_CHECK_ARG(std::isfinite(xb0) && std::isfinite(yb0) && std::isfinite(c),
+                 "pf_remesh_window_noalloc: bounds and c must be finite");
     PF_CHECK_ARG(nbx > 0 && nby > 0 && nbx < ((int64_t)1 << 30) && nby < ((int64_t)1 << 30),
                  "pf_remesh_window_noalloc: bad window %lld x %lld", (long long)nbx,
                  (long long)nby);

@@ -83,3 +83,22 @@ def test_every_entry_point_rejects_null_arguments_without_gpu():
         assert s == 1, (name, s)
         msg = L.lib.pf_last_error().decode()
         assert msg.startswith(name.replace("_tutty", "")), (name, msg)
+
+
+@pytest.mark.parametrize("bad", ["xb0", "yb0", "c"])
+def test_window_remeshes_reject_non_finite_bounds_without_gpu(bad):
+    """The window remeshes check their scalar arguments before any device
+    work: a NaN or infinite bound or Wee coefficient is an invalid argument."""
+    import pfblob._lib as L
+    vals = {"xb0": 0.0, "yb0": 0.0, "c": 0.0}
+    for v in (float("nan"), float("inf")):
+        vals[bad] = v
+        dummy = ctypes.c_void_p(16)  # never dereferenced: the checks fail first
+        s = L.lib.pf_remesh_window_noalloc(0, None, None, None, 0.01, vals["xb0"], vals["yb0"],
+                                           vals["c"], 0, 0, 1, 1, 0, None, None, None, None,
+                                           None, dummy, None, None)
+        assert s == 1 and b"finite" in L.lib.pf_last_error()
+        s = L.lib.pf_remesh_window(dummy, 0, None, None, None, 0.01, vals["xb0"], vals["yb0"],
+                                   vals["c"], 0, 0, 1, 1, 0, None, None, None, None, None, dummy,
+                                   None, None)
+        assert s == 1 and b"finite" in L.lib.pf_last_error()

@@ -302,6 +302,11 @@ extern "C" pf_status pf_batch_create(pf_ctx *ctx, int32_t n, const pf_batch_inst
         PF_CHECK_ARG(d.n >= 0 && d.n < ((int64_t)1 << 31), "instance %d: bad n", i);
         PF_CHECK_ARG(d.n == 0 || (d.x && d.y && d.g && d.vx && d.vy), "instance %d: NULL array", i);
         PF_CHECK_ARG(d.ksigmasqr > 0.0 && std::isfinite(d.ksigmasqr), "instance %d: bad ksigmasqr", i);
+        PF_CHECK_ARG(d.cutoff >= 0.0 && std::isfinite(d.cutoff), "instance %d: bad cutoff", i);
+        PF_CHECK_ARG(d.expansion_terms == 0 || d.expansion_terms == 16 || d.expansion_terms == 20 ||
+                         d.expansion_terms == 24 || d.expansion_terms == 28 ||
+                         d.expansion_terms == 32,
+                     "instance %d: expansion terms must be 0 (from tol) or one of 16,20,24,28,32", i);
         PF_CHECK_ARG(std::isfinite(d.box[0]) && std::isfinite(d.box[1]) && std::isfinite(d.box[2]) &&
                          std::isfinite(d.box[3]) && d.box[1] >= d.box[0] && d.box[3] >= d.box[2],
                      "instance %d: bad box", i);
@@ -309,7 +314,8 @@ extern "C" pf_status pf_batch_create(pf_ctx *ctx, int32_t n, const pf_batch_inst
                      "instance %d: method must be PF_FMM_METHOD or PF_DIRECT_METHOD", i);
         PF_CHECK_ARG(d.leaf_level == 0 || (d.leaf_level >= 3 && d.leaf_level <= pf::fmmx::MAX_LEVEL),
                      "instance %d: leaf level", i);
-        PF_CHECK_ARG(!d.remesh || (d.h > 0.0 && d.capacity >= 0 &&
+        PF_CHECK_ARG(!d.remesh || (d.h > 0.0 && std::isfinite(d.h) && std::isfinite(d.xb0) &&
+                                   std::isfinite(d.yb0) && std::isfinite(d.c) && d.capacity >= 0 &&
                                    (d.capacity == 0 || (d.x_out && d.y_out && d.g_out))),
                      "instance %d: bad remesh arguments", i);
     }

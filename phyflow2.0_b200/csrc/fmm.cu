@@ -1711,7 +1711,12 @@ pf_status fmm_exec(const FmmCache &c, double x0, double y0, double w0, Bump &sc,
         case 20: return exec_fmm<20>(sc, a, c, x0, y0, w0, ctr, ev, st);
         case 24: return exec_fmm<24>(sc, a, c, x0, y0, w0, ctr, ev, st);
         case 28: return exec_fmm<28>(sc, a, c, x0, y0, w0, ctr, ev, st);
-        default: return exec_fmm<32>(sc, a, c, x0, y0, w0, ctr, ev, st);
+        case 32: return exec_fmm<32>(sc, a, c, x0, y0, w0, ctr, ev, st);
+        default:
+            // the plan's coefficient arrays are sized for c.np: never run another size on them
+            set_error("FMM: %d expansion terms is not an instantiated size (16, 20, 24, 28, 32)",
+                      c.np);
+            return PF_ERR_INVALID_ARG;
     }
 }
 

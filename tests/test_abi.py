@@ -102,3 +102,50 @@ def test_window_remeshes_reject_non_finite_bounds_without_gpu(bad):
                                    vals["c"], 0, 0, 1, 1, 0, None, None, None, None, None, dummy,
                                    None, None)
         assert s == 1 and b"finite" in L.lib.pf_last_error()
+
+
+def _batch_instance(**kw):
+    import pfblob._lib as L
+    d = L.BatchInstance()
+    d.n = 0
+    d.ksigmasqr = 8e-6
+    d.cutoff = 0.01
+    for i, v in enumerate((0.0, 1.0, 0.0, 1.0)):
+        d.box[i] = v
+    d.method = 0
+    d.h = 0.0016
+    for k, v in kw.items():
+        setattr(d, k, v)
+    return d
+
+
+@pytest.mark.parametrize("field,value,words", [
+    ("expansion_terms", 17, "expansion terms"),
+    ("expansion_terms", 64, "expansion terms"),
+    ("cutoff", float("nan"), "bad cutoff"),
+    ("cutoff", -1.0, "bad cutoff"),
+    ("ksigmasqr", 0.0, "bad ksigmasqr"),
+    ("method", 7, "method"),
+    ("leaf_level", 2, "leaf level"),
+])
+def test_batch_rejects_bad_instances_without_gpu(field, value, words):
+    """pf_batch_create checks every instance before it touches the device
+    (the FMM's coefficient arrays are sized by the expansion terms, so an
+    uninstantiated size must never reach the kernels)."""
+    import pfblob._lib as L
+    dummy_ctx = ctypes.c_void_p(16)  # never dereferenced: the checks fail first
+    inst = (L.BatchInstance * 1)(_batch_instance(**{field: value}))
+    out = ctypes.c_void_p()
+    s = L.lib.pf_batch_create(dummy_ctx, 1, inst, 1e-6, 1, ctypes.byref(out))
+    assert s == 1 and out.value is None
+    assert words in L.lib.pf_last_error().decode()
+
+
+@pytest.mark.parametrize("field", ["h", "xb0", "yb0", "c"])
+def test_batch_rejects_non_finite_remesh_arguments_without_gpu(field):
+    import pfblob._lib as L
+    dummy_ctx = ctypes.c_void_p(16)
+    inst = (L.BatchInstance * 1)(_batch_instance(remesh=1, **{field: float("inf")}))
+    out = ctypes.c_void_p()
+    assert L.lib.pf_batch_create(dummy_ctx, 1, inst, 1e-6, 1, ctypes.byref(out)) == 1
+    assert "bad remesh arguments" in L.lib.pf_last_error().decode()

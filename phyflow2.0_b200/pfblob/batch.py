@@ -13,6 +13,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._arrays import require
 from .induced import default_cutoff
 from .tune import Tuner
 
@@ -37,6 +38,7 @@ class Batch:
         for i, s in enumerate(sims):
             x, y, g = s["x"], s["y"], s["g"]
             n = x.numel()
+            require(n, self.device, x=x, y=y, g=g)
             sigma = float(s["sigma"])
             k = float(s.get("k", 2.0))
             overlap = float(s.get("overlap", 0.8))

@@ -147,8 +147,8 @@ class Blobs:
             xt, yt, host = self._x, self._y, True
         else:
             host = not isinstance(xEval, torch.Tensor)
-            xt = xEval.to(self.device, torch.float64) if not host else self._dev(xEval)
-            yt = yEval.to(self.device, torch.float64) if not host else self._dev(yEval)
+            xt = xEval.to(self.device, torch.float64).contiguous() if not host else self._dev(xEval)
+            yt = yEval.to(self.device, torch.float64).contiguous() if not host else self._dev(yEval)
         vx, vy = self._velocity_at(self._x, self._y, xt, yt, Ndirect, tol, cutoff)
         return (vx.cpu().numpy(), vy.cpu().numpy()) if host else (vx, vy)
 

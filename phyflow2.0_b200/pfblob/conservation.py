@@ -4,14 +4,16 @@ import ctypes
 import torch
 
 from . import _lib
-from ._arrays import ptr
+from ._arrays import ptr, require
 
 
 def moments_device(x, y, g, out=None, stream=None):
     """Device tensor [sum g, sum g x, sum g y, sum |g|] (fixed reduction order)."""
     dev = x.device
+    require(x.numel(), dev, x=x, y=y, g=g)
     if out is None:
         out = torch.empty(4, dtype=torch.float64, device=dev)
+    require(4, dev, out=out)
     st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
     _lib.check(_lib.lib.pf_moments(_lib.context(dev.index), x.numel(), ptr(x), ptr(y), ptr(g),
                                    ptr(out), st))

@@ -18,7 +18,7 @@ import math
 import torch
 
 from . import _lib
-from ._arrays import Marshal, ptr
+from ._arrays import Marshal, ptr, require
 
 GAUSS_KERNEL = 1
 CUTOFF_KERNEL = 0
@@ -59,7 +59,11 @@ def velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=DIRECT_METHOD, xo
     """Device-tensor entry: all arguments CUDA float64 tensors; writes vx, vy.
     ``box = (xmin, xmax, ymin, ymax)`` containing all sources and targets lets
     the FMM skip its bounding-box read-back (pf_velocity_fmm_box)."""
-    dev = x.device.index if device is None else device
+    require(x.numel(), x.device, x=x, y=y, g=g)
+    require(xt.numel(), x.device, xt=xt, yt=yt, vx=vx, vy=vy)
+    if device is not None and device != x.device.index:
+        raise ValueError(f"pfblob: device {device} given for tensors on {x.device}")
+    dev = x.device.index
     st = ctypes.c_void_p(torch.cuda.current_stream(x.device).cuda_stream if stream is None
                          else stream)
     ctx = _lib.context(dev)
@@ -132,6 +136,8 @@ def vorticity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None,
         xt, yt = x, y
     else:
         xt, yt = m.dev(xEval), m.dev(yEval)
+    require(x.numel(), m.device, xBlob=x, yBlob=y, wBlob=g)
+    require(xt.numel(), m.device, xEval=xt, yEval=yt)
     w = m.empty(xt.numel())
     ctx = _lib.context(m.index)
     _lib.check(_lib.lib.pf_vorticity_direct(ctx, x.numel(), ptr(x), ptr(y), ptr(g), xt.numel(),

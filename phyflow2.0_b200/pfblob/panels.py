@@ -10,7 +10,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._arrays import Marshal, ptr
+from ._arrays import Marshal, ptr, require
 
 CPU_HARDWARE = 0
 GPU_HARDWARE = 1
@@ -22,6 +22,8 @@ PANEL_KERNEL_CSV = 1  # constant-strength vortex
 def panel_velocity_device(gamma, xs, ys, xe, ye, cosa, sina, xv, yv, vx, vy, accumulate=False,
                           stream=None):
     dev = xv.device
+    require(gamma.numel(), dev, gamma=gamma, xs=xs, ys=ys, xe=xe, ye=ye, cosa=cosa, sina=sina)
+    require(xv.numel(), dev, xv=xv, yv=yv, vx=vx, vy=vy)
     st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
     _lib.check(_lib.lib.pf_panel_velocity(_lib.context(dev.index), gamma.numel(), ptr(gamma),
                                           ptr(xs), ptr(ys), ptr(xe), ptr(ye), ptr(cosa), ptr(sina),
@@ -62,6 +64,8 @@ def influenceMatrix(xCP, yCP, xPanelStart, yPanelStart, xPanelEnd, yPanelEnd, co
     arrs = [m.dev(a) for a in (xCP, yCP, xPanelStart, yPanelStart, xPanelEnd, yPanelEnd,
                                cosAlpha, sinAlpha)]
     n = arrs[0].numel()
+    require(n, m.device, **dict(zip(("xCP", "yCP", "xPanelStart", "yPanelStart", "xPanelEnd",
+                                     "yPanelEnd", "cosAlpha", "sinAlpha"), arrs)))
     A = torch.empty((n, n), dtype=torch.float64, device=m.device)
     _lib.check(_lib.lib.pf_panel_influence_matrix(_lib.context(m.index), n,
                                                   *[ptr(a) for a in arrs], ptr(A), m.stream))
@@ -100,6 +104,8 @@ def lu_solve(lu_and_piv, b):
         torch.from_numpy(np.ascontiguousarray(piv, dtype=np.int32)).to(m.device)
     x = m.dev(b).clone()
     n = x.numel()
+    require(n * n, m.device, lu=LU)
+    require(n, m.device, dtype=torch.int32, piv=P)
     _lib.check(_lib.lib.pf_dense_lu_solve(_lib.context(m.index), n, ptr(LU), ptr(P), ptr(x),
                                           m.stream))
     return m.outs(x)[0]

@@ -7,7 +7,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._arrays import Marshal, ptr
+from ._arrays import Marshal, ptr, require
 
 M4PRIME_INTERPKERNEL = 0
 
@@ -24,6 +24,7 @@ def remesh_device(x, y, g, h, xb0, yb0, c=0.0, capacity=None, with_indices=False
     M4' (``c`` is then unused)."""
     n = x.numel()
     dev = x.device
+    require(n, dev, x=x, y=y, g=g)
     st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
     ctx = _lib.context(dev.index)
     if capacity is None:
@@ -87,6 +88,7 @@ def remesh_window_device(x, y, g, h, xb0, yb0, window, c=0.0, stream=None):
     with the number of new blobs (the first n_out entries)."""
     n = x.numel()
     dev = x.device
+    require(n, dev, x=x, y=y, g=g)
     st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
     ctx = _lib.context(dev.index)
     ixmin, iymin, nbx, nby = (int(v) for v in window)
@@ -108,6 +110,7 @@ def population_control_device(x, y, g, g_threshold_local, g_threshold_global, st
     synchronisation)."""
     n = x.numel()
     dev = x.device
+    require(n, dev, x=x, y=y, g=g)
     st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
     ctx = _lib.context(dev.index)
     xo = torch.empty(n, dtype=torch.float64, device=dev)

@@ -80,13 +80,17 @@ class Blobs:
         return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(self.device)
 
     def _blobs_from_function(self, wField, h):
-        """(wExactFunction, xBounds, yBounds): blobs on the lattice of spacing h
-        containing (0, 0), inside the bounds, circulation w(x, y) h^2."""
+        """(wExactFunction, xBounds, yBounds): floor(width / h) blobs per
+        direction at the cell centres xBounds[0] + h/2 + i h, x varying
+        fastest, circulation w(x, y) h^2 -- the reference's
+        ``__read_input_wField_function`` (``__blobsClass.py:1406-1419``)."""
         f, xb, yb = wField
-        ix = np.arange(math.ceil(xb[0] / h), math.floor(xb[1] / h) + 1)
-        iy = np.arange(math.ceil(yb[0] / h), math.floor(yb[1] / h) + 1)
-        X, Y = np.meshgrid(ix * h, iy * h, indexing="ij")
-        x, y = X.ravel(), Y.ravel()
+        nx = int(np.floor((xb[1] - xb[0]) / h))
+        ny = int(np.floor((yb[1] - yb[0]) / h))
+        xs = xb[0] + 0.5 * h + np.arange(0, nx) * h
+        ys = yb[0] + 0.5 * h + np.arange(0, ny) * h
+        X, Y = np.meshgrid(xs, ys)
+        x, y = X.flatten(), Y.flatten()
         return x, y, f(x, y) * h * h
 
     def _compute_deltaTd(self):

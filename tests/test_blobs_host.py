@@ -52,3 +52,16 @@ def test_round_half_away():
     from pfblob.blobs import _round_half_away
     assert [_round_half_away(v) for v in (1.0, 1.49999, 1.5, 2.5, 2.5000001, 7.0)] == \
         [1, 1, 2, 3, 3, 7]
+
+
+def test_blobs_from_a_vorticity_function_sit_at_cell_centres():
+    """wField = (w, xBounds, yBounds): floor(width / h) blobs per direction at
+    xBounds[0] + h/2 + i h, x varying fastest, circulation w h^2
+    (__blobsClass.py:1406-1419)."""
+    import numpy as np
+    from pfblob.blobs import Blobs
+    b = Blobs.__new__(Blobs)
+    x, y, g = b._blobs_from_function((lambda x, y: x + 10.0 * y, [-1.0, 1.0], [0.0, 1.2]), 0.5)
+    assert np.array_equal(x, [-0.75, -0.25, 0.25, 0.75] * 2)
+    assert np.array_equal(y, [0.25] * 4 + [0.75] * 4)
+    assert np.array_equal(g, (x + 10.0 * y) * 0.25)

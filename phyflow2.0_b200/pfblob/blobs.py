@@ -212,7 +212,7 @@ class Blobs:
         elif redistribute:
             self.redistribute()
         self.tStep += 1
-        self.t += self.deltaTc
+        self.t = self.deltaTc * self.tStep  # as the reference's _advanceTime, not a running sum
         if control and not fused:
             self.populationControl()
 
@@ -222,10 +222,26 @@ class Blobs:
         self._g = torch.cat([self._g, self._dev(gNew)])
 
     def removeBlobs(self, iBlobs):
-        iBlobs = np.asarray(iBlobs)
-        keep = np.ones(self.numBlobs, dtype=bool)
-        keep[iBlobs] = False
-        k = torch.from_numpy(keep).to(self.device)
+        """As the reference's ``removeBlobs`` (``__blobsClass.py:935-955``):
+        an int64 array lists the blobs to delete; a bool array of numBlobs
+        entries selects the blobs to KEEP (the reference indexes with it);
+        anything else raises TypeError."""
+        if type(iBlobs) != np.ndarray:
+            raise TypeError('iBlobs must be a numpy.array, it is a %s.' % str(type(iBlobs)))
+        if iBlobs.dtype == np.dtype('int64'):
+            if iBlobs.size and iBlobs.max() >= self.numBlobs:
+                raise TypeError('iBlobs values must be smaller than the numBlobs: %d.'
+                                % self.numBlobs)
+            keep = np.ones(self.numBlobs, dtype=bool)
+            keep[iBlobs] = False  # numpy.delete: negative indices count from the end
+        elif iBlobs.dtype == np.dtype('bool'):
+            if iBlobs.shape != (self.numBlobs,):
+                raise TypeError('iBlobs of type bool must have as many elements as numBlobs: %d.'
+                                % self.numBlobs)
+            keep = iBlobs
+        else:
+            raise TypeError('iBlobs must be of type int64 or bool, it is a %s.' % str(iBlobs.dtype))
+        k = torch.from_numpy(np.ascontiguousarray(keep)).to(self.device)
         self._x, self._y, self._g = self._x[k], self._y[k], self._g[k]
 
     # -- properties ---------------------------------------------------------------

@@ -65,3 +65,36 @@ def test_blobs_from_a_vorticity_function_sit_at_cell_centres():
     assert np.array_equal(x, [-0.75, -0.25, 0.25, 0.75] * 2)
     assert np.array_equal(y, [0.25] * 4 + [0.75] * 4)
     assert np.array_equal(g, (x + 10.0 * y) * 0.25)
+
+
+def _blobs_with_state(n):
+    import torch
+    from pfblob.blobs import Blobs
+    b = Blobs.__new__(Blobs)
+    b.device = torch.device("cpu")  # the host logic only; the state is a plain tensor here
+    b._x = torch.arange(n, dtype=torch.float64)
+    b._y = 10.0 * b._x
+    b._g = 100.0 * b._x
+    return b
+
+
+def test_remove_blobs_like_the_reference():
+    """int64 indices delete (negative ones from the end, as numpy.delete);
+    a bool mask of numBlobs entries KEEPS the selected blobs, because the
+    reference indexes with it (__blobsClass.py:935-955)."""
+    import numpy as np
+    b = _blobs_with_state(6)
+    b.removeBlobs(np.array([0, 3, -1], dtype=np.int64))
+    assert b._x.tolist() == [1.0, 2.0, 4.0] and b._g.tolist() == [100.0, 200.0, 400.0]
+    b.removeBlobs(np.array([True, False, True]))
+    assert b._x.tolist() == [1.0, 4.0] and b._y.tolist() == [10.0, 40.0]
+
+
+def test_remove_blobs_rejects_what_the_reference_rejects():
+    import numpy as np
+    b = _blobs_with_state(4)
+    for bad in ([1, 2], np.array([4], dtype=np.int64), np.array([True, False]),
+                np.array([1.0, 2.0])):
+        with pytest.raises(TypeError):
+            b.removeBlobs(bad)
+    assert b.numBlobs == 4

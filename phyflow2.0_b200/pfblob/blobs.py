@@ -10,7 +10,12 @@ redistribution (:490-494), and ``evolve`` (:705-781) with the reference's
 convection integrators (``_evolution.py:537-701``) and Wee or Tutty diffusion
 (``_evolution.py:138-445``, ``_diffusion`` :1002-1111, time step from
 ``__compute_deltaTd`` :2248-2318).
-Properties return numpy copies, as the reference's numpy-backed object does.
+Properties return numpy copies, as the reference's numpy-backed object does,
+and are read-only where the reference's are (:2324-3020): setting or deleting
+one raises AttributeError; ``vInf``, ``hardware`` and ``plotVelocity`` can be
+set.  ``evaluateVorticity`` is kept as the reference has it (:631-703, a method
+without a body that returns None); the induced vorticity itself is
+``pfblob.vorticity``.
 """
 import math
 
@@ -35,6 +40,28 @@ def _round_half_away(r):
     return int(q) + (1 if r - q >= 0.5 else 0)
 
 
+def _read_only(name, attr=None):
+    """Property returning self.<attr> (default _<name>); setting or deleting it
+    raises AttributeError with the reference's message."""
+    attr = attr or "_" + name
+
+    def get(self):
+        return getattr(self, attr)
+
+    def set_(self, value):
+        raise AttributeError('%s cannot be manually set by the user, user can only get the value '
+                             'of %s.' % (name, name))
+
+    def del_(self):
+        raise AttributeError('%s cannot be manually deleted by the user, user can only get the '
+                             'value of %s.' % (name, name))
+
+    return property(get, set_, del_)
+
+
+HARDWARE_OPTIONS = ('cpu', 'gpu')
+
+
 class Blobs:
     def __init__(self, wField, vInf, nu, deltaTc, h, overlap,
                  timeIntegrationParams=default_time_integration_params,
@@ -43,7 +70,7 @@ class Blobs:
                  diffusionParams=default_diffusion_params, device=None):
         if len(wField) != 3:
             raise ValueError("wField must have exactly 3 arrays. It has %d." % len(wField))
-        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        self.device = self._device_for(device)
         if callable(wField[0]):
             x, y, g = self._blobs_from_function(wField, h)
         else:
@@ -51,31 +78,39 @@ class Blobs:
             if not (x.shape == y.shape == g.shape):
                 raise ValueError("wField arrays must have the same shape")
         self._x, self._y, self._g = (self._dev(a) for a in (x, y, g))
-        self.vInf = np.asarray(vInf, dtype=np.float64)
-        self.nu = float(nu)
-        self.deltaTc = float(deltaTc)
-        self.h = float(h)
-        self.overlap = float(overlap)
-        self.sigma = self.h / self.overlap
-        self.timeIntegrationParams = dict(timeIntegrationParams)
-        self.blobControlParams = dict(blobControlParams)
-        self.velocityComputationParams = dict(velocityComputationParams)
-        self.diffusionParams = dict(diffusionParams)
+        self._vInf = np.asarray(vInf, dtype=np.float64)
+        self._nu = float(nu)
+        self._deltaTc = float(deltaTc)
+        self._h = float(h)
+        self._overlap = float(overlap)
+        self._sigma = self._h / self._overlap
+        self._timeIntegrationParams = dict(timeIntegrationParams)
+        self._blobControlParams = dict(blobControlParams)
+        self._velocityComputationParams = dict(velocityComputationParams)
+        self._diffusionParams = dict(diffusionParams)
         if self.timeIntegrationParams['method'] not in ('euler', 'rk4'):
             raise ValueError("timeIntegrationParams['method'] must be 'euler' or 'rk4'")
         if self.velocityComputationParams['method'] not in ('fmm', 'direct'):
             raise ValueError("velocityComputationParams['method'] must be 'fmm' or 'direct'")
+        if self.velocityComputationParams.get('hardware', 'gpu') not in HARDWARE_OPTIONS:
+            raise ValueError("velocityComputationParams['hardware'] must be 'cpu' or 'gpu'")
         if self.diffusionParams['method'] not in ('regrid_wee', 'regrid_tutty'):
             raise ValueError("diffusionParams['method'] must be 'regrid_wee' or 'regrid_tutty'")
-        self.deltaTd, self.stepDiffusion = self._compute_deltaTd()
-        self.tStep = 0
-        self.t = 0.0
+        self._deltaTd, self._stepDiffusion = self._compute_deltaTd()
+        self._tStep = 0
+        self._t = 0.0
+        self._plotVelocity = False
         if self.stepPopulationControl > 0:
             self.populationControl()
         if self.stepRedistribution > 0:
             self.redistribute()
 
     # -- helpers ----------------------------------------------------------------
+    @staticmethod
+    def _device_for(device):
+        """The CUDA device holding the blob set (the current one if None)."""
+        return torch.device("cuda", torch.cuda.current_device() if device is None else device)
+
     def _dev(self, a):
         return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(self.device)
 
@@ -156,6 +191,12 @@ class Blobs:
         vx, vy = self._velocity_at(self._x, self._y, xt, yt, Ndirect, tol, cutoff)
         return (vx.cpu().numpy(), vy.cpu().numpy()) if host else (vx, vy)
 
+    def evaluateVorticity(self, xEval, yEval):
+        """The reference's method has no body and returns None
+        (``__blobsClass.py:631-703``); kept so that code calling it behaves the
+        same.  The induced vorticity is ``pfblob.vorticity``."""
+        return None
+
     def redistribute(self, interpKernel=0):
         """M4' remesh onto the lattice containing (0, 0) (xBounds = [-1.5h, 1.5h])."""
         if interpKernel != 0:
@@ -211,8 +252,8 @@ class Blobs:
             self._regrid(0.0, population_control=True)
         elif redistribute:
             self.redistribute()
-        self.tStep += 1
-        self.t = self.deltaTc * self.tStep  # as the reference's _advanceTime, not a running sum
+        self._tStep += 1
+        self._t = self.deltaTc * self._tStep  # as the reference's _advanceTime, not a running sum
         if control and not fused:
             self.populationControl()
 
@@ -245,42 +286,115 @@ class Blobs:
         self._x, self._y, self._g = self._x[k], self._y[k], self._g[k]
 
     # -- properties ---------------------------------------------------------------
+    # read-only unless noted, with the reference's AttributeError messages
+    h = _read_only("h")
+    sigma = _read_only("sigma")
+    overlap = _read_only("overlap")
+    deltaTc = _read_only("deltaTc")
+    deltaTd = _read_only("deltaTd")
+    nu = _read_only("nu")
+    tStep = _read_only("tStep")
+    t = _read_only("t")
+    stepDiffusion = _read_only("stepDiffusion")
+    diffusionParams = _read_only("diffusionParams")
+    timeIntegrationParams = _read_only("timeIntegrationParams")
+    blobControlParams = _read_only("blobControlParams")
+    velocityComputationParams = _read_only("velocityComputationParams")
+    x = _read_only("x", "_x_host")
+    y = _read_only("y", "_y_host")
+    g = _read_only("g", "_g_host")
+    numBlobs = _read_only("numBlobs", "_num_blobs")
+    stepRedistribution = _read_only("stepRedistribution", "_step_redistribution")
+    stepPopulationControl = _read_only("stepPopulationControl", "_step_population_control")
+    gThresholdLocal = _read_only("gThresholdLocal", "_g_threshold_local")
+    gThresholdGlobal = _read_only("gThresholdGlobal", "_g_threshold_global")
+    integrationMethod = _read_only("integrationMethod", "_integration_method")
+    computationMethod = _read_only("computationMethod", "_computation_method")
+
     @property
-    def x(self):
+    def _x_host(self):
         return self._x.cpu().numpy()
 
     @property
-    def y(self):
+    def _y_host(self):
         return self._y.cpu().numpy()
 
     @property
-    def g(self):
+    def _g_host(self):
         return self._g.cpu().numpy()
 
     @property
-    def numBlobs(self):
+    def _num_blobs(self):
         return self._x.numel()
 
     @property
-    def stepRedistribution(self):
+    def _step_redistribution(self):
         return int(self.blobControlParams['stepRedistribution'])
 
     @property
-    def stepPopulationControl(self):
+    def _step_population_control(self):
         return int(self.blobControlParams['stepPopulationControl'])
 
     @property
-    def gThresholdLocal(self):
+    def _g_threshold_local(self):
         return float(self.blobControlParams['gThresholdLocal'])
 
     @property
-    def gThresholdGlobal(self):
+    def _g_threshold_global(self):
         return float(self.blobControlParams['gThresholdGlobal'])
 
     @property
-    def integrationMethod(self):
+    def _integration_method(self):
         return self.timeIntegrationParams['method']
 
     @property
-    def computationMethod(self):
-        return (self.velocityComputationParams['method'], self.velocityComputationParams['hardware'])
+    def _computation_method(self):
+        return self.velocityComputationParams['method']
+
+    @property
+    def vInf(self):
+        return self._vInf
+
+    @vInf.setter
+    def vInf(self, vInfnew):
+        v = np.asarray(vInfnew, dtype=np.float64)
+        if v.shape != (2,):
+            raise ValueError('vInf must have shape (2,0). It has shape %s.' % str(v.shape))
+        self._vInf = v
+
+    @vInf.deleter
+    def vInf(self):
+        raise AttributeError('vInf cannot be manually deleted by the user, user can only get the '
+                             'value of vInf.')
+
+    @property
+    def hardware(self):
+        """'cpu' or 'gpu' as given; every computation here runs on the GPU."""
+        return self.velocityComputationParams['hardware']
+
+    @hardware.setter
+    def hardware(self, hardwarenew):
+        if hardwarenew not in HARDWARE_OPTIONS:
+            raise ValueError("velocityComputationParams['hardware'] must be 'cpu' or 'gpu'")
+        self.velocityComputationParams['hardware'] = hardwarenew
+
+    @hardware.deleter
+    def hardware(self):
+        raise AttributeError('hardware cannot be deleted by the user, user can only get and set '
+                             'the value of hardware.')
+
+    @property
+    def plotVelocity(self):
+        return self._plotVelocity
+
+    @plotVelocity.setter
+    def plotVelocity(self, plotVelocitynew):
+        if type(plotVelocitynew) != bool:
+            raise TypeError('plotVelocity must be of type bool. It is of type: %s'
+                            % str(type(plotVelocitynew)))
+        self._plotVelocity = plotVelocitynew
+
+    @plotVelocity.deleter
+    def plotVelocity(self):
+        raise AttributeError('plotVelocity cannot be deleted by the user, user can only get and set '
+                             'the value of plotVelocity.')

@@ -7,8 +7,8 @@ import pytest
 def _blobs(method, nu, h, deltaTc, c2="optimized"):
     from pfblob.blobs import Blobs
     b = Blobs.__new__(Blobs)
-    b.nu, b.h, b.deltaTc = float(nu), float(h), float(deltaTc)
-    b.diffusionParams = {"method": method, "c2": c2}
+    b._nu, b._h, b._deltaTc = float(nu), float(h), float(deltaTc)
+    b._diffusionParams = {"method": method, "c2": c2}
     return b
 
 

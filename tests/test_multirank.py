@@ -26,7 +26,7 @@ def _worker(rank, world, port, out):
 def test_reduce_max_over_two_gloo_ranks():
     world = 2
     port = 29500 + os.getpid() % 1000
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of a threaded process
         out = m.dict()
         mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
         assert out[0] == out[1] == 2.5

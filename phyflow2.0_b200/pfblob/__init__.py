@@ -6,7 +6,7 @@ Entry points (same names, arguments and results as pHyFlow):
 * ``vorticity``        - pHyFlow.blobs.base.induced.vorticity (direct, Gauss)
 * ``Regrid``           - pHyFlow.blobs.base.regrid.Regrid (M4' remesh)
 * ``PopulationControl`` - pHyFlow.blobs.base.regrid.PopulationControl
-* ``diffusion_wee``, ``diffusion_tutty`` - pHyFlow.blobs.base.evolution
+* ``convection``, ``diffusion_wee``, ``diffusion_tutty`` - pHyFlow.blobs.base.evolution
 * ``inducedVelocity``, ``influenceMatrix`` - pHyFlow.panels.base.panelSolver
 * ``lu_factor``, ``lu_solve`` - the panel-strength solve of pHyFlow.panels.Panels
 * ``Blobs``            - the evaluateVelocity / redistribute surface of pHyFlow.blobs.Blobs
@@ -18,13 +18,15 @@ from . import _lib
 from .blobs import Blobs
 from .conservation import conservation_error, moments_device
 from .diffusion import diffusion_tutty, diffusion_wee
+from .evolution import convection, convection_device
 from .induced import (CPU_HARDWARE, DIRECT_METHOD, FMM_METHOD, GAUSS_KERNEL, GPU_HARDWARE,
                       fmm_parameters, velocity, velocity_device, vorticity)
 from .panels import inducedVelocity, influenceMatrix, lu_factor, lu_solve, panel_velocity_device
 from .regrid import PopulationControl, Regrid, population_control_device, remesh_device
 
 __all__ = ["Blobs", "velocity", "velocity_device", "vorticity", "Regrid", "remesh_device", "PopulationControl",
-           "population_control_device", "diffusion_wee", "diffusion_tutty", "inducedVelocity",
+           "population_control_device", "convection", "convection_device", "diffusion_wee",
+           "diffusion_tutty", "inducedVelocity",
            "influenceMatrix", "lu_factor", "lu_solve",
            "panel_velocity_device", "moments_device", "conservation_error", "fmm_parameters",
            "GAUSS_KERNEL", "CPU_HARDWARE", "GPU_HARDWARE", "FMM_METHOD", "DIRECT_METHOD"]

@@ -2,7 +2,8 @@
 property surface run with the device entry points replaced by the oracle on
 CPU tensors, and are compared with the same sequence of oracle steps written
 out by hand (the reference's order: convection, diffusion, redistribution,
-time advance, population control; __blobsClass.py:705-781).  This checks the
+time advance, population control; __blobsClass.py:705-781), and the
+convection function against the reference's integrators.  This checks the
 orchestration only; the device kernels are checked against the oracle by the
 GPU tests."""
 import numpy as np
@@ -163,3 +164,35 @@ def test_property_surface(host_blobs):
     with pytest.raises(TypeError):
         b.plotVelocity = 1
     assert b.evaluateVorticity(np.zeros(2), np.zeros(2)) is None
+
+
+def test_convection_matches_the_reference_integrators(monkeypatch):
+    """convection_device with the oracle velocity against the reference's two
+    integrators written out in numpy: forward Euler (_evolution.py:539-546)
+    and the RK4 loop with its stage increment left at zero (:664-693), four
+    velocity evaluations included."""
+    from pfblob import evolution as E
+    monkeypatch.setattr(E, "velocity_device", _velocity)
+    c1, x, y = _c1()
+    g = c1.g
+    sigma, dt, vinf = c1.h / 0.8, 0.02, (0.3, -0.1)
+    ks = 2 * sigma * sigma
+    # forward Euler
+    xn, yn = E.convection_device(dt, T(x), T(y), T(g), sigma, vInf=vinf, integrator=0)
+    vx, vy = oracle.velocity_direct(x, y, g, ks, x, y)
+    assert np.array_equal(xn.numpy(), x + dt * (vx + vinf[0]))
+    assert np.array_equal(yn.numpy(), y + dt * (vy + vinf[1]))
+    # RK4 as the reference runs it
+    xr, yr = x.copy(), y.copy()
+    kx_rk4, ky_rk4 = np.zeros(x.shape), np.zeros(y.shape)
+    tf = np.array([0.0, 0.5, 0.5, 1.0])
+    kw = np.array([1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0])
+    for i in range(4):
+        xs, ys = x + kx_rk4 * dt * tf[i], y + ky_rk4 * dt * tf[i]
+        vx, vy = oracle.velocity_direct(xs, ys, g, ks, xs, ys)
+        xr += kw[i] * (vx + vinf[0]) * dt
+        yr += kw[i] * (vy + vinf[1]) * dt
+    xn, yn = E.convection_device(dt, T(x), T(y), T(g), sigma, vInf=vinf, integrator=1)
+    assert np.array_equal(xn.numpy(), xr) and np.array_equal(yn.numpy(), yr)
+    with pytest.raises(ValueError):
+        E.convection_device(dt, T(x), T(y), T(g), sigma, integrator=2)

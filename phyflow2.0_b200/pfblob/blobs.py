@@ -22,6 +22,7 @@ import math
 import numpy as np
 import torch
 
+from .evolution import FE_INTEGRATOR, RK4_INTEGRATOR, convection_device
 from .induced import DIRECT_METHOD, FMM_METHOD, fmm_parameters, velocity_device
 from .regrid import population_control_device, remesh_device
 
@@ -217,23 +218,11 @@ class Blobs:
         (Wee every stepDiffusion steps, or Tutty every step), redistribution
         and population control.  With Wee and nu = 0 the reference divides by
         stepDiffusion = 0; here diffusion is skipped."""
-        vinf = self.vInf
-        if self.timeIntegrationParams['method'] == 'euler':
-            vx, vy = self._velocity_at(self._x, self._y, self._x, self._y)
-            xn = self._x + (vx + vinf[0]) * self.deltaTc
-            yn = self._y + (vy + vinf[1]) * self.deltaTc
-        else:
-            # _evolution.py:679-693 evaluates all four stages at the start
-            # positions (the stage increment it adds stays zero), so the four
-            # velocities are identical: evaluate once, apply the four weighted
-            # updates in the reference's order.
-            vx, vy = self._velocity_at(self._x, self._y, self._x, self._y)
-            kx, ky = vx + vinf[0], vy + vinf[1]
-            xn, yn = self._x.clone(), self._y.clone()
-            for w in (1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0):
-                xn += w * kx * self.deltaTc
-                yn += w * ky * self.deltaTc
-        self._x, self._y = xn, yn
+        # convection (_evolution.py:37-135): forward Euler, or the reference's
+        # RK4, whose four stages all sit at the start positions
+        integrator = FE_INTEGRATOR if self.integrationMethod == 'euler' else RK4_INTEGRATOR
+        self._x, self._y = convection_device(self.deltaTc, self._x, self._y, self._g, self.sigma,
+                                             2.0, self.vInf, self._method(), integrator)
         if self.diffusionParams['method'] == 'regrid_tutty':
             # __blobsClass.py:1073-1111: redistribute, then Tutty's diffusive
             # redistribution, every step (hNu = 0 when nu = 0)

@@ -12,6 +12,7 @@ import torch
 
 import oracle
 from pfblob import blobs as B
+from pfblob import evolution as E
 from pfblob import workloads as wl
 
 T = torch.from_numpy
@@ -45,6 +46,7 @@ def _popctl(x, y, g, tl, tg, **kw):
 def host_blobs(monkeypatch):
     monkeypatch.setattr(B.Blobs, "_device_for", staticmethod(lambda device: torch.device("cpu")))
     monkeypatch.setattr(B, "velocity_device", _velocity)
+    monkeypatch.setattr(E, "velocity_device", _velocity)
     monkeypatch.setattr(B, "remesh_device", _remesh)
     monkeypatch.setattr(B, "population_control_device", _popctl)
     return B.Blobs
@@ -171,7 +173,6 @@ def test_convection_matches_the_reference_integrators(monkeypatch):
     integrators written out in numpy: forward Euler (_evolution.py:539-546)
     and the RK4 loop with its stage increment left at zero (:664-693), four
     velocity evaluations included."""
-    from pfblob import evolution as E
     monkeypatch.setattr(E, "velocity_device", _velocity)
     c1, x, y = _c1()
     g = c1.g

@@ -8,8 +8,10 @@ Cython vortex-panel kernel
 the C++ CPU FMM (``src/cpp/blobs/c++/fmm2d_py_cpu_gpu/*.cpp`` behind
 ``oracle/ref_fmm_driver.cpp``) and the induced-vorticity loop of
 ``src/cpp/blobs/c/ww2parGauss_C/ww2parGauss_C_cpu.c`` (behind
-``oracle/ref_ww2_driver.c``).  The built files travel with the repository
-snapshot; the sources they were built from do not.
+``oracle/ref_ww2_driver.c``), and the M4' weight loop of
+``src/cpp/blobs/c++/interpolation_kernels_1d/_interpolation_kernels_1d.cpp``
+(behind ``oracle/ref_m4_driver.cpp``).  The built files travel with the
+repository snapshot; the sources they were built from do not.
 """
 import ctypes
 import importlib.util
@@ -115,3 +117,23 @@ def panel_influence(xcp, ycp, xs, ys, xe, ye, cosa, sina):
     """Reference Cython assemble_influenceMatrix -> A (M, M)."""
     f = [np.ascontiguousarray(a, dtype=np.float64) for a in (xcp, ycp, xs, ys, xe, ye, cosa, sina)]
     return np.array(_module("_vortexPanel_Cython_cpu").assemble_influenceMatrix(*f))
+
+
+def m4_available():
+    return os.path.exists(os.path.join(REF_DIR, "libref_m4.so"))
+
+
+def m4kernel_1d(x, c):
+    """The reference's own m4kernel_1d loop (_interpolation_kernels_1d.cpp:
+    74-89) -> the M4' weights of the points x (flattened), Wee coefficient c."""
+    if "m4" not in _cache:
+        lib = ctypes.CDLL(os.path.join(REF_DIR, "libref_m4.so"))
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.ref_m4kernel_1d.argtypes = [ctypes.c_size_t, dp, ctypes.c_double, dp]
+        lib.ref_m4kernel_1d.restype = None
+        _cache["m4"] = lib
+    x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).ravel())
+    w = np.empty_like(x)
+    p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    _cache["m4"].ref_m4kernel_1d(x.shape[0], p(x), float(c), p(w))
+    return w

@@ -3,7 +3,8 @@
 Run here, where the pHyFlow sources exist (they do not travel with the repo):
 
     make -C oracle ref
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref PATH]   (default: $PHYFLOW_REFERENCE, else
+                                                      ../reference beside the repository)
 
 Sources of truth:
 * direct Gauss velocity   - the reference Cython kernel
@@ -15,8 +16,9 @@ Sources of truth:
   (src/python/blobs/base/regrid/_regridding.py), imported under Python 3 with
   stub modules for its two pHyFlow imports: ``blobOptions`` (the constant
   M4PRIME_INTERPKERNEL = 0) and ``m4kernel_1d``, which the reference builds
-  with boost.python and which is supplied here by our C restatement of
-  _interpolation_kernels_1d.cpp:75-89;
+  with boost.python; here its own weight loop
+  (_interpolation_kernels_1d.cpp:74-89, extracted and compiled into
+  oracle/_ref/libref_m4.so) stands in for it;
 * FMM                     - the reference C++ CPU FMM (oracle/_ref/libreffmm.so);
 * population control      - the reference ``PopulationControl`` (same module
   as ``Regrid``);
@@ -94,7 +96,9 @@ def load_reference_regrid(refroot):
     cpp = types.ModuleType("pHyFlow.cpp")
     cppb = types.ModuleType("pHyFlow.cpp.blobs")
     rem = types.ModuleType("pHyFlow.cpp.blobs.remesh")
-    rem.m4kernel_1d = lambda x, c: oracle.m4prime(np.asarray(x).ravel(), c)
+    if not ref.m4_available():
+        raise SystemExit("oracle/_ref/libref_m4.so missing: run `make -C oracle ref` first")
+    rem.m4kernel_1d = lambda x, c: ref.m4kernel_1d(x, c)
     rem.__all__ = ["m4kernel_1d"]
     for name, mod in [("pHyFlow", pk), ("pHyFlow.blobs", blobs), ("pHyFlow.blobs.blobOptions", opts),
                       ("pHyFlow.cpp", cpp), ("pHyFlow.cpp.blobs", cppb),
@@ -132,8 +136,10 @@ def rand_blobs(n, sigma, seed, lo=0.0, hi=1.0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    ap.add_argument("--only", choices=["popctl", "tutty", "vorticity", "influence"], default=None,
+    ap.add_argument("--ref", default=os.environ.get(
+        "PHYFLOW_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference")))
+    ap.add_argument("--only", choices=["popctl", "tutty", "vorticity", "influence", "regrid"],
+                    default=None,
                     help="write only this group of fixtures")
     args = ap.parse_args()
     if args.only == "popctl":
@@ -147,6 +153,10 @@ def main():
         return
     if args.only == "influence":
         influence_fixtures()
+        return
+    if args.only == "regrid":  # M4' sweep, Regrid and Tutty fixtures
+        regrid_fixtures(args.ref)
+        tutty_fixtures(args.ref)
         return
     assert ref.available(), "build oracle/_ref first: make -C oracle ref"
 
@@ -185,9 +195,40 @@ def main():
     np.savez_compressed(os.path.join(HERE, "panel_cyl.npz"), gamma=ps.gamma, xs=ps.xs, ys=ps.ys,
                         xe=ps.xe, ye=ps.ye, cosa=ps.cosa, sina=ps.sina, xv=xv, yv=yv, vx=vx, vy=vy)
 
-    # 4. remesh through the reference Regrid: C1 lattice, and random blobs with
-    #    and without the Wee diffusion term, and blobs sitting exactly on nodes
-    R = load_reference_regrid(args.ref)
+    regrid_fixtures(args.ref)
+
+    # 5. reference CPU FMM on random blobs (cross-check of the FMM path)
+    x, y, g, sigma = rand_blobs(4096, 0.01, 17)
+    vx, vy = ref.fmm_velocity(x, y, g, sigma, tol=1e-6)
+    np.savez_compressed(os.path.join(HERE, "fmm_rand.npz"), x=x, y=y, g=g, sigma=sigma,
+                        tol=1e-6, vx=vx, vy=vy)
+    population_control_fixtures(args.ref)
+    tutty_fixtures(args.ref)
+    vorticity_fixtures()
+    influence_fixtures()
+    print("golden fixtures written to", HERE)
+
+
+def m4_fixture():
+    """0. the reference's own M4' weight loop on a sweep of points (the branch
+    boundaries |x| = 0, 1, 2 exactly, points just inside and outside them,
+    and a dense grid) for several Wee coefficients."""
+    base = np.concatenate([np.linspace(-2.5, 2.5, 2001),
+                           np.array([0.0, 1.0, -1.0, 2.0, -2.0]),
+                           np.nextafter(np.array([1.0, 1.0, 2.0, 2.0]), np.array([0.0, 3.0, 0.0, 3.0])),
+                           np.random.Generator(np.random.PCG64(5)).uniform(-2.2, 2.2, 3000)])
+    cs = np.array([0.0, 0.1, 0.3, 0.7])
+    w = np.stack([ref.m4kernel_1d(base, c) for c in cs])
+    np.savez_compressed(os.path.join(HERE, "m4_ref.npz"), x=base, c=cs, w=w)
+
+
+def regrid_fixtures(refroot):
+    """4. remesh through the reference Regrid (with the reference's own M4'
+    loop): C1 lattice, random blobs with and without the Wee diffusion term,
+    and blobs sitting exactly on nodes."""
+    m4_fixture()
+    c1 = wl.lamb_oseen_lattice()
+    R = load_reference_regrid(refroot)
     xb, yb = c1.bounds()
     xn, yn, gn = R.Regrid(c1.x, c1.y, c1.g, c1.sigma, c1.overlap, xb, yb, 0, 0.0)
     np.savez_compressed(os.path.join(HERE, "regrid_c1.npz"), x=c1.x, y=c1.y, g=c1.g,
@@ -204,16 +245,6 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"regrid_rand_{tag}.npz"), x=x, y=y, g=g,
                             sigma=sigma, overlap=0.8, xb=xb, yb=xb, c=c, xn=xn, yn=yn, gn=gn)
 
-    # 5. reference CPU FMM on random blobs (cross-check of the FMM path)
-    x, y, g, sigma = rand_blobs(4096, 0.01, 17)
-    vx, vy = ref.fmm_velocity(x, y, g, sigma, tol=1e-6)
-    np.savez_compressed(os.path.join(HERE, "fmm_rand.npz"), x=x, y=y, g=g, sigma=sigma,
-                        tol=1e-6, vx=vx, vy=vy)
-    population_control_fixtures(args.ref)
-    tutty_fixtures(args.ref)
-    vorticity_fixtures()
-    influence_fixtures()
-    print("golden fixtures written to", HERE)
 
 
 def influence_fixtures():

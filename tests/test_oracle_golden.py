@@ -2,6 +2,7 @@
 tests/golden/, made by tests/golden/make_golden.py from the compiled reference
 Cython kernels, the reference Regrid and the reference C++ FMM)."""
 import numpy as np
+import pytest
 
 import oracle
 from conftest import normwise_err
@@ -63,6 +64,27 @@ def test_m4prime_branches():
     for s in (0.1, 0.37, 0.73):
         u = np.array([1.0, 0.0, -1.0, -2.0]) + s
         assert abs(oracle.m4prime(u, 0.0).sum() - 1.0) < 1e-15
+
+
+def test_m4prime_matches_reference_loop(golden):
+    """The oracle's M4' equals, bit for bit, the reference's own m4kernel_1d
+    loop (_interpolation_kernels_1d.cpp:74-89, compiled from its source lines)
+    on the branch boundaries, just inside and outside them, and a dense sweep,
+    for four Wee coefficients."""
+    r = golden("m4_ref")
+    for k, c in enumerate(r["c"]):
+        assert np.array_equal(oracle.m4prime(r["x"], float(c)), r["w"][k]), float(c)
+
+
+def test_m4prime_matches_compiled_reference_when_present():
+    """Same check against the compiled loop itself on fresh random points
+    (where oracle/_ref holds it)."""
+    from oracle import ref
+    if not ref.m4_available():
+        pytest.skip("oracle/_ref/libref_m4.so not built here")
+    x = np.random.default_rng(9).uniform(-2.5, 2.5, 100000)
+    for c in (0.0, 0.25, 1.3):
+        assert np.array_equal(oracle.m4prime(x, c), ref.m4kernel_1d(x, c))
 
 
 def test_reference_fmm_within_tolerance_of_direct_oracle(golden):

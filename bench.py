@@ -116,10 +116,49 @@ def gpu_id_for_smi(torch):
 N_DEFAULT = 1 << 20
 
 
+def workloads():
+    """The seeded generators (pfblob/workloads.py), loaded by file so that the
+    reference arm never imports pfblob (whose import loads libpfblob.so)."""
+    import importlib.util
+    name = "pfblob_workloads_file"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(
+            name, os.path.join(ROOT, "phyflow2.0_b200", "pfblob", "workloads.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules[name] = mod
+    return sys.modules[name]
+
+
 def workload_c2(n=None):
     """C2 blobs; a smaller n (profiling cases) keeps sigma and the domain."""
-    from pfblob import workloads as wl
-    return wl.uniform_square(n=n or N_DEFAULT, sigma=0.002, overlap=0.8, config=2, instance=0)
+    return workloads().uniform_square(n=n or N_DEFAULT, sigma=0.002, overlap=0.8, config=2,
+                                      instance=0)
+
+
+METRIC = "blob velocity evals/s at <=1e-6 rel err vs FP64 (velocity + M4' remesh step)"
+
+
+def workload_config(n, method, sigma, world):
+    """The config object both arms print (identical for the same workload)."""
+    return {"workload": f"single large instance: N={n} blobs U[0,1)^2, sigma=0.002, "
+                        f"velocity at all blobs ({method}) + M4' remesh h=0.8 sigma",
+            "n_blobs": n, "method": method, "sigma": sigma,
+            "l2": "GPU arm: L2 flushed between timed steps (256 MB write outside the step "
+                  "events); the step's inputs are 24 MB",
+            "parallelism": f"replicas x{world}"}
+
+
+def host_info():
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count() or 1, "cpu_model": model}
 
 
 def pick_method(arg):
@@ -152,6 +191,7 @@ def run_ours(args, rank, world):
     import torch
     import pfblob
     from pfblob import _lib
+    from pfblob.regrid import remesh_device_async
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
@@ -167,6 +207,9 @@ def run_ours(args, rank, world):
     vy = torch.empty_like(vx)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
+    # the remesh scratch bound of a resident blob set: its previous window
+    # plus 25% (found by the first warm-up step)
+    mb = [max(4 * n, 4096)]
 
     def step(ev=None):
         if ev is not None:
@@ -175,15 +218,31 @@ def run_ours(args, rank, world):
                                tol=1e-6, ndirect=args.ndirect)
         if ev is not None:
             ev[1].record(stream)
-        out = pfblob.remesh_device(x, y, g, b.h, xb[0], yb[0], 0.0, capacity=8 * n)
+        out = remesh_device_async(x, y, g, b.h, xb[0], yb[0], 0.0, max_base_cells=mb[0],
+                                  with_indices=True)
         if ev is not None:
             ev[2].record(stream)
         return out
 
+    def settle(out):
+        """Host side of a step's remesh, after the device work: the output
+        count, the status word (8 = window beyond the bound: raise it), the
+        window."""
+        k, st_, w = int(out[5].item()), int(out[6].item()), out[7].cpu().tolist()
+        if st_ & 8:
+            mb[0] = int(w[2] * w[3] * 5 // 4) + 1
+        elif st_:
+            raise RuntimeError(f"remesh status {st_}")
+        return k, st_, w
+
     for _ in range(args.warmup):
-        step()
+        o = step()
+        settle(o)
+        w = o[7].cpu().tolist()
+        mb[0] = int(w[2] * w[3] * 5 // 4) + 1
     torch.cuda.synchronize()
-    nout = step()[0].numel()
+    last = step()
+    nout, _, win = settle(last)
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     if world > 1:
         torch.distributed.barrier()
@@ -192,16 +251,20 @@ def run_ours(args, rank, world):
     if method == "fmm":
         _lib.fmm_profile(True, dev.index)
     l0 = _lib.kernel_launches()
+    outs = []
     with ClockSampler(gpu_id_for_smi(torch)) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
-            step(evs[k])
-            if method == "fmm":  # the remesh already synchronised the stream
+            outs.append(step(evs[k]))
+            if method == "fmm":  # reads the FMM's events: synchronises after the step
                 fmm_stats.append(_lib.fmm_last_stats(dev.index))
         torch.cuda.synchronize()
     launches = _lib.kernel_launches() - l0
     if method == "fmm":
         _lib.fmm_profile(False, dev.index)
+    for o in outs:  # every timed step completed its remesh on the first try
+        kk, st_, _ = settle(o)
+        assert st_ == 0 and kk == nout, (kk, st_, nout)
     if world > 1:
         torch.distributed.barrier()
     vel_ms = [e[0].elapsed_time(e[1]) for e in evs]
@@ -210,23 +273,27 @@ def run_ours(args, rank, world):
     t_max = reduce_max(step_ms, dev, world)
     value = world * n / (t_max * 1e-3)
 
-    # end to end through the public API with host (numpy) buffers
+    # end to end through the public API with host (numpy) buffers: one upload
+    # of x, y, g, velocity and remesh, results read back
     e2e = None
     if not args.no_e2e:
-        hx, hy, hg = b.x, b.y, b.g
+        # the step's inputs in pinned host memory (as a caller staging them)
+        hx, hy, hg = (torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+                      for a in (b.x, b.y, b.g))
         e2e_ms = []
         for k in range(max(2, min(args.steps, 5)) + 1):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            ux, uy = pfblob.velocity(hx, hy, hg, b.sigma, k=b.k, hardware=1, method=meth_id,
-                                     Ndirect=args.ndirect, tol=1e-6)
-            rxn, ryn, rgn = pfblob.Regrid(hx, hy, hg, b.sigma, b.overlap, xb, yb)
+            ux, uy, rxn, ryn, rgn = pfblob.velocity_and_regrid(
+                hx, hy, hg, b.sigma, b.overlap, xb, yb, k=b.k, method=meth_id,
+                Ndirect=args.ndirect, tol=1e-6)
             torch.cuda.synchronize()
             if k > 0:
                 e2e_ms.append((time.perf_counter() - t0) * 1e3)
         em = reduce_max(statistics.median(e2e_ms), dev, world)
         e2e = {"value": world * n / (em * 1e-3), "unit": "evals/s", "ms_per_step": em,
-               "h2d_bytes_per_step": 2 * 24 * n, "d2h_bytes_per_step": 16 * n + 24 * rxn.shape[0]}
+               "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 16 * n + 24 * rxn.shape[0],
+               "api": "pfblob.velocity_and_regrid (pinned host tensors in, numpy out)"}
 
     pk = peaks()
     vel_avg = statistics.mean(vel_ms)
@@ -243,6 +310,7 @@ def run_ours(args, rank, world):
                 "peak_source": f"{MUFU_PER_SM_CLK} MUFU/SM/clk x SMs x sm_max_mhz "
                                f"({pk['source']}) / {MUFU_PER_INTERACTION} MUFU per interaction",
                 "per_unit": "1 interaction = 2 MUFU (ex2, rcp) + 14 FP32 flops"}
+        fmm_info = None
     else:
         st0 = fmm_stats[-1]
         ms_p2p = statistics.mean(f["ms_p2p"] for f in fmm_stats)
@@ -285,109 +353,194 @@ def run_ours(args, rank, world):
                                            "ms_p2p", "ms_l2p", "ms_total")},
                     "roofline_m2l": roof_m2l}
     alg_bytes = 24 * n + 24 * nout
-    roof_rm = {"bound": "hbm", "kernel": "remesh (all passes)", "achieved": alg_bytes / (rm_avg * 1e-3) / 1e9,
-               "peak": pk["hbm_gbs"], "unit": "GB/s",
+    roof_rm = {"bound": "hbm", "kernel": "remesh (all passes, pf_remesh_async)",
+               "achieved": alg_bytes / (rm_avg * 1e-3) / 1e9, "peak": pk["hbm_gbs"], "unit": "GB/s",
                "frac": alg_bytes / (rm_avg * 1e-3) / 1e9 / pk["hbm_gbs"],
-               "traffic": traffic.get("remesh"), "algorithmic_bytes": alg_bytes}
+               "traffic": traffic.get("remesh"), "algorithmic_bytes": alg_bytes,
+               "per_unit": "24 B per input blob (x, y, g read) + 24 B per output blob (x, y, g "
+                           "written)"}
+    cfg = workload_config(n, method, b.sigma, world)
+    cfg["n_out_remesh"] = nout
     line = {
-        "metric": "blob velocity evals/s at <=1e-6 rel err vs FP64 (velocity + M4' remesh step)",
+        "metric": METRIC,
         "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32-compensated velocity, f64 remesh",
         "data": "synthetic (seeded U[0,1)^2 blobs, g~N(0,1)/N)",
-        "config": {"workload": f"single large instance: N={n} blobs U[0,1)^2, sigma=0.002, "
-                               f"velocity at all blobs ({method}) + M4' remesh h=0.8 sigma",
-                   "n_blobs": n, "method": method, "sigma": b.sigma, "n_out_remesh": nout,
-                   "l2": "flushed between timed steps (256 MB write outside the step events)",
-                   "parallelism": f"replicas x{world}"},
+        "config": cfg,
         "phase_ms": {"velocity": vel_avg, "remesh": rm_avg},
         "gpu_launches": launches, "roofline": roof, "roofline_remesh": roof_rm,
-        "fmm": fmm_info if method == "fmm" else None,
+        "fmm": fmm_info,
         "clocks": clk.summary(), "e2e": e2e,
     }
+    if rank == 0 and not args.no_check:
+        line["err_vs_fp64"] = check_step(b, vx, vy, last, nout)
     return line
 
 
-# ---------------------------------------------------------------------------
-# CPU side: the reference's own CPU code (oracle/_ref) on a bounded sample
-def cpu_reference_step(method, rng_seed=0):
-    """One bounded sample of the workload on the host with the reference's CPU
-    implementation.  Returns (evals/s scaled to the full workload, description,
-    threads)."""
+def check_step(b, vx, vy, out, nout, n_targets=4096):
+    """Accuracy of the timed step's results, outside the timed region: the
+    velocity against the FP64 oracle direct sum on a seeded subset of targets
+    (normwise: max |dv| / max |v_ref|), the remesh against the oracle Regrid
+    (indices and coordinates bit-exact, values normwise), and conservation."""
     import oracle
-    from oracle import ref
-    b = workload_c2()
-    threads = os.cpu_count() or 1
-    if method == "direct":
-        # 1/8 x 1/8 sub-square: same density; direct cost scales as N^2
-        sel = (b.x < 0.125) & (b.y < 0.125)
-        xs, ys, gs = b.x[sel], b.y[sel], b.g[sel]
-        ns = xs.shape[0]
-        t0 = time.perf_counter()
-        if ref.available():
-            ref.direct_gauss(xs, ys, gs, b.ksigmasqr)
-            kind = "reference"
-        else:
-            oracle.velocity_direct(xs, ys, gs, b.ksigmasqr, nthreads=threads)
-            kind = "port"
-        tv = time.perf_counter() - t0
-        rate = float(ns) * ns / tv  # interactions/s
-        xb, yb = b.bounds()
-        t0 = time.perf_counter()
-        oracle.regrid(xs, ys, gs, b.sigma, b.overlap, xb, yb)
-        tr = (time.perf_counter() - t0) / ns  # s per blob
-        t_full = float(b.n) * b.n / rate + tr * b.n
-        desc = (f"{ns} blobs of the 1/8 x 1/8 sub-square (same density): reference Cython direct "
-                f"(OpenMP, {threads} threads) scaled to N^2 pairs + numpy/scipy Regrid per blob")
-        return b.n / t_full, desc, threads, kind
-    # FMM path: 1/4 x 1/4 sub-square, reference C++ FMM (single thread) + Regrid
-    sel = (b.x < 0.25) & (b.y < 0.25)
-    xs, ys, gs = b.x[sel], b.y[sel], b.g[sel]
-    ns = xs.shape[0]
     t0 = time.perf_counter()
-    if ref.available():
-        ref.fmm_velocity(xs, ys, gs, b.sigma, k=b.k, tol=1e-6, ndirect=35)
-        kind = "reference"
-    else:
-        oracle.velocity_direct(xs, ys, gs, b.ksigmasqr, nthreads=threads)
-        kind = "port"
+    rng = np.random.default_rng(20261203)
+    sub = np.sort(rng.choice(b.n, size=min(n_targets, b.n), replace=False))
+    rx, ry = oracle.velocity_direct(b.x, b.y, b.g, b.ksigmasqr, b.x[sub].copy(), b.y[sub].copy(),
+                                    nthreads=os.cpu_count() or 1)
+    gx, gy = vx.cpu().numpy()[sub], vy.cpu().numpy()[sub]
+    d = np.sqrt((gx - rx) ** 2 + (gy - ry) ** 2)
+    vref = np.sqrt(rx ** 2 + ry ** 2)
+    strong = vref >= 1e-3 * vref.max()
     xb, yb = b.bounds()
-    oracle.regrid(xs, ys, gs, b.sigma, b.overlap, xb, yb)
-    t = time.perf_counter() - t0
-    desc = (f"{ns} blobs of the 1/4 x 1/4 sub-square (same density): reference C++ CPU FMM "
-            f"(tol 1e-6, Ndirect 35, single-threaded as built) + numpy/scipy Regrid")
-    return ns / t, desc, (1 if kind == "reference" else threads), kind
+    ox, oy, og, oix, oiy = oracle.regrid(b.x, b.y, b.g, b.sigma, b.overlap, xb, yb)
+    k = nout
+    rx_, ry_, rg_, rix, riy = (t[:k].cpu().numpy() for t in out[:5])
+    m0 = oracle.moments(b.x, b.y, b.g)
+    m1 = oracle.moments(rx_, ry_, rg_)
+    xs = float(max(np.abs(b.x).max(), np.abs(b.y).max()))
+    return {"velocity_normwise": float(d.max() / vref.max()),
+            "velocity_pointwise_max": float((d[strong] / vref[strong]).max()),
+            "targets": int(sub.size), "gate": 1e-6,
+            "remesh_indices_bit_exact": bool(k == oix.size and np.array_equal(rix, oix)
+                                             and np.array_equal(riy, oiy)),
+            "remesh_coords_bit_exact": bool(k == ox.size and np.array_equal(rx_, ox)
+                                            and np.array_equal(ry_, oy)),
+            "remesh_values_normwise": float(np.abs(rg_ - og).max() / np.abs(og).max())
+            if k == og.size else None,
+            "circulation": float(abs(m1[0] - m0[0]) / m0[3]),
+            "linear_impulse": float(max(abs(m1[1] - m0[1]), abs(m1[2] - m0[2])) / (m0[3] * xs)),
+            "oracle": "FP64 direct Gauss sum (C restatement of vv2parGauss) on a seeded target "
+                      "subset; numpy/scipy Regrid restatement",
+            "check_s": time.perf_counter() - t0}
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the reference's own CPU code (oracle/_ref) on the same workload.
+# The reference FMM (fmm2dInteract, fmm.cpp:88-304) is single-threaded as
+# built; its API takes targets apart from sources, so each host process runs
+# it with all sources on a contiguous share of the targets, and the Regrid
+# (numpy + scipy restatement of _regridding.py:107-222, pinned bit-exact to
+# the reference's own function) runs in the parent meanwhile.
+_REF_STATE = {}
+
+
+def _ref_worker_init(x, y, g, sigma, k):
+    from oracle import ref
+    _REF_STATE.update(x=x, y=y, g=g, sigma=sigma, k=k, ref=ref)
+
+
+def _ref_worker_chunk(lohi):
+    lo, hi = lohi
+    st = _REF_STATE
+    vx, vy = st["ref"].fmm_velocity(st["x"], st["y"], st["g"], st["sigma"], k=st["k"],
+                                    xt=st["x"][lo:hi].copy(), yt=st["y"][lo:hi].copy(),
+                                    tol=1e-6, ndirect=35)
+    return lo, vx, vy
+
+
+class ReferenceStep:
+    """One step of the workload on the host with the reference's CPU code:
+    FMM velocity at every blob + Regrid of every blob."""
+
+    def __init__(self, b, procs=None):
+        import multiprocessing as mp
+        from oracle import ref
+        self.b = b
+        self.kind = "reference" if ref.available() else "port"
+        self.procs = procs or max(1, min(os.cpu_count() or 1, 64))
+        self.pool = None
+        if self.kind == "reference":
+            ctx = mp.get_context("spawn")  # no fork of a process that may hold a GPU context
+            self.pool = ctx.Pool(self.procs, initializer=_ref_worker_init,
+                                 initargs=(b.x, b.y, b.g, b.sigma, b.k))
+        edges = np.linspace(0, b.n, self.procs + 1).astype(np.int64)
+        self.chunks = [(int(edges[i]), int(edges[i + 1])) for i in range(self.procs)]
+
+    def run(self):
+        import oracle
+        b = self.b
+        xb, yb = b.bounds()
+        vx = np.empty(b.n)
+        vy = np.empty(b.n)
+        if self.pool is not None:
+            pending = self.pool.map_async(_ref_worker_chunk, self.chunks)
+            rx, ry, rg, _, _ = oracle.regrid(b.x, b.y, b.g, b.sigma, b.overlap, xb, yb)
+            for lo, cx, cy in pending.get():
+                vx[lo:lo + cx.shape[0]] = cx
+                vy[lo:lo + cy.shape[0]] = cy
+        else:  # reference not compiled here: the oracle port, all cores
+            vx, vy = oracle.velocity_direct(b.x, b.y, b.g, b.ksigmasqr, nthreads=self.procs)
+            rx, ry, rg, _, _ = oracle.regrid(b.x, b.y, b.g, b.sigma, b.overlap, xb, yb)
+        return vx, vy, rx.shape[0]
+
+    def describe(self):
+        hi = host_info()
+        if self.kind == "reference":
+            what = (f"reference C++ CPU FMM (tol 1e-6, Ndirect 35; single-threaded as built) on "
+                    f"all {self.b.n} blobs as sources, targets split over {self.procs} host "
+                    f"processes, + numpy/scipy Regrid of all blobs in the parent meanwhile")
+        else:
+            what = (f"oracle FP64 direct sum ({self.procs} threads) + numpy/scipy Regrid, all "
+                    f"{self.b.n} blobs")
+        return f"full workload every step: {what}; host {hi['nproc']} x {hi['cpu_model']}"
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.close()
+            self.pool.join()
 
 
 def run_reference(args):
-    method = "fmm" if args.method in ("auto", "fmm") else "direct"
-    for _ in range(args.warmup):
-        cpu_reference_step(method)
-    vals = []
-    desc = threads = kind = None
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        v, desc, threads, kind = cpu_reference_step(method)
-        vals.append(v)
-    wall = time.perf_counter() - t0
-    value = statistics.median(vals)
-    n = 1 << 20
+    b = workload_c2(args.n)
+    rs = ReferenceStep(b)
+    try:
+        nout = None
+        for _ in range(args.warmup):
+            _, _, nout = rs.run()
+        times = []
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            t1 = time.perf_counter()
+            _, _, nout = rs.run()
+            times.append(time.perf_counter() - t1)
+        wall = time.perf_counter() - t0
+    finally:
+        rs.close()
+    ms = statistics.mean(times) * 1e3
+    value = b.n / (ms * 1e-3)
+    cfg = workload_config(b.n, "fmm", b.sigma, args.gpus)
+    cfg["n_out_remesh"] = nout
+    hi = host_info()
     return {
-        "impl": "reference",
-        "metric": "blob velocity evals/s at <=1e-6 rel err vs FP64 (velocity + M4' remesh step)",
+        "impl": "reference", "metric": METRIC,
         "value": value, "unit": "evals/s", "n_gpus": args.gpus, "device": "host cores",
-        "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": n / value * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"single large instance: N={n} blobs U[0,1)^2, sigma=0.002, "
-                               f"velocity at all blobs ({method}) + M4' remesh h=0.8 sigma",
-                   "n_blobs": n, "method": method},
-        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": kind,
-                         "sample": desc},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded U[0,1)^2 "
+        "blobs, g~N(0,1)/N)", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": rs.procs, "kind": rs.kind,
+                         "sample": rs.describe(), "nproc": hi["nproc"], "cpu_model": hi["cpu_model"]},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "wall_s": wall,
     }
+
+
+def cpu_baseline(n=None):
+    """One full step of the reference's CPU path on this host (rank 0, N=1)."""
+    b = workload_c2(n)
+    rs = ReferenceStep(b)
+    try:
+        t0 = time.perf_counter()
+        rs.run()
+        t = time.perf_counter() - t0
+    finally:
+        rs.close()
+    hi = host_info()
+    return {"value": b.n / t, "unit": "evals/s", "cores": rs.procs, "kind": rs.kind,
+            "sample": "one step, " + rs.describe(), "ms_per_step": t * 1e3, "nproc": hi["nproc"],
+            "cpu_model": hi["cpu_model"]}
 
 
 # ---------------------------------------------------------------------------
@@ -464,12 +617,121 @@ def run_batched(dev, n_sims=256, steps=5):
     return out
 
 
+def run_c3(dev, steps=5, warmup=2):
+    """The near-wall shear-layer configuration at its stated size: N = 2^22
+    blobs in the annulus 1 <= r <= 1.5 plus 512 vortex panels on the unit
+    circle.  One step = FMM blob velocity + panel velocity added on top + the
+    M4' remesh (window found on the device).  CUDA events per phase."""
+    import torch
+    import pfblob
+    from pfblob import _lib
+    from pfblob.regrid import remesh_device_async
+    wl = workloads()
+    b = wl.shear_layer(n=1 << 22)
+    ps = wl.cylinder_panels(512)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    x, y, g = T(b.x), T(b.y), T(b.g)
+    pan = [T(a) for a in (ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina)]
+    vx, vy = torch.empty_like(x), torch.empty_like(x)
+    ks, xo, cut = pfblob.fmm_parameters(b.sigma)
+    xb, yb = b.bounds()
+    mb = int((3.1 / b.h) ** 2)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    st = torch.cuda.current_stream(dev)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(st)
+        pfblob.velocity_device(x, y, g, ks, x, y, vx, vy, method=pfblob.FMM_METHOD, xopt=xo,
+                               cutoff=cut)
+        if ev:
+            ev[1].record(st)
+        pfblob.panel_velocity_device(*pan, x, y, vx, vy, accumulate=True)
+        if ev:
+            ev[2].record(st)
+        out = remesh_device_async(x, y, g, b.h, xb[0], yb[0], max_base_cells=mb)
+        if ev:
+            ev[3].record(st)
+        return out
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    _lib.fmm_profile(True, dev.index)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
+    stats, outs = [], []
+    for k in range(steps):
+        flush.fill_(float(k))
+        outs.append(step(evs[k]))
+        stats.append(_lib.fmm_last_stats(dev.index))
+    torch.cuda.synchronize(dev)
+    _lib.fmm_profile(False, dev.index)
+    ph = {name: statistics.mean(e[i].elapsed_time(e[i + 1]) for e in evs)
+          for i, name in enumerate(("fmm", "panels", "remesh"))}
+    ms = sum(ph.values())
+    st0 = stats[-1]
+    ms_p2p = statistics.mean(f["ms_p2p"] for f in stats)
+    pk = peaks()
+    sm_clk = pk["sm_max_mhz"] * 1e6 * torch.cuda.get_device_properties(dev).multi_processor_count
+    pairs, far = st0["p2p_pairs"], st0["p2p_pairs_far"]
+    t_mufu = (MUFU_PER_INTERACTION * pairs - far) / (MUFU_PER_SM_CLK * sm_clk)
+    t_fp32 = (FP32_OPS_FULL * (pairs - far) + FP32_OPS_FAR * far) / (FP32_PER_SM_CLK * sm_clk)
+    ppairs = 512.0 * b.n
+    k_out, status = int(outs[-1][3].item()), int(outs[-1][4].item())
+    mom = outs[-1][6].cpu().numpy()
+    circ, imp = pfblob.conservation_error(mom[:4], mom[4:], float(np.abs(b.x).max()))
+    return {"workload": f"near-wall shear layer: N={b.n} blobs in 1<=r<=1.5 (h={b.h:.4e}, "
+                        "sigma=h/0.8), 512 vortex panels on the unit circle; FMM blob velocity + "
+                        "panel velocity + M4' remesh per step",
+            "n_blobs": b.n, "ms_per_step": ms, "evals_per_s": b.n / (ms * 1e-3), "phase_ms": ph,
+            "roofline_p2p": {"achieved": pairs / (ms_p2p * 1e-3) / 1e9,
+                             "peak": pairs / max(t_mufu, t_fp32) / 1e9, "unit": "Ginteractions/s",
+                             "frac": max(t_mufu, t_fp32) / (ms_p2p * 1e-3), "pairs": pairs,
+                             "pairs_far": far, "launch_ms": ms_p2p},
+            "panel_pairs_per_s": ppairs / (ph["panels"] * 1e-3),
+            "remesh": {"n_out": k_out, "status": status, "circulation": circ,
+                       "linear_impulse": imp},
+            "l2": "flushed between timed steps"}
+
+
+def run_evolve(dev, steps=10, warmup=2):
+    """A moving blob set: ``Blobs.evolve`` on the C2 blobs (forward-Euler
+    convection by the FMM velocity, redistribution and population control
+    every step, as the reference's defaults do; a free stream moves the set),
+    so the FMM box and the remesh window drift every step.  Reports the step
+    time and the FMM plans built per step after warm-up."""
+    import torch
+    import pfblob
+    from pfblob import _lib
+    b = workload_c2()
+    bl = pfblob.Blobs((b.x, b.y, b.g), vInf=[0.3, -0.2], nu=0.0, deltaTc=1e-3, h=b.h,
+                      overlap=b.overlap, timeIntegrationParams={'method': 'euler'},
+                      velocityComputationParams={'method': 'fmm', 'hardware': 'gpu'},
+                      device=dev.index)
+    for _ in range(warmup):
+        bl.evolve()
+    torch.cuda.synchronize(dev)
+    n0 = bl.numBlobs
+    p0 = _lib.fmm_plan_builds()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        bl.evolve()
+    torch.cuda.synchronize(dev)
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    return {"workload": "Blobs.evolve of the C2 set after construction-time redistribution "
+                        f"({n0} lattice blobs): FE convection (FMM velocity, free stream (0.3, -0.2), "
+                        "dt 1e-3) + redistribution + population control every step",
+            "n_blobs": int(n0), "ms_per_step": ms, "evals_per_s": n0 / (ms * 1e-3),
+            "plan_builds_per_step": (_lib.fmm_plan_builds() - p0) / steps, "steps": steps,
+            "timing": "host wall clock around evolve(), synchronised (evolve reads counts back)"}
+
+
 def run_served(dev, n_sims=1024, n_req=400, rates=(100, 1000, 5000), slots=8):
     """1024 resident simulations, N log-uniform in [1024, 2^20]; Poisson arrivals
     of velocity+remesh requests; continuous batching over `slots` worker streams
     vs one request at a time."""
     from pfblob import workloads as wl
-    from pfblob.serve import Server, Simulation, poisson_trace, summarize
+    from pfblob.serve import Server, Simulation, conservation, poisson_trace, summarize
     sizes = wl.log_uniform_sizes(n_sims, 1024, 1 << 20, config=5)
     sims = [Simulation(x, y, g, sigma=b.sigma) for b, x, y, g in _sims_on_device(sizes, 5, dev)]
     out = {"workload": f"{n_sims} resident simulations, N log-uniform [1024, 1048576] "
@@ -477,8 +739,16 @@ def run_served(dev, n_sims=1024, n_req=400, rates=(100, 1000, 5000), slots=8):
            "slots": slots, "rates": {}}
     srv = Server(sims, n_slots=slots)
     srv.warmup()
+    worst = {"circulation": 0.0, "linear_impulse": 0.0, "steps_checked": 0}
     for rate in rates:
-        out["rates"][str(rate)] = summarize(srv.run_trace(poisson_trace(n_req, rate, n_sims, seed=rate)))
+        done = srv.run_trace(poisson_trace(n_req, rate, n_sims, seed=rate))
+        out["rates"][str(rate)] = summarize(done)
+        c = conservation(done, srv.sims)
+        worst = {k: (max(worst[k], c[k]) if k != "steps_checked" else worst[k] + c[k])
+                 for k in worst}
+    out["conservation"] = dict(worst, gate=1e-12,
+                               note="FP64 moments of every served step, before and after its "
+                                    "remesh (fused into the remesh kernels)")
     srv.close()
     one = Server(sims, n_slots=1)
     one.warmup(every_sim=False)
@@ -502,6 +772,8 @@ def main():
                     help="blob count (default 2^20; smaller only for profiling captures)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-check", action="store_true",
+                    help="skip the accuracy check of the timed step against the FP64 oracle")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched (256 simulations) and served (1024 simulations) sections")
     args = ap.parse_args()
@@ -521,12 +793,12 @@ def main():
     line = run_ours(args, rank, world)
     if rank == 0 and world == 1 and not args.no_extras and args.n is None:
         dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+        line["c3"] = run_c3(dev)
+        line["evolve"] = run_evolve(dev)
         line["batched"] = run_batched(dev)
         line["served"] = run_served(dev)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, desc, threads, kind = cpu_reference_step(line["config"]["method"])
-        line["cpu_baseline"] = {"value": v, "unit": "evals/s", "cores": threads, "kind": kind,
-                                "sample": desc}
+        line["cpu_baseline"] = cpu_baseline(args.n)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

@@ -127,6 +127,15 @@ pf_status pf_velocity_fmm_box(pf_ctx *ctx, int64_t n_src, const double *x, const
                               int ndirect, const double *box, double *vx, double *vy,
                               void *stream);
 
+/* Number of FMM plans (interaction tables and operators on the device) built
+ * by this process so far.  Plans are cached by leaf level, block size,
+ * expansion order and the separation key of the cutoff / root-width ratio (the
+ * smallest well-separated squared box offset per level), so a blob set whose
+ * box drifts from step to step reuses its plan until a list changes.  No
+ * counterpart in the reference (its fmm2dInteract rebuilds its tree and lists
+ * on every call, src/cpp/blobs/c++/fmm2d_py_cpu_gpu/fmm.cpp:88-304). */
+uint64_t pf_fmm_plan_builds(void);
+
 /* Tuning of the FMM for the calling host thread (0 = automatic):
  * leaf_level in [2, 11]; expansion_terms (p+1) in {16, 20, 24, 28, 32};
  * block_level_drop in [0, 2] (P2P blocks of 2^drop x 2^drop leaves).  The
@@ -238,8 +247,11 @@ pf_status pf_dense_lu_solve(pf_ctx *ctx, int64_t m, const double *lu, const int3
  * (host pointer) receives the number of new blobs.  If capacity is too small
  * the call returns PF_ERR_CAPACITY with *n_out set to the size needed and
  * writes nothing.  ix_out / iy_out (optional, may be NULL) receive the int64
- * lattice indices.  This call synchronises `stream` twice (to read the
- * lattice extent, then the output count).  The context's scratch arena is
+ * lattice indices.  The lattice window is found on the device; the call
+ * synchronises `stream` once, at its end, to read the output count.  Its
+ * scratch is sized for the context's previous window plus 25% (at least n
+ * base cells); a larger window is detected on the device and costs one more
+ * pass on the exact window.  The context's scratch arena is
  * shared by all calls on that context: calls issued on different streams with
  * one context must be ordered by the caller.
  *
@@ -284,6 +296,62 @@ pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, const double
                            int32_t *status_dev, void *stream);
 
 /* ---------------------------------------------------------------------------
+ * Remesh with the window computed on the device and no host synchronisation
+ * (resident blob sets in stream-ordered pipelines).  The scratch is sized for
+ * windows of at most `max_base_cells` base cells (nbx nby); a larger window
+ * does nothing and sets bit 8 of the DEVICE int32 *status_dev (may be NULL);
+ * bits 1 and 2 report a NaN/Inf coordinate and a lattice index beyond
+ * +-2^30 (nothing done either).  The DEVICE int64 *n_out_dev receives the
+ * output count (0 when nothing was done; if it exceeds `capacity` nothing is
+ * written), the DEVICE int64 window_dev[4] (may be NULL) the window
+ * {ixmin, iymin, nbx, nby} of the blobs, so that a caller can retry with
+ * max_base_cells = nbx nby.  The DEVICE double moments_dev[8] (may be NULL)
+ * receives the FP64 moments {sum g, sum g x, sum g y, sum |g|} of the input
+ * blobs, then of the new blobs, each summed in a fixed order (the
+ * circulation and linear-impulse check of the step, no extra pass).  Same
+ * values and order as pf_remesh.
+ * Replaces Regrid (src/python/blobs/base/regrid/_regridding.py:36-222) for
+ * callers that keep blobs on the device, as Blobs.redistribute
+ * (src/python/blobs/__blobsClass.py:828-897) does between steps.
+ * ------------------------------------------------------------------------- */
+pf_status pf_remesh_async(pf_ctx *ctx, int64_t n, const double *x, const double *y,
+                          const double *g, double h, double xb0, double yb0, double c,
+                          int64_t max_base_cells, int64_t capacity, double *x_out, double *y_out,
+                          double *g_out, int64_t *ix_out, int64_t *iy_out, int64_t *n_out_dev,
+                          int32_t *status_dev, int64_t *window_dev, double *moments_dev,
+                          void *stream);
+
+/* ---------------------------------------------------------------------------
+ * One step of a resident blob set in one call, with no host synchronisation:
+ * the induced velocity at the blobs -- FMM on the given tree box (as
+ * pf_velocity_fmm_box, Ndirect 35, leaf level `leaf_level` or automatic) or
+ * the direct sum (as pf_velocity_direct) -- written to vx, vy, then the M4'
+ * remesh of the same blobs with the window found on the device (as
+ * pf_remesh_async: count, status word and the 8 FP64 moments to device
+ * memory).  All arrays are DEVICE arrays.  Replaces the pair of calls a
+ * stepping loop makes, Blobs.evaluateVelocity then Blobs.redistribute
+ * (src/python/blobs/__blobsClass.py:546-626, 828-897), for a serving loop that
+ * issues one call per request.
+ * ------------------------------------------------------------------------- */
+typedef struct pf_step {
+    int64_t n;                 /* blobs */
+    const double *x, *y, *g;   /* blob positions and circulations */
+    double ksigmasqr, xopt, cutoff, tol;
+    int32_t method;            /* PF_FMM_METHOD or PF_DIRECT_METHOD */
+    int32_t leaf_level;        /* 0 = automatic */
+    double box[4];             /* FMM tree box {xmin, xmax, ymin, ymax} holding the blobs */
+    double *vx, *vy;           /* velocity out, n entries */
+    double h, xb0, yb0, c;     /* remesh lattice and Wee coefficient */
+    int64_t max_base_cells;    /* remesh window bound (pf_remesh_async) */
+    int64_t capacity;          /* entries of x_out, y_out, g_out */
+    double *x_out, *y_out, *g_out;
+    int64_t *n_out_dev;        /* output count */
+    int32_t *status_dev;       /* may be NULL */
+    double *moments_dev;       /* 8 doubles, may be NULL */
+} pf_step;
+pf_status pf_blob_step(pf_ctx *ctx, const pf_step *step, void *stream);
+
+/* ---------------------------------------------------------------------------
  * pf_remesh_window without any device allocation, for callers that cannot
  * allocate: a process whose device memory is already committed to another
  * allocator (e.g. a serving loop that gives all free HBM to its own pool), or
@@ -291,13 +359,21 @@ pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, const double
  * synchronisation cudaMalloc/cudaFree can cause.  No counterpart in the
  * reference (its Regrid allocates new arrays on every call).
  *
- * Scratch is one fixed buffer of PF_NOALLOC_SCRATCH_BYTES per GPU, held from
- * library load to process exit; no pf_ctx is needed and none is created.  The
- * call works on the current device; its first call on a device looks up the
- * buffer's device address (make that first call before any stream capture).
- * Blob sets needing more scratch than the buffer holds (about 12 bytes per
- * blob plus 160 bytes per window cell) are rejected with PF_ERR_INVALID_ARG.
- * Every call shares the buffer: calls that overlap on the GPU (different
+ * Scratch is one fixed buffer of PF_NOALLOC_SCRATCH_BYTES per GPU, held until
+ * the process exits; no pf_ctx is needed and none is created.  The call works
+ * on the current device.  Its first call on a device does the set-up: it
+ * looks up the buffer's device address, and with lazy module loading (the
+ * CUDA default; CUDA_MODULE_LOADING=EAGER loads at start-up instead) that
+ * lookup loads the library's device code, which is when the driver commits
+ * the buffer's memory.  So make that first call early: before handing the
+ * device's free memory to another allocator, and before any stream capture.
+ * The address is kept per device for the process: do not use the entry point
+ * across a cudaDeviceReset.  Blob sets needing more scratch than the buffer
+ * holds (about 85 bytes per blob plus 8 bytes per base cell and 5 bytes per
+ * output cell of the window, and 66 KB) are rejected with
+ * PF_ERR_INVALID_ARG.  Every
+ * call shares the buffer, which keeps the last call's contents (the call
+ * clears what must start at zero): calls that overlap on the GPU (different
  * streams, or different host threads) race and must be serialised by the
  * caller.  Arguments and results as pf_remesh_window.
  * ------------------------------------------------------------------------- */

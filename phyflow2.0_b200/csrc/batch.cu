@@ -21,7 +21,7 @@
 
 #include "direct_api.cuh"
 #include "fmm_api.cuh"
-#include "popctl.cuh"
+#include "remesh.cuh"
 
 namespace {
 
@@ -46,6 +46,9 @@ int64_t left_index_host(double x, double b0, double h) {
     volatile double t = ((x - b0) - h2);
     t = t + h05;
     volatile double q = t / h;
+    // far outside any admissible window (the caller rejects it); keeps the
+    // conversion defined
+    if (!(std::fabs(q) < 1e15)) return q > 0 ? ((int64_t)1 << 52) : -((int64_t)1 << 52);
     return (int64_t)std::ceil(q) - 1;
 }
 
@@ -180,13 +183,18 @@ static pf_status batch_build(pf_batch *b, double tol) {
             b->iymin[i] = left_index_host(d.box[2], d.yb0, d.h);
             b->nbx[i] = left_index_host(d.box[1], d.xb0, d.h) - b->ixmin[i] + 1;
             b->nby[i] = left_index_host(d.box[3], d.yb0, d.h) - b->iymin[i] + 1;
-            if (b->nbx[i] <= 0 || b->nby[i] <= 0 ||
+            const int64_t lim = (int64_t)1 << 30;
+            if (b->nbx[i] <= 0 || b->nby[i] <= 0 || b->nbx[i] >= lim || b->nby[i] >= lim ||
+                b->ixmin[i] <= -lim || b->iymin[i] <= -lim || b->ixmin[i] + b->nbx[i] >= lim ||
+                b->iymin[i] + b->nby[i] >= lim ||
                 (b->nbx[i] + 3) * (b->nby[i] + 3) >= ((int64_t)1 << 31)) {
                 pf::set_error("pf_batch_create: instance %d remesh window invalid", i);
                 return PF_ERR_INVALID_ARG;
             }
             jobs.push_back({i, 1, 0.05 * (double)d.n,
-                            pf::remesh_scratch_bytes(d.n, b->nbx[i], b->nby[i]) + 1024});
+                            pf::remesh_scratch_bytes(d.n, b->nbx[i] * b->nby[i],
+                                                     (b->nbx[i] + 3) * (b->nby[i] + 3), false) +
+                                1024});
         }
     }
     // direct work items, largest first
@@ -273,11 +281,13 @@ static pf_status batch_enqueue(pf_batch *b) {
                 PF_TRY(pf::fmmx::plan_exec(b->plans[j.inst], sc, d.n, d.x, d.y, d.g, d.n, d.x, d.y,
                                            d.ksigmasqr, d.vx, d.vy, b->d_ctr + pf::fmmx::FMM_COUNTERS * s, nullptr, st));
             } else {
-                PF_TRY(pf::remesh_core(sc, d.n, d.x, d.y, d.g, d.h, d.xb0, d.yb0, d.c,
-                                       (int32_t)b->ixmin[j.inst], (int32_t)b->iymin[j.inst],
-                                       b->nbx[j.inst], b->nby[j.inst], d.capacity, d.x_out,
-                                       d.y_out, d.g_out, nullptr, nullptr, b->d_totals + j.inst,
-                                       b->d_bads + j.inst, st));
+                const int64_t nbx = b->nbx[j.inst], nby = b->nby[j.inst];
+                const pf::RmWindow win{false, (int32_t)b->ixmin[j.inst], (int32_t)b->iymin[j.inst],
+                                       nbx, nby, nbx * nby, (nbx + 3) * (nby + 3), 0};
+                PF_TRY(pf::remesh_core(sc, d.n, d.x, d.y, d.g, d.h, d.xb0, d.yb0, d.c, win,
+                                       d.capacity, d.x_out, d.y_out, d.g_out, nullptr, nullptr,
+                                       b->d_totals + j.inst, b->d_bads + j.inst, st,
+                                       b->ctx->num_sms));
             }
         }
         PF_CUDA_TRY(cudaEventRecord(b->events[2 + s], st));

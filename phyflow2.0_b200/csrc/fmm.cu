@@ -1262,7 +1262,8 @@ k_l2p(int64_t nt, int L, double x0, double y0, double wl, const double *__restri
 // Host: plan cache (tables + operators on the device)
 struct FmmCache {
     int L = -1, kb = -1, np = -1;
-    double ratio = -1.0;  // cutoff / root width
+    double ratio = -1.0;       // cutoff / root width the tables were built with
+    std::vector<int64_t> sep;  // separation key of those tables (fmm_plan.cuh)
     int maxpos = 0, nq = 0, nqp = 0;
     int4 *d_far = nullptr;
     int32_t *d_far_ptr = nullptr;
@@ -1322,6 +1323,8 @@ static pf_status upload(T **dst, const std::vector<T> &v, size_t &tally) {
     PF_CUDA_TRY(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
     return PF_OK;
 }
+
+static std::atomic<uint64_t> g_plan_builds{0};  // plans built in this process
 
 static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, double cutoff) {
     c.release();
@@ -1450,6 +1453,8 @@ static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, doub
     c.kb = kb;
     c.np = np;
     c.ratio = cutoff / w0;
+    pf::fmm::separation_key(L, 1.0, c.ratio, THETA, c.sep);
+    g_plan_builds.fetch_add(1, std::memory_order_relaxed);
     return PF_OK;
 }
 
@@ -1721,19 +1726,21 @@ pf_status fmm_exec(const FmmCache &c, double x0, double y0, double w0, Bump &sc,
 }
 
 // Process-wide cache of read-only plans, shared by every context and thread.
-// Tables depend on the geometry only through cutoff / root width, so plans are
-// built normalised (root width 1) and keyed by (device, L, kb, np, ratio).
+// Tables depend on the geometry only through cutoff / root width, and on that
+// ratio only through its separation key (fmm_plan.cuh), so plans are built
+// normalised (root width 1) and keyed by (device, L, kb, np, key): a moving
+// blob set whose box width drifts keeps its plan until a list changes.
 // Least recently used plans are dropped past PF_PLAN_CACHE_BYTES (env,
 // default 4 GiB); their device memory is freed when the last user lets go.
 struct PlanKey {
     int dev, L, kb, np;
-    double ratio;
+    std::vector<int64_t> sep;
     bool operator<(const PlanKey &o) const {
         if (dev != o.dev) return dev < o.dev;
         if (L != o.L) return L < o.L;
         if (kb != o.kb) return kb < o.kb;
         if (np != o.np) return np < o.np;
-        return ratio < o.ratio;
+        return sep < o.sep;
     }
 };
 struct PlanCacheStore {
@@ -1754,7 +1761,8 @@ static size_t plan_budget() {
 pf_status shared_plan(int dev, int L, int kb, int np, double ratio,
                       std::shared_ptr<FmmCache> *out) {
     PlanCacheStore &ps = plan_store();
-    const PlanKey key{dev, L, kb, np, ratio};
+    PlanKey key{dev, L, kb, np, {}};
+    pf::fmm::separation_key(L, 1.0, ratio, THETA, key.sep);
     std::lock_guard<std::mutex> lock(ps.mu);
     auto it = ps.map.find(key);
     if (it != ps.map.end()) {
@@ -1782,6 +1790,10 @@ pf_status shared_plan(int dev, int L, int kb, int np, double ratio,
 }
 
 }  // namespace pf
+
+extern "C" uint64_t pf_fmm_plan_builds(void) {
+    return g_plan_builds.load(std::memory_order_relaxed);
+}
 
 extern "C" pf_status pf_fmm_set_tuning(int leaf_level, int expansion_terms, int block_level_drop) {
     pf::clear_error();
@@ -2001,7 +2013,9 @@ void plan_free(Plan *p) {
 pf_status plan_build(Plan *p, int L, int kb, int np, double x0, double y0, double w0,
                      double cutoff, bool *p2p_ok) {
     const double ratio = cutoff / w0;
-    if (p->c.L != L || p->c.kb != kb || p->c.np != np || p->c.ratio != ratio)
+    std::vector<int64_t> sep;
+    pf::fmm::separation_key(L, 1.0, ratio, THETA, sep);
+    if (p->c.L != L || p->c.kb != kb || p->c.np != np || p->c.sep != sep)
         PF_TRY(build_cache(p->c, L, kb, np, 1.0, ratio));
     p->x0 = x0;
     p->y0 = y0;
@@ -2022,6 +2036,18 @@ pf_status plan_exec(const Plan *p, Bump &sc, int64_t ns, const double *x, const 
                     cudaEvent_t *ev, cudaStream_t st) {
     FmmArgs a{ns, nt, x, y, g, xt, yt, ksigmasqr, 0.0, 0.0, 0, vx, vy};
     return fmm_exec(p->c, p->x0, p->y0, p->w0, sc, a, ctr, ev, st);
+}
+
+void tuning_get(int *leaf_level, int *np, int *kb) {
+    *leaf_level = g_tune.leaf_level;
+    *np = g_tune.np;
+    *kb = g_tune.kb;
+}
+
+void tuning_set(int leaf_level, int np, int kb) {
+    g_tune.leaf_level = leaf_level;
+    g_tune.np = np;
+    g_tune.kb = kb;
 }
 
 int auto_level(int64_t ns, int ndirect) {

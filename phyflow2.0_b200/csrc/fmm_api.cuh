@@ -27,6 +27,9 @@ pf_status plan_exec(const Plan *p, Bump &sc, int64_t ns, const double *x, const 
 int auto_level(int64_t ns, int ndirect);
 // expansion terms for a tolerance
 int np_for_tol(double tol);
+// the calling thread's tuning (pf_fmm_set_tuning), to save and restore it
+void tuning_get(int *leaf_level, int *np, int *kb);
+void tuning_set(int leaf_level, int np, int kb);
 constexpr int MAX_LEVEL = 11;
 // device counters one FMM call writes (see exec_fmm)
 constexpr int FMM_COUNTERS = 3;

@@ -9,11 +9,32 @@
 namespace pf {
 namespace fmm {
 
-static bool well_separated(int i, int j, double w, double cutoff, double theta) {
-    const double s2 = (double)((int64_t)i * i + (int64_t)j * j);
+static bool separated_s2(int64_t k, double w, double cutoff, double theta) {
+    const double s2 = (double)k;
     const bool sep_theta = s2 * (theta * theta) >= 2.0;
     const bool sep_cut = (std::sqrt(s2) - std::sqrt(2.0)) * w >= cutoff;
     return sep_theta && sep_cut;
+}
+
+static bool well_separated(int i, int j, double w, double cutoff, double theta) {
+    return separated_s2((int64_t)i * i + (int64_t)j * j, w, cutoff, theta);
+}
+
+void separation_key(int L, double w0, double cutoff, double theta, std::vector<int64_t> &key) {
+    key.assign(L + 1, 0);
+    for (int l = 0; l <= L; ++l) {
+        const int64_t ext = ((int64_t)1 << l) - 1;
+        const double w = std::ldexp(w0, -l);
+        int64_t lo = 0, hi = 2 * ext * ext + 1;  // answer in [lo, hi]; hi: none separated
+        while (lo < hi) {
+            const int64_t mid = lo + (hi - lo) / 2;
+            if (separated_s2(mid, w, cutoff, theta))
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        key[l] = lo;
+    }
 }
 
 static int floordiv2(int a) { return (a >= 0) ? a / 2 : -((-a + 1) / 2); }

@@ -47,6 +47,13 @@ struct Tables {
 // Build every table for a tree with leaf level L.
 void build_tables(int L, int kb, double w0, double cutoff, double theta, Tables &t);
 
+// What the tables depend on: for each level l = 0..L, the smallest integer
+// s2 = i^2 + j^2 whose offsets are well separated at that level (both checks
+// are monotone in s2), or 2 (2^l - 1)^2 + 1 when none is.  Two (w0, cutoff)
+// pairs with the same key build the same tables, so plans are keyed by it
+// rather than by the exact cutoff / width ratio of a moving blob set.
+void separation_key(int L, double w0, double cutoff, double theta, std::vector<int64_t> &key);
+
 // Flattened form (int32), shared with pf_fmm_lists():
 //   L, kb, then for l = 0..L: n, (i, j) * n;
 //   then for l = 1..L: npos, for each pos: n, (i, j) * n;

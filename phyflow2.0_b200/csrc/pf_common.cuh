@@ -76,6 +76,11 @@ struct pf_ctx {
     cudaEvent_t ev[8] = {};
     cudaStream_t last_stream = nullptr;
     pf_fmm_stats last_stats = {};
+    // base cells the remesh scratch is sized for (the last window + 25%)
+    int64_t rm_cap_base = 0;
+    // row / column lists of a compressed remesh window (sparse blob sets)
+    void *rm_rows = nullptr;
+    size_t rm_rows_cap = 0;
 };
 
 namespace pf {

@@ -124,6 +124,7 @@ pf_status pf_destroy(pf_ctx *ctx) {
     if (ctx->arena.base) cudaFree(ctx->arena.base);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
     if (ctx->dev_small) cudaFree(ctx->dev_small);
+    if (ctx->rm_rows) cudaFree(ctx->rm_rows);
     for (int k = 0; k < 8; ++k)
         if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     delete ctx;

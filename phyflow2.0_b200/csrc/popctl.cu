@@ -38,12 +38,14 @@ struct Decades {
 };
 
 __global__ void __launch_bounds__(PC_THREADS)
-k_pc_loss(int64_t n, const double *__restrict__ g, const int32_t *__restrict__ flag, Decades d,
-          double limit, double *__restrict__ part, pf::PcState *__restrict__ st) {
+k_pc_loss(int64_t n, const int64_t *__restrict__ n_dev, const double *__restrict__ g,
+          const int32_t *__restrict__ flag, Decades d, double limit, double *__restrict__ part,
+          pf::PcState *__restrict__ st) {
     __shared__ double s_w[PC_THREADS / 32][PC_DECADES];
     __shared__ double s_tot[PC_DECADES];
     __shared__ int s_last;
     if (st->decided) return;  // decided by an earlier launch: same value for every CTA
+    if (n_dev) n = *n_dev;    // the value count known on the device only (n bounds it)
     const int64_t chunk = (n + PC_BLOCKS - 1) / PC_BLOCKS;
     const int64_t lo = (int64_t)blockIdx.x * chunk;
     const int64_t hi = min(n, lo + chunk);
@@ -147,7 +149,7 @@ size_t popctl_scratch_bytes() {
 }
 
 pf_status popctl_decide(Bump &sc, int64_t n, const double *g, const int32_t *flag,
-                        const PopCtlArgs &pc, cudaStream_t st) {
+                        const PopCtlArgs &pc, cudaStream_t st, const int64_t *n_dev) {
     double *part = (double *)sc.take(sizeof(double) * PC_BLOCKS * PC_DECADES);
     if (!part) {
         set_error("population control: scratch too small");
@@ -168,7 +170,8 @@ pf_status popctl_decide(Bump &sc, int64_t n, const double *g, const int32_t *fla
         }
         d.base = L * PC_DECADES;
         d.last = (L == launches - 1);
-        k_pc_loss<<<PC_BLOCKS, PC_THREADS, 0, st>>>(n, g, flag, d, pc.thr_global, part, pc.state);
+        k_pc_loss<<<PC_BLOCKS, PC_THREADS, 0, st>>>(n, n_dev, g, flag, d, pc.thr_global, part,
+                                                    pc.state);
         PF_TRY(launch_status("k_pc_loss"));
     }
     return PF_OK;

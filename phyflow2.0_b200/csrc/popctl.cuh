@@ -30,25 +30,16 @@ pf_status popctl_check(double thr_local, double thr_global, const char *who);
 size_t popctl_scratch_bytes();
 
 // Enqueue the decision over the values |g[i]| (only where flag[i] != 0 when
-// flag is non-null).  No host synchronisation.
+// flag is non-null).  No host synchronisation.  With n_dev non-null the value
+// count is *n_dev (a device int64 written by earlier work, at most n); the
+// partition of the sums over CTAs then follows *n_dev, so the decision is the
+// same as a call with that count given on the host.
 pf_status popctl_decide(Bump &sc, int64_t n, const double *g, const int32_t *flag,
-                        const PopCtlArgs &pc, cudaStream_t st);
+                        const PopCtlArgs &pc, cudaStream_t st, const int64_t *n_dev = nullptr);
 
 // flag_out[i] = (flag_in ? flag_in[i] != 0 : 1) && !(|g[i]| < state->thr).
 // flag_in and flag_out may alias.
 pf_status popctl_flags(int64_t n, const double *g, const int32_t *flag_in, const PcState *state,
                        int32_t *flag_out, cudaStream_t st);
-
-// Remesh core (remesh.cu), optionally followed by population control of the
-// remeshed cells before they are emitted.  kernel REMESH_M4: M4' weights with
-// the Wee coefficient c; REMESH_TUTTY: Tutty weights with c = hNu.
-constexpr int REMESH_M4 = 0;
-constexpr int REMESH_TUTTY = 1;
-size_t remesh_scratch_bytes(int64_t n, int64_t nbx, int64_t nby);
-pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, const double *g,
-                      double h, double xb0, double yb0, double c, int32_t ixmin, int32_t iymin,
-                      int64_t nbx, int64_t nby, int64_t capacity, double *xo, double *yo,
-                      double *go, int64_t *ixo, int64_t *iyo, int32_t *total, int32_t *bad,
-                      cudaStream_t st, const PopCtlArgs *pc = nullptr, int kernel = REMESH_M4);
 
 }  // namespace pf

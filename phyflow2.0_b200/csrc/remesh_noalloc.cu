@@ -7,7 +7,7 @@
 // that must not trigger the device-wide synchronisation that cudaMalloc and
 // cudaFree can cause.  pf_remesh and pf_remesh_window grow a per-context arena
 // with cudaMalloc; this entry point instead works inside one static device
-// buffer of PF_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds
+// buffer of PF_NOALLOC_SCRATCH_BYTES that every GPU using the library holds
 // until the process exits.  It needs no pf_ctx either (creating one allocates).
 //
 // The same kernels as pf_remesh_window run on that buffer, so results are the
@@ -15,37 +15,37 @@
 #include <cmath>
 #include <mutex>
 
-#include "popctl.cuh"
+#include "remesh.cuh"
 
 namespace {
 
 constexpr size_t NOALLOC_BYTES = (size_t)PF_NOALLOC_SCRATCH_BYTES;
-constexpr size_t NOALLOC_HEAD = 512;  // output count and status words, then the scratch
 constexpr int MAX_DEVICES = 128;
 
 // The scratch.  In host code this name is only a stand-in for the symbol: the
 // device address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
+struct DeviceSetup {
+    char *addr = nullptr;  // device address of g_noalloc_scratch in this device's context
+    int num_sms = 0;
+};
+
 std::mutex g_mu;
-void *g_addr[MAX_DEVICES] = {};
+DeviceSetup g_setup[MAX_DEVICES];
 
-__global__ void k_noalloc_finish(const int32_t *__restrict__ total,
-                                 const int32_t *__restrict__ bad, int64_t *__restrict__ n_out,
-                                 int32_t *__restrict__ status) {
-    *n_out = *total;
-    if (status) *status = *bad;
-}
-
-// Device address of the scratch on the current device, looked up once per
-// device (the first call on a device does this set-up).
-pf_status scratch_address(int device, char **out) {
+// Set-up of the current device, once per device (the first call on a device
+// does it): the device address of the scratch and the SM count.  With lazy
+// module loading (the CUDA default) the first cudaGetSymbolAddress also loads
+// the module, which is when the driver commits the buffer's memory.
+pf_status device_setup(int device, DeviceSetup *out) {
     std::lock_guard<std::mutex> lock(g_mu);
     if (device < 0 || device >= MAX_DEVICES) {
         pf::set_error("pf_remesh_window_noalloc: device %d outside [0, %d)", device, MAX_DEVICES);
         return PF_ERR_INVALID_ARG;
     }
-    if (!g_addr[device]) {
+    DeviceSetup &s = g_setup[device];
+    if (!s.addr) {
         void *p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) {
@@ -53,9 +53,17 @@ pf_status scratch_address(int device, char **out) {
                           cudaGetErrorString(e));
             return PF_ERR_CUDA;
         }
-        g_addr[device] = p;
+        int sms = 0;
+        const cudaError_t e2 = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e2 != cudaSuccess || sms <= 0) {
+            pf::set_error("pf_remesh_window_noalloc: SM count query failed: %s",
+                          cudaGetErrorString(e2));
+            return PF_ERR_CUDA;
+        }
+        s.num_sms = sms;
+        s.addr = static_cast<char *>(p);
     }
-    *out = static_cast<char *>(g_addr[device]);
+    *out = s;
     return PF_OK;
 }
 
@@ -73,7 +81,10 @@ extern "C" pf_status pf_remesh_window_noalloc(int64_t n, const double *x, const 
     PF_CHECK_ARG(h > 0.0 && h < 1e300, "pf_remesh_window_noalloc: h must be positive and finite");
     PF_CHECK_ARG(std::isfinite(xb0) && std::isfinite(yb0) && std::isfinite(c),
                  "pf_remesh_window_noalloc: bounds and c must be finite");
-    PF_CHECK_ARG(nbx > 0 && nby > 0 && nbx < ((int64_t)1 << 30) && nby < ((int64_t)1 << 30),
+    // each side below 2^30 and the output window below 2^31 cells: the byte
+    // counts below cannot overflow
+    PF_CHECK_ARG(nbx > 0 && nby > 0 && nbx < ((int64_t)1 << 30) && nby < ((int64_t)1 << 30) &&
+                     (nbx + 3) * (nby + 3) < ((int64_t)1 << 31),
                  "pf_remesh_window_noalloc: bad window %lld x %lld", (long long)nbx,
                  (long long)nby);
     PF_CHECK_ARG(ixmin > -((int64_t)1 << 30) && iymin > -((int64_t)1 << 30) &&
@@ -83,7 +94,9 @@ extern "C" pf_status pf_remesh_window_noalloc(int64_t n, const double *x, const 
     PF_CHECK_ARG(capacity >= 0 && (capacity == 0 || (x_out && y_out && g_out)),
                  "pf_remesh_window_noalloc: bad output arrays");
     PF_CHECK_ARG(n_out_dev != nullptr, "pf_remesh_window_noalloc: n_out_dev is NULL");
-    const size_t need = NOALLOC_HEAD + pf::remesh_scratch_bytes(n, nbx, nby);
+    const pf::RmWindow win{false, (int32_t)ixmin, (int32_t)iymin, nbx, nby, nbx * nby,
+                           (nbx + 3) * (nby + 3), 0};
+    const size_t need = pf::remesh_scratch_bytes(n, win.cap_base, win.cap_cell, false);
     if (need > NOALLOC_BYTES) {
         pf::set_error("pf_remesh_window_noalloc: %lld blobs on a %lld x %lld window need %zu bytes "
                       "of scratch; the fixed buffer holds %zu (use pf_remesh_window)",
@@ -92,17 +105,15 @@ extern "C" pf_status pf_remesh_window_noalloc(int64_t n, const double *x, const 
     }
     int device = -1;
     PF_CUDA_TRY(cudaGetDevice(&device));
-    char *base = nullptr;
-    PF_TRY(scratch_address(device, &base));
+    DeviceSetup ds;
+    PF_TRY(device_setup(device, &ds));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    int32_t *total = reinterpret_cast<int32_t *>(base);
-    int32_t *bad = reinterpret_cast<int32_t *>(base + 256);
-    // the buffer keeps the previous call's contents: zero what must start at zero
-    PF_CUDA_TRY(cudaMemsetAsync(base, 0, NOALLOC_HEAD, st));
-    pf::Bump sc{base + NOALLOC_HEAD, NOALLOC_BYTES - NOALLOC_HEAD, 0};
-    if (n > 0)
-        PF_TRY(pf::remesh_core(sc, n, x, y, g, h, xb0, yb0, c, (int32_t)ixmin, (int32_t)iymin, nbx,
-                               nby, capacity, x_out, y_out, g_out, ix_out, iy_out, total, bad, st));
-    k_noalloc_finish<<<1, 1, 0, st>>>(total, bad, n_out_dev, status_dev);
-    return pf::launch_status("k_noalloc_finish");
+    // the buffer keeps the previous call's contents: remesh_core zeroes what
+    // must start at zero (its head and cell counts) on the stream first
+    pf::Bump sc{ds.addr, NOALLOC_BYTES, 0};
+    pf::RmHead *hd = nullptr;
+    PF_TRY(pf::remesh_core(sc, n, x, y, g, h, xb0, yb0, c, win, capacity, x_out, y_out, g_out,
+                           ix_out, iy_out, nullptr, nullptr, st, ds.num_sms, nullptr,
+                           pf::REMESH_M4, &hd));
+    return pf::remesh_finish(hd, n_out_dev, status_dev, nullptr, nullptr, st);
 }

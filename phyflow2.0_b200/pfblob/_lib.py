@@ -59,10 +59,14 @@ PROTOTYPES = {
                                      _c.POINTER(_dbl), _vp],
     "pf_remesh_window": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _i64, _i64,
                          _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pf_remesh_async": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _vp, _vp,
+                        _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pf_blob_step": [_vp, _vp, _vp],
     "pf_remesh_window_noalloc": [_i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _i64,
                                  _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "pf_fmm_lists": [_int, _int, _dbl, _dbl, _dbl, _vp, _i64, _c.POINTER(_i64)],
     "pf_fmm_set_tuning": [_int, _int, _int],
+    "pf_fmm_plan_builds": [],
     "pf_batch_create": [_vp, _c.c_int32, _vp, _dbl, _c.c_int32, _c.POINTER(_vp)],
     "pf_batch_run": [_vp, _vp],
     "pf_batch_results": [_vp, _vp, _vp],
@@ -82,6 +86,7 @@ for _name, _args in PROTOTYPES.items():
 lib.pf_last_error.restype = _c.c_char_p
 lib.pf_version.restype = _int
 lib.pf_kernel_launches.restype = _c.c_uint64
+lib.pf_fmm_plan_builds.restype = _c.c_uint64
 
 
 class PfError(RuntimeError):
@@ -132,6 +137,11 @@ def version():
     return lib.pf_version()
 
 
+def fmm_plan_builds():
+    """Process-wide number of FMM plans built so far."""
+    return int(lib.pf_fmm_plan_builds())
+
+
 def kernel_launches():
     """Process-wide number of library kernel launches so far."""
     return int(lib.pf_kernel_launches())
@@ -173,3 +183,15 @@ class BatchInstance(_c.Structure):
                 ("expansion_terms", _c.c_int32), ("remesh", _c.c_int32), ("h", _c.c_double),
                 ("xb0", _c.c_double), ("yb0", _c.c_double), ("c", _c.c_double),
                 ("capacity", _c.c_int64), ("x_out", _vp), ("y_out", _vp), ("g_out", _vp)]
+
+
+class Step(_c.Structure):
+    """Mirror of pf_step (include/pfblob.h)."""
+    _fields_ = [("n", _c.c_int64), ("x", _vp), ("y", _vp), ("g", _vp),
+                ("ksigmasqr", _c.c_double), ("xopt", _c.c_double), ("cutoff", _c.c_double),
+                ("tol", _c.c_double), ("method", _c.c_int32), ("leaf_level", _c.c_int32),
+                ("box", _c.c_double * 4), ("vx", _vp), ("vy", _vp), ("h", _c.c_double),
+                ("xb0", _c.c_double), ("yb0", _c.c_double), ("c", _c.c_double),
+                ("max_base_cells", _c.c_int64), ("capacity", _c.c_int64), ("x_out", _vp),
+                ("y_out", _vp), ("g_out", _vp), ("n_out_dev", _vp), ("status_dev", _vp),
+                ("moments_dev", _vp)]

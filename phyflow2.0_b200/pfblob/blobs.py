@@ -223,14 +223,7 @@ class Blobs:
         integrator = FE_INTEGRATOR if self.integrationMethod == 'euler' else RK4_INTEGRATOR
         self._x, self._y = convection_device(self.deltaTc, self._x, self._y, self._g, self.sigma,
                                              2.0, self.vInf, self._method(), integrator)
-        if self.diffusionParams['method'] == 'regrid_tutty':
-            # __blobsClass.py:1073-1111: redistribute, then Tutty's diffusive
-            # redistribution, every step (hNu = 0 when nu = 0)
-            self.redistribute()
-            if self.numBlobs > 0:
-                self._regrid(0.0, tutty_hnu=float(np.sqrt(self.deltaTd * self.nu)))
-        elif self.stepDiffusion != 0 and (self.tStep % self.stepDiffusion) == 0:
-            self._regrid(math.sqrt(self.nu * self.deltaTd) / self.h)
+        self._diffusion()
         redistribute = self.stepRedistribution != 0 and (self.tStep % self.stepRedistribution) == 0
         control = (self.stepPopulationControl != 0 and
                    ((self.tStep + 1) % self.stepPopulationControl) == 0)
@@ -241,10 +234,27 @@ class Blobs:
             self._regrid(0.0, population_control=True)
         elif redistribute:
             self.redistribute()
-        self._tStep += 1
-        self._t = self.deltaTc * self._tStep  # as the reference's _advanceTime, not a running sum
+        self._advanceTime()
         if control and not fused:
             self.populationControl()
+
+    def _diffusion(self):
+        """Diffusion step (__blobsClass.py:1002-1111): Wee's diffusive remesh
+        every stepDiffusion steps, or -- with 'regrid_tutty' -- a
+        redistribution followed by Tutty's diffusive redistribution, every
+        call (hNu = 0 when nu = 0)."""
+        if self.diffusionParams['method'] == 'regrid_tutty':
+            self.redistribute()
+            if self.numBlobs > 0:
+                self._regrid(0.0, tutty_hnu=float(np.sqrt(self.deltaTd * self.nu)))
+        elif self.stepDiffusion != 0 and (self.tStep % self.stepDiffusion) == 0:
+            self._regrid(math.sqrt(self.nu * self.deltaTd) / self.h)
+
+    def _advanceTime(self):
+        """tStep + 1 and t = deltaTc * tStep, as the reference's _advanceTime
+        (a product, not a running sum)."""
+        self._tStep += 1
+        self._t = self.deltaTc * self._tStep
 
     def addBlobs(self, xNew, yNew, gNew):
         self._x = torch.cat([self._x, self._dev(xNew)])

@@ -66,6 +66,44 @@ def remesh_device(x, y, g, h, xb0, yb0, c=0.0, capacity=None, with_indices=False
         return out
 
 
+def remesh_device_async(x, y, g, h, xb0, yb0, c=0.0, max_base_cells=None, capacity=None,
+                        with_indices=False, stream=None):
+    """Remesh with the lattice window found on the device and no host
+    synchronisation (pf_remesh_async).  Returns (x, y, g[, ix, iy], n_out,
+    status, window, moments): outputs of ``capacity`` entries (default: the
+    output cells of a window of ``max_base_cells``), and CUDA tensors with the
+    output count, the status word (0 = done; 8 = the window exceeded
+    ``max_base_cells``: retry with ``window[2] * window[3]``), the window
+    {ixmin, iymin, nbx, nby} and the FP64 moments {sum g, sum g x, sum g y,
+    sum |g|} of the input blobs then of the new blobs (8 values; see
+    ``conservation_error``).  ``max_base_cells`` defaults to 4 n."""
+    n = x.numel()
+    dev = x.device
+    require(n, dev, x=x, y=y, g=g)
+    st = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream if stream is None else stream)
+    ctx = _lib.context(dev.index)
+    mb = int(max_base_cells) if max_base_cells is not None else max(4 * n, 4096)
+    if capacity is None:
+        capacity = mb + mb // 2 + 65536
+    xo = torch.empty(capacity, dtype=torch.float64, device=dev)
+    yo = torch.empty(capacity, dtype=torch.float64, device=dev)
+    go = torch.empty(capacity, dtype=torch.float64, device=dev)
+    ixo = torch.empty(capacity, dtype=torch.int64, device=dev) if with_indices else None
+    iyo = torch.empty(capacity, dtype=torch.int64, device=dev) if with_indices else None
+    nout = torch.zeros(1, dtype=torch.int64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    window = torch.zeros(4, dtype=torch.int64, device=dev)
+    moments = torch.zeros(8, dtype=torch.float64, device=dev)
+    _lib.check(_lib.lib.pf_remesh_async(ctx, n, ptr(x), ptr(y), ptr(g), float(h), float(xb0),
+                                        float(yb0), float(c), mb, capacity, ptr(xo), ptr(yo),
+                                        ptr(go), ptr(ixo), ptr(iyo), ptr(nout), ptr(status),
+                                        ptr(window), ptr(moments), st))
+    out = (xo, yo, go)
+    if with_indices:
+        out = out + (ixo, iyo)
+    return out + (nout, status, window, moments)
+
+
 def lattice_window(box, h, xb0, yb0):
     """Base-cell window (ixmin, iymin, nbx, nby) holding every blob inside
     box = (xmin, xmax, ymin, ymax): the remesh's window-left index
@@ -154,3 +192,34 @@ def Regrid(xBlob, yBlob, wBlob, sigma, overlap, xBounds, yBounds, interpKernel=0
     yb0 = float(np.asarray(yBounds)[0]) if not isinstance(yBounds, torch.Tensor) else float(yBounds[0])
     xn, yn, gn = remesh_device(x, y, g, h, xb0, yb0, c)
     return m.outs(xn, yn, gn)
+
+
+def velocity_and_regrid(xBlob, yBlob, wBlob, sigma, overlap, xBounds, yBounds, k=2, method=0,
+                        Ndirect=35, tol=1.0e-6, cutoff=None, c=0.0):
+    """One blob step's two hot calls from a single upload: the induced
+    velocity at the blobs (``velocity(xBlob, yBlob, wBlob, sigma, k, ...,
+    method, Ndirect, tol, cutoff)``) and the redistribution
+    ``Regrid(xBlob, yBlob, wBlob, sigma, overlap, xBounds, yBounds, 0, c)``
+    of the same blobs, as a caller of both would make them (the reference's
+    ``Blobs.evaluateVelocity`` then ``Blobs.redistribute``,
+    ``src/python/blobs/__blobsClass.py:546-626, 828-897``).  Returns
+    ``(vx, vy, x_new, y_new, g_new)``; numpy (or CPU tensor) input is copied to
+    the device once, and the results come back with one synchronisation."""
+    from .induced import FMM_METHOD, DIRECT_METHOD, fmm_parameters, velocity_device
+    if method not in (FMM_METHOD, DIRECT_METHOD):
+        raise ValueError(f"pfblob: unknown method {method}")
+    m = Marshal(xBlob.device.index if isinstance(xBlob, torch.Tensor) and xBlob.is_cuda else None)
+    x, y, g = m.dev(xBlob), m.dev(yBlob), m.dev(wBlob)
+    if not (x.numel() == y.numel() == g.numel()):
+        raise ValueError("pfblob: xBlob, yBlob, wBlob must have the same length")
+    vx, vy = m.empty(x.numel()), m.empty(x.numel())
+    ksigmasqr, xopt, cut = fmm_parameters(float(sigma), float(k), cutoff, float(tol))
+    velocity_device(x, y, g, ksigmasqr, x, y, vx, vy, method=method, xopt=xopt, cutoff=cut,
+                    tol=float(tol), ndirect=int(Ndirect), device=m.index)
+    if x.numel() < 1:
+        return m.outs(vx, vy, x, y, g)
+    h = sigma * overlap
+    xb0 = float(np.asarray(xBounds)[0]) if not isinstance(xBounds, torch.Tensor) else float(xBounds[0])
+    yb0 = float(np.asarray(yBounds)[0]) if not isinstance(yBounds, torch.Tensor) else float(yBounds[0])
+    xn, yn, gn = remesh_device(x, y, g, h, xb0, yb0, c)
+    return m.outs(vx, vy, xn, yn, gn)

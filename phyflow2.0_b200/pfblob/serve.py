@@ -19,6 +19,7 @@ runs beside it.
 
 The reference has no counterpart (one blob set per call, synchronous).
 """
+import ctypes
 import math
 import queue
 import threading
@@ -30,7 +31,7 @@ import torch
 
 from . import _lib
 from .induced import DIRECT_METHOD, FMM_METHOD, fmm_parameters, velocity_device
-from .regrid import lattice_window, remesh_device, remesh_window_device
+from .regrid import lattice_window, remesh_device, remesh_device_async
 from .tune import Tuner
 
 # scratch bytes per blob of one step (FMM arrays + remesh arrays), measured
@@ -75,6 +76,8 @@ class Request:
     slot: int = -1
     claim: int = 0
     result: dict = field(default_factory=dict)
+    moments: object = None  # FP64 {sum g, sum g x, sum g y, sum |g|} before, after (device)
+    idx: int = 0            # position in its trace (row of the server's moment pool)
     error: str = ""
 
     @property
@@ -106,6 +109,13 @@ class Server:
         self._claimed = 0                    # bytes of growth claimed by admitted requests
         self._queues = [queue.Queue() for _ in range(n_slots)]
         self._done = []
+        # per-slot device buffers of the lean path (one pf_blob_step per
+        # request): velocity and remesh outputs sized for the largest
+        # simulation, the count and status words; step descriptors per
+        # (slot, simulation), built on first use
+        self._slot_buf = [None] * n_slots
+        self._desc = {}
+        self._mom = torch.zeros((0, 8), dtype=torch.float64, device=self.device)
         self._threads = [threading.Thread(target=self._worker, args=(i,), daemon=True)
                          for i in range(n_slots)]
         for t in self._threads:
@@ -166,11 +176,72 @@ class Server:
                 self._done.append(req)
                 self._lock.notify_all()
 
+    def _bound(self, s, moved):
+        nbx, nby = s.window[2], s.window[3]
+        b = (nbx + 16) * (nby + 16)
+        return 4 * b if moved else b
+
+    def _slot_buffers(self, slot, need_n=0, need_cap=0):
+        """The slot's buffers, (re)allocated when a simulation outgrows them.
+        Called by the slot's own worker between requests (its stream idle),
+        so replaced buffers are no longer in use; the slot's descriptors
+        pointing at them are dropped."""
+        b = self._slot_buf[slot]
+        if b is not None and (len(b["vx"]) < need_n or b["cap"] < need_cap):
+            for key in [k for k in self._desc if k[0] == slot]:
+                self._desc.pop(key, None)
+            b = None
+        if b is None:
+            nmax = max(max(s.n for s in self.sims), need_n)
+            cmax = max(max(self._bound(s, False) * 3 // 2 + 65536 for s in self.sims if s.n),
+                       need_cap)
+            f64 = dict(dtype=torch.float64, device=self.device)
+            b = {"vx": torch.empty(nmax, **f64), "vy": torch.empty(nmax, **f64),
+                 "out": torch.empty((3, cmax), **f64), "cap": cmax,
+                 "nout": torch.zeros(1, dtype=torch.int64, device=self.device),
+                 "status": torch.zeros(1, dtype=torch.int32, device=self.device)}
+            self._slot_buf[slot] = b
+        return b
+
+    def _descriptor(self, slot, sim):
+        """pf_step of simulation `sim` on slot `slot` (cached; rebuilt when
+        the simulation's state is replaced)."""
+        s = self.sims[sim]
+        b = self._slot_buffers(slot, s.n, self._bound(s, False) * 3 // 2 + 65536)
+        key = (slot, sim, s.x.data_ptr(), s.n)
+        d = self._desc.get(key)
+        if d is None:
+            ks, xo, cut = fmm_parameters(s.sigma, s.k, tol=self.tol)
+            h = s.h
+            d = _lib.Step()
+            d.n, d.x, d.y, d.g = s.n, s.x.data_ptr(), s.y.data_ptr(), s.g.data_ptr()
+            d.ksigmasqr, d.xopt, d.cutoff, d.tol = ks, xo, cut, self.tol
+            d.method, d.leaf_level = s.method, s.leaf_level if s.method == FMM_METHOD else 0
+            for i, v in enumerate(self._box(s)):
+                d.box[i] = v
+            d.vx, d.vy = b["vx"].data_ptr(), b["vy"].data_ptr()
+            d.h, d.xb0, d.yb0, d.c = h, -1.5 * h, -1.5 * h, s.c
+            d.max_base_cells, d.capacity = self._bound(s, False), b["cap"]
+            o = b["out"]
+            d.x_out, d.y_out, d.g_out = o[0].data_ptr(), o[1].data_ptr(), o[2].data_ptr()
+            d.n_out_dev, d.status_dev = b["nout"].data_ptr(), b["status"].data_ptr()
+            self._desc[key] = d
+        return d
+
     def _step(self, req):
         """Enqueue one step on the current stream.  With the blob box known
         (resident state, no move) nothing here waits for the device: the FMM
-        takes the cached box and the remesh the cached lattice window."""
+        takes the cached box and the remesh finds its window on the device;
+        such a step is one pf_blob_step call into slot buffers."""
         s = self.sims[req.sim]
+        if req.dt == 0.0 and not (self.keep or req.update) and s.n:
+            d = self._descriptor(req.slot, req.sim)
+            d.moments_dev = self._mom[req.idx].data_ptr()
+            st = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+            _lib.check(_lib.lib.pf_blob_step(_lib.context(self.device.index), ctypes.byref(d), st))
+            req.n = s.n
+            req.moments = self._mom[req.idx]
+            return
         ks, xo, cut = fmm_parameters(s.sigma, s.k, tol=self.tol)
         vx = torch.empty_like(s.x)
         vy = torch.empty_like(s.x)
@@ -180,19 +251,24 @@ class Server:
         velocity_device(s.x, s.y, s.g, ks, s.x, s.y, vx, vy, method=s.method, xopt=xo, cutoff=cut,
                         tol=self.tol, box=box)
         h = s.h
-        if req.dt == 0.0 and box is not None:
-            xn, yn, gn, nout = remesh_window_device(s.x, s.y, s.g, h, -1.5 * h, -1.5 * h,
-                                                    s.window, s.c)
-            if self.keep or req.update:
-                k = int(nout.item())
+        xm, ym = s.x, s.y
+        if req.dt != 0.0:
+            xm = s.x + req.dt * vx
+            ym = s.y + req.dt * vy
+        # remesh with the window found on the device (bounded by the resident
+        # set's window with a margin for moved blobs) and the FP64 moments of
+        # the blobs before and after (the step's circulation and impulse check)
+        xn, yn, gn, nout, status, win, mom = remesh_device_async(
+            xm, ym, s.g, h, -1.5 * h, -1.5 * h, s.c, max_base_cells=self._bound(s, req.dt != 0.0))
+        if req.dt != 0.0 or self.keep or req.update:
+            k, st = int(nout.item()), int(status.item())
+            if st:  # moved past the bound: the synchronous remesh finds any window
+                xn, yn, gn = remesh_device(xm, ym, s.g, h, -1.5 * h, -1.5 * h, s.c)
+                mom = None
+            else:
                 xn, yn, gn = xn[:k], yn[:k], gn[:k]
-        else:
-            xm, ym = s.x, s.y
-            if req.dt != 0.0:
-                xm = s.x + req.dt * vx
-                ym = s.y + req.dt * vy
-            xn, yn, gn = remesh_device(xm, ym, s.g, h, -1.5 * h, -1.5 * h, s.c)
         req.n = s.n
+        req.moments = mom
         if self.keep:
             req.result = {"vx": vx, "vy": vy, "x": xn, "y": yn, "g": gn}
         if req.update:
@@ -225,6 +301,8 @@ class Server:
         """Replay (t_offset_seconds, sim_id) arrivals in real time; returns the
         completed requests in completion order."""
         trace = sorted(trace)
+        if self._mom.shape[0] < len(trace):  # a moment row per request of the trace
+            self._mom = torch.zeros((len(trace), 8), dtype=torch.float64, device=self.device)
         t0 = time.perf_counter()
         pending = []
         reqs = []
@@ -235,7 +313,8 @@ class Server:
         while True:
             now = time.perf_counter()
             while i < len(trace) and t0 + trace[i][0] <= now:
-                r = Request(sim=int(trace[i][1]), t_arrival=t0 + trace[i][0], dt=dt, update=update)
+                r = Request(sim=int(trace[i][1]), t_arrival=t0 + trace[i][0], dt=dt, update=update,
+                            idx=i)
                 pending.append(r)
                 reqs.append(r)
                 i += 1
@@ -267,6 +346,24 @@ def poisson_trace(n_requests, rate, n_sims, seed=0):
     t = np.cumsum(rng.exponential(1.0 / rate, n_requests))
     sims = rng.integers(0, n_sims, n_requests)
     return list(zip(t.tolist(), sims.tolist()))
+
+
+def conservation(done, sims):
+    """Largest relative circulation and linear-impulse change over the served
+    steps (FP64 moments from the remesh, read after the trace; impulse
+    normalised by sum |g| times the largest coordinate of the blobs)."""
+    circ = imp = 0.0
+    checked = 0
+    for r in done:
+        if r.error or r.moments is None:
+            continue
+        m = r.moments.cpu().tolist()
+        den = m[3] if m[3] > 0 else 1.0
+        sc = max(abs(v) for v in sims[r.sim].box) if sims[r.sim].box else 1.0
+        circ = max(circ, abs(m[4] - m[0]) / den)
+        imp = max(imp, max(abs(m[5] - m[1]), abs(m[6] - m[2])) / (den * (sc or 1.0)))
+        checked += 1
+    return {"circulation": circ, "linear_impulse": imp, "steps_checked": checked}
 
 
 def summarize(done, t_span=None):

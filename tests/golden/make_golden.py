@@ -244,6 +244,15 @@ def regrid_fixtures(refroot):
         xn, yn, gn = R.Regrid(x, y, g, sigma, 0.8, xb, xb, 0, c)
         np.savez_compressed(os.path.join(HERE, f"regrid_rand_{tag}.npz"), x=x, y=y, g=g,
                             sigma=sigma, overlap=0.8, xb=xb, yb=xb, c=c, xn=xn, yn=yn, gn=gn)
+    # a sparse set: the same blobs plus a few far from them (the dense lattice
+    # window would hold ~1e11 cells)
+    xf = np.concatenate([x, np.array([2000.0, 2000.0013, -1500.25, 3.0])])
+    yf = np.concatenate([y, np.array([-0.2, -0.2021, 1800.5, -2500.0])])
+    gf = np.concatenate([g, np.array([0.5, -0.25, 1.0, 2.0]) / 2000])
+    xb = np.array([-1.5 * h, 1.5 * h])
+    xn, yn, gn = R.Regrid(xf, yf, gf, sigma, 0.8, xb, xb, 0, 0.0)
+    np.savez_compressed(os.path.join(HERE, "regrid_far.npz"), x=xf, y=yf, g=gf, sigma=sigma,
+                        overlap=0.8, xb=xb, yb=xb, c=0.0, xn=xn, yn=yn, gn=gn)
 
 
 

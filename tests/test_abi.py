@@ -60,7 +60,7 @@ def test_null_context_is_rejected_without_gpu():
     assert b"NULL context" in L.lib.pf_last_error()
 
 
-NO_STATUS = {"pf_last_error", "pf_version", "pf_kernel_launches"}
+NO_STATUS = {"pf_last_error", "pf_version", "pf_kernel_launches", "pf_fmm_plan_builds"}
 NULL_IS_NOOP = {"pf_destroy", "pf_batch_destroy"}  # like free(NULL)
 ZEROS_VALID = {"pf_fmm_set_tuning"}  # 0 = automatic choice of every knob
 
@@ -149,3 +149,59 @@ def test_batch_rejects_non_finite_remesh_arguments_without_gpu(field):
     out = ctypes.c_void_p()
     assert L.lib.pf_batch_create(dummy_ctx, 1, inst, 1e-6, 1, ctypes.byref(out)) == 1
     assert "bad remesh arguments" in L.lib.pf_last_error().decode()
+
+
+def test_noalloc_rejects_window_whose_cell_count_overflows_without_gpu():
+    """Each window side below 2^30 but (nbx + 3)(nby + 3) far above 2^31: the
+    scratch size would wrap; the argument check rejects the window before any
+    CUDA call."""
+    import pfblob._lib as L
+    dummy = ctypes.c_void_p(16)  # never dereferenced: the checks fail first
+    s = L.lib.pf_remesh_window_noalloc(4, dummy, dummy, dummy, 0.01, 0.0, 0.0, 0.0, 0, 0,
+                                       847355459, 143221333, 0, None, None, None, None, None,
+                                       dummy, None, None)
+    assert s == 1 and b"bad window" in L.lib.pf_last_error()
+    s = L.lib.pf_remesh_window(dummy, 4, dummy, dummy, dummy, 0.01, 0.0, 0.0, 0.0, 0, 0,
+                               847355459, 143221333, 0, None, None, None, None, None, dummy,
+                               None, None)
+    assert s == 1 and b"bad window" in L.lib.pf_last_error()
+
+
+def test_async_remesh_checks_its_bound_without_gpu():
+    import pfblob._lib as L
+    dummy = ctypes.c_void_p(16)
+    for mb in (0, 1 << 30):
+        s = L.lib.pf_remesh_async(dummy, 4, dummy, dummy, dummy, 0.01, 0.0, 0.0, 0.0, mb, 0, None,
+                                  None, None, None, None, dummy, None, None, None, None)
+        assert s == 1 and b"max_base_cells" in L.lib.pf_last_error()
+
+
+@pytest.mark.parametrize("struct,mirror", [("pf_step", "Step"),
+                                           ("pf_batch_instance", "BatchInstance"),
+                                           ("pf_fmm_stats", "FmmStats")])
+def test_struct_mirrors_match_the_header_layout(tmp_path, struct, mirror):
+    """The ctypes mirrors have the header's size and field offsets (checked by
+    compiling the header with the host C compiler)."""
+    import shutil
+    import subprocess
+    import pfblob._lib as L
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    m = getattr(L, mirror)
+    fields = [f for f, _ in m._fields_]
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pfblob.h"', 'int main(void) {',
+             f'  printf("%zu\\n", sizeof({struct}));']
+    lines += [f'  printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    lines += ['  return 0;', '}']
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    inc = ["-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include"]
+    r = subprocess.run([cc, *inc, str(src), "-o", str(exe)], capture_output=True, text=True)
+    if r.returncode != 0:
+        pytest.skip("header does not compile with the host compiler here: " + r.stderr[-300:])
+    out = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    assert out[0] == ctypes.sizeof(m)
+    assert out[1:] == [getattr(m, f).offset for f in fields]

@@ -95,3 +95,34 @@ def test_autotuner_prefers_direct_for_small_and_fmm_for_large():
     t = Tuner(0)
     assert t.choose(2000, 2 * 0.005 ** 2, (-1, 1, -1, 1))[0] == 1
     assert t.choose(1 << 20, 2 * 0.002 ** 2, (0, 1, 0, 1))[0] == 0
+
+
+def test_batch_of_256_simulations_equals_alone_and_oracle():
+    """The batched configuration at its stated size: 256 simulations, N
+    log-uniform in [2048, 262144] (Lamb-Oseen + uniform mix, sigma in
+    [0.002, 0.01]).  Every simulation's velocity and remesh equal its
+    single-simulation calls bitwise; eight of them (both methods) are within
+    1e-6 of the FP64 oracle."""
+    from pfblob import workloads as wl
+    from pfblob.batch import Batch
+    sizes = wl.log_uniform_sizes(256, 2048, 262144, config=4)
+    sims = make_sims(sizes)
+    bt = Batch(sims, tol=1e-6, n_streams=8)
+    bt.run()
+    res = bt.results()
+    methods = [r["method"] for r in bt.sims]
+    assert 0 in methods and 1 in methods
+    for s, r in zip(sims, res):
+        assert r["status"] == 0
+        vx, vy, xn, yn, gn = alone(s, r["method"], r["leaf_level"])
+        assert torch.equal(vx, r["vx"]) and torch.equal(vy, r["vy"])
+        assert torch.equal(xn, r["x"]) and torch.equal(yn, r["y"]) and torch.equal(gn, r["g"])
+    picks = [i for i, m in enumerate(methods) if m == 0][:4] + \
+            [i for i, m in enumerate(methods) if m == 1][:4]
+    for i in picks:
+        b = sims[i]["blob"]
+        idx = np.random.default_rng(i).choice(b.n, min(b.n, 1000), replace=False)
+        rx, ry = oracle.velocity_direct(b.x, b.y, b.g, b.ksigmasqr, b.x[idx], b.y[idx])
+        assert normwise_err(res[i]["vx"].cpu().numpy()[idx], res[i]["vy"].cpu().numpy()[idx],
+                            rx, ry) <= 1e-6, (i, methods[i])
+    bt.close()

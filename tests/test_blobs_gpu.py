@@ -110,3 +110,33 @@ def test_tutty_diffusion_step_matches_reference_sequence():
     # the stability bound hNu/h <= 1/sqrt(2) is enforced as in the reference
     with pytest.raises(ValueError):
         pfblob.Blobs((c1.x, c1.y, c1.g), **dict(kw, deltaTc=1.0))
+
+
+@pytest.mark.parametrize("method", ["direct", "fmm"])
+def test_evolve_rk4_step_matches_reference_integrator(method):
+    """Blobs with the RK4 integrator: one evolve equals the reference's RK4
+    loop (_evolution.py:668-693: four stages, all evaluated at the start
+    positions since its stage increment stays zero, each adding
+    w_k (v + vInf) dt in the reference's order), with the velocity from the
+    FP64 oracle; displacements within 1e-6 normwise."""
+    import pfblob
+    from pfblob import workloads as wl
+    c1 = wl.lamb_oseen_lattice()
+    dt, vinf = 0.01, (0.1, -0.05)
+    b = pfblob.Blobs((c1.x, c1.y, c1.g), vInf=list(vinf), nu=0.0, deltaTc=dt, h=c1.h,
+                     overlap=0.8, timeIntegrationParams={'method': 'rk4'},
+                     velocityComputationParams={'method': method, 'hardware': 'gpu'},
+                     blobControlParams={'stepRedistribution': 0, 'stepPopulationControl': 0,
+                                        'gThresholdLocal': 1e-8, 'gThresholdGlobal': 1e-8})
+    x0, y0, g0 = b.x, b.y, b.g
+    b.evolve()
+    vx, vy = oracle.velocity_direct(x0, y0, g0, 2 * b.sigma ** 2)
+    xr, yr = x0.copy(), y0.copy()
+    for w in np.array([1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0]):
+        xr += w * (vx + vinf[0]) * dt
+        yr += w * (vy + vinf[1]) * dt
+    d = np.sqrt(((b.x - x0) - (xr - x0)) ** 2 + ((b.y - y0) - (yr - y0)) ** 2)
+    ref = np.sqrt((xr - x0) ** 2 + (yr - y0) ** 2)
+    assert d.max() <= 1e-6 * ref.max()
+    assert np.array_equal(b.g, g0)  # circulations unchanged by convection
+    assert b.tStep == 1 and abs(b.t - dt) < 1e-15

@@ -184,3 +184,24 @@ def test_stats_pair_counts():
     assert 0 < st["p2p_pairs_far"] < st["p2p_pairs"]
     assert st["m2l_translations"] > 0
     assert n <= st["p2p_pairs"] <= n * n  # each blob meets at least itself
+
+
+def test_plan_reused_while_the_box_drifts():
+    """A blob set that moves a little every step (its box width drifting by
+    about 1e-4) keeps its FMM plan: plans are keyed by the separation key of
+    cutoff / width, not by the exact ratio.  Results stay within the gate."""
+    import pfblob
+    from pfblob import _lib
+    from pfblob import workloads as wl
+    b = wl.uniform_square(n=65536, sigma=0.004, config=2, instance=21)
+    fmm(b.x, b.y, b.g, b.sigma)  # builds (or finds) the plan
+    n0 = _lib.fmm_plan_builds()
+    rng = np.random.default_rng(1)
+    for step in range(8):
+        s = 1.0 + 1e-4 * rng.uniform(-1.0, 1.0)
+        x, y = 0.5 + (b.x - 0.5) * s, 0.5 + (b.y - 0.5) * s
+        vx, vy = fmm(x, y, b.g, b.sigma)
+    assert _lib.fmm_plan_builds() - n0 <= 1
+    idx = np.arange(0, b.n, 97)
+    rx, ry = oracle.velocity_direct(x, y, b.g, 2 * b.sigma ** 2, x[idx], y[idx])
+    assert normwise_err(vx[idx], vy[idx], rx, ry) <= TOL

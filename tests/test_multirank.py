@@ -62,3 +62,13 @@ def test_reference_arm_line_on_rank0():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
     assert d["config"]["n_blobs"] == 1 << 20
     assert "velocity at all blobs" in d["config"]["workload"]
+
+
+def test_reference_arm_does_not_load_the_library():
+    """The reference arm's workload comes from the generator file alone: the
+    pfblob package (whose import loads libpfblob.so) is never imported."""
+    code = ("import sys; sys.argv=['bench.py']; import bench; b = bench.workload_c2(4096); "
+            "assert b.n == 4096; assert 'pfblob' not in sys.modules, sorted(sys.modules)")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]

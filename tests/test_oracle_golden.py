@@ -35,7 +35,7 @@ def test_panel_bit_exact(golden):
 
 
 def test_regrid_matches_reference_regrid(golden):
-    for name in ("regrid_c1", "regrid_rand_c0", "regrid_rand_c3"):
+    for name in ("regrid_c1", "regrid_rand_c0", "regrid_rand_c3", "regrid_far"):
         r = golden(name)
         xn, yn, gn, ix, iy = oracle.regrid(r["x"], r["y"], r["g"], float(r["sigma"]),
                                            float(r["overlap"]), r["xb"], r["yb"], float(r["c"]))

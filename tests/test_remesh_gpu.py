@@ -17,8 +17,11 @@ def _regrid_gpu(x, y, g, sigma, overlap, xb, yb, c=0.0):
     return pfblob.Regrid(x, y, g, sigma, overlap, xb, yb, 0, c)
 
 
-@pytest.mark.parametrize("name", ["regrid_c1", "regrid_rand_c0", "regrid_rand_c3"])
+@pytest.mark.parametrize("name", ["regrid_c1", "regrid_rand_c0", "regrid_rand_c3", "regrid_far"])
 def test_vs_reference_regrid_golden(golden, name):
+    """regrid_far: four blobs thousands of units from the other 2000, so that
+    the dense lattice window would hold ~1e11 cells; the remesh then runs on
+    the window compressed to the lattice rows and columns the blobs touch."""
     r = golden(name)
     xn, yn, gn = _regrid_gpu(r["x"], r["y"], r["g"], float(r["sigma"]), float(r["overlap"]),
                              r["xb"], r["yb"], float(r["c"]))
@@ -193,5 +196,55 @@ def test_wee_diffusion_matches_remesh_with_c():
     xn, yn, gn = pfblob.diffusion_wee(dt, nu, h, x, y, g, sigma, b, b, overlap=ov)
     c = np.sqrt(nu * dt) / h
     rx, ry, rg, _, _ = oracle.regrid(x, y, g, sigma, ov, b, b, c)
+    assert np.array_equal(xn, rx) and np.array_equal(yn, ry)
+    assert np.abs(gn - rg).max() <= GTOL * np.abs(rg).max()
+
+
+def test_async_remesh_equals_remesh_and_reports_its_window():
+    """pf_remesh_async (window found on the device, no host synchronisation)
+    gives bitwise the pf_remesh result; a bound below the blobs' window does
+    nothing, sets status bit 8 and returns the window, and the retry with
+    that window's size succeeds."""
+    import pfblob
+    from pfblob import workloads as wl
+    from pfblob.regrid import lattice_window, remesh_device_async
+    b = wl.mixed_instance(100000, config=4, instance=5)
+    dev = torch.device("cuda", 0)
+    x, y, g = (torch.from_numpy(a).to(dev) for a in (b.x, b.y, b.g))
+    xb, yb = b.bounds()
+    ref = pfblob.remesh_device(x, y, g, b.h, xb[0], yb[0], with_indices=True)
+    box = (b.x.min(), b.x.max(), b.y.min(), b.y.max())
+    win = lattice_window(box, b.h, xb[0], yb[0])
+    out = remesh_device_async(x, y, g, b.h, xb[0], yb[0], max_base_cells=win[2] * win[3],
+                              with_indices=True)
+    nout, status, window = out[5:]
+    k = int(nout.item())
+    assert int(status.item()) == 0 and k == ref[0].numel()
+    assert tuple(window.cpu().tolist()) == tuple(win)
+    for u, v in zip(out[:5], ref):
+        assert torch.equal(u[:k], v)
+    small = remesh_device_async(x, y, g, b.h, xb[0], yb[0], max_base_cells=100)
+    assert int(small[4].item()) == 8 and int(small[3].item()) == 0
+    w = small[5].cpu().tolist()
+    assert tuple(w) == tuple(win)
+    again = remesh_device_async(x, y, g, b.h, xb[0], yb[0], max_base_cells=w[2] * w[3])
+    assert int(again[4].item()) == 0 and int(again[3].item()) == k
+    assert torch.equal(again[2][:k], ref[2])
+
+
+def test_remesh_window_larger_than_the_previous_one():
+    """pf_remesh sizes its scratch from the context's previous window; a set
+    with a much larger window is found on the device and redone on its exact
+    window, with the same result as the oracle."""
+    import pfblob
+    rng = np.random.default_rng(21)
+    h = 0.004
+    b = np.array([-1.5 * h, 1.5 * h])
+    xs, ys = rng.uniform(0, 0.05, 2000), rng.uniform(0, 0.05, 2000)
+    _regrid_gpu(xs, ys, rng.standard_normal(2000), h / 0.8, 0.8, b, b)
+    x, y = rng.uniform(-2.0, 2.0, 3000), rng.uniform(-1.0, 1.0, 3000)
+    g = rng.standard_normal(3000)
+    xn, yn, gn = _regrid_gpu(x, y, g, h / 0.8, 0.8, b, b)
+    rx, ry, rg, _, _ = oracle.regrid(x, y, g, h / 0.8, 0.8, b, b)
     assert np.array_equal(xn, rx) and np.array_equal(yn, ry)
     assert np.abs(gn - rg).max() <= GTOL * np.abs(rg).max()

@@ -106,6 +106,24 @@ def test_same_result_alone_and_in_the_mix():
         assert a.sim == b.sim
         for k in ("vx", "vy", "x", "y", "g"):
             assert torch.equal(a.result[k], b.result[k]), k
+        assert torch.equal(a.moments, b.moments)
+
+
+@pytest.mark.gpu
+def test_served_steps_conserve_circulation_and_impulse():
+    """Every served step carries the FP64 moments of its blobs before and
+    after the remesh; circulation and linear impulse are conserved to 1e-12,
+    with and without a forward-Euler move."""
+    from pfblob.serve import Server, conservation, poisson_trace
+    sims = _sims([1500, 6000, 20000, 50000, 120000])
+    srv = Server(sims, n_slots=4)
+    done = srv.run_trace(poisson_trace(20, 5000.0, len(sims), seed=4), timeout=120)
+    c = conservation(done, srv.sims)
+    assert c["steps_checked"] == 20 and c["circulation"] <= 1e-12 and c["linear_impulse"] <= 1e-12
+    moved = srv.run_trace(poisson_trace(10, 5000.0, len(sims), seed=5), dt=1e-3, timeout=120)
+    c = conservation(moved, srv.sims)
+    assert c["steps_checked"] == 10 and c["circulation"] <= 1e-12 and c["linear_impulse"] <= 1e-12
+    srv.close()
 
 
 @pytest.mark.gpu

@@ -18,10 +18,11 @@
 //      touched when one of the 4 x 4 base cells whose windows cover it holds a
 //      blob (explicit zeros are kept, like the CSR sum of the reference,
 //      _regridding.py:200-202), so the output order is known before any value.
-//   4. k_rm_place  : blob -> its slot in cell order: its index (perm), its four
-//      x weights M4'(ux_a) and four y weights M4'(uy_b)
+//   4. k_rm_place  : blob -> its slot in cell order: a 96-byte record of its
+//      four x weights M4'(ux_a) and four y weights M4'(uy_b)
 //      (_interpolation_kernels_1d.cpp:75-89; u as _regridding.py:183) or
-//      Tutty's, and g -- the weights are computed once per blob, here.
+//      Tutty's, g and its input index -- the weights are computed once per
+//      blob, here.
 //   5. seg_sort_listed + k_rm_stencil_big : cells of more than SEG_SMALL blobs
 //      (dense clusters), one CTA per cell, stencil partial sums to a side table.
 //   6. k_rm_tile   : one CTA per tile of 8 x 29 output cells.  Each thread
@@ -113,6 +114,17 @@ __device__ __forceinline__ int64_t find_sorted(const int32_t *__restrict__ a, in
     }
     return (lo < n && (int64_t)a[lo] == v) ? lo : -1;
 }
+
+// One blob in cell order: its eight weights, g and input index, written by
+// k_rm_place as three whole 32-byte sectors (no partial-sector writes).
+struct WRec {
+    double wx[4];
+    double wy[4];
+    double g;
+    long long idx;
+    double pad[2];
+};
+static_assert(sizeof(WRec) == 96, "WRec layout");
 
 __device__ __forceinline__ int64_t left_index(double x, double b0, double h2, double h05,
                                               double h) {
@@ -554,8 +566,7 @@ __global__ void __launch_bounds__(RM_THREADS)
 k_rm_place(int64_t n, RmHead *hd, const int32_t *__restrict__ cell,
            const int32_t *__restrict__ rank, const int32_t *__restrict__ start,
            const double *__restrict__ x, const double *__restrict__ y,
-           const double *__restrict__ g, WParams wp, int32_t *__restrict__ perm,
-           double4 *__restrict__ wxs, double4 *__restrict__ wys, double *__restrict__ gs,
+           const double *__restrict__ g, WParams wp, WRec *__restrict__ recs,
            int32_t *__restrict__ big, double *__restrict__ mpart) {
     Win w;
     if (!load_win(hd, w)) return;  // the same for every CTA
@@ -569,20 +580,34 @@ k_rm_place(int64_t n, RmHead *hd, const int32_t *__restrict__ cell,
         const double xi = x[i], yi = y[i], gi = g[i];
         double wx[4], wy[4];
         blob_w8<TUTTY>(xi, yi, lat_x(w, bx), lat_y(w, by), wp, wx, wy);
-        perm[p] = (int32_t)i;
-        double2 *dx = reinterpret_cast<double2 *>(wxs + p);
-        double2 *dy = reinterpret_cast<double2 *>(wys + p);
-        dx[0] = make_double2(wx[0], wx[1]);
-        dx[1] = make_double2(wx[2], wx[3]);
-        dy[0] = make_double2(wy[0], wy[1]);
-        dy[1] = make_double2(wy[2], wy[3]);
-        gs[p] = gi;
+        double2 *d = reinterpret_cast<double2 *>(recs + p);
+        d[0] = make_double2(wx[0], wx[1]);
+        d[1] = make_double2(wx[2], wx[3]);
+        d[2] = make_double2(wy[0], wy[1]);
+        d[3] = make_double2(wy[2], wy[3]);
+        d[4] = make_double2(gi, __longlong_as_double((long long)i));
+        d[5] = make_double2(0.0, 0.0);
         add_moments(m, xi, yi, gi);
         // a cell of more than SEG_SMALL blobs (exactly one has this rank) is
         // listed for the segment sort
         if (r == pf::SEG_SMALL) big[atomicAdd(&hd->big_n, 1)] = c;
     }
     grid_moments<RM_THREADS>(m, mpart, &hd->ticket_in, hd->mom);
+}
+
+// The input indices of each listed cell of more than SEG_SMALL blobs, from its
+// records into vals[start ..] (for the segment sort).
+__global__ void __launch_bounds__(RM_THREADS)
+k_rm_big_gather(const int32_t *__restrict__ list, const RmHead *__restrict__ hd,
+                const int32_t *__restrict__ start, const int32_t *__restrict__ count,
+                const WRec *__restrict__ recs, int32_t *__restrict__ vals) {
+    if (!hd->ok) return;
+    const int nlist = hd->big_n;
+    for (int k = blockIdx.x; k < nlist; k += gridDim.x) {
+        const int64_t bc = list[k];
+        const int cnt = count[bc], s0 = start[bc];
+        for (int j = threadIdx.x; j < cnt; j += RM_THREADS) vals[s0 + j] = (int32_t)recs[s0 + j].idx;
+    }
 }
 
 // The stencil of each listed cell of more than SEG_SMALL blobs (sorted by
@@ -648,9 +673,8 @@ struct TileOut {
 template <bool TUTTY, bool EMIT>
 __global__ void __launch_bounds__(TILE_THREADS, 2)
 k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
-          const int32_t *__restrict__ start, const int32_t *__restrict__ perm,
-          const double4 *__restrict__ wxs, const double4 *__restrict__ wys,
-          const double *__restrict__ gs, const double *__restrict__ part_big, WParams wp,
+          const int32_t *__restrict__ start, const WRec *__restrict__ recs,
+          const double *__restrict__ part_big, WParams wp,
           TileOut to, double *__restrict__ mpart, RmHead *hmom) {
     __shared__ double s_p[16][TILE_THREADS];
     __shared__ unsigned char s_occ[TILE_THREADS];
@@ -675,25 +699,24 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
                 const int64_t bc = bx * w.nby + by;
                 cnt = count[bc];
                 if (cnt > 0) {
-                    const int64_t s0 = start[bc];
-                    const int32_t *pm = perm + s0;
+                    const WRec *rc = recs + start[bc];
                     // the cell's blobs in input-index order (the atomic ranks
                     // of k_rm_count are not reproducible)
-                    int last = -1;
+                    long long last = -1;
                     for (int k = 0; k < cnt; ++k) {
-                        int best = INT_MAX, bj = 0;
+                        long long best = LLONG_MAX;
+                        int bj = 0;
                         for (int j = 0; j < cnt; ++j) {
-                            const int v = pm[j];
+                            const long long v = rc[j].idx;
                             if (v > last && v < best) {
                                 best = v;
                                 bj = j;
                             }
                         }
                         last = best;
-                        const double2 *qx = reinterpret_cast<const double2 *>(wxs + s0 + bj);
-                        const double2 *qy = reinterpret_cast<const double2 *>(wys + s0 + bj);
-                        const double2 x01 = qx[0], x23 = qx[1], y01 = qy[0], y23 = qy[1];
-                        const double gv = gs[s0 + bj];
+                        const double2 *q = reinterpret_cast<const double2 *>(rc + bj);
+                        const double2 x01 = q[0], x23 = q[1], y01 = q[2], y23 = q[3];
+                        const double gv = q[4].x;
                         const double wx[4] = {x01.x, x01.y, x23.x, x23.y};
                         const double wy[4] = {y01.x, y01.y, y23.x, y23.y};
 #pragma unroll
@@ -818,8 +841,8 @@ static int64_t big_slots(int64_t n) { return n / (SEG_SMALL + 1) + 1; }
 
 size_t remesh_scratch_bytes(int64_t n, int64_t cap_base, int64_t cap_cell, bool cells_mode) {
     const int64_t ntA = ceil_div(cap_base, SC_TILE), ntB = ceil_div(cap_cell, SC_TILE);
-    size_t b = align256(sizeof(RmHead)) + align256(4 * cap_base) + 3 * align256(4 * n) +
-               2 * align256(32 * n) + align256(8 * n) + align256(4 * cap_base) +
+    size_t b = align256(sizeof(RmHead)) + align256(4 * cap_base) + 2 * align256(4 * n) +
+               align256(sizeof(WRec) * n) + align256(4 * cap_base) +
                align256(4 * cap_cell) + align256(cap_cell) +
                align256(4 * (ntA + 1)) + align256(4 * (ntB + 1)) + align256(4 * big_slots(n)) +
                align256(128 * big_slots(n)) + align256(32 * (ceil_div(n, RM_THREADS) + 1 + 2 * 1024 + 1)) +
@@ -849,10 +872,7 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     char *zero_end = cells ? (char *)(flag + cap_cell) : (char *)(count + cap_base);
     int32_t *cell = (int32_t *)sc.take(4 * n);
     int32_t *rank = (int32_t *)sc.take(4 * n);
-    int32_t *perm = (int32_t *)sc.take(4 * n);
-    double4 *wxs = (double4 *)sc.take(32 * n);
-    double4 *wys = (double4 *)sc.take(32 * n);
-    double *gs = (double *)sc.take(8 * n);
+    WRec *recs = (WRec *)sc.take(sizeof(WRec) * n);
     uint8_t *oflag = (uint8_t *)sc.take(cap_cell);
     int32_t *start = (int32_t *)sc.take(4 * cap_base);
     int32_t *slot = (int32_t *)sc.take(4 * cap_cell);
@@ -908,14 +928,17 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
         PF_TRY(launch_status("k_rm_scan_down"));
         if (tutty)
             k_rm_place<true><<<gn, RM_THREADS, 0, st>>>(n, hd, cell, rank, start, x, y, g, wp,
-                                                        perm, wxs, wys, gs, bigc, mpart);
+                                                        recs, bigc, mpart);
         else
             k_rm_place<false><<<gn, RM_THREADS, 0, st>>>(n, hd, cell, rank, start, x, y, g, wp,
-                                                         perm, wxs, wys, gs, bigc, mpart);
+                                                         recs, bigc, mpart);
         PF_TRY(launch_status("k_rm_place"));
         // cells above SEG_SMALL blobs (dense clusters); the ranks are free now
-        PF_TRY(seg_sort_listed(bigc, &hd->big_n, start, count, perm, rank, nbig, st));
         const unsigned gbig = (unsigned)std::min<int64_t>(nbig, 64);
+        k_rm_big_gather<<<gbig, RM_THREADS, 0, st>>>(bigc, hd, start, count, recs, cell);
+        PF_TRY(launch_status("k_rm_big_gather"));
+        int32_t *perm = cell;  // the cell ids are no longer needed: sorted indices of big cells
+        PF_TRY(seg_sort_listed(bigc, &hd->big_n, start, count, perm, rank, nbig, st));
         if (tutty)
             k_rm_stencil_big<true><<<gbig, RM_THREADS, 0, st>>>(bigc, hd, start, count, perm, x, y,
                                                                 g, wp, part_big);
@@ -931,19 +954,19 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
             1, std::min<int64_t>(std::min<int64_t>(2 * num_sms, gt_max), tiles_cap));
         TileOut to{slot, capacity, xo, yo, go, ixo, iyo, acc, flag};
         if (tutty && cells)
-            k_rm_tile<true, false><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, perm, wxs, wys, gs,
+            k_rm_tile<true, false><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs,
                                                                  part_big, wp, to,
                                                                  mpart + 4 * gn_max, hd);
         else if (tutty)
-            k_rm_tile<true, true><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, perm, wxs, wys, gs,
+            k_rm_tile<true, true><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs,
                                                                 part_big, wp, to,
                                                                  mpart + 4 * gn_max, hd);
         else if (cells)
-            k_rm_tile<false, false><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, perm, wxs, wys, gs,
+            k_rm_tile<false, false><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs,
                                                                   part_big, wp, to,
                                                                  mpart + 4 * gn_max, hd);
         else
-            k_rm_tile<false, true><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, perm, wxs, wys, gs,
+            k_rm_tile<false, true><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs,
                                                                  part_big, wp, to,
                                                                  mpart + 4 * gn_max, hd);
         PF_TRY(launch_status("k_rm_tile"));

@@ -221,5 +221,31 @@ def velocity_and_regrid(xBlob, yBlob, wBlob, sigma, overlap, xBounds, yBounds, k
     h = sigma * overlap
     xb0 = float(np.asarray(xBounds)[0]) if not isinstance(xBounds, torch.Tensor) else float(xBounds[0])
     yb0 = float(np.asarray(yBounds)[0]) if not isinstance(yBounds, torch.Tensor) else float(yBounds[0])
+    hv = None
+    if m.host:  # the velocities go back on a side stream while the remesh runs
+        main = torch.cuda.current_stream(m.device)
+        done = torch.cuda.Event()
+        done.record(main)
+        side = _side_stream(m.device)
+        hv = [torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for t in (vx, vy)]
+        with torch.cuda.stream(side):
+            side.wait_event(done)
+            for hh, t in zip(hv, (vx, vy)):
+                hh.copy_(t, non_blocking=True)
     xn, yn, gn = remesh_device(x, y, g, h, xb0, yb0, c)
-    return m.outs(vx, vy, xn, yn, gn)
+    if hv is None:
+        return m.outs(vx, vy, xn, yn, gn)
+    rest = m.outs(xn, yn, gn)
+    side.synchronize()
+    return (hv[0].numpy(), hv[1].numpy()) + tuple(rest)
+
+
+_SIDE = {}
+
+
+def _side_stream(dev):
+    """A second stream per device for copies that overlap the main stream's work."""
+    s = _SIDE.get(dev.index)
+    if s is None:
+        s = _SIDE[dev.index] = torch.cuda.Stream(dev)
+    return s

@@ -217,12 +217,17 @@ def test_async_remesh_equals_remesh_and_reports_its_window():
     win = lattice_window(box, b.h, xb[0], yb[0])
     out = remesh_device_async(x, y, g, b.h, xb[0], yb[0], max_base_cells=win[2] * win[3],
                               with_indices=True)
-    nout, status, window = out[5:]
+    nout, status, window, moments = out[5:]
     k = int(nout.item())
     assert int(status.item()) == 0 and k == ref[0].numel()
     assert tuple(window.cpu().tolist()) == tuple(win)
     for u, v in zip(out[:5], ref):
         assert torch.equal(u[:k], v)
+    m = moments.cpu().numpy()
+    m_in = oracle.moments(b.x, b.y, b.g)
+    assert np.allclose(m[:4], m_in, rtol=0, atol=1e-13 * m_in[3])
+    circ, imp = pfblob.conservation_error(m[:4], m[4:], float(np.abs(b.x).max()))
+    assert circ <= 1e-12 and imp <= 1e-12
     small = remesh_device_async(x, y, g, b.h, xb[0], yb[0], max_base_cells=100)
     assert int(small[4].item()) == 8 and int(small[3].item()) == 0
     w = small[5].cpu().tolist()
@@ -248,3 +253,21 @@ def test_remesh_window_larger_than_the_previous_one():
     rx, ry, rg, _, _ = oracle.regrid(x, y, g, h / 0.8, 0.8, b, b)
     assert np.array_equal(xn, rx) and np.array_equal(yn, ry)
     assert np.abs(gn - rg).max() <= GTOL * np.abs(rg).max()
+
+
+def test_velocity_and_regrid_equals_the_two_calls():
+    """The one-upload step (velocity at the blobs, then Regrid of the same
+    blobs, velocities read back while the remesh runs) gives bitwise the
+    results of pfblob.velocity and pfblob.Regrid called one after the other,
+    from numpy and from pinned host tensors."""
+    import pfblob
+    from pfblob import workloads as wl
+    b = wl.uniform_square(n=60000, sigma=0.004, config=2, instance=13)
+    xb, yb = b.bounds()
+    vx, vy = pfblob.velocity(b.x, b.y, b.g, b.sigma, method=pfblob.FMM_METHOD, hardware=1)
+    xn, yn, gn = pfblob.Regrid(b.x, b.y, b.g, b.sigma, b.overlap, xb, yb)
+    for inp in ((b.x, b.y, b.g), tuple(torch.from_numpy(a).pin_memory() for a in (b.x, b.y, b.g))):
+        out = pfblob.velocity_and_regrid(*inp, b.sigma, b.overlap, xb, yb,
+                                         method=pfblob.FMM_METHOD)
+        for u, v in zip(out, (vx, vy, xn, yn, gn)):
+            assert isinstance(u, np.ndarray) and np.array_equal(u, v)

@@ -369,7 +369,7 @@ pf_status pf_blob_step(pf_ctx *ctx, const pf_step *step, void *stream);
  * device's free memory to another allocator, and before any stream capture.
  * The address is kept per device for the process: do not use the entry point
  * across a cudaDeviceReset.  Blob sets needing more scratch than the buffer
- * holds (about 105 bytes per blob plus 8 bytes per base cell and 5 bytes per
+ * holds (about 90 bytes per blob plus 8 bytes per base cell and 5 bytes per
  * output cell of the window, and 66 KB) are rejected with
  * PF_ERR_INVALID_ARG.  Every
  * call shares the buffer, which keeps the last call's contents (the call

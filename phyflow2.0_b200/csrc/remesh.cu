@@ -18,18 +18,18 @@
 //      touched when one of the 4 x 4 base cells whose windows cover it holds a
 //      blob (explicit zeros are kept, like the CSR sum of the reference,
 //      _regridding.py:200-202), so the output order is known before any value.
-//   4. k_rm_place  : blob -> its slot in cell order: a 96-byte record of its
-//      four x weights M4'(ux_a) and four y weights M4'(uy_b)
-//      (_interpolation_kernels_1d.cpp:75-89; u as _regridding.py:183) or
-//      Tutty's, g and its input index -- the weights are computed once per
-//      blob, here.
+//   4. k_rm_place  : blob -> its slot in cell order: a 32-byte record {x/h,
+//      y/h, g, index} (the IEEE quotients of _regridding.py:183 computed once
+//      per blob; x, y for Tutty).
 //   5. seg_sort_listed + k_rm_stencil_big : cells of more than SEG_SMALL blobs
 //      (dense clusters), one CTA per cell, stencil partial sums to a side table.
 //   6. k_rm_tile   : one CTA per tile of 8 x 29 output cells.  Each thread
 //      takes one of the 11 x 32 base cells feeding the tile (a warp per base
-//      row), walks the cell's blobs in input-index order and accumulates the
-//      cell's 4 x 4 stencil of partial sums sum (wx_a wy_b) g in shared
-//      memory.  Then each output cell adds the 16 partial sums of the base
+//      row), walks the cell's blobs in input-index order (found in
+//      registers), forms their four x weights M4'(ux_a) and four y weights
+//      M4'(uy_b) (_interpolation_kernels_1d.cpp:75-89) or Tutty's, and
+//      accumulates the cell's 4 x 4 stencil of partial sums sum (wx_a wy_b) g
+//      in shared memory.  Then each output cell adds the 16 partial sums of the base
 //      cells that cover it in fixed (b, a) order and writes x = ix*h + 0.5h +
 //      xb0 (same order as :217-218), g, ix, iy at its slot.
 //      [pf_remesh_population_control: the cell values and flags go to HBM
@@ -66,6 +66,7 @@ constexpr int SC_TILE = SC_THREADS * SC_ITEMS;
 constexpr int TOX = 8, TOY = 29;
 constexpr int TBX = TOX + 3, TBY = TOY + 3;
 constexpr int TILE_THREADS = TBX * TBY;  // 352
+constexpr int TILE_PREF = 4;  // cell sizes whose blob order is found in registers
 static_assert(TBY == 32, "one warp per base row");
 
 struct Win {
@@ -115,16 +116,16 @@ __device__ __forceinline__ int64_t find_sorted(const int32_t *__restrict__ a, in
     return (lo < n && (int64_t)a[lo] == v) ? lo : -1;
 }
 
-// One blob in cell order: its eight weights, g and input index, written by
-// k_rm_place as three whole 32-byte sectors (no partial-sector writes).
+// One blob in cell order, written by k_rm_place as one whole 32-byte sector:
+// v1, v2 = x/h, y/h (M4': the IEEE quotients of the reference's u = (ix +
+// 0.5 + xb0/h) - x/h) or x, y (Tutty), its circulation and input index.
+// (Weights computed here instead, 64 more bytes per blob, measured slower:
+// k_rm_place 26 -> 60 us, k_rm_tile 94 -> 78 us at N = 2^20.)
 struct WRec {
-    double wx[4];
-    double wy[4];
-    double g;
+    double v1, v2, g;
     long long idx;
-    double pad[2];
 };
-static_assert(sizeof(WRec) == 96, "WRec layout");
+static_assert(sizeof(WRec) == 32, "WRec layout");
 
 __device__ __forceinline__ int64_t left_index(double x, double b0, double h2, double h05,
                                               double h) {
@@ -200,7 +201,8 @@ __device__ __forceinline__ void add_moments(double (&m)[4], double x, double y, 
 __global__ void __launch_bounds__(RM_THREADS)
 k_rm_extent(const double *__restrict__ x, const double *__restrict__ y, int64_t n, double xb0,
             double yb0, double h2, double h05, double h, RmHead *hd, int64_t cap_base,
-            int64_t cap_cell, int64_t limit) {
+            int64_t cap_cell, int64_t limit, int32_t *__restrict__ xl_out,
+            int32_t *__restrict__ yl_out) {
     __shared__ int s_v[5][RM_THREADS / 32];
     __shared__ int s_last;
     int xhi = 0, xlo = 0, yhi = 0, ylo = 0, bad = 0;
@@ -218,16 +220,22 @@ k_rm_extent(const double *__restrict__ x, const double *__restrict__ y, int64_t 
         for (int u = 0; u < 4; ++u) {
             if (i0 + u * stride >= n) continue;
             const double xi = xs[u], yi = ys[u];
+            const int64_t iu = i0 + u * stride;
             if (!isfinite(xi) || !isfinite(yi)) {
                 bad |= 1;
+                xl_out[iu] = yl_out[iu] = INT32_MIN;
                 continue;
             }
             const int64_t a = left_index(xi, xb0, h2, h05, h);
             const int64_t b = left_index(yi, yb0, h2, h05, h);
             if (a <= -IDX_LIMIT || a >= IDX_LIMIT || b <= -IDX_LIMIT || b >= IDX_LIMIT) {
                 bad |= 2;
+                xl_out[iu] = yl_out[iu] = INT32_MIN;
                 continue;
             }
+            // for k_rm_count (|a|, |b| < 2^30 here)
+            xl_out[iu] = (int32_t)a;
+            yl_out[iu] = (int32_t)b;
             xhi = max(xhi, (int)a + RM_IDX_OFF);
             xlo = max(xlo, RM_IDX_OFF - (int)a);
             yhi = max(yhi, (int)b + RM_IDX_OFF);
@@ -379,14 +387,20 @@ __device__ __forceinline__ void blob_w8(double xv, double yv, int64_t ix0, int64
 __global__ void __launch_bounds__(RM_THREADS)
 k_rm_count(const double *__restrict__ x, const double *__restrict__ y, int64_t n, double xb0,
            double yb0, double h2, double h05, double h, RmHead *hd, int32_t *__restrict__ cell,
-           int32_t *__restrict__ rank, int32_t *__restrict__ count) {
+           int32_t *__restrict__ rank, int32_t *__restrict__ count, bool pre) {
     Win w;
     if (!load_win(hd, w)) return;
     const int64_t i = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     if (i >= n) return;
-    const double xi = x[i], yi = y[i];
     int64_t a = -1, b = -1;
-    if (isfinite(xi) && isfinite(yi)) {
+    if (pre) {  // left indices from k_rm_extent, in cell[] / rank[] (INT32_MIN: not finite)
+        const int32_t pa = cell[i], pb = rank[i];
+        if (pa != INT32_MIN) {
+            a = pa - w.ixmin;
+            b = pb - w.iymin;
+        }
+    } else if (isfinite(x[i]) && isfinite(y[i])) {
+        const double xi = x[i], yi = y[i];
         a = left_index(xi, xb0, h2, h05, h);
         b = left_index(yi, yb0, h2, h05, h);
         a = w.rows ? find_sorted(w.rows, w.nbx, a) : a - w.ixmin;
@@ -558,9 +572,9 @@ k_rm_scan_down(RmHead *__restrict__ hd, const int32_t *__restrict__ count, int64
         hd->total = pre + s_x[SC_THREADS / 32];
 }
 
-// Blob -> its slot in cell order: its index, its eight weights (computed here
-// once per blob, with every thread busy) and its circulation; and the FP64
-// moments of the blobs placed.
+// Blob -> its slot in cell order: a 32-byte record (x/h and y/h -- the
+// divisions done once per blob, with every thread busy -- or x, y for Tutty,
+// g, its index); and the FP64 moments of the blobs placed.
 template <bool TUTTY>
 __global__ void __launch_bounds__(RM_THREADS)
 k_rm_place(int64_t n, RmHead *hd, const int32_t *__restrict__ cell,
@@ -570,23 +584,20 @@ k_rm_place(int64_t n, RmHead *hd, const int32_t *__restrict__ cell,
            int32_t *__restrict__ big, double *__restrict__ mpart) {
     Win w;
     if (!load_win(hd, w)) return;  // the same for every CTA
-    const int64_t i = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x;
     double m[4] = {0.0, 0.0, 0.0, 0.0};
-    const int32_t c = i < n ? cell[i] : -1;
-    if (c >= 0) {
+    // grid-stride: a few blobs per thread, one moment reduction per CTA
+    for (int64_t i = (int64_t)blockIdx.x * RM_THREADS + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * RM_THREADS) {
+        const int32_t c = cell[i];
+        if (c < 0) continue;
         const int32_t r = rank[i];
         const int64_t p = (int64_t)start[c] + r;
-        const int32_t bx = c / (int32_t)w.nby, by = c - bx * (int32_t)w.nby;
         const double xi = x[i], yi = y[i], gi = g[i];
-        double wx[4], wy[4];
-        blob_w8<TUTTY>(xi, yi, lat_x(w, bx), lat_y(w, by), wp, wx, wy);
+        const double v1 = TUTTY ? xi : __ddiv_rn(xi, wp.h);
+        const double v2 = TUTTY ? yi : __ddiv_rn(yi, wp.h);
         double2 *d = reinterpret_cast<double2 *>(recs + p);
-        d[0] = make_double2(wx[0], wx[1]);
-        d[1] = make_double2(wx[2], wx[3]);
-        d[2] = make_double2(wy[0], wy[1]);
-        d[3] = make_double2(wy[2], wy[3]);
-        d[4] = make_double2(gi, __longlong_as_double((long long)i));
-        d[5] = make_double2(0.0, 0.0);
+        d[0] = make_double2(v1, v2);
+        d[1] = make_double2(gi, __longlong_as_double((long long)i));
         add_moments(m, xi, yi, gi);
         // a cell of more than SEG_SMALL blobs (exactly one has this rank) is
         // listed for the segment sort
@@ -607,6 +618,24 @@ k_rm_big_gather(const int32_t *__restrict__ list, const RmHead *__restrict__ hd,
         const int64_t bc = list[k];
         const int cnt = count[bc], s0 = start[bc];
         for (int j = threadIdx.x; j < cnt; j += RM_THREADS) vals[s0 + j] = (int32_t)recs[s0 + j].idx;
+    }
+}
+
+// blob_w8 from a record's values: M4' takes x/h, y/h as computed in
+// k_rm_place (the same IEEE quotients blob_w8 forms), Tutty takes x, y.
+template <bool TUTTY>
+__device__ __forceinline__ void rec_w8(double v1, double v2, int64_t ix0, int64_t iy0,
+                                       const WParams &wp, double (&wx)[4], double (&wy)[4]) {
+    if (TUTTY) {
+        blob_w8<true>(v1, v2, ix0, iy0, wp, wx, wy);
+    } else {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const double px = __dadd_rn(((double)ix0 + (double)a) + 0.5, wp.qx0);
+            const double py = __dadd_rn(((double)iy0 + (double)a) + 0.5, wp.qy0);
+            wx[a] = m4p(__dsub_rn(px, v1), wp.prm);
+            wy[a] = m4p(__dsub_rn(py, v2), wp.prm);
+        }
     }
 }
 
@@ -678,13 +707,14 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
           TileOut to, double *__restrict__ mpart, RmHead *hmom) {
     __shared__ double s_p[16][TILE_THREADS];
     __shared__ unsigned char s_occ[TILE_THREADS];
+    __shared__ double s_mom[TILE_THREADS / 32][4];  // per warp, summed over its tiles in order
     Win w;
     if (!load_win(hd, w)) return;
     const int64_t ntx = (w.nox + TOX - 1) / TOX, nty = (w.noy + TOY - 1) / TOY;
     const int64_t ntiles = ntx * nty;
     const bool emit_ok = !EMIT || (int64_t)hd->total <= to.capacity;
     const int lbx = threadIdx.x >> 5, lby = threadIdx.x & 31;
-    double mom[4] = {0.0, 0.0, 0.0, 0.0};  // of the new blobs this thread writes
+    if (EMIT && threadIdx.x < (TILE_THREADS / 32) * 4) s_mom[threadIdx.x >> 2][threadIdx.x & 3] = 0.0;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t tx = t / nty, ty = t - tx * nty;
         const int64_t ox0 = tx * TOX, oy0 = ty * TOY;
@@ -700,25 +730,39 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
                 cnt = count[bc];
                 if (cnt > 0) {
                     const WRec *rc = recs + start[bc];
+                    const int64_t ix0 = lat_x(w, bx), iy0 = lat_y(w, by);
                     // the cell's blobs in input-index order (the atomic ranks
-                    // of k_rm_count are not reproducible)
-                    long long last = -1;
+                    // of k_rm_count are not reproducible): up to TILE_PREF
+                    // indices are loaded at once and ordered in registers
+                    int ids[TILE_PREF];  // input indices are below 2^31
+#pragma unroll
+                    for (int j = 0; j < TILE_PREF; ++j)
+                        ids[j] = j < cnt ? (int)rc[j].idx : INT_MAX;
+                    int last = -1;
                     for (int k = 0; k < cnt; ++k) {
-                        long long best = LLONG_MAX;
+                        int best = INT_MAX;
                         int bj = 0;
-                        for (int j = 0; j < cnt; ++j) {
-                            const long long v = rc[j].idx;
-                            if (v > last && v < best) {
-                                best = v;
-                                bj = j;
+                        if (cnt <= TILE_PREF) {
+#pragma unroll
+                            for (int j = 0; j < TILE_PREF; ++j)
+                                if (ids[j] > last && ids[j] < best) {
+                                    best = ids[j];
+                                    bj = j;
+                                }
+                        } else {
+                            for (int j = 0; j < cnt; ++j) {
+                                const int v = (int)rc[j].idx;
+                                if (v > last && v < best) {
+                                    best = v;
+                                    bj = j;
+                                }
                             }
                         }
                         last = best;
-                        const double2 *q = reinterpret_cast<const double2 *>(rc + bj);
-                        const double2 x01 = q[0], x23 = q[1], y01 = q[2], y23 = q[3];
-                        const double gv = q[4].x;
-                        const double wx[4] = {x01.x, x01.y, x23.x, x23.y};
-                        const double wy[4] = {y01.x, y01.y, y23.x, y23.y};
+                        const double2 vv = *reinterpret_cast<const double2 *>(rc + bj);
+                        const double gv = rc[bj].g;
+                        double wx[4], wy[4];
+                        rec_w8<TUTTY>(vv.x, vv.y, ix0, iy0, wp, wx, wy);
 #pragma unroll
                         for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -737,6 +781,7 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
         __syncthreads();
         // 2. each output cell: the partial sums of its 16 covering base cells,
         // in fixed (b, a) order (empty or outside cells add nothing: +0.0)
+        double mom[4] = {0.0, 0.0, 0.0, 0.0};  // of the new blob this thread writes
         if (threadIdx.x < TOX * TOY) {
             const int lx = threadIdx.x / TOY, ly = threadIdx.x - lx * TOY;
             const int64_t ox = ox0 + lx, oy = oy0 + ly;
@@ -776,9 +821,26 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
                 }
             }
         }
+        if (EMIT) {  // this tile's moments, warp by warp in a fixed order
+            const int wid = threadIdx.x >> 5;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                double v = mom[q];
+#pragma unroll
+                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if ((threadIdx.x & 31) == 0) s_mom[wid][q] += v;
+            }
+        }
         __syncthreads();
     }
-    if (EMIT) grid_moments<TILE_THREADS>(mom, mpart, &hmom->ticket_out, hmom->mom + 4);
+    if (EMIT) {
+        double m[4] = {0.0, 0.0, 0.0, 0.0};
+        if (threadIdx.x == 0)
+            for (int k = 0; k < TILE_THREADS / 32; ++k)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) m[q] += s_mom[k][q];
+        grid_moments<TILE_THREADS>(m, mpart, &hmom->ticket_out, hmom->mom + 4);
+    }
 }
 
 // cells mode: emit the flagged cells at their slots (cid up to the capacity;
@@ -896,11 +958,12 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     PF_CUDA_TRY(cudaMemsetAsync(hd, 0, (size_t)(zero_end - (char *)hd), st));
     if (win.from_blobs) {
         int64_t grid = ceil_div(n, RM_THREADS);
-        const int64_t cap = (int64_t)num_sms * 2;  // few CTAs: few same-address atomics
+        const int64_t cap = (int64_t)num_sms * 8;
         if (grid > cap) grid = cap;
         if (grid < 1) grid = 1;
         k_rm_extent<<<(unsigned)grid, RM_THREADS, 0, st>>>(x, y, n, xb0, yb0, h2, h05, h, hd,
-                                                           cap_base, cap_cell, win.cell_limit);
+                                                           cap_base, cap_cell, win.cell_limit,
+                                                           cell, rank);
         PF_TRY(launch_status("k_rm_extent"));
     } else {
         if (win.nbx < 1 || win.nby < 1 || win.nbx * win.nby > cap_base ||
@@ -918,7 +981,7 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
     if (n > 0) {
         const unsigned gn = (unsigned)ceil_div(n, RM_THREADS);
         k_rm_count<<<gn, RM_THREADS, 0, st>>>(x, y, n, xb0, yb0, h2, h05, h, hd, cell, rank,
-                                              count);
+                                              count, win.from_blobs);
         PF_TRY(launch_status("k_rm_count"));
         const unsigned gsc = (unsigned)(ntA + (cells ? 0 : ntB));
         k_rm_scan_up<<<gsc, SC_THREADS, 0, st>>>(hd, count, ntA, tsA, tsB, oflag);
@@ -926,11 +989,12 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
         k_rm_scan_down<<<gsc, SC_THREADS, 0, st>>>(hd, count, ntA, tsA, tsB, oflag, start,
                                                   slot);
         PF_TRY(launch_status("k_rm_scan_down"));
+        const unsigned gp = (unsigned)std::min<int64_t>(gn, (int64_t)num_sms * 8);
         if (tutty)
-            k_rm_place<true><<<gn, RM_THREADS, 0, st>>>(n, hd, cell, rank, start, x, y, g, wp,
+            k_rm_place<true><<<gp, RM_THREADS, 0, st>>>(n, hd, cell, rank, start, x, y, g, wp,
                                                         recs, bigc, mpart);
         else
-            k_rm_place<false><<<gn, RM_THREADS, 0, st>>>(n, hd, cell, rank, start, x, y, g, wp,
+            k_rm_place<false><<<gp, RM_THREADS, 0, st>>>(n, hd, cell, rank, start, x, y, g, wp,
                                                          recs, bigc, mpart);
         PF_TRY(launch_status("k_rm_place"));
         // cells above SEG_SMALL blobs (dense clusters); the ranks are free now

@@ -90,10 +90,11 @@ def remesh_device_async(x, y, g, h, xb0, yb0, c=0.0, max_base_cells=None, capaci
     go = torch.empty(capacity, dtype=torch.float64, device=dev)
     ixo = torch.empty(capacity, dtype=torch.int64, device=dev) if with_indices else None
     iyo = torch.empty(capacity, dtype=torch.int64, device=dev) if with_indices else None
-    nout = torch.zeros(1, dtype=torch.int64, device=dev)
-    status = torch.zeros(1, dtype=torch.int32, device=dev)
-    window = torch.zeros(4, dtype=torch.int64, device=dev)
-    moments = torch.zeros(8, dtype=torch.float64, device=dev)
+    # written by the call's last kernel, whatever happens on the device
+    nout = torch.empty(1, dtype=torch.int64, device=dev)
+    status = torch.empty(1, dtype=torch.int32, device=dev)
+    window = torch.empty(4, dtype=torch.int64, device=dev)
+    moments = torch.empty(8, dtype=torch.float64, device=dev)
     _lib.check(_lib.lib.pf_remesh_async(ctx, n, ptr(x), ptr(y), ptr(g), float(h), float(xb0),
                                         float(yb0), float(c), mb, capacity, ptr(xo), ptr(yo),
                                         ptr(go), ptr(ixo), ptr(iyo), ptr(nout), ptr(status),

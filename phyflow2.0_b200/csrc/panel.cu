@@ -4,14 +4,38 @@
 // rotate the point into the panel frame (xP, yP), panel end at (x2, 0), then
 //   vxP =  g/(2pi) * theta,  theta = atan2(yP, xP-x2) - atan2(yP, xP)
 //   vyP = -g/(4pi) * log((xP^2+yP^2)/((xP-x2)^2+yP^2))
-// and rotate back.  Evaluated here as
+// and rotate back.  In complex form (z = x + iy, w = vx - i vy) this is
+//   w_j(z) = K_j log((z - z2_j) / (z - z1_j)),   K_j = -i g_j e^{-i alpha_j} / (2pi),
+// z1 = (xs, ys), z2 = z1 + x2 e^{i alpha} (the panel end the reference's
+// frame places at (x2, 0)).
+//
+// The panels are taken in groups of PC_G consecutive ones (a body's boundary
+// is a chain, so a group is a short arc).  A group is enclosed by the circle
+// |z - c| <= R around its end points' bounding-box centre, and outside it
+//   sum_j w_j(z) = sum_{k>=1} A_k (R / (z - c))^k,
+//   A_k = sum_j K_j (a_j^k - b_j^k) / k,  a_j = (z1_j - c)/R, b_j = (z2_j - c)/R
+// (log(1 - u) = -sum u^k / k for |u| < 1; both logs have positive-real
+// arguments there, so the branch is the principal one the single atan2 below
+// gives).  For a point with rho = R / |z - c| <= PC_RHO the series is summed
+// in FP64 to the first P terms, P the least with rho^P <= PC_EPS (1 - rho) / 2
+// (remainder <= PC_EPS * rho * sum |K_j|, i.e. a relative 1e-10 of the
+// group's share); nearer points take the pair formula for each panel of the
+// group.  This is the reference's sum evaluated in fewer operations: every
+// term it adds is kept, to 1e-10 of the group's share far away and exactly
+// (up to FP32 transcendentals) near.  Nothing depends on the panel order but
+// the speed: a group of scattered panels has a large R and is summed pair by
+// pair for every point.
+//
+// The pair formula is evaluated as
 //   theta = atan2(yP*x2, xP*(xP-x2) + yP^2)         (one atan2, same value in
 //           (-pi, pi]: the angle between the two end-point rays)
 //   log   = log1p(u), u = x2*(2xP-x2) / ((xP-x2)^2 + yP^2), while |u| < 1/2
 //           (no cancellation far away), else log of the ratio itself (no
 //           cancellation in 1+u next to the panel's start point)
 // Geometry and accumulation in FP64, the two transcendentals in FP32.
-// Panels are staged through shared memory in tiles; one target per thread.
+#include <algorithm>
+#include <cmath>
+
 #include "pf_common.cuh"
 
 namespace {
@@ -20,70 +44,206 @@ constexpr int PN_THREADS = 256;
 constexpr double INV_2PI = 0.15915494309189535;
 constexpr double INV_4PI = 0.07957747154594767;
 
+constexpr int PC_G = 16;           // panels per group
+constexpr int PC_P = 28;           // most series terms (P at rho = PC_RHO)
+constexpr double PC_RHO = 0.4;     // series used where R / |z - c| <= PC_RHO
+constexpr double PC_EPS = 1e-10;   // relative remainder of a group's share
+constexpr int PC_TILE = 32;        // groups staged in shared memory at once
+
 struct PanelSm {
     double xs, ys, c, s, x2, gam;
 };
 
+// One group: centre, radius, (R / PC_RHO)^2 and the scaled series A_1..A_P.
+struct PanelGroup {
+    double cx, cy, R, far_r2;
+    double2 a[PC_P];
+};
+static_assert(sizeof(PanelGroup) % 16 == 0, "PanelGroup layout");
+
+__device__ __forceinline__ void pair_velocity(const PanelSm &q, double px, double py, double &ax,
+                                              double &ay) {
+    const double dx = px - q.xs, dy = py - q.ys;
+    const double xp = q.c * dx + q.s * dy;
+    const double yp = -q.s * dx + q.c * dy;
+    const double xm = xp - q.x2;
+    const double a2 = xm * xm + yp * yp;
+    const double num_t = yp * q.x2;
+    const double den_t = xp * xm + yp * yp;
+    const double num_l = q.x2 * (2.0 * xp - q.x2);
+    const float theta = atan2f((float)num_t, (float)den_t);
+    // log(b2/a2): log1p of u = (b2 - a2)/a2 while |u| < 1/2, else the log of
+    // the FP32-rounded ratio; both ~1 ulp absolute.
+    const float a2f = (float)a2;
+    const float u = (float)num_l / a2f;
+    const float lg = (fabsf(u) < 0.5f) ? log1pf(u) : logf((float)(xp * xp + yp * yp) / a2f);
+    const double vxp = (q.gam * INV_2PI) * (double)theta;
+    const double vyp = -(q.gam * INV_4PI) * (double)lg;
+    ax += q.c * vxp - q.s * vyp;
+    ay += q.s * vxp + q.c * vyp;
+}
+
+// One warp per group: the panels' frame records, the enclosing circle and the
+// series coefficients (lane k forms A_{k+1}).
+__global__ void __launch_bounds__(32)
+k_panel_groups(int64_t m, const double *__restrict__ gamma, const double *__restrict__ xs,
+               const double *__restrict__ ys, const double *__restrict__ xe,
+               const double *__restrict__ ye, const double *__restrict__ cosa,
+               const double *__restrict__ sina, PanelGroup *__restrict__ groups,
+               PanelSm *__restrict__ pan) {
+    const int64_t j0 = (int64_t)blockIdx.x * PC_G;
+    const int lane = threadIdx.x;
+    const int cnt = (int)min((int64_t)PC_G, m - j0);
+    const bool has = lane < cnt;
+    double x1 = 0.0, y1 = 0.0, x2e = 0.0, y2e = 0.0, kr = 0.0, ki = 0.0;
+    double bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
+    if (has) {
+        const int64_t j = j0 + lane;
+        PanelSm q;
+        q.xs = xs[j];
+        q.ys = ys[j];
+        q.c = cosa[j];
+        q.s = sina[j];
+        const double lx = xe[j] - q.xs, ly = ye[j] - q.ys;
+        q.x2 = q.c * lx + q.s * ly;
+        q.gam = gamma[j];
+        pan[j] = q;
+        x1 = q.xs;
+        y1 = q.ys;
+        x2e = q.xs + q.x2 * q.c;
+        y2e = q.ys + q.x2 * q.s;
+        kr = -(q.gam * INV_2PI) * q.s;
+        ki = -(q.gam * INV_2PI) * q.c;
+        bx0 = fmin(x1, x2e);
+        bx1 = fmax(x1, x2e);
+        by0 = fmin(y1, y2e);
+        by1 = fmax(y1, y2e);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        bx0 = fmin(bx0, __shfl_xor_sync(0xffffffffu, bx0, o));
+        bx1 = fmax(bx1, __shfl_xor_sync(0xffffffffu, bx1, o));
+        by0 = fmin(by0, __shfl_xor_sync(0xffffffffu, by0, o));
+        by1 = fmax(by1, __shfl_xor_sync(0xffffffffu, by1, o));
+    }
+    const double cx = 0.5 * (bx0 + bx1), cy = 0.5 * (by0 + by1);
+    double r2 = 0.0;
+    if (has) {
+        const double d1 = (x1 - cx) * (x1 - cx) + (y1 - cy) * (y1 - cy);
+        const double d2 = (x2e - cx) * (x2e - cx) + (y2e - cy) * (y2e - cy);
+        r2 = fmax(d1, d2);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+    const double R = sqrt(r2);
+    const double inv = R > 0.0 ? 1.0 / R : 0.0;
+    const double ar = (x1 - cx) * inv, ai = (y1 - cy) * inv;
+    const double br = (x2e - cx) * inv, bi = (y2e - cy) * inv;
+    const int k = lane + 1;
+    double sr = 0.0, si = 0.0;
+    for (int j = 0; j < cnt; ++j) {
+        const double jar = __shfl_sync(0xffffffffu, ar, j), jai = __shfl_sync(0xffffffffu, ai, j);
+        const double jbr = __shfl_sync(0xffffffffu, br, j), jbi = __shfl_sync(0xffffffffu, bi, j);
+        const double jkr = __shfl_sync(0xffffffffu, kr, j), jki = __shfl_sync(0xffffffffu, ki, j);
+        double pr = 1.0, pi = 0.0, qr = 1.0, qi = 0.0;  // a^k, b^k
+        for (int e = 0; e < k && k <= PC_P; ++e) {
+            const double t1 = pr * jar - pi * jai;
+            pi = pr * jai + pi * jar;
+            pr = t1;
+            const double t2 = qr * jbr - qi * jbi;
+            qi = qr * jbi + qi * jbr;
+            qr = t2;
+        }
+        const double dr = pr - qr, di = pi - qi;
+        sr += jkr * dr - jki * di;
+        si += jkr * di + jki * dr;
+    }
+    PanelGroup *gp = groups + blockIdx.x;
+    if (k <= PC_P) gp->a[lane] = make_double2(sr / k, si / k);
+    if (lane == 0) {
+        gp->cx = cx;
+        gp->cy = cy;
+        gp->R = R;
+        gp->far_r2 = r2 * (1.0 / (PC_RHO * PC_RHO));
+    }
+}
+
+// Velocity at the points: one point per thread, the groups (series and
+// panels) staged through shared memory PC_TILE at a time; a persistent grid
+// keeps one staging when all groups fit one tile.
 __global__ void __launch_bounds__(PN_THREADS)
-k_panel_velocity(int64_t m, const double *__restrict__ gamma, const double *__restrict__ xs,
-                 const double *__restrict__ ys, const double *__restrict__ xe,
-                 const double *__restrict__ ye, const double *__restrict__ cosa,
-                 const double *__restrict__ sina, int64_t n, const double *__restrict__ xv,
-                 const double *__restrict__ yv, double *__restrict__ vx,
-                 double *__restrict__ vy, int accumulate) {
-    __shared__ PanelSm sp[PN_THREADS];
-    const int64_t i = (int64_t)blockIdx.x * PN_THREADS + threadIdx.x;
-    double px = 0.0, py = 0.0;
-    if (i < n) {
-        px = xv[i];
-        py = yv[i];
-    }
-    double ax = 0.0, ay = 0.0;
-    for (int64_t t0 = 0; t0 < m; t0 += PN_THREADS) {
-        const int64_t j = t0 + threadIdx.x;
-        __syncthreads();
-        if (j < m) {
-            PanelSm q;
-            q.xs = xs[j];
-            q.ys = ys[j];
-            q.c = cosa[j];
-            q.s = sina[j];
-            const double lx = xe[j] - q.xs, ly = ye[j] - q.ys;
-            q.x2 = q.c * lx + q.s * ly;
-            q.gam = gamma[j];
-            sp[threadIdx.x] = q;
+k_panel_velocity(int64_t ngroups, const PanelGroup *__restrict__ groups,
+                 const PanelSm *__restrict__ pan, int64_t m, int64_t n,
+                 const double *__restrict__ xv, const double *__restrict__ yv,
+                 double *__restrict__ vx, double *__restrict__ vy, int accumulate,
+                 float log2_tol) {
+    __shared__ PanelGroup s_g[PC_TILE];
+    __shared__ PanelSm s_p[PC_TILE * PC_G];
+    const int64_t ntiles = (ngroups + PC_TILE - 1) / PC_TILE;
+    bool staged = false;
+    for (int64_t base = (int64_t)blockIdx.x * PN_THREADS; base < n;
+         base += (int64_t)gridDim.x * PN_THREADS) {
+        const int64_t i = base + threadIdx.x;
+        double px = 0.0, py = 0.0;
+        if (i < n) {
+            px = xv[i];
+            py = yv[i];
         }
-        __syncthreads();
-        const int cnt = (int)min((int64_t)PN_THREADS, m - t0);
-        for (int k = 0; k < cnt; ++k) {
-            const PanelSm q = sp[k];
-            const double dx = px - q.xs, dy = py - q.ys;
-            const double xp = q.c * dx + q.s * dy;
-            const double yp = -q.s * dx + q.c * dy;
-            const double xm = xp - q.x2;
-            const double a2 = xm * xm + yp * yp;
-            const double num_t = yp * q.x2;
-            const double den_t = xp * xm + yp * yp;
-            const double num_l = q.x2 * (2.0 * xp - q.x2);
-            const float theta = atan2f((float)num_t, (float)den_t);
-            // log(b2/a2): log1p of u = (b2 - a2)/a2 while |u| < 1/2, else the
-            // log of the FP32-rounded ratio; both ~1 ulp absolute.
-            const float a2f = (float)a2;
-            const float u = (float)num_l / a2f;
-            const float lg = (fabsf(u) < 0.5f) ? log1pf(u) : logf((float)(xp * xp + yp * yp) / a2f);
-            const double vxp = (q.gam * INV_2PI) * (double)theta;
-            const double vyp = -(q.gam * INV_4PI) * (double)lg;
-            ax += q.c * vxp - q.s * vyp;
-            ay += q.s * vxp + q.c * vyp;
+        double ax = 0.0, ay = 0.0;
+        for (int64_t t = 0; t < ntiles; ++t) {
+            const int64_t g0 = t * PC_TILE;
+            const int gc = (int)min((int64_t)PC_TILE, ngroups - g0);
+            if (!staged || ntiles > 1) {
+                __syncthreads();
+                const double2 *srcg = reinterpret_cast<const double2 *>(groups + g0);
+                double2 *dstg = reinterpret_cast<double2 *>(s_g);
+                const int ng2 = gc * (int)(sizeof(PanelGroup) / 16);
+                for (int e = threadIdx.x; e < ng2; e += PN_THREADS) dstg[e] = srcg[e];
+                const int64_t p0 = g0 * PC_G;
+                const int pc = (int)min((int64_t)PC_TILE * PC_G, m - p0);
+                const double2 *srcp = reinterpret_cast<const double2 *>(pan + p0);
+                double2 *dstp = reinterpret_cast<double2 *>(s_p);
+                const int np2 = pc * (int)(sizeof(PanelSm) / 16);
+                for (int e = threadIdx.x; e < np2; e += PN_THREADS) dstp[e] = srcp[e];
+                __syncthreads();
+                staged = true;
+            }
+            for (int c = 0; c < gc; ++c) {
+                const double dx = px - s_g[c].cx, dy = py - s_g[c].cy;
+                const double r2 = dx * dx + dy * dy;
+                if (r2 < s_g[c].far_r2) {
+                    const int j1 = (int)min((int64_t)PC_G, m - (g0 + c) * PC_G);
+                    for (int j = 0; j < j1; ++j) pair_velocity(s_p[c * PC_G + j], px, py, ax, ay);
+                } else {
+                    const double R = s_g[c].R;
+                    const double q = R / r2;
+                    const double sr = dx * q, si = -dy * q;  // s = R / (z - c)
+                    const float lr = 0.5f * __log2f((float)(R * q));
+                    // at least one term (rho^2 may underflow in FP32)
+                    const int P = max(1, min(PC_P, (int)ceilf(log2_tol / lr)));
+                    const int Pw = __reduce_max_sync(__activemask(), P);
+                    double wr = 0.0, wi = 0.0;
+                    for (int k = Pw - 1; k >= 0; --k) {
+                        const double2 a = s_g[c].a[k];
+                        if (k < P) {
+                            const double tr = fma(sr, wr, fma(-si, wi, a.x));
+                            wi = fma(sr, wi, fma(si, wr, a.y));
+                            wr = tr;
+                        }
+                    }
+                    ax += sr * wr - si * wi;
+                    ay -= sr * wi + si * wr;
+                }
+            }
         }
-    }
-    if (i < n) {
-        if (accumulate) {
-            ax += vx[i];
-            ay += vy[i];
+        if (i < n) {
+            if (accumulate) {
+                ax += vx[i];
+                ay += vy[i];
+            }
+            vx[i] = ax;
+            vy[i] = ay;
         }
-        vx[i] = ax;
-        vy[i] = ay;
     }
 }
 
@@ -121,6 +281,7 @@ extern "C" pf_status pf_panel_influence_matrix(pf_ctx *ctx, int64_t m, const dou
                                                const double *ys, const double *xe,
                                                const double *ye, const double *cosa,
                                                const double *sina, double *A, void *stream) {
+    PF_RANGE("pf_panel_influence_matrix");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_panel_influence_matrix: NULL context");
     PF_CHECK_ARG(m >= 0 && m <= 32768, "pf_panel_influence_matrix: m = %lld outside [0, 32768]",
@@ -140,6 +301,7 @@ extern "C" pf_status pf_panel_velocity(pf_ctx *ctx, int64_t m, const double *gam
                                        const double *ye, const double *cosa, const double *sina,
                                        int64_t n, const double *xv, const double *yv, double *vx,
                                        double *vy, int accumulate, void *stream) {
+    PF_RANGE("pf_panel_velocity");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_panel_velocity: NULL context");
     PF_CHECK_ARG(m >= 0 && m <= 65536, "pf_panel_velocity: panel count %lld outside [0, 65536]",
@@ -158,9 +320,24 @@ extern "C" pf_status pf_panel_velocity(pf_ctx *ctx, int64_t m, const double *gam
         }
         return PF_OK;
     }
-    const int64_t grid = pf::ceil_div(n, PN_THREADS);
-    PF_CHECK_ARG(grid <= INT32_MAX, "pf_panel_velocity: too many points");
-    k_panel_velocity<<<(unsigned)grid, PN_THREADS, 0, st>>>(m, gamma, xs, ys, xe, ye, cosa, sina,
-                                                           n, xv, yv, vx, vy, accumulate);
+    const int64_t ngroups = pf::ceil_div(m, PC_G);
+    const size_t gbytes = sizeof(PanelGroup) * (size_t)ngroups;
+    const size_t pbytes = sizeof(PanelSm) * (size_t)m;
+    PF_TRY(pf::arena_reserve(ctx, pf::align256(gbytes) + pf::align256(pbytes)));
+    auto *groups = static_cast<PanelGroup *>(pf::arena_take(ctx, gbytes));
+    auto *pan = static_cast<PanelSm *>(pf::arena_take(ctx, pbytes));
+    if (!groups || !pan) {
+        pf::set_error("pf_panel_velocity: scratch too small");
+        return PF_ERR_OOM;
+    }
+    k_panel_groups<<<(unsigned)ngroups, 32, 0, st>>>(m, gamma, xs, ys, xe, ye, cosa, sina, groups,
+                                                     pan);
+    PF_TRY(pf::launch_status("k_panel_groups"));
+    // persistent grid: a few CTAs per SM, each over many blocks of points
+    const int64_t grid = std::min<int64_t>(pf::ceil_div(n, PN_THREADS), (int64_t)ctx->num_sms * 4);
+    // P = ceil(log2(PC_EPS (1 - PC_RHO) / 2) / log2(rho)) terms for rho <= PC_RHO
+    const float log2_tol = (float)std::log2(PC_EPS * (1.0 - PC_RHO) / 2.0);
+    k_panel_velocity<<<(unsigned)grid, PN_THREADS, 0, st>>>(ngroups, groups, pan, m, n, xv, yv, vx,
+                                                           vy, accumulate, log2_tol);
     return pf::launch_status("k_panel_velocity");
 }

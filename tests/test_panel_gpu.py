@@ -51,3 +51,40 @@ def test_accumulate_onto_blob_velocity():
     rx, ry = oracle.panel_velocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina,
                                    xv.cpu().numpy(), yv.cpu().numpy())
     assert normwise_err(vx.cpu().numpy() - 0.25, vy.cpu().numpy() + 0.5, rx, ry) <= TOL
+
+
+def test_far_points_series_to_1e10():
+    """Points well away from the body take the groups' series only: they match
+    the FP64 pair formula to 1e-10 (the series' stated remainder), far inside
+    the 1e-6 gate that the FP32 transcendentals of the near field set."""
+    import pfblob
+    from pfblob import workloads as wl
+    ps = wl.cylinder_panels(512)
+    rng = np.random.default_rng(4)
+    r = rng.uniform(2.0, 6.0, 20000)
+    t = rng.uniform(-np.pi, np.pi, 20000)
+    xv, yv = r * np.cos(t), r * np.sin(t)
+    rx, ry = oracle.panel_velocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina, xv, yv)
+    vx, vy = pfblob.inducedVelocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina, xv, yv)
+    assert normwise_err(vx, vy, rx, ry) <= 1e-10
+
+
+def test_shuffled_panels_and_many_groups():
+    """The grouping never changes the sum: panels in random order (every group
+    spans the body, so every point is near) and a body of 1000 panels (a
+    partial last group, several shared-memory tiles) both meet the gate."""
+    import pfblob
+    from pfblob import workloads as wl
+    rng = np.random.default_rng(6)
+    r = rng.uniform(1.0, 3.0, 8000)
+    t = rng.uniform(-np.pi, np.pi, 8000)
+    xv, yv = r * np.cos(t), r * np.sin(t)
+    for m, shuffle in ((512, True), (1000, False), (1000, True)):
+        ps = wl.cylinder_panels(m)
+        arrs = [ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina]
+        if shuffle:
+            perm = rng.permutation(m)
+            arrs = [a[perm] for a in arrs]
+        rx, ry = oracle.panel_velocity(*arrs, xv, yv)
+        vx, vy = pfblob.inducedVelocity(*arrs, xv, yv)
+        assert normwise_err(vx, vy, rx, ry) <= TOL, (m, shuffle)

@@ -255,7 +255,9 @@ def run_ours(args, rank, world):
     with ClockSampler(gpu_id_for_smi(torch)) as clk:
         for k in range(args.steps):
             flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
-            outs.append(step(evs[k]))
+            # keep only the step's small status tensors: the output blobs are
+            # released, so the allocator reuses their blocks step after step
+            outs.append(step(evs[k])[5:8])
             if method == "fmm":  # reads the FMM's events: synchronises after the step
                 fmm_stats.append(_lib.fmm_last_stats(dev.index))
         torch.cuda.synchronize()
@@ -263,7 +265,7 @@ def run_ours(args, rank, world):
     if method == "fmm":
         _lib.fmm_profile(False, dev.index)
     for o in outs:  # every timed step completed its remesh on the first try
-        kk, st_, _ = settle(o)
+        kk, st_ = int(o[0].item()), int(o[1].item())
         assert st_ == 0 and kk == nout, (kk, st_, nout)
     if world > 1:
         torch.distributed.barrier()
@@ -661,13 +663,17 @@ def run_c3(dev, steps=5, warmup=2):
     torch.cuda.synchronize(dev)
     _lib.fmm_profile(True, dev.index)
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(steps)]
-    stats, outs = [], []
+    stats, out = [], None
     for k in range(steps):
         flush.fill_(float(k))
-        outs.append(step(evs[k]))
+        # the previous step's outputs are released first, so the allocator
+        # reuses their blocks (no device allocation inside the timed steps)
+        out = None
+        out = step(evs[k])
         stats.append(_lib.fmm_last_stats(dev.index))
     torch.cuda.synchronize(dev)
     _lib.fmm_profile(False, dev.index)
+    outs = [out]
     ph = {name: statistics.mean(e[i].elapsed_time(e[i + 1]) for e in evs)
           for i, name in enumerate(("fmm", "panels", "remesh"))}
     ms = sum(ph.values())

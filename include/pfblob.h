@@ -60,6 +60,16 @@ int pf_version(void);
  * all threads).  Diagnostic: the difference across a region is the number of
  * library kernels enqueued in it. */
 uint64_t pf_kernel_launches(void);
+/* 1 in the bounds-checked build (libpfblob_checked.so, compiled with
+ * -DPF_BOUNDS_CHECK), else 0.  In that build the kernels test their
+ * data-dependent indices; a failed test records the first (site, index,
+ * limit) on the device and skips the access instead of trapping. */
+int pf_bounds_checked(void);
+/* Checked build: synchronise `device` (-1: the current device), read and
+ * clear every recorded bounds failure; PF_ERR_CUDA with the site, index and
+ * limit in pf_last_error() if there was one.  Normal build: PF_OK, no work.
+ * (No reference counterpart: the reference has no sanitizer build.) */
+pf_status pf_check_bounds(int device);
 
 /* ---------------------------------------------------------------------------
  * Gaussian-blob Biot-Savart velocity by direct summation, FP32 arithmetic with

@@ -301,6 +301,7 @@ static pf_status batch_enqueue(pf_batch *b) {
 
 extern "C" pf_status pf_batch_create(pf_ctx *ctx, int32_t n, const pf_batch_instance *inst,
                                      double tol, int32_t n_streams, pf_batch **out) {
+    PF_RANGE("pf_batch_create");
     pf::clear_error();
     PF_CHECK_ARG(ctx && out, "pf_batch_create: NULL argument");
     *out = nullptr;
@@ -387,6 +388,7 @@ extern "C" pf_status pf_batch_create(pf_ctx *ctx, int32_t n, const pf_batch_inst
 }
 
 extern "C" pf_status pf_batch_run(pf_batch *b, void *stream) {
+    PF_RANGE("pf_batch_run");
     pf::clear_error();
     PF_CHECK_ARG(b != nullptr, "pf_batch_run: NULL batch");
     pf::DeviceGuard dg(b->ctx->device);

@@ -165,6 +165,7 @@ k_lu_solve(int64_t m, const double *__restrict__ LU, const int32_t *__restrict__
 
 extern "C" pf_status pf_dense_lu_factor(pf_ctx *ctx, int64_t m, double *a, int32_t *ipiv,
                                         int32_t *info_dev, void *stream) {
+    PF_RANGE("pf_dense_lu_factor");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_dense_lu_factor: NULL context");
     PF_CHECK_ARG(m >= 0 && m <= 32768, "pf_dense_lu_factor: m = %lld outside [0, 32768]",
@@ -192,6 +193,7 @@ extern "C" pf_status pf_dense_lu_factor(pf_ctx *ctx, int64_t m, double *a, int32
 
 extern "C" pf_status pf_dense_lu_solve(pf_ctx *ctx, int64_t m, const double *lu,
                                        const int32_t *ipiv, double *b, void *stream) {
+    PF_RANGE("pf_dense_lu_solve");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_dense_lu_solve: NULL context");
     PF_CHECK_ARG(m >= 0 && m <= 32768, "pf_dense_lu_solve: m = %lld outside [0, 32768]",

@@ -259,6 +259,7 @@ extern "C" pf_status pf_velocity_direct(pf_ctx *ctx, int64_t n_src, const double
                                         const double *y, const double *g, int64_t n_tgt,
                                         const double *xt, const double *yt, double ksigmasqr,
                                         double *vx, double *vy, void *stream) {
+    PF_RANGE("pf_velocity_direct");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_velocity_direct: NULL context");
     PF_CHECK_ARG(n_src >= 0 && n_tgt >= 0, "pf_velocity_direct: negative size");

@@ -207,7 +207,8 @@ k_place(int64_t n, const uint32_t *__restrict__ key, const int32_t *__restrict__
         int32_t *__restrict__ big_n) {
     const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (i >= n) return;
-    perm[start[key[i]] + rank[i]] = (int32_t)i;
+    const int64_t p = (int64_t)start[key[i]] + rank[i];
+    if (PF_IDX_OK(p, n, 201)) perm[p] = (int32_t)i;
     // a leaf of more than SEG_SMALL particles (exactly one has this rank) is
     // listed for the segment sort
     if (rank[i] == pf::SEG_SMALL) big[atomicAdd(big_n, 1)] = (int32_t)key[i];
@@ -249,6 +250,7 @@ k_gather_sorted(int64_t n, const int32_t *__restrict__ perm, const double *__res
     const int64_t j = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (j >= n) return;
     const int32_t i = perm[j];
+    if (!PF_IDX_OK(i, n, 202)) return;
     if (skey) skey[j] = key[i];  // leaf key in sorted order (targets)
     const double a = x[i], b = y[i];
     sx[j] = a;
@@ -965,6 +967,7 @@ struct P2PWork {
     unsigned *heavy_n;   // entries in heavy
     int32_t *heavy;      // blocks with several target groups [nblk]
     int32_t *grp_next;   // groups of each heavy block handed out so far [nblk]
+    int64_t ns, nt;      // sorted sources and targets (bounds-checked build)
 };
 
 // Target group gi of block b (groups of at most 96 targets, balanced: sizes
@@ -978,7 +981,7 @@ __device__ __forceinline__ void p2p_group_body(
     const int32_t *__restrict__ run_off, const int2 *__restrict__ runs, pfd::GaussParams gp,
     double2 *__restrict__ nearv, ulonglong2 (*s_hi)[P2P_BUF], ulonglong2 (*s_lo)[P2P_BUF],
     unsigned long long (*s_g2)[P2P_BUF], int *s_rs, int *s_rp, unsigned long long &npairs,
-    unsigned long long &nfar) {
+    unsigned long long &nfar, int64_t ns_all, int64_t nt_all) {
     const int lane = threadIdx.x;
     const unsigned lt = (1u << lane) - 1u;
     const float rser = sqrtf(gp.r2_series);
@@ -993,6 +996,7 @@ __device__ __forceinline__ void p2p_group_body(
     const int qs = cval ? lane / rem : 32;
     const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane % rem;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!PF_IDX_OK((int64_t)t0 + tg + gsz - 1, nt_all, 204)) return;  // the group's last target
     const float4 ta = (lane < gsz) ? thl[t0 + ia] : z4;
     const float4 tb = (lane + 32 < gsz) ? thl[t0 + ib] : z4;
     const float4 tc = cval ? thl[t0 + ic] : z4;
@@ -1056,8 +1060,10 @@ __device__ __forceinline__ void p2p_group_body(
             if (p < S) {
                 while (rr + 1 < nrc && s_rp[rr + 1] <= p) ++rr;
                 const int src = s_rs[rr] + (p - s_rp[rr]);
-                v = shl[src];
-                w = sg32[src];
+                if (PF_IDX_OK(src, ns_all, 203)) {
+                    v = shl[src];
+                    w = sg32[src];
+                }
             }
         };
         fetch(lane, spv, gg);
@@ -1193,7 +1199,8 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
         } else {
             for (int gi = 0; gi < ngrp; ++gi)
                 p2p_group_body(b, t0, tn, ngrp, gi, sstart, scnt, shl, sg32, thl, run_off, runs,
-                               gp, nearv, s_hi, s_lo, s_g2, s_rs, s_rp, npairs, nfar);
+                               gp, nearv, s_hi, s_lo, s_g2, s_rs, s_rp, npairs, nfar, work.ns,
+                               work.nt);
         }
     } else {
         const unsigned nh = *work.heavy_n;  // complete: written by the first launch
@@ -1208,7 +1215,8 @@ k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *_
                 gi = __shfl_sync(0xffffffffu, gi, 0);
                 if ((int)gi >= ngrp) break;
                 p2p_group_body(b, t0, tn, ngrp, (int)gi, sstart, scnt, shl, sg32, thl, run_off,
-                               runs, gp, nearv, s_hi, s_lo, s_g2, s_rs, s_rp, npairs, nfar);
+                               runs, gp, nearv, s_hi, s_lo, s_g2, s_rs, s_rp, npairs, nfar,
+                               work.ns, work.nt);
             }
         }
     }
@@ -1253,6 +1261,7 @@ k_l2p(int64_t nt, int L, double x0, double y0, double wl, const double *__restri
     for (int n = NP - 2; n >= 0; --n) w = cfma(w, z, lam[n]);
     const double2 nv = nearv[i];
     const int32_t o = perm[i];
+    if (!PF_IDX_OK(o, nt, 205)) return;
     vx[o] = nv.x + INV_2PI * iw * w.y;
     vy[o] = nv.y + INV_2PI * iw * w.x;
 }
@@ -1662,7 +1671,8 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     {
         const int64_t nblk = (int64_t)1 << (2 * (L - kb));
         PF_CUDA_TRY(cudaMemsetAsync(p2pw_mem, 0, p2pw_bytes, st));
-        P2PWork work{p2pw_mem, (int32_t *)(p2pw_mem + 64), (int32_t *)(p2pw_mem + 64) + nblk};
+        P2PWork work{p2pw_mem, (int32_t *)(p2pw_mem + 64), (int32_t *)(p2pw_mem + 64) + nblk, ns,
+                     nt};
         const pfd::GaussParams gp = pfd::make_gauss_params(a.ksigmasqr);
         k_p2p<false><<<(unsigned)nblk, 32, 0, st>>>(
             nblk, kb, tstart, T.cnt, S.start, S.cnt, S.hl, S.g32, T.hl, c.d_run_off, c.d_runs,
@@ -1813,6 +1823,7 @@ extern "C" pf_status pf_fmm_set_tuning(int leaf_level, int expansion_terms, int 
 extern "C" pf_status pf_fmm_tree_keys(pf_ctx *ctx, int64_t n, const double *x, const double *y,
                                       double x0, double y0, double leaf_width, int leaf_level,
                                       uint32_t *keys, void *stream) {
+    PF_RANGE("pf_fmm_tree_keys");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_fmm_tree_keys: NULL context");
     PF_CHECK_ARG(leaf_level >= 1 && leaf_level <= 15, "pf_fmm_tree_keys: leaf level outside [1, 15]");
@@ -1937,6 +1948,7 @@ extern "C" pf_status pf_velocity_fmm(pf_ctx *ctx, int64_t n_src, const double *x
                                      const double *yt, double ksigmasqr, double xopt,
                                      double cutoff, double tol, int ndirect, double *vx,
                                      double *vy, void *stream) {
+    PF_RANGE("pf_velocity_fmm");
     pf::clear_error();
     (void)xopt;
     return velocity_fmm(ctx, n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, cutoff, tol, ndirect, vx,
@@ -1949,6 +1961,7 @@ extern "C" pf_status pf_velocity_fmm_box(pf_ctx *ctx, int64_t n_src, const doubl
                                          double xopt, double cutoff, double tol, int ndirect,
                                          const double *box, double *vx, double *vy,
                                          void *stream) {
+    PF_RANGE("pf_velocity_fmm_box");
     pf::clear_error();
     (void)xopt;
     PF_CHECK_ARG(box != nullptr, "pf_velocity_fmm_box: NULL box");

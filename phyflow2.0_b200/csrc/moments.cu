@@ -74,6 +74,7 @@ k_moments_final(const M4 *__restrict__ part, double *__restrict__ out4) {
 
 extern "C" pf_status pf_moments(pf_ctx *ctx, int64_t n, const double *x, const double *y,
                                 const double *g, double *out4, void *stream) {
+    PF_RANGE("pf_moments");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_moments: NULL context");
     PF_CHECK_ARG(n >= 0, "pf_moments: negative size");

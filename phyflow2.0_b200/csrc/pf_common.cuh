@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <cstdarg>
 #include <cstdio>
 #include <memory>
@@ -38,6 +40,31 @@ void clear_error();
             return PF_ERR_INVALID_ARG;                                            \
         }                                                                         \
     } while (0)
+
+// --------------------------------------------------------------------------
+// NVTX range over one C-ABI call, named after the entry point (ncu --nvtx
+// filters on it; with no tool attached NVTX v3 costs one predicted branch).
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
+#define PF_RANGE(name) ::pf::Range pf_range_(name)
+
+// --------------------------------------------------------------------------
+// Bounds-checked build (-DPF_BOUNDS_CHECK, libpfblob_checked.so): kernels test
+// their data-dependent indices with PF_IDX_OK(i, n, site); a failed test
+// records (site, i, n) in a device word of its translation unit -- the first
+// one wins -- and the access is skipped, so nothing traps or faults.
+// pf_check_bounds() synchronises and reads and clears every unit's word.  In
+// the normal build PF_IDX_OK is the constant true and compiles away.
+struct BoundsRecord {
+    unsigned long long site;  // 0: no failure
+    long long index, limit;
+};
+using BoundsReader = bool (*)(BoundsRecord *rec);  // reads and clears; false on CUDA error
+void bounds_register(BoundsReader r);
 
 #define PF_TRY(expr)                                                              \
     do {                                                                          \
@@ -161,3 +188,40 @@ __device__ __forceinline__ float rcp_approx(float x) {
 }
 
 }  // namespace pfd
+
+// Per translation unit: the device word of the bounds-checked build and its
+// host reader, registered at load time.
+#ifdef PF_BOUNDS_CHECK
+namespace {
+__device__ pf::BoundsRecord pf_bounds_word;
+
+__device__ __noinline__ bool pf_idx_fail(long long i, long long n, int site) {
+    if (atomicCAS(&pf_bounds_word.site, 0ull, (unsigned long long)site) == 0ull) {
+        pf_bounds_word.index = i;
+        pf_bounds_word.limit = n;
+    }
+    return false;
+}
+
+__device__ __forceinline__ bool pf_idx_ok(long long i, long long n, int site) {
+    return (i >= 0 && i < n) ? true : pf_idx_fail(i, n, site);
+}
+
+bool pf_bounds_read(pf::BoundsRecord *rec) {
+    const pf::BoundsRecord zero = {0ull, 0, 0};
+    if (cudaMemcpyFromSymbol(rec, pf_bounds_word, sizeof(*rec)) != cudaSuccess) return false;
+    if (rec->site != 0ull && cudaMemcpyToSymbol(pf_bounds_word, &zero, sizeof(zero)) != cudaSuccess)
+        return false;
+    return true;
+}
+
+struct PfBoundsRegistration {
+    PfBoundsRegistration() { pf::bounds_register(&pf_bounds_read); }
+};
+PfBoundsRegistration pf_bounds_registration;
+}  // namespace
+#define PF_IDX_OK(i, n, site) pf_idx_ok((long long)(i), (long long)(n), (site))
+#else
+#define PF_IDX_OK(i, n, site) true
+#endif
+

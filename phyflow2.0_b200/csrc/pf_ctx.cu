@@ -1,4 +1,7 @@
 // pf_ctx.cu -- context, scratch arena and error reporting of libpfblob.
+#include <mutex>
+#include <vector>
+
 #include "pf_common.cuh"
 
 #include <atomic>
@@ -60,6 +63,19 @@ pf_status arena_reserve(pf_ctx *ctx, size_t bytes) {
     ctx->arena.base = static_cast<char *>(p);
     ctx->arena.cap = want;
     return PF_OK;
+}
+
+// Readers of the translation units' bounds words (checked build).  A
+// function-local static: units register during library load, in any order.
+static std::vector<BoundsReader> &bounds_readers() {
+    static std::vector<BoundsReader> v;
+    return v;
+}
+static std::mutex g_bounds_mu;
+
+void bounds_register(BoundsReader r) {
+    std::lock_guard<std::mutex> lk(g_bounds_mu);
+    bounds_readers().push_back(r);
 }
 
 void *arena_take(pf_ctx *ctx, size_t bytes) {
@@ -155,5 +171,39 @@ pf_status pf_trim(pf_ctx *ctx) {
 int pf_version(void) { return PF_VERSION; }
 
 uint64_t pf_kernel_launches(void) { return pf::g_launches.load(std::memory_order_relaxed); }
+
+int pf_bounds_checked(void) {
+#ifdef PF_BOUNDS_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+pf_status pf_check_bounds(int device) {
+    pf::clear_error();
+#ifdef PF_BOUNDS_CHECK
+    int cur = 0;
+    PF_CUDA_TRY(cudaGetDevice(&cur));
+    pf::DeviceGuard dg(device >= 0 ? device : cur);
+    PF_CUDA_TRY(cudaDeviceSynchronize());
+    std::lock_guard<std::mutex> lk(pf::g_bounds_mu);
+    for (pf::BoundsReader r : pf::bounds_readers()) {
+        pf::BoundsRecord rec;
+        if (!r(&rec)) {
+            pf::set_error("pf_check_bounds: reading a bounds word failed");
+            return PF_ERR_CUDA;
+        }
+        if (rec.site != 0ull) {
+            pf::set_error("bounds check failed at site %llu: index %lld outside [0, %lld)",
+                          rec.site, rec.index, rec.limit);
+            return PF_ERR_CUDA;
+        }
+    }
+#else
+    (void)device;
+#endif
+    return PF_OK;
+}
 
 }  // extern "C"

@@ -193,6 +193,7 @@ extern "C" pf_status pf_population_control(pf_ctx *ctx, int64_t n, const double 
                                            double *x_out, double *y_out, double *g_out,
                                            int64_t *n_out_dev, double *threshold_dev,
                                            void *stream) {
+    PF_RANGE("pf_population_control");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_population_control: NULL context");
     PF_CHECK_ARG(n >= 0 && n < ((int64_t)1 << 31), "pf_population_control: n = %lld outside [0, 2^31)",

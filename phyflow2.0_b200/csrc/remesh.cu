@@ -412,6 +412,10 @@ k_rm_count(const double *__restrict__ x, const double *__restrict__ y, int64_t n
         return;
     }
     const int32_t c = (int32_t)(a * w.nby + b);
+    if (!PF_IDX_OK(c, (int64_t)w.nbx * w.nby, 101)) {
+        cell[i] = -1;
+        return;
+    }
     cell[i] = c;
     rank[i] = atomicAdd(&count[c], 1);
 }
@@ -592,6 +596,7 @@ k_rm_place(int64_t n, RmHead *hd, const int32_t *__restrict__ cell,
         if (c < 0) continue;
         const int32_t r = rank[i];
         const int64_t p = (int64_t)start[c] + r;
+        if (!PF_IDX_OK(p, n, 102)) continue;
         const double xi = x[i], yi = y[i], gi = g[i];
         const double v1 = TUTTY ? xi : __ddiv_rn(xi, wp.h);
         const double v2 = TUTTY ? yi : __ddiv_rn(yi, wp.h);
@@ -621,13 +626,42 @@ k_rm_big_gather(const int32_t *__restrict__ list, const RmHead *__restrict__ hd,
     }
 }
 
+// Weights of the tile kernel: M4' with any c, M4' with c = 0, Tutty.
+constexpr int WK_M4 = 0, WK_M4_PLAIN = 1, WK_TUTTY = 2;
+
+// M4' at c = 0 on the node's known branch.  x_L = ceil(s) - 1 with s = x/h -
+// xb0/h - 1.5 (_regridding.py:162) puts u_a = x_L + a - (s + 1) in [-2, -1),
+// [-1, 0), [0, 1), [1, 2) for a = 0..3, so nodes 0 and 3 take the outer
+// polynomial and nodes 1 and 2 the inner one.  At |u| = 1 both are 0 (which is
+// also the reference's value there), and where rounding puts a computed u an
+// ulp across 1 both polynomials are within an ulp-sized amount of 0, so the
+// weights match the value-branched m4p to ~1e-16 absolute.
+__device__ __forceinline__ double m4p_outer(double u) {
+    const double a = fabs(u);
+    const double t = 2.0 - a;
+    return 0.5 * (t * t) * (1.0 - a);
+}
+__device__ __forceinline__ double m4p_inner(double u) {
+    const double a = fabs(u);
+    const double a2 = u * u;
+    return 1.0 - 2.5 * a2 + 1.5 * (a2 * a);
+}
+
 // blob_w8 from a record's values: M4' takes x/h, y/h as computed in
 // k_rm_place (the same IEEE quotients blob_w8 forms), Tutty takes x, y.
-template <bool TUTTY>
+template <int WK>
 __device__ __forceinline__ void rec_w8(double v1, double v2, int64_t ix0, int64_t iy0,
                                        const WParams &wp, double (&wx)[4], double (&wy)[4]) {
-    if (TUTTY) {
+    if (WK == WK_TUTTY) {
         blob_w8<true>(v1, v2, ix0, iy0, wp, wx, wy);
+    } else if (WK == WK_M4_PLAIN) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const double ux = __dsub_rn(__dadd_rn(((double)ix0 + (double)a) + 0.5, wp.qx0), v1);
+            const double uy = __dsub_rn(__dadd_rn(((double)iy0 + (double)a) + 0.5, wp.qy0), v2);
+            wx[a] = (a == 0 || a == 3) ? m4p_outer(ux) : m4p_inner(ux);
+            wy[a] = (a == 0 || a == 3) ? m4p_outer(uy) : m4p_inner(uy);
+        }
     } else {
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
@@ -694,12 +728,13 @@ struct TileOut {
     int64_t *ixo, *iyo;
     double *acc;    // cell values (cells mode)
     int32_t *flag;  // touched flags (cells mode)
+    int64_t nrec;   // records (blobs placed): bounds-checked build
 };
 
 // One CTA per tile of TOX x TOY output cells (persistent loop over tiles).
 // EMIT: the new blobs are written at their slots; else the cell values and
 // touched flags of every window cell go to acc / flag.
-template <bool TUTTY, bool EMIT>
+template <int WK, bool EMIT>
 __global__ void __launch_bounds__(TILE_THREADS, 2)
 k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
           const int32_t *__restrict__ start, const WRec *__restrict__ recs,
@@ -728,6 +763,7 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
             if (bx >= 0 && bx < w.nbx && by >= 0 && by < w.nby) {
                 const int64_t bc = bx * w.nby + by;
                 cnt = count[bc];
+                if (cnt > 0 && !PF_IDX_OK((int64_t)start[bc] + cnt - 1, to.nrec, 105)) cnt = 0;
                 if (cnt > 0) {
                     const WRec *rc = recs + start[bc];
                     const int64_t ix0 = lat_x(w, bx), iy0 = lat_y(w, by);
@@ -762,7 +798,7 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
                         const double2 vv = *reinterpret_cast<const double2 *>(rc + bj);
                         const double gv = rc[bj].g;
                         double wx[4], wy[4];
-                        rec_w8<TUTTY>(vv.x, vv.y, ix0, iy0, wp, wx, wy);
+                        rec_w8<WK>(vv.x, vv.y, ix0, iy0, wp, wx, wy);
 #pragma unroll
                         for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -800,7 +836,7 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
                     }
                 const int64_t cid = ox * w.noy + oy;
                 if (EMIT) {
-                    if (touched && emit_ok) {
+                    if (touched && emit_ok && PF_IDX_OK(to.slot[cid], to.capacity, 106)) {
                         const int64_t q = to.slot[cid];
                         const int64_t ix = lat_x(w, ox), iy = lat_y(w, oy);
                         // (ix*h + 0.5h) + xb0, each operation rounded (no FMA)
@@ -860,6 +896,7 @@ k_rm_emit(int64_t cap_cell, const RmHead *__restrict__ hd, WParams wp,
     const int64_t ox = cid / w.noy, oy = cid - ox * w.noy;
     const int64_t ix = lat_x(w, ox), iy = lat_y(w, oy);
     const int64_t p = slot[cid];
+    if (!PF_IDX_OK(p, capacity, 107)) return;
     xo[p] = __dadd_rn(__dadd_rn(__dmul_rn((double)ix, wp.h), wp.h05), wp.xb0);
     yo[p] = __dadd_rn(__dadd_rn(__dmul_rn((double)iy, wp.h), wp.h05), wp.yb0);
     go[p] = acc[cid];
@@ -1016,23 +1053,21 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
         const int64_t tiles_cap = ceil_div(cap_cell, (int64_t)TOX * TOY) + 64;
         const unsigned gt = (unsigned)std::max<int64_t>(
             1, std::min<int64_t>(std::min<int64_t>(2 * num_sms, gt_max), tiles_cap));
-        TileOut to{slot, capacity, xo, yo, go, ixo, iyo, acc, flag};
-        if (tutty && cells)
-            k_rm_tile<true, false><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs,
-                                                                 part_big, wp, to,
-                                                                 mpart + 4 * gn_max, hd);
-        else if (tutty)
-            k_rm_tile<true, true><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs,
-                                                                part_big, wp, to,
-                                                                 mpart + 4 * gn_max, hd);
-        else if (cells)
-            k_rm_tile<false, false><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs,
-                                                                  part_big, wp, to,
-                                                                 mpart + 4 * gn_max, hd);
-        else
-            k_rm_tile<false, true><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs,
-                                                                 part_big, wp, to,
-                                                                 mpart + 4 * gn_max, hd);
+        TileOut to{slot, capacity, xo, yo, go, ixo, iyo, acc, flag, n};
+        const int wk = tutty ? WK_TUTTY : (wp.prm == 0.0 ? WK_M4_PLAIN : WK_M4);
+        double *const mp = mpart + 4 * gn_max;
+#define PF_RM_TILE(K, E) \
+    k_rm_tile<K, E><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs, part_big, wp, to, mp, hd)
+        if (cells) {
+            if (wk == WK_TUTTY) PF_RM_TILE(WK_TUTTY, false);
+            else if (wk == WK_M4_PLAIN) PF_RM_TILE(WK_M4_PLAIN, false);
+            else PF_RM_TILE(WK_M4, false);
+        } else {
+            if (wk == WK_TUTTY) PF_RM_TILE(WK_TUTTY, true);
+            else if (wk == WK_M4_PLAIN) PF_RM_TILE(WK_M4_PLAIN, true);
+            else PF_RM_TILE(WK_M4, true);
+        }
+#undef PF_RM_TILE
         PF_TRY(launch_status("k_rm_tile"));
     }
     if (cells) {
@@ -1229,6 +1264,7 @@ extern "C" pf_status pf_remesh(pf_ctx *ctx, int64_t n, const double *x, const do
                                const double *g, double h, double xb0, double yb0, double c,
                                int64_t capacity, double *x_out, double *y_out, double *g_out,
                                int64_t *ix_out, int64_t *iy_out, int64_t *n_out, void *stream) {
+    PF_RANGE("pf_remesh");
     pf::clear_error();
     return remesh_sync(ctx, n, x, y, g, h, xb0, yb0, c, capacity, x_out, y_out, g_out, ix_out,
                        iy_out, n_out, nullptr, nullptr, pf::REMESH_M4, stream);
@@ -1239,6 +1275,7 @@ extern "C" pf_status pf_remesh_tutty(pf_ctx *ctx, int64_t n, const double *x, co
                                      double hnu, int64_t capacity, double *x_out, double *y_out,
                                      double *g_out, int64_t *ix_out, int64_t *iy_out,
                                      int64_t *n_out, void *stream) {
+    PF_RANGE("pf_remesh_tutty");
     pf::clear_error();
     PF_CHECK_ARG(std::isfinite(hnu) && hnu >= 0.0, "pf_remesh_tutty: hnu must be >= 0 and finite");
     return remesh_sync(ctx, n, x, y, g, h, xb0, yb0, hnu, capacity, x_out, y_out, g_out, ix_out,
@@ -1250,6 +1287,7 @@ extern "C" pf_status pf_remesh_population_control(
     double xb0, double yb0, double c, double g_threshold_local, double g_threshold_global,
     int64_t capacity, double *x_out, double *y_out, double *g_out, int64_t *ix_out,
     int64_t *iy_out, int64_t *n_out, double *threshold_used, void *stream) {
+    PF_RANGE("pf_remesh_population_control");
     pf::clear_error();
     PF_CHECK_ARG(n_out != nullptr, "pf_remesh_population_control: n_out is NULL");
     *n_out = 0;
@@ -1267,6 +1305,7 @@ extern "C" pf_status pf_remesh_async(pf_ctx *ctx, int64_t n, const double *x, co
                                      double *y_out, double *g_out, int64_t *ix_out,
                                      int64_t *iy_out, int64_t *n_out_dev, int32_t *status_dev,
                                      int64_t *window_dev, double *moments_dev, void *stream) {
+    PF_RANGE("pf_remesh_async");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_remesh_async: NULL context");
     PF_TRY(check_remesh_args("pf_remesh_async", n, x, y, g, h, xb0, yb0, c, capacity, x_out, y_out,
@@ -1294,6 +1333,7 @@ extern "C" pf_status pf_remesh_window(pf_ctx *ctx, int64_t n, const double *x, c
                                       int64_t capacity, double *x_out, double *y_out,
                                       double *g_out, int64_t *ix_out, int64_t *iy_out,
                                       int64_t *n_out_dev, int32_t *status_dev, void *stream) {
+    PF_RANGE("pf_remesh_window");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_remesh_window: NULL context");
     PF_TRY(check_remesh_args("pf_remesh_window", n, x, y, g, h, xb0, yb0, c, capacity, x_out,

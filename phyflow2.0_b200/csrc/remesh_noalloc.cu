@@ -76,6 +76,7 @@ extern "C" pf_status pf_remesh_window_noalloc(int64_t n, const double *x, const 
                                               double *y_out, double *g_out, int64_t *ix_out,
                                               int64_t *iy_out, int64_t *n_out_dev,
                                               int32_t *status_dev, void *stream) {
+    PF_RANGE("pf_remesh_window_noalloc");
     pf::clear_error();
     PF_CHECK_ARG(n >= 0 && n < ((int64_t)1 << 31), "pf_remesh_window_noalloc: bad n");
     PF_CHECK_ARG(h > 0.0 && h < 1e300, "pf_remesh_window_noalloc: h must be positive and finite");

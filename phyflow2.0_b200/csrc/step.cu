@@ -8,6 +8,7 @@
 #include "fmm_api.cuh"
 
 extern "C" pf_status pf_blob_step(pf_ctx *ctx, const pf_step *s, void *stream) {
+    PF_RANGE("pf_blob_step");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_blob_step: NULL context");
     PF_CHECK_ARG(s != nullptr, "pf_blob_step: NULL step");

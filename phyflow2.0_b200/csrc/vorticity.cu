@@ -124,6 +124,7 @@ extern "C" pf_status pf_vorticity_direct(pf_ctx *ctx, int64_t n_src, const doubl
                                          const double *y, const double *g, int64_t n_tgt,
                                          const double *xt, const double *yt, double ksigmasqr,
                                          double *w, void *stream) {
+    PF_RANGE("pf_vorticity_direct");
     pf::clear_error();
     PF_CHECK_ARG(ctx != nullptr, "pf_vorticity_direct: NULL context");
     PF_CHECK_ARG(n_src >= 0 && n_tgt >= 0, "pf_vorticity_direct: negative size");

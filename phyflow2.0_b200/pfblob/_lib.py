@@ -8,12 +8,15 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libpfblob.so")
+# PFBLOB_CHECKED=1 selects the bounds-checked build (libpfblob_checked.so):
+# every call is then followed by pf_check_bounds, which synchronises.
+CHECKED = os.environ.get("PFBLOB_CHECKED", "0") not in ("", "0")
+LIB_PATH = os.path.join(_HERE, "libpfblob_checked.so" if CHECKED else "libpfblob.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(
-        f"pfblob: {LIB_PATH} is not built; run `python phyflow2.0_b200/build.py` "
-        "(the package has no CPU fallback)")
+        f"pfblob: {LIB_PATH} is not built; run `python phyflow2.0_b200/build.py"
+        f"{' --checked' if CHECKED else ''}` (the package has no CPU fallback)")
 
 lib = ctypes.CDLL(LIB_PATH)
 
@@ -37,6 +40,8 @@ PROTOTYPES = {
     "pf_trim": [_vp],
     "pf_version": [],
     "pf_kernel_launches": [],
+    "pf_bounds_checked": [],
+    "pf_check_bounds": [_int],
     "pf_velocity_direct": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _vp, _vp, _vp],
     "pf_vorticity_direct": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _vp, _vp],
     "pf_velocity_fmm": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _int,
@@ -104,6 +109,8 @@ class CapacityError(PfError):
 
 
 def check(status):
+    if status == PF_OK and CHECKED:
+        status = lib.pf_check_bounds(-1)
     if status != PF_OK:
         msg = lib.pf_last_error()
         raise PfError(status, msg.decode() if msg else "")

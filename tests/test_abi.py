@@ -31,6 +31,22 @@ def test_library_exports_every_declared_symbol():
     assert not missing, f"libpfblob.so lacks {missing}"
 
 
+def test_checked_library_exports_every_declared_symbol():
+    """The bounds-checked build (-DPF_BOUNDS_CHECK) has the same ABI and says
+    which build it is; the normal build says it is not checked, and its
+    pf_check_bounds is a no-op that needs no GPU."""
+    path = os.path.join(ROOT, "phyflow2.0_b200", "pfblob", "libpfblob_checked.so")
+    if not os.path.exists(path):
+        pytest.skip("libpfblob_checked.so not built (build.py --checked)")
+    lib = ctypes.CDLL(path)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, f"libpfblob_checked.so lacks {missing}"
+    assert lib.pf_bounds_checked() == 1
+    plain = ctypes.CDLL(LIB)
+    assert plain.pf_bounds_checked() == 0
+    assert plain.pf_check_bounds(-1) == 0
+
+
 def test_python_prototypes_cover_header():
     import pfblob._lib as L
     assert set(declared_symbols()) <= set(L.PROTOTYPES)
@@ -60,9 +76,12 @@ def test_null_context_is_rejected_without_gpu():
     assert b"NULL context" in L.lib.pf_last_error()
 
 
-NO_STATUS = {"pf_last_error", "pf_version", "pf_kernel_launches", "pf_fmm_plan_builds"}
+NO_STATUS = {"pf_last_error", "pf_version", "pf_kernel_launches", "pf_fmm_plan_builds",
+             "pf_bounds_checked"}
 NULL_IS_NOOP = {"pf_destroy", "pf_batch_destroy"}  # like free(NULL)
-ZEROS_VALID = {"pf_fmm_set_tuning"}  # 0 = automatic choice of every knob
+# pf_fmm_set_tuning: 0 = automatic choice of every knob; pf_check_bounds: a
+# no-op in the normal build
+ZEROS_VALID = {"pf_fmm_set_tuning", "pf_check_bounds"}
 
 
 def test_every_entry_point_rejects_null_arguments_without_gpu():

@@ -621,9 +621,9 @@ def run_batched(dev, n_sims=256, steps=5, n_streams=8):
     return out
 
 
-def run_c3(dev, steps=5, warmup=2):
+def run_c3(dev, n=1 << 22, steps=5, warmup=2):
     """The near-wall shear-layer configuration at its stated size: N = 2^22
-    blobs in the annulus 1 <= r <= 1.5 plus 512 vortex panels on the unit
+    blobs (n) in the annulus 1 <= r <= 1.5 plus 512 vortex panels on the unit
     circle.  One step = FMM blob velocity + panel velocity added on top + the
     M4' remesh (window found on the device).  CUDA events per phase."""
     import torch
@@ -631,7 +631,7 @@ def run_c3(dev, steps=5, warmup=2):
     from pfblob import _lib
     from pfblob.regrid import remesh_device_async
     wl = workloads()
-    b = wl.shear_layer(n=1 << 22)
+    b = wl.shear_layer(n=n)
     ps = wl.cylinder_panels(512)
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     x, y, g = T(b.x), T(b.y), T(b.g)
@@ -790,6 +790,11 @@ def main():
                     help="skip the accuracy check of the timed step against the FP64 oracle")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched (256 simulations) and served (1024 simulations) sections")
+    ap.add_argument("--only", default=None, choices=["c3", "evolve", "batched", "served"],
+                    help="run one extra section alone and print its JSON (profiling captures)")
+    ap.add_argument("--c3-n", type=int, default=1 << 22,
+                    help="blobs of the near-wall section (default 2^22; smaller for captures)")
+    ap.add_argument("--c3-steps", type=int, default=5)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
 
@@ -804,10 +809,18 @@ def main():
         import datetime
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.only is not None:
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        sec = {"c3": lambda: run_c3(dev, n=args.c3_n, steps=args.c3_steps),
+               "evolve": lambda: run_evolve(dev), "batched": lambda: run_batched(dev),
+               "served": lambda: run_served(dev)}[args.only]()
+        print(json.dumps({"section": args.only, **sec}), flush=True)
+        return
     line = run_ours(args, rank, world)
     if rank == 0 and world == 1 and not args.no_extras and args.n is None:
         dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
-        line["c3"] = run_c3(dev)
+        line["c3"] = run_c3(dev, n=args.c3_n, steps=args.c3_steps)
         line["evolve"] = run_evolve(dev)
         line["batched"] = run_batched(dev)
         line["served"] = run_served(dev)

@@ -531,8 +531,40 @@ def run_reference(args):
     }
 
 
+def kernel_baselines():
+    """The reference's compiled Cython kernels on this host's cores (OpenMP,
+    every host thread): the direct Gauss sum on the C1 Lamb-Oseen lattice
+    (10,000 blobs, all 1e8 pairs) and the vortex-panel velocity on 16,384
+    seeded points of the near-wall set x 512 panels.  Pairs per second."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    wl = workloads()
+    out = {"threads": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))}
+    c1 = wl.lamb_oseen_lattice()
+    ref.direct_gauss(c1.x[:64], c1.y[:64], c1.g[:64], c1.ksigmasqr)  # load the module
+    t0 = time.perf_counter()
+    ref.direct_gauss(c1.x, c1.y, c1.g, c1.ksigmasqr)
+    t = time.perf_counter() - t0
+    out["direct_c1"] = {"pairs_per_s": float(c1.n) ** 2 / t, "ms": t * 1e3, "n": c1.n,
+                        "kernel": "vv2parGauss_Cython_cpu (reference Cython, OpenMP)"}
+    sl = wl.shear_layer(n=1 << 22)
+    ps = wl.cylinder_panels(512)
+    idx = np.sort(np.random.default_rng(7).choice(sl.n, 16384, replace=False))
+    args = (ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina)
+    ref.panel_velocity(*args, sl.x[idx[:64]], sl.y[idx[:64]])
+    t0 = time.perf_counter()
+    ref.panel_velocity(*args, sl.x[idx], sl.y[idx])
+    t = time.perf_counter() - t0
+    out["panels_c3_sample"] = {"pairs_per_s": 16384 * 512 / t, "ms": t * 1e3, "points": 16384,
+                               "panels": 512,
+                               "kernel": "_vortexPanel_Cython_cpu.inducedVelocity (reference Cython)"}
+    return out
+
+
 def cpu_baseline(n=None):
-    """One full step of the reference's CPU path on this host (rank 0, N=1)."""
+    """One full step of the reference's CPU path on this host (rank 0, N=1),
+    plus the reference's Cython direct and panel kernels on their own."""
     b = workload_c2(n)
     rs = ReferenceStep(b)
     try:
@@ -544,7 +576,7 @@ def cpu_baseline(n=None):
     hi = host_info()
     return {"value": b.n / t, "unit": "evals/s", "cores": rs.procs, "kind": rs.kind,
             "sample": "one step, " + rs.describe(), "ms_per_step": t * 1e3, "nproc": hi["nproc"],
-            "cpu_model": hi["cpu_model"]}
+            "cpu_model": hi["cpu_model"], "kernels": kernel_baselines()}
 
 
 # ---------------------------------------------------------------------------
@@ -708,6 +740,51 @@ def run_c3(dev, n=1 << 22, steps=5, warmup=2):
             "l2": "flushed between timed steps"}
 
 
+def run_c1(dev, steps=20, warmup=3):
+    """The reference's CPU-runnable configuration: the 100 x 100 Lamb-Oseen
+    lattice (N = 10,000, h = 0.02), direct-sum velocity at every blob and one
+    M4' remesh, timed per phase with CUDA events on inputs already on the GPU."""
+    import torch
+    import pfblob
+    from pfblob.regrid import remesh_device_async
+    b = workloads().lamb_oseen_lattice()
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    x, y, g = T(b.x), T(b.y), T(b.g)
+    vx, vy = torch.empty_like(x), torch.empty_like(x)
+    xb, yb = b.bounds()
+    st = torch.cuda.current_stream(dev)
+    mb = max(4 * b.n, 4096)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(st)
+        pfblob.velocity_device(x, y, g, b.ksigmasqr, x, y, vx, vy, method=pfblob.DIRECT_METHOD)
+        if ev:
+            ev[1].record(st)
+        out = remesh_device_async(x, y, g, b.h, xb[0], yb[0], max_base_cells=mb)
+        if ev:
+            ev[2].record(st)
+        return out
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    out = None
+    for k in range(steps):
+        out = None
+        out = step(evs[k])
+    torch.cuda.synchronize(dev)
+    vel = statistics.median(e[0].elapsed_time(e[1]) for e in evs)
+    rm = statistics.median(e[1].elapsed_time(e[2]) for e in evs)
+    return {"workload": "C1 Lamb-Oseen lattice: N=10000 (h=0.02, sigma=h/0.8), direct velocity at "
+                        "every blob + M4' remesh", "n_blobs": b.n, "ms_per_step": vel + rm,
+            "phase_ms": {"velocity": vel, "remesh": rm},
+            "direct_pairs_per_s": float(b.n) ** 2 / (vel * 1e-3),
+            "n_out": int(out[3].item()), "status": int(out[4].item()),
+            "timing": "medians of CUDA-event phases; inputs resident, L2 not flushed (the set is 0.24 MB)"}
+
+
 def run_evolve(dev, steps=10, warmup=2):
     """A moving blob set: ``Blobs.evolve`` on the C2 blobs (forward-Euler
     convection by the FMM velocity, redistribution and population control
@@ -790,7 +867,7 @@ def main():
                     help="skip the accuracy check of the timed step against the FP64 oracle")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched (256 simulations) and served (1024 simulations) sections")
-    ap.add_argument("--only", default=None, choices=["c3", "evolve", "batched", "served"],
+    ap.add_argument("--only", default=None, choices=["c1", "c3", "evolve", "batched", "served"],
                     help="run one extra section alone and print its JSON (profiling captures)")
     ap.add_argument("--c3-n", type=int, default=1 << 22,
                     help="blobs of the near-wall section (default 2^22; smaller for captures)")
@@ -812,7 +889,7 @@ def main():
     if args.only is not None:
         dev = torch.device("cuda", 0)
         torch.cuda.set_device(dev)
-        sec = {"c3": lambda: run_c3(dev, n=args.c3_n, steps=args.c3_steps),
+        sec = {"c1": lambda: run_c1(dev), "c3": lambda: run_c3(dev, n=args.c3_n, steps=args.c3_steps),
                "evolve": lambda: run_evolve(dev), "batched": lambda: run_batched(dev),
                "served": lambda: run_served(dev)}[args.only]()
         print(json.dumps({"section": args.only, **sec}), flush=True)
@@ -820,6 +897,7 @@ def main():
     line = run_ours(args, rank, world)
     if rank == 0 and world == 1 and not args.no_extras and args.n is None:
         dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+        line["c1"] = run_c1(dev)
         line["c3"] = run_c3(dev, n=args.c3_n, steps=args.c3_steps)
         line["evolve"] = run_evolve(dev)
         line["batched"] = run_batched(dev)

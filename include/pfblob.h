@@ -90,6 +90,19 @@ pf_status pf_velocity_direct(pf_ctx *ctx, int64_t n_src, const double *x, const 
                              const double *yt, double ksigmasqr, double *vx, double *vy,
                              void *stream);
 
+/* Cutoff (Rosenhead-Krasny) kernel by direct summation, same arithmetic
+ * scheme as pf_velocity_direct:
+ *   v_k = 1/(2 pi) sum_m g_m (-dy, dx) / (dx^2 + dy^2 + sigmasqr).
+ * Replaces vv2par_C_cpu (src/cpp/blobs/c/vv2par_C/vv2par_C_cpu.c:88-161) and
+ * vv2par_gpu (src/cpp/blobs/cuda/vv2par_gpu/vv2par_device.cu:59-70), reached
+ * from _velocity_direct_{cpu,gpu}_cutoff (src/python/blobs/base/induced/
+ * _induced.py:521-699) with sigmasqr = sigma^2.  The reference has no FMM for
+ * this kernel (_induced.py:159-163). */
+pf_status pf_velocity_direct_cutoff(pf_ctx *ctx, int64_t n_src, const double *x, const double *y,
+                                    const double *g, int64_t n_tgt, const double *xt,
+                                    const double *yt, double sigmasqr, double *vx, double *vy,
+                                    void *stream);
+
 /* ---------------------------------------------------------------------------
  * Induced vorticity of Gaussian blobs by direct summation (same FP32
  * hi/lo + compensated scheme as pf_velocity_direct), FP64 in and out:
@@ -104,6 +117,15 @@ pf_status pf_velocity_direct(pf_ctx *ctx, int64_t n_src, const double *x, const 
 pf_status pf_vorticity_direct(pf_ctx *ctx, int64_t n_src, const double *x, const double *y,
                               const double *g, int64_t n_tgt, const double *xt,
                               const double *yt, double ksigmasqr, double *w, void *stream);
+
+/* Induced vorticity of the cutoff kernel as the reference computes it,
+ *   w_k = 1/(2 pi) sum_m g_m / sqrt(dx^2 + dy^2 + sigmasqr).
+ * Replaces ww2par_C_cpu (src/cpp/blobs/c/ww2par_C/ww2par_C_cpu.c:88-150) and
+ * ww2par_gpu (src/cpp/blobs/cuda/ww2par_gpu/ww2par_device.cu:59-70), reached
+ * from _vorticity_direct_{cpu,gpu}_cutoff (_induced.py:969-1123). */
+pf_status pf_vorticity_direct_cutoff(pf_ctx *ctx, int64_t n_src, const double *x, const double *y,
+                                     const double *g, int64_t n_tgt, const double *xt,
+                                     const double *yt, double sigmasqr, double *w, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Blob velocity by the 2D fast multipole method (uniform quadtree, FP64

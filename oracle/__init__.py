@@ -22,9 +22,11 @@ Contents
     pHyFlow sources into ``oracle/_ref/`` (Cython direct Gauss, Cython vortex
     panels, the C++ CPU FMM).  These pin the restatement.
 """
-from .core import (velocity_direct, vorticity_direct, panel_velocity, m4prime, remesh_left_index,
-                   moments, oracle_lib)
+from .core import (velocity_direct, vorticity_direct, velocity_direct_cutoff,
+                   vorticity_direct_cutoff, panel_velocity, m4prime, remesh_left_index, moments,
+                   oracle_lib)
 from .regrid import diffusion_tutty, population_control, regrid
 
-__all__ = ["velocity_direct", "vorticity_direct", "panel_velocity", "m4prime", "remesh_left_index",
+__all__ = ["velocity_direct", "vorticity_direct", "velocity_direct_cutoff",
+           "vorticity_direct_cutoff", "panel_velocity", "m4prime", "remesh_left_index",
            "moments", "regrid", "population_control", "diffusion_tutty", "oracle_lib"]

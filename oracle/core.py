@@ -33,11 +33,16 @@ def oracle_lib():
         lib.or_velocity_direct_gauss.argtypes = [i64, _dp, _dp, _dp, i64, _dp, _dp, dbl, _dp, _dp, cint]
         lib.or_vorticity_direct_gauss.argtypes = [i64, _dp, _dp, _dp, i64, _dp, _dp, dbl, _dp,
                                                   cint]
+        lib.or_velocity_direct_cutoff.argtypes = [i64, _dp, _dp, _dp, i64, _dp, _dp, dbl, _dp,
+                                                  _dp, cint]
+        lib.or_vorticity_direct_cutoff.argtypes = [i64, _dp, _dp, _dp, i64, _dp, _dp, dbl, _dp,
+                                                   cint]
         lib.or_panel_velocity.argtypes = [i64, _dp, _dp, _dp, _dp, _dp, _dp, _dp, i64, _dp, _dp, _dp, _dp, cint]
         lib.or_m4prime.argtypes = [i64, _dp, dbl, _dp]
         lib.or_remesh_left_index.argtypes = [i64, _dp, dbl, dbl, _ip]
         lib.or_moments.argtypes = [i64, _dp, _dp, _dp, _dp]
         for f in (lib.or_velocity_direct_gauss, lib.or_vorticity_direct_gauss,
+                  lib.or_velocity_direct_cutoff, lib.or_vorticity_direct_cutoff,
                   lib.or_panel_velocity, lib.or_m4prime,
                   lib.or_remesh_left_index, lib.or_moments):
             f.restype = None
@@ -76,6 +81,31 @@ def vorticity_direct(xs, ys, gs, ksigmasqr, xt=None, yt=None, nthreads=0):
     w = np.empty(xt.shape[0])
     oracle_lib().or_vorticity_direct_gauss(xs.shape[0], _p(xs), _p(ys), _p(gs), xt.shape[0],
                                            _p(xt), _p(yt), float(ksigmasqr), _p(w), int(nthreads))
+    return w
+
+
+def velocity_direct_cutoff(xs, ys, gs, sigmasqr, xt=None, yt=None, nthreads=0):
+    """FP64 cutoff-kernel velocity; restates ``vv2par_C_cpu`` (sigmasqr =
+    sigma^2, as ``_velocity_direct_cpu_cutoff`` passes it)."""
+    xs, ys, gs = _f64(xs), _f64(ys), _f64(gs)
+    xt = xs if xt is None else _f64(xt)
+    yt = ys if yt is None else _f64(yt)
+    vx = np.empty(xt.shape[0])
+    vy = np.empty(xt.shape[0])
+    oracle_lib().or_velocity_direct_cutoff(xs.shape[0], _p(xs), _p(ys), _p(gs), xt.shape[0],
+                                           _p(xt), _p(yt), float(sigmasqr), _p(vx), _p(vy),
+                                           int(nthreads))
+    return vx, vy
+
+
+def vorticity_direct_cutoff(xs, ys, gs, sigmasqr, xt=None, yt=None, nthreads=0):
+    """FP64 cutoff-kernel induced vorticity; restates ``ww2par_C_cpu``."""
+    xs, ys, gs = _f64(xs), _f64(ys), _f64(gs)
+    xt = xs if xt is None else _f64(xt)
+    yt = ys if yt is None else _f64(yt)
+    w = np.empty(xt.shape[0])
+    oracle_lib().or_vorticity_direct_cutoff(xs.shape[0], _p(xs), _p(ys), _p(gs), xt.shape[0],
+                                            _p(xt), _p(yt), float(sigmasqr), _p(w), int(nthreads))
     return w
 
 

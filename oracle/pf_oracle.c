@@ -81,6 +81,59 @@ void or_vorticity_direct_gauss(int64_t ns, const double *xs, const double *ys,
     }
 }
 
+/* Cutoff-kernel velocity by direct summation: restates vv2par_C_cpu
+ * (src/cpp/blobs/c/vv2par_C/vv2par_C_cpu.c:135-151) and the Cython twin
+ * (src/cpp/blobs/cython/vv2par_Cython/vv2par_Cython_cpu.pyx):
+ *   r2 = dx*dx + dy*dy + sigmasqr ;  s = g/r2 ;  vx -= dy*s ; vy += dx*s
+ * then both scaled by 1/(2 pi). */
+void or_velocity_direct_cutoff(int64_t ns, const double *xs, const double *ys,
+                               const double *gs, int64_t nt, const double *xt,
+                               const double *yt, double sigmasqr, double *vx,
+                               double *vy, int nthreads)
+{
+    const double inv_2pi = 0.5 / OR_PI;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t k = 0; k < nt; ++k) {
+        double ax = 0.0, ay = 0.0;
+        for (int64_t m = 0; m < ns; ++m) {
+            const double dx = xt[k] - xs[m];
+            const double dy = yt[k] - ys[m];
+            const double r2 = dx * dx + dy * dy + sigmasqr;
+            const double s = gs[m] / r2;
+            ax -= dy * s;
+            ay += dx * s;
+        }
+        vx[k] = inv_2pi * ax;
+        vy[k] = inv_2pi * ay;
+    }
+}
+
+/* Cutoff-kernel induced vorticity as the reference computes it: restates
+ * ww2par_C_cpu (src/cpp/blobs/c/ww2par_C/ww2par_C_cpu.c:132-145):
+ *   w_k = (1/(2 pi)) sum_m g_m / sqrt(dx^2 + dy^2 + sigmasqr) */
+void or_vorticity_direct_cutoff(int64_t ns, const double *xs, const double *ys,
+                                const double *gs, int64_t nt, const double *xt,
+                                const double *yt, double sigmasqr, double *w, int nthreads)
+{
+    const double inv_2pi = 0.5 / OR_PI;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t k = 0; k < nt; ++k) {
+        double wk = 0.0;
+        for (int64_t m = 0; m < ns; ++m) {
+            const double dx = xt[k] - xs[m];
+            const double dy = yt[k] - ys[m];
+            wk += gs[m] / sqrt(dx * dx + dy * dy + sigmasqr);
+        }
+        w[k] = inv_2pi * wk;
+    }
+}
+
 /* Constant-strength straight vortex panels, induced velocity at points.
  * Follows src/cpp/panels/cython/vortexPanel_Cython/_vortexPanel_Cython_cpu.pyx
  * :352-393 (Katz & Plotkin 11.2.3): rotate the point into the panel frame,

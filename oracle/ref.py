@@ -137,3 +137,49 @@ def m4kernel_1d(x, c):
     p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     _cache["m4"].ref_m4kernel_1d(x.shape[0], p(x), float(c), p(w))
     return w
+
+
+def cutoff_available():
+    return os.path.exists(os.path.join(REF_DIR, "libref_cutoff.so"))
+
+
+def _cutoff_lib():
+    if "cutoff" not in _cache:
+        lib = ctypes.CDLL(os.path.join(REF_DIR, "libref_cutoff.so"))
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib.ref_vv2par_cutoff.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, dp, dp,
+                                          ctypes.c_double, dp, dp]
+        lib.ref_ww2par_cutoff.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, dp, dp,
+                                          ctypes.c_double, dp]
+        lib.ref_vv2par_cutoff.restype = None
+        lib.ref_ww2par_cutoff.restype = None
+        _cache["cutoff"] = lib
+    return _cache["cutoff"]
+
+
+def _targets(x, y, g, xt, yt):
+    x, y, g = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, g))
+    xt = x if xt is None else np.ascontiguousarray(xt, dtype=np.float64)
+    yt = y if yt is None else np.ascontiguousarray(yt, dtype=np.float64)
+    return x, y, g, xt, yt
+
+
+def velocity_cutoff(x, y, g, sigmasqr, xt=None, yt=None):
+    """The reference's own cutoff-kernel velocity loop (vv2par_C_cpu.c:133-151)
+    -> (vx, vy) at the targets (the blobs if None)."""
+    x, y, g, xt, yt = _targets(x, y, g, xt, yt)
+    vx, vy = np.empty(xt.shape[0]), np.empty(xt.shape[0])
+    p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    _cutoff_lib().ref_vv2par_cutoff(x.shape[0], p(x), p(y), p(g), xt.shape[0], p(xt), p(yt),
+                                    float(sigmasqr), p(vx), p(vy))
+    return vx, vy
+
+
+def vorticity_cutoff(x, y, g, sigmasqr, xt=None, yt=None):
+    """The reference's own cutoff-kernel vorticity loop (ww2par_C_cpu.c:130-145)."""
+    x, y, g, xt, yt = _targets(x, y, g, xt, yt)
+    w = np.empty(xt.shape[0])
+    p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    _cutoff_lib().ref_ww2par_cutoff(x.shape[0], p(x), p(y), p(g), xt.shape[0], p(xt), p(yt),
+                                    float(sigmasqr), p(w))
+    return w

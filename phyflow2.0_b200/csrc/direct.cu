@@ -16,7 +16,10 @@
 //
 // Replaces vv2par_kernel (src/cpp/blobs/cuda/vv2parGauss_gpu/
 // vv2parGauss_device.cu:107-162: FP64, one target per thread, 2 exp per pair,
-// targets padded to a multiple of the block size by the Python caller).
+// targets padded to a multiple of the block size by the Python caller).  The
+// CUTOFF variant sums the cutoff kernel g / (r^2 + sigma^2) of vv2par_C_cpu
+// (src/cpp/blobs/c/vv2par_C/vv2par_C_cpu.c:135-151) and its GPU twin
+// (src/cpp/blobs/cuda/vv2par_gpu/vv2par_device.cu:59-70) the same way.
 #include "direct_api.cuh"
 #include "gauss_pair.cuh"
 
@@ -31,9 +34,11 @@ constexpr int64_t DT_TILE = DT_THREADS * 2;      // targets per CTA
 
 // One CTA computes the 2*DT_THREADS targets of tile `tile`: each thread owns
 // targets base and base + DT_THREADS and evaluates both against every source
-// with the packed f32x2 pair arithmetic (gauss_pair.cuh).
+// with the packed f32x2 pair arithmetic (gauss_pair.cuh); CUTOFF: the cutoff
+// kernel with core size squared s2.
 // Sources [s_begin, s_end) only; with `part` non-null the (hi, lo) sums go to
 // part[split * nt + target] instead of the velocities.
+template <bool CUTOFF = false>
 __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
                                             const double *__restrict__ ys,
                                             const double *__restrict__ gs, int64_t s_begin,
@@ -42,7 +47,8 @@ __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
                                             const pfd::GaussParams &gp, double *__restrict__ vx,
                                             double *__restrict__ vy, float4 *__restrict__ part,
                                             int64_t split, int64_t tile, ulonglong2 *s_hi,
-                                            ulonglong2 *s_lo, unsigned long long *s_g2) {
+                                            ulonglong2 *s_lo, unsigned long long *s_g2,
+                                            float s2 = 0.f) {
     const int64_t base = tile * DT_TILE + threadIdx.x;
     float th[2][4];
 #pragma unroll
@@ -59,6 +65,7 @@ __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
     const pfd::f32x2 txh = pfd::pack2(th[0][0], th[1][0]), tyh = pfd::pack2(th[0][1], th[1][1]);
     const pfd::f32x2 txl = pfd::pack2(th[0][2], th[1][2]), tyl = pfd::pack2(th[0][3], th[1][3]);
     const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
+    const pfd::f32x2 s22 = pfd::pack2(s2, s2);
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 
     for (int64_t t0 = s_begin; t0 < s_end; t0 += DT_THREADS) {
@@ -82,9 +89,14 @@ __device__ __forceinline__ void direct_tile(const double *__restrict__ xs,
         for (int c0 = 0; c0 < nvalid; c0 += DT_CHUNK) {
             pfd::f32x2 nx = 0ull, ny = 0ull;
 #pragma unroll 4
-            for (int k = 0; k < DT_CHUNK; ++k)
-                pfd::pair2(s_hi[c0 + k], s_lo[c0 + k], s_g2[c0 + k], txh, tyh, txl, tyl, gp2, nx,
-                           ny);
+            for (int k = 0; k < DT_CHUNK; ++k) {
+                if (CUTOFF)
+                    pfd::pair2_cutoff(s_hi[c0 + k], s_lo[c0 + k], s_g2[c0 + k], txh, tyh, txl, tyl,
+                                      s22, nx, ny);
+                else
+                    pfd::pair2(s_hi[c0 + k], s_lo[c0 + k], s_g2[c0 + k], txh, tyh, txl, tyl, gp2,
+                               nx, ny);
+            }
             float nxa, nxb, nya, nyb;
             pfd::unpack2(nx, nxa, nxb);
             pfd::unpack2(ny, nya, nyb);
@@ -130,20 +142,20 @@ k_direct_reduce(const float4 *__restrict__ part, int64_t nt, int splits, double 
 }
 
 // grid (target tiles, source segments); one segment = the plain sum.
-template <int TPT>
+template <int TPT, bool CUTOFF = false>
 __global__ void __launch_bounds__(DT_THREADS)
 k_direct_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
                const double *__restrict__ gs, int64_t ns, int64_t seg,
                const double *__restrict__ xt, const double *__restrict__ yt, int64_t nt,
                pfd::GaussParams gp, double *__restrict__ vx, double *__restrict__ vy,
-               float4 *__restrict__ part) {
+               float4 *__restrict__ part, float s2 = 0.f) {
     static_assert(TPT == 2, "two targets per thread (packed pairs)");
     __shared__ ulonglong2 s_hi[DT_THREADS];  // {x_hi, x_hi}, {y_hi, y_hi}
     __shared__ ulonglong2 s_lo[DT_THREADS];  // {x_lo, x_lo}, {y_lo, y_lo}
     __shared__ unsigned long long s_g2[DT_THREADS];
     const int64_t s0 = (int64_t)blockIdx.y * seg;
-    direct_tile(xs, ys, gs, s0, min(ns, s0 + seg), xt, yt, nt, gp, vx, vy, part, blockIdx.y,
-                blockIdx.x, s_hi, s_lo, s_g2);
+    direct_tile<CUTOFF>(xs, ys, gs, s0, min(ns, s0 + seg), xt, yt, nt, gp, vx, vy, part,
+                        blockIdx.y, blockIdx.x, s_hi, s_lo, s_g2, s2);
 }
 
 // Persistent batched direct sum: CTAs take (instance, target tile) items from
@@ -203,9 +215,11 @@ DirectSplit direct_split(int64_t ns, int64_t nt) {
 // take their partial buffer from the context's arena.
 pf_status launch_direct(pf_ctx *ctx, int64_t ns, const double *x, const double *y,
                         const double *g, int64_t nt, const double *xt, const double *yt,
-                        double ksigmasqr, double *vx, double *vy, cudaStream_t stream) {
+                        double ksigmasqr, double *vx, double *vy, cudaStream_t stream,
+                        bool cutoff) {
     if (nt == 0) return PF_OK;
-    const pfd::GaussParams gp = pfd::make_gauss_params(ksigmasqr);
+    // cutoff: ksigmasqr is sigma^2 and only enters as the core term of r^2
+    const pfd::GaussParams gp = pfd::make_gauss_params(cutoff ? 1.0 : ksigmasqr);
     constexpr int TPT = 2;
     const int64_t grid = ceil_div(nt, DT_TILE);
     if (grid > INT32_MAX) {
@@ -223,8 +237,14 @@ pf_status launch_direct(pf_ctx *ctx, int64_t ns, const double *x, const double *
             return PF_ERR_OOM;
         }
     }
-    k_direct_gauss<TPT><<<dim3((unsigned)grid, (unsigned)sp.splits), DT_THREADS, 0, stream>>>(
-        x, y, g, ns, sp.seg, xt, yt, nt, gp, vx, vy, part);
+    if (cutoff) {
+        k_direct_gauss<TPT, true>
+            <<<dim3((unsigned)grid, (unsigned)sp.splits), DT_THREADS, 0, stream>>>(
+                x, y, g, ns, sp.seg, xt, yt, nt, gp, vx, vy, part, (float)ksigmasqr);
+    } else {
+        k_direct_gauss<TPT><<<dim3((unsigned)grid, (unsigned)sp.splits), DT_THREADS, 0, stream>>>(
+            x, y, g, ns, sp.seg, xt, yt, nt, gp, vx, vy, part);
+    }
     PF_TRY(launch_status("k_direct_gauss"));
     if (!part) return PF_OK;
     k_direct_reduce<<<(unsigned)ceil_div(nt, DT_THREADS), DT_THREADS, 0, stream>>>(part, nt,
@@ -277,4 +297,30 @@ extern "C" pf_status pf_velocity_direct(pf_ctx *ctx, int64_t n_src, const double
         return PF_OK;
     }
     return pf::launch_direct(ctx, n_src, x, y, g, n_tgt, xt, yt, ksigmasqr, vx, vy, st);
+}
+
+extern "C" pf_status pf_velocity_direct_cutoff(pf_ctx *ctx, int64_t n_src, const double *x,
+                                               const double *y, const double *g, int64_t n_tgt,
+                                               const double *xt, const double *yt,
+                                               double sigmasqr, double *vx, double *vy,
+                                               void *stream) {
+    PF_RANGE("pf_velocity_direct_cutoff");
+    pf::clear_error();
+    PF_CHECK_ARG(ctx != nullptr, "pf_velocity_direct_cutoff: NULL context");
+    PF_CHECK_ARG(n_src >= 0 && n_tgt >= 0, "pf_velocity_direct_cutoff: negative size");
+    PF_CHECK_ARG(sigmasqr > 0.0 && sigmasqr < 1e30,
+                 "pf_velocity_direct_cutoff: sigmasqr must be positive and finite (got %g)",
+                 sigmasqr);
+    PF_CHECK_ARG(n_src == 0 || (x && y && g), "pf_velocity_direct_cutoff: NULL blob array");
+    PF_CHECK_ARG(n_tgt == 0 || (xt && yt && vx && vy),
+                 "pf_velocity_direct_cutoff: NULL target/output array");
+    pf::DeviceGuard dg(ctx->device);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (n_tgt == 0) return PF_OK;
+    if (n_src == 0) {
+        PF_CUDA_TRY(cudaMemsetAsync(vx, 0, sizeof(double) * n_tgt, st));
+        PF_CUDA_TRY(cudaMemsetAsync(vy, 0, sizeof(double) * n_tgt, st));
+        return PF_OK;
+    }
+    return pf::launch_direct(ctx, n_src, x, y, g, n_tgt, xt, yt, sigmasqr, vx, vy, st, true);
 }

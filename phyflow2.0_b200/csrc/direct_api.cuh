@@ -39,8 +39,10 @@ int direct_batch_grid(int num_sms);
 pf_status launch_direct_batch(const DirectInstance *inst_dev, const int2 *items_dev, int n_items,
                               const int2 *reduce_items_dev, int n_reduce, int *counter_dev,
                               int grid, cudaStream_t st);
+// cutoff = true: the cutoff kernel g / (r^2 + ksigmasqr), ksigmasqr = sigma^2
 pf_status launch_direct(pf_ctx *ctx, int64_t ns, const double *x, const double *y,
                         const double *g, int64_t nt, const double *xt, const double *yt,
-                        double ksigmasqr, double *vx, double *vy, cudaStream_t stream);
+                        double ksigmasqr, double *vx, double *vy, cudaStream_t stream,
+                        bool cutoff = false);
 
 }  // namespace pf

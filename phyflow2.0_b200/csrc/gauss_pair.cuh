@@ -187,4 +187,21 @@ __device__ __forceinline__ void pair2_far(const ulonglong2 &hi, const ulonglong2
     ny = fma2(dx, s, ny);
 }
 
+// Cutoff (Rosenhead-Krasny) kernel of the reference's vv2par
+// (src/cpp/blobs/c/vv2par_C/vv2par_C_cpu.c:143-148): s = g / (r^2 + sigma^2),
+// nx += dy*s, ny += dx*s; s2 = {sigma^2, sigma^2}.  The pair2_far arithmetic
+// with sigma^2 in place of 1e-12.
+__device__ __forceinline__ void pair2_cutoff(const ulonglong2 &hi, const ulonglong2 &lo, f32x2 g2,
+                                             f32x2 txh, f32x2 tyh, f32x2 txl, f32x2 tyl, f32x2 s2,
+                                             f32x2 &nx, f32x2 &ny) {
+    const f32x2 dx = add2(sub2(txh, hi.x), sub2(txl, lo.x));
+    const f32x2 dy = add2(sub2(tyh, hi.y), sub2(tyl, lo.y));
+    const f32x2 r2 = fma2(dx, dx, fma2(dy, dy, s2));
+    float ra, rb;
+    unpack2(r2, ra, rb);
+    const f32x2 s = mul2(g2, pack2(rcp_approx(ra), rcp_approx(rb)));
+    nx = fma2(dy, s, nx);
+    ny = fma2(dx, s, ny);
+}
+
 }  // namespace pfd

@@ -187,6 +187,12 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return y;
 }
 
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 }  // namespace pfd
 
 // Per translation unit: the device word of the bounds-checked build and its

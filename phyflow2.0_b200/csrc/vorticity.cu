@@ -11,6 +11,11 @@
 // stream through shared memory as hi/lo float pairs, FP32 partial sums over 32
 // sources fold into TwoSum-compensated (hi, lo) accumulators, and small sets
 // cut the sources into segments (direct_split) reduced in segment order.
+//
+// The CUTOFF variant is the cutoff kernel's induced vorticity of
+// ww2par_C_cpu (src/cpp/blobs/c/ww2par_C/ww2par_C_cpu.c:132-145) and its GPU
+// twin (src/cpp/blobs/cuda/ww2par_gpu/ww2par_device.cu:59-70), as
+// those compute it: w_k = 1/(2 pi) sum_m g_m / sqrt(r2 + sigma^2).
 #include "direct_api.cuh"
 #include "gauss_pair.cuh"
 
@@ -22,6 +27,7 @@ constexpr int VT_THREADS = 256;
 constexpr int VT_CHUNK = 32;
 constexpr int64_t VT_TILE = VT_THREADS * 2;
 constexpr double INV_PI = 0.3183098861837907;  // 1/pi
+constexpr double INV_2PI = 0.15915494309189535;  // 1/(2 pi)
 
 // Two targets (packed) against one source: acc += g * 2^(r2 * c_t).
 __device__ __forceinline__ void wpair2(const ulonglong2 &hi, const ulonglong2 &lo, pfd::f32x2 g2,
@@ -36,11 +42,27 @@ __device__ __forceinline__ void wpair2(const ulonglong2 &hi, const ulonglong2 &l
     acc = pfd::fma2(g2, pfd::pack2(pfd::ex2_approx(ta), pfd::ex2_approx(tb)), acc);
 }
 
+// Cutoff kernel: acc += g / sqrt(r2 + sigma^2), s2 = {sigma^2, sigma^2}.
+__device__ __forceinline__ void wpair2_cutoff(const ulonglong2 &hi, const ulonglong2 &lo,
+                                              pfd::f32x2 g2, pfd::f32x2 txh, pfd::f32x2 tyh,
+                                              pfd::f32x2 txl, pfd::f32x2 tyl, pfd::f32x2 s2,
+                                              pfd::f32x2 &acc) {
+    const pfd::f32x2 dx = pfd::add2(pfd::sub2(txh, hi.x), pfd::sub2(txl, lo.x));
+    const pfd::f32x2 dy = pfd::add2(pfd::sub2(tyh, hi.y), pfd::sub2(tyl, lo.y));
+    const pfd::f32x2 r2 = pfd::fma2(dx, dx, pfd::fma2(dy, dy, s2));
+    float ra, rb;
+    pfd::unpack2(r2, ra, rb);
+    acc = pfd::fma2(g2, pfd::pack2(pfd::rsqrt_approx(ra), pfd::rsqrt_approx(rb)), acc);
+}
+
+// w = (c1 * sum) / scale: Gauss c1 = 1/pi, scale = ksigmasqr; cutoff c1 =
+// 1/(2 pi), scale = 1.
+template <bool CUTOFF>
 __global__ void __launch_bounds__(VT_THREADS)
 k_vort_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
              const double *__restrict__ gs, int64_t ns, int64_t seg,
              const double *__restrict__ xt, const double *__restrict__ yt, int64_t nt,
-             pfd::GaussParams gp, double scale, double *__restrict__ w,
+             pfd::GaussParams gp, double c1, double scale, float s2, double *__restrict__ w,
              float2 *__restrict__ part) {
     __shared__ ulonglong2 s_hi[VT_THREADS];  // {x_hi, x_hi}, {y_hi, y_hi}
     __shared__ ulonglong2 s_lo[VT_THREADS];  // {x_lo, x_lo}, {y_lo, y_lo}
@@ -63,6 +85,7 @@ k_vort_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
     const pfd::f32x2 txh = pfd::pack2(th[0][0], th[1][0]), tyh = pfd::pack2(th[0][1], th[1][1]);
     const pfd::f32x2 txl = pfd::pack2(th[0][2], th[1][2]), tyl = pfd::pack2(th[0][3], th[1][3]);
     const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
+    const pfd::f32x2 s22 = pfd::pack2(s2, s2);
     float acc[4] = {0.f, 0.f, 0.f, 0.f};  // (hi, lo) of targets a and b
     for (int64_t t0 = s_begin; t0 < s_end; t0 += VT_THREADS) {
         const int64_t s = t0 + threadIdx.x;
@@ -85,8 +108,13 @@ k_vort_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
         for (int c0 = 0; c0 < nvalid; c0 += VT_CHUNK) {
             pfd::f32x2 p = 0ull;
 #pragma unroll 4
-            for (int k = 0; k < VT_CHUNK; ++k)
-                wpair2(s_hi[c0 + k], s_lo[c0 + k], s_g2[c0 + k], txh, tyh, txl, tyl, gp2, p);
+            for (int k = 0; k < VT_CHUNK; ++k) {
+                if (CUTOFF)
+                    wpair2_cutoff(s_hi[c0 + k], s_lo[c0 + k], s_g2[c0 + k], txh, tyh, txl, tyl,
+                                  s22, p);
+                else
+                    wpair2(s_hi[c0 + k], s_lo[c0 + k], s_g2[c0 + k], txh, tyh, txl, tyl, gp2, p);
+            }
             float pa, pb;
             pfd::unpack2(p, pa, pb);
             pfd::comp_add(acc[0], acc[1], pa);
@@ -100,13 +128,13 @@ k_vort_gauss(const double *__restrict__ xs, const double *__restrict__ ys,
         if (part)
             part[(int64_t)blockIdx.y * nt + i] = make_float2(acc[2 * j], acc[2 * j + 1]);
         else
-            w[i] = (INV_PI * ((double)acc[2 * j] + (double)acc[2 * j + 1])) / scale;
+            w[i] = (c1 * ((double)acc[2 * j] + (double)acc[2 * j + 1])) / scale;
     }
 }
 
-// w = (1/pi * sum over segments of (hi + lo)) / ksigmasqr, segments in order.
+// w = (c1 * sum over segments of (hi + lo)) / scale, segments in order.
 __global__ void __launch_bounds__(VT_THREADS)
-k_vort_reduce(const float2 *__restrict__ part, int64_t nt, int splits, double scale,
+k_vort_reduce(const float2 *__restrict__ part, int64_t nt, int splits, double c1, double scale,
               double *__restrict__ w) {
     const int64_t i = (int64_t)blockIdx.x * VT_THREADS + threadIdx.x;
     if (i >= nt) return;
@@ -115,23 +143,22 @@ k_vort_reduce(const float2 *__restrict__ part, int64_t nt, int splits, double sc
         const float2 p = part[(int64_t)k * nt + i];
         s += (double)p.x + (double)p.y;
     }
-    w[i] = (INV_PI * s) / scale;
+    w[i] = (c1 * s) / scale;
 }
 
 }  // namespace
 
-extern "C" pf_status pf_vorticity_direct(pf_ctx *ctx, int64_t n_src, const double *x,
-                                         const double *y, const double *g, int64_t n_tgt,
-                                         const double *xt, const double *yt, double ksigmasqr,
-                                         double *w, void *stream) {
-    PF_RANGE("pf_vorticity_direct");
-    pf::clear_error();
-    PF_CHECK_ARG(ctx != nullptr, "pf_vorticity_direct: NULL context");
-    PF_CHECK_ARG(n_src >= 0 && n_tgt >= 0, "pf_vorticity_direct: negative size");
-    PF_CHECK_ARG(ksigmasqr > 0.0 && ksigmasqr < 1e300,
-                 "pf_vorticity_direct: ksigmasqr must be positive and finite (got %g)", ksigmasqr);
-    PF_CHECK_ARG(n_src == 0 || (x && y && g), "pf_vorticity_direct: NULL blob array");
-    PF_CHECK_ARG(n_tgt == 0 || (xt && yt && w), "pf_vorticity_direct: NULL target/output array");
+static pf_status vorticity_direct(pf_ctx *ctx, const char *name, int64_t n_src, const double *x,
+                                  const double *y, const double *g, int64_t n_tgt,
+                                  const double *xt, const double *yt, double param, double *w,
+                                  void *stream, bool cutoff) {
+    PF_CHECK_ARG(ctx != nullptr, "%s: NULL context", name);
+    PF_CHECK_ARG(n_src >= 0 && n_tgt >= 0, "%s: negative size", name);
+    PF_CHECK_ARG(param > 0.0 && param < (cutoff ? 1e30 : 1e300),
+                 "%s: %s must be positive and finite (got %g)", name,
+                 cutoff ? "sigmasqr" : "ksigmasqr", param);
+    PF_CHECK_ARG(n_src == 0 || (x && y && g), "%s: NULL blob array", name);
+    PF_CHECK_ARG(n_tgt == 0 || (xt && yt && w), "%s: NULL target/output array", name);
     pf::DeviceGuard dg(ctx->device);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (n_tgt == 0) return PF_OK;
@@ -140,9 +167,10 @@ extern "C" pf_status pf_vorticity_direct(pf_ctx *ctx, int64_t n_src, const doubl
         return PF_OK;
     }
     const int64_t grid = pf::ceil_div(n_tgt, VT_TILE);
-    PF_CHECK_ARG(grid <= INT32_MAX, "pf_vorticity_direct: too many targets (%lld)",
-                 (long long)n_tgt);
-    const pfd::GaussParams gp = pfd::make_gauss_params(ksigmasqr);
+    PF_CHECK_ARG(grid <= INT32_MAX, "%s: too many targets (%lld)", name, (long long)n_tgt);
+    const pfd::GaussParams gp = pfd::make_gauss_params(cutoff ? 1.0 : param);
+    const double c1 = cutoff ? INV_2PI : INV_PI, scale = cutoff ? 1.0 : param;
+    const float s2 = cutoff ? (float)param : 0.f;
     const pf::DirectSplit sp = pf::direct_split(n_src, n_tgt);
     float2 *part = nullptr;
     if (sp.splits > 1) {
@@ -150,15 +178,40 @@ extern "C" pf_status pf_vorticity_direct(pf_ctx *ctx, int64_t n_src, const doubl
         PF_TRY(pf::arena_reserve(ctx, bytes + 256));
         part = static_cast<float2 *>(pf::arena_take(ctx, bytes));
         if (!part) {
-            pf::set_error("pf_vorticity_direct: scratch too small");
+            pf::set_error("%s: scratch too small", name);
             return PF_ERR_OOM;
         }
     }
-    k_vort_gauss<<<dim3((unsigned)grid, (unsigned)sp.splits), VT_THREADS, 0, st>>>(
-        x, y, g, n_src, sp.seg, xt, yt, n_tgt, gp, ksigmasqr, w, part);
+    const dim3 grd((unsigned)grid, (unsigned)sp.splits);
+    if (cutoff)
+        k_vort_gauss<true><<<grd, VT_THREADS, 0, st>>>(x, y, g, n_src, sp.seg, xt, yt, n_tgt, gp,
+                                                       c1, scale, s2, w, part);
+    else
+        k_vort_gauss<false><<<grd, VT_THREADS, 0, st>>>(x, y, g, n_src, sp.seg, xt, yt, n_tgt, gp,
+                                                        c1, scale, s2, w, part);
     PF_TRY(pf::launch_status("k_vort_gauss"));
     if (!part) return PF_OK;
     k_vort_reduce<<<(unsigned)pf::ceil_div(n_tgt, VT_THREADS), VT_THREADS, 0, st>>>(
-        part, n_tgt, sp.splits, ksigmasqr, w);
+        part, n_tgt, sp.splits, c1, scale, w);
     return pf::launch_status("k_vort_reduce");
+}
+
+extern "C" pf_status pf_vorticity_direct(pf_ctx *ctx, int64_t n_src, const double *x,
+                                         const double *y, const double *g, int64_t n_tgt,
+                                         const double *xt, const double *yt, double ksigmasqr,
+                                         double *w, void *stream) {
+    PF_RANGE("pf_vorticity_direct");
+    pf::clear_error();
+    return vorticity_direct(ctx, "pf_vorticity_direct", n_src, x, y, g, n_tgt, xt, yt, ksigmasqr,
+                            w, stream, false);
+}
+
+extern "C" pf_status pf_vorticity_direct_cutoff(pf_ctx *ctx, int64_t n_src, const double *x,
+                                                const double *y, const double *g, int64_t n_tgt,
+                                                const double *xt, const double *yt,
+                                                double sigmasqr, double *w, void *stream) {
+    PF_RANGE("pf_vorticity_direct_cutoff");
+    pf::clear_error();
+    return vorticity_direct(ctx, "pf_vorticity_direct_cutoff", n_src, x, y, g, n_tgt, xt, yt,
+                            sigmasqr, w, stream, true);
 }

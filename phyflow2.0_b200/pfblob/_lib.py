@@ -43,7 +43,9 @@ PROTOTYPES = {
     "pf_bounds_checked": [],
     "pf_check_bounds": [_int],
     "pf_velocity_direct": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _vp, _vp, _vp],
+    "pf_velocity_direct_cutoff": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _vp, _vp, _vp],
     "pf_vorticity_direct": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _vp, _vp],
+    "pf_vorticity_direct_cutoff": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _vp, _vp],
     "pf_velocity_fmm": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _int,
                         _vp, _vp, _vp],
     "pf_velocity_fmm_box": [_vp, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _dbl, _dbl, _dbl, _dbl,

@@ -3,13 +3,14 @@
 ``velocity`` keeps the signature, argument meaning and option constants of
 ``pHyFlow.blobs.base.induced.velocity`` (``src/python/blobs/base/induced/
 _induced.py:34-166``): ``fullOption = 100*method + 10*hardware + kernel``
-selects direct or FMM summation of the Gaussian kernel.
+selects direct or FMM summation of the Gaussian kernel (``kernel=1``) or the
+direct sum of the cutoff kernel (``kernel=0``); the FMM of the cutoff kernel
+raises the reference's own exception (:159-163).
 
 Differences, by design of this library:
 * every combination runs on the B200 (``hardware`` is accepted for
-  compatibility; there is no CPU path);
-* the cutoff kernel (``kernel=0``) is outside this library's scope and raises,
-  as the reference does for its unsupported combinations (:159-163);
+  compatibility, and selects only which of the reference's messages an
+  unavailable combination raises; there is no CPU path);
 * ``blocksize`` is accepted and ignored: no padding is needed.
 """
 import ctypes
@@ -92,15 +93,20 @@ def velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=DIRECT_METHOD, xo
 
 def velocity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None, hardware=0,
              blocksize=128, method=0, Ndirect=35, tol=1.0e-6, cutoff=None):
-    """Induced velocity of Gaussian vortex blobs at (xEval, yEval).
+    """Induced velocity of vortex blobs at (xEval, yEval): Gaussian kernel
+    (direct or FMM) or cutoff kernel (direct).
 
     Same arguments and return value as pHyFlow's ``velocity``; returns
     ``(vx, vy)`` as numpy arrays for numpy input, CUDA tensors for CUDA input.
     """
-    if kernel != GAUSS_KERNEL:
-        raise NotImplementedError("pfblob: only the Gaussian kernel (kernel=1) is provided")
+    if kernel not in (GAUSS_KERNEL, CUTOFF_KERNEL):
+        raise ValueError(f"pfblob: unknown kernel {kernel}")
     if method not in (FMM_METHOD, DIRECT_METHOD):
         raise ValueError(f"pfblob: unknown method {method}")
+    if kernel == CUTOFF_KERNEL and method == FMM_METHOD:
+        # the reference's messages for these combinations (_induced.py:159-163)
+        where = "GPU" if hardware == GPU_HARDWARE else "CPU"
+        raise Exception(f'FMM calculation of cutoff kernel on the {where} not yet available')
     m = Marshal(xBlob.device.index if isinstance(xBlob, torch.Tensor) and xBlob.is_cuda else None)
     x, y, g = m.dev(xBlob), m.dev(yBlob), m.dev(wBlob)
     if not (x.numel() == y.numel() == g.numel()):
@@ -112,22 +118,41 @@ def velocity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None, 
         if xt.numel() != yt.numel():
             raise ValueError("pfblob: xEval and yEval must have the same length")
     vx, vy = m.empty(xt.numel()), m.empty(xt.numel())
+    if kernel == CUTOFF_KERNEL:
+        velocity_cutoff_device(x, y, g, float(sigma) * float(sigma), xt, yt, vx, vy,
+                               device=m.index)
+        return m.outs(vx, vy)
     ksigmasqr, xopt, cut = fmm_parameters(float(sigma), float(k), cutoff, float(tol))
     velocity_device(x, y, g, ksigmasqr, xt, yt, vx, vy, method=method, xopt=xopt, cutoff=cut,
                     tol=float(tol), ndirect=int(Ndirect), device=m.index)
     return m.outs(vx, vy)
 
 
+def velocity_cutoff_device(x, y, g, sigmasqr, xt, yt, vx, vy, stream=None, device=None):
+    """Device-tensor entry of the cutoff kernel's direct sum
+    (pf_velocity_direct_cutoff): v = 1/(2 pi) sum g (-dy, dx)/(r^2 + sigmasqr)."""
+    require(x.numel(), x.device, x=x, y=y, g=g)
+    require(xt.numel(), x.device, xt=xt, yt=yt, vx=vx, vy=vy)
+    if device is not None and device != x.device.index:
+        raise ValueError(f"pfblob: device {device} given for tensors on {x.device}")
+    st = ctypes.c_void_p(torch.cuda.current_stream(x.device).cuda_stream if stream is None
+                         else stream)
+    _lib.check(_lib.lib.pf_velocity_direct_cutoff(_lib.context(x.device.index), x.numel(), ptr(x),
+                                                  ptr(y), ptr(g), xt.numel(), ptr(xt), ptr(yt),
+                                                  float(sigmasqr), ptr(vx), ptr(vy), st))
+
+
 def vorticity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None, hardware=0,
               blocksize=128, method=1):
-    """Induced vorticity of Gaussian vortex blobs at (xEval, yEval) (the blobs
-    if None), by direct summation on the GPU.
+    """Induced vorticity of vortex blobs at (xEval, yEval) (the blobs if
+    None), by direct summation on the GPU: Gaussian kernel (``kernel=1``) or,
+    as the reference computes it, the cutoff kernel (``kernel=0``).
 
     Same arguments and return value as pHyFlow's ``vorticity``
     (``src/python/blobs/base/induced/_induced.py:702-789``); like the
     reference, the FMM method is not available for the vorticity."""
-    if kernel != GAUSS_KERNEL:
-        raise NotImplementedError("pfblob: only the Gaussian kernel (kernel=1) is provided")
+    if kernel not in (GAUSS_KERNEL, CUTOFF_KERNEL):
+        raise ValueError(f"pfblob: unknown kernel {kernel}")
     if method != DIRECT_METHOD:
         raise Exception('FMM method not implemented yet')
     m = Marshal(xBlob.device.index if isinstance(xBlob, torch.Tensor) and xBlob.is_cuda else None)
@@ -140,7 +165,13 @@ def vorticity(xBlob, yBlob, wBlob, sigma, k=2, kernel=1, xEval=None, yEval=None,
     require(xt.numel(), m.device, xEval=xt, yEval=yt)
     w = m.empty(xt.numel())
     ctx = _lib.context(m.index)
-    _lib.check(_lib.lib.pf_vorticity_direct(ctx, x.numel(), ptr(x), ptr(y), ptr(g), xt.numel(),
-                                            ptr(xt), ptr(yt), float(k) * sigma * sigma, ptr(w),
-                                            m.stream))
+    if kernel == CUTOFF_KERNEL:
+        _lib.check(_lib.lib.pf_vorticity_direct_cutoff(ctx, x.numel(), ptr(x), ptr(y), ptr(g),
+                                                       xt.numel(), ptr(xt), ptr(yt),
+                                                       float(sigma) * float(sigma), ptr(w),
+                                                       m.stream))
+    else:
+        _lib.check(_lib.lib.pf_vorticity_direct(ctx, x.numel(), ptr(x), ptr(y), ptr(g),
+                                                xt.numel(), ptr(xt), ptr(yt),
+                                                float(k) * sigma * sigma, ptr(w), m.stream))
     return m.outs(w)[0]

@@ -138,7 +138,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=os.environ.get(
         "PHYFLOW_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference")))
-    ap.add_argument("--only", choices=["popctl", "tutty", "vorticity", "influence", "regrid"],
+    ap.add_argument("--only", choices=["popctl", "tutty", "vorticity", "influence", "regrid",
+                                       "cutoff"],
                     default=None,
                     help="write only this group of fixtures")
     args = ap.parse_args()
@@ -153,6 +154,9 @@ def main():
         return
     if args.only == "influence":
         influence_fixtures()
+        return
+    if args.only == "cutoff":
+        cutoff_fixtures()
         return
     if args.only == "regrid":  # M4' sweep, Regrid and Tutty fixtures
         regrid_fixtures(args.ref)
@@ -206,6 +210,7 @@ def main():
     tutty_fixtures(args.ref)
     vorticity_fixtures()
     influence_fixtures()
+    cutoff_fixtures()
     print("golden fixtures written to", HERE)
 
 
@@ -290,6 +295,32 @@ def vorticity_fixtures():
     w = ref.vorticity_gauss(x, y, g, k2, xt, yt)
     np.savez_compressed(os.path.join(HERE, "vort_rand.npz"), x=x, y=y, g=g, sigma=sigma,
                         ksigmasqr=k2, xt=xt, yt=yt, w=w)
+
+
+def cutoff_fixtures():
+    """9. the reference's cutoff-kernel loops (vv2par_C_cpu.c, ww2par_C_cpu.c,
+    extracted into oracle/_ref/): the C1 lattice at the blobs with sigmasqr =
+    sigma^2, and random blobs (a duplicated blob, a zero one, a far one) at
+    separate points, a few of them on blobs."""
+    assert ref.cutoff_available(), "build oracle/_ref first: make -C oracle ref"
+    c1 = wl.lamb_oseen_lattice()
+    s2 = c1.sigma * c1.sigma
+    vx, vy = ref.velocity_cutoff(c1.x, c1.y, c1.g, s2)
+    w = ref.vorticity_cutoff(c1.x, c1.y, c1.g, s2)
+    np.savez_compressed(os.path.join(HERE, "cutoff_c1.npz"), x=c1.x, y=c1.y, g=c1.g,
+                        sigma=c1.sigma, sigmasqr=s2, vx=vx, vy=vy, w=w)
+    x, y, g, sigma = rand_blobs(3000, 0.01, 41)
+    x[10], y[10] = x[11], y[11]
+    g[20] = 0.0
+    x[30], y[30] = 25.0, -13.0
+    rng = np.random.Generator(np.random.PCG64(43))
+    xt, yt = rng.uniform(-0.1, 1.1, 1500), rng.uniform(-0.1, 1.1, 1500)
+    xt[:5], yt[:5] = x[:5], y[:5]
+    s2 = sigma * sigma
+    vx, vy = ref.velocity_cutoff(x, y, g, s2, xt, yt)
+    w = ref.vorticity_cutoff(x, y, g, s2, xt, yt)
+    np.savez_compressed(os.path.join(HERE, "cutoff_rand.npz"), x=x, y=y, g=g, sigma=sigma,
+                        sigmasqr=s2, xt=xt, yt=yt, vx=vx, vy=vy, w=w)
 
 
 def tutty_fixtures(refroot):

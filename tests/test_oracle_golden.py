@@ -125,3 +125,20 @@ def test_vorticity_matches_reference_loop(golden):
     d = golden("vort_rand")
     w = oracle.vorticity_direct(d["x"], d["y"], d["g"], float(d["ksigmasqr"]), d["xt"], d["yt"])
     assert np.array_equal(w, d["w"])
+
+
+def test_cutoff_kernels_match_reference_loops(golden):
+    """The cutoff-kernel restatements are bit-exact against the reference's
+    own vv2par_C_cpu / ww2par_C_cpu loops (golden, at the blobs and at
+    separate points with a duplicated, a zero and a far blob)."""
+    d = golden("cutoff_c1")
+    s2 = float(d["sigmasqr"])
+    vx, vy = oracle.velocity_direct_cutoff(d["x"], d["y"], d["g"], s2)
+    assert np.array_equal(vx, d["vx"]) and np.array_equal(vy, d["vy"])
+    assert np.array_equal(oracle.vorticity_direct_cutoff(d["x"], d["y"], d["g"], s2), d["w"])
+    d = golden("cutoff_rand")
+    s2 = float(d["sigmasqr"])
+    vx, vy = oracle.velocity_direct_cutoff(d["x"], d["y"], d["g"], s2, d["xt"], d["yt"])
+    assert np.array_equal(vx, d["vx"]) and np.array_equal(vy, d["vy"])
+    w = oracle.vorticity_direct_cutoff(d["x"], d["y"], d["g"], s2, d["xt"], d["yt"])
+    assert np.array_equal(w, d["w"])

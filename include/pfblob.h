@@ -249,6 +249,18 @@ pf_status pf_panel_velocity(pf_ctx *ctx, int64_t m, const double *gamma, const d
                             const double *xv, const double *yv, double *vx, double *vy,
                             int accumulate, void *stream);
 
+/* Constant-strength source panels (strengths sigma), otherwise as
+ * pf_panel_velocity: in the panel frame vxP = s/(4 pi) log(r1^2/r2^2),
+ * vyP = s/(2 pi) (atan2(yP, xP-x2) - atan2(yP, xP)).  Replaces
+ * _sourcePanel_Cython_cpu.inducedVelocity (src/cpp/panels/cython/
+ * sourcePanel_Cython/_sourcePanel_Cython_cpu.pyx:244-393, formula :368-390), reached from
+ * panelSolver.inducedVelocity with panelKernel = 0 (panelSolver.py:252-253). */
+pf_status pf_source_panel_velocity(pf_ctx *ctx, int64_t m, const double *sigma, const double *xs,
+                                   const double *ys, const double *xe, const double *ye,
+                                   const double *cosa, const double *sina, int64_t n,
+                                   const double *xv, const double *yv, double *vx, double *vy,
+                                   int accumulate, void *stream);
+
 /* Influence matrix of M vortex panels on their collocation points, FP64:
  * A[i*M + j] = (velocity at (xcp_i, ycp_i) of panel j at unit strength) .
  * (cos_i, sin_i), row-major, device array of M*M.  Replaces
@@ -260,6 +272,16 @@ pf_status pf_panel_influence_matrix(pf_ctx *ctx, int64_t m, const double *xcp, c
                                     const double *xs, const double *ys, const double *xe,
                                     const double *ye, const double *cosa, const double *sina,
                                     double *A, void *stream);
+
+/* Influence matrix of source panels: the velocity of panel j at unit
+ * strength at collocation point i projected on the normal (-sin_i, cos_i).
+ * Replaces _sourcePanel_Cython_cpu.assemble_influenceMatrix (src/cpp/panels/
+ * cython/sourcePanel_Cython/_sourcePanel_Cython_cpu.pyx:82-237, formula :209-234), reached from
+ * panelSolver.influenceMatrix with panelKernel = 0 (panelSolver.py:133-134). */
+pf_status pf_source_panel_influence_matrix(pf_ctx *ctx, int64_t m, const double *xcp,
+                                           const double *ycp, const double *xs, const double *ys,
+                                           const double *xe, const double *ye, const double *cosa,
+                                           const double *sina, double *A, void *stream);
 
 /* Dense LU factorisation with partial pivoting of the row-major m x m FP64
  * device matrix `a`, in place: P a = L U, L unit lower; ipiv[k] (device

@@ -23,10 +23,11 @@ Contents
     panels, the C++ CPU FMM).  These pin the restatement.
 """
 from .core import (velocity_direct, vorticity_direct, velocity_direct_cutoff,
-                   vorticity_direct_cutoff, panel_velocity, m4prime, remesh_left_index, moments,
-                   oracle_lib)
+                   vorticity_direct_cutoff, panel_velocity, source_panel_velocity, m4prime,
+                   remesh_left_index, moments, oracle_lib)
 from .regrid import diffusion_tutty, population_control, regrid
 
 __all__ = ["velocity_direct", "vorticity_direct", "velocity_direct_cutoff",
-           "vorticity_direct_cutoff", "panel_velocity", "m4prime", "remesh_left_index",
+           "vorticity_direct_cutoff", "panel_velocity", "source_panel_velocity", "m4prime",
+           "remesh_left_index",
            "moments", "regrid", "population_control", "diffusion_tutty", "oracle_lib"]

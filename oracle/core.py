@@ -38,12 +38,13 @@ def oracle_lib():
         lib.or_vorticity_direct_cutoff.argtypes = [i64, _dp, _dp, _dp, i64, _dp, _dp, dbl, _dp,
                                                    cint]
         lib.or_panel_velocity.argtypes = [i64, _dp, _dp, _dp, _dp, _dp, _dp, _dp, i64, _dp, _dp, _dp, _dp, cint]
+        lib.or_source_panel_velocity.argtypes = lib.or_panel_velocity.argtypes
         lib.or_m4prime.argtypes = [i64, _dp, dbl, _dp]
         lib.or_remesh_left_index.argtypes = [i64, _dp, dbl, dbl, _ip]
         lib.or_moments.argtypes = [i64, _dp, _dp, _dp, _dp]
         for f in (lib.or_velocity_direct_gauss, lib.or_vorticity_direct_gauss,
                   lib.or_velocity_direct_cutoff, lib.or_vorticity_direct_cutoff,
-                  lib.or_panel_velocity, lib.or_m4prime,
+                  lib.or_panel_velocity, lib.or_source_panel_velocity, lib.or_m4prime,
                   lib.or_remesh_left_index, lib.or_moments):
             f.restype = None
         _LIB = lib
@@ -107,6 +108,17 @@ def vorticity_direct_cutoff(xs, ys, gs, sigmasqr, xt=None, yt=None, nthreads=0):
     oracle_lib().or_vorticity_direct_cutoff(xs.shape[0], _p(xs), _p(ys), _p(gs), xt.shape[0],
                                             _p(xt), _p(yt), float(sigmasqr), _p(w), int(nthreads))
     return w
+
+
+def source_panel_velocity(sigma, xs, ys, xe, ye, cosa, sina, xv, yv, nthreads=0):
+    """FP64 source-panel velocity; restates ``_sourcePanel_Cython_cpu.inducedVelocity``."""
+    arrs = [_f64(a) for a in (sigma, xs, ys, xe, ye, cosa, sina)]
+    xv, yv = _f64(xv), _f64(yv)
+    vx = np.empty(xv.shape[0])
+    vy = np.empty(xv.shape[0])
+    oracle_lib().or_source_panel_velocity(arrs[0].shape[0], *[_p(a) for a in arrs], xv.shape[0],
+                                          _p(xv), _p(yv), _p(vx), _p(vy), int(nthreads))
+    return vx, vy
 
 
 def panel_velocity(gamma, xs, ys, xe, ye, cosa, sina, xv, yv, nthreads=0):

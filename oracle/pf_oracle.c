@@ -171,6 +171,43 @@ void or_panel_velocity(int64_t m, const double *gamma, const double *xs,
     }
 }
 
+/* Constant-strength source panels, induced velocity at points.  Follows
+ * src/cpp/panels/cython/sourcePanel_Cython/_sourcePanel_Cython_cpu.pyx
+ * :368-390: in the panel frame
+ *   vxP = s/(4pi) log((xP^2+yP^2)/((xP-x2)^2+yP^2))
+ *   vyP = s/(2pi) (atan2(yP, xP-x2) - atan2(yP, xP))
+ * and rotate back. */
+void or_source_panel_velocity(int64_t m, const double *sigma, const double *xs,
+                              const double *ys, const double *xe, const double *ye,
+                              const double *cosa, const double *sina, int64_t n,
+                              const double *xv, const double *yv, double *vx,
+                              double *vy, int nthreads)
+{
+    const double inv_2pi = 1.0 / (2.0 * OR_PI);
+    const double inv_4pi = inv_2pi / 2.0;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t i = 0; i < n; ++i) {
+        double ax = 0.0, ay = 0.0;
+        for (int64_t j = 0; j < m; ++j) {
+            const double Lx = xe[j] - xs[j];
+            const double Ly = ye[j] - ys[j];
+            const double x2 = cosa[j] * Lx + sina[j] * Ly;
+            const double xP = cosa[j] * (xv[i] - xs[j]) + sina[j] * (yv[i] - ys[j]);
+            const double yP = -sina[j] * (xv[i] - xs[j]) + cosa[j] * (yv[i] - ys[j]);
+            const double vxP = (sigma[j] * inv_4pi) *
+                               log((xP * xP + yP * yP) / ((xP - x2) * (xP - x2) + yP * yP));
+            const double vyP = (sigma[j] * inv_2pi) * (atan2(yP, (xP - x2)) - atan2(yP, xP));
+            ax += cosa[j] * vxP - sina[j] * vyP;
+            ay += sina[j] * vxP + cosa[j] * vyP;
+        }
+        vx[i] = ax;
+        vy[i] = ay;
+    }
+}
+
 /* One-dimensional M4' interpolation weights with the Wee diffusion term c^2.
  * Follows src/cpp/blobs/c++/interpolation_kernels_1d/
  * _interpolation_kernels_1d.cpp:75-89, including its branch structure: the

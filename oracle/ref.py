@@ -119,6 +119,23 @@ def panel_influence(xcp, ycp, xs, ys, xe, ye, cosa, sina):
     return np.array(_module("_vortexPanel_Cython_cpu").assemble_influenceMatrix(*f))
 
 
+def source_panel_available():
+    return os.path.exists(os.path.join(REF_DIR, "_sourcePanel_Cython_cpu" + _SUF))
+
+
+def source_panel_velocity(sigma, xs, ys, xe, ye, cosa, sina, xv, yv):
+    """Reference Cython source-panel induced velocity -> (vx, vy)."""
+    f = [np.ascontiguousarray(a, dtype=np.float64) for a in (sigma, xv, yv, xs, ys, xe, ye, cosa, sina)]
+    vx, vy = _module("_sourcePanel_Cython_cpu").inducedVelocity(*f)
+    return np.array(vx), np.array(vy)
+
+
+def source_panel_influence(xcp, ycp, xs, ys, xe, ye, cosa, sina):
+    """Reference Cython source-panel assemble_influenceMatrix -> A (M, M)."""
+    f = [np.ascontiguousarray(a, dtype=np.float64) for a in (xcp, ycp, xs, ys, xe, ye, cosa, sina)]
+    return np.array(_module("_sourcePanel_Cython_cpu").assemble_influenceMatrix(*f))
+
+
 def m4_available():
     return os.path.exists(os.path.join(REF_DIR, "libref_m4.so"))
 

@@ -33,6 +33,14 @@
 //           (no cancellation far away), else log of the ratio itself (no
 //           cancellation in 1+u next to the panel's start point)
 // Geometry and accumulation in FP64, the two transcendentals in FP32.
+//
+// Constant-source panels (SOURCE, the reference's 'css' kernel,
+// _sourcePanel_Cython_cpu.pyx:209-234 and :368-390): in the panel
+// frame vxP = s/(4pi) log(r1^2/r2^2), vyP = s/(2pi) theta, i.e. the same two
+// quantities with their roles exchanged; in complex form
+// w = -(s/2pi) e^{-i alpha} log((z - z2)/(z - z1)), so the groups' series is
+// the same with K_j = -s_j e^{-i alpha_j}/(2pi).  The source influence matrix
+// projects on the normal (-sin alpha_i, cos alpha_i) instead of the tangent.
 #include <algorithm>
 #include <cmath>
 
@@ -63,6 +71,7 @@ struct PanelGroup {
 };
 static_assert(sizeof(PanelGroup) % 16 == 0, "PanelGroup layout");
 
+template <bool SOURCE>
 __device__ __forceinline__ void pair_velocity(const PanelSm &q, double px, double py, double &ax,
                                               double &ay) {
     const double dx = px - q.xs, dy = py - q.ys;
@@ -79,14 +88,15 @@ __device__ __forceinline__ void pair_velocity(const PanelSm &q, double px, doubl
     const float a2f = (float)a2;
     const float u = (float)num_l / a2f;
     const float lg = (fabsf(u) < 0.5f) ? log1pf(u) : logf((float)(xp * xp + yp * yp) / a2f);
-    const double vxp = (q.gam * INV_2PI) * (double)theta;
-    const double vyp = -(q.gam * INV_4PI) * (double)lg;
+    const double vxp = SOURCE ? (q.gam * INV_4PI) * (double)lg : (q.gam * INV_2PI) * (double)theta;
+    const double vyp = SOURCE ? (q.gam * INV_2PI) * (double)theta : -(q.gam * INV_4PI) * (double)lg;
     ax += q.c * vxp - q.s * vyp;
     ay += q.s * vxp + q.c * vyp;
 }
 
 // One warp per group: the panels' frame records, the enclosing circle and the
 // series coefficients (lane k forms A_{k+1}).
+template <bool SOURCE>
 __global__ void __launch_bounds__(32)
 k_panel_groups(int64_t m, const double *__restrict__ gamma, const double *__restrict__ xs,
                const double *__restrict__ ys, const double *__restrict__ xe,
@@ -114,8 +124,9 @@ k_panel_groups(int64_t m, const double *__restrict__ gamma, const double *__rest
         y1 = q.ys;
         x2e = q.xs + q.x2 * q.c;
         y2e = q.ys + q.x2 * q.s;
-        kr = -(q.gam * INV_2PI) * q.s;
-        ki = -(q.gam * INV_2PI) * q.c;
+        // vortex: K = -i g e^{-i alpha}/(2 pi); source: K = -s e^{-i alpha}/(2 pi)
+        kr = SOURCE ? -(q.gam * INV_2PI) * q.c : -(q.gam * INV_2PI) * q.s;
+        ki = SOURCE ? (q.gam * INV_2PI) * q.s : -(q.gam * INV_2PI) * q.c;
         bx0 = fmin(x1, x2e);
         bx1 = fmax(x1, x2e);
         by0 = fmin(y1, y2e);
@@ -173,6 +184,7 @@ k_panel_groups(int64_t m, const double *__restrict__ gamma, const double *__rest
 // Velocity at the points: one point per thread, the groups (series and
 // panels) staged through shared memory PC_TILE at a time; a persistent grid
 // keeps one staging when all groups fit one tile.
+template <bool SOURCE>
 __global__ void __launch_bounds__(PN_THREADS)
 k_panel_velocity(int64_t ngroups, const PanelGroup *__restrict__ groups,
                  const PanelSm *__restrict__ pan, int64_t m, int64_t n,
@@ -215,7 +227,8 @@ k_panel_velocity(int64_t ngroups, const PanelGroup *__restrict__ groups,
                 const double r2 = dx * dx + dy * dy;
                 if (r2 < s_g[c].far_r2) {
                     const int j1 = (int)min((int64_t)PC_G, m - (g0 + c) * PC_G);
-                    for (int j = 0; j < j1; ++j) pair_velocity(s_p[c * PC_G + j], px, py, ax, ay);
+                    for (int j = 0; j < j1; ++j)
+                        pair_velocity<SOURCE>(s_p[c * PC_G + j], px, py, ax, ay);
                 } else {
                     const double R = s_g[c].R;
                     const double q = R / r2;
@@ -253,7 +266,10 @@ k_panel_velocity(int64_t ngroups, const PanelGroup *__restrict__ groups,
 // (_vortexPanel_Cython_cpu.pyx:217-234, all in FP64 as there): A[i][j] =
 // velocity induced at collocation point i by panel j at unit strength,
 // projected on the tangent (cos_i, sin_i) of panel i.  One thread per (i, j),
-// j fastest (coalesced rows).
+// j fastest (coalesced rows).  SOURCE: source panels
+// (_sourcePanel_Cython_cpu.pyx:209-234), projected on the normal
+// (-sin_i, cos_i).
+template <bool SOURCE>
 __global__ void __launch_bounds__(PN_THREADS)
 k_panel_influence(int64_t m, const double *__restrict__ xcp, const double *__restrict__ ycp,
                   const double *__restrict__ xs, const double *__restrict__ ys,
@@ -269,49 +285,50 @@ k_panel_influence(int64_t m, const double *__restrict__ xcp, const double *__res
     const double dx = xcp[i] - xs[j], dy = ycp[i] - ys[j];
     const double xp = cj * dx + sj * dy;
     const double yp = -sj * dx + cj * dy;
-    const double vxp = INV_2PI * (atan2(yp, xp - x2) - atan2(yp, xp));
-    const double vyp = -INV_4PI * log((xp * xp + yp * yp) / ((xp - x2) * (xp - x2) + yp * yp));
+    const double th = atan2(yp, xp - x2) - atan2(yp, xp);
+    const double lg = log((xp * xp + yp * yp) / ((xp - x2) * (xp - x2) + yp * yp));
+    const double vxp = SOURCE ? INV_4PI * lg : INV_2PI * th;
+    const double vyp = SOURCE ? INV_2PI * th : -INV_4PI * lg;
     const double vx = cj * vxp - sj * vyp;
     const double vy = sj * vxp + cj * vyp;
-    A[e] = vx * cosa[i] + vy * sina[i];
+    A[e] = SOURCE ? vx * -sina[i] + vy * cosa[i] : vx * cosa[i] + vy * sina[i];
 }
 
 }  // namespace
 
-extern "C" pf_status pf_panel_influence_matrix(pf_ctx *ctx, int64_t m, const double *xcp,
-                                               const double *ycp, const double *xs,
-                                               const double *ys, const double *xe,
-                                               const double *ye, const double *cosa,
-                                               const double *sina, double *A, void *stream) {
-    PF_RANGE("pf_panel_influence_matrix");
-    pf::clear_error();
-    PF_CHECK_ARG(ctx != nullptr, "pf_panel_influence_matrix: NULL context");
-    PF_CHECK_ARG(m >= 0 && m <= 32768, "pf_panel_influence_matrix: m = %lld outside [0, 32768]",
-                 (long long)m);
+static pf_status influence_matrix(pf_ctx *ctx, const char *name, int64_t m, const double *xcp,
+                                  const double *ycp, const double *xs, const double *ys,
+                                  const double *xe, const double *ye, const double *cosa,
+                                  const double *sina, double *A, void *stream, bool source) {
+    PF_CHECK_ARG(ctx != nullptr, "%s: NULL context", name);
+    PF_CHECK_ARG(m >= 0 && m <= 32768, "%s: m = %lld outside [0, 32768]", name, (long long)m);
     PF_CHECK_ARG(m == 0 || (xcp && ycp && xs && ys && xe && ye && cosa && sina && A),
-                 "pf_panel_influence_matrix: NULL array");
+                 "%s: NULL array", name);
     pf::DeviceGuard dg(ctx->device);
     if (m == 0) return PF_OK;
-    k_panel_influence<<<(unsigned)pf::ceil_div(m * m, PN_THREADS), PN_THREADS, 0,
-                        static_cast<cudaStream_t>(stream)>>>(m, xcp, ycp, xs, ys, xe, ye, cosa,
+    const unsigned grid = (unsigned)pf::ceil_div(m * m, PN_THREADS);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (source)
+        k_panel_influence<true><<<grid, PN_THREADS, 0, st>>>(m, xcp, ycp, xs, ys, xe, ye, cosa,
                                                              sina, A);
+    else
+        k_panel_influence<false><<<grid, PN_THREADS, 0, st>>>(m, xcp, ycp, xs, ys, xe, ye, cosa,
+                                                              sina, A);
     return pf::launch_status("k_panel_influence");
 }
 
-extern "C" pf_status pf_panel_velocity(pf_ctx *ctx, int64_t m, const double *gamma,
-                                       const double *xs, const double *ys, const double *xe,
-                                       const double *ye, const double *cosa, const double *sina,
-                                       int64_t n, const double *xv, const double *yv, double *vx,
-                                       double *vy, int accumulate, void *stream) {
-    PF_RANGE("pf_panel_velocity");
-    pf::clear_error();
-    PF_CHECK_ARG(ctx != nullptr, "pf_panel_velocity: NULL context");
-    PF_CHECK_ARG(m >= 0 && m <= 65536, "pf_panel_velocity: panel count %lld outside [0, 65536]",
+static pf_status panel_velocity(pf_ctx *ctx, const char *name, int64_t m, const double *gamma,
+                                const double *xs, const double *ys, const double *xe,
+                                const double *ye, const double *cosa, const double *sina,
+                                int64_t n, const double *xv, const double *yv, double *vx,
+                                double *vy, int accumulate, void *stream, bool source) {
+    PF_CHECK_ARG(ctx != nullptr, "%s: NULL context", name);
+    PF_CHECK_ARG(m >= 0 && m <= 65536, "%s: panel count %lld outside [0, 65536]", name,
                  (long long)m);
-    PF_CHECK_ARG(n >= 0, "pf_panel_velocity: negative target count");
+    PF_CHECK_ARG(n >= 0, "%s: negative target count", name);
     PF_CHECK_ARG(m == 0 || (gamma && xs && ys && xe && ye && cosa && sina),
-                 "pf_panel_velocity: NULL panel array");
-    PF_CHECK_ARG(n == 0 || (xv && yv && vx && vy), "pf_panel_velocity: NULL point array");
+                 "%s: NULL panel array", name);
+    PF_CHECK_ARG(n == 0 || (xv && yv && vx && vy), "%s: NULL point array", name);
     pf::DeviceGuard dg(ctx->device);
     if (n == 0) return PF_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -329,17 +346,71 @@ extern "C" pf_status pf_panel_velocity(pf_ctx *ctx, int64_t m, const double *gam
     auto *groups = static_cast<PanelGroup *>(pf::arena_take(ctx, gbytes));
     auto *pan = static_cast<PanelSm *>(pf::arena_take(ctx, pbytes));
     if (!groups || !pan) {
-        pf::set_error("pf_panel_velocity: scratch too small");
+        pf::set_error("%s: scratch too small", name);
         return PF_ERR_OOM;
     }
-    k_panel_groups<<<(unsigned)ngroups, 32, 0, st>>>(m, gamma, xs, ys, xe, ye, cosa, sina, groups,
-                                                     pan);
+    if (source)
+        k_panel_groups<true><<<(unsigned)ngroups, 32, 0, st>>>(m, gamma, xs, ys, xe, ye, cosa,
+                                                               sina, groups, pan);
+    else
+        k_panel_groups<false><<<(unsigned)ngroups, 32, 0, st>>>(m, gamma, xs, ys, xe, ye, cosa,
+                                                                sina, groups, pan);
     PF_TRY(pf::launch_status("k_panel_groups"));
     // persistent grid: a few CTAs per SM, each over many blocks of points
     const int64_t grid = std::min<int64_t>(pf::ceil_div(n, PN_THREADS), (int64_t)ctx->num_sms * 4);
     // P = ceil(log2(PC_EPS (1 - PC_RHO) / 2) / log2(rho)) terms for rho <= PC_RHO
     const float log2_tol = (float)std::log2(PC_EPS * (1.0 - PC_RHO) / 2.0);
-    k_panel_velocity<<<(unsigned)grid, PN_THREADS, 0, st>>>(ngroups, groups, pan, m, n, xv, yv, vx,
-                                                           vy, accumulate, log2_tol);
+    if (source)
+        k_panel_velocity<true><<<(unsigned)grid, PN_THREADS, 0, st>>>(
+            ngroups, groups, pan, m, n, xv, yv, vx, vy, accumulate, log2_tol);
+    else
+        k_panel_velocity<false><<<(unsigned)grid, PN_THREADS, 0, st>>>(
+            ngroups, groups, pan, m, n, xv, yv, vx, vy, accumulate, log2_tol);
     return pf::launch_status("k_panel_velocity");
+}
+
+extern "C" pf_status pf_panel_influence_matrix(pf_ctx *ctx, int64_t m, const double *xcp,
+                                               const double *ycp, const double *xs,
+                                               const double *ys, const double *xe,
+                                               const double *ye, const double *cosa,
+                                               const double *sina, double *A, void *stream) {
+    PF_RANGE("pf_panel_influence_matrix");
+    pf::clear_error();
+    return influence_matrix(ctx, "pf_panel_influence_matrix", m, xcp, ycp, xs, ys, xe, ye, cosa,
+                            sina, A, stream, false);
+}
+
+extern "C" pf_status pf_source_panel_influence_matrix(pf_ctx *ctx, int64_t m, const double *xcp,
+                                                      const double *ycp, const double *xs,
+                                                      const double *ys, const double *xe,
+                                                      const double *ye, const double *cosa,
+                                                      const double *sina, double *A,
+                                                      void *stream) {
+    PF_RANGE("pf_source_panel_influence_matrix");
+    pf::clear_error();
+    return influence_matrix(ctx, "pf_source_panel_influence_matrix", m, xcp, ycp, xs, ys, xe, ye,
+                            cosa, sina, A, stream, true);
+}
+
+extern "C" pf_status pf_panel_velocity(pf_ctx *ctx, int64_t m, const double *gamma,
+                                       const double *xs, const double *ys, const double *xe,
+                                       const double *ye, const double *cosa, const double *sina,
+                                       int64_t n, const double *xv, const double *yv, double *vx,
+                                       double *vy, int accumulate, void *stream) {
+    PF_RANGE("pf_panel_velocity");
+    pf::clear_error();
+    return panel_velocity(ctx, "pf_panel_velocity", m, gamma, xs, ys, xe, ye, cosa, sina, n, xv,
+                          yv, vx, vy, accumulate, stream, false);
+}
+
+extern "C" pf_status pf_source_panel_velocity(pf_ctx *ctx, int64_t m, const double *sigma,
+                                              const double *xs, const double *ys,
+                                              const double *xe, const double *ye,
+                                              const double *cosa, const double *sina, int64_t n,
+                                              const double *xv, const double *yv, double *vx,
+                                              double *vy, int accumulate, void *stream) {
+    PF_RANGE("pf_source_panel_velocity");
+    pf::clear_error();
+    return panel_velocity(ctx, "pf_source_panel_velocity", m, sigma, xs, ys, xe, ye, cosa, sina,
+                          n, xv, yv, vx, vy, accumulate, stream, true);
 }

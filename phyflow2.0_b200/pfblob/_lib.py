@@ -52,12 +52,15 @@ PROTOTYPES = {
                             _int, _c.POINTER(_dbl), _vp, _vp, _vp],
     "pf_panel_velocity": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp,
                           _int, _vp],
+    "pf_source_panel_velocity": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp,
+                          _int, _vp],
     "pf_remesh": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp, _vp, _vp,
                   _c.POINTER(_i64), _vp],
     "pf_remesh_tutty": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp,
                         _vp, _vp, _c.POINTER(_i64), _vp],
     "pf_moments": [_vp, _i64, _vp, _vp, _vp, _vp, _vp],
     "pf_panel_influence_matrix": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "pf_source_panel_influence_matrix": [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "pf_dense_lu_factor": [_vp, _i64, _vp, _vp, _vp, _vp],
     "pf_dense_lu_solve": [_vp, _i64, _vp, _vp, _vp, _vp],
     "pf_population_control": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _vp, _vp, _vp, _vp, _vp, _vp],

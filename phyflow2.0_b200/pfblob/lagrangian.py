@@ -7,10 +7,14 @@ body geometry (rotation by thetaLocal about cmGlobal, panel ends, normals,
 tangents, collocation points moved inside by a tenth of the panel length,
 :964-1058), the influence matrix (:872-962, ``pf_panel_influence_matrix``),
 ``solve`` (:715-823; 'fixed' by LU, 'prescribed' by the least-squares system
-of the influence matrix plus one total-circulation row per body) and
-``evaluateVelocity`` (:641-712, ``pf_panel_velocity``).  Only constant-
-strength vortex panels ('csv') and fixed bodies exist here; the iterative
-'moving' solvers and body motion are not part of this library.
+of the influence matrix plus one total-circulation row per body, 'moving' by
+the direct solve of the re-assembled matrix), ``updateBody`` (:530-637: new
+cmGlobal and thetaLocal, coordinates and influence matrix rebuilt) and
+``evaluateVelocity`` (:641-712, ``pf_panel_velocity``), for constant-
+strength vortex ('csv') or source ('css') panels.  For a moving body the reference
+solves with scipy's 'gmres' or 'bicgstab' to its 'tol', or 'direct'
+(``numpy.linalg.solve``); every method here is the direct solve by LU on the
+GPU, the solution the iterations approach.
 
 ``LagrangianSolver`` mirrors ``pHyFlow.lagrangian.LagrangianSolver``
 (``src/python/lagrangian/__lagrangianSolverClass.py``): ``evaluateVelocity``
@@ -28,7 +32,7 @@ import torch
 from . import _lib
 from ._arrays import ptr
 from .induced import DIRECT_METHOD, FMM_METHOD, fmm_parameters, velocity_device
-from .panels import panel_velocity_device
+from .panels import PANEL_KERNEL_CSS, PANEL_KERNEL_CSV, panel_velocity_device
 
 PANEL_KERNELS = ('csv', 'css')
 PROBLEM_TYPES = ('fixed', 'moving', 'prescribed')
@@ -68,12 +72,12 @@ class Panels:
                             "'thetaLocal', 'dPanel'] in a dictionary format.")
         if panelKernel not in PANEL_KERNELS:
             raise ValueError("panelKernel must be one of %s" % str(PANEL_KERNELS))
-        if panelKernel != 'csv':
-            raise NotImplementedError("pfblob: only constant-strength vortex panels ('csv')")
         if problemType not in PROBLEM_TYPES:
             raise ValueError("problemType must be one of %s" % str(PROBLEM_TYPES))
-        if problemType == 'moving':
-            raise NotImplementedError("pfblob: moving bodies (iterative solvers) are not provided")
+        if problemType == 'moving' and solverCompParams.get('method') not in (
+                'gmres', 'bicgstab', 'direct'):
+            raise ValueError("solverCompParams['method'] must be one of "
+                             "('gmres', 'bicgstab', 'direct') for a moving problem")
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None
                                    else device)
         self._panelKernel = panelKernel
@@ -133,7 +137,8 @@ class Panels:
         T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
         self._d = {k: T(v) for k, v in (("xs", start[0]), ("ys", start[1]), ("xe", end[0]),
                                         ("ye", end[1]), ("cosa", cs[0]), ("sina", cs[1]),
-                                        ("tx", tang[0]), ("ty", tang[1]), ("xcp", cp[0]),
+                                        ("tx", tang[0]), ("ty", tang[1]), ("nx", norm[0]),
+                                        ("ny", norm[1]), ("xcp", cp[0]),
                                         ("ycp", cp[1]))}
 
     def _assemble(self):
@@ -144,12 +149,13 @@ class Panels:
         M = int(self._nPanelsTotal)
         A = torch.empty((M, M), dtype=torch.float64, device=self.device)
         st = torch.cuda.current_stream(self.device).cuda_stream
-        _lib.check(_lib.lib.pf_panel_influence_matrix(
-            _lib.context(self.device.index), M, *[ptr(d[k]) for k in ("xcp", "ycp", "xs", "ys",
-                                                                    "xe", "ye", "cosa", "sina")],
-            ptr(A), st))
+        fn = _lib.lib.pf_source_panel_influence_matrix if self._panelKernel == 'css' \
+            else _lib.lib.pf_panel_influence_matrix
+        _lib.check(fn(_lib.context(self.device.index), M,
+                      *[ptr(d[k]) for k in ("xcp", "ycp", "xs", "ys", "xe", "ye", "cosa", "sina")],
+                      ptr(A), st))
         self._A = A
-        if self._problemType == 'fixed':
+        if self._problemType in ('fixed', 'moving'):
             self._lu = _lu(self.device, A)
         else:
             B = torch.zeros((M + self._nBodies, M), dtype=torch.float64, device=self.device)
@@ -174,17 +180,22 @@ class Panels:
     def _velocity_device(self, xt, yt, vx, vy, accumulate):
         d = self._d
         panel_velocity_device(self._sPanel, d["xs"], d["ys"], d["xe"], d["ye"], d["cosa"],
-                              d["sina"], xt, yt, vx, vy, accumulate=accumulate)
+                              d["sina"], xt, yt, vx, vy, accumulate=accumulate,
+                              panelKernel=PANEL_KERNEL_CSS if self._panelKernel == 'css'
+                              else PANEL_KERNEL_CSV)
 
     def solve(self, vxExternel, vyExternel, gTotal=None):
         """Panel strengths for the no-slip condition at the collocation points
         under the external velocity there (RHS = -v_ext . t for vortex
-        panels, __panelsClass.py:772-775)."""
+        panels, -v_ext . n for source panels, __panelsClass.py:772-775)."""
         d = self._d
         vx = vxExternel if isinstance(vxExternel, torch.Tensor) else torch.from_numpy(np.asarray(vxExternel, dtype=np.float64)).to(self.device)
         vy = vyExternel if isinstance(vyExternel, torch.Tensor) else torch.from_numpy(np.asarray(vyExternel, dtype=np.float64)).to(self.device)
-        rhs = (-vx) * d["tx"] + (-vy) * d["ty"]
-        if self._problemType == 'fixed':
+        if self._panelKernel == 'css':
+            rhs = (-vx) * d["nx"] + (-vy) * d["ny"]
+        else:
+            rhs = (-vx) * d["tx"] + (-vy) * d["ty"]
+        if self._problemType in ('fixed', 'moving'):
             self._sPanel = _lu_solve(self.device, *self._lu, rhs)
         else:
             if gTotal is None:
@@ -192,6 +203,34 @@ class Panels:
             g = torch.as_tensor(np.asarray(gTotal, dtype=np.float64), device=self.device)
             b = torch.cat([rhs, -g])
             self._sPanel = _lu_solve(self.device, *self._lu, self._B.T @ b)
+
+    def updateBody(self, cmGlobalNew, thetaLocalNew):
+        """New position and rotation of every body (dicts keyed by geometry
+        key, all keys required, as __panelsClass.py:1304-1350 checks them):
+        the global coordinates, normals, tangents and collocation points are
+        recomputed and the influence matrix re-assembled (and re-factored)
+        on the GPU (__panelsClass.py:530-637)."""
+        keys = self.geometryKeys
+        if type(thetaLocalNew) != dict or any(k not in thetaLocalNew for k in keys):
+            raise TypeError("'thetaLocal' must either be a dictionary containing the following "
+                            "keys: %s" % str(keys))
+        if type(cmGlobalNew) != dict or any(k not in cmGlobalNew for k in keys):
+            raise TypeError("'cmGlobal' must either be a dictionary containing the following "
+                            "keys: %s" % str(keys))
+        for k in keys:
+            if type(thetaLocalNew[k]) not in (float, np.float64):
+                raise TypeError("thetaLocal['%s'] must be a float. It is a %s"
+                                % (k, type(thetaLocalNew[k])))
+            cm = np.asarray(cmGlobalNew[k], dtype=np.float64)
+            if cm.shape != (2,):
+                raise ValueError("cmGlobal['%s'] must have shape (2,). It has shape %s."
+                                 % (k, str(cm.shape)))
+        for k in keys:  # thetaLocal first, then cmGlobal, as the reference sets them
+            self._geometries[k]['thetaLocal'] = thetaLocalNew[k]
+        for k in keys:
+            self._geometries[k]['cmGlobal'] = np.asarray(cmGlobalNew[k], dtype=np.float64)
+        self._update_coordinates()
+        self._assemble()
 
     def _advanceTime(self, deltaTNew):
         """__panelsClass.py:825-870: deltaT kept, tStep + 1, t = deltaT tStep."""
@@ -213,6 +252,70 @@ class Panels:
         return self._nPanelsTotal
 
     @property
+    def geometryKeys(self):
+        return list(self._geometries.keys())
+
+    @property
+    def cmGlobal(self):
+        """Per body, as __panelsClass.py:1365-1373 (a list in body order)."""
+        return [np.asarray(gd['cmGlobal'], dtype=np.float64).copy()
+                for gd in self._geometries.values()]
+
+    @property
+    def thetaLocal(self):
+        return [gd['thetaLocal'] for gd in self._geometries.values()]
+
+    def _per_body(self, a):
+        """([a[0] of body i], [a[1] of body i]) (the reference's per-body lists)."""
+        ix = self._index
+        return ([a[0, ix[i]:ix[i + 1]].copy() for i in range(self._nBodies)],
+                [a[1, ix[i]:ix[i + 1]].copy() for i in range(self._nBodies)])
+
+    @property
+    def normCat(self):
+        return self._host["norm"].copy()
+
+    @property
+    def tangCat(self):
+        return self._host["tang"].copy()
+
+    @property
+    def xyCPGlobal(self):
+        return self._per_body(self._host["cp"])
+
+    @property
+    def xyPanelGlobal(self):
+        """Per body, closed: its start points and its first start point again."""
+        xs, ys = self._per_body(self._host["start"])
+        return [np.append(a, a[0]) for a in xs], [np.append(a, a[0]) for a in ys]
+
+    @property
+    def xyPanelLocal(self):
+        return ([np.asarray(gd['xPanel']) for gd in self._geometries.values()],
+                [np.asarray(gd['yPanel']) for gd in self._geometries.values()])
+
+    @property
+    def gTotal(self):
+        """Total circulation of each body, sum(-gamma L) (__panelsClass.py);
+        zero for source panels."""
+        if self._panelKernel == 'css':
+            return np.zeros(self._nBodies)
+        s, L, ix = self.sPanel, self._host["L"], self._index
+        return [np.sum(-s[ix[i]:ix[i + 1]] * L[ix[i]:ix[i + 1]]) for i in range(self._nBodies)]
+
+    @property
+    def velCompParams(self):
+        return dict(self._velCompParams)
+
+    @property
+    def deltaT(self):
+        return self._deltaT
+
+    @property
+    def solverCompParams(self):
+        return dict(self._solverCompParams)
+
+    @property
     def nPanels(self):
         return self._nPanels
 
@@ -226,16 +329,19 @@ class Panels:
 
     @property
     def xyPanelGlobalCat(self):
-        h = self._host
-        return np.hstack((h["start"], h["end"][:, -1:]))
+        """(2, nPanelsTotal + nBodies): each body's start points closed by its
+        first start point."""
+        xs, ys = self.xyPanelGlobal
+        return np.vstack((np.concatenate(xs), np.concatenate(ys)))
 
     @property
     def norm(self):
-        return self._host["norm"].copy()
+        """Per body, as __panelsClass.py:1400-1409; normCat is the (2, M) array."""
+        return self._per_body(self._host["norm"])
 
     @property
     def tang(self):
-        return self._host["tang"].copy()
+        return self._per_body(self._host["tang"])
 
     @property
     def t(self):

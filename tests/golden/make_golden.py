@@ -139,7 +139,7 @@ def main():
     ap.add_argument("--ref", default=os.environ.get(
         "PHYFLOW_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference")))
     ap.add_argument("--only", choices=["popctl", "tutty", "vorticity", "influence", "regrid",
-                                       "cutoff"],
+                                       "cutoff", "source"],
                     default=None,
                     help="write only this group of fixtures")
     args = ap.parse_args()
@@ -157,6 +157,9 @@ def main():
         return
     if args.only == "cutoff":
         cutoff_fixtures()
+        return
+    if args.only == "source":
+        source_panel_fixtures()
         return
     if args.only == "regrid":  # M4' sweep, Regrid and Tutty fixtures
         regrid_fixtures(args.ref)
@@ -211,6 +214,7 @@ def main():
     vorticity_fixtures()
     influence_fixtures()
     cutoff_fixtures()
+    source_panel_fixtures()
     print("golden fixtures written to", HERE)
 
 
@@ -321,6 +325,34 @@ def cutoff_fixtures():
     w = ref.vorticity_cutoff(x, y, g, s2, xt, yt)
     np.savez_compressed(os.path.join(HERE, "cutoff_rand.npz"), x=x, y=y, g=g, sigma=sigma,
                         sigmasqr=s2, xt=xt, yt=yt, vx=vx, vy=vy, w=w)
+
+
+def source_panel_fixtures():
+    """10. the reference's Cython constant-source panel kernel: velocity of
+    64 panels on a circle (seeded strengths) at points around it (a few on
+    panel 0's line extension and next to its midpoint), and the influence
+    matrix on the collocation points (moved inside by a tenth of the panel
+    length, as Panels places them)."""
+    assert ref.source_panel_available(), "build oracle/_ref first: make -C oracle ref"
+    ps = wl.cylinder_panels(64, instance=3)
+    rng = np.random.Generator(np.random.PCG64(47))
+    r = rng.uniform(1.0005, 3.0, 2000)
+    t = rng.uniform(-np.pi, np.pi, 2000)
+    xv, yv = r * np.cos(t), r * np.sin(t)
+    dx, dy = ps.xe[0] - ps.xs[0], ps.ye[0] - ps.ys[0]
+    xv[:3] = ps.xe[0] + dx * np.array([0.5, 1.0, 3.0])
+    yv[:3] = ps.ye[0] + dy * np.array([0.5, 1.0, 3.0])
+    xv[3] = 0.5 * (ps.xs[0] + ps.xe[0]) - 1e-6 * dy
+    yv[3] = 0.5 * (ps.ys[0] + ps.ye[0]) + 1e-6 * dx
+    vx, vy = ref.source_panel_velocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina,
+                                       xv, yv)
+    L = np.sqrt((ps.xe - ps.xs) ** 2 + (ps.ye - ps.ys) ** 2)
+    xcp = 0.5 * (ps.xs + ps.xe) + ps.sina * L * 0.1
+    ycp = 0.5 * (ps.ys + ps.ye) - ps.cosa * L * 0.1
+    A = ref.source_panel_influence(xcp, ycp, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina)
+    np.savez_compressed(os.path.join(HERE, "source_panel.npz"), sigma=ps.gamma, xs=ps.xs,
+                        ys=ps.ys, xe=ps.xe, ye=ps.ye, cosa=ps.cosa, sina=ps.sina, xv=xv, yv=yv,
+                        vx=vx, vy=vy, xcp=xcp, ycp=ycp, A=A)
 
 
 def tutty_fixtures(refroot):

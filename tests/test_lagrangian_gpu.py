@@ -75,3 +75,52 @@ def test_total_velocity_is_blobs_plus_panels_plus_free_stream():
     rx, ry = bx + px + 0.5, by + py - 0.25
     err = np.sqrt((vx - rx) ** 2 + (vy - ry) ** 2).max() / np.sqrt(rx ** 2 + ry ** 2).max()
     assert err <= 1e-6
+
+
+def test_moving_body_update_and_solve():
+    """A 'moving' body (__panelsClass.py:530-637, 715-823): after updateBody
+    (translation + rotation) the collocation points follow the reference's
+    geometry, the re-assembled influence matrix matches the reference Cython
+    kernel, and solve returns the direct solution of A s = -v.t (the
+    reference's 'direct' method; its 'gmres'/'bicgstab' approach the same
+    solution to their tolerance)."""
+    import pfblob
+    if not ref.available():
+        pytest.skip("reference Cython panel kernel (oracle/_ref) not built")
+    geo = cylinder(96)
+    panels = pfblob.Panels(geo, problemType='moving',
+                           solverCompParams={'method': 'bicgstab', 'tol': 1e-12, 'assemble': 'all'})
+    cm, th = np.array([0.3, -0.2]), 0.7
+    panels.updateBody({'cyl': cm}, {'cyl': th})
+    gd = geo["cyl"]
+    st, en, L, cs, norm, tang, cp = olag.panel_geometry(gd["xPanel"], gd["yPanel"], cm, th)
+    assert np.allclose(panels.xyCPGlobalCat, cp, rtol=0, atol=1e-15)
+    assert np.allclose(panels.normCat, norm, rtol=0, atol=1e-15)
+    assert np.allclose(panels.cmGlobal[0], cm) and panels.thetaLocal == [th]
+    A = ref.panel_influence(cp[0], cp[1], st[0], st[1], en[0], en[1], cs[0], cs[1])
+    assert np.abs(panels.A - A).max() <= 1e-12 * np.abs(A).max()
+    rng = np.random.default_rng(11)
+    vx, vy = rng.standard_normal(96), rng.standard_normal(96)
+    panels.solve(vx, vy)
+    rhs = (-vx) * tang[0] + (-vy) * tang[1]
+    s_ref = np.linalg.solve(A, rhs)
+    assert np.abs(panels.sPanel - s_ref).max() <= 1e-10 * np.abs(s_ref).max()
+    # a second move re-assembles again
+    panels.updateBody({'cyl': np.array([0.0, 0.0])}, {'cyl': 0.0})
+    geom0 = olag.panel_geometry(gd["xPanel"], gd["yPanel"], np.zeros(2), 0.0)
+    assert np.allclose(panels.xyCPGlobalCat, geom0[6], rtol=0, atol=1e-15)
+
+
+def test_update_body_checks_its_arguments():
+    import pfblob
+    panels = pfblob.Panels(cylinder(32), problemType='moving',
+                           solverCompParams={'method': 'direct', 'tol': 1e-12, 'assemble': 'all'})
+    with pytest.raises(TypeError):
+        panels.updateBody({'other': np.zeros(2)}, {'cyl': 0.1})
+    with pytest.raises(TypeError):
+        panels.updateBody({'cyl': np.zeros(2)}, {'cyl': 1})
+    with pytest.raises(ValueError):
+        panels.updateBody({'cyl': np.zeros(3)}, {'cyl': 0.1})
+    with pytest.raises(ValueError):
+        pfblob.Panels(cylinder(32), problemType='moving',
+                      solverCompParams={'method': 'lu', 'tol': 1e-12, 'assemble': 'all'})

@@ -142,3 +142,12 @@ def test_cutoff_kernels_match_reference_loops(golden):
     assert np.array_equal(vx, d["vx"]) and np.array_equal(vy, d["vy"])
     w = oracle.vorticity_direct_cutoff(d["x"], d["y"], d["g"], s2, d["xt"], d["yt"])
     assert np.array_equal(w, d["w"])
+
+
+def test_source_panel_matches_reference_cython(golden):
+    """The constant-source panel restatement is bit-exact against the
+    reference's Cython kernel (_sourcePanel_Cython_cpu.inducedVelocity)."""
+    d = golden("source_panel")
+    vx, vy = oracle.source_panel_velocity(d["sigma"], d["xs"], d["ys"], d["xe"], d["ye"],
+                                          d["cosa"], d["sina"], d["xv"], d["yv"])
+    assert np.array_equal(vx, d["vx"]) and np.array_equal(vy, d["vy"])

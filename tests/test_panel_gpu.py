@@ -88,3 +88,51 @@ def test_shuffled_panels_and_many_groups():
         rx, ry = oracle.panel_velocity(*arrs, xv, yv)
         vx, vy = pfblob.inducedVelocity(*arrs, xv, yv)
         assert normwise_err(vx, vy, rx, ry) <= TOL, (m, shuffle)
+
+
+def test_source_panels_vs_reference_golden(golden):
+    """Constant-source panels (panelKernel=0): velocity against the
+    reference's Cython kernel (gate 1e-6; the point 1e-6 from panel 0 and the
+    points on its line extension as for vortex panels) and the influence
+    matrix against its assemble_influenceMatrix (1e-12)."""
+    import pfblob
+    d = golden("source_panel")
+    args = [d[k] for k in ("sigma", "xs", "ys", "xe", "ye", "cosa", "sina")]
+    vx, vy = pfblob.inducedVelocity(*args, d["xv"], d["yv"], panelKernel=0)
+    assert normwise_err(vx[4:], vy[4:], d["vx"][4:], d["vy"][4:]) <= TOL
+    e3 = np.hypot(vx[3] - d["vx"][3], vy[3] - d["vy"][3])
+    assert e3 <= 1e-5 * np.hypot(d["vx"][3], d["vy"][3]) + 1e-6
+    assert np.allclose(vx[:3], d["vx"][:3], rtol=1e-5, atol=1e-7)
+    assert np.allclose(vy[:3], d["vy"][:3], rtol=1e-5, atol=1e-7)
+    A = pfblob.influenceMatrix(d["xcp"], d["ycp"], *args[1:], panelKernel=0)
+    assert np.abs(A - d["A"]).max() <= 1e-12 * np.abs(d["A"]).max()
+
+
+def test_source_panels_far_field_and_panels_class():
+    """Far points take the groups' series only (1e-10 against the FP64
+    oracle); a 'css' Panels body solves the no-through-flow condition
+    (RHS = -v.n) with the source influence matrix."""
+    import pfblob
+    from pfblob import workloads as wl
+    ps = wl.cylinder_panels(512)
+    rng = np.random.default_rng(8)
+    r = rng.uniform(2.0, 6.0, 8000)
+    t = rng.uniform(-np.pi, np.pi, 8000)
+    xv, yv = r * np.cos(t), r * np.sin(t)
+    args = (ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina)
+    rx, ry = oracle.source_panel_velocity(*args, xv, yv)
+    vx, vy = pfblob.inducedVelocity(*args, xv, yv, panelKernel=0)
+    assert normwise_err(vx, vy, rx, ry) <= 1e-10
+    m = 64
+    th = np.linspace(0.0, 2.0 * np.pi, m + 1)
+    th[-1] = 0.0
+    geo = {"b": {"xPanel": 0.5 * np.cos(th), "yPanel": 0.5 * np.sin(th),
+                 "cmGlobal": np.array([0.1, 0.2]), "thetaLocal": 0.3, "dPanel": 0.01}}
+    panels = pfblob.Panels(geo, panelKernel='css', problemType='fixed')
+    vxe, vye = rng.standard_normal(m), rng.standard_normal(m)
+    panels.solve(vxe, vye)
+    n = panels.normCat
+    rhs = (-vxe) * n[0] + (-vye) * n[1]
+    s_ref = np.linalg.solve(panels.A, rhs)
+    assert np.abs(panels.sPanel - s_ref).max() <= 1e-10 * np.abs(s_ref).max()
+    assert np.all(np.asarray(panels.gTotal) == 0.0)

@@ -1,6 +1,6 @@
 """Direct Gaussian-blob velocity on the GPU vs the FP64 oracle.
 
-Tolerance (north-star gate): max_i |v_i - v_ref_i| / max_i |v_ref_i| <= 1e-6."""
+Tolerance (the accuracy gate of the velocity): max_i |v_i - v_ref_i| / max_i |v_ref_i| <= 1e-6."""
 import numpy as np
 import pytest
 import torch

@@ -47,6 +47,9 @@
 
 namespace {
 
+using pf::fmmx::P2PDesc;
+using pf::fmmx::P2PWork;
+
 constexpr double THETA = 0.5;
 constexpr double INV_2PI = 0.15915494309189535;
 constexpr int MAX_LEVEL = pf::fmmx::MAX_LEVEL;
@@ -962,13 +965,6 @@ __device__ __forceinline__ float warp_max(float v) {
 
 constexpr int P2P_OWN_GROUPS = 4;  // target groups a block's own CTA computes at most
 
-// Work-distribution state of the P2P launches, zeroed before the first.
-struct P2PWork {
-    unsigned *heavy_n;   // entries in heavy
-    int32_t *heavy;      // blocks with several target groups [nblk]
-    int32_t *grp_next;   // groups of each heavy block handed out so far [nblk]
-    int64_t ns, nt;      // sorted sources and targets (bounds-checked build)
-};
 
 // Target group gi of block b (groups of at most 96 targets, balanced: sizes
 // differ by at most one; every group streams all the block's sources, so a
@@ -1159,71 +1155,97 @@ __device__ __forceinline__ void p2p_group_body(
     }
 }
 
-// Two launches of one kernel.  HEAVY = false: one CTA per P2P block (in
-// launch order) computes the block's target groups, unless there are more
-// than P2P_OWN_GROUPS of them: such a block (a dense cluster) is listed as
-// heavy.  HEAVY = true: persistent CTAs share out the groups of the heavy
-// blocks through per-block counters (counters only, no waits; each group is
-// computed by exactly one CTA, so results do not depend on the schedule).
-// Without dense clusters the second launch finds nothing to do.
-template <bool HEAVY>
-__global__ void __launch_bounds__(32, P2P_MIN_CTAS)
-k_p2p(int64_t nblk, int kb, const int32_t *__restrict__ tstart, const int32_t *__restrict__ tcnt,
-      const int32_t *__restrict__ sstart, const int32_t *__restrict__ scnt,
-      const float4 *__restrict__ shl, const float *__restrict__ sg32,
-      const float4 *__restrict__ thl, const int32_t *__restrict__ run_off,
-      const int2 *__restrict__ runs, const int32_t *__restrict__ order, pfd::GaussParams gp,
-      double2 *__restrict__ nearv, unsigned long long *__restrict__ pairs, P2PWork work) {
-    __shared__ int s_rs[P2P_RUNS_SM];      // particle start of run
-    __shared__ int s_rp[P2P_RUNS_SM + 1];  // stream prefix of run
+// Shared memory of one P2P CTA (one warp).
+struct P2PSmem {
     // source buffers, one per mode: [P2P_FAR], [P2P_FULL], [P2P_SERIES]
-    __shared__ ulonglong2 s_hi[3][P2P_BUF];  // {x_hi, x_hi}, {y_hi, y_hi}
-    __shared__ ulonglong2 s_lo[3][P2P_BUF];  // {x_lo, x_lo}, {y_lo, y_lo}
-    __shared__ unsigned long long s_g2[3][P2P_BUF];  // {g, g}
-    const int lane = threadIdx.x;
-    unsigned long long npairs = 0, nfar = 0;
-    auto targets = [&](int64_t b, int &t0) {
-        const uint32_t leaf0 = (uint32_t)b << (2 * kb), nl = 1u << (2 * kb);
-        t0 = tstart[leaf0];
-        return tstart[leaf0 + nl - 1] + tcnt[leaf0 + nl - 1] - t0;
-    };
-    if (!HEAVY) {
-        if ((int64_t)blockIdx.x >= nblk) return;
-        const int64_t b = order[blockIdx.x];
-        int t0;
-        const int tn = targets(b, t0);
-        if (tn == 0) return;
-        const int ngrp = (tn + 95) / 96;
-        if (ngrp > P2P_OWN_GROUPS) {  // left to the second launch
-            if (lane == 0) work.heavy[atomicAdd(work.heavy_n, 1u)] = (int32_t)b;
-        } else {
-            for (int gi = 0; gi < ngrp; ++gi)
-                p2p_group_body(b, t0, tn, ngrp, gi, sstart, scnt, shl, sg32, thl, run_off, runs,
-                               gp, nearv, s_hi, s_lo, s_g2, s_rs, s_rp, npairs, nfar, work.ns,
-                               work.nt);
-        }
+    ulonglong2 hi[3][P2P_BUF];  // {x_hi, x_hi}, {y_hi, y_hi}
+    ulonglong2 lo[3][P2P_BUF];  // {x_lo, x_lo}, {y_lo, y_lo}
+    unsigned long long g2[3][P2P_BUF];  // {g, g}
+    int rs[P2P_RUNS_SM];      // particle start of run
+    int rp[P2P_RUNS_SM + 1];  // stream prefix of run
+};
+
+// Targets of P2P block b: first sorted target t0, count returned.
+__device__ __forceinline__ int p2p_targets(const P2PDesc &d, int64_t b, int &t0) {
+    const uint32_t leaf0 = (uint32_t)b << (2 * d.kb), nl = 1u << (2 * d.kb);
+    t0 = d.tstart[leaf0];
+    return d.tstart[leaf0 + nl - 1] + d.tcnt[leaf0 + nl - 1] - t0;
+}
+
+__device__ __forceinline__ void p2p_group(const P2PDesc &d, int64_t b, int t0, int tn, int ngrp,
+                                          int gi, P2PSmem &sm, unsigned long long &npairs,
+                                          unsigned long long &nfar) {
+    p2p_group_body(b, t0, tn, ngrp, gi, d.sstart, d.scnt, d.shl, d.sg32, d.thl, d.run_off, d.runs,
+                   d.gp, d.nearv, sm.hi, sm.lo, sm.g2, sm.rs, sm.rp, npairs, nfar, d.work.ns,
+                   d.work.nt);
+}
+
+// The CTA of P2P block `local` (launch order): its target groups, unless
+// there are more than P2P_OWN_GROUPS of them: such a block (a dense cluster)
+// is listed as heavy for the second launch.
+__device__ __forceinline__ void p2p_own_block(const P2PDesc &d, int64_t local, P2PSmem &sm,
+                                              unsigned long long &npairs,
+                                              unsigned long long &nfar) {
+    const int64_t b = d.order[local];
+    int t0;
+    const int tn = p2p_targets(d, b, t0);
+    if (tn == 0) return;
+    const int ngrp = (tn + 95) / 96;
+    if (ngrp > P2P_OWN_GROUPS) {  // left to the second launch
+        if (threadIdx.x == 0) d.work.heavy[atomicAdd(d.work.heavy_n, 1u)] = (int32_t)b;
     } else {
-        const unsigned nh = *work.heavy_n;  // complete: written by the first launch
-        for (unsigned k = 0; k < nh; ++k) {
-            const int64_t b = work.heavy[k];
-            int t0;
-            const int tn = targets(b, t0);
-            const int ngrp = (tn + 95) / 96;
-            for (;;) {
-                unsigned gi = 0;
-                if (lane == 0) gi = atomicAdd((unsigned *)&work.grp_next[b], 1u);
-                gi = __shfl_sync(0xffffffffu, gi, 0);
-                if ((int)gi >= ngrp) break;
-                p2p_group_body(b, t0, tn, ngrp, (int)gi, sstart, scnt, shl, sg32, thl, run_off,
-                               runs, gp, nearv, s_hi, s_lo, s_g2, s_rs, s_rp, npairs, nfar,
-                               work.ns, work.nt);
-            }
-        }
+        for (int gi = 0; gi < ngrp; ++gi) p2p_group(d, b, t0, tn, ngrp, gi, sm, npairs, nfar);
     }
-    if (lane == 0) {
-        atomicAdd(pairs, npairs);
-        atomicAdd(pairs + 2, nfar);
+}
+
+// The groups of one heavy block, shared out through its counter (counters
+// only, no waits; each group is computed by exactly one CTA, so results do
+// not depend on the schedule).
+__device__ __forceinline__ void p2p_heavy_block(const P2PDesc &d, int64_t b, P2PSmem &sm,
+                                                unsigned long long &npairs,
+                                                unsigned long long &nfar) {
+    int t0;
+    const int tn = p2p_targets(d, b, t0);
+    const int ngrp = (tn + 95) / 96;
+    for (;;) {
+        unsigned gi = 0;
+        if (threadIdx.x == 0) gi = atomicAdd((unsigned *)&d.work.grp_next[b], 1u);
+        gi = __shfl_sync(0xffffffffu, gi, 0);
+        if ((int)gi >= ngrp) break;
+        p2p_group(d, b, t0, tn, ngrp, (int)gi, sm, npairs, nfar);
     }
+}
+
+__device__ __forceinline__ void p2p_heavy_blocks(const P2PDesc &d, P2PSmem &sm,
+                                                 unsigned long long &npairs,
+                                                 unsigned long long &nfar) {
+    const unsigned nh = *d.work.heavy_n;  // complete: written by the first launch
+    for (unsigned k = 0; k < nh; ++k) p2p_heavy_block(d, d.work.heavy[k], sm, npairs, nfar);
+}
+
+__device__ __forceinline__ void p2p_count(const P2PDesc &d, unsigned long long npairs,
+                                          unsigned long long nfar) {
+    if (threadIdx.x == 0 && (npairs | nfar)) {
+        atomicAdd(d.pairs, npairs);
+        atomicAdd(d.pairs + 2, nfar);
+    }
+}
+
+// Two launches of one kernel.  HEAVY = false: one CTA per P2P block (in
+// launch order) computes the block's target groups (or lists the block as
+// heavy).  HEAVY = true: persistent CTAs share out the groups of the heavy
+// blocks.  Without dense clusters the second launch finds nothing to do.
+template <bool HEAVY>
+__global__ void __launch_bounds__(32, P2P_MIN_CTAS) k_p2p(const P2PDesc d) {
+    __shared__ P2PSmem sm;
+    unsigned long long npairs = 0, nfar = 0;
+    if (!HEAVY) {
+        if ((int64_t)blockIdx.x >= d.nblk) return;
+        p2p_own_block(d, blockIdx.x, sm, npairs, nfar);
+    } else {
+        p2p_heavy_blocks(d, sm, npairs, nfar);
+    }
+    p2p_count(d, npairs, nfar);
 }
 
 // SMs of the current device (cached per device; host threads may race to
@@ -1622,6 +1644,26 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
                            big, st));
     PF_TRY(count_up(L, scnt_all, st));
     if (!same) PF_TRY(count_up(L, tcnt_all, st));
+    // the near field's description
+    const int64_t nblk = (int64_t)1 << (2 * (L - kb));
+    P2PDesc pd;
+    pd.nblk = nblk;
+    pd.kb = kb;
+    pd.tstart = tstart;
+    pd.tcnt = T.cnt;
+    pd.sstart = S.start;
+    pd.scnt = S.cnt;
+    pd.shl = S.hl;
+    pd.sg32 = S.g32;
+    pd.thl = T.hl;
+    pd.run_off = c.d_run_off;
+    pd.runs = c.d_runs;
+    pd.order = c.d_blk_order;
+    pd.gp = pfd::make_gauss_params(a.ksigmasqr);
+    pd.nearv = nearv;
+    pd.pairs = ctr;
+    pd.work = P2PWork{p2pw_mem, (int32_t *)(p2pw_mem + 64), (int32_t *)(p2pw_mem + 64) + nblk, ns,
+                      nt};
 
     PF_TRY(mark(1));
     // upward pass
@@ -1669,20 +1711,12 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     PF_TRY(mark(4));
     // near field
     {
-        const int64_t nblk = (int64_t)1 << (2 * (L - kb));
         PF_CUDA_TRY(cudaMemsetAsync(p2pw_mem, 0, p2pw_bytes, st));
-        P2PWork work{p2pw_mem, (int32_t *)(p2pw_mem + 64), (int32_t *)(p2pw_mem + 64) + nblk, ns,
-                     nt};
-        const pfd::GaussParams gp = pfd::make_gauss_params(a.ksigmasqr);
-        k_p2p<false><<<(unsigned)nblk, 32, 0, st>>>(
-            nblk, kb, tstart, T.cnt, S.start, S.cnt, S.hl, S.g32, T.hl, c.d_run_off, c.d_runs,
-            c.d_blk_order, gp, nearv, ctr, work);
+        k_p2p<false><<<(unsigned)nblk, 32, 0, st>>>(pd);
         PF_TRY(pf::launch_status("k_p2p"));
         // the remaining groups of blocks with more than 96 targets (if any)
         const int64_t grid = std::min<int64_t>((int64_t)p2p_sm_count() * P2P_MIN_CTAS, nt / 96 + 1);
-        k_p2p<true><<<(unsigned)grid, 32, 0, st>>>(
-            nblk, kb, tstart, T.cnt, S.start, S.cnt, S.hl, S.g32, T.hl, c.d_run_off, c.d_runs,
-            c.d_blk_order, gp, nearv, ctr, work);
+        k_p2p<true><<<(unsigned)grid, 32, 0, st>>>(pd);
         PF_TRY(pf::launch_status("k_p2p"));
     }
     PF_TRY(mark(5));

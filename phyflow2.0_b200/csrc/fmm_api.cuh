@@ -2,6 +2,7 @@
 // (the batch runtime): plans are built on the host once, executions only
 // enqueue kernels (no synchronisation, capturable in a CUDA graph).
 #pragma once
+#include "gauss_pair.cuh"
 #include "pf_common.cuh"
 
 namespace pf {
@@ -33,6 +34,34 @@ void tuning_set(int leaf_level, int np, int kb);
 constexpr int MAX_LEVEL = 11;
 // device counters one FMM call writes (see exec_fmm)
 constexpr int FMM_COUNTERS = 3;
+
+// Work-distribution state of the P2P launches of one FMM call, zeroed before
+// the first.
+struct P2PWork {
+    unsigned *heavy_n;   // entries in heavy
+    int32_t *heavy;      // blocks with several target groups [nblk]
+    int32_t *grp_next;   // groups of each heavy block handed out so far [nblk]
+    int64_t ns, nt;      // sorted sources and targets (bounds-checked build)
+};
+
+// Everything the near field (P2P) of one FMM call reads and writes: its
+// sorted points and leaf tables, the plan's run lists and launch order, the
+// kernel parameters and its outputs (the P2P kernels' one argument).
+struct P2PDesc {
+    int64_t nblk;  // P2P blocks
+    int kb;        // block level drop
+    const int32_t *tstart, *tcnt, *sstart, *scnt;
+    const float4 *shl;
+    const float *sg32;
+    const float4 *thl;
+    const int32_t *run_off;
+    const int2 *runs;
+    const int32_t *order;
+    pfd::GaussParams gp;
+    double2 *nearv;
+    unsigned long long *pairs;
+    P2PWork work;
+};
 
 }  // namespace fmmx
 }  // namespace pf

@@ -27,7 +27,8 @@
 //      takes one of the 11 x 32 base cells feeding the tile (a warp per base
 //      row), walks the cell's blobs in input-index order (found in
 //      registers), forms their four x weights M4'(ux_a) and four y weights
-//      M4'(uy_b) (_interpolation_kernels_1d.cpp:75-89) or Tutty's, and
+//      M4'(uy_b) (_interpolation_kernels_1d.cpp:75-89; with c = 0 each node on
+//      its known branch, m4p_outer / m4p_inner) or Tutty's, and
 //      accumulates the cell's 4 x 4 stencil of partial sums sum (wx_a wy_b) g
 //      in shared memory.  Then each output cell adds the 16 partial sums of the base
 //      cells that cover it in fixed (b, a) order and writes x = ix*h + 0.5h +

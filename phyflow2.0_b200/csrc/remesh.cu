@@ -40,6 +40,7 @@
 // No floating-point atomics: each partial and each output value is produced
 // by one thread in a fixed order, so results are bitwise reproducible.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -732,16 +733,83 @@ struct TileOut {
     int64_t nrec;   // records (blobs placed): bounds-checked build
 };
 
+// The lane L of the warp whose exclusive offset off_L is the last one <= o
+// (offsets non-decreasing over the lanes, off_0 = 0): the cell of blob o of
+// the warp's row.  Every lane of the warp must call it.
+__device__ __forceinline__ int row_owner(int off, int o) {
+    int L = 0;
+#pragma unroll
+    for (int s = 16; s; s >>= 1) {
+        const int v = __shfl_sync(0xffffffffu, off, L + s);
+        if (v <= o) L += s;
+    }
+    return L;
+}
+
+// The 16 stencil partial sums of one base cell from its blobs in input-index
+// order (the atomic ranks of k_rm_count are not reproducible, so the order is
+// found here): cnt blobs, whose input index is ids(j) and whose four x
+// weights times g and four y weights are wv(j, 0..7), j in [0, cnt).  Up to
+// TILE_PREF indices are ordered in registers.
+template <class Ids, class Wv>
+__device__ __forceinline__ void cell_sums(int cnt, Ids ids_of, Wv wv, double (&p)[16]) {
+    int ids[TILE_PREF];  // input indices are below 2^31
+#pragma unroll
+    for (int j = 0; j < TILE_PREF; ++j) ids[j] = j < cnt ? ids_of(j) : INT_MAX;
+    int last = -1;
+    for (int k = 0; k < cnt; ++k) {
+        int best = INT_MAX;
+        int bj = 0;
+        if (cnt <= TILE_PREF) {
+#pragma unroll
+            for (int j = 0; j < TILE_PREF; ++j)
+                if (ids[j] > last && ids[j] < best) {
+                    best = ids[j];
+                    bj = j;
+                }
+        } else {
+            for (int j = 0; j < cnt; ++j) {
+                const int v = ids_of(j);
+                if (v > last && v < best) {
+                    best = v;
+                    bj = j;
+                }
+            }
+        }
+        last = best;
+        double wxg[4], wy[4];
+        wv(bj, wxg, wy);
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) p[a * 4 + b] = __fma_rn(wxg[a], wy[b], p[a * 4 + b]);
+    }
+}
+
+// Records of one base row (one warp) staged in shared memory with their
+// weights: TW_CAP per warp; a row with more runs the per-cell walk on the
+// records in HBM instead.  The row's stencil partials (16 x 32 doubles) reuse
+// the first 4 KB of the same region once the row is summed.
+constexpr int TW_CAP = 128;
+constexpr int TW_BYTES = TW_CAP * 8 * (int)sizeof(double) + TW_CAP * (int)sizeof(int);
+constexpr int TILE_SMEM = TBX * TW_BYTES;
+static_assert(16 * 32 * (int)sizeof(double) <= TW_CAP * 8 * (int)sizeof(double),
+              "row partials fit in the row's staging");
+
 // One CTA per tile of TOX x TOY output cells (persistent loop over tiles).
-// EMIT: the new blobs are written at their slots; else the cell values and
-// touched flags of every window cell go to acc / flag.
+// Warp r takes base row r of the tile, lane l its base cell l.  The row's
+// blobs (contiguous runs of records, one per cell) are spread over the lanes:
+// each lane forms the eight weights of one blob (all lanes busy), then each
+// lane sums its own cell's blobs from shared memory in input-index order
+// (16 FMA per blob).  EMIT: the new blobs are written at their slots; else the
+// cell values and touched flags of every window cell go to acc / flag.
 template <int WK, bool EMIT>
 __global__ void __launch_bounds__(TILE_THREADS, 2)
 k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
           const int32_t *__restrict__ start, const WRec *__restrict__ recs,
           const double *__restrict__ part_big, WParams wp,
           TileOut to, double *__restrict__ mpart, RmHead *hmom) {
-    __shared__ double s_p[16][TILE_THREADS];
+    extern __shared__ __align__(16) unsigned char s_tile[];
     __shared__ unsigned char s_occ[TILE_THREADS];
     __shared__ double s_mom[TILE_THREADS / 32][4];  // per warp, summed over its tiles in order
     Win w;
@@ -750,10 +818,14 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
     const int64_t ntiles = ntx * nty;
     const bool emit_ok = !EMIT || (int64_t)hd->total <= to.capacity;
     const int lbx = threadIdx.x >> 5, lby = threadIdx.x & 31;
+    double *const sw = reinterpret_cast<double *>(s_tile + lbx * TW_BYTES);  // [8][TW_CAP]
+    int *const sid = reinterpret_cast<int *>(sw + 8 * TW_CAP);
     if (EMIT && threadIdx.x < (TILE_THREADS / 32) * 4) s_mom[threadIdx.x >> 2][threadIdx.x & 3] = 0.0;
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int64_t tx = t / nty, ty = t - tx * nty;
-        const int64_t ox0 = tx * TOX, oy0 = ty * TOY;
+    // tiles are fewer than the window's cells (< 2^31): 32-bit tile indices
+    const int nty32 = (int)nty;
+    for (int t = blockIdx.x; t < (int)ntiles; t += gridDim.x) {
+        const int tx = t / nty32, ty = t - tx * nty32;
+        const int64_t ox0 = (int64_t)tx * TOX, oy0 = (int64_t)ty * TOY;
         // 1. the 16 partial sums of this thread's base cell
         {
             const int64_t bx = ox0 - 3 + lbx, by = oy0 - 3 + lby;
@@ -761,59 +833,119 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
 #pragma unroll
             for (int q = 0; q < 16; ++q) p[q] = 0.0;
             int cnt = 0;
+            int64_t st = 0;
             if (bx >= 0 && bx < w.nbx && by >= 0 && by < w.nby) {
                 const int64_t bc = bx * w.nby + by;
                 cnt = count[bc];
-                if (cnt > 0 && !PF_IDX_OK((int64_t)start[bc] + cnt - 1, to.nrec, 105)) cnt = 0;
-                if (cnt > 0) {
-                    const WRec *rc = recs + start[bc];
-                    const int64_t ix0 = lat_x(w, bx), iy0 = lat_y(w, by);
-                    // the cell's blobs in input-index order (the atomic ranks
-                    // of k_rm_count are not reproducible): up to TILE_PREF
-                    // indices are loaded at once and ordered in registers
-                    int ids[TILE_PREF];  // input indices are below 2^31
+                st = start[bc];
+                if (cnt > 0 && !PF_IDX_OK(st + cnt - 1, to.nrec, 105)) cnt = 0;
+            }
+            // a tile fed by no blob touches no output cell
+            if (!__syncthreads_or(cnt != 0)) {
+                if (!EMIT && threadIdx.x < TOX * TOY) {
+                    const int lx = threadIdx.x / TOY, ly = threadIdx.x - lx * TOY;
+                    const int64_t ox = ox0 + lx, oy = oy0 + ly;
+                    if (ox < w.nox && oy < w.noy) {
+                        to.acc[ox * w.noy + oy] = 0.0;
+                        to.flag[ox * w.noy + oy] = 0;
+                    }
+                }
+                continue;
+            }
+            // the row's blobs of cells walked here (a big cell's stencil is
+            // in its table): exclusive warp scan of the counts
+            const int cs = cnt > 0 ? cnt : 0;
+            int inc = cs;
 #pragma unroll
-                    for (int j = 0; j < TILE_PREF; ++j)
-                        ids[j] = j < cnt ? (int)rc[j].idx : INT_MAX;
-                    int last = -1;
-                    for (int k = 0; k < cnt; ++k) {
-                        int best = INT_MAX;
-                        int bj = 0;
-                        if (cnt <= TILE_PREF) {
-#pragma unroll
-                            for (int j = 0; j < TILE_PREF; ++j)
-                                if (ids[j] > last && ids[j] < best) {
-                                    best = ids[j];
-                                    bj = j;
-                                }
-                        } else {
-                            for (int j = 0; j < cnt; ++j) {
-                                const int v = (int)rc[j].idx;
-                                if (v > last && v < best) {
-                                    best = v;
-                                    bj = j;
-                                }
-                            }
-                        }
-                        last = best;
-                        const double2 vv = *reinterpret_cast<const double2 *>(rc + bj);
-                        const double gv = rc[bj].g;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lby >= o) inc += u;
+            }
+            const int off = inc - cs;
+            const int total = __shfl_sync(0xffffffffu, inc, 31);
+            const int64_t iy0 = cnt > 0 ? lat_y(w, by) : 0;
+            // rows with at most two blobs per cell (a set near its lattice)
+            // walk their cells directly: little divergence there
+            const bool staged =
+                total <= TW_CAP && __reduce_max_sync(0xffffffffu, (unsigned)cs) > 2u;
+            if (staged) {
+                const int64_t ix0 = lat_x(w, bx);
+                const int st32 = (int)st;  // record positions are below 2^31
+                // (a) input indices of the row's blobs (blob o of the row is
+                // blob o - off[L] of the cell of lane L = row_owner(off, o))
+                for (int o0 = 0; o0 < total; o0 += 32) {
+                    const int o = o0 + lby;
+                    const int L = row_owner(off, o);
+                    const int stL = __shfl_sync(0xffffffffu, st32, L);
+                    const int offL = __shfl_sync(0xffffffffu, off, L);
+                    if (o < total) sid[o] = (int)recs[stL + (o - offL)].idx;
+                }
+                __syncwarp();
+                // (b) each blob's rank in its cell by input index (indices are
+                // distinct); its weights go to that position of the cell
+                for (int o0 = 0; o0 < total; o0 += 32) {
+                    const int o = o0 + lby;
+                    const int L = row_owner(off, o);
+                    const int stL = __shfl_sync(0xffffffffu, st32, L);
+                    const int offL = __shfl_sync(0xffffffffu, off, L);
+                    const int cntL = __shfl_sync(0xffffffffu, cs, L);
+                    const int iyL = __shfl_sync(0xffffffffu, (int)iy0, L);
+                    if (o < total) {
+                        const int me = sid[o];
+                        int r = 0;
+                        for (int j = 0; j < cntL; ++j) r += sid[offL + j] < me;
+                        const WRec *rc = recs + stL + (o - offL);
+                        const double2 vv = *reinterpret_cast<const double2 *>(rc);
+                        const double gv = rc->g;
                         double wx[4], wy[4];
+                        rec_w8<WK>(vv.x, vv.y, ix0, (int64_t)iyL, wp, wx, wy);
+                        const int d = offL + r;
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) {
+                            sw[a * TW_CAP + d] = wx[a] * gv;
+                            sw[(4 + a) * TW_CAP + d] = wy[a];
+                        }
+                    }
+                }
+                __syncwarp();
+                // (c) this lane's cell, its blobs in input-index order
+                for (int k = 0; k < cnt; ++k) {
+                    double wxg[4], wy[4];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        wxg[a] = sw[a * TW_CAP + off + k];
+                        wy[a] = sw[(4 + a) * TW_CAP + off + k];
+                    }
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+#pragma unroll
+                        for (int b = 0; b < 4; ++b)
+                            p[a * 4 + b] = __fma_rn(wxg[a], wy[b], p[a * 4 + b]);
+                }
+            } else if (cnt > 0) {  // weights per visit (sparse rows, rows above TW_CAP)
+                const WRec *rc = recs + st;
+                const int64_t ix0 = lat_x(w, bx);
+                cell_sums(
+                    cnt, [&](int j) { return (int)rc[j].idx; },
+                    [&](int j, double (&wxg)[4], double (&wy)[4]) {
+                        const double2 vv = *reinterpret_cast<const double2 *>(rc + j);
+                        const double gv = rc[j].g;
+                        double wx[4];
                         rec_w8<WK>(vv.x, vv.y, ix0, iy0, wp, wx, wy);
 #pragma unroll
-                        for (int a = 0; a < 4; ++a)
-#pragma unroll
-                            for (int b = 0; b < 4; ++b) p[a * 4 + b] += (wx[a] * wy[b]) * gv;
-                    }
-                } else if (cnt < 0) {  // a cell of more than SEG_SMALL blobs
-                    const double *pb = part_big + (int64_t)(-cnt - 1) * 16;
-#pragma unroll
-                    for (int q = 0; q < 16; ++q) p[q] = pb[q];
-                }
+                        for (int a = 0; a < 4; ++a) wxg[a] = wx[a] * gv;
+                    },
+                    p);
             }
+            if (cnt < 0) {  // a cell of more than SEG_SMALL blobs
+                const double *pb = part_big + (int64_t)(-cnt - 1) * 16;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) p[q] = pb[q];
+            }
+            __syncwarp();  // the row's staging is read; its partials overwrite it
             s_occ[threadIdx.x] = cnt != 0;
 #pragma unroll
-            for (int q = 0; q < 16; ++q) s_p[q][threadIdx.x] = p[q];
+            for (int q = 0; q < 16; ++q) sw[q * 32 + lby] = p[q];
         }
         __syncthreads();
         // 2. each output cell: the partial sums of its 16 covering base cells,
@@ -832,7 +964,8 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
                         const int s = (lx + 3 - a) * TBY + (ly + 3 - b);
                         if (s_occ[s]) {
                             touched = 1;
-                            sum += s_p[a * 4 + b][s];
+                            sum += reinterpret_cast<const double *>(
+                                s_tile + (lx + 3 - a) * TW_BYTES)[(a * 4 + b) * 32 + (ly + 3 - b)];
                         }
                     }
                 const int64_t cid = ox * w.noy + oy;
@@ -878,6 +1011,22 @@ k_rm_tile(const RmHead *hd, const int32_t *__restrict__ count,
                 for (int q = 0; q < 4; ++q) m[q] += s_mom[k][q];
         grid_moments<TILE_THREADS>(m, mpart, &hmom->ticket_out, hmom->mom + 4);
     }
+}
+
+// The tile kernels' dynamic shared memory (above the 48 KB default), set once
+// per device and kernel.
+template <int WK, bool EMIT>
+cudaError_t tile_smem_attr() {
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(k_rm_tile<WK, EMIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TILE_SMEM);
+    if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
 }
 
 // cells mode: emit the flagged cells at their slots (cid up to the capacity;
@@ -1057,8 +1206,12 @@ pf_status remesh_core(Bump &sc, int64_t n, const double *x, const double *y, con
         TileOut to{slot, capacity, xo, yo, go, ixo, iyo, acc, flag, n};
         const int wk = tutty ? WK_TUTTY : (wp.prm == 0.0 ? WK_M4_PLAIN : WK_M4);
         double *const mp = mpart + 4 * gn_max;
-#define PF_RM_TILE(K, E) \
-    k_rm_tile<K, E><<<gt, TILE_THREADS, 0, st>>>(hd, count, start, recs, part_big, wp, to, mp, hd)
+#define PF_RM_TILE(K, E)                                                                  \
+    do {                                                                                  \
+        PF_CUDA_TRY((tile_smem_attr<K, E>()));                                            \
+        k_rm_tile<K, E><<<gt, TILE_THREADS, TILE_SMEM, st>>>(hd, count, start, recs, part_big, \
+                                                             wp, to, mp, hd);             \
+    } while (0)
         if (cells) {
             if (wk == WK_TUTTY) PF_RM_TILE(WK_TUTTY, false);
             else if (wk == WK_M4_PLAIN) PF_RM_TILE(WK_M4_PLAIN, false);

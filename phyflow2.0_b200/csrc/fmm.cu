@@ -459,108 +459,119 @@ k_m2m2(int lc, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
     }
 }
 
-// M2L for all levels 2..L: lane n of a box group = local coefficient n
+// One FP64 tensor-core product d = a b + d of an 8 x 4 by 4 x 8 tile
+// (mma.sync m8n8k4 .f64; tcgen05 has no FP64 kind).  Fragments: a = A[lane/4]
+// [lane%4], b = B[lane%4][lane/4], (d0, d1) = D[lane/4][2 (lane%4) + 0, 1].
+__device__ __forceinline__ void mma_f64(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+constexpr int M2L_THREADS = 128;  // 4 warps, four target boxes each
+
+// M2L for all levels 2..L on the FP64 tensor cores.  One translation adds
+//   L_n += r^(n+1) sum_k C(n+k, k) c_k,   c_k = (-1)^(k+1) M_k r^k
+// (r: the operator's powers), so the binomial matrix is the same for every
+// translation.  A warp holds it as the A operand (rows n, columns k, in 8 x 4
+// fragments) and takes four target boxes of one level with the same far list
+// (same position class: Morton indices r0 + q stride) as the 8 columns of B,
+// the real and imaginary parts of their c.  Per far-list entry: B from the
+// four sources' multipoles, KS mma per 8 rows, then lane (n = lane/4 + 8 mt,
+// box lane%4) scales its (re, im) pair by r^(n+1) into its coefficient.
 template <int NP>
-__global__ void __launch_bounds__(WARP_BOX_THREADS)
-k_m2l(int L, int Bp, int64_t npair, const int32_t *__restrict__ scnt,
+__global__ void __launch_bounds__(M2L_THREADS)
+k_m2l(int L, int Bp, int64_t nquad, const int32_t *__restrict__ scnt,
       const int32_t *__restrict__ tcnt, const double2 *__restrict__ M, double2 *__restrict__ Lc,
       const int4 *__restrict__ far, const int32_t *__restrict__ far_ptr, int maxpos,
       const double2 *__restrict__ pw /* [nop][NP+1] */, const double *__restrict__ binom,
       unsigned long long *__restrict__ ntrans) {
-    using BL = BoxLanes<NP>;
-    __shared__ double2 s_c[WARP_BOX_THREADS / 32][2][32];
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int half = lane / BL::W, n = lane % BL::W;
-    // Each lane group takes two target boxes A, B of one level with the same
-    // far list (same position class): interleaving their translations gives
-    // two independent load chains per step, sharing the list entry, the
-    // operator powers and the binomial row.  Pair unit u -> level l, pair j.
-    const int64_t u = ((int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid) * BL::BPW + half;
+    constexpr int MT = (NP + 7) / 8, KS = (NP + 3) / 4;
+    const int lane = threadIdx.x & 31;
+    const int64_t u = (int64_t)blockIdx.x * (M2L_THREADS / 32) + (threadIdx.x >> 5);
+    if (u >= nquad) return;  // the whole warp
     int l = 2;
-    int64_t j = u < npair ? u : 0;
-    while (l < L && j >= ((int64_t)1 << (2 * l)) / 2) {
-        j -= ((int64_t)1 << (2 * l)) / 2;
+    int64_t j = u;
+    while (l < L && j >= ((int64_t)1 << (2 * l)) / 4) {
+        j -= ((int64_t)1 << (2 * l)) / 4;
         ++l;
     }
-    // boxes r and r + stride share the position class (Morton order)
     const int64_t stride = (l == L) ? (int64_t)Bp * Bp : 4;
-    const int64_t rA = (j / stride) * 2 * stride + (j % stride);
-    const int64_t bgA = level_off(l) + rA, bgB = bgA + stride;
-    const bool liveA = u < npair && tcnt[bgA] != 0;
-    const bool liveB = u < npair && tcnt[bgB] != 0;
-    if (!__any_sync(0xffffffffu, liveA || liveB)) return;
-    // this lane's row of the binomial matrix C(n+k, k), in registers (from
-    // shared memory instead, the dot product below measured 28% slower)
-    double brow[NP];
+    const int64_t r0 = (j / stride) * 4 * stride + (j % stride);
+    // B column lane/4: box tb, part (0 real, 1 imaginary); B row k = 4 s + kq
+    const int tb = lane >> 3, part = (lane >> 2) & 1, kq = lane & 3;
+    // D: box td, rows n = nr + 8 mt
+    const int td = lane & 3, nr = lane >> 2;
+    const uint32_t mb = (uint32_t)(r0 + tb * stride);
+    const int64_t lo = level_off(l);
+    const bool liveb = tcnt[lo + mb] != 0;
+    if (!__any_sync(0xffffffffu, liveb)) return;
+    const bool lived = __shfl_sync(0xffffffffu, liveb, 8 * td);
+    double af[MT][KS];
 #pragma unroll
-    for (int k = 0; k < NP; ++k) brow[k] = (n < NP) ? binom[k * NP + n] : 0.0;
-    const uint32_t mA = (uint32_t)rA, mB = (uint32_t)(rA + stride);
-    const int ixA = (int)compact1by1(mA), iyA = (int)compact1by1(mA >> 1);
-    const int ixB = (int)compact1by1(mB), iyB = (int)compact1by1(mB >> 1);
-    const int pos = (l == L) ? ((ixA % Bp) + Bp * (iyA % Bp)) : ((ixA & 1) | ((iyA & 1) << 1));
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+        for (int s = 0; s < KS; ++s) {
+            const int n = 8 * mt + nr, k = 4 * s + kq;
+            af[mt][s] = (n < NP && k < NP) ? binom[k * NP + n] : 0.0;
+        }
+    const int ixb = (int)compact1by1(mb), iyb = (int)compact1by1(mb >> 1);
+    // the same for the four boxes
+    const int pos = (l == L) ? ((ixb % Bp) + Bp * (iyb % Bp)) : ((ixb & 1) | ((iyb & 1) << 1));
     const int side = 1 << l;
     const int e0 = far_ptr[l * maxpos + pos];
-    const int len = (liveA || liveB) ? far_ptr[l * maxpos + pos + 1] - e0 : 0;
-    int lmax = len;
+    const int len = far_ptr[l * maxpos + pos + 1] - e0;
+    const double sgn = (kq & 1) ? 1.0 : -1.0;  // (-1)^(k+1)
+    double2 acc[MT];
 #pragma unroll
-    for (int o = 16; o; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    double2 accA = make_double2(0.0, 0.0), accB = make_double2(0.0, 0.0);
+    for (int mt = 0; mt < MT; ++mt) acc[mt] = make_double2(0.0, 0.0);
     unsigned nt = 0;
-    const double2 *scA = &s_c[wid][0][half * BL::W];
-    const double2 *scB = &s_c[wid][1][half * BL::W];
-    for (int e = 0; e < lmax; ++e) {
-        bool useA = false, useB = false;
-        int64_t sgA = 0, sgB = 0;
-        int op = 0;
-        if (e < len) {
-            const int4 f = far[e0 + e];
-            op = f.z;
-            const int sxA = ixA + f.x, syA = iyA + f.y, sxB = ixB + f.x, syB = iyB + f.y;
-            useA = liveA && sxA >= 0 && syA >= 0 && sxA < side && syA < side;
-            useB = liveB && sxB >= 0 && syB >= 0 && sxB < side && syB < side;
-            if (useA) sgA = level_off(l) + morton_add(mA, (uint32_t)f.w);
-            if (useB) sgB = level_off(l) + morton_add(mB, (uint32_t)f.w);
-        }
-        // the sources' counts and multipoles are loaded together (boxes in
-        // range either way); an empty source box is then skipped
-        const int cA = useA ? scnt[sgA] : 0, cB = useB ? scnt[sgB] : 0;
-        const double2 *rp = pw + (int64_t)op * (NP + 1);
-        const double2 z2 = make_double2(0.0, 0.0);
-        const double2 mvA = (useA && n < NP) ? M[sgA * NP + n] : z2;
-        const double2 mvB = (useB && n < NP) ? M[sgB * NP + n] : z2;
-        useA = useA && cA != 0;
-        useB = useB && cB != 0;
-        nt += (useA ? 1u : 0u) + (useB ? 1u : 0u);
-        if ((useA || useB) && n < NP) {
-            const double2 r = rp[n];
-            double2 ca = useA ? cmul(mvA, r) : z2, cb = useB ? cmul(mvB, r) : z2;
-            if ((n & 1) == 0) {  // (-1)^(k+1)
-                ca = make_double2(-ca.x, -ca.y);
-                cb = make_double2(-cb.x, -cb.y);
-            }
-            s_c[wid][0][lane] = ca;
-            s_c[wid][1][lane] = cb;
-        }
-        __syncwarp();
-        if ((useA || useB) && n < NP) {
-            double uxa = 0.0, uya = 0.0, uxb = 0.0, uyb = 0.0;
+    for (int e = 0; e < len; ++e) {
+        const int4 f = far[e0 + e];
+        const int sx = ixb + f.x, sy = iyb + f.y;
+        const bool inr = liveb && sx >= 0 && sy >= 0 && sx < side && sy < side;
+        const int64_t sg = inr ? lo + morton_add(mb, (uint32_t)f.w) : 0;
+        // the source's count and multipole are loaded together (the box is
+        // in range either way); an empty source is then skipped
+        const int cs = inr ? scnt[sg] : 0;
+        const double2 *rp = pw + (int64_t)f.z * (NP + 1);
+        double2 mv[KS], rv[KS];
 #pragma unroll
-            for (int k = 0; k < NP; ++k) {
-                const double2 a = scA[k], b = scB[k];
-                uxa = fma(brow[k], a.x, uxa);
-                uya = fma(brow[k], a.y, uya);
-                uxb = fma(brow[k], b.x, uxb);
-                uyb = fma(brow[k], b.y, uyb);
-            }
-            const double2 r1 = rp[n + 1];
-            if (useA) accA = cfma(r1, make_double2(uxa, uya), accA);
-            if (useB) accB = cfma(r1, make_double2(uxb, uyb), accB);
+        for (int s = 0; s < KS; ++s) {
+            const int k = 4 * s + kq;
+            mv[s] = (inr && k < NP) ? M[sg * NP + k] : make_double2(0.0, 0.0);
+            rv[s] = (k < NP) ? rp[k] : make_double2(0.0, 0.0);
         }
-        __syncwarp();
+        const bool use = inr && cs != 0;
+        if (!__any_sync(0xffffffffu, use)) continue;
+        const bool used = __shfl_sync(0xffffffffu, use, 8 * td);
+        nt += ((lane & 7) == 0 && use) ? 1u : 0u;
+        double b[KS];
+#pragma unroll
+        for (int s = 0; s < KS; ++s) {
+            const double2 m = mv[s], r = rv[s];
+            const double v = part ? fma(m.x, r.y, m.y * r.x) : fma(m.x, r.x, -(m.y * r.y));
+            b[s] = use ? sgn * v : 0.0;
+        }
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+            for (int s = 0; s < KS; ++s) mma_f64(d0, d1, af[mt][s], b[s]);
+            const int n = 8 * mt + nr;
+            if (used && n < NP) acc[mt] = cfma(rp[n + 1], make_double2(d0, d1), acc[mt]);
+        }
     }
-    if (liveA && n < NP) Lc[bgA * NP + n] = accA;
-    if (liveB && n < NP) Lc[bgB * NP + n] = accB;
-    if ((liveA || liveB) && n == 0 && nt) atomicAdd(ntrans, (unsigned long long)nt);
+    if (lived) {
+        const int64_t bgd = lo + r0 + td * stride;
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            const int n = 8 * mt + nr;
+            if (n < NP) Lc[bgd * NP + n] = acc[mt];
+        }
+    }
+    nt = __reduce_add_sync(0xffffffffu, nt);
+    if (lane == 0 && nt) atomicAdd(ntrans, (unsigned long long)nt);
 }
 
 // L2L into child level l: lane n of a box group = coefficient n
@@ -1688,9 +1699,9 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     // M2L, all levels >= 2
     const int B = 1 << kb, Bp = B > 2 ? B : 2;
     {
-        const int64_t npair = (nbox - level_off(2)) / 2;  // box pairs of levels 2..L
-        k_m2l<NP><<<(unsigned)pf::ceil_div(npair, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
-            L, Bp, npair, scnt_all, tcnt_all, M, Lc, c.d_far, c.d_far_ptr, c.maxpos, c.d_pw,
+        const int64_t nquad = (nbox - level_off(2)) / 4;  // box quads of levels 2..L
+        k_m2l<NP><<<(unsigned)pf::ceil_div(nquad, M2L_THREADS / 32), M2L_THREADS, 0, st>>>(
+            L, Bp, nquad, scnt_all, tcnt_all, M, Lc, c.d_far, c.d_far_ptr, c.maxpos, c.d_pw,
             c.d_bin, ctr + 1);
         PF_TRY(pf::launch_status("k_m2l"));
     }

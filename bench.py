@@ -338,14 +338,20 @@ def run_ours(args, rank, world):
                             f"(pairs_far): 1 MUFU (rcp) + {FP32_OPS_FAR} FP32 ops"}
         npt = st0["expansion_terms"]
         ms_m2l = statistics.mean(f["ms_m2l"] for f in fmm_stats)
-        m2l_flops = st0["m2l_translations"] * 8.0 * npt * npt
+        # executed FP64 work of one translation: the real binomial matrix times
+        # the complex vector (4 (p+1)^2, on the FP64 tensor cores) and the
+        # scalings by the operator's powers before and after (16 (p+1))
+        m2l_flops = st0["m2l_translations"] * (4.0 * npt * npt + 16.0 * npt)
         fp64_peak = 148 * 64 * 2 * pk["sm_max_mhz"] * 1e6
         roof_m2l = {"bound": "fp64", "kernel": "k_m2l", "achieved": m2l_flops / (ms_m2l * 1e-3) / 1e12,
                     "peak": fp64_peak / 1e12, "unit": "TFLOP/s",
                     "frac": m2l_flops / (ms_m2l * 1e-3) / fp64_peak,
-                    "per_unit": "8 (p+1)^2 FP64 flops per translation",
+                    "per_unit": "4 (p+1)^2 + 16 (p+1) FP64 flops per translation (real binomial "
+                                "matrix x complex vector on the FP64 tensor cores, scalings by the "
+                                "operator's powers)",
                     "translations": st0["m2l_translations"],
-                    "peak_source": "148 SMs x 64 FP64 FMA/clk x 2 x sm_max_mhz (nominal)"}
+                    "peak_source": "148 SMs x 64 FP64 FMA/clk x 2 x sm_max_mhz (nominal; the FP64 "
+                                   "tensor-core rate is the same)"}
         fmm_info = {"leaf_level": st0["leaf_level"], "expansion_terms": npt,
                     "block_level_drop": st0["block_level_drop"], "p2p_pairs": pairs,
                     "p2p_pairs_far": far,

@@ -247,33 +247,78 @@ def run_ours(args, rank, world):
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
+    # eager pass: the step issued call by call (velocity_device, which finds
+    # the tree box on the device and reads it back, then remesh_device_async),
+    # with events between the two calls and the FMM's own phase events; it
+    # gives the phase split and the kernel rooflines
     fmm_stats = []
     if method == "fmm":
         _lib.fmm_profile(True, dev.index)
     l0 = _lib.kernel_launches()
     outs = []
-    with ClockSampler(gpu_id_for_smi(torch)) as clk:
-        for k in range(args.steps):
-            flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
-            # keep only the step's small status tensors: the output blobs are
-            # released, so the allocator reuses their blocks step after step
-            outs.append(step(evs[k])[5:8])
-            if method == "fmm":  # reads the FMM's events: synchronises after the step
-                fmm_stats.append(_lib.fmm_last_stats(dev.index))
-        torch.cuda.synchronize()
-    launches = _lib.kernel_launches() - l0
+    for k in range(args.steps):
+        flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
+        # keep only the step's small status tensors: the output blobs are
+        # released, so the allocator reuses their blocks step after step
+        outs.append(step(evs[k])[5:8])
+        if method == "fmm":  # reads the FMM's events: synchronises after the step
+            fmm_stats.append(_lib.fmm_last_stats(dev.index))
+    torch.cuda.synchronize()
+    eager_launches = _lib.kernel_launches() - l0
     if method == "fmm":
         _lib.fmm_profile(False, dev.index)
     for o in outs:  # every timed step completed its remesh on the first try
         kk, st_ = int(o[0].item()), int(o[1].item())
         assert st_ == 0 and kk == nout, (kk, st_, nout)
-    if world > 1:
-        torch.distributed.barrier()
     vel_ms = [e[0].elapsed_time(e[1]) for e in evs]
     rm_ms = [e[1].elapsed_time(e[2]) for e in evs]
-    step_ms = sum(vel_ms + rm_ms) / args.steps
+    eager_ms = sum(vel_ms + rm_ms) / args.steps
+    last = step()  # the eager step's results (with indices) for the check
+    torch.cuda.synchronize()
+
+    # the headline: the same step as ONE graph launch (pfblob.StepGraph, the
+    # captured pf_blob_step: FMM on the set's bounding box, remesh with its
+    # window found on the device), inputs resident, L2 flushed between steps
+    box = (float(b.x.min()), float(b.x.max()), float(b.y.min()), float(b.y.max()))
+    sg = pfblob.StepGraph(x, y, g, ks, xopt, cut, 1e-6, box, b.h, xb[0], yb[0], 0.0,
+                          method=meth_id, max_base_cells=mb[0])
+    for _ in range(3):
+        sg.launch()
+    torch.cuda.synchronize()
+    gev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    chk = torch.zeros((args.steps, 2), dtype=torch.int64, device=dev)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    l0 = _lib.kernel_launches()
+    with ClockSampler(gpu_id_for_smi(torch)) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))  # L2 flush between timed steps (outside the events)
+            gev[k][0].record(stream)
+            sg.launch(stream.cuda_stream)
+            gev[k][1].record(stream)
+            chk[k, 0].copy_(sg.n_out[0])  # outside the events
+            chk[k, 1].copy_(sg.status[0])
+        torch.cuda.synchronize()
+    launches = _lib.kernel_launches() - l0
+    for kk, st_ in chk.cpu().tolist():
+        assert st_ == 0 and kk == nout, (kk, st_, nout)
+    if world > 1:
+        torch.distributed.barrier()
+    graph_ms = [e[0].elapsed_time(e[1]) for e in gev]
+    step_ms = sum(graph_ms) / args.steps
     t_max = reduce_max(step_ms, dev, world)
     value = world * n / (t_max * 1e-3)
+    graph_info = {"kernels_per_launch": sg.kernels,
+                  "ms_per_step_median": statistics.median(graph_ms),
+                  "equals_eager_bitwise": bool(
+                      torch.equal(sg.vx, vx) and torch.equal(sg.vy, vy) and
+                      all(torch.equal(sg.out[i, :nout], last[i][:nout]) for i in range(3)))}
+    eager_info = {"ms_per_step": eager_ms, "value": world * n / (reduce_max(eager_ms, dev, world)
+                                                                  * 1e-3),
+                  "gpu_launches": eager_launches,
+                  "issue": "velocity_device (tree box found on the device and read back) then "
+                           "remesh_device_async, kernel by kernel"}
 
     # end to end through the public API with host (numpy) buffers: one upload
     # of x, y, g, velocity and remesh, results read back
@@ -382,9 +427,18 @@ def run_ours(args, rank, world):
         "gpu_launches": launches, "roofline": roof, "roofline_remesh": roof_rm,
         "fmm": fmm_info,
         "clocks": clk.summary(), "e2e": e2e,
+        "step_issue": "one CUDA graph launch per step (pfblob.StepGraph: pf_blob_step "
+                      "captured; FMM on the set's bounding box, remesh window found on the "
+                      "device); phase_ms and the rooflines are from the eager pass",
+        "graph": graph_info, "eager": eager_info,
     }
     if rank == 0 and not args.no_check:
-        line["err_vs_fp64"] = check_step(b, vx, vy, last, nout)
+        line["err_vs_fp64"] = check_step(
+            b, sg.vx, sg.vy, (sg.out[0], sg.out[1], sg.out[2], last[3], last[4]), nout)
+        line["err_vs_fp64"]["checked"] = ("the graph's velocity and new blobs (their lattice "
+                                          "indices from the eager step, which the graph equals "
+                                          "bitwise)")
+    sg.close()
     return line
 
 

@@ -57,8 +57,8 @@ pf_status pf_trim(pf_ctx *ctx);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
 int pf_version(void);
 /* Process-wide count of kernels this library has launched (all contexts,
- * all threads).  Diagnostic: the difference across a region is the number of
- * library kernels enqueued in it. */
+ * all threads; a step-graph launch adds its kernel nodes).  Diagnostic: the
+ * difference across a region is the number of library kernels enqueued in it. */
 uint64_t pf_kernel_launches(void);
 /* 1 in the bounds-checked build (libpfblob_checked.so, compiled with
  * -DPF_BOUNDS_CHECK), else 0.  In that build the kernels test their
@@ -410,6 +410,27 @@ typedef struct pf_step {
     double *moments_dev;       /* 8 doubles, may be NULL */
 } pf_step;
 pf_status pf_blob_step(pf_ctx *ctx, const pf_step *step, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * pf_blob_step as one CUDA graph, for a resident set stepped many times.
+ * pf_step_graph_create waits for the device, runs the step once (sizing the
+ * scratch, building or finding the FMM plan), then captures the same call;
+ * the graph owns a private context, so its scratch and FMM plan stay fixed
+ * while it lives.  pf_step_graph_launch enqueues the whole step on `stream`
+ * with one graph launch, ordered after prior work there.  The step's arrays
+ * may change in value between launches, not in address or size; the box,
+ * lattice and window bound are those of `step`.  Results are bitwise those
+ * of pf_blob_step.  No reference counterpart (the reference issues every
+ * kernel of a step separately, src/python/blobs/__blobsClass.py:546-626,
+ * 828-897).
+ * ------------------------------------------------------------------------- */
+typedef struct pf_step_graph pf_step_graph;
+pf_status pf_step_graph_create(pf_ctx *ctx, const pf_step *step, pf_step_graph **out);
+pf_status pf_step_graph_launch(pf_step_graph *graph, void *stream);
+/* Kernel nodes of the captured step (each launch adds them to
+ * pf_kernel_launches). */
+pf_status pf_step_graph_kernels(const pf_step_graph *graph, int64_t *kernels);
+pf_status pf_step_graph_destroy(pf_step_graph *graph);
 
 /* ---------------------------------------------------------------------------
  * pf_remesh_window without any device allocation, for callers that cannot

@@ -75,6 +75,10 @@ void bounds_register(BoundsReader r);
 // Last launch error of this thread, as a status.  Every kernel launch site
 // calls it right after the launch, which also counts the launch.
 pf_status launch_status(const char *what);
+// Adds kernels launched by other means (a graph launch: its kernel nodes).
+void count_launches(uint64_t kernels);
+// Kernel nodes of a captured graph.
+cudaError_t graph_kernel_nodes(cudaGraph_t g, int64_t *out);
 
 // --------------------------------------------------------------------------
 // Device scratch arena: one grow-only allocation per context, carved into

@@ -23,6 +23,26 @@ void clear_error() { g_err[0] = 0; }
 
 static std::atomic<uint64_t> g_launches{0};
 
+void count_launches(uint64_t kernels) { g_launches.fetch_add(kernels, std::memory_order_relaxed); }
+
+cudaError_t graph_kernel_nodes(cudaGraph_t g, int64_t *out) {
+    size_t nn = 0;
+    cudaError_t e = cudaGraphGetNodes(g, nullptr, &nn);
+    if (e != cudaSuccess) return e;
+    std::vector<cudaGraphNode_t> nodes(nn);
+    e = cudaGraphGetNodes(g, nodes.data(), &nn);
+    if (e != cudaSuccess) return e;
+    int64_t k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        e = cudaGraphNodeGetType(nd, &t);
+        if (e != cudaSuccess) return e;
+        if (t == cudaGraphNodeTypeKernel) ++k;
+    }
+    *out = k;
+    return cudaSuccess;
+}
+
 pf_status launch_status(const char *what) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     cudaError_t e = cudaGetLastError();

@@ -13,6 +13,8 @@ Entry points (same names, arguments and results as pHyFlow):
 * ``Blobs``            - the evaluateVelocity / redistribute surface of pHyFlow.blobs.Blobs
 * ``Panels``, ``LagrangianSolver`` - fixed vortex-panel bodies and the coupled
   blob + panel step of pHyFlow.panels.Panels / pHyFlow.lagrangian.LagrangianSolver
+* ``StepGraph``        - a resident set's velocity + remesh step as one CUDA graph
+  launch (no pHyFlow counterpart)
 
 All computation runs in libpfblob.so (hand-written CUDA for sm_100a) through
 the C ABI of include/pfblob.h; PyTorch provides device buffers and streams.
@@ -28,8 +30,9 @@ from .induced import (CPU_HARDWARE, DIRECT_METHOD, FMM_METHOD, GAUSS_KERNEL, GPU
 from .panels import inducedVelocity, influenceMatrix, lu_factor, lu_solve, panel_velocity_device
 from .regrid import (PopulationControl, Regrid, population_control_device, remesh_device,
                      remesh_device_async, velocity_and_regrid)
+from .stepgraph import StepGraph
 
-__all__ = ["Blobs", "Panels", "LagrangianSolver", "velocity", "velocity_device", "vorticity", "Regrid", "remesh_device",
+__all__ = ["Blobs", "Panels", "LagrangianSolver", "StepGraph", "velocity", "velocity_device", "vorticity", "Regrid", "remesh_device",
            "remesh_device_async", "velocity_and_regrid", "PopulationControl",
            "population_control_device", "convection", "convection_device", "diffusion_wee",
            "diffusion_tutty", "inducedVelocity",

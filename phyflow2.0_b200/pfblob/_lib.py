@@ -72,6 +72,10 @@ PROTOTYPES = {
     "pf_remesh_async": [_vp, _i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _vp, _vp,
                         _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "pf_blob_step": [_vp, _vp, _vp],
+    "pf_step_graph_create": [_vp, _vp, _c.POINTER(_vp)],
+    "pf_step_graph_launch": [_vp, _vp],
+    "pf_step_graph_kernels": [_vp, _c.POINTER(_i64)],
+    "pf_step_graph_destroy": [_vp],
     "pf_remesh_window_noalloc": [_i64, _vp, _vp, _vp, _dbl, _dbl, _dbl, _dbl, _i64, _i64, _i64,
                                  _i64, _i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     "pf_fmm_lists": [_int, _int, _dbl, _dbl, _dbl, _vp, _i64, _c.POINTER(_i64)],

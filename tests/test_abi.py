@@ -78,7 +78,7 @@ def test_null_context_is_rejected_without_gpu():
 
 NO_STATUS = {"pf_last_error", "pf_version", "pf_kernel_launches", "pf_fmm_plan_builds",
              "pf_bounds_checked"}
-NULL_IS_NOOP = {"pf_destroy", "pf_batch_destroy"}  # like free(NULL)
+NULL_IS_NOOP = {"pf_destroy", "pf_batch_destroy", "pf_step_graph_destroy"}  # like free(NULL)
 # pf_fmm_set_tuning: 0 = automatic choice of every knob; pf_check_bounds: a
 # no-op in the normal build
 ZEROS_VALID = {"pf_fmm_set_tuning", "pf_check_bounds"}

@@ -383,8 +383,9 @@ k_m2m(int l, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
         if (use && k < NP) {
             const double2 *op = opT + (int64_t)c * NP * NP;
             const double2 *sa = &s_a[wid][half * BL::W];
-#pragma unroll 4
-            for (int mm = 0; mm <= k; ++mm) acc = cfma(op[mm * NP + k], sa[mm], acc);
+            // fixed length: op[mm][k] is 0 for mm > k, so the tail adds nothing
+#pragma unroll
+            for (int mm = 0; mm < NP; ++mm) acc = cfma(op[mm * NP + k], sa[mm], acc);
         }
         __syncwarp();
     }
@@ -408,7 +409,8 @@ k_m2m2(int lc, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
     const int64_t g0 = level_off(lc) + 16 * pb, c0 = level_off(lc - 1) + 4 * pb;
     for (int t = threadIdx.x; t < 16 * NP; t += 256) {
         const int gi = t / NP, k = t - gi * NP;
-        s_g[gi][k] = scnt[g0 + gi] != 0 ? M[(g0 + gi) * NP + k] : make_double2(0.0, 0.0);
+        const double2 m = M[(g0 + gi) * NP + k];  // loaded with the count (box in range)
+        s_g[gi][k] = scnt[g0 + gi] != 0 ? m : make_double2(0.0, 0.0);
     }
     __syncthreads();
     // level lc-1: output (ci, k) is the sum over its 4 children c; one thread
@@ -418,7 +420,9 @@ k_m2m2(int lc, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
         double2 acc = make_double2(0.0, 0.0);
         if (scnt[g0 + 4 * ci + c] != 0) {
             const double2 *op = opT + (int64_t)c * NP * NP;
-            for (int mm = 0; mm <= k; ++mm)
+            // fixed length (op[mm][k] = 0 for mm > k): every load issued at once
+#pragma unroll
+            for (int mm = 0; mm < NP; ++mm)
                 acc = cfma(op[mm * NP + k], s_g[4 * ci + c][mm], acc);
         }
         s_part[c][o] = acc;
@@ -443,7 +447,8 @@ k_m2m2(int lc, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
         double2 acc = make_double2(0.0, 0.0);
         if (scnt[c0 + c] != 0) {
             const double2 *op = opT + (int64_t)c * NP * NP;
-            for (int mm = 0; mm <= k; ++mm) acc = cfma(op[mm * NP + k], s_c[c][mm], acc);
+#pragma unroll
+            for (int mm = 0; mm < NP; ++mm) acc = cfma(op[mm * NP + k], s_c[c][mm], acc);
         }
         s_part[c][k] = acc;
     }
@@ -596,8 +601,9 @@ k_l2l(int l, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
         const double2 *op = opT + (int64_t)c * NP * NP;
         const double2 *sb = &s_b[wid][half * BL::W];
         double2 acc = Lc[bg * NP + n];
-#pragma unroll 4
-        for (int mm = n; mm < NP; ++mm) acc = cfma(op[mm * NP + n], sb[mm], acc);
+        // fixed length: op[mm][n] is 0 for mm < n, so the head adds nothing
+#pragma unroll
+        for (int mm = 0; mm < NP; ++mm) acc = cfma(op[mm * NP + n], sb[mm], acc);
         Lc[bg * NP + n] = acc;
     }
 }
@@ -626,7 +632,11 @@ k_l2l2(int lp, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
         double2 acc = make_double2(0.0, 0.0);
         if (tcnt[c0 + ci] != 0) {
             const double2 *op = opT + (int64_t)ci * NP * NP;
-            for (int mm = n + j; mm < NP; mm += 4) acc = cfma(op[mm * NP + n], s_p[mm], acc);
+#pragma unroll
+            for (int i = 0; i < (NP + 3) / 4; ++i) {
+                const int mm = n + j + 4 * i;
+                if (mm < NP) acc = cfma(op[mm * NP + n], s_p[mm], acc);
+            }
         }
         s_part[j][o] = acc;
     }
@@ -649,7 +659,8 @@ k_l2l2(int lp, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
         if (tcnt[g0 + gi] == 0) continue;
         const double2 *op = opT + (int64_t)(gi & 3) * NP * NP;
         double2 acc = Lc[(g0 + gi) * NP + n];
-        for (int mm = n; mm < NP; ++mm) acc = cfma(op[mm * NP + n], s_c[gi >> 2][mm], acc);
+#pragma unroll
+        for (int mm = 0; mm < NP; ++mm) acc = cfma(op[mm * NP + n], s_c[gi >> 2][mm], acc);
         Lc[(g0 + gi) * NP + n] = acc;
     }
 }

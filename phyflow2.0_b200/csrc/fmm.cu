@@ -221,51 +221,47 @@ __host__ __device__ __forceinline__ int64_t level_off(int l) {
     return ((((int64_t)1) << (2 * l)) - 1) / 3;
 }
 
-// Per leaf: order the leaf's particles by input index (the counting sort's
-// atomic ranks are not reproducible; this fixes every later sum's order).
-__global__ void __launch_bounds__(128)
-k_leaf_sort(int64_t nleaf, const int32_t *__restrict__ start, const int32_t *__restrict__ cnt,
-            int32_t *__restrict__ perm) {
-    const int64_t m = (int64_t)blockIdx.x * 128 + threadIdx.x;
-    if (m >= nleaf) return;
-    const int c = cnt[m];
-    if (c < 2 || c > pf::SEG_SMALL) return;  // larger leaves: seg_sort_listed
-    const int s0 = start[m];
-    for (int k = 1; k < c; ++k) {
-        const int32_t v = perm[s0 + k];
-        int j = k - 1;
-        while (j >= 0 && perm[s0 + j] > v) {
-            perm[s0 + j + 1] = perm[s0 + j];
-            --j;
-        }
-        perm[s0 + j + 1] = v;
-    }
-}
-
-// Sorted copies of the points, one thread per sorted position (coalesced
-// writes): FP64 x, y (g), the hi/lo float4 and float g of the near field.
+// Sorted copies of the points in leaf order, each leaf's particles by input
+// index (the counting sort's atomic ranks are not reproducible; this fixes
+// every later sum's order).  Thread j takes the particle i = perm[j] that the
+// counting sort placed in its leaf's range [s0, s0 + c); its final position
+// is s0 + (number of the leaf's particles with a smaller index), found by
+// reading the leaf's c entries of perm (leaves above SEG_SMALL particles are
+// already in index order: seg_sort_listed).  Writes the final permutation to
+// perm_out and, at that position, FP64 x, y (g), the hi/lo float4 and float g
+// of the near field and the leaf key.
 __global__ void __launch_bounds__(256)
-k_gather_sorted(int64_t n, const int32_t *__restrict__ perm, const double *__restrict__ x,
-                const double *__restrict__ y, const double *__restrict__ g,
-                const uint32_t *__restrict__ key, double *__restrict__ sx,
-                double *__restrict__ sy, double *__restrict__ sg, float4 *__restrict__ hl,
-                float *__restrict__ g32, uint32_t *__restrict__ skey) {
+k_gather_sorted(int64_t n, const int32_t *__restrict__ perm, const uint32_t *__restrict__ key,
+                const int32_t *__restrict__ start, const int32_t *__restrict__ cnt,
+                const double *__restrict__ x, const double *__restrict__ y,
+                const double *__restrict__ g, int32_t *__restrict__ perm_out,
+                double *__restrict__ sx, double *__restrict__ sy, double *__restrict__ sg,
+                float4 *__restrict__ hl, float *__restrict__ g32, uint32_t *__restrict__ skey) {
     const int64_t j = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (j >= n) return;
     const int32_t i = perm[j];
     if (!PF_IDX_OK(i, n, 202)) return;
-    if (skey) skey[j] = key[i];  // leaf key in sorted order (targets)
+    const uint32_t m = key[i];
     const double a = x[i], b = y[i];
-    sx[j] = a;
-    sy[j] = b;
+    const double gi = g ? g[i] : 0.0;
+    const int s0 = start[m], c = cnt[m];
+    int64_t d = j;
+    if (c <= pf::SEG_SMALL && PF_IDX_OK((int64_t)s0 + c - 1, n, 206)) {
+        int r = 0;
+        for (int q = 0; q < c; ++q) r += perm[s0 + q] < i;
+        d = (int64_t)s0 + r;
+    }
+    perm_out[d] = i;
+    if (skey) skey[d] = m;  // leaf key in sorted order (targets)
+    sx[d] = a;
+    sy[d] = b;
     float4 h;
     pfd::split_hilo(a, h.x, h.z);
     pfd::split_hilo(b, h.y, h.w);
-    hl[j] = h;
+    hl[d] = h;
     if (g) {
-        const double gi = g[i];
-        sg[j] = gi;
-        g32[j] = (float)gi;
+        sg[d] = gi;
+        g32[d] = (float)gi;
     }
 }
 
@@ -1536,13 +1532,13 @@ static pf_status sort_points(int64_t n, const double *x, const double *y,
     PF_CUDA_TRY(cudaMemsetAsync(big_n, 0, sizeof(int32_t), st));
     k_place<<<gn, 256, 0, st>>>(n, s.key, s.rank, s.start, s.perm, big, big_n);
     PF_TRY(pf::launch_status("k_place"));
-    k_leaf_sort<<<(unsigned)pf::ceil_div(nleaf, 128), 128, 0, st>>>(nleaf, s.start, s.cnt, s.perm);
-    PF_TRY(pf::launch_status("k_leaf_sort"));
     // leaves above SEG_SMALL particles (dense clusters); the ranks are free now
     PF_TRY(pf::seg_sort_listed(big, big_n, s.start, s.cnt, s.perm, s.rank,
                                n / (pf::SEG_SMALL + 1) + 1, st));
-    k_gather_sorted<<<gn, 256, 0, st>>>(n, s.perm, x, y, g, s.key, s.x, s.y, s.g, s.hl, s.g32,
-                                        skey);
+    // the ranks are free again: they receive the final permutation
+    k_gather_sorted<<<gn, 256, 0, st>>>(n, s.perm, s.key, s.start, s.cnt, x, y, g, s.rank, s.x,
+                                        s.y, s.g, s.hl, s.g32, skey);
+    std::swap(s.perm, s.rank);
     return pf::launch_status("k_gather_sorted");
 }
 
@@ -1664,6 +1660,7 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     if (!same)
         PF_TRY(sort_points(nt, a.xt, a.yt, nullptr, x0, y0, wl, L, T, tmp, tkey_sorted, big + 1,
                            big, st));
+    if (same) T = S;  // sort_points replaced S.perm by the final permutation
     PF_TRY(count_up(L, scnt_all, st));
     if (!same) PF_TRY(count_up(L, tcnt_all, st));
     // the near field's description

@@ -61,7 +61,6 @@ constexpr int P2P_BUF = 64;      // sources per warp buffer (three buffers)
 // it (targets per lane x mode), which must stay within the instruction cache
 constexpr int P2P_UNROLL = 8;
 constexpr int P2P_MIN_CTAS = 24; // one-warp CTAs resident per SM (shared memory bound)
-constexpr int WARP_BOX_THREADS = 128;  // 4 warps, one box each
 constexpr unsigned INVALID_KEY = 0xFFFFFFFFu;
 
 // ---------------------------------------------------------------------------
@@ -347,119 +346,6 @@ k_p2m(int L, double x0, double y0, double wl, const int32_t *__restrict__ start,
 }
 
 
-// Boxes handled per warp by the translation kernels: with p+1 <= 16 terms two
-// boxes share a warp (one half-warp each, lane n = coefficient n), otherwise
-// one box per warp.
-template <int NP>
-struct BoxLanes {
-    static constexpr int BPW = NP <= 16 ? 2 : 1;  // boxes per warp
-    static constexpr int W = 32 / BPW;            // lanes per box
-};
-
-// M2M at parent level l: lane k of a box group = coefficient k
-template <int NP>
-__global__ void __launch_bounds__(WARP_BOX_THREADS)
-k_m2m(int l, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
-      const double2 *__restrict__ opT /* [4][NP(m)][NP(k)] */) {
-    using BL = BoxLanes<NP>;
-    __shared__ double2 s_a[WARP_BOX_THREADS / 32][32];
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int half = lane / BL::W, k = lane % BL::W;
-    const int64_t m = ((int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid) * BL::BPW + half;
-    const bool box_ok = m < ((int64_t)1 << (2 * l));
-    const int64_t bg = level_off(l) + (box_ok ? m : 0);
-    const bool live = box_ok && scnt[bg] != 0;
-    if (!__any_sync(0xffffffffu, live)) return;
-    double2 acc = make_double2(0.0, 0.0);
-    for (int c = 0; c < 4; ++c) {
-        const int64_t cg = level_off(l + 1) + 4 * (box_ok ? m : 0) + c;
-        const bool use = live && scnt[cg] != 0;
-        if (use && k < NP) s_a[wid][lane] = M[cg * NP + k];
-        __syncwarp();
-        if (use && k < NP) {
-            const double2 *op = opT + (int64_t)c * NP * NP;
-            const double2 *sa = &s_a[wid][half * BL::W];
-            // fixed length: op[mm][k] is 0 for mm > k, so the tail adds nothing
-#pragma unroll
-            for (int mm = 0; mm < NP; ++mm) acc = cfma(op[mm * NP + k], sa[mm], acc);
-        }
-        __syncwarp();
-    }
-    if (live && k < NP) M[bg * NP + k] = acc;
-}
-
-// M2M over two levels in one launch: CTA b owns box b of level lc - 2, its 4
-// children (level lc - 1) and 16 grandchildren (level lc).  The grandchildren
-// are staged in shared memory (empty boxes as zeros, which they do not
-// contribute), the children are formed there and written, then the parent.
-// Every coefficient is summed in the order of k_m2m (child c = 0..3, then
-// mm = 0..k), so the results are bitwise those of two k_m2m launches.
-template <int NP>
-__global__ void __launch_bounds__(256)
-k_m2m2(int lc, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
-       const double2 *__restrict__ opT /* [4][NP(m)][NP(k)] */) {
-    __shared__ double2 s_g[16][NP];
-    __shared__ double2 s_part[4][4 * NP];  // [child term c][output]
-    __shared__ double2 s_c[4][NP];
-    const int64_t pb = blockIdx.x;
-    const int64_t g0 = level_off(lc) + 16 * pb, c0 = level_off(lc - 1) + 4 * pb;
-    for (int t = threadIdx.x; t < 16 * NP; t += 256) {
-        const int gi = t / NP, k = t - gi * NP;
-        const double2 m = M[(g0 + gi) * NP + k];  // loaded with the count (box in range)
-        s_g[gi][k] = scnt[g0 + gi] != 0 ? m : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    // level lc-1: output (ci, k) is the sum over its 4 children c; one thread
-    // per (output, c), the 4 partial sums added in c order
-    for (int t = threadIdx.x; t < 16 * NP; t += 256) {
-        const int c = t / (4 * NP), o = t - c * 4 * NP, ci = o / NP, k = o - ci * NP;
-        double2 acc = make_double2(0.0, 0.0);
-        if (scnt[g0 + 4 * ci + c] != 0) {
-            const double2 *op = opT + (int64_t)c * NP * NP;
-            // fixed length (op[mm][k] = 0 for mm > k): every load issued at once
-#pragma unroll
-            for (int mm = 0; mm < NP; ++mm)
-                acc = cfma(op[mm * NP + k], s_g[4 * ci + c][mm], acc);
-        }
-        s_part[c][o] = acc;
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < 4 * NP; o += 256) {
-        const int ci = o / NP, k = o - ci * NP;
-        double2 acc = make_double2(0.0, 0.0);
-        if (scnt[c0 + ci] != 0) {
-            acc = s_part[0][o];
-#pragma unroll
-            for (int c = 1; c < 4; ++c)
-                acc = make_double2(acc.x + s_part[c][o].x, acc.y + s_part[c][o].y);
-            M[(c0 + ci) * NP + k] = acc;
-        }
-        s_c[ci][k] = acc;
-    }
-    __syncthreads();
-    // level lc-2: the same over the 4 boxes just formed
-    for (int t = threadIdx.x; t < 4 * NP; t += 256) {
-        const int c = t / NP, k = t - c * NP;
-        double2 acc = make_double2(0.0, 0.0);
-        if (scnt[c0 + c] != 0) {
-            const double2 *op = opT + (int64_t)c * NP * NP;
-#pragma unroll
-            for (int mm = 0; mm < NP; ++mm) acc = cfma(op[mm * NP + k], s_c[c][mm], acc);
-        }
-        s_part[c][k] = acc;
-    }
-    __syncthreads();
-    const int64_t p = level_off(lc - 2) + pb;
-    for (int k = threadIdx.x; k < NP; k += 256) {
-        if (scnt[p] == 0) continue;
-        double2 acc = s_part[0][k];
-#pragma unroll
-        for (int c = 1; c < 4; ++c)
-            acc = make_double2(acc.x + s_part[c][k].x, acc.y + s_part[c][k].y);
-        M[p * NP + k] = acc;
-    }
-}
-
 // One FP64 tensor-core product d = a b + d of an 8 x 4 by 4 x 8 tile
 // (mma.sync m8n8k4 .f64; tcgen05 has no FP64 kind).  Fragments: a = A[lane/4]
 // [lane%4], b = B[lane%4][lane/4], (d0, d1) = D[lane/4][2 (lane%4) + 0, 1].
@@ -467,6 +353,225 @@ __device__ __forceinline__ void mma_f64(double &d0, double &d1, double a, double
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
+}
+
+// M2M and L2L on the FP64 tensor cores.  The translation of a box's
+// expansion to (M2M) or from (L2L) child position c is a fixed complex NP x NP
+// matrix T_c (lower triangular for M2M, upper for L2L).  A warp task applies
+// it to four boxes at once: the B operand holds their coefficients (column
+// 2j real, 2j + 1 imaginary parts of box j), the A operand the real and the
+// imaginary part of T_c, from fragment tables built with the plan
+// (frag[c][part][mt][ks][lane] = part of T_c[8 mt + lane/4][4 ks + lane%4]);
+// tiles of zeros are skipped.  With U = Re T B and V = Im T B, lane (box
+// lane%4, row n = lane/4 + 8 mt) holds Re = U_re - V_im and Im = U_im + V_re.
+template <int NP>
+struct TcShape {
+    static constexpr int MT = (NP + 7) / 8, KS = (NP + 3) / 4;
+};
+
+// TRI = 1: T[row][col] = 0 for col > row (M2M); TRI = -1: for col < row (L2L)
+template <int TRI>
+__device__ __forceinline__ constexpr bool tc_tile_live(int mt, int ks) {
+    return TRI > 0 ? 4 * ks <= 8 * mt + 7 : 4 * ks + 3 >= 8 * mt;
+}
+
+// d[mt] = T_c b for the lane's (box lane%4, rows lane/4 + 8 mt); b[s] = the
+// lane's B element of k block s (row 4 s + lane%4, column lane/4).
+template <int NP, int TRI>
+__device__ __forceinline__ void tc_apply(const double *__restrict__ fr,
+                                         const double (&b)[TcShape<NP>::KS],
+                                         double2 (&d)[TcShape<NP>::MT]) {
+    constexpr int MT = TcShape<NP>::MT, KS = TcShape<NP>::KS;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+        double u0 = 0.0, u1 = 0.0, v0 = 0.0, v1 = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks) {
+            if (!tc_tile_live<TRI>(mt, ks)) continue;
+            mma_f64(u0, u1, __ldg(fr + ((0 * MT + mt) * KS + ks) * 32 + lane), b[ks]);
+            mma_f64(v0, v1, __ldg(fr + ((1 * MT + mt) * KS + ks) * 32 + lane), b[ks]);
+        }
+        d[mt] = make_double2(u0 - v1, u1 + v0);
+    }
+}
+
+// The lane's B elements of four boxes' coefficients: coef(j, m) is
+// coefficient m of box j (zero for an empty box).
+template <int NP, class Coef>
+__device__ __forceinline__ void tc_load_b(Coef coef, double (&b)[TcShape<NP>::KS]) {
+    const int lane = threadIdx.x & 31;
+    const int j = lane >> 3, part = (lane >> 2) & 1, kq = lane & 3;
+#pragma unroll
+    for (int ks = 0; ks < TcShape<NP>::KS; ++ks) {
+        const int m = 4 * ks + kq;
+        const double2 v = m < NP ? coef(j, m) : make_double2(0.0, 0.0);
+        b[ks] = part ? v.y : v.x;
+    }
+}
+
+constexpr int TC_THREADS = 128;  // four warp tasks per CTA
+
+// M2M into parent level l for four consecutive parents per warp task:
+// out_j[k] = sum_c T_c (children 4 P_j + c, empty ones as zeros), written for
+// the non-empty parents.  With two_level, the same warp then forms the
+// grandparent (level l - 1, box task) from those four parents.
+template <int NP>
+__global__ void __launch_bounds__(TC_THREADS)
+k_m2m_tc(int l, bool two_level, const int32_t *__restrict__ scnt, double2 *__restrict__ M,
+         const double *__restrict__ frag /* [4][2][MT][KS][32] */) {
+    constexpr int MT = TcShape<NP>::MT;
+    constexpr int FR = 2 * MT * TcShape<NP>::KS * 32;  // doubles per child position
+    __shared__ double2 s_par[TC_THREADS / 32][4][NP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int64_t task = (int64_t)blockIdx.x * (TC_THREADS / 32) + wid;
+    if (task >= ((int64_t)1 << (2 * l)) / 4) return;  // the whole warp
+    const int64_t p0 = level_off(l) + 4 * task;        // parents p0 .. p0 + 3
+    const int64_t c0 = level_off(l + 1) + 16 * task;   // their children
+    double2 out[MT];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) out[mt] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        double b[TcShape<NP>::KS];
+        tc_load_b<NP>(
+            [&](int j, int m) {
+                const int64_t ch = c0 + 4 * j + c;
+                const double2 v = M[ch * NP + m];  // loaded with the count
+                return scnt[ch] != 0 ? v : make_double2(0.0, 0.0);
+            },
+            b);
+        double2 d[MT];
+        tc_apply<NP, 1>(frag + c * FR, b, d);
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt)
+            out[mt] = make_double2(out[mt].x + d[mt].x, out[mt].y + d[mt].y);
+    }
+    const int jd = lane & 3, nr = lane >> 2;
+    const bool live = scnt[p0 + jd] != 0;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) {
+        const int n = 8 * mt + nr;
+        if (n >= NP) continue;
+        if (live) M[(p0 + jd) * NP + n] = out[mt];
+        s_par[wid][jd][n] = live ? out[mt] : make_double2(0.0, 0.0);
+    }
+    if (!two_level) return;
+    __syncwarp();
+    // grandparent (task) of level l - 1 from the four parents: column 0 only
+    double2 g[MT];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt) g[mt] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        double b[TcShape<NP>::KS];
+        tc_load_b<NP>([&](int j, int m) { return j == 0 ? s_par[wid][c][m] : make_double2(0.0, 0.0); },
+                      b);
+        double2 d[MT];
+        tc_apply<NP, 1>(frag + c * FR, b, d);
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) g[mt] = make_double2(g[mt].x + d[mt].x, g[mt].y + d[mt].y);
+    }
+    const int64_t gp = level_off(l - 1) + task;
+    if (jd == 0 && scnt[gp] != 0)
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            const int n = 8 * mt + nr;
+            if (n < NP) M[gp * NP + n] = g[mt];
+        }
+}
+
+// L2L from parent level l - 1 into child level l for four consecutive parents
+// per warp task: child 4 P_j + c += T_c L_{P_j}, for the non-empty children.
+// With two_level the same warp first forms the four parents themselves from
+// their parent (level l - 2, box task), then their children.
+template <int NP>
+__global__ void __launch_bounds__(TC_THREADS)
+k_l2l_tc(int l, bool two_level, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
+         const double *__restrict__ frag /* [4][2][MT][KS][32] */) {
+    constexpr int MT = TcShape<NP>::MT;
+    constexpr int FR = 2 * MT * TcShape<NP>::KS * 32;
+    __shared__ double2 s_par[TC_THREADS / 32][4][NP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int jd = lane & 3, nr = lane >> 2;
+    const int64_t task = (int64_t)blockIdx.x * (TC_THREADS / 32) + wid;
+    if (task >= ((int64_t)1 << (2 * l)) / 16) return;  // the whole warp
+    const int64_t p0 = level_off(l - 1) + 4 * task;     // parents p0 .. p0 + 3
+    const int64_t c0 = level_off(l) + 16 * task;        // their children
+    if (two_level) {
+        // the parents (children of box `task` of level l - 2): column 0 only
+        const int64_t gp = level_off(l - 2) + task;
+        const bool glive = tcnt[gp] != 0;
+        double b[TcShape<NP>::KS];
+        tc_load_b<NP>([&](int j, int m) {
+            return (j == 0 && glive) ? Lc[gp * NP + m] : make_double2(0.0, 0.0);
+        }, b);
+        // lanes of column 0 (jd == 0) take parent c's rows: its own local
+        // expansion is loaded before the products
+        double2 old[4][MT];
+        bool plive[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            plive[c] = tcnt[p0 + c] != 0;
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+                const int n = 8 * mt + nr;
+                old[c][mt] = (jd == 0 && n < NP) ? Lc[(p0 + c) * NP + n] : make_double2(0.0, 0.0);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            double2 d[MT];
+            tc_apply<NP, -1>(frag + c * FR, b, d);
+            if (jd == 0)
+#pragma unroll
+                for (int mt = 0; mt < MT; ++mt) {
+                    const int n = 8 * mt + nr;
+                    if (n >= NP) continue;
+                    double2 v = make_double2(0.0, 0.0);
+                    if (plive[c]) {
+                        v = make_double2(old[c][mt].x + d[mt].x, old[c][mt].y + d[mt].y);
+                        Lc[(p0 + c) * NP + n] = v;
+                    }
+                    s_par[wid][c][n] = v;  // broadcast to the warp by shared memory
+                }
+        }
+        __syncwarp();
+    } else {
+        for (int t = lane; t < 4 * NP; t += 32) {
+            const int j = t / NP, n = t - j * NP;
+            s_par[wid][j][n] = tcnt[p0 + j] != 0 ? Lc[(p0 + j) * NP + n] : make_double2(0.0, 0.0);
+        }
+        __syncwarp();
+    }
+    // the children's own local expansions, loaded before the products
+    double2 old[4][MT];
+    bool clive[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int64_t ch = c0 + 4 * jd + c;
+        clive[c] = tcnt[ch] != 0;
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            const int n = 8 * mt + nr;
+            old[c][mt] = n < NP ? Lc[ch * NP + n] : make_double2(0.0, 0.0);
+        }
+    }
+    double b[TcShape<NP>::KS];
+    tc_load_b<NP>([&](int j, int m) { return s_par[wid][j][m]; }, b);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        double2 d[MT];
+        tc_apply<NP, -1>(frag + c * FR, b, d);
+        if (!clive[c]) continue;
+        const int64_t ch = c0 + 4 * jd + c;
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+            const int n = 8 * mt + nr;
+            if (n < NP)
+                Lc[ch * NP + n] = make_double2(old[c][mt].x + d[mt].x, old[c][mt].y + d[mt].y);
+        }
+    }
 }
 
 constexpr int M2L_THREADS = 128;  // 4 warps, four target boxes each
@@ -573,92 +678,6 @@ k_m2l(int L, int Bp, int64_t nquad, const int32_t *__restrict__ scnt,
     }
     nt = __reduce_add_sync(0xffffffffu, nt);
     if (lane == 0 && nt) atomicAdd(ntrans, (unsigned long long)nt);
-}
-
-// L2L into child level l: lane n of a box group = coefficient n
-template <int NP>
-__global__ void __launch_bounds__(WARP_BOX_THREADS)
-k_l2l(int l, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
-      const double2 *__restrict__ opT /* [4][NP(m)][NP(n)] */) {
-    using BL = BoxLanes<NP>;
-    __shared__ double2 s_b[WARP_BOX_THREADS / 32][32];
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int half = lane / BL::W, n = lane % BL::W;
-    const int64_t m = ((int64_t)blockIdx.x * (WARP_BOX_THREADS / 32) + wid) * BL::BPW + half;
-    const bool box_ok = m < ((int64_t)1 << (2 * l));
-    const int64_t bg = level_off(l) + (box_ok ? m : 0);
-    const bool live = box_ok && tcnt[bg] != 0;
-    if (!__any_sync(0xffffffffu, live)) return;
-    const int64_t pg = level_off(l - 1) + ((box_ok ? m : 0) >> 2);
-    const int c = (int)(m & 3);
-    if (live && n < NP) s_b[wid][lane] = Lc[pg * NP + n];
-    __syncwarp();
-    if (live && n < NP) {
-        const double2 *op = opT + (int64_t)c * NP * NP;
-        const double2 *sb = &s_b[wid][half * BL::W];
-        double2 acc = Lc[bg * NP + n];
-        // fixed length: op[mm][n] is 0 for mm < n, so the head adds nothing
-#pragma unroll
-        for (int mm = 0; mm < NP; ++mm) acc = cfma(op[mm * NP + n], sb[mm], acc);
-        Lc[bg * NP + n] = acc;
-    }
-}
-
-// L2L over two levels in one launch: CTA b owns box b of level lp, its 4
-// children (level lp + 1) and 16 grandchildren (level lp + 2); each child's
-// local expansion receives its parent's, then each grandchild its child's,
-// in the order of k_l2l (bitwise equal to two k_l2l launches).
-template <int NP>
-__global__ void __launch_bounds__(256)
-k_l2l2(int lp, const int32_t *__restrict__ tcnt, double2 *__restrict__ Lc,
-       const double2 *__restrict__ opT /* [4][NP(m)][NP(n)] */) {
-    __shared__ double2 s_p[NP];
-    __shared__ double2 s_part[4][4 * NP];  // [term residue j][output]
-    __shared__ double2 s_c[4][NP];
-    const int64_t pb = blockIdx.x;
-    const int64_t p = level_off(lp) + pb;
-    const int64_t c0 = level_off(lp + 1) + 4 * pb, g0 = level_off(lp + 2) + 16 * pb;
-    for (int k = threadIdx.x; k < NP; k += 256) s_p[k] = Lc[p * NP + k];
-    __syncthreads();
-    // level lp+1: output (ci, n) sums the parent's terms mm >= n; one thread
-    // per (output, j) takes mm = n + j, n + j + 4, ...; partial sums added in
-    // j order
-    for (int t = threadIdx.x; t < 16 * NP; t += 256) {
-        const int j = t / (4 * NP), o = t - j * 4 * NP, ci = o / NP, n = o - ci * NP;
-        double2 acc = make_double2(0.0, 0.0);
-        if (tcnt[c0 + ci] != 0) {
-            const double2 *op = opT + (int64_t)ci * NP * NP;
-#pragma unroll
-            for (int i = 0; i < (NP + 3) / 4; ++i) {
-                const int mm = n + j + 4 * i;
-                if (mm < NP) acc = cfma(op[mm * NP + n], s_p[mm], acc);
-            }
-        }
-        s_part[j][o] = acc;
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < 4 * NP; o += 256) {
-        const int ci = o / NP, n = o - ci * NP;
-        double2 acc = make_double2(0.0, 0.0);
-        if (tcnt[c0 + ci] != 0) {
-            acc = Lc[(c0 + ci) * NP + n];
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                acc = make_double2(acc.x + s_part[j][o].x, acc.y + s_part[j][o].y);
-            Lc[(c0 + ci) * NP + n] = acc;
-        }
-        s_c[ci][n] = acc;
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < 16 * NP; t += 256) {
-        const int gi = t / NP, n = t - gi * NP;
-        if (tcnt[g0 + gi] == 0) continue;
-        const double2 *op = opT + (int64_t)(gi & 3) * NP * NP;
-        double2 acc = Lc[(g0 + gi) * NP + n];
-#pragma unroll
-        for (int mm = 0; mm < NP; ++mm) acc = cfma(op[mm * NP + n], s_c[gi >> 2][mm], acc);
-        Lc[(g0 + gi) * NP + n] = acc;
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1323,7 +1342,8 @@ struct FmmCache {
     int64_t nruns = 0;
     size_t dev_bytes = 0;          // device memory held by this plan
     size_t bytes() const { return dev_bytes; }
-    double2 *d_pw = nullptr, *d_m2m = nullptr, *d_l2l = nullptr;
+    double2 *d_pw = nullptr;
+    double *d_m2m = nullptr, *d_l2l = nullptr;  // tensor-core fragment tables
     double *d_bin = nullptr;
     void release() {
         cudaFree(d_far);
@@ -1441,6 +1461,28 @@ static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, doub
                 l2l[(size_t)cc * np * np + (size_t)m * np + k] = make_double2(b.re, b.im);
             }
     }
+    // the same operators as A-operand fragment tables of the tensor-core
+    // kernels: [c][part][mt][ks][lane] = part of T_c[8 mt + lane/4][4 ks + lane%4]
+    // with T_c[k][m] = m2m[c][m][k] (M2M) and T_c[n][m] = l2l[c][m][n] (L2L)
+    const int MTh = (np + 7) / 8, KSh = (np + 3) / 4;
+    std::vector<double> m2mf(4 * 2 * MTh * KSh * 32), l2lf(m2mf.size());
+    for (int cc = 0; cc < 4; ++cc)
+        for (int part = 0; part < 2; ++part)
+            for (int mt = 0; mt < MTh; ++mt)
+                for (int ks = 0; ks < KSh; ++ks)
+                    for (int ln = 0; ln < 32; ++ln) {
+                        const int row = 8 * mt + ln / 4, col = 4 * ks + ln % 4;
+                        const size_t o = ((((size_t)cc * 2 + part) * MTh + mt) * KSh + ks) * 32 + ln;
+                        double vm = 0.0, vl = 0.0;
+                        if (row < np && col < np) {
+                            const double2 a = m2m[(size_t)cc * np * np + (size_t)col * np + row];
+                            const double2 b = l2l[(size_t)cc * np * np + (size_t)col * np + row];
+                            vm = part ? a.y : a.x;
+                            vl = part ? b.y : b.x;
+                        }
+                        m2mf[o] = vm;
+                        l2lf[o] = vl;
+                    }
     std::vector<double> bin(np * np);
     for (int k = 0; k < np; ++k)
         for (int n = 0; n < np; ++n) bin[k * np + n] = binom_d(n + k, k);
@@ -1453,8 +1495,8 @@ static pf_status build_cache(FmmCache &c, int L, int kb, int np, double w0, doub
     PF_TRY(upload(&c.d_far_ptr, ptr, tally));
     PF_TRY(upload(&c.d_q, q, tally));
     PF_TRY(upload(&c.d_pw, pw, tally));
-    PF_TRY(upload(&c.d_m2m, m2m, tally));
-    PF_TRY(upload(&c.d_l2l, l2l, tally));
+    PF_TRY(upload(&c.d_m2m, m2mf, tally));
+    PF_TRY(upload(&c.d_l2l, l2lf, tally));
     PF_TRY(upload(&c.d_bin, bin, tally));
     if (c.nqp <= P2P_QMAX) {
         // P2P run lists of every block (geometry only, reused by every call)
@@ -1689,19 +1731,19 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     k_p2m<NP><<<(unsigned)pf::ceil_div(4 * nleaf, 128), 128, 0, st>>>(L, x0, y0, wl, S.start, S.cnt,
                                                                  S.x, S.y, S.g, M);
     PF_TRY(pf::launch_status("k_p2m"));
-    constexpr int BOXES_PER_CTA = (WARP_BOX_THREADS / 32) * BoxLanes<NP>::BPW;
     // parents at levels L-1 .. 2: two levels per launch, one more when odd
     int lp = L - 1;
     for (; lp - 1 >= 2; lp -= 2) {
-        k_m2m2<NP><<<(unsigned)((int64_t)1 << (2 * (lp - 1))), 256, 0, st>>>(lp + 1, scnt_all, M,
-                                                                            c.d_m2m);
-        PF_TRY(pf::launch_status("k_m2m2"));
+        const int64_t tasks = ((int64_t)1 << (2 * lp)) / 4;
+        k_m2m_tc<NP><<<(unsigned)pf::ceil_div(tasks, TC_THREADS / 32), TC_THREADS, 0, st>>>(
+            lp, true, scnt_all, M, c.d_m2m);
+        PF_TRY(pf::launch_status("k_m2m_tc"));
     }
     if (lp >= 2) {
-        const int64_t nb = (int64_t)1 << (2 * lp);
-        k_m2m<NP><<<(unsigned)pf::ceil_div(nb, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
-            lp, scnt_all, M, c.d_m2m);
-        PF_TRY(pf::launch_status("k_m2m"));
+        const int64_t tasks = ((int64_t)1 << (2 * lp)) / 4;
+        k_m2m_tc<NP><<<(unsigned)pf::ceil_div(tasks, TC_THREADS / 32), TC_THREADS, 0, st>>>(
+            lp, false, scnt_all, M, c.d_m2m);
+        PF_TRY(pf::launch_status("k_m2m_tc"));
     }
     PF_TRY(mark(2));
     // M2L, all levels >= 2
@@ -1717,15 +1759,16 @@ static pf_status exec_fmm(pf::Bump &sc, const FmmArgs &a, const FmmCache &c, dou
     // child levels 3 .. L: two levels per launch, one more when odd
     int lch = 3;
     for (; lch + 1 <= L; lch += 2) {
-        k_l2l2<NP><<<(unsigned)((int64_t)1 << (2 * (lch - 1))), 256, 0, st>>>(lch - 1, tcnt_all, Lc,
-                                                                             c.d_l2l);
-        PF_TRY(pf::launch_status("k_l2l2"));
+        const int64_t tasks = ((int64_t)1 << (2 * (lch + 1))) / 16;
+        k_l2l_tc<NP><<<(unsigned)pf::ceil_div(tasks, TC_THREADS / 32), TC_THREADS, 0, st>>>(
+            lch + 1, true, tcnt_all, Lc, c.d_l2l);
+        PF_TRY(pf::launch_status("k_l2l_tc"));
     }
     if (lch <= L) {
-        const int64_t nb = (int64_t)1 << (2 * lch);
-        k_l2l<NP><<<(unsigned)pf::ceil_div(nb, BOXES_PER_CTA), WARP_BOX_THREADS, 0, st>>>(
-            lch, tcnt_all, Lc, c.d_l2l);
-        PF_TRY(pf::launch_status("k_l2l"));
+        const int64_t tasks = ((int64_t)1 << (2 * lch)) / 16;
+        k_l2l_tc<NP><<<(unsigned)pf::ceil_div(tasks, TC_THREADS / 32), TC_THREADS, 0, st>>>(
+            lch, false, tcnt_all, Lc, c.d_l2l);
+        PF_TRY(pf::launch_status("k_l2l_tc"));
     }
     PF_TRY(mark(4));
     // near field

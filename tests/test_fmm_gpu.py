@@ -205,3 +205,27 @@ def test_plan_reused_while_the_box_drifts():
     idx = np.arange(0, b.n, 97)
     rx, ry = oracle.velocity_direct(x, y, b.g, 2 * b.sigma ** 2, x[idx], y[idx])
     assert normwise_err(vx[idx], vy[idx], rx, ry) <= TOL
+
+
+@pytest.mark.parametrize("terms", [16, 20, 24, 28, 32])
+@pytest.mark.parametrize("sigma", [0.002, 1e-5])
+def test_every_expansion_order_vs_oracle(terms, sigma):
+    """Every instantiated expansion order, forced through pf_fmm_set_tuning
+    (the tensor-core M2M, M2L and L2L pad their 8 x 4 tiles for 20 and 28
+    terms); sigma = 1e-5 is the point-vortex limit, where the far field
+    carries most of the velocity."""
+    from pfblob import _lib
+    rng = np.random.default_rng(7)
+    n = 30000
+    x, y = rng.random(n), rng.random(n)
+    g = rng.standard_normal(n) / n
+    _lib.fmm_set_tuning(0, terms, 1)
+    try:
+        vx, vy = fmm(x, y, g, sigma)
+        st = _lib.fmm_last_stats(DEV.index)
+    finally:
+        _lib.fmm_set_tuning(0, 0, 1)
+    assert st["expansion_terms"] == terms
+    sub = np.arange(0, n, 15)
+    rx, ry = oracle.velocity_direct(x, y, g, 2 * sigma * sigma, x[sub].copy(), y[sub].copy())
+    assert normwise_err(vx[sub], vy[sub], rx, ry) <= TOL

@@ -110,3 +110,31 @@ def test_graph_reports_window_beyond_its_bound():
     sg.launch()
     assert sg.result()[3] == 0
     sg.close()
+
+
+def test_direct_method_graph_equals_eager_step():
+    """The direct-sum step (method = PF_DIRECT_METHOD) captured and replayed:
+    bitwise the eager pf_blob_step, and within 1e-6 of the FP64 oracle."""
+    import pfblob
+    dev = torch.device("cuda", 0)
+    n = 6000
+    sigma = 0.01
+    ks, xopt, cut = pfblob.fmm_parameters(sigma, 2.0, tol=1e-6)
+    h = 0.8 * sigma
+    x, y, g = (torch.from_numpy(a).to(dev) for a in _set(n, 9))
+    sg = pfblob.StepGraph(x, y, g, ks, xopt, cut, 1e-6, (0.0, 1.0, 0.0, 1.0), h, -1.5 * h,
+                          -1.5 * h, method=pfblob.DIRECT_METHOD,
+                          max_base_cells=4 * int((1.0 / h + 8) ** 2))
+    sg.launch()
+    xo, yo, go, status = sg.result()
+    assert status == 0 and xo.numel() > 0
+    vx, vy, out, st_e, mom = _eager_step(sg, sg.out.shape[1])
+    assert st_e == 0
+    assert torch.equal(sg.vx, vx) and torch.equal(sg.vy, vy)
+    assert torch.equal(out[2], go)
+    xs, ys, gs = x.cpu().numpy(), y.cpu().numpy(), g.cpu().numpy()
+    ux, uy = oracle.velocity_direct(xs, ys, gs, ks)
+    gx, gy = sg.vx.cpu().numpy(), sg.vy.cpu().numpy()
+    err = np.sqrt(np.sum((gx - ux) ** 2 + (gy - uy) ** 2) / np.sum(ux ** 2 + uy ** 2))
+    assert err < 1e-6, err
+    sg.close()

@@ -129,6 +129,14 @@ struct WRec {
 };
 static_assert(sizeof(WRec) == 32, "WRec layout");
 
+// One 32-byte record written by a single 256-bit store (sm_100), so the
+// sector is written whole.
+__device__ __forceinline__ void st_rec(WRec *r, double a, double b, double c, double d) {
+    asm volatile("st.global.v4.b64 [%0], {%1, %2, %3, %4};" ::"l"(r), "d"(a), "d"(b), "d"(c),
+                 "d"(d)
+                 : "memory");
+}
+
 __device__ __forceinline__ int64_t left_index(double x, double b0, double h2, double h05,
                                               double h) {
     // ((x - b0) - 2h) + 0.5h, then / h, ceil, -1 ; each op rounded separately
@@ -602,9 +610,8 @@ k_rm_place(int64_t n, RmHead *hd, const int32_t *__restrict__ cell,
         const double xi = x[i], yi = y[i], gi = g[i];
         const double v1 = TUTTY ? xi : __ddiv_rn(xi, wp.h);
         const double v2 = TUTTY ? yi : __ddiv_rn(yi, wp.h);
-        double2 *d = reinterpret_cast<double2 *>(recs + p);
-        d[0] = make_double2(v1, v2);
-        d[1] = make_double2(gi, __longlong_as_double((long long)i));
+        // the whole 32-byte sector in one store (records are 32-byte aligned)
+        st_rec(recs + p, v1, v2, gi, __longlong_as_double((long long)i));
         add_moments(m, xi, yi, gi);
         // a cell of more than SEG_SMALL blobs (exactly one has this rank) is
         // listed for the segment sort

@@ -21,6 +21,9 @@
 // (reference counterparts: mpexp_init fmm.cpp:1452-1509, shift_m2m
 // fmmshift.cpp:80-236, shift_m2ps fmmshift.cpp:237-621, shift_p2p
 // fmmshift.cpp:622-767, mpexp_eval fmm.cpp:1875-1931).
+// M2M, M2L and L2L run on the FP64 tensor cores (mma.sync m8n8k4 .f64):
+// their operators are fixed matrices (per child position, or the binomial
+// matrix between the scalings by rho), applied to four boxes per warp task.
 //
 // Near field: the Gaussian kernel itself, FP32 with hi/lo coordinates and
 // compensated accumulation (gauss_pair.cuh), for every target of a P2P block

@@ -952,21 +952,6 @@ __device__ __noinline__ float2 p2p_split_sums(uint32_t a_hi, uint32_t a_lo, uint
     return make_float2(px, py);
 }
 
-// Drop the first 32 entries of a source buffer holding 32 + rest: entries
-// [32, 32 + rest) move to [0, rest) (rest < 32).
-__device__ __forceinline__ void p2p_buf_shift(ulonglong2 *__restrict__ shi,
-                                              ulonglong2 *__restrict__ slo,
-                                              unsigned long long *__restrict__ sg2, int rest,
-                                              int lane) {
-    __syncwarp();
-    if (lane < rest) {
-        shi[lane] = shi[32 + lane];
-        slo[lane] = slo[32 + lane];
-        sg2[lane] = sg2[32 + lane];
-    }
-    __syncwarp();
-}
-
 // p2p_chunk for the group's targets-per-lane count nt (warp-uniform).
 // nt = 3: targets a, b packed plus the lane's share (qs of msp) of a
 // remainder target c.
@@ -1056,7 +1041,11 @@ __device__ __forceinline__ void p2p_group_body(
     // centre for the far sources' relative coordinates (any float near the group)
     const float cx = 0.5f * (bx0 + bx1), cy = 0.5f * (by0 + by1);
     float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    int c0 = 0, c1 = 0, c2 = 0;  // entries waiting in the three buffers
+    // the three buffers are rings of P2P_BUF = 64 entries: entries waiting
+    // c0, c1, c2 from heads h0, h1, h2; a chunk is always the 32 entries at
+    // the head (0 or 32), so it never wraps, and taking it flips the head
+    int c0 = 0, c1 = 0, c2 = 0;
+    int h0 = 0, h1 = 0, h2 = 0;
     for (int rc = r0; rc < r1; rc += P2P_RUNS_SM) {
         const int nrc = min(P2P_RUNS_SM, r1 - rc);
         int pre = 0;
@@ -1118,7 +1107,9 @@ __device__ __forceinline__ void p2p_group_body(
             const unsigned m2 = __ballot_sync(0xffffffffu, cls == 2);
             if (cls >= 0) {
                 const unsigned mm = cls == 0 ? m0 : cls == 1 ? m1 : m2;
-                const int k = (cls == 0 ? c0 : cls == 1 ? c1 : c2) + __popc(mm & lt);
+                const int k =
+                    ((cls == 0 ? h0 + c0 : cls == 1 ? h1 + c1 : h2 + c2) + __popc(mm & lt)) &
+                    (P2P_BUF - 1);
                 if (cls == 0) {  // far: coordinates relative to the group centre
                     const float lx = (spv.x - cx) + spv.z, ly = (spv.y - cy) + spv.w;
                     s_hi[0][k] = make_ulonglong2(pfd::pack2(lx, lx), pfd::pack2(ly, ly));
@@ -1137,38 +1128,44 @@ __device__ __forceinline__ void p2p_group_body(
             gg = 0.f;
             fetch(p + 32, spv, gg);
             __syncwarp();
+            bool ran = false;  // warp-uniform
             if (c0 >= 32) {
-                p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], 32, ta, tb, tc,
-                                       qs, msp, cx, cy, gp, acc);
+                p2p_run_chunk<P2P_FAR>(nt, s_hi[0] + h0, s_lo[0] + h0, s_g2[0] + h0, 32, ta, tb,
+                                       tc, qs, msp, cx, cy, gp, acc);
                 nfar += 32ull * (unsigned long long)gsz;
                 c0 -= 32;
-                p2p_buf_shift(s_hi[0], s_lo[0], s_g2[0], c0, lane);
+                h0 ^= 32;
+                ran = true;
             }
             if (c1 >= 32) {
-                p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], 32, ta, tb, tc,
-                                        qs, msp, cx, cy, gp, acc);
+                p2p_run_chunk<P2P_FULL>(nt, s_hi[1] + h1, s_lo[1] + h1, s_g2[1] + h1, 32, ta,
+                                        tb, tc, qs, msp, cx, cy, gp, acc);
                 c1 -= 32;
-                p2p_buf_shift(s_hi[1], s_lo[1], s_g2[1], c1, lane);
+                h1 ^= 32;
+                ran = true;
             }
             if (c2 >= 32) {
-                p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], 32, ta, tb, tc,
-                                          qs, msp, cx, cy, gp, acc);
+                p2p_run_chunk<P2P_SERIES>(nt, s_hi[2] + h2, s_lo[2] + h2, s_g2[2] + h2, 32, ta,
+                                          tb, tc, qs, msp, cx, cy, gp, acc);
                 c2 -= 32;
-                p2p_buf_shift(s_hi[2], s_lo[2], s_g2[2], c2, lane);
+                h2 ^= 32;
+                ran = true;
             }
+            if (ran) __syncwarp();  // the chunks are read before the next round refills them
         }
     }
     // what is left in the buffers (fewer than 32 each)
+    // (fewer than 32 from a head of 0 or 32: no wrap)
     if (c0)
-        p2p_run_chunk<P2P_FAR>(nt, s_hi[0], s_lo[0], s_g2[0], c0, ta, tb, tc,
+        p2p_run_chunk<P2P_FAR>(nt, s_hi[0] + h0, s_lo[0] + h0, s_g2[0] + h0, c0, ta, tb, tc,
                                qs, msp, cx, cy, gp, acc);
     nfar += (unsigned long long)c0 * (unsigned long long)gsz;
     if (c1)
-        p2p_run_chunk<P2P_FULL>(nt, s_hi[1], s_lo[1], s_g2[1], c1, ta, tb, tc,
+        p2p_run_chunk<P2P_FULL>(nt, s_hi[1] + h1, s_lo[1] + h1, s_g2[1] + h1, c1, ta, tb, tc,
                                 qs, msp, cx, cy, gp, acc);
     if (c2)
-        p2p_run_chunk<P2P_SERIES>(nt, s_hi[2], s_lo[2], s_g2[2], c2, ta, tb, tc,
-                                  qs, msp, cx, cy, gp, acc);
+        p2p_run_chunk<P2P_SERIES>(nt, s_hi[2] + h2, s_lo[2] + h2, s_g2[2] + h2, c2, ta, tb,
+                                  tc, qs, msp, cx, cy, gp, acc);
     __syncwarp();
     if (lane < gsz)
         nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),

@@ -912,7 +912,7 @@ __device__ __forceinline__ void p2p_chunk(const ulonglong2 *shi, const ulonglong
                                           const unsigned long long *sg2, int cnt,
                                           const float4 &ta, const float4 &tb, const float4 &tc,
                                           float cx, float cy, const pfd::GaussParams &gp,
-                                          float (&acc)[12]) {
+                                          float (&acc)[16]) {
     const P2PSums r = p2p_chunk_sums<NT, MODE>(
         (uint32_t)__cvta_generic_to_shared(shi), (uint32_t)__cvta_generic_to_shared(slo),
         (uint32_t)__cvta_generic_to_shared(sg2), cnt, ta, tb, tc, cx, cy, gp);
@@ -929,50 +929,61 @@ __device__ __forceinline__ void p2p_chunk(const ulonglong2 *shi, const ulonglong
 }
 
 // The third target slot of a group of 65..96 targets: the rem = size - 64
-// remainder targets are spread over the warp, m = 32 / rem lanes per target,
-// lane (j + rem q) taking sources q, q + m, q + 2m, ... of the chunk for
-// target j; the m partial sums are combined at the end of the group.  Lanes
-// with no share get q >= 32.
+// remainder targets are paired (c, d) into rp = ceil(rem / 2) packed pairs
+// spread over the warp, m = 32 / rp lanes per pair, lane (j + rp q) taking
+// sources q, q + m, q + 2m, ... of the chunk for pair j with the packed pair
+// code of the main slots; the m partial sums are combined at the end of the
+// group.  Lanes with no share get q >= 32.  Returns -nx_c, ny_c, -nx_d, ny_d.
 template <int MODE>
-__device__ __noinline__ float2 p2p_split_sums(uint32_t a_hi, uint32_t a_lo, uint32_t a_g, int cnt,
-                                              int q, int m, float4 tc, float cx, float cy,
-                                              pfd::GaussParams gp) {
-    float px = 0.f, py = 0.f;
+__device__ __noinline__ float4 p2p_split_sums(uint32_t a_hi, uint32_t a_lo, uint32_t a_g, int cnt,
+                                              int q, int m, float4 tc, float4 td, float cx,
+                                              float cy, pfd::GaussParams gp) {
+    const pfd::GaussParams2 gp2 = pfd::make_params2(gp);
+    pfd::f32x2 nx = 0ull, ny = 0ull;
     if constexpr (MODE == P2P_FAR) {
-        const float tx = (tc.x - cx) + tc.z, ty = (tc.y - cy) + tc.w;
+        const pfd::f32x2 txc = pfd::pack2((tc.x - cx) + tc.z, (td.x - cx) + td.z);
+        const pfd::f32x2 tyc = pfd::pack2((tc.y - cy) + tc.w, (td.y - cy) + td.w);
 #pragma unroll 2
         for (int k = q; k < cnt; k += m)
-            far_local_scalar(lds_u64x2(a_hi + 16 * k), lds_u64(a_g + 8 * k), tx, ty, px, py);
+            pfd::pair2_far_local(lds_u64x2(a_hi + 16 * k), lds_u64(a_g + 8 * k), txc, tyc, gp2, nx,
+                                 ny);
     } else {
+        const pfd::f32x2 txh = pfd::pack2(tc.x, td.x), tyh = pfd::pack2(tc.y, td.y);
+        const pfd::f32x2 txl = pfd::pack2(tc.z, td.z), tyl = pfd::pack2(tc.w, td.w);
 #pragma unroll 2
         for (int k = q; k < cnt; k += m)
-            scalar_pair<MODE>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k),
-                              lds_u64(a_g + 8 * k), tc, gp, px, py);
+            pfd::pair2<MODE == P2P_SERIES>(lds_u64x2(a_hi + 16 * k), lds_u64x2(a_lo + 16 * k),
+                                            lds_u64(a_g + 8 * k), txh, tyh, txl, tyl, gp2, nx, ny);
     }
-    return make_float2(px, py);
+    float nxc, nxd, nyc, nyd;
+    pfd::unpack2(nx, nxc, nxd);
+    pfd::unpack2(ny, nyc, nyd);
+    return make_float4(-nxc, nyc, -nxd, nyd);
 }
 
 // p2p_chunk for the group's targets-per-lane count nt (warp-uniform).
 // nt = 3: targets a, b packed plus the lane's share (qs of msp) of a
-// remainder target c.
+// remainder target pair (c, d).
 template <int MODE>
 __device__ __forceinline__ void p2p_run_chunk(int nt, const ulonglong2 *shi, const ulonglong2 *slo,
                                               const unsigned long long *sg2, int cnt,
                                               const float4 &ta, const float4 &tb,
-                                              const float4 &tc, int qs, int msp, float cx,
-                                              float cy, const pfd::GaussParams &gp,
-                                              float (&acc)[12]) {
+                                              const float4 &tc, const float4 &td, int qs,
+                                              int msp, float cx, float cy,
+                                              const pfd::GaussParams &gp, float (&acc)[16]) {
     if (nt == 1) {
         p2p_chunk<1, MODE>(shi, slo, sg2, cnt, ta, tb, tc, cx, cy, gp, acc);
         return;
     }
     p2p_chunk<2, MODE>(shi, slo, sg2, cnt, ta, tb, tc, cx, cy, gp, acc);
     if (nt == 3) {
-        const float2 r = p2p_split_sums<MODE>(
+        const float4 r = p2p_split_sums<MODE>(
             (uint32_t)__cvta_generic_to_shared(shi), (uint32_t)__cvta_generic_to_shared(slo),
-            (uint32_t)__cvta_generic_to_shared(sg2), cnt, qs, msp, tc, cx, cy, gp);
+            (uint32_t)__cvta_generic_to_shared(sg2), cnt, qs, msp, tc, td, cx, cy, gp);
         pfd::comp_add(acc[8], acc[9], r.x);
         pfd::comp_add(acc[10], acc[11], r.y);
+        pfd::comp_add(acc[12], acc[13], r.z);
+        pfd::comp_add(acc[14], acc[15], r.w);
     }
 }
 
@@ -1010,22 +1021,26 @@ __device__ __forceinline__ void p2p_group_body(
     const int tg = (int)((int64_t)gi * tn / ngrp);
     const int gsz = (int)((int64_t)(gi + 1) * tn / ngrp) - tg;
     const int nt = (gsz <= 32) ? 1 : (gsz <= 64) ? 2 : 3;  // warp-uniform
-    // nt = 3: remainder targets tg + 64 + j, j < rem, each on msp lanes
+    // nt = 3: remainder targets tg + 64 + j, j < rem, in rp packed pairs
+    // (tg + 64 + 2 p, + 1), each pair on msp lanes
     const int rem = nt == 3 ? gsz - 64 : 32;
-    const int msp = 32 / rem;
-    const bool cval = nt == 3 && lane < rem * msp;
-    const int qs = cval ? lane / rem : 32;
-    const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + lane % rem;
+    const int rp = (rem + 1) / 2;
+    const int msp = 32 / rp;
+    const bool cval = nt == 3 && lane < rp * msp;
+    const int qs = cval ? lane / rp : 32;
+    const int ia = tg + lane, ib = tg + 32 + lane, ic = tg + 64 + 2 * (lane % rp), id = ic + 1;
+    const bool dval = cval && id < tg + gsz;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     if (!PF_IDX_OK((int64_t)t0 + tg + gsz - 1, nt_all, 204)) return;  // the group's last target
     const float4 ta = (lane < gsz) ? thl[t0 + ia] : z4;
     const float4 tb = (lane + 32 < gsz) ? thl[t0 + ib] : z4;
     const float4 tc = cval ? thl[t0 + ic] : z4;
+    const float4 td = dval ? thl[t0 + id] : tc;  // an odd remainder's last pair repeats c
     // box of the group's targets (hi parts), for the series-free test
     float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
     if (lane < gsz) { bx0 = bx1 = ta.x; by0 = by1 = ta.y; }
     if (lane + 32 < gsz) { bx0 = fminf(bx0, tb.x); bx1 = fmaxf(bx1, tb.x); by0 = fminf(by0, tb.y); by1 = fmaxf(by1, tb.y); }
-    if (cval) { bx0 = fminf(bx0, tc.x); bx1 = fmaxf(bx1, tc.x); by0 = fminf(by0, tc.y); by1 = fmaxf(by1, tc.y); }
+    if (cval) { bx0 = fminf(bx0, fminf(tc.x, td.x)); bx1 = fmaxf(bx1, fmaxf(tc.x, td.x)); by0 = fminf(by0, fminf(tc.y, td.y)); by1 = fmaxf(by1, fmaxf(tc.y, td.y)); }
     bx0 = warp_min(bx0);
     bx1 = warp_max(bx1);
     by0 = warp_min(by0);
@@ -1040,7 +1055,8 @@ __device__ __forceinline__ void p2p_group_body(
     const float reachf2 = reachf * reachf;
     // centre for the far sources' relative coordinates (any float near the group)
     const float cx = 0.5f * (bx0 + bx1), cy = 0.5f * (by0 + by1);
-    float acc[12] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float acc[16] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f,
+                     0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     // the three buffers are rings of P2P_BUF = 64 entries: entries waiting
     // c0, c1, c2 from heads h0, h1, h2; a chunk is always the 32 entries at
     // the head (0 or 32), so it never wraps, and taking it flips the head
@@ -1131,7 +1147,7 @@ __device__ __forceinline__ void p2p_group_body(
             bool ran = false;  // warp-uniform
             if (c0 >= 32) {
                 p2p_run_chunk<P2P_FAR>(nt, s_hi[0] + h0, s_lo[0] + h0, s_g2[0] + h0, 32, ta, tb,
-                                       tc, qs, msp, cx, cy, gp, acc);
+                                       tc, td, qs, msp, cx, cy, gp, acc);
                 nfar += 32ull * (unsigned long long)gsz;
                 c0 -= 32;
                 h0 ^= 32;
@@ -1139,14 +1155,14 @@ __device__ __forceinline__ void p2p_group_body(
             }
             if (c1 >= 32) {
                 p2p_run_chunk<P2P_FULL>(nt, s_hi[1] + h1, s_lo[1] + h1, s_g2[1] + h1, 32, ta,
-                                        tb, tc, qs, msp, cx, cy, gp, acc);
+                                        tb, tc, td, qs, msp, cx, cy, gp, acc);
                 c1 -= 32;
                 h1 ^= 32;
                 ran = true;
             }
             if (c2 >= 32) {
                 p2p_run_chunk<P2P_SERIES>(nt, s_hi[2] + h2, s_lo[2] + h2, s_g2[2] + h2, 32, ta,
-                                          tb, tc, qs, msp, cx, cy, gp, acc);
+                                          tb, tc, td, qs, msp, cx, cy, gp, acc);
                 c2 -= 32;
                 h2 ^= 32;
                 ran = true;
@@ -1158,14 +1174,14 @@ __device__ __forceinline__ void p2p_group_body(
     // (fewer than 32 from a head of 0 or 32: no wrap)
     if (c0)
         p2p_run_chunk<P2P_FAR>(nt, s_hi[0] + h0, s_lo[0] + h0, s_g2[0] + h0, c0, ta, tb, tc,
-                               qs, msp, cx, cy, gp, acc);
+                               td, qs, msp, cx, cy, gp, acc);
     nfar += (unsigned long long)c0 * (unsigned long long)gsz;
     if (c1)
         p2p_run_chunk<P2P_FULL>(nt, s_hi[1] + h1, s_lo[1] + h1, s_g2[1] + h1, c1, ta, tb, tc,
-                                qs, msp, cx, cy, gp, acc);
+                                td, qs, msp, cx, cy, gp, acc);
     if (c2)
         p2p_run_chunk<P2P_SERIES>(nt, s_hi[2] + h2, s_lo[2] + h2, s_g2[2] + h2, c2, ta, tb,
-                                  tc, qs, msp, cx, cy, gp, acc);
+                                  tc, td, qs, msp, cx, cy, gp, acc);
     __syncwarp();
     if (lane < gsz)
         nearv[t0 + ia] = make_double2(INV_2PI * ((double)acc[0] + (double)acc[1]),
@@ -1173,22 +1189,26 @@ __device__ __forceinline__ void p2p_group_body(
     if (lane + 32 < gsz)
         nearv[t0 + ib] = make_double2(INV_2PI * ((double)acc[4] + (double)acc[5]),
                                       INV_2PI * ((double)acc[6] + (double)acc[7]));
-    if (nt == 3) {  // combine the msp shares of each remainder target, in lane order
-        float h0 = acc[8], l0 = acc[9], h1 = acc[10], l1 = acc[11];
+    if (nt == 3) {  // combine the msp shares of each remainder pair, in lane order
+        float h[4] = {acc[8], acc[10], acc[12], acc[14]};
+        float l[4] = {acc[9], acc[11], acc[13], acc[15]};
         for (int q = 1; q < msp; ++q) {
-            const int sl = lane % rem + rem * q;  // < rem * msp <= 32
-            const float a = __shfl_sync(0xffffffffu, acc[8], sl);
-            const float b = __shfl_sync(0xffffffffu, acc[9], sl);
-            const float c = __shfl_sync(0xffffffffu, acc[10], sl);
-            const float d = __shfl_sync(0xffffffffu, acc[11], sl);
-            pfd::comp_add(h0, l0, a);
-            l0 += b;
-            pfd::comp_add(h1, l1, c);
-            l1 += d;
+            const int sl = lane % rp + rp * q;  // < rp * msp <= 32
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const float a = __shfl_sync(0xffffffffu, acc[8 + 2 * v], sl);
+                const float b = __shfl_sync(0xffffffffu, acc[9 + 2 * v], sl);
+                pfd::comp_add(h[v], l[v], a);
+                l[v] += b;
+            }
         }
-        if (lane < rem)
-            nearv[t0 + ic] = make_double2(INV_2PI * ((double)h0 + (double)l0),
-                                          INV_2PI * ((double)h1 + (double)l1));
+        if (lane < rp) {
+            nearv[t0 + ic] = make_double2(INV_2PI * ((double)h[0] + (double)l[0]),
+                                          INV_2PI * ((double)h[1] + (double)l[1]));
+            if (dval)
+                nearv[t0 + id] = make_double2(INV_2PI * ((double)h[2] + (double)l[2]),
+                                              INV_2PI * ((double)h[3] + (double)l[3]));
+        }
     }
 }
 

@@ -63,7 +63,7 @@ constexpr int P2P_BUF = 64;      // sources per warp buffer (three buffers)
 // unroll of the pair loop over a full chunk: the kernel holds nine copies of
 // it (targets per lane x mode), which must stay within the instruction cache
 constexpr int P2P_UNROLL = 8;
-constexpr int P2P_MIN_CTAS = 24; // one-warp CTAs resident per SM (shared memory bound)
+constexpr int P2P_MIN_CTAS = 20; // one-warp CTAs resident per SM: 96 registers each
 constexpr unsigned INVALID_KEY = 0xFFFFFFFFu;
 
 // ---------------------------------------------------------------------------

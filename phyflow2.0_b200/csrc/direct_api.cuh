@@ -21,7 +21,7 @@ struct DirectInstance {
 // tiles are fewer than DT_SPLIT_CTAS, into at most DT_SPLIT_MAX segments of
 // at least DT_SPLIT_MIN_SRC sources (a multiple of the 256-blob load tile).
 constexpr int64_t DT_SPLIT_CTAS = 1184;  // 8 CTAs on each of 148 SMs
-constexpr int64_t DT_SPLIT_MIN_SRC = 1024;
+constexpr int64_t DT_SPLIT_MIN_SRC = 256;
 constexpr int64_t DT_SPLIT_MAX = 64;
 struct DirectSplit {
     int splits;

@@ -152,27 +152,39 @@ k_panel_groups(int64_t m, const double *__restrict__ gamma, const double *__rest
     const double inv = R > 0.0 ? 1.0 / R : 0.0;
     const double ar = (x1 - cx) * inv, ai = (y1 - cy) * inv;
     const double br = (x2e - cx) * inv, bi = (y2e - cy) * inv;
-    const int k = lane + 1;
-    double sr = 0.0, si = 0.0;
-    for (int j = 0; j < cnt; ++j) {
-        const double jar = __shfl_sync(0xffffffffu, ar, j), jai = __shfl_sync(0xffffffffu, ai, j);
-        const double jbr = __shfl_sync(0xffffffffu, br, j), jbi = __shfl_sync(0xffffffffu, bi, j);
-        const double jkr = __shfl_sync(0xffffffffu, kr, j), jki = __shfl_sync(0xffffffffu, ki, j);
-        double pr = 1.0, pi = 0.0, qr = 1.0, qi = 0.0;  // a^k, b^k
-        for (int e = 0; e < k && k <= PC_P; ++e) {
-            const double t1 = pr * jar - pi * jai;
-            pi = pr * jai + pi * jar;
-            pr = t1;
-            const double t2 = qr * jbr - qi * jbi;
-            qi = qr * jbi + qi * jbr;
-            qr = t2;
-        }
-        const double dr = pr - qr, di = pi - qi;
-        sr += jkr * dr - jki * di;
-        si += jkr * di + jki * dr;
+    // the group's scaled end points and strengths, for every lane's terms
+    __shared__ double s_e[6][PC_G];
+    if (has) {
+        s_e[0][lane] = ar;
+        s_e[1][lane] = ai;
+        s_e[2][lane] = br;
+        s_e[3][lane] = bi;
+        s_e[4][lane] = kr;
+        s_e[5][lane] = ki;
     }
+    __syncwarp();
     PanelGroup *gp = groups + blockIdx.x;
-    if (k <= PC_P) gp->a[lane] = make_double2(sr / k, si / k);
+    // terms k = lane + 1 and lane + 33 (PC_P > 32 of them)
+    for (int k = lane + 1; k <= PC_P; k += 32) {
+        double sr = 0.0, si = 0.0;
+        for (int j = 0; j < cnt; ++j) {
+            const double jar = s_e[0][j], jai = s_e[1][j], jbr = s_e[2][j], jbi = s_e[3][j];
+            const double jkr = s_e[4][j], jki = s_e[5][j];
+            double pr = 1.0, pi = 0.0, qr = 1.0, qi = 0.0;  // a^k, b^k
+            for (int e = 0; e < k; ++e) {
+                const double t1 = pr * jar - pi * jai;
+                pi = pr * jai + pi * jar;
+                pr = t1;
+                const double t2 = qr * jbr - qi * jbi;
+                qi = qr * jbi + qi * jbr;
+                qr = t2;
+            }
+            const double dr = pr - qr, di = pi - qi;
+            sr += jkr * dr - jki * di;
+            si += jkr * di + jki * dr;
+        }
+        gp->a[k - 1] = make_double2(sr / k, si / k);
+    }
     if (lane == 0) {
         gp->cx = cx;
         gp->cy = cy;
@@ -262,6 +274,245 @@ k_panel_velocity(int64_t ngroups, const PanelGroup *__restrict__ groups,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Large point sets: the far groups through local expansions on a box grid.
+// The points' bounding square is cut into PL_NB x PL_NB boxes.  For box b
+// (centre zb, radius rb = half its diagonal) a group (c, R) is far when
+// |zb - c| >= max(2R + rb, R + 2rb): then every point z of the box has
+// R / |z - c| <= 1/2, inside the range where the group's series is summed to
+// its stated remainder, and the series' expansion about zb converges with
+// ratio |z - zb| / (|zb - c| - R) <= 1/2.  With D = zb - c and u = (z - zb)/rb,
+//   sum_k A_k (R / (z - c))^k = sum_n L_n u^n,
+//   L_n = (-rb / D)^n sum_{k>=1} C(n+k-1, n) A_k (R / D)^k,
+// and PL_P = 40 terms leave 2^-40 of the group's share.  The box keeps the sum
+// of its far groups' L_n and a bit mask of its near groups, which its points
+// evaluate as before (series or the pair formula).
+constexpr int PL_NB = 64;         // boxes per side of the grid
+constexpr int PL_P = 40;          // local expansion terms
+constexpr int64_t PL_MIN_POINTS = 32768;  // below: every group per point
+constexpr int PL_MIN_GROUPS = 8;
+
+struct PanelGrid {
+    double x0, y0, wb;  // grid origin and box width
+    unsigned long long mn[2], mx[2];  // ordered images of the points' min, max
+};
+
+__device__ __forceinline__ unsigned long long pl_ord(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double pl_unord(unsigned long long o) {
+    const unsigned long long b = (o & 0x8000000000000000ull) ? (o & 0x7fffffffffffffffull) : ~o;
+    return __longlong_as_double((long long)b);
+}
+
+__global__ void k_panel_grid_init(PanelGrid *gd) {
+    gd->mn[0] = gd->mn[1] = ~0ull;
+    gd->mx[0] = gd->mx[1] = 0ull;
+}
+
+// min / max of the point coordinates (order-preserving integer images)
+__global__ void __launch_bounds__(PN_THREADS)
+k_panel_bbox(int64_t n, const double *__restrict__ xv, const double *__restrict__ yv,
+             PanelGrid *gd) {
+    unsigned long long mnx = ~0ull, mny = ~0ull, mxx = 0ull, mxy = 0ull;
+    for (int64_t i = (int64_t)blockIdx.x * PN_THREADS + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * PN_THREADS) {
+        const unsigned long long ox = pl_ord(xv[i]), oy = pl_ord(yv[i]);
+        mnx = min(mnx, ox);
+        mxx = max(mxx, ox);
+        mny = min(mny, oy);
+        mxy = max(mxy, oy);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mnx = min(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+        mxx = max(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+        mny = min(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+        mxy = max(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&gd->mn[0], mnx);
+        atomicMax(&gd->mx[0], mxx);
+        atomicMin(&gd->mn[1], mny);
+        atomicMax(&gd->mx[1], mxy);
+    }
+}
+
+__global__ void k_panel_grid_set(PanelGrid *gd) {
+    const double x0 = pl_unord(gd->mn[0]), x1 = pl_unord(gd->mx[0]);
+    const double y0 = pl_unord(gd->mn[1]), y1 = pl_unord(gd->mx[1]);
+    double e = fmax(x1 - x0, y1 - y0);
+    // non-finite coordinates give no usable grid: one box holding everything
+    // would be near every group, i.e. the per-point path
+    if (!(e > 0.0) || !isfinite(e)) e = 1.0;
+    gd->x0 = isfinite(x0) ? x0 : 0.0;
+    gd->y0 = isfinite(y0) ? y0 : 0.0;
+    gd->wb = e * (1.0 + 1e-9) / PL_NB;
+}
+
+// One warp per box: the near-group mask (mwords words) and the local
+// expansion of the far groups' series (lane n holds L_n and L_{n+32}).
+__global__ void __launch_bounds__(128)
+k_panel_locals(int64_t ngroups, const PanelGroup *__restrict__ groups, const PanelGrid *gd,
+               int mwords, double2 *__restrict__ locals, unsigned *__restrict__ masks) {
+    __shared__ double s_bin[PL_P][PC_P];  // C(n + k - 1, n), k = 1 .. PC_P
+    __shared__ double2 s_beta[4][PC_P];   // per warp: A_k (R / D)^k
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int nn = threadIdx.x; nn < PL_P; nn += blockDim.x) {
+        double c = 1.0;  // C(n, n)
+        for (int k = 1; k <= PC_P; ++k) {
+            s_bin[nn][k - 1] = c;
+            c = c * (double)(nn + k) / (double)k;  // C(n + k, n)
+        }
+    }
+    __syncthreads();
+    const int box = blockIdx.x * 4 + wid;
+    if (box >= PL_NB * PL_NB) return;  // the whole warp
+    const int bx = box / PL_NB, by = box - bx * PL_NB;
+    const double wb = gd->wb;
+    const double zbx = gd->x0 + ((double)bx + 0.5) * wb, zby = gd->y0 + ((double)by + 0.5) * wb;
+    const double rb = 0.70710678118654757 * wb;
+    double2 l0 = make_double2(0.0, 0.0), l1 = make_double2(0.0, 0.0);  // L_lane, L_lane+32
+    for (int w = 0; w < mwords; ++w) {
+        const int64_t g = (int64_t)w * 32 + lane;
+        bool near = false;
+        if (g < ngroups) {
+            const double dx = zbx - groups[g].cx, dy = zby - groups[g].cy;
+            const double R = groups[g].R;
+            const double d = sqrt(dx * dx + dy * dy);
+            near = !(d >= fmax(2.0 * R + rb, R + 2.0 * rb) * 1.0000001);
+        }
+        const unsigned nm = __ballot_sync(0xffffffffu, near);
+        const unsigned valid = __ballot_sync(0xffffffffu, g < ngroups);
+        if (lane == 0) masks[(int64_t)box * mwords + w] = nm;
+        unsigned far = valid & ~nm;
+        while (far) {
+            const int j = __ffs(far) - 1;
+            far &= far - 1;
+            const PanelGroup &G = groups[(int64_t)w * 32 + j];
+            const double dx = zbx - G.cx, dy = zby - G.cy;
+            const double inv = 1.0 / (dx * dx + dy * dy);
+            const double rr = dx * inv, ri = -dy * inv;  // 1 / D
+            // beta_k = A_k (R / D)^k, k = lane + 1 (and lane + 33)
+            for (int k = lane + 1; k <= PC_P; k += 32) {
+                double pr = 1.0, pi = 0.0, br = G.R * rr, bi = G.R * ri;
+                for (int e = k; e; e >>= 1) {  // (R / D)^k by squaring
+                    if (e & 1) {
+                        const double t = pr * br - pi * bi;
+                        pi = pr * bi + pi * br;
+                        pr = t;
+                    }
+                    const double t = br * br - bi * bi;
+                    bi = 2.0 * br * bi;
+                    br = t;
+                }
+                const double2 a = G.a[k - 1];
+                s_beta[wid][k - 1] = make_double2(a.x * pr - a.y * pi, a.x * pi + a.y * pr);
+            }
+            __syncwarp();
+            // L_n += (-rb / D)^n sum_k C(n + k - 1, n) beta_k
+            for (int n = lane, h = 0; n < PL_P; n += 32, ++h) {
+                double sr = 0.0, si = 0.0;
+                for (int k = 0; k < PC_P; ++k) {
+                    const double c = s_bin[n][k];
+                    sr = fma(c, s_beta[wid][k].x, sr);
+                    si = fma(c, s_beta[wid][k].y, si);
+                }
+                double pr = 1.0, pi = 0.0, br = -rb * rr, bi = -rb * ri;  // (-rb / D)^n
+                for (int e = n; e; e >>= 1) {
+                    if (e & 1) {
+                        const double t = pr * br - pi * bi;
+                        pi = pr * bi + pi * br;
+                        pr = t;
+                    }
+                    const double t = br * br - bi * bi;
+                    bi = 2.0 * br * bi;
+                    br = t;
+                }
+                const double vr = sr * pr - si * pi, vi = sr * pi + si * pr;
+                if (h == 0) l0 = make_double2(l0.x + vr, l0.y + vi);
+                else l1 = make_double2(l1.x + vr, l1.y + vi);
+            }
+            __syncwarp();  // s_beta is read before the next group refills it
+        }
+    }
+    double2 *L = locals + (int64_t)box * PL_P;
+    L[lane] = l0;
+    if (lane + 32 < PL_P) L[lane + 32] = l1;
+}
+
+// Velocity at the points through the box grid: the box's local expansion
+// (its far groups), then its near groups one by one as k_panel_velocity does.
+template <bool SOURCE>
+__global__ void __launch_bounds__(PN_THREADS)
+k_panel_velocity_boxed(int64_t ngroups, const PanelGroup *__restrict__ groups,
+                       const PanelSm *__restrict__ pan, int64_t m, int64_t n,
+                       const double *__restrict__ xv, const double *__restrict__ yv,
+                       double *__restrict__ vx, double *__restrict__ vy, int accumulate,
+                       float log2_tol, const PanelGrid *gd, int mwords,
+                       const double2 *__restrict__ locals, const unsigned *__restrict__ masks) {
+    const double x0 = gd->x0, y0 = gd->y0, wb = gd->wb;
+    const double rb = 0.70710678118654757 * wb, irb = 1.0 / rb;
+    for (int64_t i = (int64_t)blockIdx.x * PN_THREADS + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * PN_THREADS) {
+        const double px = xv[i], py = yv[i];
+        const int bx = min(max((int)floor((px - x0) / wb), 0), PL_NB - 1);
+        const int by = min(max((int)floor((py - y0) / wb), 0), PL_NB - 1);
+        const int box = bx * PL_NB + by;
+        // the far groups: sum_n L_n u^n, u = (z - zb) / rb
+        const double ur = (px - (x0 + ((double)bx + 0.5) * wb)) * irb;
+        const double ui = (py - (y0 + ((double)by + 0.5) * wb)) * irb;
+        const double2 *L = locals + (int64_t)box * PL_P;
+        double wr = 0.0, wi = 0.0;
+#pragma unroll 4
+        for (int k = PL_P - 1; k >= 0; --k) {
+            const double2 a = L[k];
+            const double tr = fma(ur, wr, fma(-ui, wi, a.x));
+            wi = fma(ur, wi, fma(ui, wr, a.y));
+            wr = tr;
+        }
+        double ax = wr, ay = -wi;
+        // the near groups
+        for (int w = 0; w < mwords; ++w) {
+            unsigned nm = masks[(int64_t)box * mwords + w];
+            while (nm) {
+                const int j = __ffs(nm) - 1;
+                nm &= nm - 1;
+                const int64_t g = (int64_t)w * 32 + j;
+                const PanelGroup &G = groups[g];
+                const double dx = px - G.cx, dy = py - G.cy;
+                const double r2 = dx * dx + dy * dy;
+                if (r2 < G.far_r2) {
+                    const int j1 = (int)min((int64_t)PC_G, m - g * PC_G);
+                    for (int q = 0; q < j1; ++q) pair_velocity<SOURCE>(pan[g * PC_G + q], px, py, ax, ay);
+                } else {
+                    const double R = G.R;
+                    const double q = R / r2;
+                    const double sr = dx * q, si = -dy * q;  // s = R / (z - c)
+                    const float lr = 0.5f * __log2f((float)(R * q));
+                    const int P = max(1, min(PC_P, (int)ceilf(log2_tol / lr)));
+                    double tr0 = 0.0, ti0 = 0.0;
+                    for (int k = P - 1; k >= 0; --k) {
+                        const double2 a = G.a[k];
+                        const double t = fma(sr, tr0, fma(-si, ti0, a.x));
+                        ti0 = fma(sr, ti0, fma(si, tr0, a.y));
+                        tr0 = t;
+                    }
+                    ax += sr * tr0 - si * ti0;
+                    ay -= sr * ti0 + si * tr0;
+                }
+            }
+        }
+        if (accumulate) {
+            ax += vx[i];
+            ay += vy[i];
+        }
+        vx[i] = ax;
+        vy[i] = ay;
+    }
+}
+
 // Influence matrix of the panels on their collocation points
 // (_vortexPanel_Cython_cpu.pyx:217-234, all in FP64 as there): A[i][j] =
 // velocity induced at collocation point i by panel j at unit strength,
@@ -342,10 +593,27 @@ static pf_status panel_velocity(pf_ctx *ctx, const char *name, int64_t m, const 
     const int64_t ngroups = pf::ceil_div(m, PC_G);
     const size_t gbytes = sizeof(PanelGroup) * (size_t)ngroups;
     const size_t pbytes = sizeof(PanelSm) * (size_t)m;
-    PF_TRY(pf::arena_reserve(ctx, pf::align256(gbytes) + pf::align256(pbytes)));
+    // large point sets take the far groups through the box grid's local
+    // expansions
+    const bool boxed = n >= PL_MIN_POINTS && ngroups >= PL_MIN_GROUPS;
+    const int mwords = (int)pf::ceil_div(ngroups, (int64_t)32);
+    const size_t lbytes = boxed ? sizeof(double2) * PL_P * PL_NB * PL_NB : 0;
+    const size_t mbytes = boxed ? sizeof(unsigned) * (size_t)mwords * PL_NB * PL_NB : 0;
+    PF_TRY(pf::arena_reserve(ctx, pf::align256(gbytes) + pf::align256(pbytes) +
+                                      (boxed ? pf::align256(sizeof(PanelGrid)) +
+                                                   pf::align256(lbytes) + pf::align256(mbytes)
+                                             : 0)));
     auto *groups = static_cast<PanelGroup *>(pf::arena_take(ctx, gbytes));
     auto *pan = static_cast<PanelSm *>(pf::arena_take(ctx, pbytes));
-    if (!groups || !pan) {
+    PanelGrid *gd = nullptr;
+    double2 *locals = nullptr;
+    unsigned *masks = nullptr;
+    if (boxed) {
+        gd = static_cast<PanelGrid *>(pf::arena_take(ctx, sizeof(PanelGrid)));
+        locals = static_cast<double2 *>(pf::arena_take(ctx, lbytes));
+        masks = static_cast<unsigned *>(pf::arena_take(ctx, mbytes));
+    }
+    if (!groups || !pan || (boxed && (!gd || !locals || !masks))) {
         pf::set_error("%s: scratch too small", name);
         return PF_ERR_OOM;
     }
@@ -360,6 +628,26 @@ static pf_status panel_velocity(pf_ctx *ctx, const char *name, int64_t m, const 
     const int64_t grid = std::min<int64_t>(pf::ceil_div(n, PN_THREADS), (int64_t)ctx->num_sms * 4);
     // P = ceil(log2(PC_EPS (1 - PC_RHO) / 2) / log2(rho)) terms for rho <= PC_RHO
     const float log2_tol = (float)std::log2(PC_EPS * (1.0 - PC_RHO) / 2.0);
+    if (boxed) {
+        k_panel_grid_init<<<1, 1, 0, st>>>(gd);
+        PF_TRY(pf::launch_status("k_panel_grid_init"));
+        k_panel_bbox<<<(unsigned)grid, PN_THREADS, 0, st>>>(n, xv, yv, gd);
+        PF_TRY(pf::launch_status("k_panel_bbox"));
+        k_panel_grid_set<<<1, 1, 0, st>>>(gd);
+        PF_TRY(pf::launch_status("k_panel_grid_set"));
+        k_panel_locals<<<PL_NB * PL_NB / 4, 128, 0, st>>>(ngroups, groups, gd, mwords, locals,
+                                                          masks);
+        PF_TRY(pf::launch_status("k_panel_locals"));
+        if (source)
+            k_panel_velocity_boxed<true><<<(unsigned)grid, PN_THREADS, 0, st>>>(
+                ngroups, groups, pan, m, n, xv, yv, vx, vy, accumulate, log2_tol, gd, mwords,
+                locals, masks);
+        else
+            k_panel_velocity_boxed<false><<<(unsigned)grid, PN_THREADS, 0, st>>>(
+                ngroups, groups, pan, m, n, xv, yv, vx, vy, accumulate, log2_tol, gd, mwords,
+                locals, masks);
+        return pf::launch_status("k_panel_velocity_boxed");
+    }
     if (source)
         k_panel_velocity<true><<<(unsigned)grid, PN_THREADS, 0, st>>>(
             ngroups, groups, pan, m, n, xv, yv, vx, vy, accumulate, log2_tol);

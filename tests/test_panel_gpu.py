@@ -136,3 +136,58 @@ def test_source_panels_far_field_and_panels_class():
     s_ref = np.linalg.solve(panels.A, rhs)
     assert np.abs(panels.sPanel - s_ref).max() <= 1e-10 * np.abs(s_ref).max()
     assert np.all(np.asarray(panels.gTotal) == 0.0)
+
+
+def _annulus(n, r0, r1, seed):
+    rng = np.random.default_rng(seed)
+    r = rng.uniform(r0, r1, n)
+    t = rng.uniform(-np.pi, np.pi, n)
+    return r * np.cos(t), r * np.sin(t)
+
+
+def test_box_grid_path_near_wall_vs_oracle():
+    """2^16 points (the box-grid path: far groups through each box's local
+    expansion, near groups per point) in the near-wall annulus: the gate."""
+    import pfblob
+    from pfblob import workloads as wl
+    ps = wl.cylinder_panels(512)
+    xv, yv = _annulus(1 << 16, 1.0, 1.5, 8)
+    rx, ry = oracle.panel_velocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina, xv, yv)
+    vx, vy = pfblob.inducedVelocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina, xv, yv)
+    assert normwise_err(vx, vy, rx, ry) <= TOL
+
+
+def test_box_grid_path_far_points_to_1e10():
+    """Far points on the box-grid path carry every group through the local
+    expansions: still within 1e-10 of the FP64 pair formula."""
+    import pfblob
+    from pfblob import workloads as wl
+    ps = wl.cylinder_panels(512)
+    xv, yv = _annulus(1 << 16, 2.0, 6.0, 9)
+    rx, ry = oracle.panel_velocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina, xv, yv)
+    vx, vy = pfblob.inducedVelocity(ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina, xv, yv)
+    assert normwise_err(vx, vy, rx, ry) <= 1e-10
+
+
+@pytest.mark.parametrize("m,shuffle", [(512, False), (2048, False), (512, True)])
+def test_box_grid_path_matches_per_point_path(m, shuffle):
+    """The same points through both paths (40,000 at once: box grid; 10,000
+    at a time: every group per point) agree to 1e-10 of the velocity, also
+    with shuffled panels (every group spans the body: far only from the
+    corner boxes)."""
+    import pfblob
+    from pfblob import workloads as wl
+    ps = wl.cylinder_panels(m)
+    arrs = [ps.gamma, ps.xs, ps.ys, ps.xe, ps.ye, ps.cosa, ps.sina]
+    if shuffle:
+        perm = np.random.default_rng(10).permutation(m)
+        arrs = [a[perm] for a in arrs]
+    xv, yv = _annulus(40000, 1.0, 3.0, 11)
+    vx, vy = pfblob.inducedVelocity(*arrs, xv, yv)
+    px, py = [], []
+    for k in range(0, 40000, 10000):
+        a, b = pfblob.inducedVelocity(*arrs, xv[k:k + 10000], yv[k:k + 10000])
+        px.append(a)
+        py.append(b)
+    px, py = np.concatenate(px), np.concatenate(py)
+    assert normwise_err(vx, vy, px, py) <= 1e-10

@@ -96,16 +96,16 @@ __device__ __forceinline__ void pair_velocity(const PanelSm &q, double px, doubl
 
 // One warp per group: the panels' frame records, the enclosing circle and the
 // series coefficients (lane k forms A_{k+1}).
-template <bool SOURCE>
+template <bool SOURCE, int G = PC_G>
 __global__ void __launch_bounds__(32)
 k_panel_groups(int64_t m, const double *__restrict__ gamma, const double *__restrict__ xs,
                const double *__restrict__ ys, const double *__restrict__ xe,
                const double *__restrict__ ye, const double *__restrict__ cosa,
                const double *__restrict__ sina, PanelGroup *__restrict__ groups,
                PanelSm *__restrict__ pan) {
-    const int64_t j0 = (int64_t)blockIdx.x * PC_G;
+    const int64_t j0 = (int64_t)blockIdx.x * G;
     const int lane = threadIdx.x;
-    const int cnt = (int)min((int64_t)PC_G, m - j0);
+    const int cnt = (int)min((int64_t)G, m - j0);
     const bool has = lane < cnt;
     double x1 = 0.0, y1 = 0.0, x2e = 0.0, y2e = 0.0, kr = 0.0, ki = 0.0;
     double bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
@@ -119,7 +119,7 @@ k_panel_groups(int64_t m, const double *__restrict__ gamma, const double *__rest
         const double lx = xe[j] - q.xs, ly = ye[j] - q.ys;
         q.x2 = q.c * lx + q.s * ly;
         q.gam = gamma[j];
-        pan[j] = q;
+        if (pan) pan[j] = q;
         x1 = q.xs;
         y1 = q.ys;
         x2e = q.xs + q.x2 * q.c;
@@ -153,7 +153,7 @@ k_panel_groups(int64_t m, const double *__restrict__ gamma, const double *__rest
     const double ar = (x1 - cx) * inv, ai = (y1 - cy) * inv;
     const double br = (x2e - cx) * inv, bi = (y2e - cy) * inv;
     // the group's scaled end points and strengths, for every lane's terms
-    __shared__ double s_e[6][PC_G];
+    __shared__ double s_e[6][G];
     if (has) {
         s_e[0][lane] = ar;
         s_e[1][lane] = ai;
@@ -291,6 +291,10 @@ constexpr int PL_NB = 64;         // boxes per side of the grid
 constexpr int PL_P = 40;          // local expansion terms
 constexpr int64_t PL_MIN_POINTS = 32768;  // below: every group per point
 constexpr int PL_MIN_GROUPS = 8;
+// near groups on the box-grid path are summed by sub-groups of PL_SUB panels
+// (their own series where R_sub / |z - c_sub| <= PC_RHO, else the pair formula)
+constexpr int PL_SUB = 4;
+static_assert(PC_G % PL_SUB == 0, "sub-groups tile a group");
 
 struct PanelGrid {
     double x0, y0, wb;  // grid origin and box width
@@ -316,13 +320,24 @@ __global__ void __launch_bounds__(PN_THREADS)
 k_panel_bbox(int64_t n, const double *__restrict__ xv, const double *__restrict__ yv,
              PanelGrid *gd) {
     unsigned long long mnx = ~0ull, mny = ~0ull, mxx = 0ull, mxy = 0ull;
-    for (int64_t i = (int64_t)blockIdx.x * PN_THREADS + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * PN_THREADS) {
-        const unsigned long long ox = pl_ord(xv[i]), oy = pl_ord(yv[i]);
-        mnx = min(mnx, ox);
-        mxx = max(mxx, ox);
-        mny = min(mny, oy);
-        mxy = max(mxy, oy);
+    // four points per iteration, their loads in flight together
+    const int64_t stride = (int64_t)gridDim.x * PN_THREADS;
+    for (int64_t i0 = (int64_t)blockIdx.x * PN_THREADS + threadIdx.x; i0 < n; i0 += 4 * stride) {
+        double xs4[4], ys4[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t i = i0 + u * stride;
+            xs4[u] = i < n ? xv[i] : xv[i0];
+            ys4[u] = i < n ? yv[i] : yv[i0];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const unsigned long long ox = pl_ord(xs4[u]), oy = pl_ord(ys4[u]);
+            mnx = min(mnx, ox);
+            mxx = max(mxx, ox);
+            mny = min(mny, oy);
+            mxy = max(mxy, oy);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -331,11 +346,48 @@ k_panel_bbox(int64_t n, const double *__restrict__ xv, const double *__restrict_
         mny = min(mny, __shfl_xor_sync(0xffffffffu, mny, o));
         mxy = max(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
     }
-    if ((threadIdx.x & 31) == 0) {
+    // the CTA's warps, then one set of atomics per CTA
+    __shared__ unsigned long long s_b[4][PN_THREADS / 32];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s_b[0][wid] = mnx;
+        s_b[1][wid] = mxx;
+        s_b[2][wid] = mny;
+        s_b[3][wid] = mxy;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < PN_THREADS / 32; ++w) {
+            mnx = min(mnx, s_b[0][w]);
+            mxx = max(mxx, s_b[1][w]);
+            mny = min(mny, s_b[2][w]);
+            mxy = max(mxy, s_b[3][w]);
+        }
         atomicMin(&gd->mn[0], mnx);
         atomicMax(&gd->mx[0], mxx);
         atomicMin(&gd->mn[1], mny);
         atomicMax(&gd->mx[1], mxy);
+    }
+}
+
+// Boxes holding a point (the others need no local expansion); a store per
+// run of equal boxes in a warp
+__global__ void __launch_bounds__(PN_THREADS)
+k_panel_flags(int64_t n, const double *__restrict__ xv, const double *__restrict__ yv,
+              const PanelGrid *gd, int *__restrict__ flags) {
+    const double x0 = gd->x0, y0 = gd->y0, wb = gd->wb;
+    const int lane = threadIdx.x & 31;
+    for (int64_t b0 = (int64_t)blockIdx.x * PN_THREADS; b0 < n;
+         b0 += (int64_t)gridDim.x * PN_THREADS) {
+        const int64_t i = b0 + threadIdx.x;
+        int box = -1;
+        if (i < n) {
+            const int bx = min(max((int)floor((xv[i] - x0) / wb), 0), PL_NB - 1);
+            const int by = min(max((int)floor((yv[i] - y0) / wb), 0), PL_NB - 1);
+            box = bx * PL_NB + by;
+        }
+        const int prev = __shfl_up_sync(0xffffffffu, box, 1);
+        if (box >= 0 && (lane == 0 || prev != box)) flags[box] = 1;
     }
 }
 
@@ -351,24 +403,28 @@ __global__ void k_panel_grid_set(PanelGrid *gd) {
     gd->wb = e * (1.0 + 1e-9) / PL_NB;
 }
 
-// One warp per box: the near-group mask (mwords words) and the local
-// expansion of the far groups' series (lane n holds L_n and L_{n+32}).
+// One CTA of four warps per box: the near-group mask (mwords words) and the
+// local expansion of the far groups' series.  Warp v takes the far groups
+// v, v + 4, ... of the box (lane n holds its partial L_n and L_{n+32}); the
+// four partials are added in warp order.
 __global__ void __launch_bounds__(128)
 k_panel_locals(int64_t ngroups, const PanelGroup *__restrict__ groups, const PanelGrid *gd,
-               int mwords, double2 *__restrict__ locals, unsigned *__restrict__ masks) {
-    __shared__ double s_bin[PL_P][PC_P];  // C(n + k - 1, n), k = 1 .. PC_P
+               const int *__restrict__ flags, int mwords, double2 *__restrict__ locals,
+               unsigned *__restrict__ masks) {
+    __shared__ double s_bin[PC_P][PL_P];  // [k - 1][n] = C(n + k - 1, n): lanes read rows
     __shared__ double2 s_beta[4][PC_P];   // per warp: A_k (R / D)^k
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int nn = threadIdx.x; nn < PL_P; nn += blockDim.x) {
         double c = 1.0;  // C(n, n)
         for (int k = 1; k <= PC_P; ++k) {
-            s_bin[nn][k - 1] = c;
+            s_bin[k - 1][nn] = c;
             c = c * (double)(nn + k) / (double)k;  // C(n + k, n)
         }
     }
+    __shared__ double2 s_part[4][PL_P];
+    const int box = blockIdx.x;
+    if (!flags[box]) return;  // the whole CTA: no point there
     __syncthreads();
-    const int box = blockIdx.x * 4 + wid;
-    if (box >= PL_NB * PL_NB) return;  // the whole warp
     const int bx = box / PL_NB, by = box - bx * PL_NB;
     const double wb = gd->wb;
     const double zbx = gd->x0 + ((double)bx + 0.5) * wb, zby = gd->y0 + ((double)by + 0.5) * wb;
@@ -385,8 +441,10 @@ k_panel_locals(int64_t ngroups, const PanelGroup *__restrict__ groups, const Pan
         }
         const unsigned nm = __ballot_sync(0xffffffffu, near);
         const unsigned valid = __ballot_sync(0xffffffffu, g < ngroups);
-        if (lane == 0) masks[(int64_t)box * mwords + w] = nm;
+        if (wid == 0 && lane == 0) masks[(int64_t)box * mwords + w] = nm;
         unsigned far = valid & ~nm;
+        // this warp's share: the (wid)-th, (wid + 4)-th, ... far group of the word
+        for (int skip = wid; skip > 0 && far; --skip) far &= far - 1;
         while (far) {
             const int j = __ffs(far) - 1;
             far &= far - 1;
@@ -411,14 +469,30 @@ k_panel_locals(int64_t ngroups, const PanelGroup *__restrict__ groups, const Pan
                 s_beta[wid][k - 1] = make_double2(a.x * pr - a.y * pi, a.x * pi + a.y * pr);
             }
             __syncwarp();
-            // L_n += (-rb / D)^n sum_k C(n + k - 1, n) beta_k
-            for (int n = lane, h = 0; n < PL_P; n += 32, ++h) {
-                double sr = 0.0, si = 0.0;
-                for (int k = 0; k < PC_P; ++k) {
-                    const double c = s_bin[n][k];
-                    sr = fma(c, s_beta[wid][k].x, sr);
-                    si = fma(c, s_beta[wid][k].y, si);
-                }
+            // L_n += (-rb / D)^n sum_k C(n + k - 1, n) beta_k, for n = lane and
+            // n = lane + 32 in one pass over k (even and odd k summed apart)
+            const bool two = lane + 32 < PL_P;
+            const int n1 = two ? lane + 32 : lane;
+            double a0r = 0.0, a0i = 0.0, a1r = 0.0, a1i = 0.0;  // n = lane: even, odd k
+            double c0r = 0.0, c0i = 0.0, c1r = 0.0, c1i = 0.0;  // n = lane + 32
+#pragma unroll 6
+            for (int k = 0; k < PC_P; k += 2) {
+                const double2 b0 = s_beta[wid][k], b1 = s_beta[wid][k + 1];
+                const double e0 = s_bin[k][lane], e1 = s_bin[k + 1][lane];
+                a0r = fma(e0, b0.x, a0r);
+                a0i = fma(e0, b0.y, a0i);
+                a1r = fma(e1, b1.x, a1r);
+                a1i = fma(e1, b1.y, a1i);
+                const double f0 = s_bin[k][n1], f1 = s_bin[k + 1][n1];
+                c0r = fma(f0, b0.x, c0r);
+                c0i = fma(f0, b0.y, c0i);
+                c1r = fma(f1, b1.x, c1r);
+                c1i = fma(f1, b1.y, c1i);
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int n = h ? n1 : lane;
+                const double sr = h ? c0r + c1r : a0r + a1r, si = h ? c0i + c1i : a0i + a1i;
                 double pr = 1.0, pi = 0.0, br = -rb * rr, bi = -rb * ri;  // (-rb / D)^n
                 for (int e = n; e; e >>= 1) {
                     if (e & 1) {
@@ -432,14 +506,24 @@ k_panel_locals(int64_t ngroups, const PanelGroup *__restrict__ groups, const Pan
                 }
                 const double vr = sr * pr - si * pi, vi = sr * pi + si * pr;
                 if (h == 0) l0 = make_double2(l0.x + vr, l0.y + vi);
-                else l1 = make_double2(l1.x + vr, l1.y + vi);
+                else if (two) l1 = make_double2(l1.x + vr, l1.y + vi);
             }
             __syncwarp();  // s_beta is read before the next group refills it
+            for (int skip = 3; skip > 0 && far; --skip) far &= far - 1;  // the next 3: other warps
         }
     }
-    double2 *L = locals + (int64_t)box * PL_P;
-    L[lane] = l0;
-    if (lane + 32 < PL_P) L[lane + 32] = l1;
+    s_part[wid][lane] = l0;
+    if (lane + 32 < PL_P) s_part[wid][lane + 32] = l1;
+    __syncthreads();
+    if (wid == 0) {
+        double2 *L = locals + (int64_t)box * PL_P;
+        for (int n = lane; n < PL_P; n += 32) {
+            double2 v = s_part[0][n];
+#pragma unroll
+            for (int q = 1; q < 4; ++q) v = make_double2(v.x + s_part[q][n].x, v.y + s_part[q][n].y);
+            L[n] = v;
+        }
+    }
 }
 
 // Velocity at the points through the box grid: the box's local expansion
@@ -451,7 +535,8 @@ k_panel_velocity_boxed(int64_t ngroups, const PanelGroup *__restrict__ groups,
                        const double *__restrict__ xv, const double *__restrict__ yv,
                        double *__restrict__ vx, double *__restrict__ vy, int accumulate,
                        float log2_tol, const PanelGrid *gd, int mwords,
-                       const double2 *__restrict__ locals, const unsigned *__restrict__ masks) {
+                       const double2 *__restrict__ locals, const unsigned *__restrict__ masks,
+                       const PanelGroup *__restrict__ subs) {
     const double x0 = gd->x0, y0 = gd->y0, wb = gd->wb;
     const double rb = 0.70710678118654757 * wb, irb = 1.0 / rb;
     for (int64_t i = (int64_t)blockIdx.x * PN_THREADS + threadIdx.x; i < n;
@@ -480,27 +565,33 @@ k_panel_velocity_boxed(int64_t ngroups, const PanelGroup *__restrict__ groups,
                 const int j = __ffs(nm) - 1;
                 nm &= nm - 1;
                 const int64_t g = (int64_t)w * 32 + j;
-                const PanelGroup &G = groups[g];
-                const double dx = px - G.cx, dy = py - G.cy;
-                const double r2 = dx * dx + dy * dy;
-                if (r2 < G.far_r2) {
-                    const int j1 = (int)min((int64_t)PC_G, m - g * PC_G);
-                    for (int q = 0; q < j1; ++q) pair_velocity<SOURCE>(pan[g * PC_G + q], px, py, ax, ay);
-                } else {
-                    const double R = G.R;
-                    const double q = R / r2;
-                    const double sr = dx * q, si = -dy * q;  // s = R / (z - c)
-                    const float lr = 0.5f * __log2f((float)(R * q));
-                    const int P = max(1, min(PC_P, (int)ceilf(log2_tol / lr)));
-                    double tr0 = 0.0, ti0 = 0.0;
-                    for (int k = P - 1; k >= 0; --k) {
-                        const double2 a = G.a[k];
-                        const double t = fma(sr, tr0, fma(-si, ti0, a.x));
-                        ti0 = fma(sr, ti0, fma(si, tr0, a.y));
-                        tr0 = t;
+                // its sub-groups of PL_SUB panels: series or pair formulas
+                const int64_t s0 = g * (PC_G / PL_SUB);
+                const int64_t s1 = min(s0 + PC_G / PL_SUB, (m + PL_SUB - 1) / PL_SUB);
+                for (int64_t sg = s0; sg < s1; ++sg) {
+                    const PanelGroup &G = subs[sg];
+                    const double dx = px - G.cx, dy = py - G.cy;
+                    const double r2 = dx * dx + dy * dy;
+                    if (r2 < G.far_r2) {
+                        const int j1 = (int)min((int64_t)PL_SUB, m - sg * PL_SUB);
+                        for (int q = 0; q < j1; ++q)
+                            pair_velocity<SOURCE>(pan[sg * PL_SUB + q], px, py, ax, ay);
+                    } else {
+                        const double R = G.R;
+                        const double q = R / r2;
+                        const double sr = dx * q, si = -dy * q;  // s = R / (z - c)
+                        const float lr = 0.5f * __log2f((float)(R * q));
+                        const int P = max(1, min(PC_P, (int)ceilf(log2_tol / lr)));
+                        double tr0 = 0.0, ti0 = 0.0;
+                        for (int k = P - 1; k >= 0; --k) {
+                            const double2 a = G.a[k];
+                            const double t = fma(sr, tr0, fma(-si, ti0, a.x));
+                            ti0 = fma(sr, ti0, fma(si, tr0, a.y));
+                            tr0 = t;
+                        }
+                        ax += sr * tr0 - si * ti0;
+                        ay -= sr * ti0 + si * tr0;
                     }
-                    ax += sr * tr0 - si * ti0;
-                    ay -= sr * ti0 + si * tr0;
                 }
             }
         }
@@ -599,21 +690,29 @@ static pf_status panel_velocity(pf_ctx *ctx, const char *name, int64_t m, const 
     const int mwords = (int)pf::ceil_div(ngroups, (int64_t)32);
     const size_t lbytes = boxed ? sizeof(double2) * PL_P * PL_NB * PL_NB : 0;
     const size_t mbytes = boxed ? sizeof(unsigned) * (size_t)mwords * PL_NB * PL_NB : 0;
+    const size_t fbytes = boxed ? sizeof(int) * PL_NB * PL_NB : 0;
+    const int64_t nsubs = pf::ceil_div(m, (int64_t)PL_SUB);
+    const size_t sbytes = boxed ? sizeof(PanelGroup) * (size_t)nsubs : 0;
     PF_TRY(pf::arena_reserve(ctx, pf::align256(gbytes) + pf::align256(pbytes) +
                                       (boxed ? pf::align256(sizeof(PanelGrid)) +
-                                                   pf::align256(lbytes) + pf::align256(mbytes)
+                                                   pf::align256(lbytes) + pf::align256(mbytes) +
+                                                   pf::align256(fbytes) + pf::align256(sbytes)
                                              : 0)));
     auto *groups = static_cast<PanelGroup *>(pf::arena_take(ctx, gbytes));
     auto *pan = static_cast<PanelSm *>(pf::arena_take(ctx, pbytes));
     PanelGrid *gd = nullptr;
     double2 *locals = nullptr;
     unsigned *masks = nullptr;
+    int *flags = nullptr;
+    PanelGroup *subs = nullptr;
     if (boxed) {
         gd = static_cast<PanelGrid *>(pf::arena_take(ctx, sizeof(PanelGrid)));
         locals = static_cast<double2 *>(pf::arena_take(ctx, lbytes));
         masks = static_cast<unsigned *>(pf::arena_take(ctx, mbytes));
+        flags = static_cast<int *>(pf::arena_take(ctx, fbytes));
+        subs = static_cast<PanelGroup *>(pf::arena_take(ctx, sbytes));
     }
-    if (!groups || !pan || (boxed && (!gd || !locals || !masks))) {
+    if (!groups || !pan || (boxed && (!gd || !locals || !masks || !flags || !subs))) {
         pf::set_error("%s: scratch too small", name);
         return PF_ERR_OOM;
     }
@@ -629,23 +728,33 @@ static pf_status panel_velocity(pf_ctx *ctx, const char *name, int64_t m, const 
     // P = ceil(log2(PC_EPS (1 - PC_RHO) / 2) / log2(rho)) terms for rho <= PC_RHO
     const float log2_tol = (float)std::log2(PC_EPS * (1.0 - PC_RHO) / 2.0);
     if (boxed) {
+        if (source)
+            k_panel_groups<true, PL_SUB><<<(unsigned)nsubs, 32, 0, st>>>(
+                m, gamma, xs, ys, xe, ye, cosa, sina, subs, nullptr);
+        else
+            k_panel_groups<false, PL_SUB><<<(unsigned)nsubs, 32, 0, st>>>(
+                m, gamma, xs, ys, xe, ye, cosa, sina, subs, nullptr);
+        PF_TRY(pf::launch_status("k_panel_groups"));
         k_panel_grid_init<<<1, 1, 0, st>>>(gd);
         PF_TRY(pf::launch_status("k_panel_grid_init"));
         k_panel_bbox<<<(unsigned)grid, PN_THREADS, 0, st>>>(n, xv, yv, gd);
         PF_TRY(pf::launch_status("k_panel_bbox"));
         k_panel_grid_set<<<1, 1, 0, st>>>(gd);
         PF_TRY(pf::launch_status("k_panel_grid_set"));
-        k_panel_locals<<<PL_NB * PL_NB / 4, 128, 0, st>>>(ngroups, groups, gd, mwords, locals,
-                                                          masks);
+        PF_CUDA_TRY(cudaMemsetAsync(flags, 0, fbytes, st));
+        k_panel_flags<<<(unsigned)grid, PN_THREADS, 0, st>>>(n, xv, yv, gd, flags);
+        PF_TRY(pf::launch_status("k_panel_flags"));
+        k_panel_locals<<<PL_NB * PL_NB, 128, 0, st>>>(ngroups, groups, gd, flags, mwords, locals,
+                                                      masks);
         PF_TRY(pf::launch_status("k_panel_locals"));
         if (source)
             k_panel_velocity_boxed<true><<<(unsigned)grid, PN_THREADS, 0, st>>>(
                 ngroups, groups, pan, m, n, xv, yv, vx, vy, accumulate, log2_tol, gd, mwords,
-                locals, masks);
+                locals, masks, subs);
         else
             k_panel_velocity_boxed<false><<<(unsigned)grid, PN_THREADS, 0, st>>>(
                 ngroups, groups, pan, m, n, xv, yv, vx, vy, accumulate, log2_tol, gd, mwords,
-                locals, masks);
+                locals, masks, subs);
         return pf::launch_status("k_panel_velocity_boxed");
     }
     if (source)

@@ -170,11 +170,13 @@ def test_box_grid_path_far_points_to_1e10():
 
 
 @pytest.mark.parametrize("m,shuffle", [(512, False), (2048, False), (512, True)])
-def test_box_grid_path_matches_per_point_path(m, shuffle):
+def test_box_grid_path_as_accurate_as_per_point_path(m, shuffle):
     """The same points through both paths (40,000 at once: box grid; 10,000
-    at a time: every group per point) agree to 1e-10 of the velocity, also
-    with shuffled panels (every group spans the body: far only from the
-    corner boxes)."""
+    at a time: every group per point) against the FP64 oracle: the box grid
+    meets the gate with the per-point path's accuracy (both are set by the
+    FP32 transcendentals of the pair formula at the points nearest the body;
+    the box grid takes the FP64 series of sub-groups for more of its near
+    panels); also with shuffled panels, whose groups span the body."""
     import pfblob
     from pfblob import workloads as wl
     ps = wl.cylinder_panels(m)
@@ -190,4 +192,6 @@ def test_box_grid_path_matches_per_point_path(m, shuffle):
         px.append(a)
         py.append(b)
     px, py = np.concatenate(px), np.concatenate(py)
-    assert normwise_err(vx, vy, px, py) <= 1e-10
+    rx, ry = oracle.panel_velocity(*arrs, xv, yv)
+    e_box, e_pt = normwise_err(vx, vy, rx, ry), normwise_err(px, py, rx, ry)
+    assert e_box <= TOL and e_box <= 1.5 * e_pt + 1e-10, (e_box, e_pt)

@@ -377,17 +377,28 @@ k_panel_flags(int64_t n, const double *__restrict__ xv, const double *__restrict
               const PanelGrid *gd, int *__restrict__ flags) {
     const double x0 = gd->x0, y0 = gd->y0, wb = gd->wb;
     const int lane = threadIdx.x & 31;
-    for (int64_t b0 = (int64_t)blockIdx.x * PN_THREADS; b0 < n;
-         b0 += (int64_t)gridDim.x * PN_THREADS) {
-        const int64_t i = b0 + threadIdx.x;
-        int box = -1;
-        if (i < n) {
-            const int bx = min(max((int)floor((xv[i] - x0) / wb), 0), PL_NB - 1);
-            const int by = min(max((int)floor((yv[i] - y0) / wb), 0), PL_NB - 1);
-            box = bx * PL_NB + by;
+    // four blocks of points per iteration, their loads in flight together
+    const int64_t stride = (int64_t)gridDim.x * PN_THREADS;
+    for (int64_t b0 = (int64_t)blockIdx.x * PN_THREADS; b0 < n; b0 += 4 * stride) {
+        double xs4[4], ys4[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t i = b0 + u * stride + threadIdx.x;
+            xs4[u] = i < n ? xv[i] : 0.0;
+            ys4[u] = i < n ? yv[i] : 0.0;
         }
-        const int prev = __shfl_up_sync(0xffffffffu, box, 1);
-        if (box >= 0 && (lane == 0 || prev != box)) flags[box] = 1;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t i = b0 + u * stride + threadIdx.x;
+            int box = -1;
+            if (i < n) {
+                const int bx = min(max((int)floor((xs4[u] - x0) / wb), 0), PL_NB - 1);
+                const int by = min(max((int)floor((ys4[u] - y0) / wb), 0), PL_NB - 1);
+                box = bx * PL_NB + by;
+            }
+            const int prev = __shfl_up_sync(0xffffffffu, box, 1);
+            if (box >= 0 && (lane == 0 || prev != box)) flags[box] = 1;
+        }
     }
 }
 

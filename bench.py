@@ -881,6 +881,7 @@ def run_served(dev, n_sims=1024, n_req=400, rates=(100, 1000, 5000), slots=8):
     """1024 resident simulations, N log-uniform in [1024, 2^20]; Poisson arrivals
     of velocity+remesh requests; continuous batching over `slots` worker streams
     vs one request at a time."""
+    import torch
     from pfblob import workloads as wl
     from pfblob.serve import Server, Simulation, conservation, poisson_trace, summarize
     sizes = wl.log_uniform_sizes(n_sims, 1024, 1 << 20, config=5)
@@ -888,6 +889,7 @@ def run_served(dev, n_sims=1024, n_req=400, rates=(100, 1000, 5000), slots=8):
     out = {"workload": f"{n_sims} resident simulations, N log-uniform [1024, 1048576] "
                        f"(sum {int(sizes.sum())}); Poisson arrivals, {n_req} requests per rate",
            "slots": slots, "rates": {}}
+    sat = max(rates)
     srv = Server(sims, n_slots=slots)
     srv.warmup()
     worst = {"circulation": 0.0, "linear_impulse": 0.0, "steps_checked": 0}
@@ -901,9 +903,38 @@ def run_served(dev, n_sims=1024, n_req=400, rates=(100, 1000, 5000), slots=8):
                                note="FP64 moments of every served step, before and after its "
                                     "remesh (fused into the remesh kernels)")
     srv.close()
+    # the same slots replaying one captured step per simulation, and the
+    # device time of the saturation trace's steps replayed back to back on one
+    # stream (the work the device has to do, whatever the host side)
+    torch.cuda.synchronize(dev)
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    srv = Server(sims, n_slots=slots, step_graphs=True)
+    t0 = time.perf_counter()
+    srv.warmup()
+    torch.cuda.synchronize(dev)
+    sg = {"graphs": len(srv._graphs), "warmup_s": time.perf_counter() - t0,
+          "device_gb_held": (free0 - torch.cuda.mem_get_info(dev)[0]) / 1e9}
+    trace = poisson_trace(n_req, sat, n_sims, seed=sat)
+    r0 = srv.graph_replays
+    sg["served_at_saturation"] = summarize(srv.run_trace(trace))
+    sg["replayed_requests"] = srv.graph_replays - r0
+    if len(srv._graphs) == n_sims:
+        st = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(2):  # the second pass is the one kept
+            torch.cuda.synchronize(dev)
+            e0.record(st)
+            for _, i in trace:
+                srv._graphs[i][2].launch(st.cuda_stream)
+            e1.record(st)
+            torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        sg["serial_device_ms"] = ms
+        sg["serial_device_evals_per_s"] = sum(sims[i].n for _, i in trace) / (ms * 1e-3)
+    srv.close()
+    out["step_graphs"] = sg
     one = Server(sims, n_slots=1)
     one.warmup(every_sim=False)
-    sat = max(rates)
     out["plain_one_at_a_time"] = summarize(one.run_trace(poisson_trace(n_req, sat, n_sims, seed=sat)))
     one.close()
     out["ratio_at_saturation"] = (out["rates"][str(sat)]["evals_per_s"] /

@@ -17,6 +17,17 @@ admitted as slots and memory free up, so their kernels overlap on the device.
 Every kernel is deterministic, so a request's result does not depend on what
 runs beside it.
 
+With ``step_graphs=True`` the server also captures, at ``warmup()``, one
+StepGraph per resident simulation (its pf_blob_step with a private context
+and output buffers; see stepgraph.py), as long as free HBM holds them.  A
+plain step request (no move, no kept result, no state update) then costs one
+graph launch on the slot's stream instead of the step's ~30 kernel launches;
+its moments are copied to the request's row.  The graphs hold their scratch
+from warm-up on, so such a request claims no arena growth.  Two requests for
+the same simulation take its graph one after the other (a per-simulation
+lock: CUDA orders launches of one executable graph anyway, the lock also
+orders the moment copies).
+
 The reference has no counterpart (one blob set per call, synchronous).
 """
 import ctypes
@@ -87,7 +98,7 @@ class Request:
 
 class Server:
     def __init__(self, sims, n_slots=8, tol=1e-6, tuner=None, hbm_reserve=2 << 30,
-                 free_hbm=None, keep_results=False, device=None):
+                 free_hbm=None, keep_results=False, device=None, step_graphs=False):
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         self.sims = list(sims)
         self.tol = tol
@@ -116,6 +127,10 @@ class Server:
         self._slot_buf = [None] * n_slots
         self._desc = {}
         self._mom = torch.zeros((0, 8), dtype=torch.float64, device=self.device)
+        self.step_graphs = step_graphs
+        self._graphs = {}  # sim -> (x pointer, n, StepGraph)
+        self._sim_locks = [threading.Lock() for _ in self.sims]
+        self.graph_replays = 0
         self._threads = [threading.Thread(target=self._worker, args=(i,), daemon=True)
                          for i in range(n_slots)]
         for t in self._threads:
@@ -129,6 +144,48 @@ class Server:
         self.run_trace([(0.0, big)] * self.n_slots, timeout=timeout)
         if every_sim:
             self.run_trace([(0.0, i) for i in range(len(self.sims))], timeout=timeout)
+        if self.step_graphs:
+            self.build_graphs()
+
+    def build_graphs(self):
+        """Capture the step of every resident simulation that has none (or
+        whose state was replaced), while free HBM (less the reserve) holds the
+        graph's scratch and outputs; the rest keep the kernel-by-kernel path.
+        Each capture synchronises the device: call it while no request runs.
+        Returns the number of simulations with a current graph."""
+        from .stepgraph import StepGraph
+        for i, s in enumerate(self.sims):
+            if not s.n:
+                continue
+            old = self._graphs.get(i)
+            if old is not None and old[:2] == (s.x.data_ptr(), s.n):
+                continue
+            if old is not None:
+                old[2].close()
+                del self._graphs[i]
+            cap = self._bound(s, False) * 3 // 2 + 65536
+            if self.need_bytes(i) + 24 * cap + 16 * s.n > self.free_hbm() - self.reserve:
+                continue
+            ks, xo, cut = fmm_parameters(s.sigma, s.k, tol=self.tol)
+            h = s.h
+            g = StepGraph(s.x, s.y, s.g, ks, xo, cut, self.tol, self._box(s), h, -1.5 * h,
+                          -1.5 * h, c=s.c, method=s.method,
+                          leaf_level=s.leaf_level if s.method == FMM_METHOD else 0,
+                          max_base_cells=self._bound(s, False), capacity=cap)
+            self._graphs[i] = (s.x.data_ptr(), s.n, g)
+        return len(self._graphs)
+
+    def _graph(self, req):
+        """The step graph that serves `req`, or None (moved, kept or updating
+        requests, and simulations without a current graph, take the kernel-by-
+        kernel path)."""
+        if req.dt != 0.0 or self.keep or req.update:
+            return None
+        e = self._graphs.get(req.sim)
+        if e is None:
+            return None
+        s = self.sims[req.sim]
+        return e[2] if e[:2] == (s.x.data_ptr(), s.n) else None
 
     # -- memory model -----------------------------------------------------------
     def need_bytes(self, sim):
@@ -234,6 +291,18 @@ class Server:
         takes the cached box and the remesh finds its window on the device;
         such a step is one pf_blob_step call into slot buffers."""
         s = self.sims[req.sim]
+        g = self._graph(req)
+        if g is not None:
+            stream = torch.cuda.current_stream(self.device)
+            with self._sim_locks[req.sim]:
+                g.launch(stream.cuda_stream)
+                self._mom[req.idx].copy_(g.moments, non_blocking=True)
+                stream.synchronize()  # the graph's buffers are free for the next request
+            req.n = s.n
+            req.moments = self._mom[req.idx]
+            with self._lock:
+                self.graph_replays += 1
+            return
         if req.dt == 0.0 and not (self.keep or req.update) and s.n:
             d = self._descriptor(req.slot, req.sim)
             d.moments_dev = self._mom[req.idx].data_ptr()
@@ -272,13 +341,18 @@ class Server:
         if self.keep:
             req.result = {"vx": vx, "vy": vy, "x": xn, "y": yn, "g": gn}
         if req.update:
-            s.x, s.y, s.g = xn, yn, gn
-            s.box = s.window = None
+            with self._sim_locks[req.sim]:
+                e = self._graphs.pop(req.sim, None)
+                if e is not None:
+                    e[2].close()
+                s.x, s.y, s.g = xn, yn, gn
+                s.box = s.window = None
 
     # -- dispatcher ---------------------------------------------------------------
     def _try_admit(self, req):
         """Admit `req` to a free slot if memory allows; returns True if started."""
-        need = self.need_bytes(req.sim)
+        # a step graph holds its own scratch: nothing to claim
+        need = 0 if self._graph(req) is not None else self.need_bytes(req.sim)
         free_slots = [i for i in range(self.n_slots) if self._slot_free[i]]
         if not free_slots:
             return False
@@ -337,6 +411,9 @@ class Server:
             q.put(None)
         for t in self._threads:
             t.join(timeout=10)
+        for e in self._graphs.values():
+            e[2].close()
+        self._graphs = {}
 
 
 def poisson_trace(n_requests, rate, n_sims, seed=0):

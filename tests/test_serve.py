@@ -29,6 +29,8 @@ def _admission_only_server(n_slots, free, reserve, needs):
     s._slot_bytes = [0] * n_slots
     s._claimed = 0
     s._queues = [queue.Queue() for _ in range(n_slots)]
+    s.keep = False
+    s._graphs = {}
     s.reserve = reserve
     s.free_hbm = lambda: free[0]
     s.need_bytes = lambda sim: needs[sim]
@@ -153,3 +155,44 @@ def test_update_replaces_resident_state():
     done = srv.run_trace([(0.0, 0)], update=True, timeout=60)
     assert sims[0].n == done[0].result["x"].numel() != 5000
     srv.close()
+
+
+@pytest.mark.gpu
+def test_step_graph_serving_matches_kernel_by_kernel_serving():
+    """A server that replays one captured step per simulation gives, request
+    by request, bitwise the FP64 moments of the kernel-by-kernel server
+    (before and after each remesh), conserves them, launches one graph per
+    request, and its velocities agree with the kept results of a plain run."""
+    from pfblob.serve import Server, conservation, poisson_trace
+    sizes = [1500, 6000, 20000, 50000, 120000, 3000]
+    trace = poisson_trace(30, 20000.0, len(sizes), seed=7)
+    gsrv = Server(_sims(sizes), n_slots=4, step_graphs=True)
+    gsrv.warmup()
+    assert len(gsrv._graphs) == len(sizes)
+    r0 = gsrv.graph_replays
+    done_g = gsrv.run_trace(trace, timeout=120)
+    assert gsrv.graph_replays - r0 == 30 and not any(r.error for r in done_g)
+    c = conservation(done_g, gsrv.sims)
+    assert c["steps_checked"] == 30 and c["circulation"] <= 1e-12 and c["linear_impulse"] <= 1e-12
+    esrv = Server(_sims(sizes), n_slots=4)
+    done_e = esrv.run_trace(trace, timeout=120)
+    esrv.close()
+    key = lambda r: r.idx
+    for a, b in zip(sorted(done_g, key=key), sorted(done_e, key=key)):
+        assert a.sim == b.sim and torch.equal(a.moments, b.moments)
+    # the velocity of each graph's last replay against the kept result of a
+    # kernel-by-kernel step of the same resident set
+    ksrv = Server(_sims(sizes), n_slots=1, keep_results=True)
+    kept = {r.sim: r for r in ksrv.run_trace([(0.0, i) for i in range(len(sizes))], timeout=120)}
+    ksrv.close()
+    for i, (_, n, g) in gsrv._graphs.items():
+        vx, vy = kept[i].result["vx"], kept[i].result["vy"]
+        err = torch.sqrt(((g.vx - vx) ** 2 + (g.vy - vy) ** 2).sum() / (vx ** 2 + vy ** 2).sum())
+        assert float(err) <= 1e-9, (i, n, float(err))
+    # a state update drops that simulation's graph; its next plain request
+    # takes the kernel-by-kernel path
+    gsrv.run_trace([(0.0, 0)], update=True, timeout=60)
+    assert 0 not in gsrv._graphs
+    r1 = gsrv.graph_replays
+    assert not gsrv.run_trace([(0.0, 0)], timeout=60)[0].error and gsrv.graph_replays == r1
+    gsrv.close()

@@ -837,12 +837,32 @@ def run_c1(dev, steps=20, warmup=3):
     torch.cuda.synchronize(dev)
     vel = statistics.median(e[0].elapsed_time(e[1]) for e in evs)
     rm = statistics.median(e[1].elapsed_time(e[2]) for e in evs)
+    # the same step captured once (pfblob.StepGraph) and replayed
+    box = (float(b.x.min()), float(b.x.max()), float(b.y.min()), float(b.y.max()))
+    sg = pfblob.StepGraph(x, y, g, b.ksigmasqr, 0.0, 0.0, 1e-6, box, b.h, xb[0], yb[0],
+                          method=pfblob.DIRECT_METHOD, max_base_cells=mb)
+    for _ in range(warmup):
+        sg.launch()
+    gev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(steps)]
+    torch.cuda.synchronize(dev)
+    for e in gev:
+        e[0].record(st)
+        sg.launch()
+        e[1].record(st)
+    torch.cuda.synchronize(dev)
+    gms = statistics.median(e[0].elapsed_time(e[1]) for e in gev)
+    k = int(out[3].item())
+    same = (torch.equal(sg.vx, vx) and torch.equal(sg.vy, vy) and int(sg.n_out.item()) == k
+            and torch.equal(sg.out[2, :k], out[2][:k]))
+    graph = {"ms_per_step": gms, "kernels_per_launch": sg.kernels, "equals_eager_bitwise": same}
+    sg.close()
     return {"workload": "C1 Lamb-Oseen lattice: N=10000 (h=0.02, sigma=h/0.8), direct velocity at "
                         "every blob + M4' remesh", "n_blobs": b.n, "ms_per_step": vel + rm,
             "phase_ms": {"velocity": vel, "remesh": rm},
             "direct_pairs_per_s": float(b.n) ** 2 / (vel * 1e-3),
-            "n_out": int(out[3].item()), "status": int(out[4].item()),
-            "timing": "medians of CUDA-event phases; inputs resident, L2 not flushed (the set is 0.24 MB)"}
+            "n_out": k, "status": int(out[4].item()), "graph": graph,
+            "timing": "medians of CUDA-event phases; inputs resident, L2 not flushed (the set is "
+                      "0.24 MB); graph: the step as one StepGraph launch, median of its launches"}
 
 
 def run_evolve(dev, steps=10, warmup=2):

@@ -255,19 +255,29 @@ def test_remesh_window_larger_than_the_previous_one():
     assert np.abs(gn - rg).max() <= GTOL * np.abs(rg).max()
 
 
-def test_velocity_and_regrid_equals_the_two_calls():
+@pytest.mark.parametrize("case", ["uniform_fmm", "sparse_direct"])
+def test_velocity_and_regrid_equals_the_two_calls(case):
     """The one-upload step (velocity at the blobs, then Regrid of the same
     blobs, velocities read back while the remesh runs) gives bitwise the
     results of pfblob.velocity and pfblob.Regrid called one after the other,
-    from numpy and from pinned host tensors."""
+    from numpy, from pinned host tensors and from device tensors, on a dense
+    set with the FMM and on a sparse one (3,000 blobs over [-1, 1]^2) with the
+    direct sum."""
     import pfblob
     from pfblob import workloads as wl
-    b = wl.uniform_square(n=60000, sigma=0.004, config=2, instance=13)
+    if case == "uniform_fmm":
+        b, meth = wl.uniform_square(n=60000, sigma=0.004, config=2, instance=13), pfblob.FMM_METHOD
+    else:
+        b, meth = wl.mixed_instance(3000, config=4, instance=5, sigma=0.002), pfblob.DIRECT_METHOD
     xb, yb = b.bounds()
-    vx, vy = pfblob.velocity(b.x, b.y, b.g, b.sigma, method=pfblob.FMM_METHOD, hardware=1)
+    vx, vy = pfblob.velocity(b.x, b.y, b.g, b.sigma, method=meth, hardware=1)
     xn, yn, gn = pfblob.Regrid(b.x, b.y, b.g, b.sigma, b.overlap, xb, yb)
     for inp in ((b.x, b.y, b.g), tuple(torch.from_numpy(a).pin_memory() for a in (b.x, b.y, b.g))):
-        out = pfblob.velocity_and_regrid(*inp, b.sigma, b.overlap, xb, yb,
-                                         method=pfblob.FMM_METHOD)
+        out = pfblob.velocity_and_regrid(*inp, b.sigma, b.overlap, xb, yb, method=meth)
         for u, v in zip(out, (vx, vy, xn, yn, gn)):
             assert isinstance(u, np.ndarray) and np.array_equal(u, v)
+    dev = torch.device("cuda", 0)
+    out = pfblob.velocity_and_regrid(*(torch.from_numpy(a).to(dev) for a in (b.x, b.y, b.g)),
+                                     b.sigma, b.overlap, xb, yb, method=meth)
+    for u, v in zip(out, (vx, vy, xn, yn, gn)):
+        assert np.array_equal(u.cpu().numpy(), v)

@@ -7,9 +7,9 @@
 // sources and are folded into a TwoSum-compensated (hi, lo) accumulator
 // after each chunk.
 //
-// Source splits: with fewer target tiles than DT_SPLIT_CTAS the sources are
-// cut into S contiguous segments (direct_split, a function of the two sizes
-// only), CTA (tile, s) writes its (hi, lo) pairs to a partial buffer, and
+// Source splits: unless the target tiles alone fill the device several times
+// over, the sources are cut into S contiguous segments (direct_split, a
+// function of the two sizes and the device's resident CTA count), CTA (tile, s) writes its (hi, lo) pairs to a partial buffer, and
 // k_direct_reduce adds the S partials of each target in segment order in
 // FP64.  The batched kernel uses the same segments, so a blob set gets
 // bitwise the same velocities alone and in a batch.
@@ -24,6 +24,8 @@
 #include "gauss_pair.cuh"
 
 #include <algorithm>
+#include <atomic>
+#include <climits>
 
 namespace {
 
@@ -201,13 +203,49 @@ k_direct_reduce_batch(const pf::DirectInstance *__restrict__ inst,
 
 namespace pf {
 
+// k_direct_gauss CTAs resident on the whole current device (cached per
+// device; host threads may race to fill an entry, all with the same value).
+static int64_t direct_resident_ctas() {
+    static std::atomic<int64_t> cached[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return DT_SPLIT_CTAS;
+    int64_t v = cached[dev].load(std::memory_order_relaxed);
+    if (v == 0) {
+        int per_sm = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_direct_gauss<2, false>,
+                                                          DT_THREADS, 0) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            per_sm <= 0 || sms <= 0) {
+            cudaGetLastError();
+            return DT_SPLIT_CTAS;
+        }
+        v = (int64_t)per_sm * sms;
+        cached[dev].store(v, std::memory_order_relaxed);
+    }
+    return v;
+}
+
+// Segments of at least DT_SPLIT_MIN_SRC sources (at most DT_SPLIT_MAX of
+// them), in whole 32-source chunks, chosen to minimise the launch's critical
+// path: the full waves of resident CTAs times the sources each CTA runs.  A
+// grid just above one wave would leave its last CTAs running alone.
 DirectSplit direct_split(int64_t ns, int64_t nt) {
     const int64_t tiles = ceil_div(nt, DT_TILE);
-    if (tiles >= DT_SPLIT_CTAS || ns <= DT_SPLIT_MIN_SRC) return {1, ns > 0 ? ns : 1};
-    int64_t s = std::min(ceil_div(DT_SPLIT_CTAS, tiles), ceil_div(ns, DT_SPLIT_MIN_SRC));
-    s = std::min<int64_t>(s, DT_SPLIT_MAX);
-    const int64_t seg = ceil_div(ceil_div(ns, s), DT_THREADS) * DT_THREADS;
-    return {(int)ceil_div(ns, seg), seg};
+    const int64_t R = direct_resident_ctas();
+    if (tiles >= 4 * R || ns <= DT_SPLIT_MIN_SRC) return {1, ns > 0 ? ns : 1};
+    const int64_t smax = std::min<int64_t>(DT_SPLIT_MAX, ceil_div(ns, DT_SPLIT_MIN_SRC));
+    DirectSplit best{1, ns};
+    int64_t best_cost = INT64_MAX;
+    for (int64_t s = 1; s <= smax; ++s) {
+        const int64_t seg = ceil_div(ceil_div(ns, s), (int64_t)DT_CHUNK) * DT_CHUNK;
+        const int64_t splits = ceil_div(ns, seg);
+        const int64_t cost = ceil_div(tiles * splits, R) * seg;
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = {(int)splits, splits > 1 ? seg : ns};
+        }
+    }
+    return best;
 }
 
 // Launch the plain direct sum on `stream` (no argument checks; used internally

@@ -16,11 +16,11 @@ struct DirectInstance {
     float4 *part;    // splits * nt partial sums when splits > 1
 };
 
-// Source segmentation of a direct sum: a function of the sizes only, so the
-// plain and batched paths cut (and round) identically.  Split when the target
-// tiles are fewer than DT_SPLIT_CTAS, into at most DT_SPLIT_MAX segments of
-// at least DT_SPLIT_MIN_SRC sources (a multiple of the 256-blob load tile).
-constexpr int64_t DT_SPLIT_CTAS = 1184;  // 8 CTAs on each of 148 SMs
+// Source segmentation of a direct sum: a function of the sizes and of the
+// device's resident CTA count only, so the plain and batched paths cut (and
+// round) identically.  At most DT_SPLIT_MAX segments of at least
+// DT_SPLIT_MIN_SRC sources, whole 32-source chunks (direct.cu).
+constexpr int64_t DT_SPLIT_CTAS = 740;  // resident CTAs if the device can't be asked: 5 x 148
 constexpr int64_t DT_SPLIT_MIN_SRC = 256;
 constexpr int64_t DT_SPLIT_MAX = 64;
 struct DirectSplit {
